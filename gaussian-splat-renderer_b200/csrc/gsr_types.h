@@ -1,0 +1,37 @@
+// Types and constants shared by the host renderer and the kernels (host-safe: no device code).
+#pragma once
+
+#include <cstdint>
+
+#include "gsr_b200.h"
+
+namespace gsr {
+
+constexpr int kTileSize = 16;                  // INRIA BLOCK_X = BLOCK_Y (splat_math.h:32)
+constexpr uint32_t kCullReasonCount = 5;       // Visible, NearPlane, SingularCov, OffScreen, LowOpacity
+constexpr uint32_t kCullVisible = 0, kCullNear = 1, kCullSingular = 2, kCullOffScreen = 3, kCullLowOpacity = 4;
+constexpr uint32_t kBoundsRect = 0, kBoundsTight = 1, kBoundsCutoff = 2;
+
+// Iteration limit of every device-side wait; on expiry the kernel records
+// GSR_CONTROL_TIMEOUT + where, stops waiting and finishes (the frame is then invalid).
+constexpr uint32_t kSpinLimit = 1u << 22;
+enum WaitSite : uint32_t { kWaitScan = 1, kWaitSort = 2, kWaitStandaloneScan = 3 };
+
+// The per-frame control block in device memory (GsrControl in gsr_b200.h) plus scratch
+// counters that only the kernels use.
+struct DeviceControl {
+    GsrControl c;
+    uint32_t tickets[16];       // block tickets: [0] preprocess, [1 + p] sort pass p, [12] standalone scan
+    uint32_t histDone;          // blocks of the histogram kernel that have finished
+    uint32_t forceTimeout;      // test hook: look-back waits see no predecessor for this many spins
+    uint32_t pad[14];
+};
+
+// The C library's logf fixup table on the device (see libcLogf in gsr_device.cuh).
+struct LogfFixups {
+    const uint32_t* entries;       // ((x_bits - base) << 1) | up, sorted
+    const uint32_t* bucketStart;   // per 1024-input bucket
+    uint32_t base, last, count;
+};
+
+}  // namespace gsr

@@ -1,0 +1,414 @@
+// The front of the splat-tiles frame: reset, then ONE kernel per frame that does, per gaussian
+// (one thread each, 256 per block, blocks ordered by a ticket):
+//
+//   scene decode  -> preprocess (near/opacity culls, cov3D, EWA cov2D, conic/radius, pixel
+//   centre, 16-px rectangle, SH colour) -> tight tile count -> block scan + decoupled
+//   look-back (the exclusive prefix of the counts in index order = the list offsets)
+//   -> key emission (one (tile << 32 | depth bits, index) entry per covered tile)
+//
+// i.e. the reference's passes splat_preprocess.comp (GSR_TILES), scan_reduce/blocks/downsweep
+// over the tile counts, tile_setup.comp and tile_duplicate.comp (global mode, per splat), in
+// one read of each gaussian. The placement comes from the scan in index order (INRIA's
+// scheme), so the unsorted list equals the reference's entry for entry; atomics are used only
+// for counters. Built with -fmad=false: see splat_math.cuh.
+#include <cuda_fp16.h>
+
+#include "kernels.cuh"
+#include "splat_math.cuh"
+
+namespace gsr {
+
+namespace {
+
+constexpr int kFrontThreads = 256;
+
+__device__ __forceinline__ float halfLo(uint32_t w) { return __half2float(__ushort_as_half(uint16_t(w & 0xFFFFu))); }
+__device__ __forceinline__ float halfHi(uint32_t w) { return __half2float(__ushort_as_half(uint16_t(w >> 16))); }
+__device__ __forceinline__ uint32_t word(const uint4& v, int j) { return j == 0 ? v.x : j == 1 ? v.y : j == 2 ? v.z : v.w; }
+
+// ---- scene decode (shaders/scene_decode.glsl; CPU twin decodeGaussian,
+//      src/scene/scene_compression.cpp:382-460) ------------------------------------------
+template <int GEOM>
+__device__ __forceinline__ float4 loadPosAlpha(const SceneArgs& s, uint32_t i) {
+    if (GEOM == GSR_GEOMETRY_SOA_F32) {
+        const uint4 w = __ldg(&s.b0[i]);
+        return make_float4(__uint_as_float(w.x), __uint_as_float(w.y), __uint_as_float(w.z), __uint_as_float(w.w));
+    }
+    const uint4 w = __ldg(&s.b0[size_t(i) * s.geometryStride]);
+    if (GEOM == GSR_GEOMETRY_RECORD_F32)
+        return make_float4(__uint_as_float(w.x), __uint_as_float(w.y), __uint_as_float(w.z), __uint_as_float(w.w));
+    return make_float4(__uint_as_float(w.x), __uint_as_float(w.y), __uint_as_float(w.z), halfLo(w.w));
+}
+
+template <int GEOM>
+__device__ __forceinline__ void loadShape(const SceneArgs& s, uint32_t i, float sigma[3], float q[4], uint32_t& meta) {
+    if (GEOM == GSR_GEOMETRY_SOA_F32) {
+        const uint4 sc = __ldg(&s.b1[i]);
+        const uint4 ro = __ldg(&s.b2[i]);
+        sigma[0] = __uint_as_float(sc.x); sigma[1] = __uint_as_float(sc.y); sigma[2] = __uint_as_float(sc.z);
+        meta = sc.w;
+        q[0] = __uint_as_float(ro.x); q[1] = __uint_as_float(ro.y); q[2] = __uint_as_float(ro.z); q[3] = __uint_as_float(ro.w);
+    } else if (GEOM == GSR_GEOMETRY_RECORD_F32) {
+        const size_t base = size_t(i) * s.geometryStride;
+        const uint4 g1 = __ldg(&s.b0[base + 1]);
+        const uint4 g2 = __ldg(&s.b0[base + 2]);
+        sigma[0] = __uint_as_float(g1.x); sigma[1] = __uint_as_float(g1.y); sigma[2] = __uint_as_float(g1.z);
+        meta = g1.w;
+        q[0] = __uint_as_float(g2.x); q[1] = __uint_as_float(g2.y); q[2] = __uint_as_float(g2.z); q[3] = __uint_as_float(g2.w);
+    } else {  // G16: word 3 = h(alpha, sx), 4 = h(sy, sz), 5 = h(qw, qx), 6 = h(qy, qz), 7 = meta
+        const size_t base = size_t(i) * s.geometryStride;
+        const uint32_t w3 = __ldg(&s.b0[base].w);
+        const uint4 b = __ldg(&s.b0[base + 1]);
+        sigma[0] = halfHi(w3); sigma[1] = halfLo(b.x); sigma[2] = halfHi(b.x);
+        const float r0 = halfLo(b.y), r1 = halfHi(b.y), r2 = halfLo(b.z), r3 = halfHi(b.z);
+        // decodeGaussian: q * (1 / sqrt(len2)), identity for a zero quaternion
+        const float len2 = r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
+        if (len2 > 0.0f) {
+            const float inv = 1.0f / sqrtf(len2);
+            q[0] = r0 * inv; q[1] = r1 * inv; q[2] = r2 * inv; q[3] = r3 * inv;
+        } else {
+            q[0] = 1.0f; q[1] = 0.0f; q[2] = 0.0f; q[3] = 0.0f;
+        }
+        meta = b.w;
+    }
+}
+
+// The first `used` SH triplets of gaussian i into sh[k*3 + c] (loadSH, scene_decode.glsl:107-190).
+template <int COLOR>
+__device__ __forceinline__ void loadSH(const SceneArgs& s, uint32_t i, uint32_t used, uint32_t meta, float sh[48]) {
+    const uint32_t K = s.storedCoeffs;
+    if (COLOR == GSR_COLOR_SOA_F32) {
+        if (K == 16 && s.variableSh == GSR_VARIABLE_SH_OFF) {
+            const float4* p = reinterpret_cast<const float4*>(s.shSoa) + size_t(i) * 12;
+#pragma unroll
+            for (int v = 0; v < 12; ++v) {
+                if (uint32_t(v) * 4 < used * 3) {
+                    const float4 f = __ldg(&p[v]);
+                    sh[v * 4 + 0] = f.x; sh[v * 4 + 1] = f.y; sh[v * 4 + 2] = f.z; sh[v * 4 + 3] = f.w;
+                }
+            }
+            return;
+        }
+        const size_t base = s.variableSh == GSR_VARIABLE_SH_COMPACT ? size_t(meta & 0x3FFFFFFFu) : size_t(i) * K * 3;
+#pragma unroll
+        for (int k = 0; k < 48; ++k)
+            if (uint32_t(k) < used * 3) sh[k] = __ldg(&s.shSoa[base + k]);
+        return;
+    }
+    const size_t base = s.variableSh == GSR_VARIABLE_SH_COMPACT ? size_t(meta & 0x3FFFFFFFu)
+                                                                : size_t(i) * s.colorStride + s.colorOffset;
+    if (COLOR == GSR_COLOR_RECORD_F32) {
+#pragma unroll
+        for (int v = 0; v < 12; ++v) {
+            if (uint32_t(v) * 4 < K * 3 && uint32_t(v) * 4 < used * 3) {
+                const uint4 w = __ldg(&s.b1[base + v]);
+                sh[v * 4 + 0] = __uint_as_float(w.x); sh[v * 4 + 1] = __uint_as_float(w.y);
+                sh[v * 4 + 2] = __uint_as_float(w.z); sh[v * 4 + 3] = __uint_as_float(w.w);
+            }
+        }
+    } else if (COLOR == GSR_COLOR_RECORD_F16) {
+#pragma unroll
+        for (int v = 0; v < 6; ++v) {
+            if (uint32_t(v) * 8 < K * 3 && uint32_t(v) * 8 < used * 3) {
+                const uint4 w = __ldg(&s.b1[base + v]);
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    sh[v * 8 + 2 * j] = halfLo(word(w, j));
+                    sh[v * 8 + 2 * j + 1] = halfHi(word(w, j));
+                }
+            }
+        }
+    } else {  // Q8: w0 = h(dc.r, dc.g), w1 = h(dc.b, s1), w2 = h(s2, s3), int8 rest from byte 12
+        uint4 w[4];
+#pragma unroll
+        for (int v = 0; v < 4; ++v)
+            w[v] = (uint32_t(v) * 16 < 12 + (K - 1) * 3 && uint32_t(v) * 16 < 12 + (used - 1) * 3) ? __ldg(&s.b1[base + v])
+                                                                                                    : make_uint4(0, 0, 0, 0);
+        sh[0] = halfLo(w[0].x); sh[1] = halfHi(w[0].x); sh[2] = halfLo(w[0].y);
+        const float scale1 = halfHi(w[0].y), scale2 = halfLo(w[0].z), scale3 = halfHi(w[0].z);
+#pragma unroll
+        for (int k = 1; k < 16; ++k) {
+            if (uint32_t(k) >= used) continue;
+            const float sc = k < 4 ? scale1 : (k < 9 ? scale2 : scale3);
+#pragma unroll
+            for (int ch = 0; ch < 3; ++ch) {
+                const int j = (k - 1) * 3 + ch;
+                const uint32_t wd = word(w[(3 + j / 4) >> 2], (3 + j / 4) & 3);
+                const int q = int(int8_t(uint8_t(wd >> (8 * (j % 4)))));
+                sh[k * 3 + ch] = float(q) * sc;
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t gaussianDegree(const SceneArgs& s, uint32_t meta) {
+    return s.variableSh == GSR_VARIABLE_SH_OFF ? 3u : (meta >> 30);
+}
+
+// preprocessGaussian (splat_math.cpp:153-193) with the GPU culls of splat_preprocess.comp.
+template <int GEOM, int COLOR>
+__device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, uint32_t i, DevSplat& s, TileRect& rect) {
+    const DevCamera& cam = reinterpret_cast<const DevCamera&>(a.cam);
+    const float4 pa = loadPosAlpha<GEOM>(a.scene, i);
+    const float* v = cam.v;
+    const float t[3] = {v[0] * pa.x + v[4] * pa.y + v[8] * pa.z + v[12], v[1] * pa.x + v[5] * pa.y + v[9] * pa.z + v[13],
+                        v[2] * pa.x + v[6] * pa.y + v[10] * pa.z + v[14]};
+    s.depth = t[2];
+    if (!(t[2] > kNearCullDepth)) return kCullNear;
+    if (pa.w < GSR_MIN_ALPHA) return kCullLowOpacity;
+    float sigma[3], q[4];
+    uint32_t meta = 0;
+    loadShape<GEOM>(a.scene, i, sigma, q, meta);
+    float S[9], cov[3], conic[3], radius = 0.0f;
+    cov3d(sigma[0], sigma[1], sigma[2], q[0], q[1], q[2], q[3], S);
+    cov2d(t, S, cam, cov);
+    if (!conicAndRadius(cov, conic, radius)) return kCullSingular;
+    const float ndcX = t[0] / (t[2] * cam.tanHalfFovX);
+    const float ndcY = t[1] / (t[2] * cam.tanHalfFovY);
+    const float cx = ((ndcX + 1.0f) * float(cam.width) - 1.0f) * 0.5f;
+    const float cy = ((ndcY + 1.0f) * float(cam.height) - 1.0f) * 0.5f;
+    rect = tileRect(cx, cy, radius, cam.tilesX, cam.tilesY);
+    s.cx = cx;
+    s.cy = cy;
+    if (rect.maxX <= rect.minX || rect.maxY <= rect.minY) return kCullOffScreen;
+    const uint32_t gdeg = gaussianDegree(a.scene, meta);
+    const uint32_t degree = uint32_t(a.evalDegree) < gdeg ? uint32_t(a.evalDegree) : gdeg;
+    float sh[48];
+    loadSH<COLOR>(a.scene, i, (degree + 1) * (degree + 1), meta, sh);
+    const float d0 = pa.x - cam.pos[0], d1 = pa.y - cam.pos[1], d2 = pa.z - cam.pos[2];
+    const float inv = 1.0f / sqrtf(d0 * d0 + d1 * d1 + d2 * d2);  // glm::normalize
+    float color[3];
+    evalSH(int(degree), sh, d0 * inv, d1 * inv, d2 * inv, color);
+    s.conicA = conic[0];
+    s.conicB = conic[1];
+    s.conicC = conic[2];
+    s.opacity = pa.w;
+    s.r = color[0];
+    s.g = color[1];
+    s.b = color[2];
+    s.radius = radius;
+    return kCullVisible;
+}
+
+template <int GEOM, int COLOR>
+__global__ void __launch_bounds__(kFrontThreads) frontKernel(const __grid_constant__ FrontArgs a) {
+    __shared__ uint32_t sBlock;
+    __shared__ uint32_t sWarpTotals[kFrontThreads / 32];
+    __shared__ uint32_t sCull[kCullReasonCount];
+    __shared__ uint32_t sExclusive;
+    __shared__ uint32_t sDepthMin, sDepthMax, sTileMax, sMismatch;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    DeviceControl* ctl = a.ctl;
+    if (tid == 0) {
+        sBlock = atomicAdd(&ctl->tickets[0], 1u);
+        sDepthMin = 0xFFFFFFFFu;
+        sDepthMax = 0;
+        sTileMax = 0;
+        sMismatch = 0;
+    }
+    if (tid < kCullReasonCount) sCull[tid] = 0;
+    __syncthreads();
+    const uint32_t block = sBlock;
+    const uint32_t i = block * kFrontThreads + tid;
+    const uint32_t epoch = ctl->c.epoch;
+
+    // 1) preprocess + tight count
+    uint32_t reason = kCullReasonCount;  // threads past the end
+    uint32_t count = 0;
+    DevSplat s;
+    TileRect rect{0, 0, 0, 0};
+    Coverage cv;
+    cv.useEllipse = false;
+    cv.bins = BinRect{0, 0, 0, 0};
+    if (i < a.count) {
+        reason = preprocessOne<GEOM, COLOR>(a, i, s, rect);
+        if (reason == kCullVisible) {
+            cv = makeCoverage(a.bounds, rect, a.binSize, a.gridX, a.gridY, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
+                              s.opacity, a.logf);
+            count = coverageCount(cv, a.binSize);
+            s.cullReason = kCullVisible;
+            reinterpret_cast<DevSplat*>(a.splats)[i] = s;
+        }
+        a.tileCounts[i] = count;
+    }
+    // cull counters: one ballot per reason and warp, one atomic per reason and block
+#pragma unroll
+    for (uint32_t r = 0; r < kCullReasonCount; ++r) {
+        const uint32_t n = __popc(__ballot_sync(0xFFFFFFFFu, reason == r));
+        if (lane == 0 && n) atomicAdd(&sCull[r], n);
+    }
+
+    // 2) block scan of the counts
+    uint32_t incl = count;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= uint32_t(d)) incl += o;
+    }
+    if (lane == 31) sWarpTotals[warp] = incl;
+    __syncthreads();
+    uint32_t warpBase = 0, blockTotal = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kFrontThreads / 32; ++w) {
+        const uint32_t t = sWarpTotals[w];
+        if (w < warp) warpBase += t;
+        blockTotal += t;
+    }
+    const uint32_t threadExclusive = warpBase + incl - count;
+
+    // 3) decoupled look-back over the blocks before this one
+    if (warp == 0) {
+        if (lane == 0)
+            stRelease(&a.scanStatus[block], packStatus(epoch, block == 0 ? kFlagInclusive : kFlagAggregate, blockTotal));
+        uint32_t exclusive = 0;
+        if (block > 0) exclusive = warpLookback(a.scanStatus, int(block), epoch, ctl, kWaitScan);
+        if (lane == 0) {
+            if (block > 0) stRelease(&a.scanStatus[block], packStatus(epoch, kFlagInclusive, exclusive + blockTotal));
+            sExclusive = exclusive;
+        }
+    }
+    if (tid < kCullReasonCount && sCull[tid]) atomicAdd(&ctl->c.cull_counts[tid], sCull[tid]);
+    __syncthreads();
+    const uint32_t offset = sExclusive + threadExclusive;
+    if (i < a.count) a.offsets[i] = offset;
+
+    // 4) the list size and its clamp (tile_setup.comp:16-24), by the last block
+    if (block == gridDim.x - 1 && tid == 0) {
+        const uint32_t m = sExclusive + blockTotal;
+        const uint32_t entries = m < a.capacity ? m : a.capacity;
+        ctl->c.duplicates = m;
+        ctl->c.entries = entries;
+        ctl->c.overflow = m - entries;
+        ctl->c.ranges_groups[0] = (entries + 255u) / 256u;
+        ctl->c.ranges_groups[1] = 1;
+        ctl->c.ranges_groups[2] = 1;
+    }
+
+    // 5) key emission (tile_duplicate.comp:177-221, global mode): the splat's tiles row by
+    //    row at offsets [offset, offset + count), dropped at or past the capacity
+    if (count > 0) {
+        const uint64_t depthBits = __float_as_uint(s.depth);
+        const int S = a.binSize;
+        int r0, r1;
+        coverageRows(cv, S, r0, r1);
+        uint32_t written = 0;
+        uint32_t k = offset;
+        uint32_t tileMax = 0;
+        for (int row = r0; row < r1 && written < count; ++row) {
+            int x0, x1;
+            coverageRowSpan(cv, row, S, x0, x1);
+            for (int x = x0; x < x1 && written < count; ++x, ++written, ++k) {
+                const uint32_t tile = uint32_t(row) * uint32_t(a.gridX) + uint32_t(x);
+                tileMax = tile > tileMax ? tile : tileMax;
+                if (k < a.capacity) {
+                    a.keys[k] = (uint64_t(tile) << 32) | depthBits;
+                    a.values[k] = i;
+                }
+            }
+        }
+        // fewer tiles than counted (cannot happen: same functions, same thread): sentinel tile
+        const uint32_t sentinel = uint32_t(a.gridX) * uint32_t(a.gridY);
+        if (written != count) {
+            atomicAdd(&sMismatch, 1u);
+            tileMax = sentinel;
+            for (; written < count; ++written, ++k)
+                if (k < a.capacity) {
+                    a.keys[k] = (uint64_t(sentinel) << 32) | depthBits;
+                    a.values[k] = i;
+                }
+        }
+        atomicMin(&sDepthMin, uint32_t(depthBits));
+        atomicMax(&sDepthMax, uint32_t(depthBits));
+        atomicMax(&sTileMax, tileMax);
+    }
+    __syncthreads();
+    if (tid == 0 && blockTotal > 0) {
+        atomicMin(&ctl->c.depth_min_bits, sDepthMin);
+        atomicMax(&ctl->c.depth_max_bits, sDepthMax);
+        atomicMax(&ctl->c.tile_max, sTileMax);
+        if (sMismatch) atomicAdd(&ctl->c.coverage_mismatch, sMismatch);
+    }
+}
+
+// Per-frame reset of the control block (vkCmdUpdateBuffer of TileControl{N, 0, ...}) and of the
+// tile ranges (vkCmdFillBuffer 0), splat_tile_renderer.cpp:653-661. Block 0 resets the control
+// block and the sort histograms; every block zeroes a part of the ranges.
+__global__ void frameBeginKernel(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint4* ranges,
+                                 uint32_t rangeVec4s, SortPlan* plan, uint32_t forceTimeout) {
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    for (uint32_t j = g; j < rangeVec4s; j += gridDim.x * blockDim.x) ranges[j] = make_uint4(0, 0, 0, 0);
+    if (blockIdx.x != 0) return;
+    if (plan) {
+        uint32_t* h = &plan->hist[0][0];
+        for (uint32_t j = threadIdx.x; j < kMaxSortPasses * 256; j += blockDim.x) h[j] = 0;
+    }
+    if (threadIdx.x == 0) {
+        GsrControl& c = ctl->c;
+        const uint32_t epoch = ((c.epoch + 1u) & 0x3FFFFFFFu) ? ((c.epoch + 1u) & 0x3FFFFFFFu) : 1u;
+        c.gaussian_count = count;
+        c.visible = 0;
+        c.duplicates = 0;
+        c.entries = 0;
+        for (int r = 0; r < 8; ++r) c.cull_counts[r] = 0;
+        c.overflow = 0;
+        c.ranges_groups[0] = 0;
+        c.ranges_groups[1] = 1;
+        c.ranges_groups[2] = 1;
+        c.coverage_mismatch = 0;
+        c.status = 0;
+        c.timeout_where = 0;
+        c.epoch = epoch;
+        c.sort_passes = 0;
+        c.key_bits = 0;
+        c.depth_low_bits = 0;
+        c.depth_min_bits = 0xFFFFFFFFu;
+        c.depth_max_bits = 0;
+        c.tile_max = 0;
+        c.sorted_buffer = 0;
+        c.capacity = capacity;
+        for (int t = 0; t < 16; ++t) ctl->tickets[t] = 0;
+        ctl->histDone = 0;
+        ctl->forceTimeout = forceTimeout;
+    }
+}
+
+__global__ void logfTableKernel(float* out, LogfFixups t) {
+    const uint32_t n = t.last - t.base + 1;
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+        out[j] = libcLogf(__uint_as_float(t.base + j), t);
+}
+
+}  // namespace
+
+cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint32_t* ranges,
+                             uint32_t rangeWords, SortPlan* plan, uint32_t forceTimeout, cudaStream_t s) {
+    const uint32_t vec4s = (rangeWords + 3) / 4;
+    uint32_t blocks = (vec4s + 255) / 256;
+    blocks = blocks < 1 ? 1 : (blocks > 1184 ? 1184 : blocks);
+    frameBeginKernel<<<blocks, 256, 0, s>>>(ctl, count, capacity, reinterpret_cast<uint4*>(ranges), vec4s, plan,
+                                             forceTimeout);
+    return cudaGetLastError();
+}
+
+cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s) {
+    const uint32_t blocks = (a.count + kFrontThreads - 1) / kFrontThreads;
+    if (blocks == 0) return cudaSuccess;
+    if (geometry == GSR_GEOMETRY_SOA_F32 && color == GSR_COLOR_SOA_F32)
+        frontKernel<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32><<<blocks, kFrontThreads, 0, s>>>(a);
+    else if (geometry == GSR_GEOMETRY_RECORD_F32 && color == GSR_COLOR_RECORD_F32)
+        frontKernel<GSR_GEOMETRY_RECORD_F32, GSR_COLOR_RECORD_F32><<<blocks, kFrontThreads, 0, s>>>(a);
+    else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_RECORD_F16)
+        frontKernel<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16><<<blocks, kFrontThreads, 0, s>>>(a);
+    else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_Q8)
+        frontKernel<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8><<<blocks, kFrontThreads, 0, s>>>(a);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launchLogfTable(float* out, LogfFixups t, cudaStream_t s) {
+    logfTableKernel<<<148 * 8, 256, 0, s>>>(out, t);
+    return cudaGetLastError();
+}
+
+}  // namespace gsr

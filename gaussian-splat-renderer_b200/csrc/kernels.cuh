@@ -1,0 +1,105 @@
+// Kernel argument blocks and launch entry points shared between the CUDA translation units
+// and the host renderer (renderer.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "gsr_types.h"
+
+namespace gsr {
+
+struct DevCameraArgs {  // = DevCamera (splat_math.cuh)
+    float v[16];
+    float pos[3];
+    uint32_t width, height;
+    float tanHalfFovX, tanHalfFovY, focalX, focalY;
+    uint32_t tilesX, tilesY;
+};
+
+struct SceneArgs {
+    const uint4* b0;     // soa posAlpha | geometry records | aos records
+    const uint4* b1;     // soa scales   | colour records   | aos records
+    const uint4* b2;     // soa rotations
+    const float* shSoa;  // soa sh float[]
+    uint32_t geometryStride, colorStride, colorOffset;
+    uint32_t storedCoeffs;  // K
+    uint32_t variableSh;    // GsrVariableSh
+};
+
+// Arguments of the fused per-gaussian kernel (preprocess + count + scan + key emission).
+struct FrontArgs {
+    DevCameraArgs cam;
+    SceneArgs scene;
+    uint32_t count;       // N
+    int evalDegree;       // min(stored degree, max_sh_degree)
+    uint32_t bounds;      // GsrTileBounds
+    int binSize;          // S (16)
+    int gridX, gridY;     // bin grid
+    uint32_t capacity;    // list entries
+    void* splats;         // DevSplat[N]
+    uint32_t* tileCounts; // [N]
+    uint32_t* offsets;    // [N] exclusive scan of tileCounts
+    uint64_t* keys;       // [capacity] (tile << 32 | depth bits), index order
+    uint32_t* values;     // [capacity]
+    uint64_t* scanStatus; // [ceil(N / 256)] look-back words
+    DeviceControl* ctl;
+    LogfFixups logf;
+};
+
+// Sort plan written by the histogram kernel's last block.
+constexpr int kMaxSortPasses = 8;
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+struct SortPlan {
+    uint32_t passes;        // significant 8-bit digits of the virtual key
+    uint32_t lowBits;       // W: low key bits kept below the high word
+    uint32_t keyBits;
+    uint32_t active[kMaxSortPasses];
+    uint32_t inBuffer[kMaxSortPasses];
+    uint32_t digitBase[kMaxSortPasses][256];
+    uint32_t hist[kMaxSortPasses][256];
+};
+
+struct SortArgs {
+    uint64_t* keys[2];
+    uint32_t* values[2];
+    uint64_t* status;      // [kMaxSortPasses][maxTiles][256]
+    uint32_t maxTiles;     // ceil(capacity / kSortTile)
+    SortPlan* plan;
+    DeviceControl* ctl;
+    uint32_t passesLaunched;
+    // plan source: frameMode = 1 derives the low bits from the frame's depth range and the high
+    // bits from the largest tile id; 0 uses fixedLowBits/fixedKeyBits (standalone sort).
+    uint32_t frameMode;
+    uint32_t fixedLowBits, fixedKeyBits;
+};
+
+struct RenderArgs {
+    const void* splats;       // DevSplat[N]
+    const uint32_t* values[2];
+    const uint64_t* keys[2];
+    uint32_t* ranges;         // uint2 per tile
+    float4* image;            // W*H
+    uint8_t* rgb8;            // W*H*3 or null
+    uint32_t width, height, tilesX, tilesY;
+    DeviceControl* ctl;
+};
+
+// ---- launchers (return cudaGetLastError()) ---------------------------------------------------
+cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint32_t* ranges,
+                             uint32_t rangeWords, SortPlan* plan, uint32_t forceTimeout, cudaStream_t s);
+cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s);
+cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s);
+cudaError_t launchRanges(const RenderArgs& a, uint32_t capacity, cudaStream_t s);
+cudaError_t launchRender(const RenderArgs& a, cudaStream_t s);
+cudaError_t launchLogfTable(float* out, LogfFixups t, cudaStream_t s);
+cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
+                       uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s);
+cudaError_t launchPack64(const uint32_t* lo, const uint32_t* hi, uint64_t* out, uint32_t n, cudaStream_t s);
+cudaError_t launchUnpack64(const uint64_t* in, uint32_t* lo, uint32_t* hi, uint32_t n, cudaStream_t s);
+cudaError_t launchSetEntries(DeviceControl* ctl, uint32_t count, cudaStream_t s);
+
+}  // namespace gsr

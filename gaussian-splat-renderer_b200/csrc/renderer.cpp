@@ -1,0 +1,945 @@
+// Host side of the B200 splat-tiles path: the C ABI of include/gsr_b200.h over a C++ renderer
+// that mirrors gsr::SplatTileRenderer (src/render/splat_tile_renderer.h:143-290) and
+// gsr::GpuScene (src/render/gpu_scene.h:42-78), launching the kernels of k_front.cu,
+// k_sort.cu, k_render.cu and k_encode.cu on the caller's stream.
+//
+// Per frame (render):
+//   frameBegin   reset of the control block + tile ranges      (splat_tile_renderer.cpp:653-661)
+//   front        preprocess + count + scan + setup + duplicate (passes 1, 2, 6, 7)
+//   sort         histogram/plan + onesweep passes               (pass 8, global 64-bit keys)
+//   ranges       per-tile [start, end)                          (pass 9)
+//   render       the tile rasterizer                            (pass 10)
+//   readback     control block -> the frame slot's pinned buffer, read frames_in_flight later
+//
+// Counts (V, M, entries) exist only on the device; grids over the list are sized for the
+// capacity and read the entry count from the control block, as the reference's indirect
+// dispatches do. The adaptive list (splat_tile_renderer.cpp:444-486) follows the measured M.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "encode.cuh"
+#include "gsr_b200.h"
+#include "kernels.cuh"
+
+extern "C" {
+extern const uint32_t gsr_logf_fixup_base, gsr_logf_fixup_last, gsr_logf_fixup_count, gsr_logf_bucket_count;
+extern const uint32_t gsr_logf_fixups[];
+extern const uint32_t gsr_logf_bucket_start[];
+}
+
+namespace {
+
+using namespace gsr;
+
+thread_local std::string g_lastError;
+
+int fail(int status, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_lastError = buf;
+    return status;
+}
+
+int cudaFail(cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation)
+        return fail(GSR_ERROR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+    return fail(GSR_ERROR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define GSR_CUDA(call)                                           \
+    do {                                                         \
+        const cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cudaFail(e_, #call);       \
+    } while (0)
+
+constexpr uint32_t kBlockSize = 2048;                    // list capacity granularity (GpuRadixSort::kBlockSize)
+constexpr uint32_t kMinAdaptiveCapacity = 256u * 1024u;  // entries (splat_tile_renderer.cpp:104)
+
+uint32_t bitWidth(uint32_t x) { return x ? 32u - uint32_t(__builtin_clz(x)) : 0u; }
+
+uint32_t roundUpToBlock(uint64_t n) {
+    const uint64_t b = kBlockSize;
+    return uint32_t(std::min<uint64_t>((n + b - 1) / b * b, 0xFFFFF800ull));
+}
+
+// ---- device-wide constant tables (the logf fixups), once per device ---------------------------
+struct DeviceTables {
+    uint32_t* entries = nullptr;
+    uint32_t* buckets = nullptr;
+};
+std::mutex g_tablesMutex;
+DeviceTables g_tables[64];
+
+int deviceTables(LogfFixups* out) {
+    int dev = 0;
+    GSR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(GSR_ERROR_UNSUPPORTED, "device index %d", dev);
+    std::lock_guard<std::mutex> lock(g_tablesMutex);
+    DeviceTables& t = g_tables[dev];
+    if (!t.entries) {
+        const size_t eb = size_t(std::max(gsr_logf_fixup_count, 1u)) * 4, bb = size_t(gsr_logf_bucket_count) * 4;
+        GSR_CUDA(cudaMalloc(&t.entries, eb));
+        GSR_CUDA(cudaMalloc(&t.buckets, bb));
+        GSR_CUDA(cudaMemcpy(t.entries, gsr_logf_fixups, eb, cudaMemcpyHostToDevice));
+        GSR_CUDA(cudaMemcpy(t.buckets, gsr_logf_bucket_start, bb, cudaMemcpyHostToDevice));
+    }
+    out->entries = t.entries;
+    out->bucketStart = t.buckets;
+    out->base = gsr_logf_fixup_base;
+    out->last = gsr_logf_fixup_last;
+    out->count = gsr_logf_fixup_count;
+    return GSR_OK;
+}
+
+// ---- camera (splat_math.cpp:9-42), host, same evaluation order as the device and the oracle --
+void mul4(const float* a, const float* b, float* r) {
+    for (int c = 0; c < 4; ++c)
+        for (int row = 0; row < 4; ++row)
+            r[c * 4 + row] = a[0 * 4 + row] * b[c * 4 + 0] + a[1 * 4 + row] * b[c * 4 + 1] + a[2 * 4 + row] * b[c * 4 + 2] +
+                             a[3 * 4 + row] * b[c * 4 + 3];
+}
+
+void splatCamera(const GsrCamera& in, GsrSplatCamera& cam) {
+    float flip[16], fv[16];
+    for (int i = 0; i < 16; ++i) flip[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+    flip[1 * 4 + 1] = -1.0f;
+    flip[2 * 4 + 2] = -1.0f;
+    mul4(flip, in.view, fv);
+    mul4(fv, in.model, cam.view_inria);
+    const float tanX = 1.0f / in.proj[0];
+    const float tanY = 1.0f / std::fabs(in.proj[1 * 4 + 1]);
+    const float* V = cam.view_inria;
+    for (int r = 0; r < 3; ++r)
+        cam.position[r] = -(V[r * 4 + 0] * V[12] + V[r * 4 + 1] * V[13] + V[r * 4 + 2] * V[14]);
+    cam.width = in.width;
+    cam.height = in.height;
+    cam.tan_half_fov_x = tanX;
+    cam.tan_half_fov_y = tanY;
+    cam.focal_x = float(in.width) / (2.0f * tanX);
+    cam.focal_y = float(in.height) / (2.0f * tanY);
+    cam.tiles_x = (in.width + 15) / 16;
+    cam.tiles_y = (in.height + 15) / 16;
+}
+
+// ---- device buffer RAII -------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t alloc(size_t n) {
+        release();
+        bytes = n;
+        return cudaMalloc(&p, std::max<size_t>(n, 16));
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+// ====================================================================================== scene
+struct GsrScene {
+    GsrSceneDesc desc{};
+    DevBuf buffers[4];
+};
+
+// ====================================================================================== renderer
+struct GsrRenderer {
+    GsrSceneDesc scene{};
+    GsrSettings settings{};
+    int evalDegree = 3;
+    LogfFixups logf{};
+
+    // per gaussian
+    DevBuf splats, tileCounts, offsets, scanStatus;
+    // control + plan
+    DevBuf control, plan;
+    // list
+    struct List {
+        uint32_t capacity = 0;
+        uint32_t maxTiles = 0;
+        uint32_t passes = 0;
+        DevBuf keys[2], values[2], status;
+        cudaEvent_t lastUse = nullptr;
+        ~List() {
+            if (lastUse) cudaEventDestroy(lastUse);
+        }
+    };
+    std::unique_ptr<List> list;
+    std::vector<std::unique_ptr<List>> retired;
+    uint32_t maxCapacity = 0;
+    uint32_t listResizes = 0;
+    uint32_t shrinkFrames = 0, shrinkWindowMax = 0;
+    uint64_t lastAdaptedFrame = ~0ull;
+    // per tile / image
+    uint32_t width = 0, height = 0, tilesX = 0, tilesY = 0;
+    uint32_t passesUpper = 0;
+    DevBuf ranges, image, rgb8;
+    // readback slots (2 frames late)
+    struct Slot {
+        GsrControl* host = nullptr;
+        cudaEvent_t done = nullptr;
+        bool used = false;
+        uint64_t frameIndex = 0;
+    };
+    std::vector<Slot> slots;
+    GsrControl lastStats{};
+    bool lastStatsValid = false;
+    uint64_t lastStatsFrame = 0;
+    uint64_t frameIndex = 0;
+    uint32_t forceTimeout = 0;
+    // timing
+    bool timing = false;
+    static constexpr int kPasses = 5;
+    cudaEvent_t ev[kPasses + 1] = {};
+    float passMs[kPasses] = {};
+    bool timed = false;
+
+    ~GsrRenderer() {
+        for (auto& s : slots) {
+            if (s.host) cudaFreeHost(s.host);
+            if (s.done) cudaEventDestroy(s.done);
+        }
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+
+    uint32_t passesFor(uint32_t tileCount) const {
+        // the largest key: tile ids < tileCount + 1 (sentinel) above up to 32 depth bits
+        const uint32_t keyBits = bitWidth(tileCount) + 32;
+        return (keyBits + 7) / 8;
+    }
+
+    double bytesPerEntry() const {
+        // keys (8 B) + values (4 B), each ping-ponged, + the look-back words of the passes
+        return 24.0 + 0.5 * double(std::max<uint32_t>(passesUpper, 6));
+    }
+
+    uint32_t capacityForBytes(double bytes) const {
+        uint32_t c = uint32_t(std::clamp(bytes / bytesPerEntry(), double(kBlockSize), double(0xFFFFF800u)));
+        return c - c % kBlockSize;
+    }
+
+    int createList(uint32_t capacity, std::unique_ptr<List>& out) {
+        auto l = std::make_unique<List>();
+        l->capacity = capacity;
+        l->maxTiles = (capacity + kSortTile - 1) / kSortTile;
+        l->passes = passesUpper;
+        for (int b = 0; b < 2; ++b) {
+            GSR_CUDA(l->keys[b].alloc(size_t(capacity) * 8));
+            GSR_CUDA(l->values[b].alloc(size_t(capacity) * 4));
+        }
+        GSR_CUDA(l->status.alloc(size_t(l->passes) * l->maxTiles * 256 * 8));
+        GSR_CUDA(cudaMemset(l->status.p, 0, l->status.bytes));
+        GSR_CUDA(cudaEventCreateWithFlags(&l->lastUse, cudaEventDisableTiming));
+        out = std::move(l);
+        return GSR_OK;
+    }
+
+    int resize(uint32_t w, uint32_t h) {
+        if (w == 0 || h == 0 || w > 32768 || h > 32768) return fail(GSR_ERROR_INVALID_ARGUMENT, "render size %ux%u", w, h);
+        if (w == width && h == height && list) return GSR_OK;
+        GSR_CUDA(cudaDeviceSynchronize());  // the reference calls onRenderTargetsChanged with the GPU idle
+        width = w;
+        height = h;
+        tilesX = (w + 15) / 16;
+        tilesY = (h + 15) / 16;
+        const uint32_t tileCount = tilesX * tilesY;
+        GSR_CUDA(ranges.alloc(size_t(tileCount) * 8));
+        GSR_CUDA(cudaMemset(ranges.p, 0, ranges.bytes));
+        GSR_CUDA(image.alloc(size_t(w) * h * 16));
+        if (settings.output_format == GSR_OUTPUT_RGBA32F_AND_RGB8) GSR_CUDA(rgb8.alloc(size_t(w) * h * 3));
+        else rgb8.release();
+        const uint32_t passes = passesFor(tileCount);
+        if (passes != passesUpper || !list) {
+            passesUpper = passes;
+            retired.clear();
+            maxCapacity = capacityForBytes(double(std::max(settings.budget_mb, 1u)) * 1024.0 * 1024.0);
+            uint32_t initial = maxCapacity;
+            if (settings.adaptive_list) {
+                const uint64_t guess = settings.adaptive_initial_entries
+                                           ? settings.adaptive_initial_entries
+                                           : std::max<uint64_t>(4ull * scene.count, 1u << 20);
+                initial = std::min(maxCapacity, roundUpToBlock(guess));
+            }
+            const int rc = createList(initial, list);
+            if (rc) return rc;
+        }
+        return GSR_OK;
+    }
+
+    // readSlot (splat_tile_renderer.cpp:572-613): consume a completed readback.
+    void readSlot(Slot& s) {
+        if (!s.used) return;
+        if (cudaEventQuery(s.done) != cudaSuccess) return;  // not finished: try again later
+        s.used = false;
+        if (lastStatsValid && s.frameIndex < lastStatsFrame) return;
+        lastStats = *s.host;
+        lastStatsValid = true;
+        lastStatsFrame = s.frameIndex;
+    }
+
+    // adaptCapacity (splat_tile_renderer.cpp:444-486).
+    int adaptCapacity(cudaStream_t stream) {
+        for (size_t i = 0; i < retired.size();) {
+            if (cudaEventQuery(retired[i]->lastUse) == cudaSuccess) retired.erase(retired.begin() + std::ptrdiff_t(i));
+            else ++i;
+        }
+        (void)stream;
+        if (!settings.adaptive_list || !lastStatsValid || lastStatsFrame == lastAdaptedFrame) return GSR_OK;
+        lastAdaptedFrame = lastStatsFrame;
+        const uint32_t m = lastStats.duplicates;
+        const uint32_t cap = list->capacity;
+        uint64_t target = 0;
+        if (double(m) > 0.9 * cap) {
+            target = uint64_t(1.5 * m);
+            shrinkFrames = 0;
+            shrinkWindowMax = 0;
+        } else if (double(m) < 0.4 * cap) {
+            shrinkWindowMax = std::max(shrinkWindowMax, m);
+            if (++shrinkFrames >= 120) {
+                target = uint64_t(1.5 * shrinkWindowMax);
+                shrinkFrames = 0;
+                shrinkWindowMax = 0;
+            }
+        } else {
+            shrinkFrames = 0;
+            shrinkWindowMax = 0;
+        }
+        if (target == 0) return GSR_OK;
+        const uint32_t newCap = std::clamp(roundUpToBlock(target), std::min(kMinAdaptiveCapacity, maxCapacity), maxCapacity);
+        if (newCap == cap || (newCap < cap && double(newCap) > 0.75 * cap)) return GSR_OK;
+        std::unique_ptr<List> fresh;
+        const int rc = createList(newCap, fresh);
+        if (rc) return rc;
+        retired.push_back(std::move(list));  // freed once its last frame has completed
+        list = std::move(fresh);
+        ++listResizes;
+        return GSR_OK;
+    }
+
+    int render(const GsrSplatCamera& cam, cudaStream_t stream) {
+        if (cam.width != width || cam.height != height) {
+            const int rc = resize(cam.width, cam.height);
+            if (rc) return rc;
+        }
+        if (slots.empty()) return fail(GSR_ERROR_INVALID_ARGUMENT, "renderer not initialised");
+        Slot& slot = slots[frameIndex % slots.size()];
+        readSlot(slot);
+        if (slot.used) {  // still in flight: wait for it (the reference's frame fence)
+            GSR_CUDA(cudaEventSynchronize(slot.done));
+            readSlot(slot);
+        }
+        int rc = adaptCapacity(stream);
+        if (rc) return rc;
+        List& l = *list;
+        DeviceControl* ctl = control.as<DeviceControl>();
+        SortPlan* sortPlan = plan.as<SortPlan>();
+        const uint32_t tileCount = tilesX * tilesY;
+        if (timing) GSR_CUDA(cudaEventRecord(ev[0], stream));
+
+        GSR_CUDA(launchFrameBegin(ctl, scene.count, l.capacity, ranges.as<uint32_t>(), tileCount * 2, sortPlan,
+                                  forceTimeout, stream));
+        forceTimeout = 0;
+        FrontArgs fa{};
+        static_assert(sizeof(DevCameraArgs) == sizeof(GsrSplatCamera), "camera layout");
+        std::memcpy(&fa.cam, &cam, sizeof(cam));
+        fa.scene.b0 = static_cast<const uint4*>(scene.buffers[0]);
+        fa.scene.b1 = static_cast<const uint4*>(scene.layout == GSR_LAYOUT_AOS ? scene.buffers[0] : scene.buffers[1]);
+        fa.scene.b2 = static_cast<const uint4*>(scene.buffers[2]);
+        fa.scene.shSoa = static_cast<const float*>(scene.buffers[3]);
+        fa.scene.geometryStride = scene.geometry_stride;
+        fa.scene.colorStride = scene.color_stride;
+        fa.scene.colorOffset = scene.color_offset;
+        fa.scene.storedCoeffs = scene.sh_coeffs;
+        fa.scene.variableSh = scene.variable_sh;
+        fa.count = scene.count;
+        fa.evalDegree = evalDegree;
+        fa.bounds = settings.bounds;
+        fa.binSize = int(settings.tile_size);
+        fa.gridX = int(tilesX);
+        fa.gridY = int(tilesY);
+        fa.capacity = l.capacity;
+        fa.splats = splats.p;
+        fa.tileCounts = tileCounts.as<uint32_t>();
+        fa.offsets = offsets.as<uint32_t>();
+        fa.keys = l.keys[0].as<uint64_t>();
+        fa.values = l.values[0].as<uint32_t>();
+        fa.scanStatus = scanStatus.as<uint64_t>();
+        fa.ctl = ctl;
+        fa.logf = logf;
+        GSR_CUDA(launchFront(fa, scene.geometry, scene.color, stream));
+        if (timing) GSR_CUDA(cudaEventRecord(ev[1], stream));
+
+        SortArgs sa{};
+        for (int b = 0; b < 2; ++b) {
+            sa.keys[b] = l.keys[b].as<uint64_t>();
+            sa.values[b] = l.values[b].as<uint32_t>();
+        }
+        sa.status = l.status.as<uint64_t>();
+        sa.maxTiles = l.maxTiles;
+        sa.plan = sortPlan;
+        sa.ctl = ctl;
+        sa.passesLaunched = l.passes;
+        sa.frameMode = 1;
+        GSR_CUDA(launchSort(sa, 148 * 2, stream));
+        if (timing) GSR_CUDA(cudaEventRecord(ev[2], stream));
+
+        RenderArgs ra{};
+        ra.splats = splats.p;
+        for (int b = 0; b < 2; ++b) {
+            ra.values[b] = l.values[b].as<uint32_t>();
+            ra.keys[b] = l.keys[b].as<uint64_t>();
+        }
+        ra.ranges = ranges.as<uint32_t>();
+        ra.image = image.as<float4>();
+        ra.rgb8 = rgb8.as<uint8_t>();
+        ra.width = width;
+        ra.height = height;
+        ra.tilesX = tilesX;
+        ra.tilesY = tilesY;
+        ra.ctl = ctl;
+        GSR_CUDA(launchRanges(ra, l.capacity, stream));
+        if (timing) GSR_CUDA(cudaEventRecord(ev[3], stream));
+        GSR_CUDA(launchRender(ra, stream));
+        if (timing) GSR_CUDA(cudaEventRecord(ev[4], stream));
+
+        GSR_CUDA(cudaMemcpyAsync(slot.host, &ctl->c, sizeof(GsrControl), cudaMemcpyDeviceToHost, stream));
+        GSR_CUDA(cudaEventRecord(slot.done, stream));
+        GSR_CUDA(cudaEventRecord(l.lastUse, stream));
+        if (timing) GSR_CUDA(cudaEventRecord(ev[5], stream));
+        slot.used = true;
+        slot.frameIndex = frameIndex;
+        timed = timing;
+        ++frameIndex;
+        return GSR_OK;
+    }
+};
+
+namespace {
+
+int validateScene(const GsrSceneDesc& s) {
+    if (s.count == 0) return fail(GSR_ERROR_INVALID_ARGUMENT, "empty scene");
+    if (s.sh_degree < 0 || s.sh_degree > 3) return fail(GSR_ERROR_INVALID_ARGUMENT, "sh_degree %d", s.sh_degree);
+    if (s.sh_coeffs != uint32_t((s.sh_degree + 1) * (s.sh_degree + 1)))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "sh_coeffs %u for degree %d", s.sh_coeffs, s.sh_degree);
+    const bool soa = s.geometry == GSR_GEOMETRY_SOA_F32 && s.color == GSR_COLOR_SOA_F32;
+    const bool f32 = s.geometry == GSR_GEOMETRY_RECORD_F32 && s.color == GSR_COLOR_RECORD_F32;
+    const bool f16 = s.geometry == GSR_GEOMETRY_RECORD_F16 && s.color == GSR_COLOR_RECORD_F16;
+    const bool q8 = s.geometry == GSR_GEOMETRY_RECORD_F16 && s.color == GSR_COLOR_Q8;
+    if (s.color == GSR_COLOR_CODEBOOK)
+        return fail(GSR_ERROR_UNSUPPORTED, "the codebook (cb) scene format is not implemented by this build");
+    if (!(soa || f32 || f16 || q8))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "geometry encoding %u with colour encoding %u", s.geometry, s.color);
+    if (s.variable_sh > GSR_VARIABLE_SH_COMPACT) return fail(GSR_ERROR_INVALID_ARGUMENT, "variable_sh %u", s.variable_sh);
+    if (soa && (!s.buffers[0] || !s.buffers[1] || !s.buffers[2] || !s.buffers[3]))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "soa scene needs 4 buffers");
+    if (!soa && (!s.buffers[0] || (s.layout != GSR_LAYOUT_AOS && !s.buffers[1])))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "record scene needs its buffers");
+    if (!soa && s.geometry_stride == 0) return fail(GSR_ERROR_INVALID_ARGUMENT, "geometry_stride 0");
+    for (int b = 0; b < 4; ++b)
+        if (reinterpret_cast<uintptr_t>(s.buffers[b]) % 16 != 0)
+            return fail(GSR_ERROR_INVALID_ARGUMENT, "scene buffer %d is not 16-byte aligned", b);
+    return GSR_OK;
+}
+
+}  // namespace
+
+// ====================================================================================== C ABI
+extern "C" {
+
+int gsr_abi_version(void) { return GSR_ABI_VERSION; }
+
+const char* gsr_error_string(int status) {
+    switch (status) {
+        case GSR_OK: return "ok";
+        case GSR_ERROR_INVALID_ARGUMENT: return "invalid argument";
+        case GSR_ERROR_UNSUPPORTED: return "unsupported";
+        case GSR_ERROR_CUDA: return "CUDA error";
+        case GSR_ERROR_OUT_OF_MEMORY: return "out of device memory";
+        case GSR_ERROR_DEVICE_TIMEOUT: return "a device-side wait timed out";
+        case GSR_ERROR_NOT_READY: return "not ready";
+        default: return "unknown status";
+    }
+}
+
+const char* gsr_last_error_message(void) { return g_lastError.c_str(); }
+
+void gsr_settings_default(GsrSettings* s) {
+    if (!s) return;
+    std::memset(s, 0, sizeof(*s));
+    s->bounds = GSR_BOUNDS_TIGHT;
+    s->tile_size = 16;
+    s->budget_mb = 256;
+    s->adaptive_list = 1;
+    s->adaptive_initial_entries = 0;
+    s->max_sh_degree = 3;
+    s->output_format = GSR_OUTPUT_RGBA32F;
+    s->frames_in_flight = 2;
+    s->use_graph = 0;
+}
+
+int gsr_splat_camera_from_viewer(const GsrCamera* camera, GsrSplatCamera* out) {
+    if (!camera || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    splatCamera(*camera, *out);
+    return GSR_OK;
+}
+
+void gsr_look_at(const float eye[3], const float center[3], const float up[3], float view[16]) {
+    auto normalize = [](const float v[3], float o[3]) {
+        const float inv = 1.0f / std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+        o[0] = v[0] * inv;
+        o[1] = v[1] * inv;
+        o[2] = v[2] * inv;
+    };
+    auto cross = [](const float a[3], const float b[3], float o[3]) {
+        o[0] = a[1] * b[2] - b[1] * a[2];
+        o[1] = a[2] * b[0] - b[2] * a[0];
+        o[2] = a[0] * b[1] - b[0] * a[1];
+    };
+    auto dot = [](const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; };
+    const float d[3] = {center[0] - eye[0], center[1] - eye[1], center[2] - eye[2]};
+    float f[3], sr[3], s[3], u[3];
+    normalize(d, f);
+    cross(f, up, sr);
+    normalize(sr, s);
+    cross(s, f, u);
+    for (int i = 0; i < 16; ++i) view[i] = (i % 5 == 0) ? 1.0f : 0.0f;
+    view[0] = s[0]; view[4] = s[1]; view[8] = s[2];
+    view[1] = u[0]; view[5] = u[1]; view[9] = u[2];
+    view[2] = -f[0]; view[6] = -f[1]; view[10] = -f[2];
+    view[12] = -dot(s, eye);
+    view[13] = -dot(u, eye);
+    view[14] = dot(f, eye);
+}
+
+void gsr_perspective_vk(float fovy, float aspect, float zNear, float zFar, float proj[16]) {
+    const float t = std::tan(fovy / 2.0f);
+    for (int i = 0; i < 16; ++i) proj[i] = 0.0f;
+    proj[0] = 1.0f / (aspect * t);
+    proj[5] = -(1.0f / t);
+    proj[10] = zFar / (zNear - zFar);
+    proj[11] = -1.0f;
+    proj[14] = -(zFar * zNear) / (zFar - zNear);
+}
+
+// ---- scene ------------------------------------------------------------------------------------
+int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, GsrScene** out) {
+    if (!host || !options || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (host->count == 0 || host->sh_degree < 0 || host->sh_degree > 3 || !host->pos_alpha || !host->scales ||
+        !host->rotations || !host->sh)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "host scene (count %u, degree %d)", host->count, host->sh_degree);
+    const uint32_t fmt = options->format, layout = options->layout;
+    if (fmt == GSR_FORMAT_CB) return fail(GSR_ERROR_UNSUPPORTED, "the codebook (cb) scene format is not implemented");
+    if (fmt > GSR_FORMAT_Q8 || layout > GSR_LAYOUT_AOS) return fail(GSR_ERROR_INVALID_ARGUMENT, "format %u layout %u", fmt, layout);
+    if (fmt != GSR_FORMAT_F32 && layout == GSR_LAYOUT_SOA)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "scene layout 'soa' exists only for the f32 format (use split or aos)");
+    const uint32_t n = host->count;
+    const uint32_t srcK = uint32_t((host->sh_degree + 1) * (host->sh_degree + 1));
+    const int degree = std::clamp(std::min(host->sh_degree, options->max_sh_degree), 0, 3);
+    const uint32_t K = uint32_t((degree + 1) * (degree + 1));
+    const bool variable = options->sh_threshold >= 0.0f && degree > 0;
+
+    auto scene = std::make_unique<GsrScene>();
+    GsrSceneDesc& d = scene->desc;
+    d.count = n;
+    d.sh_degree = degree;
+    d.sh_coeffs = K;
+    d.format = fmt;
+    d.layout = layout;
+    // staging: the activated f32 arrays on the device
+    DevBuf pa, sc, ro, sh, degrees, sizes, offs;
+    GSR_CUDA(pa.alloc(size_t(n) * 16));
+    GSR_CUDA(sc.alloc(size_t(n) * 16));
+    GSR_CUDA(ro.alloc(size_t(n) * 16));
+    GSR_CUDA(sh.alloc(size_t(n) * srcK * 12));
+    GSR_CUDA(cudaMemcpy(pa.p, host->pos_alpha, pa.bytes, cudaMemcpyHostToDevice));
+    GSR_CUDA(cudaMemcpy(sc.p, host->scales, sc.bytes, cudaMemcpyHostToDevice));
+    GSR_CUDA(cudaMemcpy(ro.p, host->rotations, ro.bytes, cudaMemcpyHostToDevice));
+    GSR_CUDA(cudaMemcpy(sh.p, host->sh, sh.bytes, cudaMemcpyHostToDevice));
+
+    EncodeArgs ea{};
+    ea.pa = pa.as<float4>();
+    ea.sc = sc.as<float4>();
+    ea.ro = ro.as<float4>();
+    ea.sh = sh.as<float>();
+    ea.n = n;
+    ea.srcK = srcK;
+    ea.K = K;
+    ea.degree = degree;
+    ea.variable = variable ? 1 : 0;
+    ea.threshold255 = options->sh_threshold;
+    ea.layout = layout;
+    if (layout == GSR_LAYOUT_SOA) {
+        ea.geometry = GSR_GEOMETRY_SOA_F32;
+        ea.color = GSR_COLOR_SOA_F32;
+    } else {
+        ea.geometry = fmt == GSR_FORMAT_F32 ? GSR_GEOMETRY_RECORD_F32 : GSR_GEOMETRY_RECORD_F16;
+        ea.color = fmt == GSR_FORMAT_F32 ? GSR_COLOR_RECORD_F32 : fmt == GSR_FORMAT_F16 ? GSR_COLOR_RECORD_F16 : GSR_COLOR_Q8;
+    }
+    auto vec4sFor = [](uint32_t bytes) { return (bytes + 15u) / 16u; };
+    ea.geomWords = ea.geometry == GSR_GEOMETRY_RECORD_F16 ? 8u : 12u;
+    ea.colorWords = ea.color == GSR_COLOR_RECORD_F32   ? vec4sFor(K * 12) * 4
+                    : ea.color == GSR_COLOR_RECORD_F16 ? vec4sFor(K * 6) * 4
+                    : ea.color == GSR_COLOR_Q8         ? vec4sFor(12 + (K - 1) * 3) * 4
+                                                       : 0;
+    GSR_CUDA(degrees.alloc(n));
+    const bool compact = variable && (layout == GSR_LAYOUT_SOA || layout == GSR_LAYOUT_SPLIT);
+    uint64_t compactTotal = 0;
+    if (compact) {
+        GSR_CUDA(sizes.alloc(size_t(n) * 4));
+        GSR_CUDA(offs.alloc(size_t(n) * 4));
+    }
+    GSR_CUDA(launchEncodeDegrees(ea, degrees.as<uint8_t>(), compact ? sizes.as<uint32_t>() : nullptr, 0));
+    if (compact) {
+        DevBuf total;
+        GSR_CUDA(total.alloc(4));
+        const int rc = gsr_scan(sizes.as<uint32_t>(), nullptr, offs.as<uint32_t>(), total.as<uint32_t>(), n, GSR_SCAN_PLAIN, nullptr);
+        if (rc) return rc;
+        uint32_t t = 0;
+        GSR_CUDA(cudaMemcpy(&t, total.p, 4, cudaMemcpyDeviceToHost));
+        compactTotal = t;
+        if (compactTotal >= (1ull << 30)) return fail(GSR_ERROR_INVALID_ARGUMENT, "variable SH: compacted data exceeds 2^30");
+    }
+    size_t bytes[4] = {0, 0, 0, 0};
+    if (layout == GSR_LAYOUT_SOA) {
+        bytes[0] = bytes[1] = bytes[2] = size_t(n) * 16;
+        bytes[3] = (compact ? size_t(compactTotal) : size_t(n) * K * 3) * 4;
+        d.geometry = GSR_GEOMETRY_SOA_F32;
+        d.color = GSR_COLOR_SOA_F32;
+        d.variable_sh = variable ? GSR_VARIABLE_SH_COMPACT : GSR_VARIABLE_SH_OFF;
+    } else if (layout == GSR_LAYOUT_SPLIT) {
+        bytes[0] = size_t(n) * ea.geomWords * 4;
+        bytes[1] = compact ? size_t(compactTotal) * 16 : size_t(n) * ea.colorWords * 4;
+        d.geometry = ea.geometry;
+        d.color = ea.color;
+        d.geometry_stride = ea.geomWords / 4;
+        d.color_stride = ea.colorWords / 4;
+        d.variable_sh = variable ? GSR_VARIABLE_SH_COMPACT : GSR_VARIABLE_SH_OFF;
+    } else {
+        bytes[0] = size_t(n) * (ea.geomWords + ea.colorWords) * 4;
+        d.geometry = ea.geometry;
+        d.color = ea.color;
+        d.geometry_stride = (ea.geomWords + ea.colorWords) / 4;
+        d.color_stride = (ea.geomWords + ea.colorWords) / 4;
+        d.color_offset = ea.geomWords / 4;
+        d.variable_sh = variable ? GSR_VARIABLE_SH_DEGREE_ONLY : GSR_VARIABLE_SH_OFF;
+    }
+    for (int b = 0; b < 4; ++b) {
+        if (!bytes[b]) continue;
+        GSR_CUDA(scene->buffers[b].alloc(bytes[b]));
+        GSR_CUDA(cudaMemset(scene->buffers[b].p, 0, bytes[b]));
+        ea.out[b] = scene->buffers[b].p;
+        d.buffers[b] = scene->buffers[b].p;
+        d.buffer_bytes[b] = bytes[b];
+    }
+    GSR_CUDA(launchEncodeRecords(ea, degrees.as<uint8_t>(), compact ? offs.as<uint32_t>() : nullptr, 0));
+    GSR_CUDA(cudaDeviceSynchronize());
+    *out = scene.release();
+    return GSR_OK;
+}
+
+int gsr_scene_get_desc(const GsrScene* scene, GsrSceneDesc* out) {
+    if (!scene || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = scene->desc;
+    return GSR_OK;
+}
+
+int gsr_scene_read_buffer(const GsrScene* scene, uint32_t b, void* host, uint64_t bytes) {
+    if (!scene || b > 3 || !host) return fail(GSR_ERROR_INVALID_ARGUMENT, "bad argument");
+    if (bytes != scene->desc.buffer_bytes[b]) return fail(GSR_ERROR_INVALID_ARGUMENT, "size %llu != %llu",
+                                                          (unsigned long long)bytes, (unsigned long long)scene->desc.buffer_bytes[b]);
+    if (bytes) GSR_CUDA(cudaMemcpy(host, scene->buffers[b].p, bytes, cudaMemcpyDeviceToHost));
+    return GSR_OK;
+}
+
+void gsr_scene_destroy(GsrScene* scene) { delete scene; }
+
+// ---- renderer ----------------------------------------------------------------------------------
+int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, GsrRenderer** out) {
+    if (!scene || !settings || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    int rc = validateScene(*scene);
+    if (rc) return rc;
+    if (settings->tile_size == 8)
+        return fail(GSR_ERROR_UNSUPPORTED, "--tile-size 8 is not implemented by this build (16 only)");
+    if (settings->tile_size != 16)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "--tile-size must be 8 or 16 (a divisor of INRIA's 16-px tiles)");
+    if (settings->bounds > GSR_BOUNDS_CUTOFF_ONLY) return fail(GSR_ERROR_INVALID_ARGUMENT, "bounds %u", settings->bounds);
+    if (settings->output_format > GSR_OUTPUT_RGBA32F_AND_RGB8)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "output format %u", settings->output_format);
+    auto r = std::make_unique<GsrRenderer>();
+    r->scene = *scene;
+    r->settings = *settings;
+    r->settings.max_sh_degree = std::clamp(settings->max_sh_degree, 0, 3);
+    r->settings.frames_in_flight = std::max(settings->frames_in_flight, 1u);
+    r->evalDegree = std::min(scene->sh_degree, r->settings.max_sh_degree);
+    rc = deviceTables(&r->logf);
+    if (rc) return rc;
+    const uint32_t n = scene->count;
+    GSR_CUDA(r->splats.alloc(size_t(n) * 48));
+    GSR_CUDA(cudaMemset(r->splats.p, 0, r->splats.bytes));
+    GSR_CUDA(r->tileCounts.alloc(size_t(n) * 4));
+    GSR_CUDA(r->offsets.alloc(size_t(n) * 4));
+    GSR_CUDA(r->scanStatus.alloc(size_t((n + 255) / 256) * 8));
+    GSR_CUDA(cudaMemset(r->scanStatus.p, 0, r->scanStatus.bytes));
+    GSR_CUDA(r->control.alloc(sizeof(DeviceControl)));
+    GSR_CUDA(cudaMemset(r->control.p, 0, sizeof(DeviceControl)));
+    GSR_CUDA(r->plan.alloc(sizeof(SortPlan)));
+    GSR_CUDA(cudaMemset(r->plan.p, 0, sizeof(SortPlan)));
+    r->slots.resize(r->settings.frames_in_flight);
+    for (auto& s : r->slots) {
+        GSR_CUDA(cudaMallocHost(&s.host, sizeof(GsrControl)));
+        std::memset(s.host, 0, sizeof(GsrControl));
+        GSR_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+    }
+    for (auto& e : r->ev) GSR_CUDA(cudaEventCreate(&e));
+    *out = r.release();
+    return GSR_OK;
+}
+
+int gsr_renderer_resize(GsrRenderer* r, uint32_t width, uint32_t height) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    return r->resize(width, height);
+}
+
+int gsr_render_splat_camera(GsrRenderer* r, const GsrSplatCamera* camera, void* stream) {
+    if (!r || !camera) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    return r->render(*camera, static_cast<cudaStream_t>(stream));
+}
+
+int gsr_render(GsrRenderer* r, const GsrCamera* camera, void* stream) {
+    if (!r || !camera) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    GsrSplatCamera cam;
+    splatCamera(*camera, cam);
+    return r->render(cam, static_cast<cudaStream_t>(stream));
+}
+
+int gsr_renderer_image(GsrRenderer* r, const void** rgba, const void** rgb8, uint32_t* width, uint32_t* height) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (rgba) *rgba = r->image.p;
+    if (rgb8) *rgb8 = r->rgb8.p;
+    if (width) *width = r->width;
+    if (height) *height = r->height;
+    return GSR_OK;
+}
+
+int gsr_render_to_host(GsrRenderer* r, const GsrCamera* camera, void* host, uint64_t bytes, void* stream) {
+    if (!r || !camera || !host) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    int rc = gsr_render(r, camera, stream);
+    if (rc) return rc;
+    const bool rgb = r->rgb8.p != nullptr;
+    const uint64_t need = uint64_t(r->width) * r->height * (rgb ? 3 : 16);
+    if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, image needs %llu",
+                                   (unsigned long long)bytes, (unsigned long long)need);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    GSR_CUDA(cudaMemcpyAsync(host, rgb ? r->rgb8.p : r->image.p, need, cudaMemcpyDeviceToHost, s));
+    GSR_CUDA(cudaStreamSynchronize(s));
+    return GSR_OK;
+}
+
+int gsr_renderer_last_stats(GsrRenderer* r, GsrControl* out, uint64_t* frameIndex) {
+    if (!r || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    for (auto& s : r->slots) r->readSlot(s);
+    if (!r->lastStatsValid) return GSR_ERROR_NOT_READY;
+    *out = r->lastStats;
+    if (frameIndex) *frameIndex = r->lastStatsFrame;
+    return GSR_OK;
+}
+
+int gsr_read_control(GsrRenderer* r, GsrControl* out) {
+    if (!r || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    GSR_CUDA(cudaDeviceSynchronize());
+    GSR_CUDA(cudaMemcpy(out, &r->control.as<DeviceControl>()->c, sizeof(GsrControl), cudaMemcpyDeviceToHost));
+    if (out->status & GSR_CONTROL_TIMEOUT) {
+        fail(GSR_ERROR_DEVICE_TIMEOUT, "device wait %u gave up", out->timeout_where);
+        return GSR_ERROR_DEVICE_TIMEOUT;
+    }
+    return GSR_OK;
+}
+
+int gsr_read_list(GsrRenderer* r, uint32_t* keysLo, uint32_t* keysHi, uint32_t* values, uint32_t n, uint32_t* rangesOut,
+                  uint32_t rangesWords) {
+    if (!r || !r->list) return fail(GSR_ERROR_INVALID_ARGUMENT, "no list");
+    GSR_CUDA(cudaDeviceSynchronize());
+    GsrControl c;
+    GSR_CUDA(cudaMemcpy(&c, &r->control.as<DeviceControl>()->c, sizeof(c), cudaMemcpyDeviceToHost));
+    n = std::min(n, c.entries);
+    const uint32_t b = c.sorted_buffer & 1u;
+    if (n && (keysLo || keysHi)) {
+        std::vector<uint64_t> k(n);
+        GSR_CUDA(cudaMemcpy(k.data(), r->list->keys[b].p, size_t(n) * 8, cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < n; ++i) {
+            if (keysLo) keysLo[i] = uint32_t(k[i]);
+            if (keysHi) keysHi[i] = uint32_t(k[i] >> 32);
+        }
+    }
+    if (n && values) GSR_CUDA(cudaMemcpy(values, r->list->values[b].p, size_t(n) * 4, cudaMemcpyDeviceToHost));
+    if (rangesOut) {
+        const uint32_t words = std::min<uint32_t>(rangesWords, r->tilesX * r->tilesY * 2);
+        GSR_CUDA(cudaMemcpy(rangesOut, r->ranges.p, size_t(words) * 4, cudaMemcpyDeviceToHost));
+    }
+    return GSR_OK;
+}
+
+int gsr_read_splats(GsrRenderer* r, void* splatsOut, uint32_t* tileCountsOut, uint32_t n) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    GSR_CUDA(cudaDeviceSynchronize());
+    n = std::min(n, r->scene.count);
+    if (splatsOut) GSR_CUDA(cudaMemcpy(splatsOut, r->splats.p, size_t(n) * 48, cudaMemcpyDeviceToHost));
+    if (tileCountsOut) GSR_CUDA(cudaMemcpy(tileCountsOut, r->tileCounts.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
+    return GSR_OK;
+}
+
+int gsr_read_image(GsrRenderer* r, float* rgba, uint8_t* rgb) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    GSR_CUDA(cudaDeviceSynchronize());
+    if (rgba) GSR_CUDA(cudaMemcpy(rgba, r->image.p, r->image.bytes, cudaMemcpyDeviceToHost));
+    if (rgb) {
+        if (!r->rgb8.p) return fail(GSR_ERROR_INVALID_ARGUMENT, "rgb8 output is off");
+        GSR_CUDA(cudaMemcpy(rgb, r->rgb8.p, r->rgb8.bytes, cudaMemcpyDeviceToHost));
+    }
+    return GSR_OK;
+}
+
+int gsr_renderer_set_timing(GsrRenderer* r, int enabled) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    r->timing = enabled != 0;
+    return GSR_OK;
+}
+
+int gsr_renderer_pass_times(GsrRenderer* r, float* ms, const char** names, uint32_t capacity, uint32_t* count) {
+    static const char* kNames[GsrRenderer::kPasses] = {"reset + preprocess + scan + duplicate", "tile sort (total)",
+                                                       "tile ranges", "render tiles", "control readback"};
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (!r->timed) return GSR_ERROR_NOT_READY;
+    GSR_CUDA(cudaEventSynchronize(r->ev[GsrRenderer::kPasses]));
+    const uint32_t n = std::min<uint32_t>(capacity, GsrRenderer::kPasses);
+    for (uint32_t i = 0; i < n; ++i) {
+        float t = 0.0f;
+        GSR_CUDA(cudaEventElapsedTime(&t, r->ev[i], r->ev[i + 1]));
+        if (ms) ms[i] = t;
+        if (names) names[i] = kNames[i];
+    }
+    if (count) *count = n;
+    return GSR_OK;
+}
+
+int gsr_renderer_capacity(GsrRenderer* r, uint32_t* capacity, uint32_t* maxCapacity, uint32_t* resizes) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (capacity) *capacity = r->list ? r->list->capacity : 0;
+    if (maxCapacity) *maxCapacity = r->maxCapacity;
+    if (resizes) *resizes = r->listResizes;
+    return GSR_OK;
+}
+
+int gsr_renderer_debug_force_timeout(GsrRenderer* r, uint32_t iterations) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    r->forceTimeout = iterations;
+    return GSR_OK;
+}
+
+void gsr_renderer_destroy(GsrRenderer* r) {
+    if (!r) return;
+    cudaDeviceSynchronize();
+    delete r;
+}
+
+// ---- primitives ----------------------------------------------------------------------------
+int gsr_scan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count, uint32_t mode,
+             void* stream) {
+    if (mode > GSR_SCAN_GATHER || (count && (!in || !out)) || (mode == GSR_SCAN_GATHER && count && !index))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "scan arguments");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DevBuf ctl, status;
+    const uint32_t blocks = (count + 2047) / 2048;
+    GSR_CUDA(ctl.alloc(sizeof(DeviceControl)));
+    GSR_CUDA(cudaMemsetAsync(ctl.p, 0, sizeof(DeviceControl), s));
+    GSR_CUDA(status.alloc(size_t(std::max(blocks, 1u)) * 8));
+    GSR_CUDA(cudaMemsetAsync(status.p, 0, status.bytes, s));
+    GSR_CUDA(launchFrameBegin(ctl.as<DeviceControl>(), count, 0, nullptr, 0, nullptr, 0, s));
+    GSR_CUDA(launchScan(in, index, out, total, count, mode, status.as<uint64_t>(), ctl.as<DeviceControl>(), s));
+    GSR_CUDA(cudaStreamSynchronize(s));  // the scratch is freed on return
+    DeviceControl c;
+    GSR_CUDA(cudaMemcpy(&c, ctl.p, sizeof(c), cudaMemcpyDeviceToHost));
+    if (c.c.status & GSR_CONTROL_TIMEOUT) return fail(GSR_ERROR_DEVICE_TIMEOUT, "scan look-back timed out");
+    return GSR_OK;
+}
+
+int gsr_sort_pairs(uint32_t* keysLo, uint32_t* keysHi, uint32_t* values, uint32_t count, uint32_t keyBits, void* stream) {
+    if (keyBits == 0 || keyBits > 64 || (!keysHi && keyBits > 32)) return fail(GSR_ERROR_INVALID_ARGUMENT, "key_bits %u", keyBits);
+    if (count == 0) return GSR_OK;
+    if (!keysLo || !values) return fail(GSR_ERROR_INVALID_ARGUMENT, "null keys/values");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const uint32_t passes = (keyBits + 7) / 8;
+    const uint32_t maxTiles = (count + kSortTile - 1) / kSortTile;
+    DevBuf ctl, plan, status, k0, k1, v1;
+    GSR_CUDA(ctl.alloc(sizeof(DeviceControl)));
+    GSR_CUDA(plan.alloc(sizeof(SortPlan)));
+    GSR_CUDA(status.alloc(size_t(passes) * maxTiles * 256 * 8));
+    GSR_CUDA(k0.alloc(size_t(count) * 8));
+    GSR_CUDA(k1.alloc(size_t(count) * 8));
+    GSR_CUDA(v1.alloc(size_t(count) * 4));
+    GSR_CUDA(cudaMemsetAsync(ctl.p, 0, ctl.bytes, s));
+    GSR_CUDA(cudaMemsetAsync(plan.p, 0, plan.bytes, s));
+    GSR_CUDA(cudaMemsetAsync(status.p, 0, status.bytes, s));
+    GSR_CUDA(launchFrameBegin(ctl.as<DeviceControl>(), count, count, nullptr, 0, plan.as<SortPlan>(), 0, s));
+    GSR_CUDA(launchSetEntries(ctl.as<DeviceControl>(), count, s));
+    GSR_CUDA(launchPack64(keysLo, keysHi, k0.as<uint64_t>(), count, s));
+    SortArgs sa{};
+    sa.keys[0] = k0.as<uint64_t>();
+    sa.keys[1] = k1.as<uint64_t>();
+    sa.values[0] = values;
+    sa.values[1] = v1.as<uint32_t>();
+    sa.status = status.as<uint64_t>();
+    sa.maxTiles = maxTiles;
+    sa.plan = plan.as<SortPlan>();
+    sa.ctl = ctl.as<DeviceControl>();
+    sa.passesLaunched = passes;
+    sa.frameMode = 0;
+    sa.fixedLowBits = 32;
+    sa.fixedKeyBits = keyBits;
+    GSR_CUDA(launchSort(sa, 148 * 2, s));
+    GSR_CUDA(cudaStreamSynchronize(s));
+    DeviceControl c;
+    GSR_CUDA(cudaMemcpy(&c, ctl.p, sizeof(c), cudaMemcpyDeviceToHost));
+    const uint32_t b = c.c.sorted_buffer & 1u;
+    GSR_CUDA(launchUnpack64(b ? k1.as<uint64_t>() : k0.as<uint64_t>(), keysLo, keysHi, count, s));
+    if (b) GSR_CUDA(cudaMemcpyAsync(values, v1.p, size_t(count) * 4, cudaMemcpyDeviceToDevice, s));
+    GSR_CUDA(cudaStreamSynchronize(s));
+    if (c.c.status & GSR_CONTROL_TIMEOUT) return fail(GSR_ERROR_DEVICE_TIMEOUT, "sort look-back timed out");
+    if (c.c.status & GSR_CONTROL_BOUNDS) return fail(GSR_ERROR_CUDA, "sort scatter index out of range");
+    return GSR_OK;
+}
+
+int gsr_debug_logf_table(float* outDevice, void* stream) {
+    if (!outDevice) return fail(GSR_ERROR_INVALID_ARGUMENT, "null output");
+    LogfFixups t;
+    const int rc = deviceTables(&t);
+    if (rc) return rc;
+    GSR_CUDA(launchLogfTable(outDevice, t, static_cast<cudaStream_t>(stream)));
+    return GSR_OK;
+}
+
+}  // extern "C"

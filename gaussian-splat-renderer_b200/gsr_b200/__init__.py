@@ -1,0 +1,381 @@
+"""Python access to the B200 splat-tiles library (libgsr_b200.so) through its C ABI.
+
+This mirrors the reference renderer's interface for the path (gsr::SplatTileRenderer,
+src/render/splat_tile_renderer.h:143-290, and gsr::GpuScene, src/render/gpu_scene.h:42-78):
+
+    scene = GpuScene(host_scene, fmt="f32", layout="soa")       # GpuScene::upload (+ encodeScene)
+    r = Renderer(scene, Settings(bounds="tight"))                 # SplatTileRenderer::init
+    r.render(camera)                                              # render(FrameInput)
+    keys_lo, keys_hi, values, ranges, control = r.read_back()     # readBack
+    splats, tile_counts = r.read_back_splats()                    # readBackSplats
+    rgba = r.read_back_image()                                    # readBackImage
+
+Errors of the C ABI raise GsrError (the reference throws std::runtime_error at init for invalid
+settings). The library must be built (gsr_b200.build); there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+from . import scenes  # noqa: F401  (re-exported helpers)
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libgsr_b200.so"
+
+GSR_OK = 0
+STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "out of memory",
+                5: "device timeout", 6: "not ready"}
+FORMATS = {"f32": 0, "f16": 1, "q8": 2, "cb": 3}
+LAYOUTS = {"soa": 0, "split": 1, "aos": 2}
+BOUNDS = {"rect": 0, "tight": 1, "cutoff-only": 2}
+CONTROL_TIMEOUT, CONTROL_BOUNDS, CONTROL_KEY_RANGE = 1, 2, 4
+
+SPLAT_DTYPE = np.dtype(
+    [
+        ("center", "<f4", (2,)),
+        ("depth", "<f4"),
+        ("cullReason", "<u4"),
+        ("conicOpacity", "<f4", (4,)),
+        ("color", "<f4", (3,)),
+        ("radius", "<f4"),
+    ]
+)
+
+
+class GsrError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("count", C.c_uint32), ("sh_degree", C.c_int32), ("sh_coeffs", C.c_uint32), ("format", C.c_uint32),
+        ("layout", C.c_uint32), ("geometry", C.c_uint32), ("color", C.c_uint32), ("geometry_stride", C.c_uint32),
+        ("color_stride", C.c_uint32), ("color_offset", C.c_uint32), ("codebook_stride", C.c_uint32),
+        ("variable_sh", C.c_uint32), ("buffers", C.c_void_p * 4), ("buffer_bytes", C.c_uint64 * 4),
+    ]
+
+
+class HostScene(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("sh_degree", C.c_int32), ("pos_alpha", C.c_void_p), ("scales", C.c_void_p),
+                ("rotations", C.c_void_p), ("sh", C.c_void_p)]
+
+
+class Compression(C.Structure):
+    _fields_ = [("format", C.c_uint32), ("layout", C.c_uint32), ("max_sh_degree", C.c_int32), ("sh_threshold", C.c_float)]
+
+
+class CSettings(C.Structure):
+    _fields_ = [
+        ("bounds", C.c_uint32), ("tile_size", C.c_uint32), ("budget_mb", C.c_uint32), ("adaptive_list", C.c_uint32),
+        ("adaptive_initial_entries", C.c_uint32), ("max_sh_degree", C.c_int32), ("output_format", C.c_uint32),
+        ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("reserved", C.c_uint32 * 7),
+    ]
+
+
+class CCamera(C.Structure):
+    _fields_ = [("view", C.c_float * 16), ("proj", C.c_float * 16), ("model", C.c_float * 16), ("width", C.c_uint32),
+                ("height", C.c_uint32)]
+
+
+class SplatCamera(C.Structure):
+    _fields_ = [
+        ("view_inria", C.c_float * 16), ("position", C.c_float * 3), ("width", C.c_uint32), ("height", C.c_uint32),
+        ("tan_half_fov_x", C.c_float), ("tan_half_fov_y", C.c_float), ("focal_x", C.c_float), ("focal_y", C.c_float),
+        ("tiles_x", C.c_uint32), ("tiles_y", C.c_uint32),
+    ]
+
+
+class Control(C.Structure):
+    _fields_ = [
+        ("gaussian_count", C.c_uint32), ("visible", C.c_uint32), ("duplicates", C.c_uint32), ("entries", C.c_uint32),
+        ("cull_counts", C.c_uint32 * 8), ("overflow", C.c_uint32), ("ranges_groups", C.c_uint32 * 3),
+        ("coverage_mismatch", C.c_uint32), ("pad", C.c_uint32 * 3), ("status", C.c_uint32),
+        ("timeout_where", C.c_uint32), ("epoch", C.c_uint32), ("sort_passes", C.c_uint32), ("key_bits", C.c_uint32),
+        ("depth_low_bits", C.c_uint32), ("depth_min_bits", C.c_uint32), ("depth_max_bits", C.c_uint32),
+        ("tile_max", C.c_uint32), ("sorted_buffer", C.c_uint32), ("capacity", C.c_uint32), ("ext_pad", C.c_uint32 * 5),
+    ]
+
+    def as_dict(self):
+        out = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            out[name] = list(v) if hasattr(v, "__len__") else v
+        return out
+
+
+_lib = None
+
+
+def library_path() -> Path:
+    return LIB_PATH
+
+
+def load(build_if_missing: bool = True) -> C.CDLL:
+    """Loads libgsr_b200.so (building it first when it is missing or stale and nvcc exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    from . import build as _build
+
+    if build_if_missing:
+        try:
+            if _build.stale():
+                _build.build()
+        except RuntimeError:
+            if not LIB_PATH.exists():
+                raise
+    if not LIB_PATH.exists():
+        raise GsrError(2, f"{LIB_PATH} is not built (run gsr_b200.build)")
+    lib = C.CDLL(str(LIB_PATH))
+    vp, u32, i32, u64 = C.c_void_p, C.c_uint32, C.c_int32, C.c_uint64
+    sig = {
+        "gsr_abi_version": (C.c_int, []),
+        "gsr_error_string": (C.c_char_p, [C.c_int]),
+        "gsr_last_error_message": (C.c_char_p, []),
+        "gsr_settings_default": (None, [C.POINTER(CSettings)]),
+        "gsr_splat_camera_from_viewer": (C.c_int, [C.POINTER(CCamera), C.POINTER(SplatCamera)]),
+        "gsr_look_at": (None, [vp, vp, vp, vp]),
+        "gsr_perspective_vk": (None, [C.c_float, C.c_float, C.c_float, C.c_float, vp]),
+        "gsr_scene_create": (C.c_int, [C.POINTER(HostScene), C.POINTER(Compression), C.POINTER(vp)]),
+        "gsr_scene_get_desc": (C.c_int, [vp, C.POINTER(SceneDesc)]),
+        "gsr_scene_read_buffer": (C.c_int, [vp, u32, vp, u64]),
+        "gsr_scene_destroy": (None, [vp]),
+        "gsr_renderer_create": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(CSettings), C.POINTER(vp)]),
+        "gsr_renderer_resize": (C.c_int, [vp, u32, u32]),
+        "gsr_render": (C.c_int, [vp, C.POINTER(CCamera), vp]),
+        "gsr_render_splat_camera": (C.c_int, [vp, C.POINTER(SplatCamera), vp]),
+        "gsr_renderer_image": (C.c_int, [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(u32), C.POINTER(u32)]),
+        "gsr_render_to_host": (C.c_int, [vp, C.POINTER(CCamera), vp, u64, vp]),
+        "gsr_renderer_last_stats": (C.c_int, [vp, C.POINTER(Control), C.POINTER(u64)]),
+        "gsr_read_control": (C.c_int, [vp, C.POINTER(Control)]),
+        "gsr_read_list": (C.c_int, [vp, vp, vp, vp, u32, vp, u32]),
+        "gsr_read_splats": (C.c_int, [vp, vp, vp, u32]),
+        "gsr_read_image": (C.c_int, [vp, vp, vp]),
+        "gsr_renderer_set_timing": (C.c_int, [vp, C.c_int]),
+        "gsr_renderer_pass_times": (C.c_int, [vp, vp, vp, u32, C.POINTER(u32)]),
+        "gsr_renderer_capacity": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]),
+        "gsr_renderer_debug_force_timeout": (C.c_int, [vp, u32]),
+        "gsr_renderer_destroy": (None, [vp]),
+        "gsr_scan": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
+        "gsr_sort_pairs": (C.c_int, [vp, vp, vp, u32, u32, vp]),
+        "gsr_debug_logf_table": (C.c_int, [vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(status: int):
+    if status != GSR_OK:
+        msg = load().gsr_last_error_message().decode(errors="replace")
+        raise GsrError(status, msg)
+
+
+def _f16(a) -> "C.Array":
+    return (C.c_float * 16)(*np.asarray(a, np.float32).reshape(16).tolist())
+
+
+def to_c_camera(cam) -> CCamera:
+    c = CCamera()
+    c.view = _f16(cam.view)
+    c.proj = _f16(cam.proj)
+    c.model = _f16(cam.model)
+    c.width = cam.width
+    c.height = cam.height
+    return c
+
+
+def splat_camera(cam) -> SplatCamera:
+    out = SplatCamera()
+    check(load().gsr_splat_camera_from_viewer(C.byref(to_c_camera(cam)), C.byref(out)))
+    return out
+
+
+@dataclass
+class Settings:
+    bounds: str = "tight"
+    tile_size: int = 16
+    budget_mb: int = 256
+    adaptive_list: bool = True
+    adaptive_initial_entries: int = 0
+    max_sh_degree: int = 3
+    rgb8: bool = False
+    frames_in_flight: int = 2
+    use_graph: bool = False
+
+    def to_c(self) -> CSettings:
+        s = CSettings()
+        load().gsr_settings_default(C.byref(s))
+        s.bounds = BOUNDS[self.bounds] if isinstance(self.bounds, str) else int(self.bounds)
+        s.tile_size = self.tile_size
+        s.budget_mb = self.budget_mb
+        s.adaptive_list = int(self.adaptive_list)
+        s.adaptive_initial_entries = self.adaptive_initial_entries
+        s.max_sh_degree = self.max_sh_degree
+        s.output_format = 1 if self.rgb8 else 0
+        s.frames_in_flight = self.frames_in_flight
+        s.use_graph = int(self.use_graph)
+        return s
+
+
+class GpuScene:
+    """gsr::GpuScene: the scene encoded (on the GPU) and resident in device memory."""
+
+    def __init__(self, scene, fmt: str = "f32", layout: str = "soa", max_sh_degree: int = 3, sh_threshold: float = -1.0):
+        lib = load()
+        self._arrays = [np.ascontiguousarray(a, np.float32) for a in (scene.pos_alpha, scene.scales, scene.rotations, scene.sh)]
+        hs = HostScene(scene.count, scene.sh_degree, *[a.ctypes.data for a in self._arrays])
+        comp = Compression(FORMATS[fmt], LAYOUTS[layout], max_sh_degree, sh_threshold)
+        h = C.c_void_p()
+        check(lib.gsr_scene_create(C.byref(hs), C.byref(comp), C.byref(h)))
+        self._h = h
+        self._arrays = None
+        self.desc = SceneDesc()
+        check(lib.gsr_scene_get_desc(self._h, C.byref(self.desc)))
+
+    def buffer(self, b: int) -> np.ndarray:
+        n = int(self.desc.buffer_bytes[b])
+        out = np.zeros(n // 4, np.uint32)
+        if n:
+            check(load().gsr_scene_read_buffer(self._h, b, out.ctypes.data, n))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().gsr_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Renderer:
+    """gsr::SplatTileRenderer over the C ABI."""
+
+    def __init__(self, scene: GpuScene, settings: Settings | None = None, desc: SceneDesc | None = None):
+        lib = load()
+        self.scene = scene  # keeps the scene memory alive
+        self.settings = settings or Settings()
+        h = C.c_void_p()
+        check(lib.gsr_renderer_create(C.byref(desc or scene.desc), C.byref(self.settings.to_c()), C.byref(h)))
+        self._h = h
+        self.width = self.height = 0
+
+    @property
+    def handle(self):
+        return self._h
+
+    def render(self, camera, stream: int = 0):
+        """camera: scenes.ViewerCamera (view/proj/model) or a SplatCamera."""
+        lib = load()
+        if isinstance(camera, SplatCamera):
+            check(lib.gsr_render_splat_camera(self._h, C.byref(camera), C.c_void_p(stream)))
+            self.width, self.height = camera.width, camera.height
+        else:
+            check(lib.gsr_render(self._h, C.byref(to_c_camera(camera)), C.c_void_p(stream)))
+            self.width, self.height = camera.width, camera.height
+
+    def render_to_host(self, camera, out: np.ndarray, stream: int = 0):
+        check(load().gsr_render_to_host(self._h, C.byref(to_c_camera(camera)), out.ctypes.data, out.nbytes,
+                                        C.c_void_p(stream)))
+
+    def image_pointers(self):
+        rgba, rgb = C.c_void_p(), C.c_void_p()
+        w, h = C.c_uint32(), C.c_uint32()
+        check(load().gsr_renderer_image(self._h, C.byref(rgba), C.byref(rgb), C.byref(w), C.byref(h)))
+        return rgba.value, rgb.value, w.value, h.value
+
+    def read_control(self) -> Control:
+        c = Control()
+        st = load().gsr_read_control(self._h, C.byref(c))
+        if st not in (GSR_OK, 5):
+            check(st)
+        return c
+
+    def last_stats(self):
+        c = Control()
+        idx = C.c_uint64()
+        st = load().gsr_renderer_last_stats(self._h, C.byref(c), C.byref(idx))
+        if st == 6:
+            return None, None
+        check(st)
+        return c, idx.value
+
+    def read_back(self):
+        """The sorted list (keys_lo = depth bits, keys_hi = tile id, values) and the ranges."""
+        c = self.read_control()
+        n = c.entries
+        lo = np.zeros(max(n, 1), np.uint32)
+        hi = np.zeros(max(n, 1), np.uint32)
+        val = np.zeros(max(n, 1), np.uint32)
+        tiles = ((self.width + 15) // 16) * ((self.height + 15) // 16)
+        ranges = np.zeros(2 * tiles, np.uint32)
+        check(load().gsr_read_list(self._h, lo.ctypes.data, hi.ctypes.data, val.ctypes.data, n, ranges.ctypes.data,
+                                   ranges.size))
+        return lo[:n], hi[:n], val[:n], ranges.reshape(tiles, 2), c
+
+    def read_back_splats(self, n: int):
+        sp = np.zeros(n, SPLAT_DTYPE)
+        counts = np.zeros(n, np.uint32)
+        check(load().gsr_read_splats(self._h, sp.ctypes.data, counts.ctypes.data, n))
+        return sp, counts
+
+    def read_back_image(self, rgb8: bool = False):
+        rgba = np.zeros((self.height, self.width, 4), np.float32)
+        out8 = np.zeros((self.height, self.width, 3), np.uint8) if rgb8 else None
+        check(load().gsr_read_image(self._h, rgba.ctypes.data, out8.ctypes.data if rgb8 else None))
+        return (rgba, out8) if rgb8 else rgba
+
+    def set_timing(self, enabled: bool):
+        check(load().gsr_renderer_set_timing(self._h, int(enabled)))
+
+    def pass_times(self):
+        ms = (C.c_float * 8)()
+        names = (C.c_char_p * 8)()
+        n = C.c_uint32()
+        st = load().gsr_renderer_pass_times(self._h, ms, names, 8, C.byref(n))
+        if st == 6:
+            return {}
+        check(st)
+        return {names[i].decode(): ms[i] for i in range(n.value)}
+
+    def capacity(self):
+        c, m, r = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        check(load().gsr_renderer_capacity(self._h, C.byref(c), C.byref(m), C.byref(r)))
+        return c.value, m.value, r.value
+
+    def force_timeout(self, iterations: int):
+        check(load().gsr_renderer_debug_force_timeout(self._h, iterations))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().gsr_renderer_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def scan(in_ptr: int, index_ptr: int | None, out_ptr: int, total_ptr: int | None, count: int, mode: int, stream: int = 0):
+    check(load().gsr_scan(C.c_void_p(in_ptr), C.c_void_p(index_ptr), C.c_void_p(out_ptr), C.c_void_p(total_ptr), count,
+                          mode, C.c_void_p(stream)))
+
+
+def sort_pairs(lo_ptr: int, hi_ptr: int | None, values_ptr: int, count: int, key_bits: int, stream: int = 0):
+    check(load().gsr_sort_pairs(C.c_void_p(lo_ptr), C.c_void_p(hi_ptr), C.c_void_p(values_ptr), count, key_bits,
+                                C.c_void_p(stream)))

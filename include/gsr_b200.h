@@ -1,0 +1,254 @@
+/* gsr_b200.h - C ABI of the B200 (sm_100a) splat-tiles frame path.
+ *
+ * A drop-in for the reference renderer's `splat-tiles` path (gsr::SplatTileRenderer,
+ * src/render/splat_tile_renderer.h:143-290, behind gsr::Renderer, src/render/renderer.h:59-72),
+ * with the scene buffers of gsr::GpuScene (src/render/gpu_scene.h:42-78) and the camera of
+ * gsr::FrameInput (src/render/renderer.h:28-52). Plain C types only: device memory is passed
+ * as pointers, CUDA streams as opaque handles (cudaStream_t), sizes as integers.
+ *
+ * Errors are returned as GsrStatus codes (never exceptions); gsr_error_string() names them and
+ * gsr_last_error_message() gives the detail of the calling thread's last failure. One
+ * renderer handle is used from one host thread at a time; work is stream-ordered on the
+ * stream passed to gsr_render(). The scene memory stays owned by the caller (or by a
+ * GsrScene handle); every other buffer is owned by the renderer.
+ */
+#ifndef GSR_B200_H
+#define GSR_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSR_ABI_VERSION 1
+
+typedef enum GsrStatus {
+    GSR_OK = 0,
+    GSR_ERROR_INVALID_ARGUMENT = 1, /* std::runtime_error for invalid settings (splat_tile_renderer.cpp:139-152) */
+    GSR_ERROR_UNSUPPORTED = 2,      /* a format/option this build does not implement */
+    GSR_ERROR_CUDA = 3,             /* a CUDA runtime call failed (VK_CHECK in the reference) */
+    GSR_ERROR_OUT_OF_MEMORY = 4,
+    GSR_ERROR_DEVICE_TIMEOUT = 5,   /* a bounded device-side wait gave up (GsrControl.status) */
+    GSR_ERROR_NOT_READY = 6         /* nothing to report yet (e.g. no completed frame) */
+} GsrStatus;
+
+/* ---- scene (gsr::GpuScene, src/render/gpu_scene.h:42-78) ------------------------------ */
+typedef enum GsrSceneFormat { GSR_FORMAT_F32 = 0, GSR_FORMAT_F16 = 1, GSR_FORMAT_Q8 = 2, GSR_FORMAT_CB = 3 } GsrSceneFormat;
+typedef enum GsrSceneLayout { GSR_LAYOUT_SOA = 0, GSR_LAYOUT_SPLIT = 1, GSR_LAYOUT_AOS = 2 } GsrSceneLayout;
+/* GeometryEncoding / ColorEncoding / VariableSh (src/scene/scene_compression.h:73-89). */
+typedef enum GsrGeometryEncoding { GSR_GEOMETRY_SOA_F32 = 0, GSR_GEOMETRY_RECORD_F32 = 1, GSR_GEOMETRY_RECORD_F16 = 2 } GsrGeometryEncoding;
+typedef enum GsrColorEncoding {
+    GSR_COLOR_SOA_F32 = 0, GSR_COLOR_RECORD_F32 = 1, GSR_COLOR_RECORD_F16 = 2, GSR_COLOR_Q8 = 3, GSR_COLOR_CODEBOOK = 4
+} GsrColorEncoding;
+typedef enum GsrVariableSh { GSR_VARIABLE_SH_OFF = 0, GSR_VARIABLE_SH_DEGREE_ONLY = 1, GSR_VARIABLE_SH_COMPACT = 2 } GsrVariableSh;
+
+/* The scene as the preprocess reads it: the 4 storage buffers of GpuScene's binding table
+ * (gpu_scene.h:4-17) as DEVICE pointers, plus the format fields that the reference passes as
+ * specialization constants 0-7 (shaders/scene_decode.glsl:31-40). Strides/offsets are in
+ * 16-byte units, as there.
+ *   soa   : buffers = posAlpha float4[N], scales float4[N], rotations float4[N], sh float[N*K*3]
+ *   split : buffers = geometry records, colour records, -, -
+ *   aos   : buffers = records, (same), -, - */
+typedef struct GsrSceneDesc {
+    uint32_t count;            /* N */
+    int32_t sh_degree;         /* stored degree (0..3) */
+    uint32_t sh_coeffs;        /* stored K = (sh_degree + 1)^2 */
+    uint32_t format;           /* GsrSceneFormat (informational) */
+    uint32_t layout;           /* GsrSceneLayout */
+    uint32_t geometry;         /* GsrGeometryEncoding */
+    uint32_t color;            /* GsrColorEncoding */
+    uint32_t geometry_stride;  /* uvec4 per geometry record (0 for soa) */
+    uint32_t color_stride;     /* uvec4 per colour record */
+    uint32_t color_offset;     /* uvec4 offset of the colour record (aos) */
+    uint32_t codebook_stride;  /* uvec4 per codebook entry (cb; unsupported) */
+    uint32_t variable_sh;      /* GsrVariableSh */
+    const void* buffers[4];    /* device pointers, 16-byte aligned */
+    uint64_t buffer_bytes[4];
+} GsrSceneDesc;
+
+/* Host-side activated scene (gsr::GaussianScene's GPU arrays, src/scene/gaussian_scene.h:71-102). */
+typedef struct GsrHostScene {
+    uint32_t count;
+    int32_t sh_degree;
+    const float* pos_alpha;  /* float4[N] */
+    const float* scales;     /* float4[N] */
+    const float* rotations;  /* float4[N] (w, x, y, z) */
+    const float* sh;         /* float[N * K * 3] */
+} GsrHostScene;
+
+/* gsr::CompressionOptions subset (src/scene/scene_compression.h:76-86). */
+typedef struct GsrCompression {
+    uint32_t format;        /* GsrSceneFormat (f32, f16, q8) */
+    uint32_t layout;        /* GsrSceneLayout (soa only with f32) */
+    int32_t max_sh_degree;  /* drop stored bands above this */
+    float sh_threshold;     /* per-gaussian SH degree threshold in 1/255 (< 0: off) */
+} GsrCompression;
+
+typedef struct GsrScene GsrScene;
+
+/* GpuScene::upload (src/render/gpu_scene.cpp): encodes on the GPU (encodeScene,
+ * src/scene/scene_compression.cpp:150-380, f32/f16/q8 in soa/split/aos, variable SH degree)
+ * and keeps the encoded buffers in device memory owned by the handle. */
+int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, GsrScene** out);
+/* The descriptor of a GsrScene, to pass to gsr_renderer_create. */
+int gsr_scene_get_desc(const GsrScene* scene, GsrSceneDesc* out);
+/* Copies encoded buffer b (0..3) to host memory (tests): bytes = buffer_bytes[b]. */
+int gsr_scene_read_buffer(const GsrScene* scene, uint32_t b, void* host, uint64_t bytes);
+void gsr_scene_destroy(GsrScene* scene);
+
+/* ---- settings (SplatSettings src/render/splat_draw.h:31-37 + TileSettings
+ *      src/render/splat_tile_renderer.h:96-114) ------------------------------------------ */
+typedef enum GsrTileBounds { GSR_BOUNDS_RECT = 0, GSR_BOUNDS_TIGHT = 1, GSR_BOUNDS_CUTOFF_ONLY = 2 } GsrTileBounds;
+typedef enum GsrOutputFormat { GSR_OUTPUT_RGBA32F = 0, GSR_OUTPUT_RGBA32F_AND_RGB8 = 1 } GsrOutputFormat;
+
+typedef struct GsrSettings {
+    uint32_t bounds;                   /* GsrTileBounds; reference default tight (cli.h) */
+    uint32_t tile_size;                /* 16 (INRIA tiles) */
+    uint32_t budget_mb;                /* list memory incl. sort scratch; default 256 */
+    uint32_t adaptive_list;            /* 1: capacity follows the measured entry count */
+    uint32_t adaptive_initial_entries; /* 0: max(4 N, 1 M) */
+    int32_t max_sh_degree;             /* bands evaluated (<= stored) */
+    uint32_t output_format;            /* GsrOutputFormat */
+    uint32_t frames_in_flight;         /* control readback slots (default 2) */
+    uint32_t use_graph;                /* 1: launch each frame as a captured CUDA graph */
+    uint32_t reserved[7];
+} GsrSettings;
+
+/* Reference defaults for this path (cli.h:28-50): tight bounds, 16-px tiles, 256 MB, adaptive. */
+void gsr_settings_default(GsrSettings* s);
+
+/* ---- camera (FrameInput view/proj/model, renderer.h:28-52) ------------------------------ */
+typedef struct GsrCamera {
+    float view[16];   /* world -> eye, column-major, -z forward, +y up */
+    float proj[16];   /* Vulkan perspective (y flipped); only proj[0][0], proj[1][1] are used */
+    float model[16];  /* data -> world */
+    uint32_t width, height;
+} GsrCamera;
+
+/* gsr::SplatCamera (src/splat/splat_math.h:43-50) as splatCameraFromViewer computes it. */
+typedef struct GsrSplatCamera {
+    float view_inria[16];
+    float position[3];
+    uint32_t width, height;
+    float tan_half_fov_x, tan_half_fov_y, focal_x, focal_y;
+    uint32_t tiles_x, tiles_y;
+} GsrSplatCamera;
+
+/* splatCameraFromViewer (src/splat/splat_math.cpp:29-42). */
+int gsr_splat_camera_from_viewer(const GsrCamera* camera, GsrSplatCamera* out);
+/* glm::lookAt (RH) and glm::perspective (RH, depth 0..1) with the Vulkan y flip, as the
+ * reference's viewer camera builds them (src/app/camera.cpp:41-45). Column-major outputs. */
+void gsr_look_at(const float eye[3], const float center[3], const float up[3], float view[16]);
+void gsr_perspective_vk(float fovy_radians, float aspect, float z_near, float z_far, float proj[16]);
+
+/* ---- the control block (TileControl, splat_tile_renderer.h:117-128 + extensions) -------- */
+typedef enum GsrControlStatus {
+    GSR_CONTROL_OK = 0,
+    GSR_CONTROL_TIMEOUT = 1,         /* a look-back wait hit its iteration limit */
+    GSR_CONTROL_BOUNDS = 2,          /* an index check failed; the access was skipped */
+    GSR_CONTROL_KEY_RANGE = 4        /* the sort key did not fit the planned bits */
+} GsrControlStatus;
+
+typedef struct GsrControl {
+    /* the reference's 80-byte TileControl, same order */
+    uint32_t gaussian_count;         /* N */
+    uint32_t visible;                /* V (visible splats; = cull_counts[0]) */
+    uint32_t duplicates;             /* M, unclamped */
+    uint32_t entries;                /* min(M, capacity) */
+    uint32_t cull_counts[8];         /* per CullReason: visible, near, singular, off-screen, low opacity */
+    uint32_t overflow;               /* M - entries */
+    uint32_t ranges_groups[3];       /* ceil(entries / 256), 1, 1 */
+    uint32_t coverage_mismatch;      /* splats whose written tiles != their count (always 0) */
+    uint32_t pad[3];
+    /* extensions of this build */
+    uint32_t status;                 /* GsrControlStatus bits */
+    uint32_t timeout_where;          /* id of the wait that gave up */
+    uint32_t epoch;                  /* frame counter of the device-side look-back flags */
+    uint32_t sort_passes;            /* radix passes that moved data */
+    uint32_t key_bits;               /* significant bits of the (tile | depth) key */
+    uint32_t depth_low_bits;         /* depth bits that vary across the frame's keys */
+    uint32_t depth_min_bits, depth_max_bits;
+    uint32_t tile_max;               /* largest tile id emitted */
+    uint32_t sorted_buffer;          /* which list buffer holds the sorted result */
+    uint32_t capacity;               /* list capacity of this frame */
+    uint32_t ext_pad[5];
+} GsrControl;
+
+/* ---- the renderer (SplatTileRenderer) ---------------------------------------------------- */
+typedef struct GsrRenderer GsrRenderer;
+
+/* SplatTileRenderer::init (splat_tile_renderer.cpp:127-...): validates the settings and the
+ * scene format, allocates the per-gaussian buffers and the list. The scene memory must stay
+ * valid until gsr_renderer_destroy. */
+int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, GsrRenderer** out);
+/* onRenderTargetsChanged (splat_tile_renderer.cpp:537-...): (re)creates the per-tile and
+ * image buffers for a width x height target. gsr_render calls it on a size change. */
+int gsr_renderer_resize(GsrRenderer* r, uint32_t width, uint32_t height);
+/* render (splat_tile_renderer.cpp:624-833): the whole frame, enqueued on `stream` (a
+ * cudaStream_t; NULL = the legacy default stream). The image stays in renderer-owned device
+ * memory (gsr_renderer_image); nothing is synchronized. */
+int gsr_render(GsrRenderer* r, const GsrCamera* camera, void* stream);
+/* The same frame from a precomputed SplatCamera (tests that share one camera with the oracle). */
+int gsr_render_splat_camera(GsrRenderer* r, const GsrSplatCamera* camera, void* stream);
+/* Device pointers of the last frame's outputs: rgba = float4[W*H] (C, 1 - T), rgb8 = uint8[W*H*3]
+ * (lround(clamp(C, 0, 1) * 255), NULL unless GSR_OUTPUT_RGBA32F_AND_RGB8). */
+int gsr_renderer_image(GsrRenderer* r, const void** rgba, const void** rgb8, uint32_t* width, uint32_t* height);
+/* The end-to-end call for host callers: render and copy the RGB8 (or RGBA32F when rgb8 output is
+ * off) image into `host` (pinned or pageable; `bytes` must match), then synchronize `stream`. */
+int gsr_render_to_host(GsrRenderer* r, const GsrCamera* camera, void* host, uint64_t bytes, void* stream);
+
+/* lastStats / collectPending (splat_tile_renderer.h:167-181): the control block of the most
+ * recent frame whose readback has completed (frames_in_flight frames late, no stall).
+ * GSR_ERROR_NOT_READY if none yet. frame_index receives that frame's number. */
+int gsr_renderer_last_stats(GsrRenderer* r, GsrControl* out, uint64_t* frame_index);
+/* Synchronizes and reads the current control block (readBack's TileControl). */
+int gsr_read_control(GsrRenderer* r, GsrControl* out);
+/* readBack (splat_tile_renderer.h:184-185), GPU idle: the sorted list's first n entries
+ * (keys_lo = depth bits, keys_hi = tile, values = gaussian) and 2 words per tile of ranges.
+ * Any pointer may be NULL. n is clamped to the entry count. */
+int gsr_read_list(GsrRenderer* r, uint32_t* keys_lo, uint32_t* keys_hi, uint32_t* values, uint32_t n,
+                  uint32_t* ranges, uint32_t ranges_words);
+/* readBackSplats (splat_tile_renderer.h:188): 48-byte ProjectedSplat records (visible
+ * gaussians only are written by a frame; the rest keep older contents) and tile counts. */
+int gsr_read_splats(GsrRenderer* r, void* splats, uint32_t* tile_counts, uint32_t n);
+/* readBackImage (splat_tile_renderer.h:194): rgba float4[W*H] and/or rgb8 uint8[W*H*3]. */
+int gsr_read_image(GsrRenderer* r, float* rgba, uint8_t* rgb8);
+/* Per-pass device time of the last frame in ms (GpuProfiler scopes), when timing is on. */
+int gsr_renderer_set_timing(GsrRenderer* r, int enabled);
+int gsr_renderer_pass_times(GsrRenderer* r, float* ms, const char** names, uint32_t capacity, uint32_t* count);
+/* Capacity of the current list in entries, the budget's maximum, and list resizes so far. */
+int gsr_renderer_capacity(GsrRenderer* r, uint32_t* capacity, uint32_t* max_capacity, uint32_t* resizes);
+/* Test hook: forces the look-back waits of the next frame to see no predecessor, so that
+ * they run into their iteration limit and report GSR_CONTROL_TIMEOUT (iterations = limit). */
+int gsr_renderer_debug_force_timeout(GsrRenderer* r, uint32_t iterations);
+void gsr_renderer_destroy(GsrRenderer* r);
+
+/* ---- primitives (GpuScan src/render/gpu_scan.h:25-76, GpuRadixSort
+ *      src/render/gpu_radix_sort.h:38-122) ----------------------------------------------- */
+typedef enum GsrScanMode { GSR_SCAN_PLAIN = 0, GSR_SCAN_NONZERO = 1, GSR_SCAN_GATHER = 2 } GsrScanMode;
+/* Exclusive scan of `count` u32 (device pointers): out[j] = sum_{i<j} v(i), v(i) = in[i]
+ * (plain), in[i] != 0 (non-zero flags) or in[index[i]] (gather); *total (device) = the sum.
+ * Stream-ordered; the scratch is allocated per call (see gsr_scan_scratch_bytes for reuse). */
+int gsr_scan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
+             uint32_t mode, void* stream);
+/* Stable LSD sort of (key, value) pairs by the low key_bits of the key, in place (device
+ * pointers). keys_hi may be NULL (32-bit keys); with it the key is (keys_hi << 32 | keys_lo).
+ * Bit-for-bit the order of a stable sort (DepthSorter::radixSortPairs for 32-bit keys). */
+int gsr_sort_pairs(uint32_t* keys_lo, uint32_t* keys_hi, uint32_t* values, uint32_t count, uint32_t key_bits,
+                   void* stream);
+
+/* ---- diagnostics ------------------------------------------------------------------------ */
+const char* gsr_error_string(int status);
+const char* gsr_last_error_message(void);
+int gsr_abi_version(void);
+/* Device: computes the kernel's 2 ln(255 o) threshold log for every float x in [1, 255] into
+ * out (device, 67,043,329 floats), so tests can compare it with the C library's logf. */
+int gsr_debug_logf_table(float* out_device, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GSR_B200_H */
