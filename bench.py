@@ -1,0 +1,349 @@
+"""Benchmark of the B200 splat-tiles frame path (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config plain_1080p|plain_1080p_f16|plain_720p]
+    python bench.py --impl reference ...    # the reference's own CPU renderer on this host
+
+Workload (default): the plain forward render at 1920x1080 of 1,240,000 synthetic gaussians
+(means uniform in a ball of radius 8, SH degree 3, fp32 SoA scene), on the 300-frame 360-degree
+orbit of radius 14 at height 2; tight tile bounds, adaptive list, global 64-bit key sort. A step
+renders one view of the orbit (view k = frame k mod 300, ranks start at different frames).
+
+value        views/s over all ranks, scene and camera parameters resident on the device: CUDA
+             events around K consecutive gsr_render calls on one stream (barrier + synchronize
+             on both sides, max over ranks).
+e2e          the same metric through gsr_render_to_host, the call a host application makes:
+             each step passes the camera from host memory and copies the 8-bit RGB image into
+             pinned host memory, then synchronizes. The scene upload is an init-time step
+             (GpuScene::upload in the reference) and is not part of a step.
+roofline     the front kernel (preprocess + count + scan + key emission) against the measured
+             HBM copy bandwidth: algorithmic bytes per frame / its CUDA-event duration.
+cpu_baseline the reference's own CPU renderer (renderReference compiled from its sources, else
+             the C restatement), rank 0, all host threads, a bounded sample of the orbit.
+L2           the scene (298 MB fp32) is larger than the 126 MB L2, so no flush between steps.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "gaussian-splat-renderer_b200"))
+
+METRIC = "1080p views/s at 1.24M gaussians: batched+MLP colour vs plain, PSNR>=45 dB"
+UNIT = "views/s"
+
+
+def load_peaks():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---- configurations ---------------------------------------------------------------------
+def make_config(name: str):
+    from gsr_b200 import scenes
+
+    if name in ("plain_1080p", "plain_1080p_f16"):
+        scene, cams = scenes.plain_1080p(300)
+        fmt, layout = ("f16", "split") if name.endswith("f16") else ("f32", "soa")
+        return scene, cams, fmt, layout
+    if name == "plain_720p":
+        scene, cams = scenes.plain_720p()
+        return scene, cams, "f32", "soa"
+    raise SystemExit(f"unknown config {name}")
+
+
+# ---- distributed plumbing (one process per GPU) -------------------------------------------
+class Dist:
+    def __init__(self, backend: str):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, value: float) -> float:
+        if not self.pg:
+            return value
+        import torch
+
+        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([value], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---- clocks sampled during the timed region ---------------------------------------------
+class ClockSampler:
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--id={self.index}",
+               "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+               "--format=csv,noheader,nounits", "-lms", "100"]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clocks not sampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---- algorithmic bytes of the front kernel (preprocess + scan + key emission) -------------
+def front_bytes(scene_format: str, ctl, n: int) -> float:
+    """Bytes the front kernel must move for one frame, from the frame's counts:
+    posAlpha of every gaussian, scale + rotation of those past the near/opacity culls, SH of
+    the visible ones, the visible splat records, tile counts + offsets of every gaussian, the
+    12-byte (key, value) entries, and the look-back words (8 B per 256 gaussians)."""
+    past_cull = n - ctl.cull_counts[1] - ctl.cull_counts[4]
+    vis = ctl.cull_counts[0]
+    if scene_format == "f32":
+        b = 16 * n + 32 * past_cull + 192 * vis
+    else:  # f16 split: G16 record 32 B (posAlpha in the first 16 B), colour 96 B
+        b = 16 * n + 16 * past_cull + 96 * vis
+    b += 48 * vis + 8 * n + 12 * ctl.entries + 8 * math.ceil(n / 256)
+    return float(b)
+
+
+def sort_bytes(ctl) -> float:
+    """Histogram read (8 B/key) + per active pass 24 B/entry (read + write of key and value)."""
+    return float(8 * ctl.entries + 24 * ctl.entries * ctl.sort_passes)
+
+
+# ---- the CPU baseline ----------------------------------------------------------------------
+def cpu_reference_run(scene, cams, max_frames: int, time_budget_s: float, warmup: int = 1):
+    sys.path.insert(0, str(REPO / "oracle"))
+    import oracle as O
+
+    kind = "reference" if O.reference_available() else "port"
+    orc = O.Oracle(kind)
+    threads = os.cpu_count() or 1
+    for c in cams[:warmup]:
+        cam = orc.camera_from_viewer(c.view, c.proj, c.model, c.width, c.height)
+        orc.render(scene, cam, bounds=1, threads=threads)
+    done, t0 = 0, time.perf_counter()
+    step = max(1, len(cams) // max(1, max_frames))
+    frames = []
+    for k in range(0, len(cams), step):
+        if done >= max_frames or time.perf_counter() - t0 > time_budget_s:
+            break
+        c = cams[k]
+        cam = orc.camera_from_viewer(c.view, c.proj, c.model, c.width, c.height)
+        orc.render(scene, cam, bounds=1, threads=threads)
+        frames.append(k)
+        done += 1
+    dt = time.perf_counter() - t0
+    return {"value": done / dt if dt > 0 else 0.0, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{done} views of the 300-frame orbit (every {step}th frame), tight bounds, "
+                      f"renderReference with {threads} threads, {dt:.1f} s"}
+
+
+def run_reference_arm(args):
+    # under torchrun only rank 0 runs the CPU reference; the other ranks exit without work
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    scene, cams, fmt, layout = make_config(args.config)
+    budget = 90.0
+    res = cpu_reference_run(scene, cams, max_frames=max(1, args.steps), time_budget_s=budget, warmup=min(args.warmup, 1))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(res["value"], 4), "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.config, "gaussians": scene.count, "resolution": "1920x1080",
+                   "scene_format": fmt, "bounds": "tight", "form": "plain"},
+        "cpu_baseline": res,
+        "e2e": {"value": round(res["value"], 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---- the B200 arm -----------------------------------------------------------------------
+def run_b200(args, dist: Dist):
+    import torch
+
+    import gsr_b200 as G
+
+    torch.cuda.set_device(dist.local_rank)
+    dev = torch.device("cuda", dist.local_rank)
+    scene, cams, fmt, layout = make_config(args.config)
+    gs = G.GpuScene(scene, fmt, layout)
+    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True))
+    stream = torch.cuda.Stream(device=dev)
+    sptr = stream.cuda_stream
+    first = (dist.rank * 37) % len(cams)
+    view = lambda k: cams[(first + k) % len(cams)]  # noqa: E731
+    c_cams = [G.to_c_camera(c) for c in cams]  # the GsrCamera structs a host application passes
+    scam = lambda k: c_cams[(first + k) % len(cams)]  # noqa: E731
+
+    # warm-up (also lets the adaptive list settle)
+    with torch.cuda.stream(stream):
+        for k in range(args.warmup):
+            r.render(scam(k), sptr)
+    stream.synchronize()
+
+    # device-resident timed region
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = r.kernel_launches()
+    dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dist.local_rank) as clocks:
+        start.record(stream)
+        for k in range(args.steps):
+            r.render(scam(args.warmup + k), sptr)
+        end.record(stream)
+        end.synchronize()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = start.elapsed_time(end)
+    launches = r.kernel_launches() - launches0
+    ms_max = dist.max(ms)
+    value = dist.world * args.steps / (ms_max / 1e3)
+
+    # end to end through gsr_render_to_host (camera in, RGB8 image out, synchronized)
+    img = torch.empty((1080, 1920, 3), dtype=torch.uint8).pin_memory() if args.config.startswith("plain_1080p") else \
+        torch.empty((cams[0].height, cams[0].width, 3), dtype=torch.uint8).pin_memory()
+    out = img.numpy()
+    for k in range(min(args.warmup, 5)):
+        r.render_to_host(view(k), out, sptr)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream)
+    for k in range(args.steps):
+        r.render_to_host(view(args.warmup + k), out, sptr)
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    e2e_ms = max(e0.elapsed_time(e1), wall * 1e3)
+    e2e_ms = dist.max(e2e_ms)
+    e2e_value = dist.world * args.steps / (e2e_ms / 1e3)
+
+    # per-pass times (CUDA events between the kernels, a separate run) and the roofline
+    r.set_timing(True)
+    passes = {}
+    nt = 20
+    for k in range(nt):
+        r.render(scam(k), sptr)
+        stream.synchronize()
+        for name, t in r.pass_times().items():
+            passes[name] = passes.get(name, 0.0) + t / nt
+    r.set_timing(False)
+    ctl = r.read_control()
+    peak, peak_kind = load_peaks()
+    fb = front_bytes(fmt, ctl, scene.count)
+    front_ms = passes.get("reset + preprocess + scan + duplicate", float("nan"))
+    sort_ms = passes.get("tile sort (total)", float("nan"))
+    achieved = fb / (front_ms * 1e-3) / 1e9
+    sb = sort_bytes(ctl)
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": dist.world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.config, "gaussians": scene.count, "resolution": f"{cams[0].width}x{cams[0].height}",
+                   "scene_format": f"{fmt}/{layout}", "bounds": "tight", "list": "adaptive", "sort": "global 64-bit onesweep",
+                   "form": "plain (no batching, SH colour)", "views": "300-frame orbit r=14 h=2",
+                   "l2": "inputs larger than L2 (scene 298 MB fp32), no flush",
+                   "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "1 GPU"},
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": 200,
+                "d2h_bytes_per_step": int(out.nbytes)},
+        "gpu_launches": int(launches),
+        "roofline": {"bound": "hbm", "kernel": "front (preprocess+count+scan+emit)", "achieved": round(achieved, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                     "peak_kind": peak_kind, "algorithmic_bytes": int(fb)},
+        "passes_ms": {k: round(v, 4) for k, v in passes.items()},
+        "sort": {"bytes": int(sb), "ms": round(sort_ms, 4), "GB/s": round(sb / (sort_ms * 1e-3) / 1e9, 1),
+                 "passes": ctl.sort_passes, "key_bits": ctl.key_bits},
+        "frame": {"visible": ctl.visible, "entries": ctl.entries, "duplicates": ctl.duplicates,
+                  "overflow": ctl.overflow, "capacity": r.capacity()[0]},
+        "clocks": clocks.summary(),
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_reference_run(scene, cams, max_frames=args.cpu_frames, time_budget_s=30.0)
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+    r.close()
+    gs.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=35)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default="plain_1080p")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-frames", type=int, default=10)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be >= 3")
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    dist = Dist(os.environ.get("GSR_BENCH_BACKEND", "nccl"))
+    try:
+        run_b200(args, dist)
+    finally:
+        dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -147,8 +147,8 @@ __device__ __forceinline__ uint32_t gaussianDegree(const SceneArgs& s, uint32_t 
 
 // preprocessGaussian (splat_math.cpp:153-193) with the GPU culls of splat_preprocess.comp.
 template <int GEOM, int COLOR>
-__device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, uint32_t i, DevSplat& s, TileRect& rect) {
-    const DevCamera& cam = reinterpret_cast<const DevCamera&>(a.cam);
+__device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, const DevCamera& cam, uint32_t i, DevSplat& s,
+                                                  TileRect& rect) {
     const float4 pa = loadPosAlpha<GEOM>(a.scene, i);
     const float* v = cam.v;
     const float t[3] = {v[0] * pa.x + v[4] * pa.y + v[8] * pa.z + v[12], v[1] * pa.x + v[5] * pa.y + v[9] * pa.z + v[13],
@@ -193,6 +193,7 @@ __device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, uint32_t i
 template <int GEOM, int COLOR>
 __global__ void __launch_bounds__(kFrontThreads) frontKernel(const __grid_constant__ FrontArgs a) {
     __shared__ uint32_t sBlock;
+    __shared__ DevCamera sCam;  // the frame's camera, read once per block from its device copy
     __shared__ uint32_t sWarpTotals[kFrontThreads / 32];
     __shared__ uint32_t sCull[kCullReasonCount];
     __shared__ uint32_t sExclusive;
@@ -207,6 +208,9 @@ __global__ void __launch_bounds__(kFrontThreads) frontKernel(const __grid_consta
         sMismatch = 0;
     }
     if (tid < kCullReasonCount) sCull[tid] = 0;
+    static_assert(sizeof(DevCamera) == sizeof(DevCameraArgs) && sizeof(DevCamera) % 4 == 0, "camera layout");
+    if (tid < sizeof(DevCamera) / 4)
+        reinterpret_cast<uint32_t*>(&sCam)[tid] = reinterpret_cast<const uint32_t*>(a.cam)[tid];
     __syncthreads();
     const uint32_t block = sBlock;
     const uint32_t i = block * kFrontThreads + tid;
@@ -221,7 +225,7 @@ __global__ void __launch_bounds__(kFrontThreads) frontKernel(const __grid_consta
     cv.useEllipse = false;
     cv.bins = BinRect{0, 0, 0, 0};
     if (i < a.count) {
-        reason = preprocessOne<GEOM, COLOR>(a, i, s, rect);
+        reason = preprocessOne<GEOM, COLOR>(a, sCam, i, s, rect);
         if (reason == kCullVisible) {
             cv = makeCoverage(a.bounds, rect, a.binSize, a.gridX, a.gridY, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
                               s.opacity, a.logf);

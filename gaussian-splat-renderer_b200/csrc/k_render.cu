@@ -32,8 +32,13 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
     const uint32_t tx = tile % a.tilesX, ty = tile / a.tilesX;
     const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
     const bool inside = px < a.width && py < a.height;
-    const uint2 range = reinterpret_cast<const uint2*>(a.ranges)[tile];
-    const uint32_t* values = a.values[a.ctl->c.sorted_buffer];
+    uint2 range = reinterpret_cast<const uint2*>(a.ranges)[tile];
+    // a frame whose look-back gave up (GSR_CONTROL_TIMEOUT) has meaningless ranges: every index
+    // read below stays inside the list and the scene all the same
+    const uint32_t entries = a.ctl->c.entries;
+    range.y = range.y < entries ? range.y : entries;
+    range.x = range.x < range.y ? range.x : range.y;
+    const uint32_t* values = a.values[a.ctl->c.sorted_buffer & 1u];
     const float4* records = reinterpret_cast<const float4*>(a.splats);
     const float fx = float(px), fy = float(py);
     float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
@@ -42,7 +47,11 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
         if (__syncthreads_count(done) == kRenderThreads) break;
         const uint32_t j = start + tid;
         if (j < range.y) {
-            const uint32_t g = __ldg(&values[j]);
+            uint32_t g = __ldg(&values[j]);
+            if (g >= a.count) {
+                atomicOr(&a.ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
+                g = 0;
+            }
             sCenter[tid] = __ldg(&records[size_t(g) * 3]);
             sConic[tid] = __ldg(&records[size_t(g) * 3 + 1]);
             sColor[tid] = __ldg(&records[size_t(g) * 3 + 2]);

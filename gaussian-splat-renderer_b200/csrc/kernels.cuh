@@ -30,7 +30,7 @@ struct SceneArgs {
 
 // Arguments of the fused per-gaussian kernel (preprocess + count + scan + key emission).
 struct FrontArgs {
-    DevCameraArgs cam;
+    const DevCameraArgs* cam;  // device copy of the frame's SplatCamera (written by the frame itself)
     SceneArgs scene;
     uint32_t count;       // N
     int evalDegree;       // min(stored degree, max_sh_degree)
@@ -85,6 +85,7 @@ struct RenderArgs {
     float4* image;            // W*H
     uint8_t* rgb8;            // W*H*3 or null
     uint32_t width, height, tilesX, tilesY;
+    uint32_t count;           // N: gaussian indices read from the list are checked against it
     DeviceControl* ctl;
 };
 

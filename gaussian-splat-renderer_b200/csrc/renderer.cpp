@@ -196,17 +196,28 @@ struct GsrRenderer {
     uint32_t passesUpper = 0;
     DevBuf ranges, image, rgb8;
     // readback slots (2 frames late)
+    // Per frame slot: the control readback, the camera (pinned, copied to the slot's device
+    // copy by the frame itself), and the frame captured as a CUDA graph.
     struct Slot {
         GsrControl* host = nullptr;
+        DevCameraArgs* camHost = nullptr;
+        DevBuf camDevice;
         cudaEvent_t done = nullptr;
         bool used = false;
         uint64_t frameIndex = 0;
+        cudaGraphExec_t graph = nullptr;
+        const void* graphList = nullptr;   // the list / image the graph was captured with
+        const void* graphImage = nullptr;
+        ~Slot() {
+            if (graph) cudaGraphExecDestroy(graph);
+        }
     };
-    std::vector<Slot> slots;
+    std::vector<std::unique_ptr<Slot>> slots;
     GsrControl lastStats{};
     bool lastStatsValid = false;
     uint64_t lastStatsFrame = 0;
     uint64_t frameIndex = 0;
+    uint64_t kernelLaunches = 0;  // kernels of this library launched by render()
     uint32_t forceTimeout = 0;
     // timing
     bool timing = false;
@@ -215,13 +226,17 @@ struct GsrRenderer {
     float passMs[kPasses] = {};
     bool timed = false;
 
+    cudaStream_t captureStream = nullptr;  // graphs are captured here (never the legacy stream)
+
     ~GsrRenderer() {
         for (auto& s : slots) {
-            if (s.host) cudaFreeHost(s.host);
-            if (s.done) cudaEventDestroy(s.done);
+            if (s->host) cudaFreeHost(s->host);
+            if (s->camHost) cudaFreeHost(s->camHost);
+            if (s->done) cudaEventDestroy(s->done);
         }
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
+        if (captureStream) cudaStreamDestroy(captureStream);
     }
 
     uint32_t passesFor(uint32_t tileCount) const {
@@ -344,7 +359,7 @@ struct GsrRenderer {
             if (rc) return rc;
         }
         if (slots.empty()) return fail(GSR_ERROR_INVALID_ARGUMENT, "renderer not initialised");
-        Slot& slot = slots[frameIndex % slots.size()];
+        Slot& slot = *slots[frameIndex % slots.size()];
         readSlot(slot);
         if (slot.used) {  // still in flight: wait for it (the reference's frame fence)
             GSR_CUDA(cudaEventSynchronize(slot.done));
@@ -352,18 +367,57 @@ struct GsrRenderer {
         }
         int rc = adaptCapacity(stream);
         if (rc) return rc;
+        // the slot's previous frame has completed: its pinned camera may be overwritten
+        static_assert(sizeof(DevCameraArgs) == sizeof(GsrSplatCamera), "camera layout");
+        std::memcpy(slot.camHost, &cam, sizeof(cam));
+        const bool graphed = settings.use_graph && !timing && forceTimeout == 0;
+        if (graphed) {
+            if (!slot.graph || slot.graphList != list.get() || slot.graphImage != image.p) {
+                if (slot.graph) cudaGraphExecDestroy(slot.graph);
+                slot.graph = nullptr;
+                if (!captureStream) GSR_CUDA(cudaStreamCreateWithFlags(&captureStream, cudaStreamNonBlocking));
+                GSR_CUDA(cudaStreamBeginCapture(captureStream, cudaStreamCaptureModeThreadLocal));
+                const int erc = enqueue(slot, captureStream);
+                cudaGraph_t g = nullptr;
+                const cudaError_t ce = cudaStreamEndCapture(captureStream, &g);
+                if (erc) {
+                    if (g) cudaGraphDestroy(g);
+                    return erc;
+                }
+                if (ce != cudaSuccess) return cudaFail(ce, "cudaStreamEndCapture");
+                const cudaError_t ie = cudaGraphInstantiate(&slot.graph, g, 0);
+                cudaGraphDestroy(g);
+                if (ie != cudaSuccess) return cudaFail(ie, "cudaGraphInstantiate");
+                slot.graphList = list.get();
+                slot.graphImage = image.p;
+            }
+            GSR_CUDA(cudaGraphLaunch(slot.graph, stream));
+        } else {
+            rc = enqueue(slot, stream);
+            if (rc) return rc;
+        }
+        forceTimeout = 0;
+        slot.used = true;
+        slot.frameIndex = frameIndex;
+        kernelLaunches += 5 + list->passes;  // frameBegin, front, histogram, passes, ranges, render
+        timed = timing;
+        ++frameIndex;
+        return GSR_OK;
+    }
+
+    // The frame's work on `stream`: the camera copy, the kernels, the control readback and the
+    // completion events (captured once per slot when graphs are on).
+    int enqueue(Slot& slot, cudaStream_t stream) {
         List& l = *list;
         DeviceControl* ctl = control.as<DeviceControl>();
         SortPlan* sortPlan = plan.as<SortPlan>();
         const uint32_t tileCount = tilesX * tilesY;
         if (timing) GSR_CUDA(cudaEventRecord(ev[0], stream));
-
+        GSR_CUDA(cudaMemcpyAsync(slot.camDevice.p, slot.camHost, sizeof(DevCameraArgs), cudaMemcpyHostToDevice, stream));
         GSR_CUDA(launchFrameBegin(ctl, scene.count, l.capacity, ranges.as<uint32_t>(), tileCount * 2, sortPlan,
                                   forceTimeout, stream));
-        forceTimeout = 0;
         FrontArgs fa{};
-        static_assert(sizeof(DevCameraArgs) == sizeof(GsrSplatCamera), "camera layout");
-        std::memcpy(&fa.cam, &cam, sizeof(cam));
+        fa.cam = slot.camDevice.as<DevCameraArgs>();
         fa.scene.b0 = static_cast<const uint4*>(scene.buffers[0]);
         fa.scene.b1 = static_cast<const uint4*>(scene.layout == GSR_LAYOUT_AOS ? scene.buffers[0] : scene.buffers[1]);
         fa.scene.b2 = static_cast<const uint4*>(scene.buffers[2]);
@@ -418,6 +472,7 @@ struct GsrRenderer {
         ra.height = height;
         ra.tilesX = tilesX;
         ra.tilesY = tilesY;
+        ra.count = scene.count;
         ra.ctl = ctl;
         GSR_CUDA(launchRanges(ra, l.capacity, stream));
         if (timing) GSR_CUDA(cudaEventRecord(ev[3], stream));
@@ -428,10 +483,6 @@ struct GsrRenderer {
         GSR_CUDA(cudaEventRecord(slot.done, stream));
         GSR_CUDA(cudaEventRecord(l.lastUse, stream));
         if (timing) GSR_CUDA(cudaEventRecord(ev[5], stream));
-        slot.used = true;
-        slot.frameIndex = frameIndex;
-        timed = timing;
-        ++frameIndex;
         return GSR_OK;
     }
 };
@@ -708,11 +759,14 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     GSR_CUDA(cudaMemset(r->control.p, 0, sizeof(DeviceControl)));
     GSR_CUDA(r->plan.alloc(sizeof(SortPlan)));
     GSR_CUDA(cudaMemset(r->plan.p, 0, sizeof(SortPlan)));
-    r->slots.resize(r->settings.frames_in_flight);
-    for (auto& s : r->slots) {
-        GSR_CUDA(cudaMallocHost(&s.host, sizeof(GsrControl)));
-        std::memset(s.host, 0, sizeof(GsrControl));
-        GSR_CUDA(cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+    for (uint32_t k = 0; k < r->settings.frames_in_flight; ++k) {
+        auto s = std::make_unique<GsrRenderer::Slot>();
+        GSR_CUDA(cudaMallocHost(&s->host, sizeof(GsrControl)));
+        std::memset(s->host, 0, sizeof(GsrControl));
+        GSR_CUDA(cudaMallocHost(&s->camHost, sizeof(DevCameraArgs)));
+        GSR_CUDA(s->camDevice.alloc(sizeof(DevCameraArgs)));
+        GSR_CUDA(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
+        r->slots.push_back(std::move(s));
     }
     for (auto& e : r->ev) GSR_CUDA(cudaEventCreate(&e));
     *out = r.release();
@@ -761,7 +815,7 @@ int gsr_render_to_host(GsrRenderer* r, const GsrCamera* camera, void* host, uint
 
 int gsr_renderer_last_stats(GsrRenderer* r, GsrControl* out, uint64_t* frameIndex) {
     if (!r || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
-    for (auto& s : r->slots) r->readSlot(s);
+    for (auto& s : r->slots) r->readSlot(*s);
     if (!r->lastStatsValid) return GSR_ERROR_NOT_READY;
     *out = r->lastStats;
     if (frameIndex) *frameIndex = r->lastStatsFrame;
@@ -851,6 +905,12 @@ int gsr_renderer_capacity(GsrRenderer* r, uint32_t* capacity, uint32_t* maxCapac
     if (capacity) *capacity = r->list ? r->list->capacity : 0;
     if (maxCapacity) *maxCapacity = r->maxCapacity;
     if (resizes) *resizes = r->listResizes;
+    return GSR_OK;
+}
+
+int gsr_renderer_kernel_launches(GsrRenderer* r, uint64_t* count) {
+    if (!r || !count) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    *count = r->kernelLaunches;
     return GSR_OK;
 }
 

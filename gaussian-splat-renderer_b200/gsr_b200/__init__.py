@@ -161,6 +161,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_renderer_pass_times": (C.c_int, [vp, vp, vp, u32, C.POINTER(u32)]),
         "gsr_renderer_capacity": (C.c_int, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]),
         "gsr_renderer_debug_force_timeout": (C.c_int, [vp, u32]),
+        "gsr_renderer_kernel_launches": (C.c_int, [vp, C.POINTER(u64)]),
         "gsr_renderer_destroy": (None, [vp]),
         "gsr_scan": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_sort_pairs": (C.c_int, [vp, vp, vp, u32, u32, vp]),
@@ -280,7 +281,10 @@ class Renderer:
     def render(self, camera, stream: int = 0):
         """camera: scenes.ViewerCamera (view/proj/model) or a SplatCamera."""
         lib = load()
-        if isinstance(camera, SplatCamera):
+        if isinstance(camera, CCamera):
+            check(lib.gsr_render(self._h, C.byref(camera), C.c_void_p(stream)))
+            self.width, self.height = camera.width, camera.height
+        elif isinstance(camera, SplatCamera):
             check(lib.gsr_render_splat_camera(self._h, C.byref(camera), C.c_void_p(stream)))
             self.width, self.height = camera.width, camera.height
         else:
@@ -355,6 +359,11 @@ class Renderer:
         c, m, r = C.c_uint32(), C.c_uint32(), C.c_uint32()
         check(load().gsr_renderer_capacity(self._h, C.byref(c), C.byref(m), C.byref(r)))
         return c.value, m.value, r.value
+
+    def kernel_launches(self) -> int:
+        n = C.c_uint64()
+        check(load().gsr_renderer_kernel_launches(self._h, C.byref(n)))
+        return n.value
 
     def force_timeout(self, iterations: int):
         check(load().gsr_renderer_debug_force_timeout(self._h, iterations))

@@ -220,6 +220,8 @@ int gsr_renderer_set_timing(GsrRenderer* r, int enabled);
 int gsr_renderer_pass_times(GsrRenderer* r, float* ms, const char** names, uint32_t capacity, uint32_t* count);
 /* Capacity of the current list in entries, the budget's maximum, and list resizes so far. */
 int gsr_renderer_capacity(GsrRenderer* r, uint32_t* capacity, uint32_t* max_capacity, uint32_t* resizes);
+/* Kernels of this library that gsr_render has launched on this renderer so far. */
+int gsr_renderer_kernel_launches(GsrRenderer* r, uint64_t* count);
 /* Test hook: forces the look-back waits of the next frame to see no predecessor, so that
  * they run into their iteration limit and report GSR_CONTROL_TIMEOUT (iterations = limit). */
 int gsr_renderer_debug_force_timeout(GsrRenderer* r, uint32_t iterations);

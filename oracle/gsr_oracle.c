@@ -1182,3 +1182,7 @@ void gsr_oracle_quantize_rgb8(uint32_t pixels, const float* rgb, uint32_t srcStr
             out[(size_t)p * 3 + c] = (uint8_t)lroundf(cl * 255.0f);
         }
 }
+
+void gsr_oracle_logf_range(uint32_t first_bits, uint32_t count, float* out) {
+    for (uint32_t j = 0; j < count; ++j) out[j] = logf(bitsf(first_bits + j));
+}

@@ -111,6 +111,9 @@ void gsr_oracle_decode(uint32_t n, const uint32_t* desc, const uint64_t* sizes, 
                        float* scales, float* rotations, float* sh);
 int gsr_oracle_select_sh_degree(const float* sh, int storedDegree, float opacity, float threshold255);
 
+/* logf (the C library's) of `count` consecutive float bit patterns starting at first_bits. */
+void gsr_oracle_logf_range(uint32_t first_bits, uint32_t count, float* out);
+
 /* Image helpers: quantize like the reference's PNG writer (image_io.cpp:55-56,
  * lround(clamp(v, 0, 1) * 255)), and PSNR with peak 1.0 (tools/imgdiff.cpp:127). */
 void gsr_oracle_quantize_rgb8(uint32_t pixels, const float* rgb, uint32_t srcStride, uint8_t* out);

@@ -120,6 +120,7 @@ class Oracle:
             f("perspective", None, [C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p])
             f("tile_list", C.c_uint64, None)
             f("preprocess_degrees", None, None)
+            f("logf_range", None, [C.c_uint32, C.c_uint32, C.c_void_p])
 
     def _f(self, name, restype, argtypes):
         fn = getattr(self.lib, self.prefix + name)
@@ -258,6 +259,11 @@ class Oracle:
     def select_sh_degree(self, sh_triplets, stored_degree, opacity, threshold255):
         s = np.ascontiguousarray(sh_triplets, np.float32)
         return self._select_sh_degree(_p(s), stored_degree, C.c_float(opacity), C.c_float(threshold255))
+
+    def logf_range(self, first_bits: int, count: int) -> np.ndarray:
+        out = np.zeros(count, np.float32)
+        self._logf_range(first_bits, count, _p(out))
+        return out
 
     def float_to_half(self, v: float) -> int:
         return self._float_to_half(C.c_float(v))

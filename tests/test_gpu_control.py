@@ -1,0 +1,87 @@
+"""Control block, failure detection and the adaptive list on the GPU.
+
+* Bounded device waits: a test hook makes every decoupled look-back of the next frame see no
+  published predecessor, so the waits run into their iteration limit; the frame reports
+  GSR_CONTROL_TIMEOUT (gsr_read_control returns GSR_ERROR_DEVICE_TIMEOUT), nothing faults, and
+  the next frame is correct again (the context stays usable).
+* The adaptive list (splat_tile_renderer.cpp:444-486): a list that starts too small overflows
+  (clamped, counted), grows to 1.5 M once the readback arrives, and renders exactly afterwards.
+* lastStats: the control block of a frame frames_in_flight frames old, without a stall.
+"""
+import numpy as np
+import pytest
+
+from helpers import oracle_frame, tile_raster_camera, tile_raster_scene
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def setup():
+    scene = tile_raster_scene(100_000, 21)
+    return scene, tile_raster_camera()
+
+
+def test_forced_lookback_timeout_is_reported_and_recoverable(gpu, port, setup):
+    scene, cam = setup
+    gs = gpu.GpuScene(scene)
+    r = gpu.Renderer(gs, gpu.Settings(adaptive_list=False))
+    r.render(cam)
+    good = r.read_back()
+    r.force_timeout(2000)
+    r.render(cam)
+    c = r.read_control()
+    assert c.status & gpu.CONTROL_TIMEOUT
+    assert c.timeout_where in (1, 2)
+    st = gpu.load().gsr_read_control(r.handle, gpu.C.byref(gpu.Control()))
+    assert st == 5  # GSR_ERROR_DEVICE_TIMEOUT
+    r.render(cam)  # the next frame is valid again
+    again = r.read_back()
+    assert again[4].status == 0
+    for a, b in zip(good[:4], again[:4]):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_adaptive_list_grows_after_overflow(gpu, port, setup):
+    scene, cam = setup
+    gs = gpu.GpuScene(scene)
+    r = gpu.Renderer(gs, gpu.Settings(adaptive_list=True, adaptive_initial_entries=4096, frames_in_flight=2))
+    r.render(cam)
+    c0 = r.read_control()
+    cap0 = r.capacity()[0]
+    assert cap0 == 4096 and c0.overflow > 0 and c0.entries == cap0
+    for _ in range(4):
+        r.render(cam)
+    cap1, maxcap, resizes = r.capacity()
+    assert resizes >= 1 and cap1 >= int(1.5 * c0.duplicates) // 2048 * 2048 and cap1 <= maxcap
+    lo, hi, val, ranges, ctl = r.read_back()
+    assert ctl.overflow == 0
+    _, osp, ocounts, olist = oracle_frame(port, scene, cam, bounds=1)
+    np.testing.assert_array_equal(val, olist["values"])
+    np.testing.assert_array_equal(ranges, olist["ranges"])
+
+
+def test_last_stats_arrive_late_without_stall(gpu, setup):
+    scene, cam = setup
+    gs = gpu.GpuScene(scene)
+    r = gpu.Renderer(gs, gpu.Settings(frames_in_flight=2))
+    c, idx = r.last_stats()
+    assert c is None
+    for _ in range(3):
+        r.render(cam)
+    import torch
+
+    torch.cuda.synchronize()
+    c, idx = r.last_stats()
+    assert c is not None and idx >= 0
+    assert c.duplicates == r.read_control().duplicates
+
+
+def test_kernel_launch_count(gpu, setup):
+    scene, cam = setup
+    gs = gpu.GpuScene(scene)
+    r = gpu.Renderer(gs, gpu.Settings())
+    r.render(cam)
+    n1 = r.kernel_launches()
+    r.render(cam)
+    assert r.kernel_launches() == 2 * n1 and n1 >= 6

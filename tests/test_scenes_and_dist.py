@@ -1,0 +1,87 @@
+"""Host logic without a GPU: the synthetic workloads (seeded, the stated distributions and
+sizes) and the multi-rank plumbing of bench.py (one process per GPU; max over ranks and
+barriers), run as two gloo ranks on the CPU."""
+import os
+import socket
+import subprocess
+import sys
+import textwrap
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+
+
+def test_scene_generator_is_seeded_and_activated():
+    from gsr_b200 import scenes
+
+    a = scenes.make_scene(50_000, seed=0, ball_radius=5.0)
+    b = scenes.make_scene(50_000, seed=0, ball_radius=5.0)
+    for x, y in zip((a.pos_alpha, a.scales, a.rotations, a.sh), (b.pos_alpha, b.scales, b.rotations, b.sh)):
+        assert x.dtype == np.float32 and np.array_equal(x, y)
+    r = np.linalg.norm(a.pos_alpha[:, :3], axis=1)
+    assert r.max() <= 5.0 + 1e-5 and abs(np.median(r) - 5.0 * 0.5 ** (1 / 3)) < 0.05  # uniform in the ball
+    ls = np.log(a.scales[:, :3])
+    assert abs(ls.mean() + 3.5) < 0.02 and abs(ls.std() - 0.7) < 0.02
+    q = np.linalg.norm(a.rotations, axis=1)
+    assert np.allclose(q, 1.0, atol=1e-6)
+    o = a.pos_alpha[:, 3]
+    assert 0.0 < o.min() and o.max() < 1.0 and abs(np.median(o) - 0.5) < 0.01  # sigmoid(N(0, 1))
+    sh = a.sh.reshape(-1, 16, 3)
+    assert abs(sh[:, 0].std() - 0.5) < 0.01 and abs(sh[:, 1:].std() - 0.1) < 0.002
+
+
+def test_named_workloads_sizes():
+    from gsr_b200 import scenes
+
+    s, cams = scenes.plain_720p()
+    assert s.count == 100_000 and len(cams) == 1 and (cams[0].width, cams[0].height) == (1280, 720)
+    orbit = scenes.orbit_cameras(300, 14.0, 2.0, 1920, 1080)
+    assert len(orbit) == 300
+    V = np.asarray(orbit[0].view, np.float64).reshape(4, 4)  # V[c, r]: column c, row r
+    eye0 = -V[:3, :3] @ V[3, :3]  # camera centre = -R^T t
+    assert np.allclose(eye0, [0.0, 2.0, 14.0], atol=1e-4)
+    b = scenes.batched_cameras(64, seed=2)
+    assert len(b) == 64 and {(c.width, c.height) for c in b} <= {(256, 256), (640, 480), (1280, 720), (1920, 1080)}
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+@pytest.mark.timeout(120)
+def test_bench_ranks_take_the_max_over_ranks():
+    """Two ranks (gloo, CPU) through bench.Dist: barrier, then max over ranks of each rank's
+    time, as the N-GPU bench reports it."""
+    port = _free_port()
+    code = textwrap.dedent(f"""
+        import os, sys
+        sys.path.insert(0, {str(REPO)!r})
+        import bench
+        d = bench.Dist("gloo")
+        d.barrier()
+        v = d.max(10.0 + d.rank)
+        d.barrier()
+        print("rank", d.rank, "max", v, flush=True)
+        d.close()
+    """)
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), LOCAL_RANK=str(rank), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port))
+        procs.append(subprocess.Popen([sys.executable, "-c", code], env=env, stdout=subprocess.PIPE,
+                                      stderr=subprocess.STDOUT, text=True))
+    outs = [p.communicate(timeout=100)[0] for p in procs]
+    assert all(p.returncode == 0 for p in procs), outs
+    for rank, out in enumerate(outs):
+        assert f"rank {rank} max 11.0" in out, out
+
+
+def test_reference_arm_on_other_ranks_exits_without_work():
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2")
+    r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "3"],
+                       env=env, capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.strip() == ""
