@@ -1,16 +1,15 @@
-// The front of the splat-tiles frame: reset, then ONE kernel per frame that does, per gaussian
-// (one thread each, 256 per block, blocks ordered by a ticket):
+// The front of the splat-tiles frame, the reference's passes 0-7 (splat_tile_renderer.cpp:653-739):
 //
-//   scene decode  -> preprocess (near/opacity culls, cov3D, EWA cov2D, conic/radius, pixel
-//   centre, 16-px rectangle, SH colour) -> tight tile count -> block scan + decoupled
-//   look-back (the exclusive prefix of the counts in index order = the list offsets)
-//   -> key emission (one (tile << 32 | depth bits, index) entry per covered tile)
+//   frameBegin   reset of the control block and the tile ranges
+//   preprocess   per gaussian: scene decode, near/opacity culls, cov3D, EWA cov2D, conic/radius,
+//                pixel centre, 16-px rectangle, SH colour, tight tile count (streaming, no waits)
+//   scan         exclusive prefix of the counts in index order (GpuScan, k_sort.cu) = the list
+//                offsets, whose last block clamps the list to the capacity (tile_setup)
+//   duplicate    per gaussian: one (tile << 32 | depth bits, index) entry per covered tile
 //
-// i.e. the reference's passes splat_preprocess.comp (GSR_TILES), scan_reduce/blocks/downsweep
-// over the tile counts, tile_setup.comp and tile_duplicate.comp (global mode, per splat), in
-// one read of each gaussian. The placement comes from the scan in index order (INRIA's
-// scheme), so the unsorted list equals the reference's entry for entry; atomics are used only
-// for counters. Built with -fmad=false: see splat_math.cuh.
+// The placement comes from the scan in index order (INRIA's scheme), so the unsorted list equals
+// the reference's entry for entry; atomics are used only for counters. Built with -fmad=false:
+// see splat_math.cuh.
 #include <cuda_fp16.h>
 
 #include "kernels.cuh"
@@ -190,107 +189,68 @@ __device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, const DevC
     return kCullVisible;
 }
 
+// 1) Preprocess + tight count, one thread per gaussian (splat_preprocess.comp:283-318, GSR_TILES):
+//    writes the splat record of visible gaussians and every gaussian's tile count; cull counters
+//    with one ballot per warp and one atomic per block and reason. No waits: a streaming kernel.
 template <int GEOM, int COLOR>
-__global__ void __launch_bounds__(kFrontThreads) frontKernel(const __grid_constant__ FrontArgs a) {
-    __shared__ uint32_t sBlock;
+__global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_constant__ FrontArgs a) {
     __shared__ DevCamera sCam;  // the frame's camera, read once per block from its device copy
-    __shared__ uint32_t sWarpTotals[kFrontThreads / 32];
     __shared__ uint32_t sCull[kCullReasonCount];
-    __shared__ uint32_t sExclusive;
-    __shared__ uint32_t sDepthMin, sDepthMax, sTileMax, sMismatch;
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    DeviceControl* ctl = a.ctl;
-    if (tid == 0) {
-        sBlock = atomicAdd(&ctl->tickets[0], 1u);
-        sDepthMin = 0xFFFFFFFFu;
-        sDepthMax = 0;
-        sTileMax = 0;
-        sMismatch = 0;
-    }
+    const uint32_t tid = threadIdx.x, lane = tid & 31;
     if (tid < kCullReasonCount) sCull[tid] = 0;
     static_assert(sizeof(DevCamera) == sizeof(DevCameraArgs) && sizeof(DevCamera) % 4 == 0, "camera layout");
     if (tid < sizeof(DevCamera) / 4)
         reinterpret_cast<uint32_t*>(&sCam)[tid] = reinterpret_cast<const uint32_t*>(a.cam)[tid];
     __syncthreads();
-    const uint32_t block = sBlock;
-    const uint32_t i = block * kFrontThreads + tid;
-    const uint32_t epoch = ctl->c.epoch;
-
-    // 1) preprocess + tight count
+    const uint32_t i = blockIdx.x * kFrontThreads + tid;
     uint32_t reason = kCullReasonCount;  // threads past the end
-    uint32_t count = 0;
-    DevSplat s;
-    TileRect rect{0, 0, 0, 0};
-    Coverage cv;
-    cv.useEllipse = false;
-    cv.bins = BinRect{0, 0, 0, 0};
     if (i < a.count) {
+        DevSplat s;
+        TileRect rect{0, 0, 0, 0};
+        uint32_t count = 0;
         reason = preprocessOne<GEOM, COLOR>(a, sCam, i, s, rect);
         if (reason == kCullVisible) {
-            cv = makeCoverage(a.bounds, rect, a.binSize, a.gridX, a.gridY, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
-                              s.opacity, a.logf);
+            const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, a.gridX, a.gridY, s.cx, s.cy, s.conicA,
+                                             s.conicB, s.conicC, s.opacity, a.logf);
             count = coverageCount(cv, a.binSize);
             s.cullReason = kCullVisible;
             reinterpret_cast<DevSplat*>(a.splats)[i] = s;
         }
         a.tileCounts[i] = count;
     }
-    // cull counters: one ballot per reason and warp, one atomic per reason and block
 #pragma unroll
     for (uint32_t r = 0; r < kCullReasonCount; ++r) {
         const uint32_t n = __popc(__ballot_sync(0xFFFFFFFFu, reason == r));
         if (lane == 0 && n) atomicAdd(&sCull[r], n);
     }
-
-    // 2) block scan of the counts
-    uint32_t incl = count;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-        if (lane >= uint32_t(d)) incl += o;
-    }
-    if (lane == 31) sWarpTotals[warp] = incl;
     __syncthreads();
-    uint32_t warpBase = 0, blockTotal = 0;
-#pragma unroll
-    for (uint32_t w = 0; w < kFrontThreads / 32; ++w) {
-        const uint32_t t = sWarpTotals[w];
-        if (w < warp) warpBase += t;
-        blockTotal += t;
-    }
-    const uint32_t threadExclusive = warpBase + incl - count;
+    if (tid < kCullReasonCount && sCull[tid]) atomicAdd(&a.ctl->c.cull_counts[tid], sCull[tid]);
+}
 
-    // 3) decoupled look-back over the blocks before this one
-    if (warp == 0) {
-        if (lane == 0)
-            stRelease(&a.scanStatus[block], packStatus(epoch, block == 0 ? kFlagInclusive : kFlagAggregate, blockTotal));
-        uint32_t exclusive = 0;
-        if (block > 0) exclusive = warpLookback(a.scanStatus, int(block), epoch, ctl, kWaitScan);
-        if (lane == 0) {
-            if (block > 0) stRelease(&a.scanStatus[block], packStatus(epoch, kFlagInclusive, exclusive + blockTotal));
-            sExclusive = exclusive;
-        }
+// 3) Key emission, one thread per gaussian in index order (tile_duplicate.comp:177-221, global
+//    mode): the splat's tiles row by row at offsets [offset, offset + count), dropped at or past
+//    the capacity. The coverage is rebuilt from the splat's record with the same functions and
+//    the same inputs as the count, so it enumerates exactly `count` tiles; a disagreement would be
+//    counted (coverageMismatch) and padded with the sentinel tile, as the reference does.
+__global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_constant__ FrontArgs a) {
+    __shared__ uint32_t sDepthMin, sDepthMax, sTileMax, sMismatch, sAny;
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) {
+        sDepthMin = 0xFFFFFFFFu;
+        sDepthMax = 0;
+        sTileMax = 0;
+        sMismatch = 0;
+        sAny = 0;
     }
-    if (tid < kCullReasonCount && sCull[tid]) atomicAdd(&ctl->c.cull_counts[tid], sCull[tid]);
     __syncthreads();
-    const uint32_t offset = sExclusive + threadExclusive;
-    if (i < a.count) a.offsets[i] = offset;
-
-    // 4) the list size and its clamp (tile_setup.comp:16-24), by the last block
-    if (block == gridDim.x - 1 && tid == 0) {
-        const uint32_t m = sExclusive + blockTotal;
-        const uint32_t entries = m < a.capacity ? m : a.capacity;
-        ctl->c.duplicates = m;
-        ctl->c.entries = entries;
-        ctl->c.overflow = m - entries;
-        ctl->c.ranges_groups[0] = (entries + 255u) / 256u;
-        ctl->c.ranges_groups[1] = 1;
-        ctl->c.ranges_groups[2] = 1;
-    }
-
-    // 5) key emission (tile_duplicate.comp:177-221, global mode): the splat's tiles row by
-    //    row at offsets [offset, offset + count), dropped at or past the capacity
+    const uint32_t i = blockIdx.x * kFrontThreads + tid;
+    const uint32_t count = i < a.count ? a.tileCounts[i] : 0u;
     if (count > 0) {
+        const uint32_t offset = a.offsets[i];
+        const DevSplat s = reinterpret_cast<const DevSplat*>(a.splats)[i];
+        const TileRect rect = tileRect(s.cx, s.cy, s.radius, a.cam->tilesX, a.cam->tilesY);
+        const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, a.gridX, a.gridY, s.cx, s.cy, s.conicA, s.conicB,
+                                         s.conicC, s.opacity, a.logf);
         const uint64_t depthBits = __float_as_uint(s.depth);
         const int S = a.binSize;
         int r0, r1;
@@ -310,7 +270,6 @@ __global__ void __launch_bounds__(kFrontThreads) frontKernel(const __grid_consta
                 }
             }
         }
-        // fewer tiles than counted (cannot happen: same functions, same thread): sentinel tile
         const uint32_t sentinel = uint32_t(a.gridX) * uint32_t(a.gridY);
         if (written != count) {
             atomicAdd(&sMismatch, 1u);
@@ -324,9 +283,11 @@ __global__ void __launch_bounds__(kFrontThreads) frontKernel(const __grid_consta
         atomicMin(&sDepthMin, uint32_t(depthBits));
         atomicMax(&sDepthMax, uint32_t(depthBits));
         atomicMax(&sTileMax, tileMax);
+        sAny = 1;
     }
     __syncthreads();
-    if (tid == 0 && blockTotal > 0) {
+    if (tid == 0 && sAny) {
+        DeviceControl* ctl = a.ctl;
         atomicMin(&ctl->c.depth_min_bits, sDepthMin);
         atomicMax(&ctl->c.depth_max_bits, sDepthMax);
         atomicMax(&ctl->c.tile_max, sTileMax);
@@ -397,16 +358,26 @@ cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capaci
 cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s) {
     const uint32_t blocks = (a.count + kFrontThreads - 1) / kFrontThreads;
     if (blocks == 0) return cudaSuccess;
+    // 1) preprocess + count
     if (geometry == GSR_GEOMETRY_SOA_F32 && color == GSR_COLOR_SOA_F32)
-        frontKernel<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32><<<blocks, kFrontThreads, 0, s>>>(a);
+        preprocessKernel<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32><<<blocks, kFrontThreads, 0, s>>>(a);
     else if (geometry == GSR_GEOMETRY_RECORD_F32 && color == GSR_COLOR_RECORD_F32)
-        frontKernel<GSR_GEOMETRY_RECORD_F32, GSR_COLOR_RECORD_F32><<<blocks, kFrontThreads, 0, s>>>(a);
+        preprocessKernel<GSR_GEOMETRY_RECORD_F32, GSR_COLOR_RECORD_F32><<<blocks, kFrontThreads, 0, s>>>(a);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_RECORD_F16)
-        frontKernel<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16><<<blocks, kFrontThreads, 0, s>>>(a);
+        preprocessKernel<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16><<<blocks, kFrontThreads, 0, s>>>(a);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_Q8)
-        frontKernel<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8><<<blocks, kFrontThreads, 0, s>>>(a);
+        preprocessKernel<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8><<<blocks, kFrontThreads, 0, s>>>(a);
     else
         return cudaErrorInvalidValue;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    // 2) exclusive scan of the counts (GpuScan over N), the list size and its clamp
+    //    (tile_setup.comp:16-24) by the scan's last block
+    e = launchScan(a.tileCounts, nullptr, a.offsets, &a.ctl->c.duplicates, a.count, GSR_SCAN_PLAIN, a.scanStatus, a.ctl,
+                   s, a.capacity, kWaitScan);
+    if (e != cudaSuccess) return e;
+    // 3) key emission
+    duplicateKernel<<<blocks, kFrontThreads, 0, s>>>(a);
     return cudaGetLastError();
 }
 

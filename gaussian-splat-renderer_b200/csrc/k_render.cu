@@ -1,17 +1,23 @@
 // The tile rasterizer (INRIA renderCUDA; the reference's shaders/tile_render.comp:281-400 and
 // the CPU reference's per-pixel loop, src/splat/reference_renderer.cpp:120-222).
 //
-// One 256-thread block per 16x16 tile, one thread per pixel. The tile's entries
-// [ranges[tile].x, ranges[tile].y) of the sorted list are walked front to back in batches of
-// 256: the block gathers the batch's splat records into shared memory (one record per
-// thread), then every pixel blends the batch with INRIA's test-before-accept rule:
-//   power = -0.5 (A dx^2 + C dy^2) - B dx dy; skip power > 0
-//   alpha = min(0.99, o exp(power));          skip alpha < 1/255
-//   testT = T (1 - alpha); testT < 1e-4 -> the pixel is done (this splat is not blended)
+// One 256-thread block per 16x16 tile, one thread per pixel; warp w owns pixel rows 2w, 2w+1.
+// The tile's entries [ranges[tile].x, ranges[tile].y) are walked front to back in batches of
+// 256 records, double-buffered: while batch b is blended, the records of batch b+1 are gathered
+// into shared memory with cp.async (16-byte LDGSTS, the record of gaussian values[j]). Each
+// entry is then prepared once per block: the conic pre-scaled by -log2(e)/2 so that
+//   alpha = min(0.99, o * 2^(a' dx^2 + b' dx dy + c' dy^2))   ( = o * exp(power) )
+// costs one MUFU.EX2, and the axis-aligned box of its alpha >= 1/255 cutoff ellipse (the
+// reference's threshold with a wider margin, tile_coverage.cpp:24-50) so that a warp skips a
+// splat that cannot reach any of its 32 pixels (every skipped pair has alpha < 1/255, which the
+// loop would skip anyway). Per pair, INRIA's test-before-accept rule:
+//   skip power > 0; skip alpha < 1/255; testT = T (1 - alpha); testT < 1e-4 -> done;
 //   C += colour alpha T; T = testT
-// A whole-tile vote (__syncthreads_count) ends the tile once every pixel is done. Expressions
-// follow the CPU reference's order (this unit is built without FMA contraction), so the float
-// image differs from the CPU's only where CUDA's expf and the C library's expf round apart.
+// and a whole-tile vote (__syncthreads_count) ends the tile once every pixel is done.
+//
+// FMA contraction and the hardware exp2 make the float image differ from the CPU reference's
+// in the last bits (and, for pairs within an ulp of the 1/255 or 1e-4 thresholds, by one such
+// pair's contribution); tests bound it: float PSNR > 60 dB and the 8-bit image within 1/255.
 #include "gsr_device.cuh"
 #include "kernels.cuh"
 
@@ -22,13 +28,34 @@ namespace {
 constexpr int kRenderThreads = 256;
 constexpr float kMaxAlpha = 0.99f;
 constexpr float kMinTransmittance = 1e-4f;
+constexpr float kLog2e = 1.4426950408889634f;
+
+__device__ __forceinline__ void cpAsync16(void* smemDst, const void* gsrc) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smemDst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+__device__ __forceinline__ float fastExp2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+struct RenderShared {
+    float4 raw[2][3][kRenderThreads];  // gathered ProjectedSplat records (3 x 16 B), double-buffered
+    float4 conic[kRenderThreads];      // a', b', c' (pre-scaled), opacity
+    float4 box[kRenderThreads];        // x0, x1, y0, y1 of the cutoff ellipse (pixels)
+    float4 color[kRenderThreads];      // r, g, b, -
+    float2 center[kRenderThreads];
+};
 
 __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_constant__ RenderArgs a) {
-    __shared__ float4 sCenter[kRenderThreads];  // cx, cy, depth, cullReason
-    __shared__ float4 sConic[kRenderThreads];   // A, B, C, opacity
-    __shared__ float4 sColor[kRenderThreads];   // r, g, b, radius
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    RenderShared& sm = *reinterpret_cast<RenderShared*>(smemRaw);
     const uint32_t tile = blockIdx.x;
-    const uint32_t tid = threadIdx.x;
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t tx = tile % a.tilesX, ty = tile / a.tilesX;
     const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
     const bool inside = px < a.width && py < a.height;
@@ -41,10 +68,13 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
     const uint32_t* values = a.values[a.ctl->c.sorted_buffer & 1u];
     const float4* records = reinterpret_cast<const float4*>(a.splats);
     const float fx = float(px), fy = float(py);
+    // this warp's pixel strip
+    const float wx0 = float(tx * 16), wx1 = float(tx * 16 + 15);
+    const float wy0 = float(ty * 16 + 2 * warp), wy1 = wy0 + 1.0f;
     float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
     bool done = !inside;
-    for (uint32_t start = range.x; start < range.y; start += kRenderThreads) {
-        if (__syncthreads_count(done) == kRenderThreads) break;
+
+    auto issue = [&](uint32_t start, int buf) {
         const uint32_t j = start + tid;
         if (j < range.y) {
             uint32_t g = __ldg(&values[j]);
@@ -52,34 +82,79 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
                 atomicOr(&a.ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
                 g = 0;
             }
-            sCenter[tid] = __ldg(&records[size_t(g) * 3]);
-            sConic[tid] = __ldg(&records[size_t(g) * 3 + 1]);
-            sColor[tid] = __ldg(&records[size_t(g) * 3 + 2]);
+            const float4* rec = records + size_t(g) * 3;
+            cpAsync16(&sm.raw[buf][0][tid], rec);
+            cpAsync16(&sm.raw[buf][1][tid], rec + 1);
+            cpAsync16(&sm.raw[buf][2][tid], rec + 2);
+        }
+        cpAsyncCommit();
+    };
+
+    int buf = 0;
+    if (range.x < range.y) issue(range.x, 0);
+    for (uint32_t start = range.x; start < range.y; start += kRenderThreads, buf ^= 1) {
+        if (__syncthreads_count(done) == kRenderThreads) break;
+        // prefetch the next batch while this one is prepared and blended
+        const uint32_t next = start + kRenderThreads;
+        if (next < range.y) issue(next, buf ^ 1);
+        else cpAsyncCommit();
+        cpAsyncWait<1>();
+        __syncthreads();
+        if (start + tid < range.y) {
+            const float4 r0 = sm.raw[buf][0][tid];  // cx, cy, depth, cull
+            const float4 r1 = sm.raw[buf][1][tid];  // A, B, C, opacity
+            const float4 r2 = sm.raw[buf][2][tid];  // r, g, b, radius
+            const float A = r1.x, B = r1.y, C = r1.z, o = r1.w;
+            // cutoff ellipse box (makeCutoffEllipse's threshold, wider margin)
+            float4 box = make_float4(-3.0e38f, 3.0e38f, -3.0e38f, 3.0e38f);
+            const float D = A * C - B * B;
+            if (!(o >= 1.0f / 255.0f)) {
+                box = make_float4(3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f);  // never reaches 1/255: skip everywhere
+            } else if (A > 0.0f && C > 0.0f && D > 0.0f) {
+                const float qmax = 2.0f * __logf(255.0f * o) + 1e-3f;
+                const float rho = fabsf(B) * rsqrtf(A * C);
+                const float K = 2.0f / fmaxf(1.0f - rho, 1e-30f);
+                const float t = qmax + (2e-3f + 4e-5f * K) * fmaxf(qmax, 1.0f) + 4e-3f;
+                if (t < 1e30f) {
+                    const float ex = sqrtf(t * C / D) * 1.001f + 0.05f;
+                    const float ey = sqrtf(t * A / D) * 1.001f + 0.05f;
+                    box = make_float4(r0.x - ex, r0.x + ex, r0.y - ey, r0.y + ey);
+                }
+            }
+            sm.box[tid] = box;
+            sm.conic[tid] = make_float4(-0.5f * kLog2e * A, -kLog2e * B, -0.5f * kLog2e * C, o);
+            sm.color[tid] = r2;
+            sm.center[tid] = make_float2(r0.x, r0.y);
         }
         __syncthreads();
         const uint32_t n = range.y - start < uint32_t(kRenderThreads) ? range.y - start : uint32_t(kRenderThreads);
-        for (uint32_t q = 0; !done && q < n; ++q) {
-            const float4 c = sCenter[q];
-            const float4 co = sConic[q];
-            const float dx = c.x - fx;
-            const float dy = c.y - fy;
-            const float power = -0.5f * (co.x * dx * dx + co.z * dy * dy) - co.y * dx * dy;
-            if (power > 0.0f) continue;
-            const float alpha = fminf(kMaxAlpha, co.w * expf(power));
-            if (alpha < (1.0f / 255.0f)) continue;
-            const float testT = T * (1.0f - alpha);
-            if (testT < kMinTransmittance) {
-                done = true;
-                break;
+        if (!done) {
+            for (uint32_t q = 0; q < n; ++q) {
+                const float4 bx = sm.box[q];
+                if (bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1) continue;  // warp-uniform
+                const float2 c = sm.center[q];
+                const float4 co = sm.conic[q];
+                const float dx = c.x - fx;
+                const float dy = c.y - fy;
+                const float power2 = co.x * dx * dx + co.z * dy * dy + co.y * dx * dy;
+                if (power2 > 0.0f) continue;
+                const float alpha = fminf(kMaxAlpha, co.w * fastExp2(power2));
+                if (alpha < (1.0f / 255.0f)) continue;
+                const float testT = T * (1.0f - alpha);
+                if (testT < kMinTransmittance) {
+                    done = true;
+                    break;
+                }
+                const float4 col = sm.color[q];
+                const float w = alpha * T;
+                c0 += col.x * w;
+                c1 += col.y * w;
+                c2 += col.z * w;
+                T = testT;
             }
-            const float4 col = sColor[q];
-            c0 = c0 + col.x * alpha * T;
-            c1 = c1 + col.y * alpha * T;
-            c2 = c2 + col.z * alpha * T;
-            T = testT;
         }
-        __syncthreads();
     }
+    cpAsyncWait<0>();
     if (!inside) return;
     const size_t p = size_t(py) * a.width + px;
     a.image[p] = make_float4(c0, c1, c2, 1.0f - T);
@@ -98,7 +173,14 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
 cudaError_t launchRender(const RenderArgs& a, cudaStream_t s) {
     const uint32_t tiles = a.tilesX * a.tilesY;
     if (tiles == 0) return cudaSuccess;
-    renderKernel<<<tiles, kRenderThreads, 0, s>>>(a);
+    static bool configured = false;
+    if (!configured) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(renderKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(RenderShared)));
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    renderKernel<<<tiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
     return cudaGetLastError();
 }
 

@@ -138,7 +138,9 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
 // ---- one onesweep pass ------------------------------------------------------------------------
 constexpr int kSortSmemBytes = kSortTile * 12 + 8 * 256 * 4;
 
-__global__ void __launch_bounds__(kSortThreads) sortPassKernel(const __grid_constant__ SortArgs a, uint32_t p) {
+// Three blocks per SM (<= 85 registers): the digits are recomputed from the keys instead of
+// being kept, and the warp ranks (< 512) are packed two per register.
+__global__ void __launch_bounds__(kSortThreads, 3) sortPassKernel(const __grid_constant__ SortArgs a, uint32_t p) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + kSortTile * 8);
@@ -165,36 +167,35 @@ __global__ void __launch_bounds__(kSortThreads) sortPassKernel(const __grid_cons
     const uint64_t keyMask = maskOf(plan->keyBits);
     const uint32_t shift = 8 * p;
 
+    const uint32_t itemBase = tileBase + warp * (32 * kSortItems) + lane;
+    // digit of item j; past the end: 0x100, ranked nowhere
+    auto digitOf = [&](uint64_t k, uint32_t idx) -> uint32_t {
+        return idx < entries ? uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & 0xFFu : 0x100u;
+    };
     uint64_t key[kSortItems];
     uint32_t val[kSortItems];
-    uint32_t dig[kSortItems];
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
-        const uint32_t idx = tileBase + warp * (32 * kSortItems) + j * 32 + lane;
-        if (idx < entries) {
-            key[j] = keysIn[idx];
-            val[j] = valsIn[idx];
-            dig[j] = uint32_t(virtualKey(key[j], lowBits, keyMask) >> shift) & 0xFFu;
-        } else {
-            key[j] = 0;
-            val[j] = 0;
-            dig[j] = 0x100u;  // past the end: ranked nowhere
-        }
+        const uint32_t idx = itemBase + j * 32;
+        key[j] = idx < entries ? keysIn[idx] : 0ull;
+        val[j] = idx < entries ? valsIn[idx] : 0u;
     }
     // warp-level multisplit: rank of each item among the warp's earlier items of its digit
     uint32_t* wh = sWarpHist + warp * 256;
     const uint32_t ltMask = laneMaskLt();
-    uint32_t rank[kSortItems];
+    uint32_t rank[kSortItems / 2];  // two 16-bit ranks per word
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
-        const uint32_t d = dig[j];
+        const uint32_t d = digitOf(key[j], itemBase + j * 32);
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
         const uint32_t below = peers & ltMask;
         const uint32_t pre = d < 256 ? wh[d] : 0u;
         __syncwarp();
         if (d < 256 && below == 0) wh[d] = pre + __popc(peers);
         __syncwarp();
-        rank[j] = pre + __popc(below);
+        const uint32_t r = pre + __popc(below);
+        if (j & 1) rank[j >> 1] |= r << 16;
+        else rank[j >> 1] = r;
     }
     __syncthreads();
     // digit tid: warp offsets (exclusive over warps) and the block's count
@@ -241,9 +242,10 @@ __global__ void __launch_bounds__(kSortThreads) sortPassKernel(const __grid_cons
     // local stable order in shared memory
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
-        const uint32_t dj = dig[j];
+        const uint32_t dj = digitOf(key[j], itemBase + j * 32);
         if (dj < 256) {
-            const uint32_t pos = sDigitStart[dj] + sWarpHist[warp * 256 + dj] + rank[j];
+            const uint32_t r = (j & 1) ? (rank[j >> 1] >> 16) : (rank[j >> 1] & 0xFFFFu);
+            const uint32_t pos = sDigitStart[dj] + sWarpHist[warp * 256 + dj] + r;
             sKeys[pos] = key[j];
             sVals[pos] = val[j];
         }
@@ -297,7 +299,8 @@ __global__ void rangesKernel(const __grid_constant__ RenderArgs a) {
 constexpr int kScanItems = 8;
 __global__ void __launch_bounds__(256) scanKernel(const uint32_t* __restrict__ in, const uint32_t* __restrict__ index,
                                                   uint32_t* __restrict__ out, uint32_t* total, uint32_t count,
-                                                  uint32_t mode, uint64_t* status, DeviceControl* ctl) {
+                                                  uint32_t mode, uint64_t* status, DeviceControl* ctl,
+                                                  uint32_t setupCapacity, uint32_t waitSite) {
     __shared__ uint32_t sBlock, sWarp[8], sExclusive;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) sBlock = atomicAdd(&ctl->tickets[12], 1u);
@@ -324,7 +327,7 @@ __global__ void __launch_bounds__(256) scanKernel(const uint32_t* __restrict__ i
         if (lane == 0)
             stRelease(&status[block], packStatus(epoch, block == 0 ? kFlagInclusive : kFlagAggregate, blockTotal));
         uint32_t exclusive = 0;
-        if (block > 0) exclusive = warpLookback(status, int(block), epoch, ctl, kWaitStandaloneScan);
+        if (block > 0) exclusive = warpLookback(status, int(block), epoch, ctl, waitSite);
         if (lane == 0) {
             if (block > 0) stRelease(&status[block], packStatus(epoch, kFlagInclusive, exclusive + blockTotal));
             sExclusive = exclusive;
@@ -338,7 +341,17 @@ __global__ void __launch_bounds__(256) scanKernel(const uint32_t* __restrict__ i
         if (idx < count) out[idx] = run;
         run += v[j];
     }
-    if (block == gridDim.x - 1 && tid == 255 && total) *total = run;
+    if (block == gridDim.x - 1 && tid == 255) {
+        if (total) *total = run;
+        if (setupCapacity) {  // the frame's list: entries = min(M, capacity) (tile_setup.comp:16-24)
+            const uint32_t entries = run < setupCapacity ? run : setupCapacity;
+            ctl->c.entries = entries;
+            ctl->c.overflow = run - entries;
+            ctl->c.ranges_groups[0] = (entries + 255u) / 256u;
+            ctl->c.ranges_groups[1] = 1;
+            ctl->c.ranges_groups[2] = 1;
+        }
+    }
 }
 
 __global__ void pack64Kernel(const uint32_t* lo, const uint32_t* hi, uint64_t* out, uint32_t n) {
@@ -383,13 +396,14 @@ cudaError_t launchRanges(const RenderArgs& a, uint32_t capacity, cudaStream_t s)
 }
 
 cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
-                       uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s) {
+                       uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s, uint32_t setupCapacity,
+                       uint32_t waitSite) {
     const uint32_t blocks = (count + 256 * kScanItems - 1) / (256 * kScanItems);
     if (blocks == 0) {
         if (total) return cudaMemsetAsync(total, 0, 4, s);
         return cudaSuccess;
     }
-    scanKernel<<<blocks, 256, 0, s>>>(in, index, out, total, count, mode, status, ctl);
+    scanKernel<<<blocks, 256, 0, s>>>(in, index, out, total, count, mode, status, ctl, setupCapacity, waitSite);
     return cudaGetLastError();
 }
 

@@ -28,7 +28,7 @@ struct SceneArgs {
     uint32_t variableSh;    // GsrVariableSh
 };
 
-// Arguments of the fused per-gaussian kernel (preprocess + count + scan + key emission).
+// Arguments of the per-gaussian kernels of the frame's front (preprocess, scan, key emission).
 struct FrontArgs {
     const DevCameraArgs* cam;  // device copy of the frame's SplatCamera (written by the frame itself)
     SceneArgs scene;
@@ -43,7 +43,7 @@ struct FrontArgs {
     uint32_t* offsets;    // [N] exclusive scan of tileCounts
     uint64_t* keys;       // [capacity] (tile << 32 | depth bits), index order
     uint32_t* values;     // [capacity]
-    uint64_t* scanStatus; // [ceil(N / 256)] look-back words
+    uint64_t* scanStatus; // [ceil(N / 2048)] look-back words of the scan over the counts
     DeviceControl* ctl;
     LogfFixups logf;
 };
@@ -97,8 +97,11 @@ cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s);
 cudaError_t launchRanges(const RenderArgs& a, uint32_t capacity, cudaStream_t s);
 cudaError_t launchRender(const RenderArgs& a, cudaStream_t s);
 cudaError_t launchLogfTable(float* out, LogfFixups t, cudaStream_t s);
+// Exclusive scan (decoupled look-back, 2048 items per block); with setupCapacity != 0 the last
+// block also writes the frame's entries = min(total, capacity), overflow and ranges groups.
 cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
-                       uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s);
+                       uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s, uint32_t setupCapacity = 0,
+                       uint32_t waitSite = kWaitStandaloneScan);
 cudaError_t launchPack64(const uint32_t* lo, const uint32_t* hi, uint64_t* out, uint32_t n, cudaStream_t s);
 cudaError_t launchUnpack64(const uint64_t* in, uint32_t* lo, uint32_t* hi, uint32_t n, cudaStream_t s);
 cudaError_t launchSetEntries(DeviceControl* ctl, uint32_t count, cudaStream_t s);

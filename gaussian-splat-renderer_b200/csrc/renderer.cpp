@@ -399,7 +399,7 @@ struct GsrRenderer {
         forceTimeout = 0;
         slot.used = true;
         slot.frameIndex = frameIndex;
-        kernelLaunches += 5 + list->passes;  // frameBegin, front, histogram, passes, ranges, render
+        kernelLaunches += 7 + list->passes;  // frameBegin, preprocess, scan, duplicate, histogram, passes, ranges, render
         timed = timing;
         ++frameIndex;
         return GSR_OK;

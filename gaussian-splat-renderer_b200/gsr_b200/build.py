@@ -31,7 +31,8 @@ NVCC = str(CUDA_HOME / "bin" / "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off", f"-I{INCLUDE}", f"-I{CSRC}"]
 # translation units whose floating-point results must match the reference bit for bit
-EXACT_UNITS = {"k_front.cu", "k_encode.cu", "k_render.cu"}
+# (the rasterizer's image is held to a tolerance instead and uses FMA and the hardware exp2)
+EXACT_UNITS = {"k_front.cu", "k_encode.cu"}
 CU_UNITS = ["k_front.cu", "k_sort.cu", "k_render.cu", "k_encode.cu"]
 HOST_UNITS = ["renderer.cpp"]
 

@@ -77,6 +77,28 @@ def test_last_stats_arrive_late_without_stall(gpu, setup):
     assert c.duplicates == r.read_control().duplicates
 
 
+def test_graph_frames_equal_direct_frames(gpu, port, setup):
+    """With use_graph each frame is one CUDA graph per readback slot (the camera reaches it
+    through a pinned buffer); the lists and images equal the directly launched frames', also
+    after the adaptive list has been reallocated (which re-captures the graphs)."""
+    from gsr_b200 import scenes
+
+    scene, cam = setup
+    cams = [cam] + scenes.orbit_cameras(4, 6.0, 0.5, 640, 360)
+    gs = gpu.GpuScene(scene)
+    direct = gpu.Renderer(gs, gpu.Settings(adaptive_list=True, adaptive_initial_entries=4096))
+    graphed = gpu.Renderer(gs, gpu.Settings(adaptive_list=True, adaptive_initial_entries=4096, use_graph=True))
+    for k in range(10):
+        c = cams[k % len(cams)]
+        direct.render(c)
+        graphed.render(c)
+        a, b = direct.read_back(), graphed.read_back()
+        for x, y in zip(a[:4], b[:4]):
+            np.testing.assert_array_equal(x, y)
+        assert direct.read_back_image().tobytes() == graphed.read_back_image().tobytes()
+    assert graphed.capacity()[2] >= 1  # the list grew (re-capture happened)
+
+
 def test_kernel_launch_count(gpu, setup):
     scene, cam = setup
     gs = gpu.GpuScene(scene)
