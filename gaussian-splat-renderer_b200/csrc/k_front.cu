@@ -196,14 +196,20 @@ template <int GEOM, int COLOR>
 __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_constant__ FrontArgs a) {
     __shared__ DevCamera sCam;  // the frame's camera, read once per block from its device copy
     __shared__ uint32_t sCull[kCullReasonCount];
+    __shared__ uint32_t sDepthMin, sDepthMax;
     const uint32_t tid = threadIdx.x, lane = tid & 31;
     if (tid < kCullReasonCount) sCull[tid] = 0;
+    if (tid == 0) {
+        sDepthMin = 0xFFFFFFFFu;
+        sDepthMax = 0;
+    }
     static_assert(sizeof(DevCamera) == sizeof(DevCameraArgs) && sizeof(DevCamera) % 4 == 0, "camera layout");
     if (tid < sizeof(DevCamera) / 4)
         reinterpret_cast<uint32_t*>(&sCam)[tid] = reinterpret_cast<const uint32_t*>(a.cam)[tid];
     __syncthreads();
     const uint32_t i = blockIdx.x * kFrontThreads + tid;
     uint32_t reason = kCullReasonCount;  // threads past the end
+    uint32_t dmin = 0xFFFFFFFFu, dmax = 0;
     if (i < a.count) {
         DevSplat s;
         TileRect rect{0, 0, 0, 0};
@@ -215,6 +221,7 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
             count = coverageCount(cv, a.binSize);
             s.cullReason = kCullVisible;
             reinterpret_cast<DevSplat*>(a.splats)[i] = s;
+            dmin = dmax = __float_as_uint(s.depth);  // positive: the bits order like the values
         }
         a.tileCounts[i] = count;
     }
@@ -223,8 +230,19 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
         const uint32_t n = __popc(__ballot_sync(0xFFFFFFFFu, reason == r));
         if (lane == 0 && n) atomicAdd(&sCull[r], n);
     }
+    // the visible depth range (the list keys' depths lie in it): one atomic pair per block
+    dmin = __reduce_min_sync(0xFFFFFFFFu, dmin);
+    dmax = __reduce_max_sync(0xFFFFFFFFu, dmax);
+    if (lane == 0 && dmin <= dmax) {
+        atomicMin(&sDepthMin, dmin);
+        atomicMax(&sDepthMax, dmax);
+    }
     __syncthreads();
     if (tid < kCullReasonCount && sCull[tid]) atomicAdd(&a.ctl->c.cull_counts[tid], sCull[tid]);
+    if (tid == 0 && sDepthMin <= sDepthMax) {
+        atomicMin(&a.ctl->c.depth_min_bits, sDepthMin);
+        atomicMax(&a.ctl->c.depth_max_bits, sDepthMax);
+    }
 }
 
 // 3) Key emission, one thread per gaussian in index order (tile_duplicate.comp:177-221, global
@@ -233,11 +251,9 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
 //    the same inputs as the count, so it enumerates exactly `count` tiles; a disagreement would be
 //    counted (coverageMismatch) and padded with the sentinel tile, as the reference does.
 __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_constant__ FrontArgs a) {
-    __shared__ uint32_t sDepthMin, sDepthMax, sTileMax, sMismatch, sAny;
+    __shared__ uint32_t sTileMax, sMismatch, sAny;
     const uint32_t tid = threadIdx.x;
     if (tid == 0) {
-        sDepthMin = 0xFFFFFFFFu;
-        sDepthMax = 0;
         sTileMax = 0;
         sMismatch = 0;
         sAny = 0;
@@ -246,12 +262,26 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
     const uint32_t i = blockIdx.x * kFrontThreads + tid;
     const uint32_t count = i < a.count ? a.tileCounts[i] : 0u;
     if (count > 0) {
+        const uint32_t sentinel = uint32_t(a.gridX) * uint32_t(a.gridY);
+        const KeyLayout lay = keyLayout(a.ctl, sentinel, a.count);
         const uint32_t offset = a.offsets[i];
         const DevSplat s = reinterpret_cast<const DevSplat*>(a.splats)[i];
         const TileRect rect = tileRect(s.cx, s.cy, s.radius, a.cam->tilesX, a.cam->tilesY);
         const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, a.gridX, a.gridY, s.cx, s.cy, s.conicA, s.conicB,
                                          s.conicC, s.opacity, a.logf);
         const uint64_t depthBits = __float_as_uint(s.depth);
+        // packed: (((tile << W) | depth mod 2^W) << indexBits) | index; the tile part added per entry
+        const uint64_t packedBase =
+            ((lay.lowBits >= 32 ? depthBits : (depthBits & ((1ull << lay.lowBits) - 1ull))) << lay.indexBits) | i;
+        const uint32_t tileShift = lay.lowBits + lay.indexBits;
+        auto emit = [&](uint32_t k, uint32_t tile) {
+            if (lay.packed) {
+                a.keys[k] = (uint64_t(tile) << tileShift) | packedBase;
+            } else {
+                a.keys[k] = (uint64_t(tile) << 32) | depthBits;
+                a.values[k] = i;
+            }
+        };
         const int S = a.binSize;
         int r0, r1;
         coverageRows(cv, S, r0, r1);
@@ -264,32 +294,21 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
             for (int x = x0; x < x1 && written < count; ++x, ++written, ++k) {
                 const uint32_t tile = uint32_t(row) * uint32_t(a.gridX) + uint32_t(x);
                 tileMax = tile > tileMax ? tile : tileMax;
-                if (k < a.capacity) {
-                    a.keys[k] = (uint64_t(tile) << 32) | depthBits;
-                    a.values[k] = i;
-                }
+                if (k < a.capacity) emit(k, tile);
             }
         }
-        const uint32_t sentinel = uint32_t(a.gridX) * uint32_t(a.gridY);
         if (written != count) {
             atomicAdd(&sMismatch, 1u);
             tileMax = sentinel;
             for (; written < count; ++written, ++k)
-                if (k < a.capacity) {
-                    a.keys[k] = (uint64_t(sentinel) << 32) | depthBits;
-                    a.values[k] = i;
-                }
+                if (k < a.capacity) emit(k, sentinel);
         }
-        atomicMin(&sDepthMin, uint32_t(depthBits));
-        atomicMax(&sDepthMax, uint32_t(depthBits));
         atomicMax(&sTileMax, tileMax);
         sAny = 1;
     }
     __syncthreads();
     if (tid == 0 && sAny) {
         DeviceControl* ctl = a.ctl;
-        atomicMin(&ctl->c.depth_min_bits, sDepthMin);
-        atomicMax(&ctl->c.depth_max_bits, sDepthMax);
         atomicMax(&ctl->c.tile_max, sTileMax);
         if (sMismatch) atomicAdd(&ctl->c.coverage_mismatch, sMismatch);
     }

@@ -65,7 +65,11 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
     const uint32_t entries = a.ctl->c.entries;
     range.y = range.y < entries ? range.y : entries;
     range.x = range.x < range.y ? range.x : range.y;
-    const uint32_t* values = a.values[a.ctl->c.sorted_buffer & 1u];
+    const uint32_t sortedBuffer = a.ctl->c.sorted_buffer & 1u;
+    const uint32_t* values = a.values[sortedBuffer];
+    const uint64_t* packedKeys = a.keys[sortedBuffer];
+    const bool packed = a.plan->packed != 0;
+    const uint64_t indexMask = (1ull << a.plan->indexBits) - 1ull;
     const float4* records = reinterpret_cast<const float4*>(a.splats);
     const float fx = float(px), fy = float(py);
     // this warp's pixel strip
@@ -77,7 +81,7 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
     auto issue = [&](uint32_t start, int buf) {
         const uint32_t j = start + tid;
         if (j < range.y) {
-            uint32_t g = __ldg(&values[j]);
+            uint32_t g = packed ? uint32_t(__ldg(&packedKeys[j]) & indexMask) : __ldg(&values[j]);
             if (g >= a.count) {
                 atomicOr(&a.ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
                 g = 0;

@@ -70,10 +70,12 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     __shared__ uint32_t sAny;
     DeviceControl* ctl = a.ctl;
     const uint32_t entries = ctl->c.entries;
-    uint32_t lowBits, keyBits;
+    uint32_t lowBits, keyBits, packed = 0, indexBits = 0;
     if (a.frameMode) {
-        lowBits = bitWidth(ctl->c.depth_min_bits ^ ctl->c.depth_max_bits);
-        if (ctl->c.depth_min_bits > ctl->c.depth_max_bits) lowBits = 0;  // no entries
+        const KeyLayout lay = keyLayout(ctl, a.tileCount, a.count);
+        lowBits = lay.lowBits;
+        packed = lay.packed;
+        indexBits = lay.indexBits;
         keyBits = bitWidth(ctl->c.tile_max) + lowBits;
     } else {
         lowBits = a.fixedLowBits;
@@ -89,7 +91,8 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     __syncthreads();
     const uint64_t* keys = a.keys[0];
     for (uint32_t k = blockIdx.x * 256 + threadIdx.x; k < entries; k += gridDim.x * 256) {
-        const uint64_t v = virtualKey(__ldg(&keys[k]), lowBits, keyMask);
+        const uint64_t key = __ldg(&keys[k]);
+        const uint64_t v = packed ? (key >> indexBits) : virtualKey(key, lowBits, keyMask);
         for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][uint32_t(v >> (8 * p)) & 0xFFu], 1u);
     }
     __syncthreads();
@@ -127,6 +130,10 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
         plan->passes = passes;
         plan->lowBits = lowBits;
         plan->keyBits = keyBits;
+        plan->packed = packed;
+        plan->indexBits = indexBits;
+        ctl->c.packed_entries = packed;
+        ctl->c.index_bits = indexBits;
         ctl->c.sort_passes = activeCount;
         ctl->c.sorted_buffer = activeCount & 1u;
         ctl->c.key_bits = keyBits;
@@ -139,15 +146,19 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
 constexpr int kSortSmemBytes = kSortTile * 12 + 8 * 256 * 4;
 
 // Three blocks per SM (<= 85 registers): the digits are recomputed from the keys instead of
-// being kept, and the warp ranks (< 512) are packed two per register.
-__global__ void __launch_bounds__(kSortThreads, 3) sortPassKernel(const __grid_constant__ SortArgs a, uint32_t p) {
+// being kept, and the warp ranks (< 512) are packed two per register. PACKED: the entries are
+// single words (vkey << indexBits | index) and no value array moves; the frame launches both
+// instantiations and the one that does not match the plan's layout returns at once.
+template <bool PACKED>
+__global__ void __launch_bounds__(kSortThreads, PACKED ? 4 : 3) sortPassKernel(const __grid_constant__ SortArgs a,
+                                                                                uint32_t p) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
-    uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + kSortTile * 8);
-    uint32_t* sWarpHist = reinterpret_cast<uint32_t*>(smem + kSortTile * 12);
+    uint32_t* sWarpHist = reinterpret_cast<uint32_t*>(smem + kSortTile * 8);
+    uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + kSortTile * 8 + 8 * 256 * 4);
     __shared__ uint32_t sDigitStart[256], sGlobalBase[256], sWarp[8], sTile;
     const SortPlan* plan = a.plan;
-    if (!plan->active[p]) return;
+    if (!plan->active[p] || (plan->packed != 0) != PACKED) return;
     DeviceControl* ctl = a.ctl;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t entries = ctl->c.entries;
@@ -165,20 +176,21 @@ __global__ void __launch_bounds__(kSortThreads, 3) sortPassKernel(const __grid_c
     uint32_t* valsOut = a.values[in ^ 1u];
     const uint32_t lowBits = plan->lowBits;
     const uint64_t keyMask = maskOf(plan->keyBits);
-    const uint32_t shift = 8 * p;
+    const uint32_t shift = 8 * p + (PACKED ? plan->indexBits : 0u);
 
     const uint32_t itemBase = tileBase + warp * (32 * kSortItems) + lane;
-    // digit of item j; past the end: 0x100, ranked nowhere
-    auto digitOf = [&](uint64_t k, uint32_t idx) -> uint32_t {
-        return idx < entries ? uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & 0xFFu : 0x100u;
+    // digit of a key; past the end: 0x100, ranked nowhere
+    auto digit = [&](uint64_t k) -> uint32_t {
+        return PACKED ? uint32_t(k >> shift) & 0xFFu : uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & 0xFFu;
     };
+    auto digitOf = [&](uint64_t k, uint32_t idx) -> uint32_t { return idx < entries ? digit(k) : 0x100u; };
     uint64_t key[kSortItems];
-    uint32_t val[kSortItems];
+    uint32_t val[PACKED ? 1 : kSortItems];
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const uint32_t idx = itemBase + j * 32;
         key[j] = idx < entries ? keysIn[idx] : 0ull;
-        val[j] = idx < entries ? valsIn[idx] : 0u;
+        if (!PACKED) val[PACKED ? 0 : j] = idx < entries ? valsIn[idx] : 0u;
     }
     // warp-level multisplit: rank of each item among the warp's earlier items of its digit
     uint32_t* wh = sWarpHist + warp * 256;
@@ -247,22 +259,195 @@ __global__ void __launch_bounds__(kSortThreads, 3) sortPassKernel(const __grid_c
             const uint32_t r = (j & 1) ? (rank[j >> 1] >> 16) : (rank[j >> 1] & 0xFFFFu);
             const uint32_t pos = sDigitStart[dj] + sWarpHist[warp * 256 + dj] + r;
             sKeys[pos] = key[j];
-            sVals[pos] = val[j];
+            if (!PACKED) sVals[pos] = val[PACKED ? 0 : j];
         }
     }
     __syncthreads();
     const uint32_t n = entries - tileBase < uint32_t(kSortTile) ? entries - tileBase : uint32_t(kSortTile);
     for (uint32_t k = tid; k < n; k += kSortThreads) {
         const uint64_t kk = sKeys[k];
-        const uint32_t dk = uint32_t(virtualKey(kk, lowBits, keyMask) >> shift) & 0xFFu;
+        const uint32_t dk = digit(kk);
         const uint32_t g = sGlobalBase[dk] + (k - sDigitStart[dk]);
         if (g < entries) {
             keysOut[g] = kk;
-            valsOut[g] = sVals[k];
+            if (!PACKED) valsOut[g] = sVals[k];
         } else {
             atomicOr(&ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
         }
     }
+}
+
+// ---- one onesweep pass over packed entries: 12288-key tiles, 768 threads ----------------------
+// The frame's usual layout. One block per SM: the first wave of a pass is ~148 tiles deep
+// instead of ~600, so the decoupled look-back chains stay short. Each tile publishes its
+// per-digit counts as soon as its keys are loaded (a shared-memory histogram), ranks them with
+// warp-level multisplit meanwhile, then looks back 8 predecessors per round trip.
+constexpr int kBigThreads = 768;
+constexpr int kBigTile = kBigThreads * kSortItems;  // 12288 keys
+constexpr int kBigWarps = kBigThreads / 32;
+constexpr int kBigSmemBytes = kBigTile * 8 + kBigWarps * 256 * 4;
+static_assert(kBigWarps * 256 == 8 * kBigThreads, "the warp histograms are zeroed 8 words per thread");
+
+__global__ void __launch_bounds__(kBigThreads, 1) sortPassPackedKernel(const __grid_constant__ SortArgs a, uint32_t p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
+    uint32_t* sWarpHist = reinterpret_cast<uint32_t*>(smem + kBigTile * 8);  // [kBigWarps][256]
+    __shared__ uint32_t sBlockHist[256], sDigitStart[256], sGlobalBase[256], sWarp[8], sTile;
+    const SortPlan* plan = a.plan;
+    if (!plan->active[p] || !plan->packed) return;
+    DeviceControl* ctl = a.ctl;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t entries = ctl->c.entries;
+    if (tid == 0) sTile = atomicAdd(&ctl->tickets[1 + p], 1u);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) sWarpHist[j * kBigThreads + tid] = 0;
+    if (tid < 256) sBlockHist[tid] = 0;
+    __syncthreads();
+    const uint32_t t = sTile;
+    const uint32_t tileBase = t * kBigTile;
+    if (tileBase >= entries) return;
+    const uint32_t in = plan->inBuffer[p];
+    const uint64_t* keysIn = a.keys[in];
+    uint64_t* keysOut = a.keys[in ^ 1u];
+    const uint32_t shift = 8 * p + plan->indexBits;
+    const uint32_t itemBase = tileBase + warp * (32 * kSortItems) + lane;
+    auto digitOf = [&](uint64_t k, uint32_t idx) -> uint32_t {
+        return idx < entries ? uint32_t(k >> shift) & 0xFFu : 0x100u;
+    };
+    uint64_t key[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const uint32_t idx = itemBase + j * 32;
+        key[j] = idx < entries ? keysIn[idx] : 0ull;
+    }
+    // 1) the tile's digit counts, published at once (aggregate; inclusive for the first tile)
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const uint32_t d = digitOf(key[j], itemBase + j * 32);
+        if (d < 256) atomicAdd(&sBlockHist[d], 1u);
+    }
+    __syncthreads();
+    const uint32_t epoch = ctl->c.epoch;
+    uint64_t* status = a.status + (size_t(p) * a.maxTiles) * 256;
+    uint32_t blockCount = 0;
+    if (tid < 256) {
+        blockCount = sBlockHist[tid];
+        stRelease(&status[size_t(t) * 256 + tid], packStatus(epoch, t == 0 ? kFlagInclusive : kFlagAggregate, blockCount));
+    }
+    // 2) warp-level multisplit ranks
+    uint32_t* wh = sWarpHist + warp * 256;
+    const uint32_t ltMask = laneMaskLt();
+    uint32_t rank[kSortItems / 2];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const uint32_t d = digitOf(key[j], itemBase + j * 32);
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        const uint32_t below = peers & ltMask;
+        const uint32_t pre = d < 256 ? wh[d] : 0u;
+        __syncwarp();
+        if (d < 256 && below == 0) wh[d] = pre + __popc(peers);
+        __syncwarp();
+        const uint32_t r = pre + __popc(below);
+        if (j & 1) rank[j >> 1] |= r << 16;
+        else rank[j >> 1] = r;
+    }
+    __syncthreads();
+    // 3) digit d = tid < 256: warp offsets, the tile's digit starts, and the look-back
+    if (tid < 256) {
+        const uint32_t d = tid;
+        uint32_t run = 0;
+        for (int w = 0; w < kBigThreads / 32; ++w) {
+            const uint32_t c = sWarpHist[w * 256 + d];
+            sWarpHist[w * 256 + d] = run;
+            run += c;
+        }
+        // block-wide exclusive scan of the 256 counts (warps 0-7)
+        uint32_t incl = blockCount;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= uint32_t(o)) incl += v;
+        }
+        if (lane == 31) sWarp[warp] = incl;
+    }
+    __syncthreads();
+    if (tid < 256) {
+        const uint32_t d = tid;
+        uint32_t base = 0;
+        for (uint32_t w = 0; w < warp; ++w) base += sWarp[w];
+        uint32_t incl = blockCount;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= uint32_t(o)) incl += v;
+        }
+        sDigitStart[d] = base + incl - blockCount;
+    }
+    __syncthreads();
+    // 4) local order in shared memory (before the look-back: the keys leave the registers)
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const uint32_t dj = digitOf(key[j], itemBase + j * 32);
+        if (dj < 256) {
+            const uint32_t r = (j & 1) ? (rank[j >> 1] >> 16) : (rank[j >> 1] & 0xFFFFu);
+            sKeys[sDigitStart[dj] + sWarpHist[warp * 256 + dj] + r] = key[j];
+        }
+    }
+    if (tid < 256) {
+        const uint32_t d = tid;
+        // 5) windowed look-back: 8 predecessors per round trip
+        uint32_t exclusive = 0;
+        if (t > 0) {
+            const uint32_t forced = ctl->forceTimeout;
+            uint32_t spins = 0;
+            int q = int(t) - 1;
+            bool found = false;
+            while (!found && q >= 0) {
+                uint64_t w[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    w[j] = q - j >= 0 ? ldAcquire(&status[size_t(q - j) * 256 + d]) : packStatus(epoch, kFlagInclusive, 0);
+                int used = 0;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (found || used != j) continue;
+                    bool ready = statusReady(w[j], epoch);
+                    if (forced && spins < forced) ready = false;
+                    if (!ready) continue;
+                    exclusive += uint32_t(w[j]);
+                    ++used;
+                    if (statusFlag(w[j]) == kFlagInclusive) found = true;
+                }
+                if (found) break;
+                q -= used;
+                if (used < 8) {
+                    if (++spins >= kSpinLimit || (forced && spins >= forced)) {
+                        reportTimeout(ctl, kWaitSort);
+                        break;
+                    }
+                    __nanosleep(32);
+                }
+            }
+            stRelease(&status[size_t(t) * 256 + d], packStatus(epoch, kFlagInclusive, exclusive + blockCount));
+        }
+        sGlobalBase[d] = plan->digitBase[p][d] + exclusive;
+    }
+    __syncthreads();
+    // 6) coalesced runs to the global positions
+    const uint32_t n = entries - tileBase < uint32_t(kBigTile) ? entries - tileBase : uint32_t(kBigTile);
+    for (uint32_t k = tid; k < n; k += kBigThreads) {
+        const uint64_t kk = sKeys[k];
+        const uint32_t dk = uint32_t(kk >> shift) & 0xFFu;
+        const uint32_t g = sGlobalBase[dk] + (k - sDigitStart[dk]);
+        if (g < entries) keysOut[g] = kk;
+        else atomicOr(&ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
+    }
+}
+
+// The gaussian index and the tile of sorted entry k in either layout.
+__device__ __forceinline__ uint32_t entryTile(const uint64_t* keys, uint32_t k, const SortPlan* plan) {
+    const uint64_t key = keys[k];
+    return plan->packed ? uint32_t(key >> (plan->indexBits + plan->lowBits)) : uint32_t(key >> 32);
 }
 
 // ---- tile ranges (tile_ranges.comp:22-44) -----------------------------------------------------
@@ -272,12 +457,13 @@ __global__ void rangesKernel(const __grid_constant__ RenderArgs a) {
     const uint64_t* keys = a.keys[ctl->c.sorted_buffer & 1u];
     const uint32_t tileCount = a.tilesX * a.tilesY;
     uint2* ranges = reinterpret_cast<uint2*>(a.ranges);
+    const SortPlan* plan = a.plan;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t tile = uint32_t(keys[k] >> 32);
+        const uint32_t tile = entryTile(keys, k, plan);
         if (tile >= tileCount) {
             // the sentinel tile (sorted last) closes the last real tile's range
             if (k > 0) {
-                const uint32_t prev = uint32_t(keys[k - 1] >> 32);
+                const uint32_t prev = entryTile(keys, k - 1, plan);
                 if (prev < tileCount) ranges[prev].y = k;
             }
             continue;
@@ -285,7 +471,7 @@ __global__ void rangesKernel(const __grid_constant__ RenderArgs a) {
         if (k == 0) {
             ranges[tile].x = 0;
         } else {
-            const uint32_t prev = uint32_t(keys[k - 1] >> 32);
+            const uint32_t prev = entryTile(keys, k - 1, plan);
             if (prev != tile) {
                 if (prev < tileCount) ranges[prev].y = k;
                 ranges[tile].x = k;
@@ -380,13 +566,21 @@ uint32_t gridFor(uint32_t n, uint32_t perBlock, uint32_t cap) {
 cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(sortPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortSmemBytes);
+        cudaError_t e = cudaFuncSetAttribute(sortPassKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             kSortSmemBytes);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(sortPassPackedKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBigSmemBytes);
         if (e != cudaSuccess) return e;
         configured = true;
     }
     sortHistKernel<<<histBlocks < 1 ? 1 : histBlocks, 256, 0, s>>>(a);
-    for (uint32_t p = 0; p < a.passesLaunched; ++p)
-        sortPassKernel<<<a.maxTiles < 1 ? 1 : a.maxTiles, kSortThreads, kSortSmemBytes, s>>>(a, p);
+    const uint32_t grid = a.maxTiles < 1 ? 1 : a.maxTiles;
+    const uint32_t bigGrid = (grid + (kBigTile / kSortTile) - 1) / (kBigTile / kSortTile);
+    for (uint32_t p = 0; p < a.passesLaunched; ++p) {
+        // the entry layout is decided on the device: both run, the other one returns at once
+        if (a.frameMode) sortPassPackedKernel<<<bigGrid, kBigThreads, kBigSmemBytes, s>>>(a, p);
+        sortPassKernel<false><<<grid, kSortThreads, kSortSmemBytes, s>>>(a, p);
+    }
     return cudaGetLastError();
 }
 

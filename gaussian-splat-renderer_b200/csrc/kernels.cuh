@@ -57,6 +57,8 @@ struct SortPlan {
     uint32_t passes;        // significant 8-bit digits of the virtual key
     uint32_t lowBits;       // W: low key bits kept below the high word
     uint32_t keyBits;
+    uint32_t packed;        // entries are single words (vkey << indexBits | index), see KeyLayout
+    uint32_t indexBits;
     uint32_t active[kMaxSortPasses];
     uint32_t inBuffer[kMaxSortPasses];
     uint32_t digitBase[kMaxSortPasses][256];
@@ -75,6 +77,7 @@ struct SortArgs {
     // bits from the largest tile id; 0 uses fixedLowBits/fixedKeyBits (standalone sort).
     uint32_t frameMode;
     uint32_t fixedLowBits, fixedKeyBits;
+    uint32_t tileCount, count;  // frame mode: the grid's tiles and N (for the entry layout)
 };
 
 struct RenderArgs {
@@ -87,6 +90,7 @@ struct RenderArgs {
     uint32_t width, height, tilesX, tilesY;
     uint32_t count;           // N: gaussian indices read from the list are checked against it
     DeviceControl* ctl;
+    const SortPlan* plan;     // the entry layout (packed words or key/value arrays)
 };
 
 // ---- launchers (return cudaGetLastError()) ---------------------------------------------------

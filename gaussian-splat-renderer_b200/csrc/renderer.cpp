@@ -396,10 +396,16 @@ struct GsrRenderer {
             rc = enqueue(slot, stream);
             if (rc) return rc;
         }
+        // completion of this frame (outside any capture: an event recorded while capturing only
+        // orders the captured work and is not a usable event afterwards)
+        GSR_CUDA(cudaEventRecord(slot.done, stream));
+        GSR_CUDA(cudaEventRecord(list->lastUse, stream));
+        if (timing) GSR_CUDA(cudaEventRecord(ev[5], stream));
         forceTimeout = 0;
         slot.used = true;
         slot.frameIndex = frameIndex;
-        kernelLaunches += 7 + list->passes;  // frameBegin, preprocess, scan, duplicate, histogram, passes, ranges, render
+        // frameBegin, preprocess, scan, duplicate, histogram, 2 per pass (both entry layouts), ranges, render
+        kernelLaunches += 7 + 2 * list->passes;
         timed = timing;
         ++frameIndex;
         return GSR_OK;
@@ -456,6 +462,8 @@ struct GsrRenderer {
         sa.ctl = ctl;
         sa.passesLaunched = l.passes;
         sa.frameMode = 1;
+        sa.tileCount = tileCount;
+        sa.count = scene.count;
         GSR_CUDA(launchSort(sa, 148 * 2, stream));
         if (timing) GSR_CUDA(cudaEventRecord(ev[2], stream));
 
@@ -474,15 +482,13 @@ struct GsrRenderer {
         ra.tilesY = tilesY;
         ra.count = scene.count;
         ra.ctl = ctl;
+        ra.plan = sortPlan;
         GSR_CUDA(launchRanges(ra, l.capacity, stream));
         if (timing) GSR_CUDA(cudaEventRecord(ev[3], stream));
         GSR_CUDA(launchRender(ra, stream));
         if (timing) GSR_CUDA(cudaEventRecord(ev[4], stream));
 
         GSR_CUDA(cudaMemcpyAsync(slot.host, &ctl->c, sizeof(GsrControl), cudaMemcpyDeviceToHost, stream));
-        GSR_CUDA(cudaEventRecord(slot.done, stream));
-        GSR_CUDA(cudaEventRecord(l.lastUse, stream));
-        if (timing) GSR_CUDA(cudaEventRecord(ev[5], stream));
         return GSR_OK;
     }
 };
@@ -841,15 +847,31 @@ int gsr_read_list(GsrRenderer* r, uint32_t* keysLo, uint32_t* keysHi, uint32_t* 
     GSR_CUDA(cudaMemcpy(&c, &r->control.as<DeviceControl>()->c, sizeof(c), cudaMemcpyDeviceToHost));
     n = std::min(n, c.entries);
     const uint32_t b = c.sorted_buffer & 1u;
-    if (n && (keysLo || keysHi)) {
+    SortPlan plan;
+    GSR_CUDA(cudaMemcpy(&plan, r->plan.p, sizeof(plan), cudaMemcpyDeviceToHost));
+    if (n && (keysLo || keysHi || (values && plan.packed))) {
         std::vector<uint64_t> k(n);
         GSR_CUDA(cudaMemcpy(k.data(), r->list->keys[b].p, size_t(n) * 8, cudaMemcpyDeviceToHost));
+        // packed words: (((tile << W) | depth mod 2^W) << indexBits) | index; the depth bits above
+        // W are those of the frame's smallest depth (equal in every key)
+        const uint32_t W = plan.lowBits, ib = plan.indexBits;
+        const uint32_t lowMask = W >= 32 ? 0xFFFFFFFFu : ((1u << W) - 1u);
         for (uint32_t i = 0; i < n; ++i) {
-            if (keysLo) keysLo[i] = uint32_t(k[i]);
-            if (keysHi) keysHi[i] = uint32_t(k[i] >> 32);
+            uint32_t lo, hi;
+            if (plan.packed) {
+                lo = (c.depth_min_bits & ~lowMask) | (uint32_t(k[i] >> ib) & lowMask);
+                hi = uint32_t(k[i] >> (ib + W));
+                if (values) values[i] = uint32_t(k[i] & ((1ull << ib) - 1ull));
+            } else {
+                lo = uint32_t(k[i]);
+                hi = uint32_t(k[i] >> 32);
+            }
+            if (keysLo) keysLo[i] = lo;
+            if (keysHi) keysHi[i] = hi;
         }
     }
-    if (n && values) GSR_CUDA(cudaMemcpy(values, r->list->values[b].p, size_t(n) * 4, cudaMemcpyDeviceToHost));
+    if (n && values && !plan.packed)
+        GSR_CUDA(cudaMemcpy(values, r->list->values[b].p, size_t(n) * 4, cudaMemcpyDeviceToHost));
     if (rangesOut) {
         const uint32_t words = std::min<uint32_t>(rangesWords, r->tilesX * r->tilesY * 2);
         GSR_CUDA(cudaMemcpy(rangesOut, r->ranges.p, size_t(words) * 4, cudaMemcpyDeviceToHost));

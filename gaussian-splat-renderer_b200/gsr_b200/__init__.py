@@ -98,7 +98,8 @@ class Control(C.Structure):
         ("coverage_mismatch", C.c_uint32), ("pad", C.c_uint32 * 3), ("status", C.c_uint32),
         ("timeout_where", C.c_uint32), ("epoch", C.c_uint32), ("sort_passes", C.c_uint32), ("key_bits", C.c_uint32),
         ("depth_low_bits", C.c_uint32), ("depth_min_bits", C.c_uint32), ("depth_max_bits", C.c_uint32),
-        ("tile_max", C.c_uint32), ("sorted_buffer", C.c_uint32), ("capacity", C.c_uint32), ("ext_pad", C.c_uint32 * 5),
+        ("tile_max", C.c_uint32), ("sorted_buffer", C.c_uint32), ("capacity", C.c_uint32),
+        ("packed_entries", C.c_uint32), ("index_bits", C.c_uint32), ("ext_pad", C.c_uint32 * 3),
     ]
 
     def as_dict(self):

@@ -173,7 +173,9 @@ typedef struct GsrControl {
     uint32_t tile_max;               /* largest tile id emitted */
     uint32_t sorted_buffer;          /* which list buffer holds the sorted result */
     uint32_t capacity;               /* list capacity of this frame */
-    uint32_t ext_pad[5];
+    uint32_t packed_entries;         /* 1: entries were single 64-bit words (tile|depth|index) */
+    uint32_t index_bits;             /* bits of the gaussian index in a packed entry */
+    uint32_t ext_pad[3];
 } GsrControl;
 
 /* ---- the renderer (SplatTileRenderer) ---------------------------------------------------- */

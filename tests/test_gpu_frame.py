@@ -104,6 +104,23 @@ def test_other_bounds_lists(gpu, port, mode):
     np.testing.assert_array_equal(ranges, olist["ranges"])
 
 
+@pytest.mark.parametrize("width,height,count,packed", [(640, 360, 250_000, 1), (3840, 2160, 300_000, 0)])
+def test_entry_layouts(gpu, port, width, height, count, packed):
+    """Both entry layouts give the oracle's list: single 64-bit words when tile bits + varying
+    depth bits + index bits fit in 64 (640x360: 10 + 31 + 18), else (tile << 32 | depth, index)
+    pairs (3840x2160 with depths on both sides of 2.0: 15 + 31 + 19 = 65)."""
+    scene = tile_raster_scene(count, 5)
+    cam = tile_raster_camera(width, height)
+    r = render(gpu, scene, cam)
+    lo, hi, val, ranges, ctl = r.read_back()
+    assert ctl.packed_entries == packed and ctl.status == 0
+    _, osp, ocounts, olist = oracle_frame(port, scene, cam, bounds=1)
+    np.testing.assert_array_equal(hi, olist["keys_hi"])
+    np.testing.assert_array_equal(lo, olist["keys_lo"])
+    np.testing.assert_array_equal(val, olist["values"])
+    np.testing.assert_array_equal(ranges, olist["ranges"])
+
+
 def test_tight_image_equals_rect_image(gpu):
     """Tight bounds drop only pairs with alpha < 1/255: the GPU image is bit-identical to the
     rect image (test_tight_bounds.cpp:242-264), with fewer entries."""
