@@ -25,13 +25,16 @@ __device__ __forceinline__ int ftoi(float x) {
 }
 
 // ---- memory ordering for flag-based cross-block communication ------------------------------
-__device__ __forceinline__ uint64_t ldAcquire(const uint64_t* p) {
+// Look-back status words carry their value in the word itself, so they are written and read
+// with relaxed (strong, GPU-scope) operations: no acquire/release ordering is needed, and a
+// window of relaxed loads is in flight at once (acquire loads would complete one by one).
+__device__ __forceinline__ uint64_t ldRelaxed(const uint64_t* p) {
     uint64_t v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void stRelease(uint64_t* p, uint64_t v) {
-    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+__device__ __forceinline__ void stRelaxed(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
 }
 __device__ __forceinline__ uint32_t ldAcquire32(const uint32_t* p) {
     uint32_t v;
@@ -67,7 +70,7 @@ __device__ __forceinline__ uint32_t warpLookback(const uint64_t* status, int til
     const uint32_t forced = ctl->forceTimeout;
     while (base >= 0) {
         const int idx = base - lane;
-        uint64_t s = idx >= 0 ? ldAcquire(&status[idx]) : packStatus(epoch, kFlagInclusive, 0);
+        uint64_t s = idx >= 0 ? ldRelaxed(&status[idx]) : packStatus(epoch, kFlagInclusive, 0);
         bool ready = statusReady(s, epoch);
         if (forced && spins < forced) ready = false;  // test hook: behave as if nobody published
         if (!__all_sync(0xFFFFFFFFu, ready)) {

@@ -2,10 +2,17 @@
 //
 // The sort is a stable LSD radix sort over 8-bit digits in the onesweep form (Adinets and
 // Merrill, 2022): one histogram kernel computes the digit counts of every pass in a single
-// read of the keys, then each pass is ONE kernel whose blocks (ordered by a ticket) rank their
-// 4096-key tile locally with warp-level multisplit (match.any), publish per-digit counts, get
-// their global digit offsets by a decoupled look-back over the earlier tiles, and scatter
-// through shared memory. Ties keep their input order (warp order, then lane/item order).
+// read of the keys, then each pass is ONE kernel whose blocks (ordered by a ticket) count the
+// digits of their tile and publish the counts at once, rank the tile locally with a warp-level
+// multisplit, get their global digit offsets by a decoupled look-back over the earlier tiles,
+// and scatter through shared memory. Ties keep their input order (warp order, then item and
+// lane order).
+//
+// The multisplit finds the lanes of a warp that hold the same digit through per-warp lane
+// masks in shared memory (each lane ORs its bit into mask[digit], then reads the word back).
+// On sm_100a that costs about 40 cycles per warp-step against ~95 for eight vote.ballot rounds
+// and ~235 for match.any.sync over random 8-bit digits (measured on B200 with a synthetic
+// throughput loop).
 //
 // Key shortening: the list key is (tile << 32 | depth bits). All depth bits above the highest
 // bit where the frame's smallest and largest depth differ are equal for every key, and so are
@@ -63,6 +70,7 @@ __device__ __forceinline__ uint32_t blockExclusiveScan256(uint32_t v, uint32_t* 
 }
 
 // ---- histogram of every pass's digit + the plan ---------------------------------------------
+constexpr int kHistItems = 16;
 __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ SortArgs a) {
     __shared__ uint32_t sHist[kMaxSortPasses][256];
     __shared__ uint32_t sWarp[8];
@@ -90,10 +98,22 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     for (uint32_t j = threadIdx.x; j < kMaxSortPasses * 256; j += 256) (&sHist[0][0])[j] = 0;
     __syncthreads();
     const uint64_t* keys = a.keys[0];
-    for (uint32_t k = blockIdx.x * 256 + threadIdx.x; k < entries; k += gridDim.x * 256) {
-        const uint64_t key = __ldg(&keys[k]);
-        const uint64_t v = packed ? (key >> indexBits) : virtualKey(key, lowBits, keyMask);
-        for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][uint32_t(v >> (8 * p)) & 0xFFu], 1u);
+    // kHistItems independent loads per thread in flight before the counting
+    constexpr uint32_t kChunk = 256 * kHistItems;
+    for (uint32_t base = blockIdx.x * kChunk; base < entries; base += gridDim.x * kChunk) {
+        uint64_t k[kHistItems];
+#pragma unroll
+        for (int j = 0; j < kHistItems; ++j) {
+            const uint32_t idx = base + j * 256 + threadIdx.x;
+            k[j] = idx < entries ? __ldg(&keys[idx]) : 0ull;
+        }
+#pragma unroll
+        for (int j = 0; j < kHistItems; ++j) {
+            if (base + j * 256 + threadIdx.x < entries) {
+                const uint64_t v = packed ? (k[j] >> indexBits) : virtualKey(k[j], lowBits, keyMask);
+                for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][uint32_t(v >> (8 * p)) & 0xFFu], 1u);
+            }
+        }
     }
     __syncthreads();
     for (uint32_t p = 0; p < passes; ++p) {
@@ -143,31 +163,89 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
 }
 
 // ---- one onesweep pass ------------------------------------------------------------------------
-constexpr int kSortSmemBytes = kSortTile * 12 + 8 * 256 * 4;
+// Decoupled look-back of digit d for tile t: the sum of the digit's counts over tiles 0..t-1.
+// Eight predecessors are read per round trip; a word that is not yet published (or carries an
+// older frame's epoch) stops the window and is re-read after a short sleep. Waits are bounded
+// by kSpinLimit (then the timeout is reported and the partial sum returned).
+__device__ __forceinline__ uint32_t digitLookback(const uint64_t* status, uint32_t t, uint32_t d, uint32_t epoch,
+                                                  DeviceControl* ctl) {
+    constexpr int kWindow = 8;
+    const uint32_t forced = ctl->forceTimeout;
+    uint32_t exclusive = 0, spins = 0;
+    int q = int(t) - 1;
+    while (q >= 0) {
+        uint64_t w[kWindow];
+#pragma unroll
+        for (int j = 0; j < kWindow; ++j)
+            w[j] = q - j >= 0 ? ldRelaxed(&status[size_t(q - j) * 256 + d]) : packStatus(epoch, kFlagInclusive, 0);
+        int used = 0;
+        bool found = false;
+#pragma unroll
+        for (int j = 0; j < kWindow; ++j) {
+            if (found || used != j) continue;
+            bool ready = statusReady(w[j], epoch);
+            if (forced && spins < forced) ready = false;  // test hook: behave as if nobody published
+            if (!ready) continue;
+            exclusive += uint32_t(w[j]);
+            ++used;
+            if (statusFlag(w[j]) == kFlagInclusive) found = true;
+        }
+        if (found) break;
+        q -= used;
+        if (used < kWindow) {
+            if (++spins >= kSpinLimit || (forced && spins >= forced)) {
+                reportTimeout(ctl, kWaitSort);
+                break;
+            }
+            __nanosleep(32);
+        }
+    }
+    return exclusive;
+}
 
-// Three blocks per SM (<= 85 registers): the digits are recomputed from the keys instead of
-// being kept, and the warp ranks (< 512) are packed two per register. PACKED: the entries are
-// single words (vkey << indexBits | index) and no value array moves; the frame launches both
-// instantiations and the one that does not match the plan's layout returns at once.
-template <bool PACKED>
-__global__ void __launch_bounds__(kSortThreads, PACKED ? 4 : 3) sortPassKernel(const __grid_constant__ SortArgs a,
-                                                                                uint32_t p) {
+// One pass over 256-thread tiles of kItems keys per thread. PAIRS = false: the entries are
+// single words (vkey << indexBits | index), 24 per thread; PAIRS = true: (tile << 32 | depth)
+// keys with a 32-bit value array, 16 per thread. The frame launches both and the one that does
+// not match the plan's layout returns at once. Three blocks per SM.
+//   1) load; per-warp digit counts -> the tile's counts, published at once (aggregate, or
+//      inclusive for tile 0), and the tile's digit starts;
+//   2) ranks: peer masks of each warp step, a warp-private running count per digit; every key
+//      goes straight to its place in the tile's stable order in shared memory;
+//   3) the look-back of digit tid gives the global offset of the tile's run of that digit;
+//   4) the runs are written out, coalesced.
+// Items past the end of the list are loaded as all-ones keys: their digit is the largest one
+// the key width allows, they rank after every real key of the tile and are never stored.
+template <bool PAIRS>
+struct PassShape {
+    static constexpr int kItems = PAIRS ? 16 : 24;
+    static constexpr int kTile = kSortThreads * kItems;
+    // keys, values, per-warp running counts [8][256], per-warp peer masks [8][2][256]
+    static constexpr int kSmemBytes = kTile * 8 + (PAIRS ? kTile * 4 : 0) + 8 * 256 * 4 * 3;
+};
+static_assert(kSortThreads == 256, "one digit per thread");
+static_assert(PassShape<true>::kTile == kSortTile, "the status array is sized by the smaller tile");
+
+template <bool PAIRS>
+__global__ void __launch_bounds__(kSortThreads, 3) sortPassKernel(const __grid_constant__ SortArgs a, uint32_t p) {
+    using S = PassShape<PAIRS>;
+    constexpr int kItems = S::kItems, kTile = S::kTile;
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
-    uint32_t* sWarpHist = reinterpret_cast<uint32_t*>(smem + kSortTile * 8);
-    uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + kSortTile * 8 + 8 * 256 * 4);
-    __shared__ uint32_t sDigitStart[256], sGlobalBase[256], sWarp[8], sTile;
+    uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + kTile * 8);
+    uint32_t* sWarpCnt = reinterpret_cast<uint32_t*>(smem + kTile * (PAIRS ? 12 : 8));  // [8][256]
+    uint32_t* sMask = sWarpCnt + 8 * 256;                                                // [8][2][256]
+    __shared__ uint32_t sOff[256], sScan[8], sTile;
     const SortPlan* plan = a.plan;
-    if (!plan->active[p] || (plan->packed != 0) != PACKED) return;
+    if (!plan->active[p] || (plan->packed == 0) != PAIRS) return;
     DeviceControl* ctl = a.ctl;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t entries = ctl->c.entries;
     if (tid == 0) sTile = atomicAdd(&ctl->tickets[1 + p], 1u);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) sWarpHist[j * 256 + tid] = 0;
+    for (int j = 0; j < 24; ++j) sWarpCnt[j * 256 + tid] = 0;
     __syncthreads();
     const uint32_t t = sTile;
-    const uint32_t tileBase = t * kSortTile;
+    const uint32_t tileBase = t * kTile;
     if (tileBase >= entries || t >= a.maxTiles) return;
     const uint32_t in = plan->inBuffer[p];
     const uint64_t* keysIn = a.keys[in];
@@ -176,271 +254,89 @@ __global__ void __launch_bounds__(kSortThreads, PACKED ? 4 : 3) sortPassKernel(c
     uint32_t* valsOut = a.values[in ^ 1u];
     const uint32_t lowBits = plan->lowBits;
     const uint64_t keyMask = maskOf(plan->keyBits);
-    const uint32_t shift = 8 * p + (PACKED ? plan->indexBits : 0u);
-
-    const uint32_t itemBase = tileBase + warp * (32 * kSortItems) + lane;
-    // digit of a key; past the end: 0x100, ranked nowhere
+    const uint32_t shift = 8 * p + (PAIRS ? 0u : plan->indexBits);
     auto digit = [&](uint64_t k) -> uint32_t {
-        return PACKED ? uint32_t(k >> shift) & 0xFFu : uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & 0xFFu;
+        return PAIRS ? uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & 0xFFu : uint32_t(k >> shift) & 0xFFu;
     };
-    auto digitOf = [&](uint64_t k, uint32_t idx) -> uint32_t { return idx < entries ? digit(k) : 0x100u; };
-    uint64_t key[kSortItems];
-    uint32_t val[PACKED ? 1 : kSortItems];
+
+    // 1) load, count, publish
+    const uint32_t itemBase = tileBase + warp * (32 * kItems) + lane;
+    uint64_t key[kItems];
+    uint32_t val[PAIRS ? kItems : 1];
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
+    for (int j = 0; j < kItems; ++j) {
         const uint32_t idx = itemBase + j * 32;
-        key[j] = idx < entries ? keysIn[idx] : 0ull;
-        if (!PACKED) val[PACKED ? 0 : j] = idx < entries ? valsIn[idx] : 0u;
+        key[j] = idx < entries ? __ldg(&keysIn[idx]) : ~0ull;
+        if (PAIRS) val[PAIRS ? j : 0] = idx < entries ? __ldg(&valsIn[idx]) : 0u;
     }
-    // warp-level multisplit: rank of each item among the warp's earlier items of its digit
-    uint32_t* wh = sWarpHist + warp * 256;
-    const uint32_t ltMask = laneMaskLt();
-    uint32_t rank[kSortItems / 2];  // two 16-bit ranks per word
+    uint32_t* wc = sWarpCnt + warp * 256;
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        const uint32_t d = digitOf(key[j], itemBase + j * 32);
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-        const uint32_t below = peers & ltMask;
-        const uint32_t pre = d < 256 ? wh[d] : 0u;
-        __syncwarp();
-        if (d < 256 && below == 0) wh[d] = pre + __popc(peers);
-        __syncwarp();
-        const uint32_t r = pre + __popc(below);
-        if (j & 1) rank[j >> 1] |= r << 16;
-        else rank[j >> 1] = r;
-    }
+    for (int j = 0; j < kItems; ++j)
+        if (itemBase + j * 32 < entries) atomicAdd(&wc[digit(key[j])], 1u);
     __syncthreads();
-    // digit tid: warp offsets (exclusive over warps) and the block's count
     const uint32_t d = tid;
-    uint32_t run = 0;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) {
-        const uint32_t c = sWarpHist[w * 256 + d];
-        sWarpHist[w * 256 + d] = run;
-        run += c;
-    }
-    const uint32_t blockCount = run;
-    const uint32_t epoch = ctl->c.epoch;
-    uint64_t* status = a.status + (size_t(p) * a.maxTiles) * 256;
-    stRelease(&status[size_t(t) * 256 + d], packStatus(epoch, t == 0 ? kFlagInclusive : kFlagAggregate, blockCount));
-    uint32_t total;
-    sDigitStart[d] = blockExclusiveScan256(blockCount, sWarp, &total);
-    // decoupled look-back for digit d over the earlier tiles of this pass
-    uint32_t exclusive = 0;
-    if (t > 0) {
-        const uint32_t forced = ctl->forceTimeout;
-        uint32_t spins = 0;
-        int q = int(t) - 1;
-        while (q >= 0) {
-            const uint64_t s = ldAcquire(&status[size_t(q) * 256 + d]);
-            bool ready = statusReady(s, epoch);
-            if (forced && spins < forced) ready = false;
-            if (!ready) {
-                if (++spins >= kSpinLimit || (forced && spins >= forced)) {
-                    reportTimeout(ctl, kWaitSort);
-                    break;
-                }
-                __nanosleep(32);
-                continue;
-            }
-            exclusive += uint32_t(s);
-            if (statusFlag(s) == kFlagInclusive) break;
-            --q;
-        }
-        stRelease(&status[size_t(t) * 256 + d], packStatus(epoch, kFlagInclusive, exclusive + blockCount));
-    }
-    sGlobalBase[d] = plan->digitBase[p][d] + exclusive;
-    __syncthreads();
-    // local stable order in shared memory
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        const uint32_t dj = digitOf(key[j], itemBase + j * 32);
-        if (dj < 256) {
-            const uint32_t r = (j & 1) ? (rank[j >> 1] >> 16) : (rank[j >> 1] & 0xFFFFu);
-            const uint32_t pos = sDigitStart[dj] + sWarpHist[warp * 256 + dj] + r;
-            sKeys[pos] = key[j];
-            if (!PACKED) sVals[pos] = val[PACKED ? 0 : j];
-        }
-    }
-    __syncthreads();
-    const uint32_t n = entries - tileBase < uint32_t(kSortTile) ? entries - tileBase : uint32_t(kSortTile);
-    for (uint32_t k = tid; k < n; k += kSortThreads) {
-        const uint64_t kk = sKeys[k];
-        const uint32_t dk = digit(kk);
-        const uint32_t g = sGlobalBase[dk] + (k - sDigitStart[dk]);
-        if (g < entries) {
-            keysOut[g] = kk;
-            if (!PACKED) valsOut[g] = sVals[k];
-        } else {
-            atomicOr(&ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
-        }
-    }
-}
-
-// ---- one onesweep pass over packed entries: 12288-key tiles, 768 threads ----------------------
-// The frame's usual layout. One block per SM: the first wave of a pass is ~148 tiles deep
-// instead of ~600, so the decoupled look-back chains stay short. Each tile publishes its
-// per-digit counts as soon as its keys are loaded (a shared-memory histogram), ranks them with
-// warp-level multisplit meanwhile, then looks back 8 predecessors per round trip.
-constexpr int kBigThreads = 768;
-constexpr int kBigTile = kBigThreads * kSortItems;  // 12288 keys
-constexpr int kBigWarps = kBigThreads / 32;
-constexpr int kBigSmemBytes = kBigTile * 8 + kBigWarps * 256 * 4;
-static_assert(kBigWarps * 256 == 8 * kBigThreads, "the warp histograms are zeroed 8 words per thread");
-
-__global__ void __launch_bounds__(kBigThreads, 1) sortPassPackedKernel(const __grid_constant__ SortArgs a, uint32_t p) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
-    uint32_t* sWarpHist = reinterpret_cast<uint32_t*>(smem + kBigTile * 8);  // [kBigWarps][256]
-    __shared__ uint32_t sBlockHist[256], sDigitStart[256], sGlobalBase[256], sWarp[8], sTile;
-    const SortPlan* plan = a.plan;
-    if (!plan->active[p] || !plan->packed) return;
-    DeviceControl* ctl = a.ctl;
-    const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t entries = ctl->c.entries;
-    if (tid == 0) sTile = atomicAdd(&ctl->tickets[1 + p], 1u);
-#pragma unroll
-    for (int j = 0; j < 8; ++j) sWarpHist[j * kBigThreads + tid] = 0;
-    if (tid < 256) sBlockHist[tid] = 0;
-    __syncthreads();
-    const uint32_t t = sTile;
-    const uint32_t tileBase = t * kBigTile;
-    if (tileBase >= entries) return;
-    const uint32_t in = plan->inBuffer[p];
-    const uint64_t* keysIn = a.keys[in];
-    uint64_t* keysOut = a.keys[in ^ 1u];
-    const uint32_t shift = 8 * p + plan->indexBits;
-    const uint32_t itemBase = tileBase + warp * (32 * kSortItems) + lane;
-    auto digitOf = [&](uint64_t k, uint32_t idx) -> uint32_t {
-        return idx < entries ? uint32_t(k >> shift) & 0xFFu : 0x100u;
-    };
-    uint64_t key[kSortItems];
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        const uint32_t idx = itemBase + j * 32;
-        key[j] = idx < entries ? keysIn[idx] : 0ull;
-    }
-    // 1) the tile's digit counts, published at once (aggregate; inclusive for the first tile)
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        const uint32_t d = digitOf(key[j], itemBase + j * 32);
-        if (d < 256) atomicAdd(&sBlockHist[d], 1u);
-    }
-    __syncthreads();
     const uint32_t epoch = ctl->c.epoch;
     uint64_t* status = a.status + (size_t(p) * a.maxTiles) * 256;
     uint32_t blockCount = 0;
-    if (tid < 256) {
-        blockCount = sBlockHist[tid];
-        stRelease(&status[size_t(t) * 256 + tid], packStatus(epoch, t == 0 ? kFlagInclusive : kFlagAggregate, blockCount));
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {  // warp offsets of digit d, exclusive over the warps
+        const uint32_t c = sWarpCnt[w * 256 + d];
+        sWarpCnt[w * 256 + d] = blockCount;
+        blockCount += c;
     }
-    // 2) warp-level multisplit ranks
-    uint32_t* wh = sWarpHist + warp * 256;
+    stRelaxed(&status[size_t(t) * 256 + d], packStatus(epoch, t == 0 ? kFlagInclusive : kFlagAggregate, blockCount));
+    uint32_t total;
+    const uint32_t blockStart = blockExclusiveScan256(blockCount, sScan, &total);
+#pragma unroll
+    for (int w = 0; w < 8; ++w) sWarpCnt[w * 256 + d] += blockStart;
+    __syncthreads();
+
+    // 2) ranks and the local stable order
     const uint32_t ltMask = laneMaskLt();
-    uint32_t rank[kSortItems / 2];
+    uint32_t prevDigit = 0, prevLeader = 0;
 #pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        const uint32_t d = digitOf(key[j], itemBase + j * 32);
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+    for (int j = 0; j < kItems; ++j) {
+        const uint32_t dj = digit(key[j]);
+        uint32_t* mask = sMask + (warp * 2 + (j & 1)) * 256;
+        atomicOr(&mask[dj], 1u << lane);
+        __syncwarp();
+        const uint32_t peers = mask[dj];
+        // the previous step's masks were read by every lane before the last __syncwarp
+        if (j > 0 && prevLeader) sMask[(warp * 2 + ((j & 1) ^ 1)) * 256 + prevDigit] = 0;
         const uint32_t below = peers & ltMask;
-        const uint32_t pre = d < 256 ? wh[d] : 0u;
+        prevDigit = dj;
+        prevLeader = below == 0;
         __syncwarp();
-        if (d < 256 && below == 0) wh[d] = pre + __popc(peers);
-        __syncwarp();
-        const uint32_t r = pre + __popc(below);
-        if (j & 1) rank[j >> 1] |= r << 16;
-        else rank[j >> 1] = r;
+        uint32_t first = 0;
+        if (below == 0) first = atomicAdd(&wc[dj], uint32_t(__popc(peers)));
+        const uint32_t pos = __shfl_sync(0xFFFFFFFFu, first, __ffs(peers) - 1) + __popc(below);
+        if (itemBase + j * 32 < entries) {
+            sKeys[pos] = key[j];
+            if (PAIRS) sVals[pos] = val[PAIRS ? j : 0];
+        }
     }
+
+    // 3) global offset of digit d's run
+    uint32_t exclusive = 0;
+    if (t > 0) {
+        exclusive = digitLookback(status, t, d, epoch, ctl);
+        stRelaxed(&status[size_t(t) * 256 + d], packStatus(epoch, kFlagInclusive, exclusive + blockCount));
+    }
+    sOff[d] = plan->digitBase[p][d] + exclusive - blockStart;
     __syncthreads();
-    // 3) digit d = tid < 256: warp offsets, the tile's digit starts, and the look-back
-    if (tid < 256) {
-        const uint32_t d = tid;
-        uint32_t run = 0;
-        for (int w = 0; w < kBigThreads / 32; ++w) {
-            const uint32_t c = sWarpHist[w * 256 + d];
-            sWarpHist[w * 256 + d] = run;
-            run += c;
-        }
-        // block-wide exclusive scan of the 256 counts (warps 0-7)
-        uint32_t incl = blockCount;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= uint32_t(o)) incl += v;
-        }
-        if (lane == 31) sWarp[warp] = incl;
-    }
-    __syncthreads();
-    if (tid < 256) {
-        const uint32_t d = tid;
-        uint32_t base = 0;
-        for (uint32_t w = 0; w < warp; ++w) base += sWarp[w];
-        uint32_t incl = blockCount;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= uint32_t(o)) incl += v;
-        }
-        sDigitStart[d] = base + incl - blockCount;
-    }
-    __syncthreads();
-    // 4) local order in shared memory (before the look-back: the keys leave the registers)
-#pragma unroll
-    for (int j = 0; j < kSortItems; ++j) {
-        const uint32_t dj = digitOf(key[j], itemBase + j * 32);
-        if (dj < 256) {
-            const uint32_t r = (j & 1) ? (rank[j >> 1] >> 16) : (rank[j >> 1] & 0xFFFFu);
-            sKeys[sDigitStart[dj] + sWarpHist[warp * 256 + dj] + r] = key[j];
-        }
-    }
-    if (tid < 256) {
-        const uint32_t d = tid;
-        // 5) windowed look-back: 8 predecessors per round trip
-        uint32_t exclusive = 0;
-        if (t > 0) {
-            const uint32_t forced = ctl->forceTimeout;
-            uint32_t spins = 0;
-            int q = int(t) - 1;
-            bool found = false;
-            while (!found && q >= 0) {
-                uint64_t w[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    w[j] = q - j >= 0 ? ldAcquire(&status[size_t(q - j) * 256 + d]) : packStatus(epoch, kFlagInclusive, 0);
-                int used = 0;
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    if (found || used != j) continue;
-                    bool ready = statusReady(w[j], epoch);
-                    if (forced && spins < forced) ready = false;
-                    if (!ready) continue;
-                    exclusive += uint32_t(w[j]);
-                    ++used;
-                    if (statusFlag(w[j]) == kFlagInclusive) found = true;
-                }
-                if (found) break;
-                q -= used;
-                if (used < 8) {
-                    if (++spins >= kSpinLimit || (forced && spins >= forced)) {
-                        reportTimeout(ctl, kWaitSort);
-                        break;
-                    }
-                    __nanosleep(32);
-                }
-            }
-            stRelease(&status[size_t(t) * 256 + d], packStatus(epoch, kFlagInclusive, exclusive + blockCount));
-        }
-        sGlobalBase[d] = plan->digitBase[p][d] + exclusive;
-    }
-    __syncthreads();
-    // 6) coalesced runs to the global positions
-    const uint32_t n = entries - tileBase < uint32_t(kBigTile) ? entries - tileBase : uint32_t(kBigTile);
-    for (uint32_t k = tid; k < n; k += kBigThreads) {
+
+    // 4) write-out
+    const uint32_t n = entries - tileBase < uint32_t(kTile) ? entries - tileBase : uint32_t(kTile);
+#pragma unroll 4
+    for (uint32_t k = tid; k < n; k += kSortThreads) {
         const uint64_t kk = sKeys[k];
-        const uint32_t dk = uint32_t(kk >> shift) & 0xFFu;
-        const uint32_t g = sGlobalBase[dk] + (k - sDigitStart[dk]);
-        if (g < entries) keysOut[g] = kk;
-        else atomicOr(&ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
+        const uint32_t g = sOff[digit(kk)] + k;
+        if (g < entries) {
+            keysOut[g] = kk;
+            if (PAIRS) valsOut[g] = sVals[k];
+        } else {
+            atomicOr(&ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
+        }
     }
 }
 
@@ -511,11 +407,11 @@ __global__ void __launch_bounds__(256) scanKernel(const uint32_t* __restrict__ i
     const uint32_t epoch = ctl->c.epoch;
     if (warp == 0) {
         if (lane == 0)
-            stRelease(&status[block], packStatus(epoch, block == 0 ? kFlagInclusive : kFlagAggregate, blockTotal));
+            stRelaxed(&status[block], packStatus(epoch, block == 0 ? kFlagInclusive : kFlagAggregate, blockTotal));
         uint32_t exclusive = 0;
         if (block > 0) exclusive = warpLookback(status, int(block), epoch, ctl, waitSite);
         if (lane == 0) {
-            if (block > 0) stRelease(&status[block], packStatus(epoch, kFlagInclusive, exclusive + blockTotal));
+            if (block > 0) stRelaxed(&status[block], packStatus(epoch, kFlagInclusive, exclusive + blockTotal));
             sExclusive = exclusive;
         }
     }
@@ -567,19 +463,20 @@ cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
         cudaError_t e = cudaFuncSetAttribute(sortPassKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             kSortSmemBytes);
+                                             PassShape<false>::kSmemBytes);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(sortPassPackedKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kBigSmemBytes);
+        e = cudaFuncSetAttribute(sortPassKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 PassShape<true>::kSmemBytes);
         if (e != cudaSuccess) return e;
         configured = true;
     }
     sortHistKernel<<<histBlocks < 1 ? 1 : histBlocks, 256, 0, s>>>(a);
-    const uint32_t grid = a.maxTiles < 1 ? 1 : a.maxTiles;
-    const uint32_t bigGrid = (grid + (kBigTile / kSortTile) - 1) / (kBigTile / kSortTile);
+    const uint32_t pairGrid = a.maxTiles < 1 ? 1 : a.maxTiles;
+    const uint32_t wordGrid = uint32_t((uint64_t(pairGrid) * kSortTile + PassShape<false>::kTile - 1) / PassShape<false>::kTile);
     for (uint32_t p = 0; p < a.passesLaunched; ++p) {
         // the entry layout is decided on the device: both run, the other one returns at once
-        if (a.frameMode) sortPassPackedKernel<<<bigGrid, kBigThreads, kBigSmemBytes, s>>>(a, p);
-        sortPassKernel<false><<<grid, kSortThreads, kSortSmemBytes, s>>>(a, p);
+        if (a.frameMode) sortPassKernel<false><<<wordGrid, kSortThreads, PassShape<false>::kSmemBytes, s>>>(a, p);
+        sortPassKernel<true><<<pairGrid, kSortThreads, PassShape<true>::kSmemBytes, s>>>(a, p);
     }
     return cudaGetLastError();
 }

@@ -464,7 +464,7 @@ struct GsrRenderer {
         sa.frameMode = 1;
         sa.tileCount = tileCount;
         sa.count = scene.count;
-        GSR_CUDA(launchSort(sa, 148 * 2, stream));
+        GSR_CUDA(launchSort(sa, 148 * 4, stream));
         if (timing) GSR_CUDA(cudaEventRecord(ev[2], stream));
 
         RenderArgs ra{};
@@ -1002,7 +1002,7 @@ int gsr_sort_pairs(uint32_t* keysLo, uint32_t* keysHi, uint32_t* values, uint32_
     sa.frameMode = 0;
     sa.fixedLowBits = 32;
     sa.fixedKeyBits = keyBits;
-    GSR_CUDA(launchSort(sa, 148 * 2, s));
+    GSR_CUDA(launchSort(sa, 148 * 4, s));
     GSR_CUDA(cudaStreamSynchronize(s));
     DeviceControl c;
     GSR_CUDA(cudaMemcpy(&c, ctl.p, sizeof(c), cudaMemcpyDeviceToHost));
