@@ -234,7 +234,8 @@ void gsr_renderer_destroy(GsrRenderer* r);
 typedef enum GsrScanMode { GSR_SCAN_PLAIN = 0, GSR_SCAN_NONZERO = 1, GSR_SCAN_GATHER = 2 } GsrScanMode;
 /* Exclusive scan of `count` u32 (device pointers): out[j] = sum_{i<j} v(i), v(i) = in[i]
  * (plain), in[i] != 0 (non-zero flags) or in[index[i]] (gather); *total (device) = the sum.
- * Stream-ordered; the scratch is allocated per call (see gsr_scan_scratch_bytes for reuse). */
+ * The scratch (control block, look-back words) is allocated and freed per call, and the call
+ * returns after the scan has finished on `stream`. */
 int gsr_scan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
              uint32_t mode, void* stream);
 /* Stable LSD sort of (key, value) pairs by the low key_bits of the key, in place (device
