@@ -1,6 +1,7 @@
 // Types and constants shared by the host renderer and the kernels (host-safe: no device code).
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 
 #include "gsr_b200.h"
@@ -26,6 +27,13 @@ struct DeviceControl {
     uint32_t forceTimeout;      // test hook: look-back waits see no predecessor for this many spins
     uint32_t pad[14];
 };
+
+// Layout of the static scratch of gsr_scan_static: the control block, then one look-back word
+// per 2048-item scan block of the largest accepted count.
+constexpr size_t kStaticScanCtlBytes = 512;
+constexpr size_t kStaticScanScratchBytes = kStaticScanCtlBytes + size_t(GSR_SCAN_STATIC_MAX_COUNT / 2048) * 8;
+static_assert(sizeof(DeviceControl) <= kStaticScanCtlBytes, "the control block fits its slot");
+static_assert(kStaticScanScratchBytes == 66048, "the size the header states");
 
 // The C library's logf fixup table on the device (see libcLogf in gsr_device.cuh).
 struct LogfFixups {

@@ -498,6 +498,13 @@ cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out,
     return cudaGetLastError();
 }
 
+// The scratch of gsr_scan_static: a fixed array instead of a per-call allocation (control
+// block at offset 0, look-back words from kStaticScanCtlBytes). Zero at module load; every
+// call clears what it uses. One array per device, shared by all calls on that device.
+static __device__ __align__(256) unsigned char gStaticScanScratch[kStaticScanScratchBytes];
+
+cudaError_t staticScanScratch(void** base) { return cudaGetSymbolAddress(base, gStaticScanScratch); }
+
 cudaError_t launchPack64(const uint32_t* lo, const uint32_t* hi, uint64_t* out, uint32_t n, cudaStream_t s) {
     if (!n) return cudaSuccess;
     pack64Kernel<<<gridFor(n, 256, 148 * 16), 256, 0, s>>>(lo, hi, out, n);

@@ -106,6 +106,9 @@ cudaError_t launchLogfTable(float* out, LogfFixups t, cudaStream_t s);
 cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
                        uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s, uint32_t setupCapacity = 0,
                        uint32_t waitSite = kWaitStandaloneScan);
+// Device address of the static scratch of gsr_scan_static (kStaticScanScratchBytes) on the
+// current device.
+cudaError_t staticScanScratch(void** base);
 cudaError_t launchPack64(const uint32_t* lo, const uint32_t* hi, uint64_t* out, uint32_t n, cudaStream_t s);
 cudaError_t launchUnpack64(const uint64_t* in, uint32_t* lo, uint32_t* hi, uint32_t n, cudaStream_t s);
 cudaError_t launchSetEntries(DeviceControl* ctl, uint32_t count, cudaStream_t s);

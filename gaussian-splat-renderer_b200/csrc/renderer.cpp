@@ -969,6 +969,49 @@ int gsr_scan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t*
     return GSR_OK;
 }
 
+// gsr_scan without allocation, for callers that must not allocate device memory: recovery code
+// running after an allocation failed (the device's memory is held by a resident scene), hooks of
+// a caching allocator that must not re-enter it, and streams that must not stall behind cudaFree
+// (it synchronizes the whole device). The scratch is the static array of k_sort.cu; its address
+// is looked up once per device and kept. Overlapping calls on one device share that array and
+// race (the header tells the caller to serialize them).
+namespace {
+constexpr int kMaxStaticScanDevices = 64;
+std::mutex g_staticScanMutex;
+void* g_staticScanBase[kMaxStaticScanDevices] = {};
+}  // namespace
+
+int gsr_scan_static(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
+                    uint32_t mode, void* stream) {
+    if (mode > GSR_SCAN_GATHER || (count && (!in || !out)) || (mode == GSR_SCAN_GATHER && count && !index))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "scan arguments");
+    if (count > GSR_SCAN_STATIC_MAX_COUNT)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "gsr_scan_static: count %u exceeds the static scratch limit of %u items",
+                    count, GSR_SCAN_STATIC_MAX_COUNT);
+    int dev = 0;
+    GSR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxStaticScanDevices) return fail(GSR_ERROR_INVALID_ARGUMENT, "device ordinal %d", dev);
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_staticScanMutex);
+        if (!g_staticScanBase[dev]) GSR_CUDA(staticScanScratch(&g_staticScanBase[dev]));
+        base = g_staticScanBase[dev];
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DeviceControl* ctl = static_cast<DeviceControl*>(base);
+    uint64_t* status = reinterpret_cast<uint64_t*>(static_cast<unsigned char*>(base) + kStaticScanCtlBytes);
+    const uint32_t blocks = (count + 2047) / 2048;
+    // what must start at zero: the look-back words here, the block tickets in frame begin
+    if (blocks) GSR_CUDA(cudaMemsetAsync(status, 0, size_t(blocks) * 8, s));
+    GSR_CUDA(launchFrameBegin(ctl, count, 0, nullptr, 0, nullptr, 0, s));
+    GSR_CUDA(launchScan(in, index, out, total, count, mode, status, ctl, s));
+    uint32_t st = 0;
+    GSR_CUDA(cudaMemcpyAsync(&st, &ctl->c.status, sizeof(st), cudaMemcpyDeviceToHost, s));
+    GSR_CUDA(cudaStreamSynchronize(s));
+    if (st & GSR_CONTROL_TIMEOUT) return fail(GSR_ERROR_DEVICE_TIMEOUT, "scan look-back timed out");
+    return GSR_OK;
+}
+
 int gsr_sort_pairs(uint32_t* keysLo, uint32_t* keysHi, uint32_t* values, uint32_t count, uint32_t keyBits, void* stream) {
     if (keyBits == 0 || keyBits > 64 || (!keysHi && keyBits > 32)) return fail(GSR_ERROR_INVALID_ARGUMENT, "key_bits %u", keyBits);
     if (count == 0) return GSR_OK;

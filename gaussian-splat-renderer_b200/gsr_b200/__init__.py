@@ -165,6 +165,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_renderer_kernel_launches": (C.c_int, [vp, C.POINTER(u64)]),
         "gsr_renderer_destroy": (None, [vp]),
         "gsr_scan": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
+        "gsr_scan_static": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_sort_pairs": (C.c_int, [vp, vp, vp, u32, u32, vp]),
         "gsr_debug_logf_table": (C.c_int, [vp, vp]),
     }
@@ -384,6 +385,17 @@ class Renderer:
 def scan(in_ptr: int, index_ptr: int | None, out_ptr: int, total_ptr: int | None, count: int, mode: int, stream: int = 0):
     check(load().gsr_scan(C.c_void_p(in_ptr), C.c_void_p(index_ptr), C.c_void_p(out_ptr), C.c_void_p(total_ptr), count,
                           mode, C.c_void_p(stream)))
+
+
+SCAN_STATIC_MAX_COUNT = 1 << 24  # GSR_SCAN_STATIC_MAX_COUNT
+
+
+def scan_static(in_ptr: int, index_ptr: int | None, out_ptr: int, total_ptr: int | None, count: int, mode: int,
+                stream: int = 0):
+    """gsr_scan_static: `scan` on the library's fixed static scratch (no allocation; count <= 2^24;
+    overlapping calls on one device race)."""
+    check(load().gsr_scan_static(C.c_void_p(in_ptr), C.c_void_p(index_ptr), C.c_void_p(out_ptr),
+                                 C.c_void_p(total_ptr), count, mode, C.c_void_p(stream)))
 
 
 def sort_pairs(lo_ptr: int, hi_ptr: int | None, values_ptr: int, count: int, key_bits: int, stream: int = 0):

@@ -238,6 +238,24 @@ typedef enum GsrScanMode { GSR_SCAN_PLAIN = 0, GSR_SCAN_NONZERO = 1, GSR_SCAN_GA
  * returns after the scan has finished on `stream`. */
 int gsr_scan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
              uint32_t mode, void* stream);
+/* Largest count gsr_scan_static accepts. */
+#define GSR_SCAN_STATIC_MAX_COUNT 16777216u
+/* gsr_scan without any allocation. NO COUNTERPART IN THE REFERENCE (its GpuScan, gpu_scan.h,
+ * owns scratch buffers that it creates itself); added for callers that must not allocate
+ * device memory: recovery code that runs after an allocation failed (device memory held by a
+ * resident scene), hooks of a caching allocator that must not re-enter it, and streams that
+ * must not stall behind cudaFree, which synchronizes the whole device.
+ * Same arguments, results and errors as gsr_scan. The scratch (a 512-byte control block and
+ * one look-back word per 2048 items) is a fixed 66,048-byte static device array of this
+ * library; count above GSR_SCAN_STATIC_MAX_COUNT (2^24) is rejected with
+ * GSR_ERROR_INVALID_ARGUMENT before anything is launched. The call clears what must start at
+ * zero (the block tickets and the look-back words) on `stream` and returns after the scan
+ * has finished there. Calls that overlap in time on one device (two streams or two host
+ * threads) share the array and race: the caller serializes them. The first call on each
+ * device looks the array up (cudaGetSymbolAddress) and should come before any stream
+ * capture begins on that device. */
+int gsr_scan_static(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
+                    uint32_t mode, void* stream);
 /* Stable LSD sort of (key, value) pairs by the low key_bits of the key, in place (device
  * pointers). keys_hi may be NULL (32-bit keys); with it the key is (keys_hi << 32 | keys_lo).
  * Bit-for-bit the order of a stable sort (DepthSorter::radixSortPairs for 32-bit keys). */
