@@ -22,7 +22,7 @@ enum WaitSite : uint32_t { kWaitScan = 1, kWaitSort = 2, kWaitStandaloneScan = 3
 // counters that only the kernels use.
 struct DeviceControl {
     GsrControl c;
-    uint32_t tickets[16];       // block tickets: [0] preprocess, [1 + p] sort pass p, [12] standalone scan
+    uint32_t tickets[16];       // block tickets: [1 + p] sort pass p, [12] scans, [13] the rasterizer's tile queue
     uint32_t histDone;          // blocks of the histogram kernel that have finished
     uint32_t forceTimeout;      // test hook: look-back waits see no predecessor for this many spins
     uint32_t pad[14];

@@ -189,15 +189,17 @@ __device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, const DevC
     return kCullVisible;
 }
 
-// 1) Preprocess + tight count, one thread per gaussian (splat_preprocess.comp:283-318, GSR_TILES):
-//    writes the splat record of visible gaussians and every gaussian's tile count; cull counters
-//    with one ballot per warp and one atomic per block and reason. No waits: a streaming kernel.
+// 1) Preprocess + tight count, one thread per (view, gaussian) (splat_preprocess.comp:283-318,
+//    GSR_TILES); grid.y = view. Writes the splat record of visible gaussians and every gaussian's
+//    tile count; cull counters with one ballot per warp and one atomic per block and reason. No
+//    waits: a streaming kernel.
 template <int GEOM, int COLOR>
 __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_constant__ FrontArgs a) {
-    __shared__ DevCamera sCam;  // the frame's camera, read once per block from its device copy
+    __shared__ DevCamera sCam;  // the view's camera, read once per block from its device copy
     __shared__ uint32_t sCull[kCullReasonCount];
     __shared__ uint32_t sDepthMin, sDepthMax;
     const uint32_t tid = threadIdx.x, lane = tid & 31;
+    const uint32_t view = blockIdx.y;
     if (tid < kCullReasonCount) sCull[tid] = 0;
     if (tid == 0) {
         sDepthMin = 0xFFFFFFFFu;
@@ -205,9 +207,11 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
     }
     static_assert(sizeof(DevCamera) == sizeof(DevCameraArgs) && sizeof(DevCamera) % 4 == 0, "camera layout");
     if (tid < sizeof(DevCamera) / 4)
-        reinterpret_cast<uint32_t*>(&sCam)[tid] = reinterpret_cast<const uint32_t*>(a.cam)[tid];
+        reinterpret_cast<uint32_t*>(&sCam)[tid] = reinterpret_cast<const uint32_t*>(a.cam + view)[tid];
     __syncthreads();
     const uint32_t i = blockIdx.x * kFrontThreads + tid;
+    const size_t rec = size_t(view) * a.count + i;
+    const int gx = int(sCam.tilesX) * (16 / a.binSize), gy = int(sCam.tilesY) * (16 / a.binSize);
     uint32_t reason = kCullReasonCount;  // threads past the end
     uint32_t dmin = 0xFFFFFFFFu, dmax = 0;
     if (i < a.count) {
@@ -216,14 +220,14 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
         uint32_t count = 0;
         reason = preprocessOne<GEOM, COLOR>(a, sCam, i, s, rect);
         if (reason == kCullVisible) {
-            const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, a.gridX, a.gridY, s.cx, s.cy, s.conicA,
-                                             s.conicB, s.conicC, s.opacity, a.logf);
+            const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
+                                             s.opacity, a.logf);
             count = coverageCount(cv, a.binSize);
             s.cullReason = kCullVisible;
-            reinterpret_cast<DevSplat*>(a.splats)[i] = s;
+            reinterpret_cast<DevSplat*>(a.splats)[rec] = s;
             dmin = dmax = __float_as_uint(s.depth);  // positive: the bits order like the values
         }
-        a.tileCounts[i] = count;
+        a.tileCounts[rec] = count;
     }
 #pragma unroll
     for (uint32_t r = 0; r < kCullReasonCount; ++r) {
@@ -245,14 +249,17 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
     }
 }
 
-// 3) Key emission, one thread per gaussian in index order (tile_duplicate.comp:177-221, global
-//    mode): the splat's tiles row by row at offsets [offset, offset + count), dropped at or past
-//    the capacity. The coverage is rebuilt from the splat's record with the same functions and
-//    the same inputs as the count, so it enumerates exactly `count` tiles; a disagreement would be
-//    counted (coverageMismatch) and padded with the sentinel tile, as the reference does.
+// 3) Key emission, one thread per (view, gaussian) in index order (tile_duplicate.comp:177-221,
+//    global mode): the splat's tiles row by row at offsets [offset, offset + count), dropped at or
+//    past the capacity. The coverage is rebuilt from the splat's record with the same functions
+//    and the same inputs as the count, so it enumerates exactly `count` tiles; a disagreement
+//    would be counted (coverageMismatch) and padded with the sentinel tile, as the reference
+//    does. The key's tile is the view's tile base + the tile in the view, so the list orders by
+//    view first and each view's entries form the single-view list.
 __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_constant__ FrontArgs a) {
     __shared__ uint32_t sTileMax, sMismatch, sAny;
     const uint32_t tid = threadIdx.x;
+    const uint32_t view = blockIdx.y;
     if (tid == 0) {
         sTileMax = 0;
         sMismatch = 0;
@@ -260,15 +267,18 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
     }
     __syncthreads();
     const uint32_t i = blockIdx.x * kFrontThreads + tid;
-    const uint32_t count = i < a.count ? a.tileCounts[i] : 0u;
+    const size_t rec = size_t(view) * a.count + i;
+    const uint32_t count = i < a.count ? a.tileCounts[rec] : 0u;
     if (count > 0) {
-        const uint32_t sentinel = uint32_t(a.gridX) * uint32_t(a.gridY);
+        const uint32_t sentinel = a.totalTiles;
         const KeyLayout lay = keyLayout(a.ctl, sentinel, a.count);
-        const uint32_t offset = a.offsets[i];
-        const DevSplat s = reinterpret_cast<const DevSplat*>(a.splats)[i];
-        const TileRect rect = tileRect(s.cx, s.cy, s.radius, a.cam->tilesX, a.cam->tilesY);
-        const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, a.gridX, a.gridY, s.cx, s.cy, s.conicA, s.conicB,
-                                         s.conicC, s.opacity, a.logf);
+        const uint32_t offset = a.offsets[rec];
+        const DevSplat s = reinterpret_cast<const DevSplat*>(a.splats)[rec];
+        const DevView vw = a.views[view];
+        const int gx = int(vw.tilesX) * (16 / a.binSize), gy = int(vw.tilesY) * (16 / a.binSize);
+        const TileRect rect = tileRect(s.cx, s.cy, s.radius, vw.tilesX, vw.tilesY);
+        const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
+                                         s.opacity, a.logf);
         const uint64_t depthBits = __float_as_uint(s.depth);
         // packed: (((tile << W) | depth mod 2^W) << indexBits) | index; the tile part added per entry
         const uint64_t packedBase =
@@ -292,7 +302,7 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
             int x0, x1;
             coverageRowSpan(cv, row, S, x0, x1);
             for (int x = x0; x < x1 && written < count; ++x, ++written, ++k) {
-                const uint32_t tile = uint32_t(row) * uint32_t(a.gridX) + uint32_t(x);
+                const uint32_t tile = vw.tileBase + uint32_t(row) * uint32_t(gx) + uint32_t(x);
                 tileMax = tile > tileMax ? tile : tileMax;
                 if (k < a.capacity) emit(k, tile);
             }
@@ -375,9 +385,9 @@ cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capaci
 }
 
 cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s) {
-    const uint32_t blocks = (a.count + kFrontThreads - 1) / kFrontThreads;
-    if (blocks == 0) return cudaSuccess;
-    // 1) preprocess + count
+    const dim3 blocks((a.count + kFrontThreads - 1) / kFrontThreads, a.viewCount);
+    if (blocks.x == 0 || blocks.y == 0) return cudaSuccess;
+    // 1) preprocess + count, grid (gaussian blocks, views)
     if (geometry == GSR_GEOMETRY_SOA_F32 && color == GSR_COLOR_SOA_F32)
         preprocessKernel<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32><<<blocks, kFrontThreads, 0, s>>>(a);
     else if (geometry == GSR_GEOMETRY_RECORD_F32 && color == GSR_COLOR_RECORD_F32)
@@ -390,10 +400,10 @@ cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, c
         return cudaErrorInvalidValue;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    // 2) exclusive scan of the counts (GpuScan over N), the list size and its clamp
-    //    (tile_setup.comp:16-24) by the scan's last block
-    e = launchScan(a.tileCounts, nullptr, a.offsets, &a.ctl->c.duplicates, a.count, GSR_SCAN_PLAIN, a.scanStatus, a.ctl,
-                   s, a.capacity, kWaitScan);
+    // 2) exclusive scan of the counts (GpuScan over V * N, view-major), the list size and its
+    //    clamp (tile_setup.comp:16-24) by the scan's last block
+    e = launchScan(a.tileCounts, nullptr, a.offsets, &a.ctl->c.duplicates, a.count * a.viewCount, GSR_SCAN_PLAIN,
+                   a.scanStatus, a.ctl, s, a.capacity, kWaitScan);
     if (e != cudaSuccess) return e;
     // 3) key emission
     duplicateKernel<<<blocks, kFrontThreads, 0, s>>>(a);

@@ -15,6 +15,13 @@
 //   C += colour alpha T; T = testT
 // and a whole-tile vote (__syncthreads_count) ends the tile once every pixel is done.
 //
+// Tiles are the frame's tiles over all of its views (DevView): tile t belongs to the view whose
+// [tileBase, tileBase + tilesX * tilesY) holds it, the records of that view's gaussians are at
+// view * N + g, and its pixels at the view's pixelBase. Two schedules of the same per-tile body:
+// one block per tile (a single view), or a persistent grid (a few blocks per SM) whose blocks
+// take the next tile from a queue counter until every tile of every view is done, which keeps
+// the SMs busy across views of uneven size.
+//
 // FMA contraction and the hardware exp2 make the float image differ from the CPU reference's
 // in the last bits (and, for pairs within an ulp of the 1/255 or 1e-4 thresholds, by one such
 // pair's contribution); tests bound it: float PSNR > 60 dB and the 8-bit image within 1/255.
@@ -26,6 +33,8 @@ namespace gsr {
 namespace {
 
 constexpr int kRenderThreads = 256;
+constexpr int kPersistentBlocksPerSm = 4;
+constexpr uint32_t kRenderQueueTicket = 13;  // DeviceControl::tickets slot of the persistent queue
 constexpr float kMaxAlpha = 0.99f;
 constexpr float kMinTransmittance = 1e-4f;
 constexpr float kLog2e = 1.4426950408889634f;
@@ -49,16 +58,29 @@ struct RenderShared {
     float4 box[kRenderThreads];        // x0, x1, y0, y1 of the cutoff ellipse (pixels)
     float4 color[kRenderThreads];      // r, g, b, -
     float2 center[kRenderThreads];
+    uint32_t tile;                     // persistent schedule: the block's current tile
 };
 
-__global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_constant__ RenderArgs a) {
-    extern __shared__ __align__(16) unsigned char smemRaw[];
-    RenderShared& sm = *reinterpret_cast<RenderShared*>(smemRaw);
-    const uint32_t tile = blockIdx.x;
+// The view holding frame tile t: the last view whose tileBase <= t (views are in tile order).
+__device__ __forceinline__ uint32_t viewOfTile(const RenderArgs& a, uint32_t t) {
+    uint32_t lo = 0, hi = a.viewCount;  // invariant: views[lo].tileBase <= t < views[hi].tileBase
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.views[mid].tileBase <= t) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// The whole per-tile pass for frame tile `tile`; every thread of the block calls it.
+__device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm, uint32_t tile) {
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
-    const uint32_t tx = tile % a.tilesX, ty = tile / a.tilesX;
+    const uint32_t view = viewOfTile(a, tile);
+    const DevView vw = a.views[view];
+    const uint32_t local = tile - vw.tileBase;
+    const uint32_t tx = local % vw.tilesX, ty = local / vw.tilesX;
     const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
-    const bool inside = px < a.width && py < a.height;
+    const bool inside = px < vw.width && py < vw.height;
     uint2 range = reinterpret_cast<const uint2*>(a.ranges)[tile];
     // a frame whose look-back gave up (GSR_CONTROL_TIMEOUT) has meaningless ranges: every index
     // read below stays inside the list and the scene all the same
@@ -70,7 +92,7 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
     const uint64_t* packedKeys = a.keys[sortedBuffer];
     const bool packed = a.plan->packed != 0;
     const uint64_t indexMask = (1ull << a.plan->indexBits) - 1ull;
-    const float4* records = reinterpret_cast<const float4*>(a.splats);
+    const float4* records = reinterpret_cast<const float4*>(a.splats) + size_t(view) * a.count * 3;
     const float fx = float(px), fy = float(py);
     // this warp's pixel strip
     const float wx0 = float(tx * 16), wx1 = float(tx * 16 + 15);
@@ -160,7 +182,7 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
     }
     cpAsyncWait<0>();
     if (!inside) return;
-    const size_t p = size_t(py) * a.width + px;
+    const size_t p = vw.pixelBase + size_t(py) * vw.width + px;
     a.image[p] = make_float4(c0, c1, c2, 1.0f - T);
     if (a.rgb8) {
         const float v[3] = {c0, c1, c2};
@@ -172,19 +194,49 @@ __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_cons
     }
 }
 
+// One block per frame tile.
+__global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_constant__ RenderArgs a) {
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    renderTile(a, *reinterpret_cast<RenderShared*>(smemRaw), blockIdx.x);
+}
+
+// Persistent schedule: each block takes tiles from the frame's queue counter (reset by frame
+// begin) until the counter passes the last tile.
+__global__ void __launch_bounds__(kRenderThreads) renderPersistentKernel(const __grid_constant__ RenderArgs a) {
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    RenderShared& sm = *reinterpret_cast<RenderShared*>(smemRaw);
+    for (;;) {
+        if (threadIdx.x == 0) sm.tile = atomicAdd(&a.ctl->tickets[kRenderQueueTicket], 1u);
+        __syncthreads();
+        const uint32_t tile = sm.tile;
+        if (tile >= a.totalTiles) break;
+        renderTile(a, sm, tile);
+        __syncthreads();  // every thread has read sm.tile and left the tile's shared buffers
+    }
+}
+
 }  // namespace
 
 cudaError_t launchRender(const RenderArgs& a, cudaStream_t s) {
-    const uint32_t tiles = a.tilesX * a.tilesY;
-    if (tiles == 0) return cudaSuccess;
+    if (a.totalTiles == 0) return cudaSuccess;
     static bool configured = false;
     if (!configured) {
-        const cudaError_t e =
+        cudaError_t e =
             cudaFuncSetAttribute(renderKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(RenderShared)));
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(renderPersistentKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sizeof(RenderShared)));
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    renderKernel<<<tiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
+    if (a.persistent) {
+        int sms = 148, dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const uint32_t grid = uint32_t(sms) * kPersistentBlocksPerSm;
+        renderPersistentKernel<<<grid < a.totalTiles ? grid : a.totalTiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
+    } else {
+        renderKernel<<<a.totalTiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
+    }
     return cudaGetLastError();
 }
 

@@ -351,7 +351,7 @@ __global__ void rangesKernel(const __grid_constant__ RenderArgs a) {
     const DeviceControl* ctl = a.ctl;
     const uint32_t n = ctl->c.entries;
     const uint64_t* keys = a.keys[ctl->c.sorted_buffer & 1u];
-    const uint32_t tileCount = a.tilesX * a.tilesY;
+    const uint32_t tileCount = a.totalTiles;  // every view's tiles; the sentinel is this id
     uint2* ranges = reinterpret_cast<uint2*>(a.ranges);
     const SortPlan* plan = a.plan;
     for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {

@@ -18,6 +18,19 @@ struct DevCameraArgs {  // = DevCamera (splat_math.cuh)
     uint32_t tilesX, tilesY;
 };
 
+// One view of a frame. A frame renders views [0, viewCount) of its launch together: view v's
+// tiles are the frame's tiles [tileBase, tileBase + tilesX * tilesY) (the "global" tile id, so
+// the view sits in the high bits of every list key) and its pixels start at pixelBase in the
+// image buffers. Per-gaussian arrays (records, tile counts, offsets) are indexed v * N + g.
+struct DevView {
+    uint32_t tileBase;
+    uint32_t tilesX, tilesY;
+    uint32_t width, height;
+    uint32_t pad;
+    uint64_t pixelBase;
+};
+static_assert(sizeof(DevView) == 32, "DevView layout");
+
 struct SceneArgs {
     const uint4* b0;     // soa posAlpha | geometry records | aos records
     const uint4* b1;     // soa scales   | colour records   | aos records
@@ -30,20 +43,22 @@ struct SceneArgs {
 
 // Arguments of the per-gaussian kernels of the frame's front (preprocess, scan, key emission).
 struct FrontArgs {
-    const DevCameraArgs* cam;  // device copy of the frame's SplatCamera (written by the frame itself)
+    const DevCameraArgs* cam;  // device copies of the views' SplatCameras [viewCount] (written by the frame itself)
+    const DevView* views;      // [viewCount]
+    uint32_t viewCount;        // V (grid.y of the per-gaussian kernels)
+    uint32_t totalTiles;       // tiles of all views = the sentinel tile id
     SceneArgs scene;
     uint32_t count;       // N
     int evalDegree;       // min(stored degree, max_sh_degree)
     uint32_t bounds;      // GsrTileBounds
     int binSize;          // S (16)
-    int gridX, gridY;     // bin grid
     uint32_t capacity;    // list entries
-    void* splats;         // DevSplat[N]
-    uint32_t* tileCounts; // [N]
-    uint32_t* offsets;    // [N] exclusive scan of tileCounts
-    uint64_t* keys;       // [capacity] (tile << 32 | depth bits), index order
+    void* splats;         // DevSplat[V * N]
+    uint32_t* tileCounts; // [V * N]
+    uint32_t* offsets;    // [V * N] exclusive scan of tileCounts
+    uint64_t* keys;       // [capacity] (tile << 32 | depth bits), view-major index order
     uint32_t* values;     // [capacity]
-    uint64_t* scanStatus; // [ceil(N / 2048)] look-back words of the scan over the counts
+    uint64_t* scanStatus; // [ceil(V * N / 2048)] look-back words of the scan over the counts
     DeviceControl* ctl;
     LogfFixups logf;
 };
@@ -81,13 +96,16 @@ struct SortArgs {
 };
 
 struct RenderArgs {
-    const void* splats;       // DevSplat[N]
+    const void* splats;       // DevSplat[V * N]
     const uint32_t* values[2];
     const uint64_t* keys[2];
-    uint32_t* ranges;         // uint2 per tile
-    float4* image;            // W*H
-    uint8_t* rgb8;            // W*H*3 or null
-    uint32_t width, height, tilesX, tilesY;
+    uint32_t* ranges;         // uint2 per tile of the frame (all views)
+    float4* image;            // per view W*H at the view's pixelBase
+    uint8_t* rgb8;            // per view W*H*3 at 3 * pixelBase, or null
+    const DevView* views;     // [viewCount]
+    uint32_t viewCount;
+    uint32_t totalTiles;
+    uint32_t persistent;      // 1: a fixed grid takes (view, tile) work items from a queue
     uint32_t count;           // N: gaussian indices read from the list are checked against it
     DeviceControl* ctl;
     const SortPlan* plan;     // the entry layout (packed words or key/value arrays)

@@ -191,6 +191,13 @@ struct GsrRenderer {
     uint32_t listResizes = 0;
     uint32_t shrinkFrames = 0, shrinkWindowMax = 0;
     uint64_t lastAdaptedFrame = ~0ull;
+    // views of the current frame layout (one for gsr_render); width..tilesY are view 0's
+    std::vector<GsrViewLayout> views;
+    uint32_t totalTiles = 0;
+    uint64_t totalPixels = 0;
+    uint32_t allocViews = 0;     // per-gaussian arrays and camera slots are sized for this many views
+    uint64_t layoutVersion = 0;  // changes whenever the buffers of the layout are re-created
+    DevBuf viewsDevice;          // DevView[views]
     // per tile / image
     uint32_t width = 0, height = 0, tilesX = 0, tilesY = 0;
     uint32_t passesUpper = 0;
@@ -206,8 +213,8 @@ struct GsrRenderer {
         bool used = false;
         uint64_t frameIndex = 0;
         cudaGraphExec_t graph = nullptr;
-        const void* graphList = nullptr;   // the list / image the graph was captured with
-        const void* graphImage = nullptr;
+        const void* graphList = nullptr;   // the list / layout the graph was captured with
+        uint64_t graphLayout = ~0ull;
         ~Slot() {
             if (graph) cudaGraphExecDestroy(graph);
         }
@@ -271,20 +278,78 @@ struct GsrRenderer {
         return GSR_OK;
     }
 
-    int resize(uint32_t w, uint32_t h) {
-        if (w == 0 || h == 0 || w > 32768 || h > 32768) return fail(GSR_ERROR_INVALID_ARGUMENT, "render size %ux%u", w, h);
-        if (w == width && h == height && list) return GSR_OK;
+    // Per-gaussian arrays and the frame slots' camera copies for `v` views (grown, never shrunk).
+    int ensureViews(uint32_t v) {
+        if (v <= allocViews) return GSR_OK;
+        const size_t n = size_t(scene.count) * v;
+        GSR_CUDA(splats.alloc(n * 48));
+        GSR_CUDA(cudaMemset(splats.p, 0, splats.bytes));
+        GSR_CUDA(tileCounts.alloc(n * 4));
+        GSR_CUDA(offsets.alloc(n * 4));
+        GSR_CUDA(scanStatus.alloc((n + 255) / 256 * 8));
+        GSR_CUDA(cudaMemset(scanStatus.p, 0, scanStatus.bytes));
+        for (auto& s : slots) {
+            if (s->camHost) cudaFreeHost(s->camHost);
+            s->camHost = nullptr;
+            GSR_CUDA(cudaMallocHost(&s->camHost, sizeof(DevCameraArgs) * v));
+            GSR_CUDA(s->camDevice.alloc(sizeof(DevCameraArgs) * v));
+        }
+        allocViews = v;
+        return GSR_OK;
+    }
+
+    // onRenderTargetsChanged for the views' sizes: the per-tile and image buffers of the frame's
+    // tiles and pixels over all views, and the list when the key width changes.
+    int setLayout(const uint32_t* w, const uint32_t* h, uint32_t v) {
+        if (v == 0 || v > GSR_MAX_VIEWS) return fail(GSR_ERROR_INVALID_ARGUMENT, "views %u (1..%u)", v, GSR_MAX_VIEWS);
+        if (uint64_t(scene.count) * v > 0xFFFFF800ull)
+            return fail(GSR_ERROR_INVALID_ARGUMENT, "views x gaussians = %llu exceeds 2^32",
+                        (unsigned long long)(uint64_t(scene.count) * v));
+        bool same = list && views.size() == v;
+        uint64_t tiles = 0, pixels = 0;
+        for (uint32_t i = 0; i < v; ++i) {
+            if (w[i] == 0 || h[i] == 0 || w[i] > 32768 || h[i] > 32768)
+                return fail(GSR_ERROR_INVALID_ARGUMENT, "render size %ux%u", w[i], h[i]);
+            if (same && (views[i].width != w[i] || views[i].height != h[i])) same = false;
+            tiles += uint64_t((w[i] + 15) / 16) * ((h[i] + 15) / 16);
+            pixels += uint64_t(w[i]) * h[i];
+        }
+        if (same) return GSR_OK;
+        if (tiles >= (1ull << 31)) return fail(GSR_ERROR_INVALID_ARGUMENT, "%llu tiles in one frame", (unsigned long long)tiles);
         GSR_CUDA(cudaDeviceSynchronize());  // the reference calls onRenderTargetsChanged with the GPU idle
-        width = w;
-        height = h;
-        tilesX = (w + 15) / 16;
-        tilesY = (h + 15) / 16;
-        const uint32_t tileCount = tilesX * tilesY;
+        int rc = ensureViews(v);
+        if (rc) return rc;
+        views.assign(v, GsrViewLayout{});
+        std::vector<DevView> dv(v);
+        uint32_t tileBase = 0;
+        uint64_t pixelBase = 0;
+        for (uint32_t i = 0; i < v; ++i) {
+            GsrViewLayout& L = views[i];
+            L.width = w[i];
+            L.height = h[i];
+            L.tiles_x = (w[i] + 15) / 16;
+            L.tiles_y = (h[i] + 15) / 16;
+            L.tile_base = tileBase;
+            L.pixel_base = pixelBase;
+            dv[i] = DevView{L.tile_base, L.tiles_x, L.tiles_y, L.width, L.height, 0, L.pixel_base};
+            tileBase += L.tiles_x * L.tiles_y;
+            pixelBase += uint64_t(w[i]) * h[i];
+        }
+        totalTiles = uint32_t(tiles);
+        totalPixels = pixels;
+        width = views[0].width;
+        height = views[0].height;
+        tilesX = views[0].tiles_x;
+        tilesY = views[0].tiles_y;
+        GSR_CUDA(viewsDevice.alloc(sizeof(DevView) * v));
+        GSR_CUDA(cudaMemcpy(viewsDevice.p, dv.data(), sizeof(DevView) * v, cudaMemcpyHostToDevice));
+        const uint32_t tileCount = totalTiles;
         GSR_CUDA(ranges.alloc(size_t(tileCount) * 8));
         GSR_CUDA(cudaMemset(ranges.p, 0, ranges.bytes));
-        GSR_CUDA(image.alloc(size_t(w) * h * 16));
-        if (settings.output_format == GSR_OUTPUT_RGBA32F_AND_RGB8) GSR_CUDA(rgb8.alloc(size_t(w) * h * 3));
+        GSR_CUDA(image.alloc(size_t(pixels) * 16));
+        if (settings.output_format == GSR_OUTPUT_RGBA32F_AND_RGB8) GSR_CUDA(rgb8.alloc(size_t(pixels) * 3));
         else rgb8.release();
+        ++layoutVersion;
         const uint32_t passes = passesFor(tileCount);
         if (passes != passesUpper || !list) {
             passesUpper = passes;
@@ -294,14 +359,16 @@ struct GsrRenderer {
             if (settings.adaptive_list) {
                 const uint64_t guess = settings.adaptive_initial_entries
                                            ? settings.adaptive_initial_entries
-                                           : std::max<uint64_t>(4ull * scene.count, 1u << 20);
+                                           : std::max<uint64_t>(4ull * scene.count * v, 1u << 20);
                 initial = std::min(maxCapacity, roundUpToBlock(guess));
             }
-            const int rc = createList(initial, list);
+            rc = createList(initial, list);
             if (rc) return rc;
         }
         return GSR_OK;
     }
+
+    int resize(uint32_t w, uint32_t h) { return setLayout(&w, &h, 1); }
 
     // readSlot (splat_tile_renderer.cpp:572-613): consume a completed readback.
     void readSlot(Slot& s) {
@@ -353,11 +420,23 @@ struct GsrRenderer {
         return GSR_OK;
     }
 
-    int render(const GsrSplatCamera& cam, cudaStream_t stream) {
-        if (cam.width != width || cam.height != height) {
-            const int rc = resize(cam.width, cam.height);
+    int render(const GsrSplatCamera& cam, cudaStream_t stream) { return renderViews(&cam, 1, stream); }
+
+    // One frame over cameras[0..v): the layout follows the cameras' sizes.
+    int renderViews(const GsrSplatCamera* cams, uint32_t v, cudaStream_t stream) {
+        if (v == 0 || v > GSR_MAX_VIEWS) return fail(GSR_ERROR_INVALID_ARGUMENT, "views %u (1..%u)", v, GSR_MAX_VIEWS);
+        bool same = views.size() == v;
+        for (uint32_t i = 0; same && i < v; ++i) same = cams[i].width == views[i].width && cams[i].height == views[i].height;
+        if (!same) {
+            std::vector<uint32_t> w(v), h(v);
+            for (uint32_t i = 0; i < v; ++i) w[i] = cams[i].width, h[i] = cams[i].height;
+            const int rc = setLayout(w.data(), h.data(), v);
             if (rc) return rc;
         }
+        for (uint32_t i = 0; i < v; ++i)
+            if (cams[i].tiles_x != views[i].tiles_x || cams[i].tiles_y != views[i].tiles_y)
+                return fail(GSR_ERROR_INVALID_ARGUMENT, "camera %u: tiles %ux%u for a %ux%u image", i, cams[i].tiles_x,
+                            cams[i].tiles_y, cams[i].width, cams[i].height);
         if (slots.empty()) return fail(GSR_ERROR_INVALID_ARGUMENT, "renderer not initialised");
         Slot& slot = *slots[frameIndex % slots.size()];
         readSlot(slot);
@@ -367,12 +446,12 @@ struct GsrRenderer {
         }
         int rc = adaptCapacity(stream);
         if (rc) return rc;
-        // the slot's previous frame has completed: its pinned camera may be overwritten
+        // the slot's previous frame has completed: its pinned cameras may be overwritten
         static_assert(sizeof(DevCameraArgs) == sizeof(GsrSplatCamera), "camera layout");
-        std::memcpy(slot.camHost, &cam, sizeof(cam));
+        std::memcpy(slot.camHost, cams, sizeof(GsrSplatCamera) * v);
         const bool graphed = settings.use_graph && !timing && forceTimeout == 0;
         if (graphed) {
-            if (!slot.graph || slot.graphList != list.get() || slot.graphImage != image.p) {
+            if (!slot.graph || slot.graphList != list.get() || slot.graphLayout != layoutVersion) {
                 if (slot.graph) cudaGraphExecDestroy(slot.graph);
                 slot.graph = nullptr;
                 if (!captureStream) GSR_CUDA(cudaStreamCreateWithFlags(&captureStream, cudaStreamNonBlocking));
@@ -389,7 +468,7 @@ struct GsrRenderer {
                 cudaGraphDestroy(g);
                 if (ie != cudaSuccess) return cudaFail(ie, "cudaGraphInstantiate");
                 slot.graphList = list.get();
-                slot.graphImage = image.p;
+                slot.graphLayout = layoutVersion;
             }
             GSR_CUDA(cudaGraphLaunch(slot.graph, stream));
         } else {
@@ -417,13 +496,18 @@ struct GsrRenderer {
         List& l = *list;
         DeviceControl* ctl = control.as<DeviceControl>();
         SortPlan* sortPlan = plan.as<SortPlan>();
-        const uint32_t tileCount = tilesX * tilesY;
+        const uint32_t tileCount = totalTiles;
+        const uint32_t viewCount = uint32_t(views.size());
         if (timing) GSR_CUDA(cudaEventRecord(ev[0], stream));
-        GSR_CUDA(cudaMemcpyAsync(slot.camDevice.p, slot.camHost, sizeof(DevCameraArgs), cudaMemcpyHostToDevice, stream));
-        GSR_CUDA(launchFrameBegin(ctl, scene.count, l.capacity, ranges.as<uint32_t>(), tileCount * 2, sortPlan,
-                                  forceTimeout, stream));
+        GSR_CUDA(cudaMemcpyAsync(slot.camDevice.p, slot.camHost, sizeof(DevCameraArgs) * viewCount,
+                                 cudaMemcpyHostToDevice, stream));
+        GSR_CUDA(launchFrameBegin(ctl, scene.count * viewCount, l.capacity, ranges.as<uint32_t>(), tileCount * 2,
+                                  sortPlan, forceTimeout, stream));
         FrontArgs fa{};
         fa.cam = slot.camDevice.as<DevCameraArgs>();
+        fa.views = viewsDevice.as<DevView>();
+        fa.viewCount = viewCount;
+        fa.totalTiles = tileCount;
         fa.scene.b0 = static_cast<const uint4*>(scene.buffers[0]);
         fa.scene.b1 = static_cast<const uint4*>(scene.layout == GSR_LAYOUT_AOS ? scene.buffers[0] : scene.buffers[1]);
         fa.scene.b2 = static_cast<const uint4*>(scene.buffers[2]);
@@ -437,8 +521,6 @@ struct GsrRenderer {
         fa.evalDegree = evalDegree;
         fa.bounds = settings.bounds;
         fa.binSize = int(settings.tile_size);
-        fa.gridX = int(tilesX);
-        fa.gridY = int(tilesY);
         fa.capacity = l.capacity;
         fa.splats = splats.p;
         fa.tileCounts = tileCounts.as<uint32_t>();
@@ -476,10 +558,11 @@ struct GsrRenderer {
         ra.ranges = ranges.as<uint32_t>();
         ra.image = image.as<float4>();
         ra.rgb8 = rgb8.as<uint8_t>();
-        ra.width = width;
-        ra.height = height;
-        ra.tilesX = tilesX;
-        ra.tilesY = tilesY;
+        ra.views = viewsDevice.as<DevView>();
+        ra.viewCount = viewCount;
+        ra.totalTiles = tileCount;
+        ra.persistent = settings.raster_schedule == GSR_RASTER_PERSISTENT ||
+                        (settings.raster_schedule == GSR_RASTER_AUTO && viewCount > 1);
         ra.count = scene.count;
         ra.ctl = ctl;
         ra.plan = sortPlan;
@@ -754,13 +837,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     r->evalDegree = std::min(scene->sh_degree, r->settings.max_sh_degree);
     rc = deviceTables(&r->logf);
     if (rc) return rc;
-    const uint32_t n = scene->count;
-    GSR_CUDA(r->splats.alloc(size_t(n) * 48));
-    GSR_CUDA(cudaMemset(r->splats.p, 0, r->splats.bytes));
-    GSR_CUDA(r->tileCounts.alloc(size_t(n) * 4));
-    GSR_CUDA(r->offsets.alloc(size_t(n) * 4));
-    GSR_CUDA(r->scanStatus.alloc(size_t((n + 255) / 256) * 8));
-    GSR_CUDA(cudaMemset(r->scanStatus.p, 0, r->scanStatus.bytes));
+    if (settings->raster_schedule > GSR_RASTER_PERSISTENT)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "raster schedule %u", settings->raster_schedule);
     GSR_CUDA(r->control.alloc(sizeof(DeviceControl)));
     GSR_CUDA(cudaMemset(r->control.p, 0, sizeof(DeviceControl)));
     GSR_CUDA(r->plan.alloc(sizeof(SortPlan)));
@@ -769,11 +847,11 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
         auto s = std::make_unique<GsrRenderer::Slot>();
         GSR_CUDA(cudaMallocHost(&s->host, sizeof(GsrControl)));
         std::memset(s->host, 0, sizeof(GsrControl));
-        GSR_CUDA(cudaMallocHost(&s->camHost, sizeof(DevCameraArgs)));
-        GSR_CUDA(s->camDevice.alloc(sizeof(DevCameraArgs)));
         GSR_CUDA(cudaEventCreateWithFlags(&s->done, cudaEventDisableTiming));
         r->slots.push_back(std::move(s));
     }
+    rc = r->ensureViews(1);
+    if (rc) return rc;
     for (auto& e : r->ev) GSR_CUDA(cudaEventCreate(&e));
     *out = r.release();
     return GSR_OK;
@@ -873,7 +951,7 @@ int gsr_read_list(GsrRenderer* r, uint32_t* keysLo, uint32_t* keysHi, uint32_t* 
     if (n && values && !plan.packed)
         GSR_CUDA(cudaMemcpy(values, r->list->values[b].p, size_t(n) * 4, cudaMemcpyDeviceToHost));
     if (rangesOut) {
-        const uint32_t words = std::min<uint32_t>(rangesWords, r->tilesX * r->tilesY * 2);
+        const uint32_t words = std::min<uint32_t>(rangesWords, r->totalTiles * 2);
         GSR_CUDA(cudaMemcpy(rangesOut, r->ranges.p, size_t(words) * 4, cudaMemcpyDeviceToHost));
     }
     return GSR_OK;
@@ -888,13 +966,43 @@ int gsr_read_splats(GsrRenderer* r, void* splatsOut, uint32_t* tileCountsOut, ui
     return GSR_OK;
 }
 
-int gsr_read_image(GsrRenderer* r, float* rgba, uint8_t* rgb) {
+int gsr_read_image(GsrRenderer* r, float* rgba, uint8_t* rgb) { return gsr_read_view_image(r, 0, rgba, rgb); }
+
+int gsr_render_views(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* stream) {
+    if (!r || !cameras) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    return r->renderViews(cameras, views, static_cast<cudaStream_t>(stream));
+}
+
+int gsr_renderer_view_layout(GsrRenderer* r, uint32_t view, GsrViewLayout* out, uint32_t* views) {
     if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (views) *views = uint32_t(r->views.size());
+    if (out) {
+        if (view >= r->views.size()) return fail(GSR_ERROR_INVALID_ARGUMENT, "view %u of %zu", view, r->views.size());
+        *out = r->views[view];
+    }
+    return GSR_OK;
+}
+
+int gsr_renderer_view_image(GsrRenderer* r, uint32_t view, const void** rgba, const void** rgb8) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (view >= r->views.size()) return fail(GSR_ERROR_INVALID_ARGUMENT, "view %u of %zu", view, r->views.size());
+    const uint64_t base = r->views[view].pixel_base;
+    if (rgba) *rgba = r->image.as<unsigned char>() + base * 16;
+    if (rgb8) *rgb8 = r->rgb8.p ? r->rgb8.as<unsigned char>() + base * 3 : nullptr;
+    return GSR_OK;
+}
+
+int gsr_read_view_image(GsrRenderer* r, uint32_t view, float* rgba, uint8_t* rgb) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (view >= r->views.size()) return fail(GSR_ERROR_INVALID_ARGUMENT, "view %u of %zu", view, r->views.size());
     GSR_CUDA(cudaDeviceSynchronize());
-    if (rgba) GSR_CUDA(cudaMemcpy(rgba, r->image.p, r->image.bytes, cudaMemcpyDeviceToHost));
+    const GsrViewLayout& v = r->views[view];
+    const size_t pixels = size_t(v.width) * v.height;
+    if (rgba)
+        GSR_CUDA(cudaMemcpy(rgba, r->image.as<unsigned char>() + v.pixel_base * 16, pixels * 16, cudaMemcpyDeviceToHost));
     if (rgb) {
         if (!r->rgb8.p) return fail(GSR_ERROR_INVALID_ARGUMENT, "rgb8 output is off");
-        GSR_CUDA(cudaMemcpy(rgb, r->rgb8.p, r->rgb8.bytes, cudaMemcpyDeviceToHost));
+        GSR_CUDA(cudaMemcpy(rgb, r->rgb8.as<unsigned char>() + v.pixel_base * 3, pixels * 3, cudaMemcpyDeviceToHost));
     }
     return GSR_OK;
 }

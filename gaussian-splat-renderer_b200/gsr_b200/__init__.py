@@ -32,6 +32,7 @@ STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error
 FORMATS = {"f32": 0, "f16": 1, "q8": 2, "cb": 3}
 LAYOUTS = {"soa": 0, "split": 1, "aos": 2}
 BOUNDS = {"rect": 0, "tight": 1, "cutoff-only": 2}
+RASTER_SCHEDULES = {"auto": 0, "per-tile": 1, "persistent": 2}
 CONTROL_TIMEOUT, CONTROL_BOUNDS, CONTROL_KEY_RANGE = 1, 2, 4
 
 SPLAT_DTYPE = np.dtype(
@@ -74,7 +75,8 @@ class CSettings(C.Structure):
     _fields_ = [
         ("bounds", C.c_uint32), ("tile_size", C.c_uint32), ("budget_mb", C.c_uint32), ("adaptive_list", C.c_uint32),
         ("adaptive_initial_entries", C.c_uint32), ("max_sh_degree", C.c_int32), ("output_format", C.c_uint32),
-        ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("reserved", C.c_uint32 * 7),
+        ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("raster_schedule", C.c_uint32),
+        ("reserved", C.c_uint32 * 6),
     ]
 
 
@@ -89,6 +91,11 @@ class SplatCamera(C.Structure):
         ("tan_half_fov_x", C.c_float), ("tan_half_fov_y", C.c_float), ("focal_x", C.c_float), ("focal_y", C.c_float),
         ("tiles_x", C.c_uint32), ("tiles_y", C.c_uint32),
     ]
+
+
+class ViewLayout(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("tiles_x", C.c_uint32), ("tiles_y", C.c_uint32),
+                ("tile_base", C.c_uint32), ("pad", C.c_uint32), ("pixel_base", C.c_uint64)]
 
 
 class Control(C.Structure):
@@ -164,6 +171,10 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_renderer_debug_force_timeout": (C.c_int, [vp, u32]),
         "gsr_renderer_kernel_launches": (C.c_int, [vp, C.POINTER(u64)]),
         "gsr_renderer_destroy": (None, [vp]),
+        "gsr_render_views": (C.c_int, [vp, C.POINTER(SplatCamera), u32, vp]),
+        "gsr_renderer_view_layout": (C.c_int, [vp, u32, C.POINTER(ViewLayout), C.POINTER(u32)]),
+        "gsr_renderer_view_image": (C.c_int, [vp, u32, C.POINTER(vp), C.POINTER(vp)]),
+        "gsr_read_view_image": (C.c_int, [vp, u32, vp, vp]),
         "gsr_scan": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_scan_static": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_sort_pairs": (C.c_int, [vp, vp, vp, u32, u32, vp]),
@@ -198,6 +209,8 @@ def to_c_camera(cam) -> CCamera:
 
 
 def splat_camera(cam) -> SplatCamera:
+    if isinstance(cam, SplatCamera):
+        return cam
     out = SplatCamera()
     check(load().gsr_splat_camera_from_viewer(C.byref(to_c_camera(cam)), C.byref(out)))
     return out
@@ -214,6 +227,7 @@ class Settings:
     rgb8: bool = False
     frames_in_flight: int = 2
     use_graph: bool = False
+    raster_schedule: str = "auto"
 
     def to_c(self) -> CSettings:
         s = CSettings()
@@ -227,6 +241,7 @@ class Settings:
         s.output_format = 1 if self.rgb8 else 0
         s.frames_in_flight = self.frames_in_flight
         s.use_graph = int(self.use_graph)
+        s.raster_schedule = RASTER_SCHEDULES[self.raster_schedule]
         return s
 
 
@@ -319,14 +334,50 @@ class Renderer:
         check(st)
         return c, idx.value
 
+    def render_views(self, cameras, stream: int = 0):
+        """One frame over several cameras (gsr_render_views); each may have its own size."""
+        cams = (SplatCamera * len(cameras))(*[splat_camera(c) for c in cameras])
+        check(load().gsr_render_views(self._h, cams, len(cameras), C.c_void_p(stream)))
+        self.width, self.height = cams[0].width, cams[0].height
+
+    def view_layouts(self) -> list:
+        n = C.c_uint32()
+        check(load().gsr_renderer_view_layout(self._h, 0, None, C.byref(n)))
+        out = []
+        for v in range(n.value):
+            L = ViewLayout()
+            check(load().gsr_renderer_view_layout(self._h, v, C.byref(L), None))
+            out.append(L)
+        return out
+
+    def read_view_image(self, view: int, rgb8: bool = False):
+        L = self.view_layouts()[view]
+        rgba = np.zeros((L.height, L.width, 4), np.float32)
+        out8 = np.zeros((L.height, L.width, 3), np.uint8) if rgb8 else None
+        check(load().gsr_read_view_image(self._h, view, rgba.ctypes.data, out8.ctypes.data if rgb8 else None))
+        return (rgba, out8) if rgb8 else rgba
+
+    def read_back_view(self, view: int):
+        """View `view`'s part of the frame's sorted list with the tile ids of the view alone, its
+        ranges rebased to that part, and the control block: comparable to a one-view frame."""
+        lo, hi, val, ranges, c = self.read_back()
+        L = self.view_layouts()[view]
+        tiles = L.tiles_x * L.tiles_y
+        sel = (hi >= L.tile_base) & (hi < L.tile_base + tiles)
+        first = int(np.argmax(sel)) if sel.any() else 0
+        r = ranges[L.tile_base:L.tile_base + tiles].astype(np.int64)
+        r = np.where(r[:, 1:2] > r[:, 0:1], r - first, 0).astype(np.uint32)
+        return lo[sel], hi[sel] - L.tile_base, val[sel], r, c
+
     def read_back(self):
-        """The sorted list (keys_lo = depth bits, keys_hi = tile id, values) and the ranges."""
+        """The sorted list (keys_lo = depth bits, keys_hi = frame tile id, values) and the ranges
+        of every frame tile."""
         c = self.read_control()
         n = c.entries
         lo = np.zeros(max(n, 1), np.uint32)
         hi = np.zeros(max(n, 1), np.uint32)
         val = np.zeros(max(n, 1), np.uint32)
-        tiles = ((self.width + 15) // 16) * ((self.height + 15) // 16)
+        tiles = sum(L.tiles_x * L.tiles_y for L in self.view_layouts())
         ranges = np.zeros(2 * tiles, np.uint32)
         check(load().gsr_read_list(self._h, lo.ctypes.data, hi.ctypes.data, val.ctypes.data, n, ranges.ctypes.data,
                                    ranges.size))

@@ -113,8 +113,16 @@ typedef struct GsrSettings {
     uint32_t output_format;            /* GsrOutputFormat */
     uint32_t frames_in_flight;         /* control readback slots (default 2) */
     uint32_t use_graph;                /* 1: launch each frame as a captured CUDA graph */
-    uint32_t reserved[7];
+    uint32_t raster_schedule;          /* GsrRasterSchedule (no reference counterpart) */
+    uint32_t reserved[6];
 } GsrSettings;
+
+/* How the rasterizer's blocks are given the frame's tiles. */
+typedef enum GsrRasterSchedule {
+    GSR_RASTER_AUTO = 0,       /* one block per tile for one view, the work queue for several */
+    GSR_RASTER_PER_TILE = 1,   /* one block per tile (the reference's dispatch of T workgroups) */
+    GSR_RASTER_PERSISTENT = 2  /* a fixed grid of blocks takes (view, tile) items from a queue */
+} GsrRasterSchedule;
 
 /* Reference defaults for this path (cli.h:28-50): tight bounds, 16-px tiles, 256 MB, adaptive. */
 void gsr_settings_default(GsrSettings* s);
@@ -200,6 +208,32 @@ int gsr_renderer_image(GsrRenderer* r, const void** rgba, const void** rgb8, uin
 /* The end-to-end call for host callers: render and copy the RGB8 (or RGBA32F when rgb8 output is
  * off) image into `host` (pinned or pageable; `bytes` must match), then synchronize `stream`. */
 int gsr_render_to_host(GsrRenderer* r, const GsrCamera* camera, void* host, uint64_t bytes, void* stream);
+
+/* ---- batched views (no reference counterpart: the reference renders one camera per frame) ---
+ * One frame renders `views` cameras of any sizes together: every per-gaussian kernel runs over
+ * (view, gaussian), the list keys carry the frame tile = the view's tile base + the tile in the
+ * view (the view in the key's high bits), ONE sort orders every view's entries, and the
+ * rasterizer walks (view, tile) items (GsrSettings.raster_schedule). Each view's image, list
+ * and ranges equal those of the same camera rendered alone, bit for bit. The control block
+ * sums over the views (gaussian_count = views * N). gsr_render is the one-view case; the
+ * single-view accessors (gsr_renderer_image, gsr_read_image) address view 0, and
+ * gsr_read_list returns frame tile ids and the ranges of every frame tile. */
+#define GSR_MAX_VIEWS 4096u
+typedef struct GsrViewLayout {
+    uint32_t width, height, tiles_x, tiles_y;
+    uint32_t tile_base;    /* first frame tile of the view */
+    uint32_t pad;
+    uint64_t pixel_base;   /* first pixel of the view in the frame's image buffers */
+} GsrViewLayout;
+/* Renders cameras[0..views) (each with its own width/height) as one frame; a new set of sizes
+ * re-creates the per-tile and image buffers (synchronizing, like gsr_renderer_resize). */
+int gsr_render_views(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* stream);
+/* The layout of the current frame's view `view`, and the number of views. */
+int gsr_renderer_view_layout(GsrRenderer* r, uint32_t view, GsrViewLayout* out, uint32_t* views);
+/* Device pointers of view `view`'s outputs (rgba float4[W*H], rgb8 uint8[W*H*3] or NULL). */
+int gsr_renderer_view_image(GsrRenderer* r, uint32_t view, const void** rgba, const void** rgb8);
+/* Synchronizes and copies view `view`'s images to the host (either pointer may be NULL). */
+int gsr_read_view_image(GsrRenderer* r, uint32_t view, float* rgba, uint8_t* rgb8);
 
 /* lastStats / collectPending (splat_tile_renderer.h:167-181): the control block of the most
  * recent frame whose readback has completed (frames_in_flight frames late, no stall).
