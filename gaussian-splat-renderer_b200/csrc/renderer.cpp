@@ -973,6 +973,21 @@ int gsr_render_views(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t vie
     return r->renderViews(cameras, views, static_cast<cudaStream_t>(stream));
 }
 
+int gsr_render_views_to_host(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* host, uint64_t bytes,
+                             void* stream) {
+    if (!r || !cameras || !host) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    int rc = gsr_render_views(r, cameras, views, stream);
+    if (rc) return rc;
+    const bool rgb = r->rgb8.p != nullptr;
+    const uint64_t need = r->totalPixels * (rgb ? 3 : 16);
+    if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, the views need %llu",
+                                   (unsigned long long)bytes, (unsigned long long)need);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    GSR_CUDA(cudaMemcpyAsync(host, rgb ? r->rgb8.p : r->image.p, need, cudaMemcpyDeviceToHost, s));
+    GSR_CUDA(cudaStreamSynchronize(s));
+    return GSR_OK;
+}
+
 int gsr_renderer_view_layout(GsrRenderer* r, uint32_t view, GsrViewLayout* out, uint32_t* views) {
     if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
     if (views) *views = uint32_t(r->views.size());

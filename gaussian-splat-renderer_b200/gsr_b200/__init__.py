@@ -175,6 +175,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_renderer_view_layout": (C.c_int, [vp, u32, C.POINTER(ViewLayout), C.POINTER(u32)]),
         "gsr_renderer_view_image": (C.c_int, [vp, u32, C.POINTER(vp), C.POINTER(vp)]),
         "gsr_read_view_image": (C.c_int, [vp, u32, vp, vp]),
+        "gsr_render_views_to_host": (C.c_int, [vp, C.POINTER(SplatCamera), u32, vp, u64, vp]),
         "gsr_scan": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_scan_static": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_sort_pairs": (C.c_int, [vp, vp, vp, u32, u32, vp]),
@@ -214,6 +215,11 @@ def splat_camera(cam) -> SplatCamera:
     out = SplatCamera()
     check(load().gsr_splat_camera_from_viewer(C.byref(to_c_camera(cam)), C.byref(out)))
     return out
+
+
+def camera_array(cameras) -> "C.Array":
+    """A ctypes SplatCamera[n] for gsr_render_views (build once, reuse per frame)."""
+    return (SplatCamera * len(cameras))(*[splat_camera(c) for c in cameras])
 
 
 @dataclass
@@ -335,10 +341,15 @@ class Renderer:
         return c, idx.value
 
     def render_views(self, cameras, stream: int = 0):
-        """One frame over several cameras (gsr_render_views); each may have its own size."""
-        cams = (SplatCamera * len(cameras))(*[splat_camera(c) for c in cameras])
-        check(load().gsr_render_views(self._h, cams, len(cameras), C.c_void_p(stream)))
+        """One frame over several cameras (gsr_render_views); each may have its own size.
+        `cameras`: a list of cameras, or a ctypes array of SplatCamera (see camera_array)."""
+        cams = cameras if isinstance(cameras, C.Array) else camera_array(cameras)
+        check(load().gsr_render_views(self._h, cams, len(cams), C.c_void_p(stream)))
         self.width, self.height = cams[0].width, cams[0].height
+
+    def render_views_to_host(self, cameras, out: np.ndarray, stream: int = 0):
+        cams = cameras if isinstance(cameras, C.Array) else camera_array(cameras)
+        check(load().gsr_render_views_to_host(self._h, cams, len(cams), out.ctypes.data, out.nbytes, C.c_void_p(stream)))
 
     def view_layouts(self) -> list:
         n = C.c_uint32()

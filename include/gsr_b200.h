@@ -234,6 +234,11 @@ int gsr_renderer_view_layout(GsrRenderer* r, uint32_t view, GsrViewLayout* out, 
 int gsr_renderer_view_image(GsrRenderer* r, uint32_t view, const void** rgba, const void** rgb8);
 /* Synchronizes and copies view `view`'s images to the host (either pointer may be NULL). */
 int gsr_read_view_image(GsrRenderer* r, uint32_t view, float* rgba, uint8_t* rgb8);
+/* The end-to-end call for batched host callers: render the views and copy every view's RGB8
+ * (or RGBA32F when rgb8 output is off) image into `host`, view after view at pixel_base
+ * (`bytes` must match), then synchronize `stream`. */
+int gsr_render_views_to_host(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* host, uint64_t bytes,
+                             void* stream);
 
 /* lastStats / collectPending (splat_tile_renderer.h:167-181): the control block of the most
  * recent frame whose readback has completed (frames_in_flight frames late, no stall).
