@@ -13,6 +13,7 @@
 #include <cuda_fp16.h>
 
 #include "kernels.cuh"
+#include "mlp.cuh"
 #include "splat_math.cuh"
 
 namespace gsr {
@@ -144,10 +145,30 @@ __device__ __forceinline__ uint32_t gaussianDegree(const SceneArgs& s, uint32_t 
     return s.variableSh == GSR_VARIABLE_SH_OFF ? 3u : (meta >> 30);
 }
 
+// What the colour of a visible gaussian needs once its geometry is done.
+struct ColourJob {
+    uint32_t meta, degree;
+    float dir[3];  // normalize(mean - camera position), glm::normalize's order
+};
+
+// The plain colour: the gaussian's SH coefficients, evaluated in the view direction.
+template <int COLOR>
+__device__ __forceinline__ void shColour(const FrontArgs& a, uint32_t i, const ColourJob& job, DevSplat& s) {
+    float sh[48];
+    loadSH<COLOR>(a.scene, i, (job.degree + 1) * (job.degree + 1), job.meta, sh);
+    float color[3];
+    evalSH(int(job.degree), sh, job.dir[0], job.dir[1], job.dir[2], color);
+    s.r = color[0];
+    s.g = color[1];
+    s.b = color[2];
+}
+
 // preprocessGaussian (splat_math.cpp:153-193) with the GPU culls of splat_preprocess.comp.
-template <int GEOM, int COLOR>
+// LEARNED: the colour of a visible gaussian is left to the caller (job), which decodes it with
+// the colour model or falls back to shColour.
+template <int GEOM, int COLOR, bool LEARNED>
 __device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, const DevCamera& cam, uint32_t i, DevSplat& s,
-                                                  TileRect& rect) {
+                                                  TileRect& rect, ColourJob& job) {
     const float4 pa = loadPosAlpha<GEOM>(a.scene, i);
     const float* v = cam.v;
     const float t[3] = {v[0] * pa.x + v[4] * pa.y + v[8] * pa.z + v[12], v[1] * pa.x + v[5] * pa.y + v[9] * pa.z + v[13],
@@ -171,29 +192,85 @@ __device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, const DevC
     s.cy = cy;
     if (rect.maxX <= rect.minX || rect.maxY <= rect.minY) return kCullOffScreen;
     const uint32_t gdeg = gaussianDegree(a.scene, meta);
-    const uint32_t degree = uint32_t(a.evalDegree) < gdeg ? uint32_t(a.evalDegree) : gdeg;
-    float sh[48];
-    loadSH<COLOR>(a.scene, i, (degree + 1) * (degree + 1), meta, sh);
+    job.meta = meta;
+    job.degree = uint32_t(a.evalDegree) < gdeg ? uint32_t(a.evalDegree) : gdeg;
     const float d0 = pa.x - cam.pos[0], d1 = pa.y - cam.pos[1], d2 = pa.z - cam.pos[2];
     const float inv = 1.0f / sqrtf(d0 * d0 + d1 * d1 + d2 * d2);  // glm::normalize
-    float color[3];
-    evalSH(int(degree), sh, d0 * inv, d1 * inv, d2 * inv, color);
+    job.dir[0] = d0 * inv;
+    job.dir[1] = d1 * inv;
+    job.dir[2] = d2 * inv;
+    if (!LEARNED) shColour<COLOR>(a, i, job, s);
     s.conicA = conic[0];
     s.conicB = conic[1];
     s.conicC = conic[2];
     s.opacity = pa.w;
-    s.r = color[0];
-    s.g = color[1];
-    s.b = color[2];
     s.radius = radius;
     return kCullVisible;
+}
+
+// The learned colour of the warp's visible gaussians (every lane calls it): the MLP decode on
+// the tensor cores for gaussians with a kept latent, the SH colour for the others.
+struct LearnedShared {
+    DecoderWeights w;
+    __nv_bfloat16 stage[kFrontThreads / 32][32][16];
+    float out4[kFrontThreads / 32][32][4];
+};
+template <int COLOR>
+__device__ __forceinline__ void learnedColour(const FrontArgs& a, LearnedShared& sl, uint32_t i, bool visible,
+                                              const ColourJob& job, DevSplat& s) {
+    bool mlp = false;
+    float feat[kMlpIn];
+#pragma unroll
+    for (int k = 0; k < kMlpIn; ++k) feat[k] = 0.0f;
+    if (visible) {
+        const uint4 q = __ldg(&a.latents[i]);
+        mlp = !latentIsFallback(q);
+        const uint32_t qw[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+        for (int k = 0; k < kMlpLatent; ++k) feat[k] = __half2float(__ushort_as_half(uint16_t(qw[k >> 1] >> (16 * (k & 1)))));
+#pragma unroll
+        for (int c = 0; c < 3; ++c) feat[kMlpLatent + c] = job.dir[c];
+    }
+    if (__any_sync(0xFFFFFFFFu, mlp)) {
+        const uint32_t warp = threadIdx.x >> 5;
+        float rgb[3];
+        mlpDecodeWarp(sl.w, feat, sl.stage[warp], sl.out4[warp], rgb);
+        if (mlp) {
+            s.r = rgb[0];
+            s.g = rgb[1];
+            s.b = rgb[2];
+        }
+    }
+    if (visible && !mlp) shColour<COLOR>(a, i, job, s);
+}
+
+// Decoded SH coefficients [N][48] (zeros past each gaussian's evaluated degree) and degrees,
+// for training the colour model from any scene format.
+template <int GEOM, int COLOR>
+__global__ void __launch_bounds__(kFrontThreads) shDecodeKernel(const __grid_constant__ SceneArgs scene, uint32_t count,
+                                                                int evalDegree, float* __restrict__ out,
+                                                                uint8_t* __restrict__ degrees) {
+    const uint32_t i = blockIdx.x * kFrontThreads + threadIdx.x;
+    if (i >= count) return;
+    float sigma[3], q[4];
+    uint32_t meta = 0;
+    loadShape<GEOM>(scene, i, sigma, q, meta);
+    const uint32_t gdeg = gaussianDegree(scene, meta);
+    const uint32_t degree = uint32_t(evalDegree) < gdeg ? uint32_t(evalDegree) : gdeg;
+    float sh[48];
+#pragma unroll
+    for (int k = 0; k < 48; ++k) sh[k] = 0.0f;
+    loadSH<COLOR>(scene, i, (degree + 1) * (degree + 1), meta, sh);
+#pragma unroll
+    for (int k = 0; k < 48; ++k) out[size_t(i) * 48 + k] = uint32_t(k) < (degree + 1) * (degree + 1) * 3 ? sh[k] : 0.0f;
+    degrees[i] = uint8_t(degree);
 }
 
 // 1) Preprocess + tight count, one thread per (view, gaussian) (splat_preprocess.comp:283-318,
 //    GSR_TILES); grid.y = view. Writes the splat record of visible gaussians and every gaussian's
 //    tile count; cull counters with one ballot per warp and one atomic per block and reason. No
 //    waits: a streaming kernel.
-template <int GEOM, int COLOR>
+template <int GEOM, int COLOR, bool LEARNED>
 __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_constant__ FrontArgs a) {
     __shared__ DevCamera sCam;  // the view's camera, read once per block from its device copy
     __shared__ uint32_t sCull[kCullReasonCount];
@@ -208,17 +285,27 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
     static_assert(sizeof(DevCamera) == sizeof(DevCameraArgs) && sizeof(DevCamera) % 4 == 0, "camera layout");
     if (tid < sizeof(DevCamera) / 4)
         reinterpret_cast<uint32_t*>(&sCam)[tid] = reinterpret_cast<const uint32_t*>(a.cam + view)[tid];
+    LearnedShared* sl = nullptr;
+    if constexpr (LEARNED) {
+        __shared__ LearnedShared sLearned;
+        static_assert(sizeof(DecoderWeights) % 4 == 0, "decoder layout");
+        for (uint32_t e = tid; e < sizeof(DecoderWeights) / 4; e += kFrontThreads)
+            reinterpret_cast<uint32_t*>(&sLearned.w)[e] = reinterpret_cast<const uint32_t*>(a.decoder)[e];
+        sl = &sLearned;
+    }
     __syncthreads();
     const uint32_t i = blockIdx.x * kFrontThreads + tid;
     const size_t rec = size_t(view) * a.count + i;
     const int gx = int(sCam.tilesX) * (16 / a.binSize), gy = int(sCam.tilesY) * (16 / a.binSize);
     uint32_t reason = kCullReasonCount;  // threads past the end
     uint32_t dmin = 0xFFFFFFFFu, dmax = 0;
+    DevSplat s;
+    TileRect rect{0, 0, 0, 0};
+    ColourJob job{};
+    if (i < a.count) reason = preprocessOne<GEOM, COLOR, LEARNED>(a, sCam, i, s, rect, job);
+    if constexpr (LEARNED) learnedColour<COLOR>(a, *sl, i, reason == kCullVisible, job, s);  // warp-collective
     if (i < a.count) {
-        DevSplat s;
-        TileRect rect{0, 0, 0, 0};
         uint32_t count = 0;
-        reason = preprocessOne<GEOM, COLOR>(a, sCam, i, s, rect);
         if (reason == kCullVisible) {
             const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
                                              s.opacity, a.logf);
@@ -384,18 +471,47 @@ cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capaci
     return cudaGetLastError();
 }
 
+namespace {
+template <int GEOM, int COLOR>
+void launchPreprocess(const FrontArgs& a, dim3 blocks, cudaStream_t s) {
+    if (a.latents) preprocessKernel<GEOM, COLOR, true><<<blocks, kFrontThreads, 0, s>>>(a);
+    else preprocessKernel<GEOM, COLOR, false><<<blocks, kFrontThreads, 0, s>>>(a);
+}
+template <int GEOM, int COLOR>
+void launchShDecodeT(const SceneArgs& scene, uint32_t count, int evalDegree, float* out, uint8_t* degrees, cudaStream_t s) {
+    shDecodeKernel<GEOM, COLOR><<<(count + kFrontThreads - 1) / kFrontThreads, kFrontThreads, 0, s>>>(scene, count, evalDegree,
+                                                                                                    out, degrees);
+}
+}  // namespace
+
+cudaError_t launchShDecode(const SceneArgs& scene, uint32_t geometry, uint32_t color, uint32_t count, int evalDegree,
+                           float* out, uint8_t* degrees, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    if (geometry == GSR_GEOMETRY_SOA_F32 && color == GSR_COLOR_SOA_F32)
+        launchShDecodeT<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32>(scene, count, evalDegree, out, degrees, s);
+    else if (geometry == GSR_GEOMETRY_RECORD_F32 && color == GSR_COLOR_RECORD_F32)
+        launchShDecodeT<GSR_GEOMETRY_RECORD_F32, GSR_COLOR_RECORD_F32>(scene, count, evalDegree, out, degrees, s);
+    else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_RECORD_F16)
+        launchShDecodeT<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16>(scene, count, evalDegree, out, degrees, s);
+    else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_Q8)
+        launchShDecodeT<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8>(scene, count, evalDegree, out, degrees, s);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
 cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s) {
     const dim3 blocks((a.count + kFrontThreads - 1) / kFrontThreads, a.viewCount);
     if (blocks.x == 0 || blocks.y == 0) return cudaSuccess;
     // 1) preprocess + count, grid (gaussian blocks, views)
     if (geometry == GSR_GEOMETRY_SOA_F32 && color == GSR_COLOR_SOA_F32)
-        preprocessKernel<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32><<<blocks, kFrontThreads, 0, s>>>(a);
+        launchPreprocess<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32>(a, blocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F32 && color == GSR_COLOR_RECORD_F32)
-        preprocessKernel<GSR_GEOMETRY_RECORD_F32, GSR_COLOR_RECORD_F32><<<blocks, kFrontThreads, 0, s>>>(a);
+        launchPreprocess<GSR_GEOMETRY_RECORD_F32, GSR_COLOR_RECORD_F32>(a, blocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_RECORD_F16)
-        preprocessKernel<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16><<<blocks, kFrontThreads, 0, s>>>(a);
+        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16>(a, blocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_Q8)
-        preprocessKernel<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8><<<blocks, kFrontThreads, 0, s>>>(a);
+        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8>(a, blocks, s);
     else
         return cudaErrorInvalidValue;
     cudaError_t e = cudaGetLastError();

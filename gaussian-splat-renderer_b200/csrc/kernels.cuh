@@ -31,6 +31,12 @@ struct DevView {
 };
 static_assert(sizeof(DevView) == 32, "DevView layout");
 
+// The learned colour stage's decoder for the tensor cores (mlp.cuh); the host needs its size and
+// the parameter count only.
+struct DecoderWeights;
+constexpr size_t kDecoderWeightsBytes = 32 * 16 * 2 + 32 * 32 * 2 + 8 * 32 * 2 + (32 + 32 + 8) * 4;
+constexpr uint32_t kColorModelParams = 5195;
+
 struct SceneArgs {
     const uint4* b0;     // soa posAlpha | geometry records | aos records
     const uint4* b1;     // soa scales   | colour records   | aos records
@@ -59,6 +65,8 @@ struct FrontArgs {
     uint64_t* keys;       // [capacity] (tile << 32 | depth bits), view-major index order
     uint32_t* values;     // [capacity]
     uint64_t* scanStatus; // [ceil(V * N / 2048)] look-back words of the scan over the counts
+    const uint4* latents;                 // learned colour: fp16 latents [N] (null: SH colour)
+    const struct DecoderWeights* decoder; // learned colour: the tensor-core decoder (mlp.cuh)
     DeviceControl* ctl;
     LogfFixups logf;
 };
@@ -124,6 +132,24 @@ cudaError_t launchLogfTable(float* out, LogfFixups t, cudaStream_t s);
 cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
                        uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s, uint32_t setupCapacity = 0,
                        uint32_t waitSite = kWaitStandaloneScan);
+// ---- the learned colour stage (k_mlp.cu; decoded SH from k_front.cu) -------------------------
+// Decoded SH coefficients [count][48] (zeros past each gaussian's evaluated degree) and degrees.
+cudaError_t launchShDecode(const SceneArgs& scene, uint32_t geometry, uint32_t color, uint32_t count, int evalDegree,
+                           float* out, uint8_t* degrees, cudaStream_t s);
+// One training step (batch pairs, a multiple of colorTrainBatchMultiple()): forward/backward
+// partial sums, then Adam; step = {step counter, scratch counter} advanced on the device.
+cudaError_t launchColorTrainStep(const float* sh, const uint8_t* degrees, uint32_t count, uint32_t dirs, uint32_t seed,
+                                 uint32_t batch, float* params, float* m, float* v, float* partials, uint32_t* step,
+                                 float lr, float* lossOut, uint32_t maxSteps, cudaStream_t s);
+uint32_t colorTrainBatchMultiple();
+// Latents of every gaussian and the packed decoder from the trained parameters.
+cudaError_t launchColorEncode(const float* sh, const float* params, uint4* latents, struct DecoderWeights* decoder,
+                              uint32_t count, cudaStream_t s);
+// Marks gaussians whose decoded colour is more than `gate` from the SH colour on their directions.
+cudaError_t launchColorGate(const float* sh, const uint8_t* degrees, uint32_t count, uint32_t dirs,
+                            const struct DecoderWeights* decoder, uint4* latents, float gate, uint32_t* fallbackCount,
+                            uint32_t* maxErrorBits, cudaStream_t s);
+
 // Device address of the static scratch of gsr_scan_static (kStaticScanScratchBytes) on the
 // current device.
 cudaError_t staticScanScratch(void** base);

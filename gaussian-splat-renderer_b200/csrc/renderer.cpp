@@ -155,7 +155,31 @@ struct DevBuf {
     T* as() const { return static_cast<T*>(p); }
 };
 
+// The kernels' view of a scene's buffers and format.
+SceneArgs sceneArgs(const GsrSceneDesc& scene) {
+    SceneArgs s{};
+    s.b0 = static_cast<const uint4*>(scene.buffers[0]);
+    s.b1 = static_cast<const uint4*>(scene.layout == GSR_LAYOUT_AOS ? scene.buffers[0] : scene.buffers[1]);
+    s.b2 = static_cast<const uint4*>(scene.buffers[2]);
+    s.shSoa = static_cast<const float*>(scene.buffers[3]);
+    s.geometryStride = scene.geometry_stride;
+    s.colorStride = scene.color_stride;
+    s.colorOffset = scene.color_offset;
+    s.storedCoeffs = scene.sh_coeffs;
+    s.variableSh = scene.variable_sh;
+    return s;
+}
+
 }  // namespace
+
+// ====================================================================================== colour model
+struct GsrColorModel {
+    uint32_t count = 0;
+    int degree = 3;
+    GsrColorModelStats stats{};
+    std::vector<float> loss;
+    DevBuf params, latents, decoder;
+};
 
 // ====================================================================================== scene
 struct GsrScene {
@@ -169,6 +193,9 @@ struct GsrRenderer {
     GsrSettings settings{};
     int evalDegree = 3;
     LogfFixups logf{};
+    // learned colour (gsr_renderer_set_color_model): null = SH colour
+    const uint4* colorLatents = nullptr;
+    const DecoderWeights* colorDecoder = nullptr;
 
     // per gaussian
     DevBuf splats, tileCounts, offsets, scanStatus;
@@ -508,15 +535,9 @@ struct GsrRenderer {
         fa.views = viewsDevice.as<DevView>();
         fa.viewCount = viewCount;
         fa.totalTiles = tileCount;
-        fa.scene.b0 = static_cast<const uint4*>(scene.buffers[0]);
-        fa.scene.b1 = static_cast<const uint4*>(scene.layout == GSR_LAYOUT_AOS ? scene.buffers[0] : scene.buffers[1]);
-        fa.scene.b2 = static_cast<const uint4*>(scene.buffers[2]);
-        fa.scene.shSoa = static_cast<const float*>(scene.buffers[3]);
-        fa.scene.geometryStride = scene.geometry_stride;
-        fa.scene.colorStride = scene.color_stride;
-        fa.scene.colorOffset = scene.color_offset;
-        fa.scene.storedCoeffs = scene.sh_coeffs;
-        fa.scene.variableSh = scene.variable_sh;
+        fa.scene = sceneArgs(scene);
+        fa.latents = colorLatents;
+        fa.decoder = colorDecoder;
         fa.count = scene.count;
         fa.evalDegree = evalDegree;
         fa.bounds = settings.bounds;
@@ -1069,6 +1090,164 @@ void gsr_renderer_destroy(GsrRenderer* r) {
     if (!r) return;
     cudaDeviceSynchronize();
     delete r;
+}
+
+// ---- the learned colour stage -------------------------------------------------------------------
+void gsr_color_model_options_default(GsrColorModelOptions* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->directions = 64;
+    o->batch = 65536;
+    o->steps = 2000;
+    o->learning_rate = 1e-3f;
+    o->seed = 1;
+    o->gate = 2.0f / 255.0f;
+    o->sh_degree = -1;
+}
+
+namespace {
+// Initial weights: uniform(-b, b) with b = sqrt(6 / fan_in) before a ReLU and sqrt(3 / fan_in)
+// otherwise, biases 0; drawn from a 64-bit LCG seeded with the options' seed.
+void initColorParams(uint32_t seed, std::vector<float>& p) {
+    p.assign(kColorModelParams, 0.0f);
+    uint64_t st = 0x9E3779B97F4A7C15ull ^ (uint64_t(seed) * 0xD1B54A32D192ED03ull);
+    auto uni = [&]() {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        return float((st >> 40) & 0xFFFFFF) / 16777216.0f * 2.0f - 1.0f;
+    };
+    struct Layer { uint32_t offset, in, out; bool relu; };
+    // encoder W1 [48][64], W2 [64][8]; decoder W1 [11][32], W2 [32][32], W3 [32][3]
+    const Layer layers[] = {{0, 48, 64, true}, {48 * 64 + 64, 64, 8, false}, {48 * 64 + 64 + 64 * 8 + 8, 11, 32, true},
+                            {48 * 64 + 64 + 64 * 8 + 8 + 11 * 32 + 32, 32, 32, true},
+                            {48 * 64 + 64 + 64 * 8 + 8 + 11 * 32 + 32 + 32 * 32 + 32, 32, 3, false}};
+    for (const Layer& L : layers) {
+        const float b = std::sqrt((L.relu ? 6.0f : 3.0f) / float(L.in));
+        for (uint32_t e = 0; e < L.in * L.out; ++e) p[L.offset + e] = b * uni();
+    }
+}
+}  // namespace
+
+int gsr_color_model_train(const GsrSceneDesc* scene, const GsrColorModelOptions* options, GsrColorModel** out) {
+    if (!scene || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    int rc = validateScene(*scene);
+    if (rc) return rc;
+    GsrColorModelOptions o;
+    gsr_color_model_options_default(&o);
+    if (options) o = *options;
+    const uint32_t mult = colorTrainBatchMultiple();
+    if (o.directions == 0 || o.directions > 4096) return fail(GSR_ERROR_INVALID_ARGUMENT, "directions %u", o.directions);
+    if (o.batch == 0 || o.batch % mult || o.batch > (1u << 24))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "batch %u (a multiple of %u, at most 2^24)", o.batch, mult);
+    if (o.steps == 0 || !(o.learning_rate > 0.0f) || !(o.gate >= 0.0f))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "steps %u, learning rate %g, gate %g", o.steps, o.learning_rate, o.gate);
+    const int degree = o.sh_degree < 0 ? scene->sh_degree : std::min(o.sh_degree, scene->sh_degree);
+    auto m = std::make_unique<GsrColorModel>();
+    const uint32_t n = scene->count;
+    m->count = n;
+    m->degree = degree;
+    const uint32_t blocks = o.batch / mult;
+    DevBuf sh, degrees, mom, vel, partials, step, lossDev, counters;
+    GSR_CUDA(sh.alloc(size_t(n) * 48 * 4));
+    GSR_CUDA(degrees.alloc(n));
+    GSR_CUDA(m->params.alloc(size_t(kColorModelParams) * 4));
+    GSR_CUDA(mom.alloc(size_t(kColorModelParams) * 4));
+    GSR_CUDA(vel.alloc(size_t(kColorModelParams) * 4));
+    GSR_CUDA(partials.alloc(size_t(blocks) * (kColorModelParams + 1) * 4));
+    GSR_CUDA(step.alloc(8));
+    GSR_CUDA(lossDev.alloc(size_t(o.steps) * 4));
+    GSR_CUDA(counters.alloc(8));
+    GSR_CUDA(m->latents.alloc(size_t(n) * 16));
+    GSR_CUDA(m->decoder.alloc(kDecoderWeightsBytes));
+    std::vector<float> p0;
+    initColorParams(o.seed, p0);
+    GSR_CUDA(cudaMemcpy(m->params.p, p0.data(), p0.size() * 4, cudaMemcpyHostToDevice));
+    GSR_CUDA(cudaMemset(mom.p, 0, mom.bytes));
+    GSR_CUDA(cudaMemset(vel.p, 0, vel.bytes));
+    GSR_CUDA(cudaMemset(step.p, 0, 8));
+    GSR_CUDA(cudaMemset(counters.p, 0, 8));
+    cudaStream_t s = nullptr;
+    GSR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&]() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (s) cudaStreamDestroy(s);
+    };
+    cudaError_t ce = cudaEventCreate(&e0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e0, s);
+    if (ce == cudaSuccess)
+        ce = launchShDecode(sceneArgs(*scene), scene->geometry, scene->color, n, degree, sh.as<float>(), degrees.as<uint8_t>(), s);
+    for (uint32_t k = 0; ce == cudaSuccess && k < o.steps; ++k)
+        ce = launchColorTrainStep(sh.as<float>(), degrees.as<uint8_t>(), n, o.directions, o.seed, o.batch,
+                                  m->params.as<float>(), mom.as<float>(), vel.as<float>(), partials.as<float>(),
+                                  step.as<uint32_t>(), o.learning_rate, lossDev.as<float>(), o.steps, s);
+    if (ce == cudaSuccess)
+        ce = launchColorEncode(sh.as<float>(), m->params.as<float>(), m->latents.as<uint4>(),
+                               m->decoder.as<DecoderWeights>(), n, s);
+    if (ce == cudaSuccess)
+        ce = launchColorGate(sh.as<float>(), degrees.as<uint8_t>(), n, o.directions, m->decoder.as<DecoderWeights>(),
+                             m->latents.as<uint4>(), o.gate, counters.as<uint32_t>(), counters.as<uint32_t>() + 1, s);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e1, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    float ms = 0.0f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    cleanup();
+    if (ce != cudaSuccess) return cudaFail(ce, "colour model training");
+    m->loss.resize(o.steps);
+    GSR_CUDA(cudaMemcpy(m->loss.data(), lossDev.p, size_t(o.steps) * 4, cudaMemcpyDeviceToHost));
+    uint32_t cnt[2];
+    GSR_CUDA(cudaMemcpy(cnt, counters.p, 8, cudaMemcpyDeviceToHost));
+    GsrColorModelStats& st = m->stats;
+    st.gaussians = n;
+    st.fallback = cnt[0];
+    std::memcpy(&st.max_error_kept, &cnt[1], 4);
+    st.steps = o.steps;
+    st.sh_degree = degree;
+    st.first_loss = m->loss.front();
+    st.final_loss = m->loss.back();
+    st.train_ms = ms;
+    *out = m.release();
+    return GSR_OK;
+}
+
+int gsr_color_model_stats(const GsrColorModel* model, GsrColorModelStats* out) {
+    if (!model || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = model->stats;
+    return GSR_OK;
+}
+
+int gsr_color_model_read(const GsrColorModel* model, uint16_t* latents, float* params, float* lossPerStep) {
+    if (!model) return fail(GSR_ERROR_INVALID_ARGUMENT, "null model");
+    GSR_CUDA(cudaDeviceSynchronize());
+    if (latents) GSR_CUDA(cudaMemcpy(latents, model->latents.p, size_t(model->count) * 16, cudaMemcpyDeviceToHost));
+    if (params) GSR_CUDA(cudaMemcpy(params, model->params.p, size_t(kColorModelParams) * 4, cudaMemcpyDeviceToHost));
+    if (lossPerStep) std::memcpy(lossPerStep, model->loss.data(), model->loss.size() * 4);
+    return GSR_OK;
+}
+
+int gsr_renderer_set_color_model(GsrRenderer* r, const GsrColorModel* model) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (model) {
+        if (model->count != r->scene.count)
+            return fail(GSR_ERROR_INVALID_ARGUMENT, "colour model of %u gaussians for a scene of %u", model->count,
+                        r->scene.count);
+        if (model->degree != r->evalDegree)
+            return fail(GSR_ERROR_INVALID_ARGUMENT, "colour model learned SH degree %d, the renderer evaluates %d",
+                        model->degree, r->evalDegree);
+    }
+    GSR_CUDA(cudaDeviceSynchronize());
+    r->colorLatents = model ? model->latents.as<uint4>() : nullptr;
+    r->colorDecoder = model ? model->decoder.as<DecoderWeights>() : nullptr;
+    ++r->layoutVersion;  // captured frames hold the old pointers
+    return GSR_OK;
+}
+
+void gsr_color_model_destroy(GsrColorModel* model) {
+    if (!model) return;
+    cudaDeviceSynchronize();
+    delete model;
 }
 
 // ---- primitives ----------------------------------------------------------------------------

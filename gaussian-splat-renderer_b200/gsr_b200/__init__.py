@@ -98,6 +98,20 @@ class ViewLayout(C.Structure):
                 ("tile_base", C.c_uint32), ("pad", C.c_uint32), ("pixel_base", C.c_uint64)]
 
 
+class ColorModelOptions(C.Structure):
+    _fields_ = [("directions", C.c_uint32), ("batch", C.c_uint32), ("steps", C.c_uint32), ("learning_rate", C.c_float),
+                ("seed", C.c_uint32), ("gate", C.c_float), ("sh_degree", C.c_int32), ("reserved", C.c_uint32 * 5)]
+
+
+class ColorModelStats(C.Structure):
+    _fields_ = [("gaussians", C.c_uint32), ("fallback", C.c_uint32), ("steps", C.c_uint32), ("sh_degree", C.c_int32),
+                ("first_loss", C.c_float), ("final_loss", C.c_float), ("max_error_kept", C.c_float),
+                ("train_ms", C.c_float), ("reserved", C.c_uint32 * 4)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
+
+
 class Control(C.Structure):
     _fields_ = [
         ("gaussian_count", C.c_uint32), ("visible", C.c_uint32), ("duplicates", C.c_uint32), ("entries", C.c_uint32),
@@ -176,6 +190,12 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_renderer_view_image": (C.c_int, [vp, u32, C.POINTER(vp), C.POINTER(vp)]),
         "gsr_read_view_image": (C.c_int, [vp, u32, vp, vp]),
         "gsr_render_views_to_host": (C.c_int, [vp, C.POINTER(SplatCamera), u32, vp, u64, vp]),
+        "gsr_color_model_options_default": (None, [C.POINTER(ColorModelOptions)]),
+        "gsr_color_model_train": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(ColorModelOptions), C.POINTER(vp)]),
+        "gsr_color_model_stats": (C.c_int, [vp, C.POINTER(ColorModelStats)]),
+        "gsr_color_model_read": (C.c_int, [vp, vp, vp, vp]),
+        "gsr_renderer_set_color_model": (C.c_int, [vp, vp]),
+        "gsr_color_model_destroy": (None, [vp]),
         "gsr_scan": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_scan_static": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_sort_pairs": (C.c_int, [vp, vp, vp, u32, u32, vp]),
@@ -285,6 +305,56 @@ class GpuScene:
             pass
 
 
+COLOR_MODEL_PARAMS = 5195
+
+
+class ColorModel:
+    """The learned colour stage (gsr_color_model_train): an 8-dim fp16 latent per gaussian and a
+    BF16 MLP decoder; gaussians beyond the gate keep their SH colour."""
+
+    def __init__(self, scene: GpuScene, steps: int = 2000, batch: int = 65536, directions: int = 64,
+                 learning_rate: float = 1e-3, seed: int = 1, gate: float = 2.0 / 255.0, sh_degree: int = -1):
+        lib = load()
+        o = ColorModelOptions()
+        lib.gsr_color_model_options_default(C.byref(o))
+        o.steps, o.batch, o.directions, o.learning_rate, o.seed, o.gate, o.sh_degree = (
+            steps, batch, directions, learning_rate, seed, gate, sh_degree)
+        self.scene = scene
+        self.count = int(scene.desc.count)
+        self.steps = steps
+        h = C.c_void_p()
+        check(lib.gsr_color_model_train(C.byref(scene.desc), C.byref(o), C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def stats(self) -> dict:
+        st = ColorModelStats()
+        check(load().gsr_color_model_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def read(self):
+        """(latents uint16 [N, 8] fp16 bits, params float32 [5195], loss per step)."""
+        lat = np.zeros((self.count, 8), np.uint16)
+        par = np.zeros(COLOR_MODEL_PARAMS, np.float32)
+        loss = np.zeros(self.steps, np.float32)
+        check(load().gsr_color_model_read(self._h, lat.ctypes.data, par.ctypes.data, loss.ctypes.data))
+        return lat, par, loss
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load().gsr_color_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Renderer:
     """gsr::SplatTileRenderer over the C ABI."""
 
@@ -339,6 +409,10 @@ class Renderer:
             return None, None
         check(st)
         return c, idx.value
+
+    def set_color_model(self, model: "ColorModel | None"):
+        check(load().gsr_renderer_set_color_model(self._h, model.handle if model is not None else None))
+        self.color_model = model  # keeps the model alive while the renderer uses it
 
     def render_views(self, cameras, stream: int = 0):
         """One frame over several cameras (gsr_render_views); each may have its own size.

@@ -33,7 +33,7 @@ NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contr
 # translation units whose floating-point results must match the reference bit for bit
 # (the rasterizer's image is held to a tolerance instead and uses FMA and the hardware exp2)
 EXACT_UNITS = {"k_front.cu", "k_encode.cu"}
-CU_UNITS = ["k_front.cu", "k_sort.cu", "k_render.cu", "k_encode.cu"]
+CU_UNITS = ["k_front.cu", "k_sort.cu", "k_render.cu", "k_encode.cu", "k_mlp.cu"]
 HOST_UNITS = ["renderer.cpp"]
 
 

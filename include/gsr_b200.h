@@ -232,6 +232,49 @@ int gsr_render_views(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t vie
 int gsr_renderer_view_layout(GsrRenderer* r, uint32_t view, GsrViewLayout* out, uint32_t* views);
 /* Device pointers of view `view`'s outputs (rgba float4[W*H], rgb8 uint8[W*H*3] or NULL). */
 int gsr_renderer_view_image(GsrRenderer* r, uint32_t view, const void** rgba, const void** rgb8);
+/* ---- the learned colour stage (no reference counterpart) ----------------------------------
+ * Each gaussian's SH coefficients (48 floats) are encoded to an 8-dim fp16 latent (16 bytes) and
+ * one small MLP decodes (latent, view direction) to RGB inside the preprocess, on the tensor
+ * cores (BF16 operands, FP32 accumulation): encoder 48 -> 64 -> 8, decoder (8 + 3) -> 32 -> 32 ->
+ * 3 with a sigmoid output. Training runs on the device with hand-written forward, backward and
+ * Adam kernels on (gaussian, direction) pairs whose targets are the plain SH colours. A
+ * gaussian whose decoded colour is more than `gate` (max over channels and its training
+ * directions) from its SH colour falls back to the SH evaluation, which stays the judge. */
+typedef struct GsrColorModel GsrColorModel;
+typedef struct GsrColorModelOptions {
+    uint32_t directions;   /* view directions per gaussian (uniform on the sphere); default 64 */
+    uint32_t batch;        /* (gaussian, direction) pairs per step, a multiple of 64; default 65536 */
+    uint32_t steps;        /* Adam steps; default 2000 */
+    float learning_rate;   /* default 1e-3 (beta1 0.9, beta2 0.999, eps 1e-8) */
+    uint32_t seed;         /* initial weights and the pair draws; default 1 */
+    float gate;            /* max channel error kept; default 2/255 */
+    int32_t sh_degree;     /* the SH colour it learns: -1 = the scene's degree */
+    uint32_t reserved[5];
+} GsrColorModelOptions;
+typedef struct GsrColorModelStats {
+    uint32_t gaussians;
+    uint32_t fallback;       /* gaussians that keep the SH colour */
+    uint32_t steps;
+    int32_t sh_degree;
+    float first_loss;        /* mean squared error per channel of the first and the last step */
+    float final_loss;
+    float max_error_kept;    /* largest max-channel error among the gaussians decoded by the MLP */
+    float train_ms;          /* device time of decode + training + encoding + gate */
+    uint32_t reserved[4];
+} GsrColorModelStats;
+void gsr_color_model_options_default(GsrColorModelOptions* options);
+/* Trains a colour model for the scene (synchronous; the scene must stay valid while it runs). */
+int gsr_color_model_train(const GsrSceneDesc* scene, const GsrColorModelOptions* options, GsrColorModel** out);
+int gsr_color_model_stats(const GsrColorModel* model, GsrColorModelStats* out);
+/* Host copies: latents (count x 8 fp16 bits; a NaN last half marks a fallback gaussian), the fp32
+ * parameters (5195 floats, encoder W1 [48][64], b1, W2 [64][8], b2, decoder W1 [11][32], b1,
+ * W2 [32][32], b2, W3 [32][3], b3) and the per-step loss. Any pointer may be NULL. */
+int gsr_color_model_read(const GsrColorModel* model, uint16_t* latents, float* params, float* loss_per_step);
+/* Makes the renderer colour visible gaussians with the model (NULL: SH colour again). The model
+ * must stay valid while the renderer uses it and must match the renderer's scene and degree. */
+int gsr_renderer_set_color_model(GsrRenderer* r, const GsrColorModel* model);
+void gsr_color_model_destroy(GsrColorModel* model);
+
 /* Synchronizes and copies view `view`'s images to the host (either pointer may be NULL). */
 int gsr_read_view_image(GsrRenderer* r, uint32_t view, float* rgba, uint8_t* rgb8);
 /* The end-to-end call for batched host callers: render the views and copy every view's RGB8
