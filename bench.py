@@ -299,11 +299,19 @@ def run_b200(args, dist: Dist):
     batched = run_batched(args, dist, G, gs, cams, first, stream, r)
     plain = {"views_per_s": round(value, 3), "e2e_views_per_s": round(e2e_value, 3),
              "ms_per_view": round(ms_max / args.steps, 4), "gpu_launches": int(launches)}
-    head = batched if batched["views_per_s"] > value else None
-    best = head or {"views_per_s": value, "e2e_views_per_s": e2e_value, "ms_per_view": ms_max / args.steps,
-                    "gpu_launches": launches, "views_per_frame": 1, "clocks": clocks.summary()}
-    form = (f"batched ({batched['views_per_frame']} views per frame, SH colour)" if head
-            else "plain (one view per frame, SH colour)")
+    # the batched + learned colour form: the colour model trained on this scene (2000 Adam steps of
+    # 65,536 (gaussian, direction) pairs, 64 directions per gaussian, seed 1, 2/255 gate)
+    learned, model_stats = None, None
+    if not args.no_mlp:
+        model = G.ColorModel(gs, steps=args.mlp_steps, batch=65536, directions=64, seed=1, gate=2.0 / 255.0)
+        model_stats = model.stats()
+        learned = run_batched(args, dist, G, gs, cams, first, stream, r, model=model)
+        model.close()
+    head = learned or batched
+    best = head
+    form = (f"batched ({head['views_per_frame']} views per frame) + learned colour (fp16 latent, BF16 MLP, "
+            f"{model_stats['fallback'] / model_stats['gaussians']:.1%} SH fallback)" if learned
+            else f"batched ({head['views_per_frame']} views per frame, SH colour)")
     line = {
         "metric": METRIC, "value": round(best["views_per_s"], 3), "unit": UNIT, "n_gpus": dist.world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(best["ms_per_view"], 4),
@@ -313,7 +321,10 @@ def run_b200(args, dist: Dist):
                    "form": form, "step": "one view", "views": "300-frame orbit r=14 h=2",
                    "l2": "inputs larger than L2 (scene 298 MB fp32), no flush",
                    "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "1 GPU"},
-        "forms": {"plain": plain, "batched": {k: v for k, v in batched.items() if k != "clocks"}},
+        "forms": {"plain": plain, "batched": {k: v for k, v in batched.items() if k != "clocks"},
+                  "batched+mlp": ({k: v for k, v in learned.items() if k != "clocks"} if learned else None)},
+        "color_model": ({k: (round(v, 6) if isinstance(v, float) else v) for k, v in model_stats.items()}
+                        if model_stats else None),
         "speedup_vs_plain": round(best["views_per_s"] / value, 4),
         "e2e": {"value": round(best["e2e_views_per_s"], 3), "unit": UNIT, "h2d_bytes_per_step": 200,
                 "d2h_bytes_per_step": int(out.nbytes)},
@@ -337,21 +348,41 @@ def run_b200(args, dist: Dist):
     gs.close()
 
 
-def run_batched(args, dist: Dist, G, gs, cams, first: int, stream, plain_renderer):
+def tune(args, G, gs, cams, first: int, model=None):
+    """views per frame and rasterizer schedule: --batch, or the autotuner's pick on 32 orbit views."""
+    if args.batch > 0:
+        return {"views_per_frame": args.batch, "raster_schedule": "auto", "table": None}
+    probe = G.camera_array([cams[(first + k) % len(cams)] for k in range(32)])
+    settings = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb)
+    return G.autotune(gs, settings, probe, depths=(1, 2, 4, 8, 16), frames=4, model=model)
+
+
+def run_batched(args, dist: Dist, G, gs, cams, first: int, stream, plain_renderer, model=None):
     """The batched form on the same scene and orbit: frames of D consecutive views; a step is
     still one view. Checks each view of one frame against the plain render of the same camera
     (PSNR of the 8-bit images; equal images give inf)."""
     import torch
 
-    d = max(1, args.batch)
+    tuned = tune(args, G, gs, cams, first, model)
+    d = tuned["views_per_frame"]
     nviews = len(cams)
     sptr = stream.cuda_stream
     frames = [G.camera_array([cams[(first + k * d + j) % nviews] for j in range(d)]) for k in range(nviews // d + 1)]
     nframes = len(frames)
-    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb))
+    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
+                                  raster_schedule=tuned["raster_schedule"]))
+    if model is not None:
+        r.set_color_model(model)
+    # warm-up: at least the requested views, then until the adaptive list keeps its capacity for
+    # three frames (its statistics arrive two frames late), so that no list re-allocation falls
+    # into the timed region
     with torch.cuda.stream(stream):
-        for k in range(max(args.warmup // d, 3)):
+        stable, last, k = 0, -1, 0
+        while k < 64 and (k * d < args.warmup or stable < 3):
             r.render_views(frames[k % nframes], sptr)
+            stream.synchronize()
+            cap = r.capacity()[0]
+            stable, last, k = (stable + 1 if cap == last else 0), cap, k + 1
     stream.synchronize()
     steps = max(1, args.steps // d)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -401,7 +432,8 @@ def run_batched(args, dist: Dist, G, gs, cams, first: int, stream, plain_rendere
            "psnr_vs_plain_db": None if math.isinf(min(psnrs)) else round(min(psnrs), 2),
            "images_identical_to_plain": bool(math.isinf(min(psnrs))),
            "entries_per_frame": ctl.entries, "sort_passes": ctl.sort_passes,
-           "packed_entries": ctl.packed_entries, "raster": "persistent (view, tile) queue",
+           "packed_entries": ctl.packed_entries, "raster": tuned["raster_schedule"], "autotune": tuned["table"],
+           "colour": "learned (MLP, SH fallback)" if model is not None else "SH",
            "clocks": clocks.summary()}
     r.close()
     return out
@@ -416,8 +448,10 @@ def main():
     ap.add_argument("--config", default="plain_1080p")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-frames", type=int, default=10)
-    ap.add_argument("--batch", type=int, default=8, help="views per frame of the batched form")
+    ap.add_argument("--batch", type=int, default=0, help="views per frame of the batched forms (0: autotuned)")
     ap.add_argument("--batch-budget-mb", type=int, default=8192)
+    ap.add_argument("--no-mlp", action="store_true", help="skip the batched + learned colour form")
+    ap.add_argument("--mlp-steps", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

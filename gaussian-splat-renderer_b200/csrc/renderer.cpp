@@ -1238,8 +1238,11 @@ int gsr_renderer_set_color_model(GsrRenderer* r, const GsrColorModel* model) {
                         model->degree, r->evalDegree);
     }
     GSR_CUDA(cudaDeviceSynchronize());
-    r->colorLatents = model ? model->latents.as<uint4>() : nullptr;
-    r->colorDecoder = model ? model->decoder.as<DecoderWeights>() : nullptr;
+    // a model whose gate kept no gaussian colours every one by SH: the plain path gives the same
+    // records without reading the latents
+    const bool use = model && model->stats.fallback < model->count;
+    r->colorLatents = use ? model->latents.as<uint4>() : nullptr;
+    r->colorDecoder = use ? model->decoder.as<DecoderWeights>() : nullptr;
     ++r->layoutVersion;  // captured frames hold the old pointers
     return GSR_OK;
 }
@@ -1248,6 +1251,71 @@ void gsr_color_model_destroy(GsrColorModel* model) {
     if (!model) return;
     cudaDeviceSynchronize();
     delete model;
+}
+
+// ---- autotuner ------------------------------------------------------------------------------
+int gsr_autotune(const GsrSceneDesc* scene, const GsrSettings* settings, const GsrColorModel* model,
+                 const GsrSplatCamera* cameras, uint32_t count, const uint32_t* depths, uint32_t depthCount,
+                 uint32_t frames, GsrTuneResult* out) {
+    if (!scene || !settings || !cameras || !depths || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    if (count == 0 || depthCount == 0 || frames == 0) return fail(GSR_ERROR_INVALID_ARGUMENT, "nothing to tune");
+    std::memset(out, 0, sizeof(*out));
+    const uint32_t schedules[2] = {GSR_RASTER_PER_TILE, GSR_RASTER_PERSISTENT};
+    cudaStream_t s = nullptr;
+    GSR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = GSR_OK;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = fail(GSR_ERROR_CUDA, "events");
+    for (uint32_t di = 0; rc == GSR_OK && di < depthCount; ++di) {
+        const uint32_t d = depths[di];
+        if (d == 0 || d > count || d > GSR_MAX_VIEWS) {
+            rc = fail(GSR_ERROR_INVALID_ARGUMENT, "views per frame %u (1..%u)", d, std::min(count, GSR_MAX_VIEWS));
+            break;
+        }
+        for (uint32_t sc : schedules) {
+            if (out->candidates >= GSR_TUNE_MAX_CANDIDATES) break;
+            GsrSettings st = *settings;
+            st.raster_schedule = sc;
+            GsrRenderer* r = nullptr;
+            rc = gsr_renderer_create(scene, &st, &r);
+            if (rc) break;
+            if (model) rc = gsr_renderer_set_color_model(r, model);
+            const uint32_t frameCount = count / d;  // whole frames of consecutive cameras
+            auto frame = [&](uint32_t k) { return r->renderViews(cameras + size_t(k % frameCount) * d, d, s); };
+            // warm-up: the layout, then frames until the adaptive list has kept its capacity for
+            // three frames (its statistics arrive frames_in_flight frames late)
+            uint32_t stable = 0, last = 0, k = 0;
+            for (; rc == GSR_OK && k < 24 && stable < 3; ++k) {
+                rc = frame(k);
+                if (rc == GSR_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(GSR_ERROR_CUDA, "warm-up");
+                const uint32_t cap = r->list ? r->list->capacity : 0;
+                stable = cap == last ? stable + 1 : 0;
+                last = cap;
+            }
+            if (rc == GSR_OK && cudaEventRecord(e0, s) != cudaSuccess) rc = fail(GSR_ERROR_CUDA, "event");
+            for (uint32_t j = 0; rc == GSR_OK && j < frames; ++j) rc = frame(k + j);
+            float ms = 0.0f;
+            if (rc == GSR_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                                 cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                rc = fail(GSR_ERROR_CUDA, "timing");
+            gsr_renderer_destroy(r);
+            if (rc) break;
+            GsrTuneCandidate& c = out->table[out->candidates++];
+            c.views_per_frame = d;
+            c.raster_schedule = sc;
+            c.ms_per_frame = ms / float(frames);
+            c.views_per_s = ms > 0.0f ? float(frames) * float(d) / (ms * 1e-3f) : 0.0f;
+            if (c.views_per_s > out->views_per_s) {
+                out->views_per_s = c.views_per_s;
+                out->views_per_frame = d;
+                out->raster_schedule = sc;
+            }
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    return rc;
 }
 
 // ---- primitives ----------------------------------------------------------------------------

@@ -112,6 +112,16 @@ class ColorModelStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
+class TuneCandidate(C.Structure):
+    _fields_ = [("views_per_frame", C.c_uint32), ("raster_schedule", C.c_uint32), ("views_per_s", C.c_float),
+                ("ms_per_frame", C.c_float)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("views_per_frame", C.c_uint32), ("raster_schedule", C.c_uint32), ("views_per_s", C.c_float),
+                ("candidates", C.c_uint32), ("table", TuneCandidate * 32)]
+
+
 class Control(C.Structure):
     _fields_ = [
         ("gaussian_count", C.c_uint32), ("visible", C.c_uint32), ("duplicates", C.c_uint32), ("entries", C.c_uint32),
@@ -196,6 +206,8 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_color_model_read": (C.c_int, [vp, vp, vp, vp]),
         "gsr_renderer_set_color_model": (C.c_int, [vp, vp]),
         "gsr_color_model_destroy": (None, [vp]),
+        "gsr_autotune": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(CSettings), vp, C.POINTER(SplatCamera), u32,
+                                   C.POINTER(u32), u32, u32, C.POINTER(TuneResult)]),
         "gsr_scan": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_scan_static": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_sort_pairs": (C.c_int, [vp, vp, vp, u32, u32, vp]),
@@ -516,6 +528,22 @@ class Renderer:
             self.close()
         except Exception:
             pass
+
+
+def autotune(scene: GpuScene, settings: Settings, cameras, depths=(1, 2, 4, 8, 16), frames: int = 4,
+             model: "ColorModel | None" = None) -> dict:
+    """gsr_autotune: the fastest (views per frame, rasterizer schedule) on these cameras."""
+    cams = cameras if isinstance(cameras, C.Array) else camera_array(cameras)
+    dep = (C.c_uint32 * len(depths))(*depths)
+    res = TuneResult()
+    check(load().gsr_autotune(C.byref(scene.desc), C.byref(settings.to_c()), model.handle if model else None, cams,
+                              len(cams), dep, len(depths), frames, C.byref(res)))
+    names = {v: k for k, v in RASTER_SCHEDULES.items()}
+    return {"views_per_frame": res.views_per_frame, "raster_schedule": names[res.raster_schedule],
+            "views_per_s": res.views_per_s,
+            "table": [{"views_per_frame": c.views_per_frame, "raster_schedule": names[c.raster_schedule],
+                       "views_per_s": round(c.views_per_s, 2), "ms_per_frame": round(c.ms_per_frame, 4)}
+                      for c in res.table[:res.candidates]]}
 
 
 def scan(in_ptr: int, index_ptr: int | None, out_ptr: int, total_ptr: int | None, count: int, mode: int, stream: int = 0):

@@ -275,6 +275,31 @@ int gsr_color_model_read(const GsrColorModel* model, uint16_t* latents, float* p
 int gsr_renderer_set_color_model(GsrRenderer* r, const GsrColorModel* model);
 void gsr_color_model_destroy(GsrColorModel* model);
 
+/* ---- autotuner (no reference counterpart) -------------------------------------------------
+ * Times each candidate (views per frame x rasterizer schedule) on the caller's cameras with a
+ * renderer of the given settings (and colour model, or NULL) and returns the fastest. Tile shape
+ * (16 x 16, the reference's) and radix digit width (8 bits) are fixed in this build and not among
+ * the knobs. Synchronous; allocates and frees its own renderers. */
+#define GSR_TUNE_MAX_CANDIDATES 32u
+typedef struct GsrTuneCandidate {
+    uint32_t views_per_frame;
+    uint32_t raster_schedule;  /* GSR_RASTER_PER_TILE or GSR_RASTER_PERSISTENT */
+    float views_per_s;         /* device time over whole frames of consecutive cameras */
+    float ms_per_frame;
+} GsrTuneCandidate;
+typedef struct GsrTuneResult {
+    uint32_t views_per_frame;  /* the fastest candidate */
+    uint32_t raster_schedule;
+    float views_per_s;
+    uint32_t candidates;       /* entries of table */
+    GsrTuneCandidate table[GSR_TUNE_MAX_CANDIDATES];
+} GsrTuneResult;
+/* depths: the candidate views per frame (each <= count); cameras[0..count) are rendered in frames
+ * of that many consecutive cameras, `frames` timed frames per candidate after 2 warm-up frames. */
+int gsr_autotune(const GsrSceneDesc* scene, const GsrSettings* settings, const GsrColorModel* model,
+                 const GsrSplatCamera* cameras, uint32_t count, const uint32_t* depths, uint32_t depth_count,
+                 uint32_t frames, GsrTuneResult* out);
+
 /* Synchronizes and copies view `view`'s images to the host (either pointer may be NULL). */
 int gsr_read_view_image(GsrRenderer* r, uint32_t view, float* rgba, uint8_t* rgb8);
 /* The end-to-end call for batched host callers: render the views and copy every view's RGB8
