@@ -295,6 +295,13 @@ def run_b200(args, dist: Dist):
     achieved = fb / (front_ms * 1e-3) / 1e9
     sb = sort_bytes(ctl)
 
+    if args.plain_only:  # profiling runs: the plain form alone
+        if dist.rank == 0:
+            print(json.dumps({"metric": METRIC, "value": round(value, 3), "unit": UNIT, "form": "plain only",
+                              "passes_ms": passes}), flush=True)
+        r.close()
+        gs.close()
+        return
     # the batched form: D consecutive views of the orbit per frame (one sort over all of them)
     batched = run_batched(args, dist, G, gs, cams, first, stream, r)
     plain = {"views_per_s": round(value, 3), "e2e_views_per_s": round(e2e_value, 3),
@@ -451,6 +458,7 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="views per frame of the batched forms (0: autotuned)")
     ap.add_argument("--batch-budget-mb", type=int, default=8192)
     ap.add_argument("--no-mlp", action="store_true", help="skip the batched + learned colour form")
+    ap.add_argument("--plain-only", action="store_true", help="the plain form only (profiling runs)")
     ap.add_argument("--mlp-steps", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:

@@ -225,21 +225,25 @@ struct PassShape {
 static_assert(kSortThreads == 256, "one digit per thread");
 static_assert(PassShape<true>::kTile == kSortTile, "the status array is sized by the smaller tile");
 
+static_assert(PassShape<true>::kSmemBytes == PassShape<false>::kSmemBytes, "one launch serves both layouts");
+
+// The blocks of a pass are persistent: each takes tiles by ticket (the tile order of the
+// look-back) until the list is done, so a pass launches a fixed grid of blocks that all stay
+// resident (blocks only ever wait on tiles already taken by running blocks).
 template <bool PAIRS>
-__global__ void __launch_bounds__(kSortThreads, 3) sortPassKernel(const __grid_constant__ SortArgs a, uint32_t p) {
+__device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, unsigned char* smem, uint32_t* sOff,
+                                              uint32_t* sScan, uint32_t& sTile) {
     using S = PassShape<PAIRS>;
     constexpr int kItems = S::kItems, kTile = S::kTile;
-    extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + kTile * 8);
     uint32_t* sWarpCnt = reinterpret_cast<uint32_t*>(smem + kTile * (PAIRS ? 12 : 8));  // [8][256]
     uint32_t* sMask = sWarpCnt + 8 * 256;                                                // [8][2][256]
-    __shared__ uint32_t sOff[256], sScan[8], sTile;
     const SortPlan* plan = a.plan;
-    if (!plan->active[p] || (plan->packed == 0) != PAIRS) return;
     DeviceControl* ctl = a.ctl;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t entries = ctl->c.entries;
+    for (;;) {
     if (tid == 0) sTile = atomicAdd(&ctl->tickets[1 + p], 1u);
 #pragma unroll
     for (int j = 0; j < 24; ++j) sWarpCnt[j * 256 + tid] = 0;
@@ -338,6 +342,18 @@ __global__ void __launch_bounds__(kSortThreads, 3) sortPassKernel(const __grid_c
             atomicOr(&ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
         }
     }
+    __syncthreads();  // the next tile reuses the shared buffers and sTile
+    }
+}
+
+// One pass in the layout the plan chose on the device (a skipped pass returns at once).
+__global__ void __launch_bounds__(kSortThreads, 3) sortPassKernel(const __grid_constant__ SortArgs a, uint32_t p) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ uint32_t sOff[256], sScan[8], sTile;
+    const SortPlan* plan = a.plan;
+    if (!plan->active[p]) return;
+    if (plan->packed) sortPassTiles<false>(a, p, smem, sOff, sScan, sTile);
+    else sortPassTiles<true>(a, p, smem, sOff, sScan, sTile);
 }
 
 // The gaussian index and the tile of sorted entry k in either layout.
@@ -460,24 +476,21 @@ uint32_t gridFor(uint32_t n, uint32_t perBlock, uint32_t cap) {
 }  // namespace
 
 cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s) {
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(sortPassKernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    static int passGrid = 0;
+    if (!passGrid) {
+        cudaError_t e = cudaFuncSetAttribute(sortPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              PassShape<false>::kSmemBytes);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(sortPassKernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 PassShape<true>::kSmemBytes);
-        if (e != cudaSuccess) return e;
-        configured = true;
+        int dev = 0, sms = 148, perSm = 3;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, sortPassKernel, kSortThreads, PassShape<false>::kSmemBytes);
+        passGrid = sms * (perSm > 0 ? perSm : 1);
     }
     sortHistKernel<<<histBlocks < 1 ? 1 : histBlocks, 256, 0, s>>>(a);
-    const uint32_t pairGrid = a.maxTiles < 1 ? 1 : a.maxTiles;
-    const uint32_t wordGrid = uint32_t((uint64_t(pairGrid) * kSortTile + PassShape<false>::kTile - 1) / PassShape<false>::kTile);
-    for (uint32_t p = 0; p < a.passesLaunched; ++p) {
-        // the entry layout is decided on the device: both run, the other one returns at once
-        if (a.frameMode) sortPassKernel<false><<<wordGrid, kSortThreads, PassShape<false>::kSmemBytes, s>>>(a, p);
-        sortPassKernel<true><<<pairGrid, kSortThreads, PassShape<true>::kSmemBytes, s>>>(a, p);
-    }
+    const uint32_t tiles = a.maxTiles < 1 ? 1 : a.maxTiles;
+    const uint32_t grid = tiles < uint32_t(passGrid) ? tiles : uint32_t(passGrid);
+    for (uint32_t p = 0; p < a.passesLaunched; ++p)
+        sortPassKernel<<<grid, kSortThreads, PassShape<false>::kSmemBytes, s>>>(a, p);
     return cudaGetLastError();
 }
 

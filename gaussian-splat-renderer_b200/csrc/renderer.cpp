@@ -510,8 +510,8 @@ struct GsrRenderer {
         forceTimeout = 0;
         slot.used = true;
         slot.frameIndex = frameIndex;
-        // frameBegin, preprocess, scan, duplicate, histogram, 2 per pass (both entry layouts), ranges, render
-        kernelLaunches += 7 + 2 * list->passes;
+        // frameBegin, preprocess, scan, duplicate, histogram, one per pass, ranges, render
+        kernelLaunches += 7 + list->passes;
         timed = timing;
         ++frameIndex;
         return GSR_OK;
