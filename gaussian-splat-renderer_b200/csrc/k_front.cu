@@ -309,7 +309,9 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
         if (reason == kCullVisible) {
             const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
                                              s.opacity, a.logf);
-            count = coverageCount(cv, a.binSize);
+            const RowGeom g = rowGeom(cv);
+            count = coverageCount(cv, g, a.binSize);
+            if (a.bounds != kBoundsRect) a.hints[rec] = coverageHint(cv, g);
             s.cullReason = kCullVisible;
             reinterpret_cast<DevSplat*>(a.splats)[rec] = s;
             dmin = dmax = __float_as_uint(s.depth);  // positive: the bits order like the values
@@ -364,8 +366,10 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
         const DevView vw = a.views[view];
         const int gx = int(vw.tilesX) * (16 / a.binSize), gy = int(vw.tilesY) * (16 / a.binSize);
         const TileRect rect = tileRect(s.cx, s.cy, s.radius, vw.tilesX, vw.tilesY);
-        const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
-                                         s.opacity, a.logf);
+        RowGeom g;
+        const float4 hint = a.bounds != kBoundsRect ? a.hints[rec] : make_float4(-2.0f, 0.0f, 0.0f, 0.0f);
+        const Coverage cv = coverageFromHint(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
+                                             hint, g);
         const uint64_t depthBits = __float_as_uint(s.depth);
         // packed: (((tile << W) | depth mod 2^W) << indexBits) | index; the tile part added per entry
         const uint64_t packedBase =
@@ -387,7 +391,7 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
         uint32_t tileMax = 0;
         for (int row = r0; row < r1 && written < count; ++row) {
             int x0, x1;
-            coverageRowSpan(cv, row, S, x0, x1);
+            coverageRowSpan(cv, g, row, S, x0, x1);
             for (int x = x0; x < x1 && written < count; ++x, ++written, ++k) {
                 const uint32_t tile = vw.tileBase + uint32_t(row) * uint32_t(gx) + uint32_t(x);
                 tileMax = tile > tileMax ? tile : tileMax;

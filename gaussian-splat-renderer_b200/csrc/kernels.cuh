@@ -60,6 +60,7 @@ struct FrontArgs {
     int binSize;          // S (16)
     uint32_t capacity;    // list entries
     void* splats;         // DevSplat[V * N]
+    float4* hints;        // [V * N] cutoff-ellipse terms of visible gaussians (coverageHint), tight/cutoff bounds
     uint32_t* tileCounts; // [V * N]
     uint32_t* offsets;    // [V * N] exclusive scan of tileCounts
     uint64_t* keys;       // [capacity] (tile << 32 | depth bits), view-major index order

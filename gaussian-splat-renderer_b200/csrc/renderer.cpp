@@ -198,7 +198,7 @@ struct GsrRenderer {
     const DecoderWeights* colorDecoder = nullptr;
 
     // per gaussian
-    DevBuf splats, tileCounts, offsets, scanStatus;
+    DevBuf splats, hints, tileCounts, offsets, scanStatus;
     // control + plan
     DevBuf control, plan;
     // list
@@ -311,6 +311,7 @@ struct GsrRenderer {
         const size_t n = size_t(scene.count) * v;
         GSR_CUDA(splats.alloc(n * 48));
         GSR_CUDA(cudaMemset(splats.p, 0, splats.bytes));
+        GSR_CUDA(hints.alloc(n * 16));
         GSR_CUDA(tileCounts.alloc(n * 4));
         GSR_CUDA(offsets.alloc(n * 4));
         GSR_CUDA(scanStatus.alloc((n + 255) / 256 * 8));
@@ -544,6 +545,7 @@ struct GsrRenderer {
         fa.binSize = int(settings.tile_size);
         fa.capacity = l.capacity;
         fa.splats = splats.p;
+        fa.hints = hints.as<float4>();
         fa.tileCounts = tileCounts.as<uint32_t>();
         fa.offsets = offsets.as<uint32_t>();
         fa.keys = l.keys[0].as<uint64_t>();

@@ -210,9 +210,13 @@ __device__ __forceinline__ Ellipse makeEllipse(float cx, float cy, float A, floa
     return e;
 }
 
-// floorDivClamped (tile_coverage.cpp:54).
+// floorDivClamped (tile_coverage.cpp:54). S is 16 or 8: dividing by a power of two is exactly
+// multiplying by its reciprocal (both give the exact quotient, or round the same exact value),
+// so the quotient is the reference's without a division sequence.
 __device__ __forceinline__ int floorDivClamped(float v, int S) {
-    return ftoi(floorf(sclamp(v, -65536.0f, 1048576.0f) / float(S)));
+    const float inv = S == 16 ? 0.0625f : (S == 8 ? 0.125f : 0.0f);
+    const float c = sclamp(v, -65536.0f, 1048576.0f);
+    return ftoi(floorf(inv != 0.0f ? c * inv : c / float(S)));
 }
 
 // rectToBins (tile_coverage.cpp:102-105).
@@ -259,8 +263,26 @@ __device__ __forceinline__ void coverageRows(const Coverage& cv, int S, int& r0,
     r1 = imax(lo, hi);
 }
 
+// The row-independent terms of ellipseRowSpan (tile_coverage.cpp:81-90), computed once per
+// ellipse with the reference's expressions: exTrue = sqrt(t C / D), eyRight0 = -B exTrue / C
+// (eyLeft0 = B exTrue / C is exactly -eyRight0: IEEE products and quotients are sign-symmetric),
+// At = A t, pad = 0.02 + 2e-3 exTrue. Only used when the ellipse is valid with t >= 0.
+struct RowGeom {
+    float exTrue, eyRight0, At, pad;
+};
+__device__ __forceinline__ RowGeom rowGeom(const Coverage& cv) {
+    RowGeom g{0.0f, 0.0f, 0.0f, 0.0f};
+    const Ellipse& e = cv.e;
+    if (!cv.useEllipse || e.t < 0.0f) return g;
+    g.exTrue = sqrtf(e.t * e.C / e.D);
+    g.eyRight0 = -e.B * g.exTrue / e.C;
+    g.At = e.A * e.t;
+    g.pad = 0.02f + 2e-3f * g.exTrue;
+    return g;
+}
+
 // coverageRowSpan (tile_coverage.cpp:124-127) with ellipseRowBounds/ellipseRowSpan (70-96).
-__device__ __forceinline__ void coverageRowSpan(const Coverage& cv, int row, int S, int& x0, int& x1) {
+__device__ __forceinline__ void coverageRowSpan(const Coverage& cv, const RowGeom& g, int row, int S, int& x0, int& x1) {
     if (!cv.useEllipse) {
         x0 = cv.bins.x0;
         x1 = imax(cv.bins.x0, cv.bins.x1);
@@ -276,15 +298,12 @@ __device__ __forceinline__ void coverageRowSpan(const Coverage& cv, int row, int
         x1 = cv.bins.x0;
         return;
     }
-    const float exTrue = sqrtf(e.t * e.C / e.D);
-    const float eyRight = sclamp(-e.B * exTrue / e.C, lo, hi);
-    const float eyLeft = sclamp(e.B * exTrue / e.C, lo, hi);
-    const float At = e.A * e.t;
-    const float xRight = (-e.B * eyRight + sqrtf(smax(0.0f, At - e.D * eyRight * eyRight))) / e.A;
-    const float xLeft = (-e.B * eyLeft - sqrtf(smax(0.0f, At - e.D * eyLeft * eyLeft))) / e.A;
-    const float pad = 0.02f + 2e-3f * exTrue;
-    const float fx0 = e.cx + xLeft - pad;
-    const float fx1 = e.cx + xRight + pad;
+    const float eyRight = sclamp(g.eyRight0, lo, hi);
+    const float eyLeft = sclamp(-g.eyRight0, lo, hi);
+    const float xRight = (-e.B * eyRight + sqrtf(smax(0.0f, g.At - e.D * eyRight * eyRight))) / e.A;
+    const float xLeft = (-e.B * eyLeft - sqrtf(smax(0.0f, g.At - e.D * eyLeft * eyLeft))) / e.A;
+    const float fx0 = e.cx + xLeft - g.pad;
+    const float fx1 = e.cx + xRight + g.pad;
     const int a = imax(cv.bins.x0, floorDivClamped(ceilf(fx0), S));
     const int c = imin(cv.bins.x1, floorDivClamped(floorf(fx1), S) + 1);
     x0 = a;
@@ -292,17 +311,60 @@ __device__ __forceinline__ void coverageRowSpan(const Coverage& cv, int row, int
 }
 
 // coverageCount (tile_coverage.cpp:129-138).
-__device__ __forceinline__ uint32_t coverageCount(const Coverage& cv, int S) {
+__device__ __forceinline__ uint32_t coverageCount(const Coverage& cv, const RowGeom& g, int S) {
     int r0, r1;
     coverageRows(cv, S, r0, r1);
     if (!cv.useEllipse) return uint32_t(imax(0, cv.bins.x1 - cv.bins.x0) * (r1 - r0));
     uint32_t n = 0;
     for (int r = r0; r < r1; ++r) {
         int x0, x1;
-        coverageRowSpan(cv, r, S, x0, x1);
+        coverageRowSpan(cv, g, r, S, x0, x1);
         n += uint32_t(x1 - x0);
     }
     return n;
+}
+
+// What the key emission needs of a visible gaussian's coverage beyond its record, kept by the
+// preprocess so that the emission does not evaluate the logarithm, the square roots and the
+// quotients of the cutoff ellipse again: (t, ex, ey, eyRight0), t = -2 for an invalid ellipse.
+// coverageFromHint rebuilds the same Coverage and RowGeom from the record and the hint.
+__device__ __forceinline__ float4 coverageHint(const Coverage& cv, const RowGeom& g) {
+    const Ellipse& e = cv.e;
+    if (!e.valid) return make_float4(-2.0f, 0.0f, 0.0f, 0.0f);
+    if (e.t < 0.0f) return make_float4(e.t, 0.0f, 0.0f, 0.0f);
+    // makeEllipse's ey = sqrt(t A / D); ex = sqrt(t C / D) = exTrue
+    return make_float4(e.t, g.exTrue, sqrtf(e.t * e.A / e.D), g.eyRight0);
+}
+
+__device__ __forceinline__ Coverage coverageFromHint(uint32_t mode, const TileRect& rect16, int S, int gx, int gy,
+                                                     float cx, float cy, float A, float B, float C, const float4& h,
+                                                     RowGeom& g) {
+    Coverage cv;
+    cv.bins = mode == kBoundsCutoff ? BinRect{0, 0, gx, gy} : rectToBins(rect16, S, gx, gy);
+    cv.useEllipse = false;
+    cv.e.valid = false;
+    cv.e.t = -1.0f;
+    g = RowGeom{0.0f, 0.0f, 0.0f, 0.0f};
+    if (mode == kBoundsRect) return cv;
+    Ellipse& e = cv.e;
+    e.cx = cx;
+    e.cy = cy;
+    e.A = A; e.B = B; e.C = C; e.D = A * C - B * B;
+    e.valid = h.x != -2.0f;
+    e.t = e.valid ? h.x : -1.0f;
+    e.exPad = 0.0f;
+    e.eyPad = 0.0f;
+    if (e.valid && e.t >= 0.0f) {
+        e.exPad = h.y + (0.02f + 2e-3f * h.y);  // makeEllipse's pads
+        e.eyPad = h.z + (0.02f + 2e-3f * h.z);
+        g.exTrue = h.y;
+        g.eyRight0 = h.w;
+        g.At = e.A * e.t;
+        g.pad = 0.02f + 2e-3f * h.y;
+    }
+    cv.useEllipse = e.valid;
+    if (!e.valid && mode == kBoundsCutoff) cv.bins = rectToBins(rect16, S, gx, gy);
+    return cv;
 }
 
 }  // namespace gsr
