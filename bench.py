@@ -148,23 +148,34 @@ class ClockSampler:
 
 # ---- algorithmic bytes of the front kernel (preprocess + scan + key emission) -------------
 def front_bytes(scene_format: str, ctl, n: int) -> float:
-    """Bytes the front kernel must move for one frame, from the frame's counts:
-    posAlpha of every gaussian, scale + rotation of those past the near/opacity culls, SH of
-    the visible ones, the visible splat records, tile counts + offsets of every gaussian, the
-    12-byte (key, value) entries, and the look-back words (8 B per 256 gaussians)."""
+    """Bytes the front (preprocess + scan + key emission) must move for one frame, from the
+    frame's counts. Preprocess: posAlpha of every gaussian, scale + rotation of those past the
+    near/opacity culls, SH of the visible ones; writes the tile counts, the 48-byte records and
+    16-byte coverage hints of the visible ones. Scan: counts in, offsets out. Emission: counts of
+    every gaussian, offset + record + hint of the visible ones, and the entries (8 B packed, 12 B
+    as key/value pairs)."""
     past_cull = n - ctl.cull_counts[1] - ctl.cull_counts[4]
     vis = ctl.cull_counts[0]
     if scene_format == "f32":
         b = 16 * n + 32 * past_cull + 192 * vis
     else:  # f16 split: G16 record 32 B (posAlpha in the first 16 B), colour 96 B
         b = 16 * n + 16 * past_cull + 96 * vis
-    b += 48 * vis + 8 * n + 12 * ctl.entries + 8 * math.ceil(n / 256)
+    b += 4 * n + 64 * vis  # preprocess writes
+    b += 8 * n  # scan
+    b += 4 * n + 68 * vis + (8 if ctl.packed_entries else 12) * ctl.entries  # emission
     return float(b)
 
 
+# DRAM bytes of the front per frame of the default workload, from one ncu capture
+# (profiles/kernels_plain_1080p.md: preprocess + scan + duplicate, read + write).
+FRONT_TRAFFIC_PLAIN_1080P = (296.7 + 61.3 + 5.0 + 89.3 + 8.4) * 1e6
+
+
 def sort_bytes(ctl) -> float:
-    """Histogram read (8 B/key) + per active pass 24 B/entry (read + write of key and value)."""
-    return float(8 * ctl.entries + 24 * ctl.entries * ctl.sort_passes)
+    """Histogram read (8 B/entry) + per active pass the read and write of every entry: 16 B for
+    packed 64-bit entries, 24 B for (key, value) pairs."""
+    per_pass = 16 if ctl.packed_entries else 24
+    return float(8 * ctl.entries + per_pass * ctl.entries * ctl.sort_passes)
 
 
 # ---- the CPU baseline ----------------------------------------------------------------------
@@ -338,7 +349,9 @@ def run_b200(args, dist: Dist):
         "gpu_launches": int(best["gpu_launches"]),
         "roofline": {"bound": "hbm", "kernel": "front (preprocess+count+scan+emit), plain form",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes": int(fb)},
+                     "traffic": (int(FRONT_TRAFFIC_PLAIN_1080P) if args.config == "plain_1080p" else None),
+                     "traffic_source": "ncu dram__bytes_read+write, one frame (profiles/kernels_plain_1080p.md)",
+                     "peak_kind": peak_kind, "algorithmic_bytes": int(fb)},
         "passes_ms": {k: round(v, 4) for k, v in passes.items()},
         "sort": {"bytes": int(sb), "ms": round(sort_ms, 4), "GB/s": round(sb / (sort_ms * 1e-3) / 1e9, 1),
                  "passes": ctl.sort_passes, "key_bits": ctl.key_bits},
