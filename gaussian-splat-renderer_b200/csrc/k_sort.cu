@@ -305,19 +305,19 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
         atomicOr(&mask[dj], 1u << lane);
         __syncwarp();
         const uint32_t peers = mask[dj];
+        const uint32_t run = wc[dj];  // the digit's running position in this warp's order
         // the previous step's masks were read by every lane before the last __syncwarp
         if (j > 0 && prevLeader) sMask[(warp * 2 + ((j & 1) ^ 1)) * 256 + prevDigit] = 0;
         const uint32_t below = peers & ltMask;
         prevDigit = dj;
         prevLeader = below == 0;
-        __syncwarp();
-        uint32_t first = 0;
-        if (below == 0) first = atomicAdd(&wc[dj], uint32_t(__popc(peers)));
-        const uint32_t pos = __shfl_sync(0xFFFFFFFFu, first, __ffs(peers) - 1) + __popc(below);
+        const uint32_t pos = run + __popc(below);
         if (itemBase + j * 32 < entries) {
             sKeys[pos] = key[j];
             if (PAIRS) sVals[pos] = val[PAIRS ? j : 0];
         }
+        __syncwarp();  // every lane has read wc[dj] before its digit's leader advances it
+        if (below == 0) wc[dj] = run + __popc(peers);
     }
 
     // 3) global offset of digit d's run
