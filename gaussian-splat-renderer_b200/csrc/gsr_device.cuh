@@ -110,10 +110,13 @@ struct KeyLayout {
     uint32_t tileBits;   // bits of the largest tile id incl. the sentinel
 };
 __device__ __forceinline__ uint32_t bitWidth32(uint32_t x) { return x ? 32u - __clz(x) : 0u; }
-__device__ __forceinline__ KeyLayout keyLayout(const DeviceControl* ctl, uint32_t tileCount, uint32_t count) {
+// binning: the list is emitted in (depth, index) order and sorted stably by tile alone, so its
+// entries carry no depth bits (W = 0): (tile << indexBits) | index, always one word.
+__device__ __forceinline__ KeyLayout keyLayout(const DeviceControl* ctl, uint32_t tileCount, uint32_t count,
+                                               bool binning = false) {
     KeyLayout l;
     const uint32_t dmin = ctl->c.depth_min_bits, dmax = ctl->c.depth_max_bits;
-    l.lowBits = dmin > dmax ? 0u : bitWidth32(dmin ^ dmax);
+    l.lowBits = binning || dmin > dmax ? 0u : bitWidth32(dmin ^ dmax);
     l.indexBits = count > 1 ? bitWidth32(count - 1) : 1u;
     l.tileBits = bitWidth32(tileCount);  // the sentinel tile id is tileCount
     l.packed = l.tileBits + l.lowBits + l.indexBits <= 64 ? 1u : 0u;

@@ -18,14 +18,19 @@ constexpr uint32_t kBoundsRect = 0, kBoundsTight = 1, kBoundsCutoff = 2;
 constexpr uint32_t kSpinLimit = 1u << 22;
 enum WaitSite : uint32_t { kWaitScan = 1, kWaitSort = 2, kWaitStandaloneScan = 3 };
 
+constexpr int kControlTickets = 32;
+constexpr uint32_t kListSortTickets = 1, kDepthSortTickets = 16;
+
 // The per-frame control block in device memory (GsrControl in gsr_b200.h) plus scratch
 // counters that only the kernels use.
 struct DeviceControl {
     GsrControl c;
-    uint32_t tickets[16];       // block tickets: [1 + p] sort pass p, [12] scans, [13] the rasterizer's tile queue
-    uint32_t histDone;          // blocks of the histogram kernel that have finished
+    // block tickets: [1 + p] list sort pass p, [12] scans, [13] the rasterizer's tile queue,
+    // [16 + p] depth sort pass p (binning mode)
+    uint32_t tickets[kControlTickets];
+    uint32_t histDone[2];       // blocks of the histogram kernels that have finished (list, depth sort)
     uint32_t forceTimeout;      // test hook: look-back waits see no predecessor for this many spins
-    uint32_t pad[14];
+    uint32_t pad[5];
 };
 
 // Layout of the static scratch of gsr_scan_static: the control block, then one look-back word

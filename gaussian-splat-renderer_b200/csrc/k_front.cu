@@ -317,6 +317,10 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
             dmin = dmax = __float_as_uint(s.depth);  // positive: the bits order like the values
         }
         a.tileCounts[rec] = count;
+        // binning mode: the record's depth word, depth bits above the record index; records that
+        // emit no tile get all-ones depth bits and sort after every real depth (positive floats)
+        if (a.binning)
+            a.depthKeys[0][rec] = (uint64_t(count ? __float_as_uint(s.depth) : 0xFFFFFFFFu) << a.recordBits) | rec;
     }
 #pragma unroll
     for (uint32_t r = 0; r < kCullReasonCount; ++r) {
@@ -345,23 +349,41 @@ __global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_c
 //    would be counted (coverageMismatch) and padded with the sentinel tile, as the reference
 //    does. The key's tile is the view's tile base + the tile in the view, so the list orders by
 //    view first and each view's entries form the single-view list.
+// BINNING (the reference's default construction, tile_duplicate.comp's binning build): one thread
+// per slot j of the records sorted by (depth, record index), emitting the record's tiles at the
+// offsets of the scan in that order; the entry carries the tile and the gaussian only, and the
+// stable sort by tile that follows leaves each tile's entries in (depth, index) order.
+template <bool BINNING>
 __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_constant__ FrontArgs a) {
     __shared__ uint32_t sTileMax, sMismatch, sAny;
     const uint32_t tid = threadIdx.x;
-    const uint32_t view = blockIdx.y;
     if (tid == 0) {
         sTileMax = 0;
         sMismatch = 0;
         sAny = 0;
     }
     __syncthreads();
-    const uint32_t i = blockIdx.x * kFrontThreads + tid;
-    const size_t rec = size_t(view) * a.count + i;
-    const uint32_t count = i < a.count ? a.tileCounts[rec] : 0u;
+    uint32_t view, i, count = 0;
+    size_t rec, slot;
+    if (BINNING) {
+        const uint32_t records = a.count * a.viewCount;
+        slot = size_t(blockIdx.x) * kFrontThreads + tid;
+        const uint64_t* sorted = a.depthKeys[a.depthPlan->sortedBuffer & 1u];
+        rec = slot < records ? uint32_t(sorted[slot] & ((1ull << a.recordBits) - 1ull)) : 0u;
+        view = uint32_t(rec / a.count);
+        i = uint32_t(rec - size_t(view) * a.count);
+        count = slot < records && view < a.viewCount ? a.tileCounts[rec] : 0u;
+    } else {
+        view = blockIdx.y;
+        i = blockIdx.x * kFrontThreads + tid;
+        rec = size_t(view) * a.count + i;
+        slot = rec;
+        count = i < a.count ? a.tileCounts[rec] : 0u;
+    }
     if (count > 0) {
         const uint32_t sentinel = a.totalTiles;
-        const KeyLayout lay = keyLayout(a.ctl, sentinel, a.count);
-        const uint32_t offset = a.offsets[rec];
+        const KeyLayout lay = keyLayout(a.ctl, sentinel, a.count, BINNING);
+        const uint32_t offset = a.offsets[slot];
         const DevSplat s = reinterpret_cast<const DevSplat*>(a.splats)[rec];
         const DevView vw = a.views[view];
         const int gx = int(vw.tilesX) * (16 / a.binSize), gy = int(vw.tilesY) * (16 / a.binSize);
@@ -419,12 +441,14 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
 // tile ranges (vkCmdFillBuffer 0), splat_tile_renderer.cpp:653-661. Block 0 resets the control
 // block and the sort histograms; every block zeroes a part of the ranges.
 __global__ void frameBeginKernel(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint4* ranges,
-                                 uint32_t rangeVec4s, SortPlan* plan, uint32_t forceTimeout) {
+                                 uint32_t rangeVec4s, SortPlan* plan, uint32_t forceTimeout, SortPlan* plan2) {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     for (uint32_t j = g; j < rangeVec4s; j += gridDim.x * blockDim.x) ranges[j] = make_uint4(0, 0, 0, 0);
     if (blockIdx.x != 0) return;
-    if (plan) {
-        uint32_t* h = &plan->hist[0][0];
+    SortPlan* plans[2] = {plan, plan2};
+    for (int k = 0; k < 2; ++k) {
+        if (!plans[k]) continue;
+        uint32_t* h = &plans[k]->hist[0][0];
         for (uint32_t j = threadIdx.x; j < kMaxSortPasses * 256; j += blockDim.x) h[j] = 0;
     }
     if (threadIdx.x == 0) {
@@ -451,8 +475,9 @@ __global__ void frameBeginKernel(DeviceControl* ctl, uint32_t count, uint32_t ca
         c.tile_max = 0;
         c.sorted_buffer = 0;
         c.capacity = capacity;
-        for (int t = 0; t < 16; ++t) ctl->tickets[t] = 0;
-        ctl->histDone = 0;
+        for (int t = 0; t < kControlTickets; ++t) ctl->tickets[t] = 0;
+        ctl->histDone[0] = 0;
+        ctl->histDone[1] = 0;
         ctl->forceTimeout = forceTimeout;
     }
 }
@@ -466,12 +491,13 @@ __global__ void logfTableKernel(float* out, LogfFixups t) {
 }  // namespace
 
 cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint32_t* ranges,
-                             uint32_t rangeWords, SortPlan* plan, uint32_t forceTimeout, cudaStream_t s) {
+                             uint32_t rangeWords, SortPlan* plan, uint32_t forceTimeout, cudaStream_t s,
+                             SortPlan* plan2) {
     const uint32_t vec4s = (rangeWords + 3) / 4;
     uint32_t blocks = (vec4s + 255) / 256;
     blocks = blocks < 1 ? 1 : (blocks > 1184 ? 1184 : blocks);
     frameBeginKernel<<<blocks, 256, 0, s>>>(ctl, count, capacity, reinterpret_cast<uint4*>(ranges), vec4s, plan,
-                                             forceTimeout);
+                                             forceTimeout, plan2);
     return cudaGetLastError();
 }
 
@@ -504,6 +530,35 @@ cudaError_t launchShDecode(const SceneArgs& scene, uint32_t geometry, uint32_t c
     return cudaGetLastError();
 }
 
+cudaError_t launchFrontBinningKeys(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s) {
+    const dim3 blocks((a.count + kFrontThreads - 1) / kFrontThreads, a.viewCount);
+    if (blocks.x == 0 || blocks.y == 0) return cudaSuccess;
+    if (geometry == GSR_GEOMETRY_SOA_F32 && color == GSR_COLOR_SOA_F32)
+        launchPreprocess<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32>(a, blocks, s);
+    else if (geometry == GSR_GEOMETRY_RECORD_F32 && color == GSR_COLOR_RECORD_F32)
+        launchPreprocess<GSR_GEOMETRY_RECORD_F32, GSR_COLOR_RECORD_F32>(a, blocks, s);
+    else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_RECORD_F16)
+        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16>(a, blocks, s);
+    else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_Q8)
+        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8>(a, blocks, s);
+    else
+        return cudaErrorInvalidValue;
+    return cudaGetLastError();
+}
+
+cudaError_t launchFrontBinningEmit(const FrontArgs& a, cudaStream_t s) {
+    const uint32_t records = a.count * a.viewCount;
+    if (records == 0) return cudaSuccess;
+    // the counts in (depth, record) order: the scan gathers them through the sorted depth words;
+    // its last block clamps the list to the capacity (tile_setup), in depth order
+    const ScanGather gather{{a.depthKeys[0], a.depthKeys[1]}, a.depthPlan, (1ull << a.recordBits) - 1ull};
+    cudaError_t e = launchScan(a.tileCounts, nullptr, a.offsets, &a.ctl->c.duplicates, records, kScanGatherSorted,
+                               a.scanStatus, a.ctl, s, a.capacity, kWaitScan, &gather);
+    if (e != cudaSuccess) return e;
+    duplicateKernel<true><<<(records + kFrontThreads - 1) / kFrontThreads, kFrontThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
 cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s) {
     const dim3 blocks((a.count + kFrontThreads - 1) / kFrontThreads, a.viewCount);
     if (blocks.x == 0 || blocks.y == 0) return cudaSuccess;
@@ -526,7 +581,7 @@ cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, c
                    a.scanStatus, a.ctl, s, a.capacity, kWaitScan);
     if (e != cudaSuccess) return e;
     // 3) key emission
-    duplicateKernel<<<blocks, kFrontThreads, 0, s>>>(a);
+    duplicateKernel<false><<<blocks, kFrontThreads, 0, s>>>(a);
     return cudaGetLastError();
 }
 

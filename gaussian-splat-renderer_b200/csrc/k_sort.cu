@@ -77,14 +77,20 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     __shared__ uint32_t sLast;
     __shared__ uint32_t sAny;
     DeviceControl* ctl = a.ctl;
-    const uint32_t entries = ctl->c.entries;
+    const uint32_t entries = a.frameMode == 2 ? a.count : ctl->c.entries;
     uint32_t lowBits, keyBits, packed = 0, indexBits = 0;
-    if (a.frameMode) {
-        const KeyLayout lay = keyLayout(ctl, a.tileCount, a.count);
+    if (a.frameMode == 1) {
+        const KeyLayout lay = keyLayout(ctl, a.tileCount, a.count, a.binning != 0);
         lowBits = lay.lowBits;
         packed = lay.packed;
         indexBits = lay.indexBits;
         keyBits = bitWidth(ctl->c.tile_max) + lowBits;
+    } else if (a.frameMode == 2) {  // binning mode's depth keys: W depth bits + the sentinel bit
+        const uint32_t dmin = ctl->c.depth_min_bits, dmax = ctl->c.depth_max_bits;
+        lowBits = 0;
+        packed = 1;
+        indexBits = a.indexBits;
+        keyBits = (dmin > dmax ? 0u : bitWidth(dmin ^ dmax)) + 1u;
     } else {
         lowBits = a.fixedLowBits;
         keyBits = a.fixedKeyBits;
@@ -122,7 +128,7 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) sLast = atomicAdd(&ctl->histDone, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) sLast = atomicAdd(&ctl->histDone[a.frameMode == 2 ? 1 : 0], 1u) == gridDim.x - 1;
     __syncthreads();
     if (!sLast) return;
     __threadfence();
@@ -152,6 +158,8 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
         plan->keyBits = keyBits;
         plan->packed = packed;
         plan->indexBits = indexBits;
+        plan->sortedBuffer = activeCount & 1u;
+        if (a.frameMode == 2) return;  // the list's own plan fills the control block
         ctl->c.packed_entries = packed;
         ctl->c.index_bits = indexBits;
         ctl->c.sort_passes = activeCount;
@@ -242,9 +250,10 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
     const SortPlan* plan = a.plan;
     DeviceControl* ctl = a.ctl;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint32_t entries = ctl->c.entries;
+    const uint32_t entries = a.frameMode == 2 ? a.count : ctl->c.entries;
+    const uint32_t ticket = (a.frameMode == 2 ? kDepthSortTickets : kListSortTickets) + p;
     for (;;) {
-    if (tid == 0) sTile = atomicAdd(&ctl->tickets[1 + p], 1u);
+    if (tid == 0) sTile = atomicAdd(&ctl->tickets[ticket], 1u);
 #pragma unroll
     for (int j = 0; j < 24; ++j) sWarpCnt[j * 256 + tid] = 0;
     __syncthreads();
@@ -398,8 +407,10 @@ constexpr int kScanItems = 8;
 __global__ void __launch_bounds__(256) scanKernel(const uint32_t* __restrict__ in, const uint32_t* __restrict__ index,
                                                   uint32_t* __restrict__ out, uint32_t* total, uint32_t count,
                                                   uint32_t mode, uint64_t* status, DeviceControl* ctl,
-                                                  uint32_t setupCapacity, uint32_t waitSite) {
+                                                  uint32_t setupCapacity, uint32_t waitSite,
+                                                  const __grid_constant__ ScanGather gather) {
     __shared__ uint32_t sBlock, sWarp[8], sExclusive;
+    const uint64_t* words = mode == kScanGatherSorted ? gather.words[gather.plan->sortedBuffer & 1u] : nullptr;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) sBlock = atomicAdd(&ctl->tickets[12], 1u);
     __syncthreads();
@@ -412,6 +423,7 @@ __global__ void __launch_bounds__(256) scanKernel(const uint32_t* __restrict__ i
         uint32_t x = 0;
         if (idx < count) {
             if (mode == GSR_SCAN_GATHER) x = in[index[idx]];
+            else if (mode == kScanGatherSorted) x = in[uint32_t(words[idx] & gather.mask)];
             else x = in[idx];
             if (mode == GSR_SCAN_NONZERO) x = x != 0;
         }
@@ -501,13 +513,14 @@ cudaError_t launchRanges(const RenderArgs& a, uint32_t capacity, cudaStream_t s)
 
 cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
                        uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s, uint32_t setupCapacity,
-                       uint32_t waitSite) {
+                       uint32_t waitSite, const ScanGather* gather) {
     const uint32_t blocks = (count + 256 * kScanItems - 1) / (256 * kScanItems);
     if (blocks == 0) {
         if (total) return cudaMemsetAsync(total, 0, 4, s);
         return cudaSuccess;
     }
-    scanKernel<<<blocks, 256, 0, s>>>(in, index, out, total, count, mode, status, ctl, setupCapacity, waitSite);
+    const ScanGather g = gather ? *gather : ScanGather{{nullptr, nullptr}, nullptr, 0};
+    scanKernel<<<blocks, 256, 0, s>>>(in, index, out, total, count, mode, status, ctl, setupCapacity, waitSite, g);
     return cudaGetLastError();
 }
 

@@ -66,6 +66,12 @@ struct FrontArgs {
     uint64_t* keys;       // [capacity] (tile << 32 | depth bits), view-major index order
     uint32_t* values;     // [capacity]
     uint64_t* scanStatus; // [ceil(V * N / 2048)] look-back words of the scan over the counts
+    // binning mode (the reference's default list construction): the records ordered by
+    // (depth, record index), a packed word per record, sorted on the device
+    uint32_t binning;
+    uint64_t* depthKeys[2];               // [V * N] (depth mod 2^W, or the no-tile sentinel) << recordBits | record
+    const struct SortPlan* depthPlan;     // its sort's plan (which buffer holds the result)
+    uint32_t recordBits;                  // bits of a record index (V * N - 1)
     const uint4* latents;                 // learned colour: fp16 latents [N] (null: SH colour)
     const struct DecoderWeights* decoder; // learned colour: the tensor-core decoder (mlp.cuh)
     DeviceControl* ctl;
@@ -87,6 +93,7 @@ struct SortPlan {
     uint32_t inBuffer[kMaxSortPasses];
     uint32_t digitBase[kMaxSortPasses][256];
     uint32_t hist[kMaxSortPasses][256];
+    uint32_t sortedBuffer;  // the buffer that holds the result (active passes mod 2)
 };
 
 struct SortArgs {
@@ -98,10 +105,14 @@ struct SortArgs {
     DeviceControl* ctl;
     uint32_t passesLaunched;
     // plan source: frameMode = 1 derives the low bits from the frame's depth range and the high
-    // bits from the largest tile id; 0 uses fixedLowBits/fixedKeyBits (standalone sort).
+    // bits from the largest tile id (binning = 1: tile-only keys, no depth bits); 2 = the depth
+    // keys of binning mode (packed, depth bits of the frame's range + the sentinel bit above a
+    // record index of indexBits); 0 uses fixedLowBits/fixedKeyBits (standalone sort).
     uint32_t frameMode;
     uint32_t fixedLowBits, fixedKeyBits;
     uint32_t tileCount, count;  // frame mode: the grid's tiles and N (for the entry layout)
+    uint32_t binning;
+    uint32_t indexBits;         // frameMode 2: bits of the record index
 };
 
 struct RenderArgs {
@@ -122,17 +133,29 @@ struct RenderArgs {
 
 // ---- launchers (return cudaGetLastError()) ---------------------------------------------------
 cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint32_t* ranges,
-                             uint32_t rangeWords, SortPlan* plan, uint32_t forceTimeout, cudaStream_t s);
+                             uint32_t rangeWords, SortPlan* plan, uint32_t forceTimeout, cudaStream_t s,
+                             SortPlan* plan2 = nullptr);
 cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s);
+// Binning mode, split around the depth sort: preprocess + the depth keys, then (after the sort of
+// the depth keys) the scan of the counts in depth order and the emission in that order.
+cudaError_t launchFrontBinningKeys(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s);
+cudaError_t launchFrontBinningEmit(const FrontArgs& a, cudaStream_t s);
 cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s);
 cudaError_t launchRanges(const RenderArgs& a, uint32_t capacity, cudaStream_t s);
 cudaError_t launchRender(const RenderArgs& a, cudaStream_t s);
 cudaError_t launchLogfTable(float* out, LogfFixups t, cudaStream_t s);
 // Exclusive scan (decoupled look-back, 2048 items per block); with setupCapacity != 0 the last
 // block also writes the frame's entries = min(total, capacity), overflow and ranges groups.
+// Gather source of the scan in binning mode: in[word & mask] for the sorted packed words.
+struct ScanGather {
+    const uint64_t* words[2];
+    const struct SortPlan* plan;  // plan->sortedBuffer picks the words
+    uint64_t mask;
+};
+constexpr uint32_t kScanGatherSorted = 8;  // internal scan mode next to GsrScanMode's
 cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
                        uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s, uint32_t setupCapacity = 0,
-                       uint32_t waitSite = kWaitStandaloneScan);
+                       uint32_t waitSite = kWaitStandaloneScan, const ScanGather* gather = nullptr);
 // ---- the learned colour stage (k_mlp.cu; decoded SH from k_front.cu) -------------------------
 // Decoded SH coefficients [count][48] (zeros past each gaussian's evaluated degree) and degrees.
 cudaError_t launchShDecode(const SceneArgs& scene, uint32_t geometry, uint32_t color, uint32_t count, int evalDegree,

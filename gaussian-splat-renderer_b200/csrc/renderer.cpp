@@ -134,6 +134,14 @@ void splatCamera(const GsrCamera& in, GsrSplatCamera& cam) {
 }
 
 // ---- device buffer RAII -------------------------------------------------------------------
+// A 48-byte ProjectedSplat record as the host reads it back (only the depth is used here).
+struct DevSplat48 {
+    float cx, cy;
+    uint32_t depthBits, cullReason;
+    float rest[8];
+};
+static_assert(sizeof(DevSplat48) == 48, "ProjectedSplat layout");
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -201,6 +209,14 @@ struct GsrRenderer {
     DevBuf splats, hints, tileCounts, offsets, scanStatus;
     // control + plan
     DevBuf control, plan;
+    // binning mode: the records' depth words (ping-pong), their sort's look-back words and plan
+    DevBuf depthKeys[2], depthStatus, depthPlan;
+    static constexpr uint32_t kDepthSortPasses = 4;  // 32 depth bits
+    bool binning() const { return settings.list_mode == GSR_LIST_BINNING; }
+    uint32_t recordBits() const {
+        const uint64_t n = uint64_t(scene.count) * std::max<size_t>(views.size(), 1);
+        return n > 1 ? bitWidth(uint32_t(n - 1)) : 1u;
+    }
     // list
     struct List {
         uint32_t capacity = 0;
@@ -274,8 +290,9 @@ struct GsrRenderer {
     }
 
     uint32_t passesFor(uint32_t tileCount) const {
-        // the largest key: tile ids < tileCount + 1 (sentinel) above up to 32 depth bits
-        const uint32_t keyBits = bitWidth(tileCount) + 32;
+        // the largest key: tile ids < tileCount + 1 (sentinel) above up to 32 depth bits (global)
+        // or alone (binning)
+        const uint32_t keyBits = bitWidth(tileCount) + (binning() ? 0u : 32u);
         return (keyBits + 7) / 8;
     }
 
@@ -296,7 +313,7 @@ struct GsrRenderer {
         l->passes = passesUpper;
         for (int b = 0; b < 2; ++b) {
             GSR_CUDA(l->keys[b].alloc(size_t(capacity) * 8));
-            GSR_CUDA(l->values[b].alloc(size_t(capacity) * 4));
+            if (!binning()) GSR_CUDA(l->values[b].alloc(size_t(capacity) * 4));  // binning entries are one word
         }
         GSR_CUDA(l->status.alloc(size_t(l->passes) * l->maxTiles * 256 * 8));
         GSR_CUDA(cudaMemset(l->status.p, 0, l->status.bytes));
@@ -312,6 +329,11 @@ struct GsrRenderer {
         GSR_CUDA(splats.alloc(n * 48));
         GSR_CUDA(cudaMemset(splats.p, 0, splats.bytes));
         GSR_CUDA(hints.alloc(n * 16));
+        if (binning()) {
+            for (auto& k : depthKeys) GSR_CUDA(k.alloc(n * 8));
+            GSR_CUDA(depthStatus.alloc(size_t(kDepthSortPasses) * ((n + kSortTile - 1) / kSortTile) * 256 * 8));
+            GSR_CUDA(cudaMemset(depthStatus.p, 0, depthStatus.bytes));
+        }
         GSR_CUDA(tileCounts.alloc(n * 4));
         GSR_CUDA(offsets.alloc(n * 4));
         GSR_CUDA(scanStatus.alloc((n + 255) / 256 * 8));
@@ -512,7 +534,9 @@ struct GsrRenderer {
         slot.used = true;
         slot.frameIndex = frameIndex;
         // frameBegin, preprocess, scan, duplicate, histogram, one per pass, ranges, render
-        kernelLaunches += 7 + list->passes;
+        // binning: frameBegin, preprocess, depth histogram + passes, scan, duplicate, list
+        // histogram + passes, ranges, render
+        kernelLaunches += binning() ? 8 + kDepthSortPasses + list->passes : 7 + list->passes;
         timed = timing;
         ++frameIndex;
         return GSR_OK;
@@ -530,7 +554,7 @@ struct GsrRenderer {
         GSR_CUDA(cudaMemcpyAsync(slot.camDevice.p, slot.camHost, sizeof(DevCameraArgs) * viewCount,
                                  cudaMemcpyHostToDevice, stream));
         GSR_CUDA(launchFrameBegin(ctl, scene.count * viewCount, l.capacity, ranges.as<uint32_t>(), tileCount * 2,
-                                  sortPlan, forceTimeout, stream));
+                                  sortPlan, forceTimeout, stream, binning() ? depthPlan.as<SortPlan>() : nullptr));
         FrontArgs fa{};
         fa.cam = slot.camDevice.as<DevCameraArgs>();
         fa.views = viewsDevice.as<DevView>();
@@ -553,7 +577,30 @@ struct GsrRenderer {
         fa.scanStatus = scanStatus.as<uint64_t>();
         fa.ctl = ctl;
         fa.logf = logf;
-        GSR_CUDA(launchFront(fa, scene.geometry, scene.color, stream));
+        if (binning()) {
+            fa.binning = 1;
+            fa.depthKeys[0] = depthKeys[0].as<uint64_t>();
+            fa.depthKeys[1] = depthKeys[1].as<uint64_t>();
+            fa.depthPlan = depthPlan.as<SortPlan>();
+            fa.recordBits = recordBits();
+            GSR_CUDA(launchFrontBinningKeys(fa, scene.geometry, scene.color, stream));
+            // the records by (depth, record index): 32 depth bits above the record index
+            SortArgs sd{};
+            sd.keys[0] = fa.depthKeys[0];
+            sd.keys[1] = fa.depthKeys[1];
+            sd.status = depthStatus.as<uint64_t>();
+            sd.maxTiles = uint32_t((size_t(scene.count) * viewCount + kSortTile - 1) / kSortTile);
+            sd.plan = depthPlan.as<SortPlan>();
+            sd.ctl = ctl;
+            sd.passesLaunched = kDepthSortPasses;
+            sd.frameMode = 2;
+            sd.count = scene.count * viewCount;
+            sd.indexBits = fa.recordBits;
+            GSR_CUDA(launchSort(sd, 148 * 2, stream));
+            GSR_CUDA(launchFrontBinningEmit(fa, stream));
+        } else {
+            GSR_CUDA(launchFront(fa, scene.geometry, scene.color, stream));
+        }
         if (timing) GSR_CUDA(cudaEventRecord(ev[1], stream));
 
         SortArgs sa{};
@@ -567,6 +614,7 @@ struct GsrRenderer {
         sa.ctl = ctl;
         sa.passesLaunched = l.passes;
         sa.frameMode = 1;
+        sa.binning = binning() ? 1u : 0u;
         sa.tileCount = tileCount;
         sa.count = scene.count;
         GSR_CUDA(launchSort(sa, 148 * 4, stream));
@@ -860,12 +908,15 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     r->evalDegree = std::min(scene->sh_degree, r->settings.max_sh_degree);
     rc = deviceTables(&r->logf);
     if (rc) return rc;
+    if (settings->list_mode > GSR_LIST_BINNING) return fail(GSR_ERROR_INVALID_ARGUMENT, "list mode %u", settings->list_mode);
     if (settings->raster_schedule > GSR_RASTER_PERSISTENT)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "raster schedule %u", settings->raster_schedule);
     GSR_CUDA(r->control.alloc(sizeof(DeviceControl)));
     GSR_CUDA(cudaMemset(r->control.p, 0, sizeof(DeviceControl)));
     GSR_CUDA(r->plan.alloc(sizeof(SortPlan)));
     GSR_CUDA(cudaMemset(r->plan.p, 0, sizeof(SortPlan)));
+    GSR_CUDA(r->depthPlan.alloc(sizeof(SortPlan)));
+    GSR_CUDA(cudaMemset(r->depthPlan.p, 0, sizeof(SortPlan)));
     for (uint32_t k = 0; k < r->settings.frames_in_flight; ++k) {
         auto s = std::make_unique<GsrRenderer::Slot>();
         GSR_CUDA(cudaMallocHost(&s->host, sizeof(GsrControl)));
@@ -957,12 +1008,25 @@ int gsr_read_list(GsrRenderer* r, uint32_t* keysLo, uint32_t* keysHi, uint32_t* 
         // W are those of the frame's smallest depth (equal in every key)
         const uint32_t W = plan.lowBits, ib = plan.indexBits;
         const uint32_t lowMask = W >= 32 ? 0xFFFFFFFFu : ((1u << W) - 1u);
+        // binning entries carry no depth bits: the depth comes from the gaussian's record
+        std::vector<DevSplat48> rec;
+        if (r->binning() && keysLo) {
+            rec.resize(size_t(r->scene.count) * r->views.size());
+            GSR_CUDA(cudaMemcpy(rec.data(), r->splats.p, rec.size() * 48, cudaMemcpyDeviceToHost));
+        }
         for (uint32_t i = 0; i < n; ++i) {
             uint32_t lo, hi;
             if (plan.packed) {
                 lo = (c.depth_min_bits & ~lowMask) | (uint32_t(k[i] >> ib) & lowMask);
                 hi = uint32_t(k[i] >> (ib + W));
-                if (values) values[i] = uint32_t(k[i] & ((1ull << ib) - 1ull));
+                const uint32_t g = uint32_t(k[i] & ((1ull << ib) - 1ull));
+                if (values) values[i] = g;
+                if (!rec.empty()) {
+                    size_t view = 0;  // the view holding frame tile hi
+                    while (view + 1 < r->views.size() && r->views[view + 1].tile_base <= hi) ++view;
+                    const size_t at = view * r->scene.count + g;
+                    lo = at < rec.size() ? rec[at].depthBits : 0u;
+                }
             } else {
                 lo = uint32_t(k[i]);
                 hi = uint32_t(k[i] >> 32);

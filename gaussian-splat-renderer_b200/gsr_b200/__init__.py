@@ -33,6 +33,7 @@ FORMATS = {"f32": 0, "f16": 1, "q8": 2, "cb": 3}
 LAYOUTS = {"soa": 0, "split": 1, "aos": 2}
 BOUNDS = {"rect": 0, "tight": 1, "cutoff-only": 2}
 RASTER_SCHEDULES = {"auto": 0, "per-tile": 1, "persistent": 2}
+LIST_MODES = {"global": 0, "binning": 1}
 CONTROL_TIMEOUT, CONTROL_BOUNDS, CONTROL_KEY_RANGE = 1, 2, 4
 
 SPLAT_DTYPE = np.dtype(
@@ -76,7 +77,7 @@ class CSettings(C.Structure):
         ("bounds", C.c_uint32), ("tile_size", C.c_uint32), ("budget_mb", C.c_uint32), ("adaptive_list", C.c_uint32),
         ("adaptive_initial_entries", C.c_uint32), ("max_sh_degree", C.c_int32), ("output_format", C.c_uint32),
         ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("raster_schedule", C.c_uint32),
-        ("reserved", C.c_uint32 * 6),
+        ("list_mode", C.c_uint32), ("reserved", C.c_uint32 * 5),
     ]
 
 
@@ -266,6 +267,7 @@ class Settings:
     frames_in_flight: int = 2
     use_graph: bool = False
     raster_schedule: str = "auto"
+    list_mode: str = "global"
 
     def to_c(self) -> CSettings:
         s = CSettings()
@@ -280,6 +282,7 @@ class Settings:
         s.frames_in_flight = self.frames_in_flight
         s.use_graph = int(self.use_graph)
         s.raster_schedule = RASTER_SCHEDULES[self.raster_schedule]
+        s.list_mode = LIST_MODES[self.list_mode]
         return s
 
 

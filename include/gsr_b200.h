@@ -114,8 +114,18 @@ typedef struct GsrSettings {
     uint32_t frames_in_flight;         /* control readback slots (default 2) */
     uint32_t use_graph;                /* 1: launch each frame as a captured CUDA graph */
     uint32_t raster_schedule;          /* GsrRasterSchedule (no reference counterpart) */
-    uint32_t reserved[6];
+    uint32_t list_mode;                /* GsrListMode (TileSettings' sort mode, cli.h:28) */
+    uint32_t reserved[5];
 } GsrSettings;
+
+/* How the (tile, depth) list is built and sorted; both give the same list, entry for entry,
+ * when it fits the capacity (test_tile_raster.cpp:459-464). */
+typedef enum GsrListMode {
+    GSR_LIST_GLOBAL = 0,   /* INRIA's scheme: emission in index order, one sort of (tile, depth) keys */
+    GSR_LIST_BINNING = 1   /* the reference's default: visible splats sorted by depth, emission in
+                              that order, a stable sort by tile alone; a list over the capacity is
+                              truncated in depth order */
+} GsrListMode;
 
 /* How the rasterizer's blocks are given the frame's tiles. */
 typedef enum GsrRasterSchedule {
