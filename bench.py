@@ -147,13 +147,24 @@ class ClockSampler:
 
 
 # ---- algorithmic bytes of the front kernel (preprocess + scan + key emission) -------------
-def front_bytes(scene_format: str, ctl, n: int) -> float:
+def depth_sort_passes(ctl) -> int:
+    """Digit passes of binning mode's depth sort: the depth bits that vary over the frame plus the
+    bit that puts the splats with no tiles last, 8 bits a pass."""
+    lo, hi = ctl.depth_min_bits, ctl.depth_max_bits
+    w = (lo ^ hi).bit_length() if lo <= hi else 0
+    return (w + 1 + 7) // 8
+
+
+def front_bytes(scene_format: str, ctl, n: int, list_mode: str = "global") -> float:
     """Bytes the front (preprocess + scan + key emission) must move for one frame, from the
     frame's counts. Preprocess: posAlpha of every gaussian, scale + rotation of those past the
     near/opacity culls, SH of the visible ones; writes the tile counts, the 48-byte records and
     16-byte coverage hints of the visible ones. Scan: counts in, offsets out. Emission: counts of
     every gaussian, offset + record + hint of the visible ones, and the entries (8 B packed, 12 B
-    as key/value pairs)."""
+    as key/value pairs).
+    Binning mode adds the 8-byte depth word of every gaussian (written by the preprocess), its
+    depth sort (histogram read + a read and a write of every word per pass), and walks the sorted
+    words in the scan and the emission (8 B each, with the counts and offsets gathered)."""
     past_cull = n - ctl.cull_counts[1] - ctl.cull_counts[4]
     vis = ctl.cull_counts[0]
     if scene_format == "f32":
@@ -161,6 +172,12 @@ def front_bytes(scene_format: str, ctl, n: int) -> float:
     else:  # f16 split: G16 record 32 B (posAlpha in the first 16 B), colour 96 B
         b = 16 * n + 16 * past_cull + 96 * vis
     b += 4 * n + 64 * vis  # preprocess writes
+    if list_mode == "binning":
+        b += 8 * n  # depth words
+        b += 8 * n + 16 * n * depth_sort_passes(ctl)  # depth sort
+        b += 8 * n + 4 * n + 4 * n  # gathered scan: sorted words, counts, offsets
+        b += 8 * n + 4 * n + 4 * n + 64 * vis + 8 * ctl.entries  # emission in depth order
+        return float(b)
     b += 8 * n  # scan
     b += 4 * n + 68 * vis + (8 if ctl.packed_entries else 12) * ctl.entries  # emission
     return float(b)
@@ -168,7 +185,15 @@ def front_bytes(scene_format: str, ctl, n: int) -> float:
 
 # DRAM bytes of the front per frame of the default workload, from one ncu capture
 # (profiles/kernels_plain_1080p.md: preprocess + scan + duplicate, read + write).
-FRONT_TRAFFIC_PLAIN_1080P = (296.7 + 61.3 + 5.0 + 89.3 + 8.4) * 1e6
+FRONT_TRAFFIC_PLAIN_1080P = {
+    "global": (296.7 + 61.3 + 5.0 + 89.3 + 8.4) * 1e6,
+    # preprocess, depth histogram, 4 depth passes, gathered scan, emission in depth order
+    "binning": (296.7 + 70.7 + 10.0 + 4 * 10.0 + 14.9 + 151.5 + 29.0) * 1e6,
+}
+
+
+SORT_FORMS = {"binning": "binning: depth sort of the visible splats + stable onesweep sort by tile",
+              "global": "global: one onesweep sort of (tile, depth) keys"}
 
 
 def sort_bytes(ctl) -> float:
@@ -235,7 +260,7 @@ def run_b200(args, dist: Dist):
     dev = torch.device("cuda", dist.local_rank)
     scene, cams, fmt, layout = make_config(args.config)
     gs = G.GpuScene(scene, fmt, layout)
-    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True))
+    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, list_mode=args.list_mode))
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     first = (dist.rank * 37) % len(cams)
@@ -300,8 +325,12 @@ def run_b200(args, dist: Dist):
     ctl = r.read_control()
     capacity = r.capacity()[0]
     peak, peak_kind = load_peaks()
-    fb = front_bytes(fmt, ctl, scene.count)
-    front_ms = passes.get("reset + preprocess + scan + duplicate", float("nan"))
+    fb = front_bytes(fmt, ctl, scene.count, args.list_mode)
+    if args.list_mode == "binning":
+        front_ms = sum(passes.get(k, float("nan")) for k in
+                       ("reset + preprocess (depth keys)", "depth sort (total)", "scan + duplicate (depth order)"))
+    else:
+        front_ms = passes.get("reset + preprocess + scan + duplicate", float("nan"))
     sort_ms = passes.get("tile sort (total)", float("nan"))
     achieved = fb / (front_ms * 1e-3) / 1e9
     sb = sort_bytes(ctl)
@@ -335,7 +364,7 @@ def run_b200(args, dist: Dist):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(best["ms_per_view"], 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": args.config, "gaussians": scene.count, "resolution": f"{cams[0].width}x{cams[0].height}",
-                   "scene_format": f"{fmt}/{layout}", "bounds": "tight", "list": "adaptive", "sort": "global 64-bit onesweep",
+                   "scene_format": f"{fmt}/{layout}", "bounds": "tight", "list": "adaptive", "sort": SORT_FORMS[args.list_mode],
                    "form": form, "step": "one view", "views": "300-frame orbit r=14 h=2",
                    "l2": "inputs larger than L2 (scene 298 MB fp32), no flush",
                    "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "1 GPU"},
@@ -349,7 +378,8 @@ def run_b200(args, dist: Dist):
         "gpu_launches": int(best["gpu_launches"]),
         "roofline": {"bound": "hbm", "kernel": "front (preprocess+count+scan+emit), plain form",
                      "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": (int(FRONT_TRAFFIC_PLAIN_1080P) if args.config == "plain_1080p" else None),
+                     "traffic": (int(FRONT_TRAFFIC_PLAIN_1080P[args.list_mode])
+                                 if args.config == "plain_1080p" and FRONT_TRAFFIC_PLAIN_1080P[args.list_mode] else None),
                      "traffic_source": "ncu dram__bytes_read+write, one frame (profiles/kernels_plain_1080p.md)",
                      "peak_kind": peak_kind, "algorithmic_bytes": int(fb)},
         "passes_ms": {k: round(v, 4) for k, v in passes.items()},
@@ -373,7 +403,8 @@ def tune(args, G, gs, cams, first: int, model=None):
     if args.batch > 0:
         return {"views_per_frame": args.batch, "raster_schedule": "auto", "table": None}
     probe = G.camera_array([cams[(first + k) % len(cams)] for k in range(32)])
-    settings = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb)
+    settings = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
+                          list_mode=args.list_mode)
     return G.autotune(gs, settings, probe, depths=(1, 2, 4, 8, 16), frames=4, model=model)
 
 
@@ -390,7 +421,7 @@ def run_batched(args, dist: Dist, G, gs, cams, first: int, stream, plain_rendere
     frames = [G.camera_array([cams[(first + k * d + j) % nviews] for j in range(d)]) for k in range(nviews // d + 1)]
     nframes = len(frames)
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
-                                  raster_schedule=tuned["raster_schedule"]))
+                                  raster_schedule=tuned["raster_schedule"], list_mode=args.list_mode))
     if model is not None:
         r.set_color_model(model)
     # warm-up: at least the requested views, then until the adaptive list keeps its capacity for
@@ -473,6 +504,8 @@ def main():
     ap.add_argument("--no-mlp", action="store_true", help="skip the batched + learned colour form")
     ap.add_argument("--plain-only", action="store_true", help="the plain form only (profiling runs)")
     ap.add_argument("--mlp-steps", type=int, default=2000)
+    ap.add_argument("--list-mode", default="binning", choices=["binning", "global"],
+                    help="list construction: one (tile, depth) sort, or depth sort + emission + tile sort")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

@@ -271,10 +271,14 @@ struct GsrRenderer {
     uint32_t forceTimeout = 0;
     // timing
     bool timing = false;
-    static constexpr int kPasses = 5;
+    // events between the passes: global mode times 5 passes, binning mode 7 (its front in three)
+    static constexpr int kPasses = 7;
     cudaEvent_t ev[kPasses + 1] = {};
-    float passMs[kPasses] = {};
+    int evCount = 0;       // events recorded by the last frame (passes + 1)
     bool timed = false;
+    void mark(cudaStream_t stream) {
+        if (timing && evCount <= kPasses) cudaEventRecord(ev[evCount++], stream);
+    }
 
     cudaStream_t captureStream = nullptr;  // graphs are captured here (never the legacy stream)
 
@@ -297,8 +301,9 @@ struct GsrRenderer {
     }
 
     double bytesPerEntry() const {
-        // keys (8 B) + values (4 B), each ping-ponged, + the look-back words of the passes
-        return 24.0 + 0.5 * double(std::max<uint32_t>(passesUpper, 6));
+        // keys (8 B) + values (4 B), each ping-ponged (binning: the one-word entries alone), + the
+        // look-back words of the passes
+        return (binning() ? 16.0 : 24.0) + 0.5 * double(std::max<uint32_t>(passesUpper, 6));
     }
 
     uint32_t capacityForBytes(double bytes) const {
@@ -529,7 +534,7 @@ struct GsrRenderer {
         // orders the captured work and is not a usable event afterwards)
         GSR_CUDA(cudaEventRecord(slot.done, stream));
         GSR_CUDA(cudaEventRecord(list->lastUse, stream));
-        if (timing) GSR_CUDA(cudaEventRecord(ev[5], stream));
+        mark(stream);
         forceTimeout = 0;
         slot.used = true;
         slot.frameIndex = frameIndex;
@@ -550,7 +555,8 @@ struct GsrRenderer {
         SortPlan* sortPlan = plan.as<SortPlan>();
         const uint32_t tileCount = totalTiles;
         const uint32_t viewCount = uint32_t(views.size());
-        if (timing) GSR_CUDA(cudaEventRecord(ev[0], stream));
+        evCount = 0;
+        mark(stream);
         GSR_CUDA(cudaMemcpyAsync(slot.camDevice.p, slot.camHost, sizeof(DevCameraArgs) * viewCount,
                                  cudaMemcpyHostToDevice, stream));
         GSR_CUDA(launchFrameBegin(ctl, scene.count * viewCount, l.capacity, ranges.as<uint32_t>(), tileCount * 2,
@@ -584,6 +590,7 @@ struct GsrRenderer {
             fa.depthPlan = depthPlan.as<SortPlan>();
             fa.recordBits = recordBits();
             GSR_CUDA(launchFrontBinningKeys(fa, scene.geometry, scene.color, stream));
+            mark(stream);
             // the records by (depth, record index): 32 depth bits above the record index
             SortArgs sd{};
             sd.keys[0] = fa.depthKeys[0];
@@ -597,11 +604,12 @@ struct GsrRenderer {
             sd.count = scene.count * viewCount;
             sd.indexBits = fa.recordBits;
             GSR_CUDA(launchSort(sd, 148 * 2, stream));
+            mark(stream);
             GSR_CUDA(launchFrontBinningEmit(fa, stream));
         } else {
             GSR_CUDA(launchFront(fa, scene.geometry, scene.color, stream));
         }
-        if (timing) GSR_CUDA(cudaEventRecord(ev[1], stream));
+        mark(stream);
 
         SortArgs sa{};
         for (int b = 0; b < 2; ++b) {
@@ -618,7 +626,7 @@ struct GsrRenderer {
         sa.tileCount = tileCount;
         sa.count = scene.count;
         GSR_CUDA(launchSort(sa, 148 * 4, stream));
-        if (timing) GSR_CUDA(cudaEventRecord(ev[2], stream));
+        mark(stream);
 
         RenderArgs ra{};
         ra.splats = splats.p;
@@ -638,9 +646,9 @@ struct GsrRenderer {
         ra.ctl = ctl;
         ra.plan = sortPlan;
         GSR_CUDA(launchRanges(ra, l.capacity, stream));
-        if (timing) GSR_CUDA(cudaEventRecord(ev[3], stream));
+        mark(stream);
         GSR_CUDA(launchRender(ra, stream));
-        if (timing) GSR_CUDA(cudaEventRecord(ev[4], stream));
+        mark(stream);
 
         GSR_CUDA(cudaMemcpyAsync(slot.host, &ctl->c, sizeof(GsrControl), cudaMemcpyDeviceToHost, stream));
         return GSR_OK;
@@ -908,7 +916,7 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     r->evalDegree = std::min(scene->sh_degree, r->settings.max_sh_degree);
     rc = deviceTables(&r->logf);
     if (rc) return rc;
-    if (settings->list_mode > GSR_LIST_BINNING) return fail(GSR_ERROR_INVALID_ARGUMENT, "list mode %u", settings->list_mode);
+    if (settings->list_mode > GSR_LIST_GLOBAL) return fail(GSR_ERROR_INVALID_ARGUMENT, "list mode %u", settings->list_mode);
     if (settings->raster_schedule > GSR_RASTER_PERSISTENT)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "raster schedule %u", settings->raster_schedule);
     GSR_CUDA(r->control.alloc(sizeof(DeviceControl)));
@@ -1116,12 +1124,18 @@ int gsr_renderer_set_timing(GsrRenderer* r, int enabled) {
 }
 
 int gsr_renderer_pass_times(GsrRenderer* r, float* ms, const char** names, uint32_t capacity, uint32_t* count) {
-    static const char* kNames[GsrRenderer::kPasses] = {"reset + preprocess + scan + duplicate", "tile sort (total)",
-                                                       "tile ranges", "render tiles", "control readback"};
+    static const char* kGlobal[] = {"reset + preprocess + scan + duplicate", "tile sort (total)", "tile ranges",
+                                    "render tiles", "control readback"};
+    static const char* kBinning[] = {"reset + preprocess (depth keys)", "depth sort (total)",
+                                     "scan + duplicate (depth order)", "tile sort (total)", "tile ranges",
+                                     "render tiles", "control readback"};
     if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
-    if (!r->timed) return GSR_ERROR_NOT_READY;
-    GSR_CUDA(cudaEventSynchronize(r->ev[GsrRenderer::kPasses]));
-    const uint32_t n = std::min<uint32_t>(capacity, GsrRenderer::kPasses);
+    if (!r->timed || r->evCount < 2) return GSR_ERROR_NOT_READY;
+    const uint32_t passes = uint32_t(r->evCount - 1);
+    const char** kNames = passes == 7 ? kBinning : kGlobal;
+    if (passes != 7 && passes != 5) return fail(GSR_ERROR_UNSUPPORTED, "pass events %u", passes);
+    GSR_CUDA(cudaEventSynchronize(r->ev[passes]));
+    const uint32_t n = std::min<uint32_t>(capacity, passes);
     for (uint32_t i = 0; i < n; ++i) {
         float t = 0.0f;
         GSR_CUDA(cudaEventElapsedTime(&t, r->ev[i], r->ev[i + 1]));

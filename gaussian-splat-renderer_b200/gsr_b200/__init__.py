@@ -33,7 +33,7 @@ FORMATS = {"f32": 0, "f16": 1, "q8": 2, "cb": 3}
 LAYOUTS = {"soa": 0, "split": 1, "aos": 2}
 BOUNDS = {"rect": 0, "tight": 1, "cutoff-only": 2}
 RASTER_SCHEDULES = {"auto": 0, "per-tile": 1, "persistent": 2}
-LIST_MODES = {"global": 0, "binning": 1}
+LIST_MODES = {"binning": 0, "global": 1}
 CONTROL_TIMEOUT, CONTROL_BOUNDS, CONTROL_KEY_RANGE = 1, 2, 4
 
 SPLAT_DTYPE = np.dtype(
@@ -267,7 +267,7 @@ class Settings:
     frames_in_flight: int = 2
     use_graph: bool = False
     raster_schedule: str = "auto"
-    list_mode: str = "global"
+    list_mode: str = "binning"
 
     def to_c(self) -> CSettings:
         s = CSettings()

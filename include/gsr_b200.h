@@ -121,10 +121,11 @@ typedef struct GsrSettings {
 /* How the (tile, depth) list is built and sorted; both give the same list, entry for entry,
  * when it fits the capacity (test_tile_raster.cpp:459-464). */
 typedef enum GsrListMode {
-    GSR_LIST_GLOBAL = 0,   /* INRIA's scheme: emission in index order, one sort of (tile, depth) keys */
-    GSR_LIST_BINNING = 1   /* the reference's default: visible splats sorted by depth, emission in
-                              that order, a stable sort by tile alone; a list over the capacity is
-                              truncated in depth order */
+    GSR_LIST_BINNING = 0,  /* the default (TileSortMode::Binning, splat_tile_renderer.h:76): visible
+                              splats sorted by depth, emission in that order, a stable sort by tile
+                              alone; a list over the capacity is truncated in depth order */
+    GSR_LIST_GLOBAL = 1    /* INRIA's scheme (TileSortMode::Global): emission in index order, one sort
+                              of (tile, depth) keys; a list over the capacity is truncated in index order */
 } GsrListMode;
 
 /* How the rasterizer's blocks are given the frame's tiles. */
@@ -334,7 +335,8 @@ int gsr_read_list(GsrRenderer* r, uint32_t* keys_lo, uint32_t* keys_hi, uint32_t
 int gsr_read_splats(GsrRenderer* r, void* splats, uint32_t* tile_counts, uint32_t n);
 /* readBackImage (splat_tile_renderer.h:194): rgba float4[W*H] and/or rgb8 uint8[W*H*3]. */
 int gsr_read_image(GsrRenderer* r, float* rgba, uint8_t* rgb8);
-/* Per-pass device time of the last frame in ms (GpuProfiler scopes), when timing is on. */
+/* Per-pass device time of the last frame in ms (GpuProfiler scopes), when timing is on: 5 passes
+ * in global mode, 7 in binning mode (its front as preprocess, depth sort, scan + emission). */
 int gsr_renderer_set_timing(GsrRenderer* r, int enabled);
 int gsr_renderer_pass_times(GsrRenderer* r, float* ms, const char** names, uint32_t capacity, uint32_t* count);
 /* Capacity of the current list in entries, the budget's maximum, and list resizes so far. */

@@ -24,9 +24,9 @@ def _alone(gpu, gs, cam):
     return rgba, rgb8, lo, hi, val, ranges, ctl
 
 
-def _check_views(gpu, gs, cams, schedule, use_graph=False, frames=1):
+def _check_views(gpu, gs, cams, schedule, use_graph=False, frames=1, list_mode="binning"):
     r = gpu.Renderer(gs, gpu.Settings(budget_mb=1024, adaptive_list=False, rgb8=True, raster_schedule=schedule,
-                                      use_graph=use_graph))
+                                      use_graph=use_graph, list_mode=list_mode))
     for _ in range(frames):
         r.render_views(cams)
     ctl = r.read_control()
@@ -73,17 +73,19 @@ def test_batched_views_graph_and_repeat(gpu):
     _check_views(gpu, gs, scenes.batched_cameras(4, seed=5), "auto", use_graph=True, frames=3)
 
 
-def test_batched_views_wide_keys(gpu):
-    """Four 4K views: frame tile ids need 18 bits, so tile + depth + index bits exceed 64 and the
-    entries are (tile << 32 | depth, index) pairs; the views still equal their one-view renders."""
+@pytest.mark.parametrize("list_mode,packed", [("global", 0), ("binning", 1)])
+def test_batched_views_wide_keys(gpu, list_mode, packed):
+    """Four 4K views: frame tile ids need 18 bits, so in global mode tile + depth + index bits
+    exceed 64 and the entries are (tile << 32 | depth, index) pairs (binning entries carry no
+    depth bits and stay one word); the views still equal their one-view renders."""
     from gsr_b200 import scenes
 
     scene = _scene(gpu, 70_000, seed=13, radius=5.0)
     gs = gpu.GpuScene(scene, "f32", "soa")
     cams = [scenes.viewer_camera(tuple(e), (0.0, 0.0, 0.0), 3840, 2160) for e in
             [(0.0, 0.0, 1.5), (1.0, 1.0, 9.0), (-9.0, 0.5, 2.0), (0.0, 9.5, 0.5)]]
-    ctl = _check_views(gpu, gs, cams, "auto")
-    assert ctl.packed_entries == 0
+    ctl = _check_views(gpu, gs, cams, "auto", list_mode=list_mode)
+    assert ctl.packed_entries == packed
 
 
 def test_view_layout_and_limits(gpu):

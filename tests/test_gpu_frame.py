@@ -38,17 +38,19 @@ def case(name):
     return CASES[name]
 
 
-def render(gsr, scene, cam, bounds="tight", budget_mb=256, fmt="f32", layout="soa"):
+def render(gsr, scene, cam, bounds="tight", budget_mb=256, fmt="f32", layout="soa", list_mode="binning"):
     gs = gsr.GpuScene(scene, fmt, layout)
-    r = gsr.Renderer(gs, gsr.Settings(bounds=bounds, budget_mb=budget_mb, adaptive_list=False, rgb8=True))
+    r = gsr.Renderer(gs, gsr.Settings(bounds=bounds, budget_mb=budget_mb, adaptive_list=False, rgb8=True,
+                                      list_mode=list_mode))
     r.render(cam)
     return r
 
 
+@pytest.mark.parametrize("list_mode", ["binning", "global"])
 @pytest.mark.parametrize("name", ["tile_raster_250k", "needles_120k", "plain_720p"])
-def test_frame_bit_exact(gpu, port, name):
+def test_frame_bit_exact(gpu, port, name, list_mode):
     scene, cam = case(name)
-    r = render(gpu, scene, cam)
+    r = render(gpu, scene, cam, list_mode=list_mode)
     ocam, osp, ocounts, olist = oracle_frame(port, scene, cam, bounds=1)
     sp, counts = r.read_back_splats(scene.count)
     lo, hi, val, ranges, ctl = r.read_back()
@@ -106,12 +108,12 @@ def test_other_bounds_lists(gpu, port, mode):
 
 @pytest.mark.parametrize("width,height,count,packed", [(640, 360, 250_000, 1), (3840, 2160, 300_000, 0)])
 def test_entry_layouts(gpu, port, width, height, count, packed):
-    """Both entry layouts give the oracle's list: single 64-bit words when tile bits + varying
-    depth bits + index bits fit in 64 (640x360: 10 + 31 + 18), else (tile << 32 | depth, index)
-    pairs (3840x2160 with depths on both sides of 2.0: 15 + 31 + 19 = 65)."""
+    """Global mode's two entry layouts give the oracle's list: single 64-bit words when tile bits +
+    varying depth bits + index bits fit in 64 (640x360: 10 + 31 + 18), else (tile << 32 | depth,
+    index) pairs (3840x2160 with depths on both sides of 2.0: 15 + 31 + 19 = 65)."""
     scene = tile_raster_scene(count, 5)
     cam = tile_raster_camera(width, height)
-    r = render(gpu, scene, cam)
+    r = render(gpu, scene, cam, list_mode="global")
     lo, hi, val, ranges, ctl = r.read_back()
     assert ctl.packed_entries == packed and ctl.status == 0
     _, osp, ocounts, olist = oracle_frame(port, scene, cam, bounds=1)
@@ -135,10 +137,10 @@ def test_tight_image_equals_rect_image(gpu):
 
 @pytest.mark.parametrize("budget_mb", [1])
 def test_overflow_clamps_exactly(gpu, port, budget_mb):
-    """A 1 MB budget: the list is clamped to the capacity, the overflow is exact and the kept
-    entries are the CPU list truncated in index order (test_tile_raster.cpp:501-510)."""
+    """Global mode, a 1 MB budget: the list is clamped to the capacity, the overflow is exact and
+    the kept entries are the CPU list truncated in index order (test_tile_raster.cpp:501-510)."""
     scene, cam = case("tile_raster_250k")
-    r = render(gpu, scene, cam, budget_mb=budget_mb)
+    r = render(gpu, scene, cam, budget_mb=budget_mb, list_mode="global")
     ctl = r.read_control()
     cap = r.capacity()[0]
     assert ctl.overflow > 0 and ctl.entries == cap
