@@ -271,7 +271,7 @@ __global__ void __launch_bounds__(kFrontThreads) shDecodeKernel(const __grid_con
 //    tile count; cull counters with one ballot per warp and one atomic per block and reason. No
 //    waits: a streaming kernel.
 template <int GEOM, int COLOR, bool LEARNED>
-__global__ void __launch_bounds__(kFrontThreads) preprocessKernel(const __grid_constant__ FrontArgs a) {
+__global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __grid_constant__ FrontArgs a) {
     __shared__ DevCamera sCam;  // the view's camera, read once per block from its device copy
     __shared__ uint32_t sCull[kCullReasonCount];
     __shared__ uint32_t sDepthMin, sDepthMax;

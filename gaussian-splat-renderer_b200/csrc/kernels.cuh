@@ -83,6 +83,9 @@ constexpr int kMaxSortPasses = 8;
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+// binning mode's depth sort (frameMode 2): 4096-key tiles, its status array sized by them
+constexpr int kDepthSortItems = 16;
+constexpr int kDepthSortTile = kSortThreads * kDepthSortItems;
 struct SortPlan {
     uint32_t passes;        // significant 8-bit digits of the virtual key
     uint32_t lowBits;       // W: low key bits kept below the high word
@@ -100,7 +103,7 @@ struct SortArgs {
     uint64_t* keys[2];
     uint32_t* values[2];
     uint64_t* status;      // [kMaxSortPasses][maxTiles][256]
-    uint32_t maxTiles;     // ceil(capacity / kSortTile)
+    uint32_t maxTiles;     // ceil(capacity / kSortTile); the depth sort: ceil(count / kDepthSortTile)
     SortPlan* plan;
     DeviceControl* ctl;
     uint32_t passesLaunched;

@@ -52,6 +52,15 @@ int fail(int status, const char* fmt, ...) {
     return status;
 }
 
+}  // namespace
+
+namespace gsr {
+// the calling thread's failure message (the scene input units report through it)
+void setLastError(const std::string& message) { g_lastError = message; }
+}  // namespace gsr
+
+namespace {
+
 int cudaFail(cudaError_t e, const char* what) {
     if (e == cudaErrorMemoryAllocation)
         return fail(GSR_ERROR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
@@ -336,7 +345,7 @@ struct GsrRenderer {
         GSR_CUDA(hints.alloc(n * 16));
         if (binning()) {
             for (auto& k : depthKeys) GSR_CUDA(k.alloc(n * 8));
-            GSR_CUDA(depthStatus.alloc(size_t(kDepthSortPasses) * ((n + kSortTile - 1) / kSortTile) * 256 * 8));
+            GSR_CUDA(depthStatus.alloc(size_t(kDepthSortPasses) * ((n + kDepthSortTile - 1) / kDepthSortTile) * 256 * 8));
             GSR_CUDA(cudaMemset(depthStatus.p, 0, depthStatus.bytes));
         }
         GSR_CUDA(tileCounts.alloc(n * 4));
@@ -596,7 +605,7 @@ struct GsrRenderer {
             sd.keys[0] = fa.depthKeys[0];
             sd.keys[1] = fa.depthKeys[1];
             sd.status = depthStatus.as<uint64_t>();
-            sd.maxTiles = uint32_t((size_t(scene.count) * viewCount + kSortTile - 1) / kSortTile);
+            sd.maxTiles = uint32_t((size_t(scene.count) * viewCount + kDepthSortTile - 1) / kDepthSortTile);
             sd.plan = depthPlan.as<SortPlan>();
             sd.ctl = ctl;
             sd.passesLaunched = kDepthSortPasses;
@@ -698,6 +707,8 @@ const char* gsr_error_string(int status) {
         case GSR_ERROR_OUT_OF_MEMORY: return "out of device memory";
         case GSR_ERROR_DEVICE_TIMEOUT: return "a device-side wait timed out";
         case GSR_ERROR_NOT_READY: return "not ready";
+        case GSR_ERROR_FORMAT: return "malformed input file";
+        case GSR_ERROR_IO: return "file I/O error";
         default: return "unknown status";
     }
 }

@@ -28,7 +28,7 @@ LIB_PATH = _HERE / "libgsr_b200.so"
 
 GSR_OK = 0
 STATUS_NAMES = {0: "ok", 1: "invalid argument", 2: "unsupported", 3: "CUDA error", 4: "out of memory",
-                5: "device timeout", 6: "not ready"}
+                5: "device timeout", 6: "not ready", 7: "malformed input file", 8: "file I/O error"}
 FORMATS = {"f32": 0, "f16": 1, "q8": 2, "cb": 3}
 LAYOUTS = {"soa": 0, "split": 1, "aos": 2}
 BOUNDS = {"rect": 0, "tight": 1, "cutoff-only": 2}

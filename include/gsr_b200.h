@@ -31,7 +31,9 @@ typedef enum GsrStatus {
     GSR_ERROR_CUDA = 3,             /* a CUDA runtime call failed (VK_CHECK in the reference) */
     GSR_ERROR_OUT_OF_MEMORY = 4,
     GSR_ERROR_DEVICE_TIMEOUT = 5,   /* a bounded device-side wait gave up (GsrControl.status) */
-    GSR_ERROR_NOT_READY = 6         /* nothing to report yet (e.g. no completed frame) */
+    GSR_ERROR_NOT_READY = 6,        /* nothing to report yet (e.g. no completed frame) */
+    GSR_ERROR_FORMAT = 7,           /* a malformed input file (PlyError, src/scene/ply_loader.h:29-32) */
+    GSR_ERROR_IO = 8                /* a file could not be opened or read (std::runtime_error) */
 } GsrStatus;
 
 /* ---- scene (gsr::GpuScene, src/render/gpu_scene.h:42-78) ------------------------------ */
@@ -380,6 +382,134 @@ int gsr_scan_static(const uint32_t* in, const uint32_t* index, uint32_t* out, ui
  * Bit-for-bit the order of a stable sort (DepthSorter::radixSortPairs for 32-bit keys). */
 int gsr_sort_pairs(uint32_t* keys_lo, uint32_t* keys_hi, uint32_t* values, uint32_t count, uint32_t key_bits,
                    void* stream);
+
+/* ---- scene input: 3DGS PLY files (src/scene/ply_loader.h:1-120) --------------------------
+ * Host-side: the file is validated exactly as loadGaussianPly does (same accepted files, the
+ * same error and warning texts) and decoded by all host threads into the activated SoA arrays
+ * of gsr::GaussianScene: posAlpha = (x, y, z, sigmoid(opacity)), scales = (exp(scale_i), 0),
+ * rotations = normalized (rot_0..rot_3) = (w, x, y, z), SH as RGB triplets per coefficient
+ * (the file's channel-major f_rest transposed), bit-identical to the reference loader's.
+ * gsr_loaded_scene_host() hands them to gsr_scene_create(). Errors: GSR_ERROR_FORMAT for a
+ * malformed file, GSR_ERROR_IO when it cannot be read; the message names the problem. */
+typedef struct GsrLoadedScene GsrLoadedScene;
+
+/* gsr::SceneStats (src/scene/gaussian_scene.h:47-61). */
+typedef struct GsrSceneStats {
+    float bbox_min[3], bbox_max[3];
+    float robust_min[3], robust_max[3]; /* per-axis 1st / 99th percentile: sorted[int(p (n - 1))] */
+    float alpha_min, alpha_max, alpha_mean;
+    uint32_t alpha_below_visible;       /* alpha < 1/255 */
+    float sigma_min, sigma_max, sigma_max_median;
+    float quat_norm_min, quat_norm_max; /* raw quaternion lengths */
+    uint32_t zero_quaternions;          /* replaced by identity */
+    uint64_t non_finite_values;         /* NaN/Inf in the decoded properties */
+} GsrSceneStats;
+
+/* gsr::LoadTimings (gaussian_scene.h:63-69). */
+typedef struct GsrLoadTimings {
+    double map_ms, header_ms, decode_ms, stats_ms, total_ms;
+} GsrLoadTimings;
+
+typedef struct GsrLoadedSceneInfo {
+    uint32_t count;
+    int32_t sh_degree;
+    uint32_t comment_count; /* header comment lines */
+    uint32_t warning_count; /* non-fatal issues (skipped elements, trailing bytes, NaN, ...) */
+    GsrSceneStats stats;
+    GsrLoadTimings timings;
+} GsrLoadedSceneInfo;
+
+/* Host arrays owned by the loaded scene (valid until gsr_loaded_scene_destroy). */
+typedef struct GsrLoadedSceneArrays {
+    const float* pos_alpha;     /* float4[N] */
+    const float* scales;        /* float4[N] */
+    const float* rotations;     /* float4[N] */
+    const float* sh;            /* float[N * K * 3], K = (sh_degree + 1)^2 */
+    const float* raw_opacity;   /* float[N]: the file's opacity (logit) */
+    const float* raw_log_scale; /* float3[N]: the file's scale_0..2 (log sigma) */
+    const float* raw_rotation;  /* float4[N]: the file's rot_0..3, unnormalized */
+} GsrLoadedSceneArrays;
+
+/* loadGaussianPly(path) (ply_loader.h:75-77): the file name prefixes the messages. */
+int gsr_ply_load(const char* path, GsrLoadedScene** out);
+/* loadGaussianPly(bytes, name) (ply_loader.h:78-80). */
+int gsr_ply_load_memory(const void* bytes, size_t size, const char* name, GsrLoadedScene** out);
+int gsr_loaded_scene_info(const GsrLoadedScene* scene, GsrLoadedSceneInfo* info);
+int gsr_loaded_scene_arrays(const GsrLoadedScene* scene, GsrLoadedSceneArrays* arrays);
+/* The activated arrays as a GsrHostScene, for gsr_scene_create(). */
+int gsr_loaded_scene_host(const GsrLoadedScene* scene, GsrHostScene* host);
+const char* gsr_loaded_scene_comment(const GsrLoadedScene* scene, uint32_t index);
+const char* gsr_loaded_scene_warning(const GsrLoadedScene* scene, uint32_t index);
+const char* gsr_loaded_scene_source(const GsrLoadedScene* scene);
+void gsr_loaded_scene_destroy(GsrLoadedScene* scene);
+/* shDegreeFromRestCount (ply_loader.h:72): 0/9/24/45 -> 0..3, else -1. */
+int gsr_ply_sh_degree_from_rest_count(uint64_t rest_count);
+
+/* parsePlyHeader / parsePlyHeaderPrefix (ply_loader.h:64-69): final_bytes = 0 returns
+ * GSR_ERROR_NOT_READY while the end_header line has not arrived. Property types are
+ * PlyScalar's order: int8, uint8, int16, uint16, int32, uint32, float32, float64. */
+typedef struct GsrPlyHeader GsrPlyHeader;
+typedef struct GsrPlyElementInfo {
+    const char* name;
+    uint64_t count;
+    uint32_t stride; /* bytes per record: every scalar property */
+    uint32_t has_list;
+    uint32_t property_count;
+} GsrPlyElementInfo;
+typedef struct GsrPlyPropertyInfo {
+    const char* name;
+    uint32_t type;
+    uint32_t is_list;
+    uint32_t offset; /* byte offset in the record (scalar properties) */
+} GsrPlyPropertyInfo;
+int gsr_ply_parse_header(const void* bytes, size_t size, int final_bytes, GsrPlyHeader** out);
+/* format: 0 binary_little_endian, 1 binary_big_endian, 2 ascii. */
+int gsr_ply_header_info(const GsrPlyHeader* header, uint32_t* format, uint32_t* element_count, uint32_t* comment_count,
+                        uint64_t* header_bytes);
+int gsr_ply_header_element(const GsrPlyHeader* header, uint32_t index, GsrPlyElementInfo* info);
+int gsr_ply_header_property(const GsrPlyHeader* header, uint32_t element, uint32_t property, GsrPlyPropertyInfo* info);
+const char* gsr_ply_header_comment(const GsrPlyHeader* header, uint32_t index);
+void gsr_ply_header_destroy(GsrPlyHeader* header);
+
+/* PlyStreamDecoder (ply_loader.h:82-117): bytes pushed in order in chunks of any size; the header
+ * callback runs once the header has passed its checks (info: count, degree, comments), the batch
+ * callback with each decoded batch of up to batch_capacity gaussians (0: 16384) as gaussians
+ * [first, first + batch count), valid during the call. The batches concatenated equal
+ * gsr_ply_load's arrays bit for bit, and a bad file fails with the same message. finish() runs
+ * the size checks and fills the info's warnings and NaN / zero-quaternion counters. After an
+ * error, push and finish return GSR_ERROR_INVALID_ARGUMENT. */
+typedef struct GsrPlyStream GsrPlyStream;
+typedef void (*GsrPlyHeaderCallback)(void* user, const GsrLoadedScene* info);
+typedef void (*GsrPlyBatchCallback)(void* user, uint32_t first, const GsrLoadedScene* batch);
+int gsr_ply_stream_create(const char* name, uint64_t total_bytes, GsrPlyHeaderCallback on_header,
+                          GsrPlyBatchCallback on_batch, void* user, uint32_t batch_capacity, GsrPlyStream** out);
+int gsr_ply_stream_push(GsrPlyStream* stream, const void* bytes, size_t size);
+int gsr_ply_stream_finish(GsrPlyStream* stream);
+int gsr_ply_stream_state(const GsrPlyStream* stream, uint32_t* header_parsed, uint32_t* finished,
+                         uint64_t* bytes_received, uint64_t* records_decoded);
+const GsrLoadedScene* gsr_ply_stream_info(const GsrPlyStream* stream);
+void gsr_ply_stream_destroy(GsrPlyStream* stream);
+
+/* ---- scene input: INRIA training cameras (src/scene/training_cameras.h:1-44) ------------- */
+#define GSR_IMAGE_NAME_CAPACITY 256
+typedef struct GsrTrainingCamera {
+    int32_t id;
+    uint32_t width, height;
+    float position[3];        /* camera centre, data space */
+    float camera_to_world[9]; /* column-major; the columns are the camera's right, down, forward axes */
+    float fx, fy;             /* focal lengths in pixels */
+    char image_name[GSR_IMAGE_NAME_CAPACITY]; /* NUL-terminated (truncated) */
+} GsrTrainingCamera;
+/* loadTrainingCameras (cameras.json): *count = the cameras in the file; the first `capacity`
+ * are written. GSR_ERROR_IO with "Cannot open cameras file: ..." or "Invalid cameras file ...". */
+int gsr_training_cameras_load(const char* path, GsrTrainingCamera* cameras, uint32_t capacity, uint32_t* count);
+/* TrainingCamera::fovYDeg: 2 atan(height / (2 fy)) in degrees. */
+float gsr_training_camera_fov_y_deg(const GsrTrainingCamera* camera);
+/* meanCameraUp: the normalized mean of -down over the cameras ((0, -1, 0) if it vanishes). */
+int gsr_training_cameras_mean_up(const GsrTrainingCamera* cameras, uint32_t count, float up[3]);
+/* cameraFocusPoint: the least-squares point nearest every optical axis (the centroid when the
+ * axes are parallel). */
+int gsr_training_cameras_focus_point(const GsrTrainingCamera* cameras, uint32_t count, float point[3]);
 
 /* ---- diagnostics ------------------------------------------------------------------------ */
 const char* gsr_error_string(int status);

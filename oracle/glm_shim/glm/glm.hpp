@@ -13,7 +13,9 @@
 //       (A*B)[c][r] = ((A[0][r]*B[c][0] + A[1][r]*B[c][1]) + A[2][r]*B[c][2]) (+ A[3][r]*B[c][3])
 //       (M*v)[r]    = ((M[0][r]*v.x + M[1][r]*v.y) + M[2][r]*v.z) (+ M[3][r]*v.w)
 //     including products with entries that happen to be zero (no term is dropped);
-//   * dot(a, b) = (a.x*b.x + a.y*b.y) + a.z*b.z (+ a.w*b.w);
+//   * dot(a, b) = (a.x*b.x + a.y*b.y) + a.z*b.z for vec3, and for vec4 GLM 1.0.1's generic
+//     compute_dot<vec4> (func_geometric.inl, every compiler but MSVC):
+//     (a.x*b.x + a.y*b.y) + (a.z*b.z + a.w*b.w);
 //   * normalize(v) = v * (1 / sqrt(dot(v, v))); length(v) = sqrt(dot(v, v));
 //   * max(a, b) = (a < b) ? b : a and min(a, b) = (b < a) ? b : a per component;
 //   * outerProduct(c, r)[i][j] = c[j] * r[i].
@@ -98,11 +100,12 @@ inline vec4 operator-(const vec4& a, const vec4& b) { return {a.x - b.x, a.y - b
 inline vec4 operator*(const vec4& a, const vec4& b) { return {a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w}; }
 inline vec4 operator*(const vec4& a, float s) { return {a.x * s, a.y * s, a.z * s, a.w * s}; }
 inline vec4 operator*(float s, const vec4& a) { return {s * a.x, s * a.y, s * a.z, s * a.w}; }
+inline vec4 operator/(const vec4& a, float s) { return {a.x / s, a.y / s, a.z / s, a.w / s}; }
 
 // ---- geometric functions ------------------------------------------------------------------
 inline float dot(const vec2& a, const vec2& b) { return a.x * b.x + a.y * b.y; }
 inline float dot(const vec3& a, const vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-inline float dot(const vec4& a, const vec4& b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+inline float dot(const vec4& a, const vec4& b) { return (a.x * b.x + a.y * b.y) + (a.z * b.z + a.w * b.w); }
 inline float length(const vec3& v) { return std::sqrt(dot(v, v)); }
 inline float length(const vec4& v) { return std::sqrt(dot(v, v)); }
 inline vec3 normalize(const vec3& v) { return v * (1.0f / std::sqrt(dot(v, v))); }
@@ -110,6 +113,8 @@ inline vec4 normalize(const vec4& v) { return v * (1.0f / std::sqrt(dot(v, v)));
 inline vec3 cross(const vec3& a, const vec3& b) {
     return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
 }
+
+inline vec3 exp(const vec3& v) { return {std::exp(v.x), std::exp(v.y), std::exp(v.z)}; }
 
 inline float max(float a, float b) { return (a < b) ? b : a; }
 inline float min(float a, float b) { return (b < a) ? b : a; }

@@ -115,6 +115,15 @@ class Oracle:
         f("encode", C.c_int, None)
         f("decode", None, None)
         f("select_sh_degree", C.c_int, [C.c_void_p, C.c_int, C.c_float, C.c_float])
+        if kind == "reference":
+            err = [C.c_char_p, C.c_size_t, C.POINTER(C.c_int)]
+            f("ply_load", C.c_void_p, [C.c_char_p] + err)
+            f("ply_load_memory", C.c_void_p, [C.c_void_p, C.c_size_t, C.c_char_p] + err)
+            f("ply_info", None, [C.c_void_p] + [C.c_void_p] * 5)
+            f("ply_arrays", None, [C.c_void_p] + [C.c_void_p] * 7)
+            f("ply_comment", C.c_char_p, [C.c_void_p, C.c_uint32])
+            f("ply_warning", C.c_char_p, [C.c_void_p, C.c_uint32])
+            f("ply_free", None, [C.c_void_p])
         if kind == "port":
             f("look_at", None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p])
             f("perspective", None, [C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p])
@@ -270,6 +279,38 @@ class Oracle:
 
     def half_to_float(self, h: int) -> float:
         return self._half_to_float(C.c_uint16(h))
+
+
+    # ---- the reference's PLY loader (reference kind only) ---------------------------------
+    def ply_load(self, path=None, data: bytes = None, name: str = ""):
+        """loadGaussianPly of the reference, from a file or from bytes. Returns a dict: on error
+        {"error": text, "kind": 1 for PlyError, 2 otherwise}; else count, degree, comments,
+        warnings, stats (the 96 bytes of gsr::SceneStats in GsrSceneStats order) and arrays."""
+        err = C.create_string_buffer(4096)
+        kind = C.c_int(0)
+        if data is not None:
+            buf = C.create_string_buffer(bytes(data), len(data)) if data else None
+            h = self._ply_load_memory(buf, len(data), name.encode(), err, 4096, C.byref(kind))
+        else:
+            h = self._ply_load(str(path).encode(), err, 4096, C.byref(kind))
+        if not h:
+            return {"error": err.value.decode(errors="replace"), "kind": kind.value}
+        try:
+            n, deg, nc, nw = C.c_uint32(), C.c_int(), C.c_uint32(), C.c_uint32()
+            stats = C.create_string_buffer(96)
+            self._ply_info(h, C.byref(n), C.byref(deg), C.byref(nc), C.byref(nw), stats)
+            N, K = n.value, (deg.value + 1) ** 2
+            out = {k: np.zeros(shape, np.float32) for k, shape in (
+                ("pos_alpha", (N, 4)), ("scales", (N, 4)), ("rotations", (N, 4)), ("sh", (N * K * 3,)),
+                ("raw_opacity", (N,)), ("raw_log_scale", (N, 3)), ("raw_rotation", (N, 4)))}
+            self._ply_arrays(h, *[_p(out[k]) for k in ("pos_alpha", "scales", "rotations", "sh", "raw_opacity",
+                                                       "raw_log_scale", "raw_rotation")])
+            out.update(count=N, sh_degree=deg.value, stats=stats.raw,
+                       comments=[self._ply_comment(h, i).decode() for i in range(nc.value)],
+                       warnings=[self._ply_warning(h, i).decode() for i in range(nw.value)])
+            return out
+        finally:
+            self._ply_free(h)
 
 
 def reference_available() -> bool:

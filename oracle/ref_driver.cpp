@@ -9,6 +9,7 @@
 // with gsr_oracle.h (same field order and sizes).
 #include "scene/gaussian_scene.h"
 #include "scene/half.h"
+#include "scene/ply_loader.h"
 #include "scene/scene_compression.h"
 #include "splat/depth_sort.h"
 #include "splat/reference_renderer.h"
@@ -16,7 +17,11 @@
 #include "splat/tile_coverage.h"
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
+#include <filesystem>
+#include <functional>
+#include <span>
 #include <numeric>
 #include <stdexcept>
 #include <vector>
@@ -291,5 +296,94 @@ void gsr_ref_decode(uint32_t n, const uint32_t* desc, const uint64_t* sizes, voi
 int gsr_ref_select_sh_degree(const float* sh, int storedDegree, float opacity, float threshold255) {
     return gsr::selectShDegree(reinterpret_cast<const glm::vec3*>(sh), storedDegree, opacity, threshold255);
 }
+
+// ---- the PLY loader (src/scene/ply_loader.cpp) ---------------------------------------------
+// gsr_ref_ply_load / _memory return a GaussianScene handle, or NULL with the exception's text
+// in err and *kind = 1 (PlyError) or 2 (any other exception).
+struct RefSceneStats {  // = GsrSceneStats (include/gsr_b200.h)
+    float bboxMin[3], bboxMax[3], robustMin[3], robustMax[3];
+    float alphaMin, alphaMax, alphaMean;
+    uint32_t alphaBelowVisible;
+    float sigmaMin, sigmaMax, sigmaMaxMedian, quatNormMin, quatNormMax;
+    uint32_t zeroQuaternions;
+    uint64_t nonFiniteValues;
+};
+
+static void* plyResult(const std::function<gsr::GaussianScene()>& load, char* err, size_t cap, int* kind) {
+    *kind = 0;
+    try {
+        return new gsr::GaussianScene(load());
+    } catch (const gsr::PlyError& e) {
+        *kind = 1;
+        std::snprintf(err, cap, "%s", e.what());
+    } catch (const std::exception& e) {
+        *kind = 2;
+        std::snprintf(err, cap, "%s", e.what());
+    }
+    return nullptr;
+}
+
+void* gsr_ref_ply_load(const char* path, char* err, size_t cap, int* kind) {
+    return plyResult([&] { return gsr::loadGaussianPly(std::filesystem::path(path)); }, err, cap, kind);
+}
+
+void* gsr_ref_ply_load_memory(const uint8_t* bytes, size_t size, const char* name, char* err, size_t cap, int* kind) {
+    return plyResult([&] { return gsr::loadGaussianPly(std::span<const uint8_t>(bytes, size), std::string(name)); }, err,
+                     cap, kind);
+}
+
+void gsr_ref_ply_info(const void* h, uint32_t* count, int* degree, uint32_t* comments, uint32_t* warnings,
+                      RefSceneStats* stats) {
+    const auto& s = *static_cast<const gsr::GaussianScene*>(h);
+    *count = s.count;
+    *degree = s.shDegree;
+    *comments = uint32_t(s.comments.size());
+    *warnings = uint32_t(s.warnings.size());
+    const gsr::SceneStats& t = s.stats;
+    for (int c = 0; c < 3; ++c) {
+        stats->bboxMin[c] = t.bboxMin[c];
+        stats->bboxMax[c] = t.bboxMax[c];
+        stats->robustMin[c] = t.robustMin[c];
+        stats->robustMax[c] = t.robustMax[c];
+    }
+    stats->alphaMin = t.alphaMin;
+    stats->alphaMax = t.alphaMax;
+    stats->alphaMean = t.alphaMean;
+    stats->alphaBelowVisible = t.alphaBelowVisible;
+    stats->sigmaMin = t.sigmaMin;
+    stats->sigmaMax = t.sigmaMax;
+    stats->sigmaMaxMedian = t.sigmaMaxMedian;
+    stats->quatNormMin = t.quatNormMin;
+    stats->quatNormMax = t.quatNormMax;
+    stats->zeroQuaternions = t.zeroQuaternions;
+    stats->nonFiniteValues = t.nonFiniteValues;
+}
+
+// posAlpha/scales/rotations/rawRotation float4[N], sh float[N K 3], rawOpacity [N], rawLogScale float3[N]
+void gsr_ref_ply_arrays(const void* h, float* posAlpha, float* scales, float* rotations, float* sh, float* rawOpacity,
+                        float* rawLogScale, float* rawRotation) {
+    const auto& s = *static_cast<const gsr::GaussianScene*>(h);
+    for (uint32_t i = 0; i < s.count; ++i) {
+        for (int c = 0; c < 4; ++c) {
+            posAlpha[i * 4 + c] = s.posAlpha[i][c];
+            scales[i * 4 + c] = s.scales[i][c];
+            rotations[i * 4 + c] = s.rotations[i][c];
+            rawRotation[i * 4 + c] = s.rawRotation[i][c];
+        }
+        for (int c = 0; c < 3; ++c) rawLogScale[i * 3 + c] = s.rawLogScale[i][c];
+        rawOpacity[i] = s.rawOpacity[i];
+    }
+    std::copy(s.sh.begin(), s.sh.end(), sh);
+}
+
+const char* gsr_ref_ply_comment(const void* h, uint32_t i) {
+    return static_cast<const gsr::GaussianScene*>(h)->comments.at(i).c_str();
+}
+
+const char* gsr_ref_ply_warning(const void* h, uint32_t i) {
+    return static_cast<const gsr::GaussianScene*>(h)->warnings.at(i).c_str();
+}
+
+void gsr_ref_ply_free(void* h) { delete static_cast<gsr::GaussianScene*>(h); }
 
 }  // extern "C"

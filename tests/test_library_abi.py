@@ -34,8 +34,8 @@ def test_exports_every_declared_symbol(gsr):
 def test_abi_version_and_error_strings(gsr):
     lib = gsr.load()
     assert lib.gsr_abi_version() == 1
-    names = [lib.gsr_error_string(i).decode() for i in range(7)]
-    assert names[0] == "ok" and len(set(names)) == 7
+    names = [lib.gsr_error_string(i).decode() for i in range(9)]
+    assert names[0] == "ok" and len(set(names)) == 9
 
 
 def test_settings_defaults_are_the_reference_defaults(gsr):
@@ -43,6 +43,7 @@ def test_settings_defaults_are_the_reference_defaults(gsr):
     s = gsr.CSettings()
     gsr.load().gsr_settings_default(C.byref(s))
     assert (s.bounds, s.tile_size, s.budget_mb, s.adaptive_list, s.max_sh_degree, s.frames_in_flight) == (1, 16, 256, 1, 3, 2)
+    assert s.list_mode == 0  # TileSortMode::Binning (splat_tile_renderer.h:76, 97)
 
 
 def test_camera_bit_exact_with_reference(gsr, port, ref):
