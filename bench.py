@@ -188,7 +188,7 @@ def front_bytes(scene_format: str, ctl, n: int, list_mode: str = "global") -> fl
 FRONT_TRAFFIC_PLAIN_1080P = {
     "global": (296.7 + 61.3 + 5.0 + 89.3 + 8.4) * 1e6,
     # preprocess, depth histogram, 4 depth passes, gathered scan, emission in depth order
-    "binning": (296.7 + 70.7 + 10.0 + 4 * 10.0 + 14.9 + 151.5 + 29.0) * 1e6,
+    "binning": (302.1 + 73.5 + 10.0 + 39.7 + 14.9 + 152.6 + 29.0) * 1e6,
 }
 
 
