@@ -260,7 +260,8 @@ def run_b200(args, dist: Dist):
     dev = torch.device("cuda", dist.local_rank)
     scene, cams, fmt, layout = make_config(args.config)
     gs = G.GpuScene(scene, fmt, layout)
-    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, list_mode=args.list_mode))
+    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, list_mode=args.list_mode,
+                                  render_splat=args.render_splat))
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     first = (dist.rank * 37) % len(cams)
@@ -404,7 +405,7 @@ def tune(args, G, gs, cams, first: int, model=None):
         return {"views_per_frame": args.batch, "raster_schedule": "auto", "table": None}
     probe = G.camera_array([cams[(first + k) % len(cams)] for k in range(32)])
     settings = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
-                          list_mode=args.list_mode)
+                          list_mode=args.list_mode, render_splat=args.render_splat)
     return G.autotune(gs, settings, probe, depths=(1, 2, 4, 8, 16), frames=4, model=model)
 
 
@@ -421,7 +422,8 @@ def run_batched(args, dist: Dist, G, gs, cams, first: int, stream, plain_rendere
     frames = [G.camera_array([cams[(first + k * d + j) % nviews] for j in range(d)]) for k in range(nviews // d + 1)]
     nframes = len(frames)
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
-                                  raster_schedule=tuned["raster_schedule"], list_mode=args.list_mode))
+                                  raster_schedule=tuned["raster_schedule"], list_mode=args.list_mode,
+                                  render_splat=args.render_splat))
     if model is not None:
         r.set_color_model(model)
     # warm-up: at least the requested views, then until the adaptive list keeps its capacity for
@@ -506,6 +508,8 @@ def main():
     ap.add_argument("--mlp-steps", type=int, default=2000)
     ap.add_argument("--list-mode", default="binning", choices=["binning", "global"],
                     help="list construction: one (tile, depth) sort, or depth sort + emission + tile sort")
+    ap.add_argument("--render-splat", default="full", choices=["full", "p32", "p24"],
+                    help="the per-entry record of emission and render: 48 B, or packed 32 / 24 B")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

@@ -270,7 +270,28 @@ __global__ void __launch_bounds__(kFrontThreads) shDecodeKernel(const __grid_con
 //    GSR_TILES); grid.y = view. Writes the splat record of visible gaussians and every gaussian's
 //    tile count; cull counters with one ballot per warp and one atomic per block and reason. No
 //    waits: a streaming kernel.
-template <int GEOM, int COLOR, bool LEARNED>
+// writeRenderSplat (splat_preprocess.comp:74-91), packed forms: the record, the packed tile
+// rectangle and the depth bits, each in its own array.
+__device__ __forceinline__ void writePackedSplat(const FrontArgs& a, size_t rec, const DevSplat& s, const TileRect& rect,
+                                                 uint32_t p24w0, uint32_t p24w1) {
+    const uint32_t cr = packColorRadius(s.b, s.radius);
+    if (a.renderSplat == kRenderSplatP32) {
+        uint4* p = reinterpret_cast<uint4*>(a.packed) + rec * 2;
+        p[0] = make_uint4(__float_as_uint(s.cx), __float_as_uint(s.cy), __float_as_uint(s.conicA), __float_as_uint(s.conicB));
+        p[1] = make_uint4(__float_as_uint(s.conicC), __float_as_uint(s.opacity), packHalf2(s.r, s.g), cr);
+    } else {
+        uint2* p = reinterpret_cast<uint2*>(a.packed) + rec * 3;
+        p[0] = make_uint2(__float_as_uint(s.cx), __float_as_uint(s.cy));
+        p[1] = make_uint2(p24w0, p24w1);
+        p[2] = make_uint2(packHalf2(s.r, s.g), cr);
+    }
+    a.rects[rec] = packRect(rect);
+    a.depths[rec] = __float_as_uint(s.depth);
+}
+
+// PACKED: packed render records (p32 / p24, told apart at run time) instead of the 48-byte
+// record; a compile-time switch so that the default kernel carries none of their code.
+template <int GEOM, int COLOR, bool LEARNED, bool PACKED>
 __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __grid_constant__ FrontArgs a) {
     __shared__ DevCamera sCam;  // the view's camera, read once per block from its device copy
     __shared__ uint32_t sCull[kCullReasonCount];
@@ -307,13 +328,21 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
     if (i < a.count) {
         uint32_t count = 0;
         if (reason == kCullVisible) {
-            const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
-                                             s.opacity, a.logf);
+            // the conic and opacity as the emission and the rasterizer will read them: p24 keeps
+            // them in fp16, so its tiles are counted with the decoded values
+            float cA = s.conicA, cB = s.conicB, cC = s.conicC, cO = s.opacity;
+            uint32_t p24w0 = 0, p24w1 = 0;
+            if (PACKED && a.renderSplat == kRenderSplatP24) {
+                p24ConicWords(cA, cB, cC, cO, p24w0, p24w1);
+                p24DecodeConic(p24w0, p24w1, cA, cB, cC, cO);
+            }
+            const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, cA, cB, cC, cO, a.logf);
             const RowGeom g = rowGeom(cv);
             count = coverageCount(cv, g, a.binSize);
             if (a.bounds != kBoundsRect) a.hints[rec] = coverageHint(cv, g);
             s.cullReason = kCullVisible;
-            reinterpret_cast<DevSplat*>(a.splats)[rec] = s;
+            if (!PACKED) reinterpret_cast<DevSplat*>(a.splats)[rec] = s;
+            else writePackedSplat(a, rec, s, rect, p24w0, p24w1);
             dmin = dmax = __float_as_uint(s.depth);  // positive: the bits order like the values
         }
         a.tileCounts[rec] = count;
@@ -384,15 +413,43 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
         const uint32_t sentinel = a.totalTiles;
         const KeyLayout lay = keyLayout(a.ctl, sentinel, a.count, BINNING);
         const uint32_t offset = a.offsets[slot];
-        const DevSplat s = reinterpret_cast<const DevSplat*>(a.splats)[rec];
         const DevView vw = a.views[view];
         const int gx = int(vw.tilesX) * (16 / a.binSize), gy = int(vw.tilesY) * (16 / a.binSize);
-        const TileRect rect = tileRect(s.cx, s.cy, s.radius, vw.tilesX, vw.tilesY);
+        // centre, conic, rectangle and depth from the record (full) or the packed arrays
+        float cx, cy, cA, cB, cC;
+        TileRect rect;
+        uint64_t depthBits;
+        if (a.renderSplat == kRenderSplatFull) {
+            const DevSplat s = reinterpret_cast<const DevSplat*>(a.splats)[rec];
+            cx = s.cx;
+            cy = s.cy;
+            cA = s.conicA;
+            cB = s.conicB;
+            cC = s.conicC;
+            rect = tileRect(s.cx, s.cy, s.radius, vw.tilesX, vw.tilesY);
+            depthBits = __float_as_uint(s.depth);
+        } else {
+            rect = unpackRect(a.rects[rec]);
+            depthBits = a.depths[rec];
+            if (a.renderSplat == kRenderSplatP32) {
+                const uint4 w = reinterpret_cast<const uint4*>(a.packed)[rec * 2];
+                cx = __uint_as_float(w.x);
+                cy = __uint_as_float(w.y);
+                cA = __uint_as_float(w.z);
+                cB = __uint_as_float(w.w);
+                cC = __uint_as_float(reinterpret_cast<const uint32_t*>(a.packed)[rec * 8 + 4]);
+            } else {
+                const uint2 w0 = reinterpret_cast<const uint2*>(a.packed)[rec * 3];
+                const uint2 w1 = reinterpret_cast<const uint2*>(a.packed)[rec * 3 + 1];
+                cx = __uint_as_float(w0.x);
+                cy = __uint_as_float(w0.y);
+                float o;
+                p24DecodeConic(w1.x, w1.y, cA, cB, cC, o);
+            }
+        }
         RowGeom g;
         const float4 hint = a.bounds != kBoundsRect ? a.hints[rec] : make_float4(-2.0f, 0.0f, 0.0f, 0.0f);
-        const Coverage cv = coverageFromHint(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, s.conicA, s.conicB, s.conicC,
-                                             hint, g);
-        const uint64_t depthBits = __float_as_uint(s.depth);
+        const Coverage cv = coverageFromHint(a.bounds, rect, a.binSize, gx, gy, cx, cy, cA, cB, cC, hint, g);
         // packed: (((tile << W) | depth mod 2^W) << indexBits) | index; the tile part added per entry
         const uint64_t packedBase =
             ((lay.lowBits >= 32 ? depthBits : (depthBits & ((1ull << lay.lowBits) - 1ull))) << lay.indexBits) | i;
@@ -504,8 +561,14 @@ cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capaci
 namespace {
 template <int GEOM, int COLOR>
 void launchPreprocess(const FrontArgs& a, dim3 blocks, cudaStream_t s) {
-    if (a.latents) preprocessKernel<GEOM, COLOR, true><<<blocks, kFrontThreads, 0, s>>>(a);
-    else preprocessKernel<GEOM, COLOR, false><<<blocks, kFrontThreads, 0, s>>>(a);
+    const bool packed = a.renderSplat != kRenderSplatFull;
+    if (a.latents) {
+        if (packed) preprocessKernel<GEOM, COLOR, true, true><<<blocks, kFrontThreads, 0, s>>>(a);
+        else preprocessKernel<GEOM, COLOR, true, false><<<blocks, kFrontThreads, 0, s>>>(a);
+    } else {
+        if (packed) preprocessKernel<GEOM, COLOR, false, true><<<blocks, kFrontThreads, 0, s>>>(a);
+        else preprocessKernel<GEOM, COLOR, false, false><<<blocks, kFrontThreads, 0, s>>>(a);
+    }
 }
 template <int GEOM, int COLOR>
 void launchShDecodeT(const SceneArgs& scene, uint32_t count, int evalDegree, float* out, uint8_t* degrees, cudaStream_t s) {

@@ -27,6 +27,7 @@
 // pair's contribution); tests bound it: float PSNR > 60 dB and the 8-bit image within 1/255.
 #include "gsr_device.cuh"
 #include "kernels.cuh"
+#include "render_splat.cuh"
 
 namespace gsr {
 
@@ -43,6 +44,10 @@ __device__ __forceinline__ void cpAsync16(void* smemDst, const void* gsrc) {
     const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smemDst));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gsrc) : "memory");
 }
+__device__ __forceinline__ void cpAsync8(void* smemDst, const void* gsrc) {
+    const uint32_t s = static_cast<uint32_t>(__cvta_generic_to_shared(smemDst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void cpAsyncCommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cpAsyncWait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
@@ -53,7 +58,9 @@ __device__ __forceinline__ float fastExp2(float x) {
 }
 
 struct RenderShared {
-    float4 raw[2][3][kRenderThreads];  // gathered ProjectedSplat records (3 x 16 B), double-buffered
+    // gathered records, double-buffered: full 3 x 16 B, p32 2 x 16 B, p24 3 x 8 B (as uint2 in the
+    // first half of each row)
+    float4 raw[2][3][kRenderThreads];
     float4 conic[kRenderThreads];      // a', b', c' (pre-scaled), opacity
     float4 box[kRenderThreads];        // x0, x1, y0, y1 of the cutoff ellipse (pixels)
     float4 color[kRenderThreads];      // r, g, b, -
@@ -73,6 +80,9 @@ __device__ __forceinline__ uint32_t viewOfTile(const RenderArgs& a, uint32_t t) 
 }
 
 // The whole per-tile pass for frame tile `tile`; every thread of the block calls it.
+// MODE: the record layout (kRenderSplatFull / P32 / P24), a compile-time parameter so that each
+// layout's kernel carries only its own gather and decode (a runtime switch measured 8 % slower).
+template <int MODE>
 __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm, uint32_t tile) {
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t view = viewOfTile(a, tile);
@@ -93,6 +103,9 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
     const bool packed = a.plan->packed != 0;
     const uint64_t indexMask = (1ull << a.plan->indexBits) - 1ull;
     const float4* records = reinterpret_cast<const float4*>(a.splats) + size_t(view) * a.count * 3;
+    const uint4* records32 = reinterpret_cast<const uint4*>(a.packed) + size_t(view) * a.count * 2;
+    const uint2* records24 = reinterpret_cast<const uint2*>(a.packed) + size_t(view) * a.count * 3;
+    constexpr int mode = MODE;
     const float fx = float(px), fy = float(py);
     // this warp's pixel strip
     const float wx0 = float(tx * 16), wx1 = float(tx * 16 + 15);
@@ -108,10 +121,22 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
                 atomicOr(&a.ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
                 g = 0;
             }
-            const float4* rec = records + size_t(g) * 3;
-            cpAsync16(&sm.raw[buf][0][tid], rec);
-            cpAsync16(&sm.raw[buf][1][tid], rec + 1);
-            cpAsync16(&sm.raw[buf][2][tid], rec + 2);
+            if constexpr (mode == kRenderSplatFull) {
+                const float4* rec = records + size_t(g) * 3;
+                cpAsync16(&sm.raw[buf][0][tid], rec);
+                cpAsync16(&sm.raw[buf][1][tid], rec + 1);
+                cpAsync16(&sm.raw[buf][2][tid], rec + 2);
+            } else if constexpr (mode == kRenderSplatP32) {
+                const uint4* rec = records32 + size_t(g) * 2;
+                cpAsync16(&sm.raw[buf][0][tid], rec);
+                cpAsync16(&sm.raw[buf][1][tid], rec + 1);
+            } else {  // 24-byte records start on 8-byte boundaries
+                const uint2* rec = records24 + size_t(g) * 3;
+                uint2* dst = reinterpret_cast<uint2*>(&sm.raw[buf][0][0]);
+                cpAsync8(&dst[tid], rec);
+                cpAsync8(&dst[kRenderThreads + tid], rec + 1);
+                cpAsync8(&dst[2 * kRenderThreads + tid], rec + 2);
+            }
         }
         cpAsyncCommit();
     };
@@ -127,10 +152,35 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
         cpAsyncWait<1>();
         __syncthreads();
         if (start + tid < range.y) {
-            const float4 r0 = sm.raw[buf][0][tid];  // cx, cy, depth, cull
-            const float4 r1 = sm.raw[buf][1][tid];  // A, B, C, opacity
-            const float4 r2 = sm.raw[buf][2][tid];  // r, g, b, radius
-            const float A = r1.x, B = r1.y, C = r1.z, o = r1.w;
+            float2 r0;  // cx, cy
+            float A, B, C, o;
+            float4 r2;  // r, g, b, -
+            if constexpr (mode == kRenderSplatFull) {
+                const float4 w0 = sm.raw[buf][0][tid];  // cx, cy, depth, cull
+                const float4 w1 = sm.raw[buf][1][tid];  // A, B, C, opacity
+                r0 = make_float2(w0.x, w0.y);
+                A = w1.x;
+                B = w1.y;
+                C = w1.z;
+                o = w1.w;
+                r2 = sm.raw[buf][2][tid];  // r, g, b, radius
+            } else if constexpr (mode == kRenderSplatP32) {
+                const float4 w0 = sm.raw[buf][0][tid];  // cx, cy, A, B
+                const float4 w1 = sm.raw[buf][1][tid];  // C, opacity, h(r, g), h(b) | radius
+                r0 = make_float2(w0.x, w0.y);
+                A = w0.z;
+                B = w0.w;
+                C = w1.x;
+                o = w1.y;
+                const uint32_t rg = __float_as_uint(w1.z), bw = __float_as_uint(w1.w);
+                r2 = make_float4(halfLoF(rg), halfHiF(rg), halfLoF(bw), 0.0f);
+            } else {
+                const uint2* w = reinterpret_cast<const uint2*>(&sm.raw[buf][0][0]);
+                const uint2 w0 = w[tid], w1 = w[kRenderThreads + tid], w2 = w[2 * kRenderThreads + tid];
+                r0 = make_float2(__uint_as_float(w0.x), __uint_as_float(w0.y));
+                p24DecodeConic(w1.x, w1.y, A, B, C, o);
+                r2 = make_float4(halfLoF(w2.x), halfHiF(w2.x), halfLoF(w2.y), 0.0f);
+            }
             // cutoff ellipse box (makeCutoffEllipse's threshold, wider margin)
             float4 box = make_float4(-3.0e38f, 3.0e38f, -3.0e38f, 3.0e38f);
             const float D = A * C - B * B;
@@ -195,13 +245,15 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
 }
 
 // One block per frame tile.
+template <int MODE>
 __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
-    renderTile(a, *reinterpret_cast<RenderShared*>(smemRaw), blockIdx.x);
+    renderTile<MODE>(a, *reinterpret_cast<RenderShared*>(smemRaw), blockIdx.x);
 }
 
 // Persistent schedule: each block takes tiles from the frame's queue counter (reset by frame
 // begin) until the counter passes the last tile.
+template <int MODE>
 __global__ void __launch_bounds__(kRenderThreads) renderPersistentKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     RenderShared& sm = *reinterpret_cast<RenderShared*>(smemRaw);
@@ -210,21 +262,19 @@ __global__ void __launch_bounds__(kRenderThreads) renderPersistentKernel(const _
         __syncthreads();
         const uint32_t tile = sm.tile;
         if (tile >= a.totalTiles) break;
-        renderTile(a, sm, tile);
+        renderTile<MODE>(a, sm, tile);
         __syncthreads();  // every thread has read sm.tile and left the tile's shared buffers
     }
 }
 
-}  // namespace
-
-cudaError_t launchRender(const RenderArgs& a, cudaStream_t s) {
-    if (a.totalTiles == 0) return cudaSuccess;
+template <int MODE>
+cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
     static bool configured = false;
     if (!configured) {
-        cudaError_t e =
-            cudaFuncSetAttribute(renderKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sizeof(RenderShared)));
+        cudaError_t e = cudaFuncSetAttribute(renderKernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(sizeof(RenderShared)));
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(renderPersistentKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(renderPersistentKernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sizeof(RenderShared)));
         if (e != cudaSuccess) return e;
         configured = true;
@@ -233,11 +283,21 @@ cudaError_t launchRender(const RenderArgs& a, cudaStream_t s) {
         int sms = 148, dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const uint32_t grid = uint32_t(sms) * kPersistentBlocksPerSm;
-        renderPersistentKernel<<<grid < a.totalTiles ? grid : a.totalTiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
+        renderPersistentKernel<MODE>
+            <<<grid < a.totalTiles ? grid : a.totalTiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
     } else {
-        renderKernel<<<a.totalTiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
+        renderKernel<MODE><<<a.totalTiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
     }
     return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launchRender(const RenderArgs& a, cudaStream_t s) {
+    if (a.totalTiles == 0) return cudaSuccess;
+    if (a.renderSplat == kRenderSplatP32) return launchRenderMode<kRenderSplatP32>(a, s);
+    if (a.renderSplat == kRenderSplatP24) return launchRenderMode<kRenderSplatP24>(a, s);
+    return launchRenderMode<kRenderSplatFull>(a, s);
 }
 
 }  // namespace gsr

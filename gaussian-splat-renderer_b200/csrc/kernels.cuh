@@ -59,7 +59,11 @@ struct FrontArgs {
     uint32_t bounds;      // GsrTileBounds
     int binSize;          // S (16)
     uint32_t capacity;    // list entries
-    void* splats;         // DevSplat[V * N]
+    void* splats;         // DevSplat[V * N] (full render records)
+    uint32_t renderSplat; // kRenderSplatFull / P32 / P24
+    void* packed;         // packed render records [V * N] (8 or 6 words), P32 / P24
+    uint2* rects;         // [V * N] packed tile rectangles, P32 / P24
+    uint32_t* depths;     // [V * N] depth bits, P32 / P24
     float4* hints;        // [V * N] cutoff-ellipse terms of visible gaussians (coverageHint), tight/cutoff bounds
     uint32_t* tileCounts; // [V * N]
     uint32_t* offsets;    // [V * N] exclusive scan of tileCounts
@@ -119,7 +123,9 @@ struct SortArgs {
 };
 
 struct RenderArgs {
-    const void* splats;       // DevSplat[V * N]
+    const void* splats;       // DevSplat[V * N] (full render records)
+    uint32_t renderSplat;     // kRenderSplatFull / P32 / P24
+    const void* packed;       // packed render records [V * N], P32 / P24
     const uint32_t* values[2];
     const uint64_t* keys[2];
     uint32_t* ranges;         // uint2 per tile of the frame (all views)

@@ -216,12 +216,15 @@ struct GsrRenderer {
 
     // per gaussian
     DevBuf splats, hints, tileCounts, offsets, scanStatus;
+    DevBuf packedSplats, rects, depths;  // packed render records (P32 / P24) and their side arrays
     // control + plan
     DevBuf control, plan;
     // binning mode: the records' depth words (ping-pong), their sort's look-back words and plan
     DevBuf depthKeys[2], depthStatus, depthPlan;
     static constexpr uint32_t kDepthSortPasses = 4;  // 32 depth bits
     bool binning() const { return settings.list_mode == GSR_LIST_BINNING; }
+    // words of one packed render record (P32: 8, P24: 6)
+    uint32_t packedWords() const { return settings.render_splat == GSR_RENDER_SPLAT_P32 ? 8u : 6u; }
     uint32_t recordBits() const {
         const uint64_t n = uint64_t(scene.count) * std::max<size_t>(views.size(), 1);
         return n > 1 ? bitWidth(uint32_t(n - 1)) : 1u;
@@ -340,8 +343,17 @@ struct GsrRenderer {
     int ensureViews(uint32_t v) {
         if (v <= allocViews) return GSR_OK;
         const size_t n = size_t(scene.count) * v;
-        GSR_CUDA(splats.alloc(n * 48));
-        GSR_CUDA(cudaMemset(splats.p, 0, splats.bytes));
+        if (settings.render_splat == GSR_RENDER_SPLAT_FULL) {
+            GSR_CUDA(splats.alloc(n * 48));
+            GSR_CUDA(cudaMemset(splats.p, 0, splats.bytes));
+        } else {
+            GSR_CUDA(packedSplats.alloc(n * packedWords() * 4));
+            GSR_CUDA(cudaMemset(packedSplats.p, 0, packedSplats.bytes));
+            GSR_CUDA(rects.alloc(n * 8));
+            GSR_CUDA(cudaMemset(rects.p, 0, rects.bytes));
+            GSR_CUDA(depths.alloc(n * 4));
+            GSR_CUDA(cudaMemset(depths.p, 0, depths.bytes));
+        }
         GSR_CUDA(hints.alloc(n * 16));
         if (binning()) {
             for (auto& k : depthKeys) GSR_CUDA(k.alloc(n * 8));
@@ -584,6 +596,10 @@ struct GsrRenderer {
         fa.binSize = int(settings.tile_size);
         fa.capacity = l.capacity;
         fa.splats = splats.p;
+        fa.renderSplat = settings.render_splat;
+        fa.packed = packedSplats.p;
+        fa.rects = rects.as<uint2>();
+        fa.depths = depths.as<uint32_t>();
         fa.hints = hints.as<float4>();
         fa.tileCounts = tileCounts.as<uint32_t>();
         fa.offsets = offsets.as<uint32_t>();
@@ -639,6 +655,8 @@ struct GsrRenderer {
 
         RenderArgs ra{};
         ra.splats = splats.p;
+        ra.renderSplat = settings.render_splat;
+        ra.packed = packedSplats.p;
         for (int b = 0; b < 2; ++b) {
             ra.values[b] = l.values[b].as<uint32_t>();
             ra.keys[b] = l.keys[b].as<uint64_t>();
@@ -928,6 +946,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     rc = deviceTables(&r->logf);
     if (rc) return rc;
     if (settings->list_mode > GSR_LIST_GLOBAL) return fail(GSR_ERROR_INVALID_ARGUMENT, "list mode %u", settings->list_mode);
+    if (settings->render_splat > GSR_RENDER_SPLAT_P24)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "render splat mode %u", settings->render_splat);
     if (settings->raster_schedule > GSR_RASTER_PERSISTENT)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "raster schedule %u", settings->raster_schedule);
     GSR_CUDA(r->control.alloc(sizeof(DeviceControl)));
@@ -1028,10 +1048,17 @@ int gsr_read_list(GsrRenderer* r, uint32_t* keysLo, uint32_t* keysHi, uint32_t* 
         const uint32_t W = plan.lowBits, ib = plan.indexBits;
         const uint32_t lowMask = W >= 32 ? 0xFFFFFFFFu : ((1u << W) - 1u);
         // binning entries carry no depth bits: the depth comes from the gaussian's record
-        std::vector<DevSplat48> rec;
+        std::vector<uint32_t> recDepth;  // depth bits per (view, gaussian) record
         if (r->binning() && keysLo) {
-            rec.resize(size_t(r->scene.count) * r->views.size());
-            GSR_CUDA(cudaMemcpy(rec.data(), r->splats.p, rec.size() * 48, cudaMemcpyDeviceToHost));
+            const size_t records = size_t(r->scene.count) * r->views.size();
+            recDepth.resize(records);
+            if (r->settings.render_splat == GSR_RENDER_SPLAT_FULL) {
+                std::vector<DevSplat48> rec(records);
+                GSR_CUDA(cudaMemcpy(rec.data(), r->splats.p, records * 48, cudaMemcpyDeviceToHost));
+                for (size_t k = 0; k < records; ++k) recDepth[k] = rec[k].depthBits;
+            } else {
+                GSR_CUDA(cudaMemcpy(recDepth.data(), r->depths.p, records * 4, cudaMemcpyDeviceToHost));
+            }
         }
         for (uint32_t i = 0; i < n; ++i) {
             uint32_t lo, hi;
@@ -1040,11 +1067,11 @@ int gsr_read_list(GsrRenderer* r, uint32_t* keysLo, uint32_t* keysHi, uint32_t* 
                 hi = uint32_t(k[i] >> (ib + W));
                 const uint32_t g = uint32_t(k[i] & ((1ull << ib) - 1ull));
                 if (values) values[i] = g;
-                if (!rec.empty()) {
+                if (!recDepth.empty()) {
                     size_t view = 0;  // the view holding frame tile hi
                     while (view + 1 < r->views.size() && r->views[view + 1].tile_base <= hi) ++view;
                     const size_t at = view * r->scene.count + g;
-                    lo = at < rec.size() ? rec[at].depthBits : 0u;
+                    lo = at < recDepth.size() ? recDepth[at] : 0u;
                 }
             } else {
                 lo = uint32_t(k[i]);
@@ -1065,9 +1092,25 @@ int gsr_read_list(GsrRenderer* r, uint32_t* keysLo, uint32_t* keysHi, uint32_t* 
 
 int gsr_read_splats(GsrRenderer* r, void* splatsOut, uint32_t* tileCountsOut, uint32_t n) {
     if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (splatsOut && r->settings.render_splat != GSR_RENDER_SPLAT_FULL)
+        return fail(GSR_ERROR_UNSUPPORTED, "packed render splats: read them with gsr_read_packed_splats");
     GSR_CUDA(cudaDeviceSynchronize());
     n = std::min(n, r->scene.count);
     if (splatsOut) GSR_CUDA(cudaMemcpy(splatsOut, r->splats.p, size_t(n) * 48, cudaMemcpyDeviceToHost));
+    if (tileCountsOut) GSR_CUDA(cudaMemcpy(tileCountsOut, r->tileCounts.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
+    return GSR_OK;
+}
+
+int gsr_read_packed_splats(GsrRenderer* r, uint32_t* words, uint32_t* rectsOut, uint32_t* depthsOut,
+                           uint32_t* tileCountsOut, uint32_t n) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (r->settings.render_splat == GSR_RENDER_SPLAT_FULL)
+        return fail(GSR_ERROR_UNSUPPORTED, "full render splats: read them with gsr_read_splats");
+    GSR_CUDA(cudaDeviceSynchronize());
+    n = std::min(n, r->scene.count);
+    if (words) GSR_CUDA(cudaMemcpy(words, r->packedSplats.p, size_t(n) * r->packedWords() * 4, cudaMemcpyDeviceToHost));
+    if (rectsOut) GSR_CUDA(cudaMemcpy(rectsOut, r->rects.p, size_t(n) * 8, cudaMemcpyDeviceToHost));
+    if (depthsOut) GSR_CUDA(cudaMemcpy(depthsOut, r->depths.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
     if (tileCountsOut) GSR_CUDA(cudaMemcpy(tileCountsOut, r->tileCounts.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
     return GSR_OK;
 }

@@ -12,6 +12,7 @@
 #pragma once
 
 #include "gsr_device.cuh"
+#include "render_splat.cuh"
 
 namespace gsr {
 
@@ -47,6 +48,15 @@ struct __align__(16) DevSplat {
 static_assert(sizeof(DevSplat) == 48, "ProjectedSplat layout");
 
 struct TileRect { int minX, minY, maxX, maxY; };
+
+// the packed render records' tile rectangle: minX | minY << 16, maxX | maxY << 16 (packRect,
+// render_splat.glsl)
+__device__ __forceinline__ uint2 packRect(const TileRect& r) {
+    return make_uint2(uint32_t(r.minX) | (uint32_t(r.minY) << 16), uint32_t(r.maxX) | (uint32_t(r.maxY) << 16));
+}
+__device__ __forceinline__ TileRect unpackRect(uint2 w) {
+    return TileRect{int(w.x & 0xFFFFu), int(w.x >> 16), int(w.y & 0xFFFFu), int(w.y >> 16)};
+}
 
 // computeCov3D (splat_math.cpp:44-63): S[c*3 + r] = sum_k M[k][r] M[k][c], M = R diag(sigma).
 __device__ __forceinline__ void cov3d(float sx, float sy, float sz, float qr, float qx, float qy, float qz, float S[9]) {

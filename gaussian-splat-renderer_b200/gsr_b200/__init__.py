@@ -34,6 +34,7 @@ LAYOUTS = {"soa": 0, "split": 1, "aos": 2}
 BOUNDS = {"rect": 0, "tight": 1, "cutoff-only": 2}
 RASTER_SCHEDULES = {"auto": 0, "per-tile": 1, "persistent": 2}
 LIST_MODES = {"binning": 0, "global": 1}
+RENDER_SPLATS = {"full": 0, "p32": 1, "p24": 2}
 CONTROL_TIMEOUT, CONTROL_BOUNDS, CONTROL_KEY_RANGE = 1, 2, 4
 
 SPLAT_DTYPE = np.dtype(
@@ -77,7 +78,7 @@ class CSettings(C.Structure):
         ("bounds", C.c_uint32), ("tile_size", C.c_uint32), ("budget_mb", C.c_uint32), ("adaptive_list", C.c_uint32),
         ("adaptive_initial_entries", C.c_uint32), ("max_sh_degree", C.c_int32), ("output_format", C.c_uint32),
         ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("raster_schedule", C.c_uint32),
-        ("list_mode", C.c_uint32), ("reserved", C.c_uint32 * 5),
+        ("list_mode", C.c_uint32), ("render_splat", C.c_uint32), ("reserved", C.c_uint32 * 4),
     ]
 
 
@@ -189,6 +190,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_read_control": (C.c_int, [vp, C.POINTER(Control)]),
         "gsr_read_list": (C.c_int, [vp, vp, vp, vp, u32, vp, u32]),
         "gsr_read_splats": (C.c_int, [vp, vp, vp, u32]),
+        "gsr_read_packed_splats": (C.c_int, [vp, vp, vp, vp, vp, u32]),
         "gsr_read_image": (C.c_int, [vp, vp, vp]),
         "gsr_renderer_set_timing": (C.c_int, [vp, C.c_int]),
         "gsr_renderer_pass_times": (C.c_int, [vp, vp, vp, u32, C.POINTER(u32)]),
@@ -268,6 +270,7 @@ class Settings:
     use_graph: bool = False
     raster_schedule: str = "auto"
     list_mode: str = "binning"
+    render_splat: str = "full"
 
     def to_c(self) -> CSettings:
         s = CSettings()
@@ -283,6 +286,7 @@ class Settings:
         s.use_graph = int(self.use_graph)
         s.raster_schedule = RASTER_SCHEDULES[self.raster_schedule]
         s.list_mode = LIST_MODES[self.list_mode]
+        s.render_splat = RENDER_SPLATS[self.render_splat]
         return s
 
 
@@ -482,6 +486,16 @@ class Renderer:
         check(load().gsr_read_list(self._h, lo.ctypes.data, hi.ctypes.data, val.ctypes.data, n, ranges.ctypes.data,
                                    ranges.size))
         return lo[:n], hi[:n], val[:n], ranges.reshape(tiles, 2), c
+
+    def read_back_packed_splats(self, n: int, words_per_splat: int):
+        """readBackPackedSplats: (words (n, 8 or 6), rects (n, 2), depth bits (n,), tile counts (n,))."""
+        words = np.zeros((n, words_per_splat), np.uint32)
+        rects = np.zeros((n, 2), np.uint32)
+        depths = np.zeros(n, np.uint32)
+        counts = np.zeros(n, np.uint32)
+        check(load().gsr_read_packed_splats(self._h, words.ctypes.data, rects.ctypes.data, depths.ctypes.data,
+                                            counts.ctypes.data, n))
+        return words, rects, depths, counts
 
     def read_back_splats(self, n: int):
         sp = np.zeros(n, SPLAT_DTYPE)

@@ -117,8 +117,21 @@ typedef struct GsrSettings {
     uint32_t use_graph;                /* 1: launch each frame as a captured CUDA graph */
     uint32_t raster_schedule;          /* GsrRasterSchedule (no reference counterpart) */
     uint32_t list_mode;                /* GsrListMode (TileSettings' sort mode, cli.h:28) */
-    uint32_t reserved[5];
+    uint32_t render_splat;             /* GsrRenderSplat (TileSettings::renderSplat, cli.h:34) */
+    uint32_t reserved[4];
 } GsrSettings;
+
+/* The per-entry record that key emission and the rasterizer read (RenderSplatMode,
+ * splat_tile_renderer.h:87-92; layouts of shaders/render_splat.glsl). Packed records keep the
+ * tile rectangle (2 x u32: minX | minY << 16, maxX | maxY << 16) and the depth bits in arrays of
+ * their own. Colour is fp16 in both packed forms; P24 also stores the conic (x 2^12) and the
+ * opacity in fp16 and counts the covered tiles with those decoded values, so the list can
+ * differ from FULL where a splat's cutoff ellipse changes under the rounding. */
+typedef enum GsrRenderSplat {
+    GSR_RENDER_SPLAT_FULL = 0, /* the 48-byte ProjectedSplat */
+    GSR_RENDER_SPLAT_P32 = 1,  /* 32 bytes: cx, cy, a, b | c, opacity, h(r, g), h(b) | radius << 16 */
+    GSR_RENDER_SPLAT_P24 = 2   /* 24 bytes: cx, cy | h(a S, b S), h(c S, opacity) | h(r, g), h(b) | radius << 16, S = 2^12 */
+} GsrRenderSplat;
 
 /* How the (tile, depth) list is built and sorted; both give the same list, entry for entry,
  * when it fits the capacity (test_tile_raster.cpp:459-464). */
@@ -335,6 +348,11 @@ int gsr_read_list(GsrRenderer* r, uint32_t* keys_lo, uint32_t* keys_hi, uint32_t
 /* readBackSplats (splat_tile_renderer.h:188): 48-byte ProjectedSplat records (visible
  * gaussians only are written by a frame; the rest keep older contents) and tile counts. */
 int gsr_read_splats(GsrRenderer* r, void* splats, uint32_t* tile_counts, uint32_t n);
+/* readBackPackedSplats (splat_tile_renderer.h:191-192), packed render splats only: the first n
+ * gaussians' records (8 or 6 words each), rects (2 words) and depth bits; any pointer may be
+ * NULL. GSR_ERROR_UNSUPPORTED with FULL records (gsr_read_splats reads those). */
+int gsr_read_packed_splats(GsrRenderer* r, uint32_t* words, uint32_t* rects, uint32_t* depths, uint32_t* tile_counts,
+                           uint32_t n);
 /* readBackImage (splat_tile_renderer.h:194): rgba float4[W*H] and/or rgb8 uint8[W*H*3]. */
 int gsr_read_image(GsrRenderer* r, float* rgba, uint8_t* rgb8);
 /* Per-pass device time of the last frame in ms (GpuProfiler scopes), when timing is on: 5 passes
