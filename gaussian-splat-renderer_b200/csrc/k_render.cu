@@ -233,7 +233,20 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
     cpAsyncWait<0>();
     if (!inside) return;
     const size_t p = vw.pixelBase + size_t(py) * vw.width + px;
-    a.image[p] = make_float4(c0, c1, c2, 1.0f - T);
+    if (a.imageFormat == 0) {
+        reinterpret_cast<float4*>(a.image)[p] = make_float4(c0, c1, c2, 1.0f - T);
+    } else if (a.imageFormat == 1) {
+        reinterpret_cast<uint2*>(a.image)[p] = make_uint2(packHalf2(c0, c1), packHalf2(c2, 1.0f - T));
+    } else {
+        const float v[4] = {c0, c1, c2, 1.0f - T};
+        uint32_t w = 0;
+#pragma unroll
+        for (int ch = 0; ch < 4; ++ch) {
+            const float cl = v[ch] < 0.0f ? 0.0f : (v[ch] > 1.0f ? 1.0f : v[ch]);
+            w |= uint32_t(roundf(cl * 255.0f)) << (8 * ch);
+        }
+        reinterpret_cast<uint32_t*>(a.image)[p] = w;
+    }
     if (a.rgb8) {
         const float v[3] = {c0, c1, c2};
 #pragma unroll

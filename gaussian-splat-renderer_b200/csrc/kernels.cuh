@@ -129,7 +129,8 @@ struct RenderArgs {
     const uint32_t* values[2];
     const uint64_t* keys[2];
     uint32_t* ranges;         // uint2 per tile of the frame (all views)
-    float4* image;            // per view W*H at the view's pixelBase
+    void* image;              // per view W*H at the view's pixelBase: float4, half4 or uchar4 (imageFormat)
+    uint32_t imageFormat;     // 0: float4, 1: half4 (fp16 round to nearest even), 2: uchar4 (lround(clamp(v) 255))
     uint8_t* rgb8;            // per view W*H*3 at 3 * pixelBase, or null
     const DevView* views;     // [viewCount]
     uint32_t viewCount;

@@ -61,6 +61,19 @@ void setLastError(const std::string& message) { g_lastError = message; }
 
 namespace {
 
+// IEEE binary16 bits -> float, exactly (normal, subnormal, infinity, NaN)
+float halfToFloat(uint16_t h) {
+    const uint32_t sign = uint32_t(h & 0x8000u) << 16, e = (h >> 10) & 0x1Fu, m = h & 0x3FFu;
+    if (e == 0) {
+        const float v = float(m) * (1.0f / 16777216.0f);  // m 2^-24
+        return sign ? -v : v;
+    }
+    const uint32_t bits = e == 31 ? (sign | 0x7F800000u | (m << 13)) : (sign | ((e + 112u) << 23) | (m << 13));
+    float f;
+    std::memcpy(&f, &bits, 4);
+    return f;
+}
+
 int cudaFail(cudaError_t e, const char* what) {
     if (e == cudaErrorMemoryAllocation)
         return fail(GSR_ERROR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
@@ -223,6 +236,15 @@ struct GsrRenderer {
     DevBuf depthKeys[2], depthStatus, depthPlan;
     static constexpr uint32_t kDepthSortPasses = 4;  // 32 depth bits
     bool binning() const { return settings.list_mode == GSR_LIST_BINNING; }
+    // the output image: bytes per pixel, the kernel's format code, and the RGB8 companion
+    uint32_t imageBytes() const {
+        const uint32_t f = settings.output_format;
+        return f == GSR_OUTPUT_RGBA8 ? 4u : (f == GSR_OUTPUT_RGBA16F || f == GSR_OUTPUT_RGBA16F_AND_RGB8) ? 8u : 16u;
+    }
+    uint32_t imageFormatCode() const { return imageBytes() == 16 ? 0u : imageBytes() == 8 ? 1u : 2u; }
+    bool withRgb8() const {
+        return settings.output_format == GSR_OUTPUT_RGBA32F_AND_RGB8 || settings.output_format == GSR_OUTPUT_RGBA16F_AND_RGB8;
+    }
     // words of one packed render record (P32: 8, P24: 6)
     uint32_t packedWords() const { return settings.render_splat == GSR_RENDER_SPLAT_P32 ? 8u : 6u; }
     uint32_t recordBits() const {
@@ -422,8 +444,8 @@ struct GsrRenderer {
         const uint32_t tileCount = totalTiles;
         GSR_CUDA(ranges.alloc(size_t(tileCount) * 8));
         GSR_CUDA(cudaMemset(ranges.p, 0, ranges.bytes));
-        GSR_CUDA(image.alloc(size_t(pixels) * 16));
-        if (settings.output_format == GSR_OUTPUT_RGBA32F_AND_RGB8) GSR_CUDA(rgb8.alloc(size_t(pixels) * 3));
+        GSR_CUDA(image.alloc(size_t(pixels) * imageBytes()));
+        if (withRgb8()) GSR_CUDA(rgb8.alloc(size_t(pixels) * 3));
         else rgb8.release();
         ++layoutVersion;
         const uint32_t passes = passesFor(tileCount);
@@ -662,7 +684,8 @@ struct GsrRenderer {
             ra.keys[b] = l.keys[b].as<uint64_t>();
         }
         ra.ranges = ranges.as<uint32_t>();
-        ra.image = image.as<float4>();
+        ra.image = image.p;
+        ra.imageFormat = imageFormatCode();
         ra.rgb8 = rgb8.as<uint8_t>();
         ra.views = viewsDevice.as<DevView>();
         ra.viewCount = viewCount;
@@ -935,7 +958,7 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     if (settings->tile_size != 16)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "--tile-size must be 8 or 16 (a divisor of INRIA's 16-px tiles)");
     if (settings->bounds > GSR_BOUNDS_CUTOFF_ONLY) return fail(GSR_ERROR_INVALID_ARGUMENT, "bounds %u", settings->bounds);
-    if (settings->output_format > GSR_OUTPUT_RGBA32F_AND_RGB8)
+    if (settings->output_format > GSR_OUTPUT_RGBA8)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "output format %u", settings->output_format);
     auto r = std::make_unique<GsrRenderer>();
     r->scene = *scene;
@@ -1001,7 +1024,7 @@ int gsr_render_to_host(GsrRenderer* r, const GsrCamera* camera, void* host, uint
     int rc = gsr_render(r, camera, stream);
     if (rc) return rc;
     const bool rgb = r->rgb8.p != nullptr;
-    const uint64_t need = uint64_t(r->width) * r->height * (rgb ? 3 : 16);
+    const uint64_t need = uint64_t(r->width) * r->height * (rgb ? 3 : r->imageBytes());
     if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, image needs %llu",
                                    (unsigned long long)bytes, (unsigned long long)need);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1128,7 +1151,7 @@ int gsr_render_views_to_host(GsrRenderer* r, const GsrSplatCamera* cameras, uint
     int rc = gsr_render_views(r, cameras, views, stream);
     if (rc) return rc;
     const bool rgb = r->rgb8.p != nullptr;
-    const uint64_t need = r->totalPixels * (rgb ? 3 : 16);
+    const uint64_t need = r->totalPixels * (rgb ? 3 : r->imageBytes());
     if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, the views need %llu",
                                    (unsigned long long)bytes, (unsigned long long)need);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -1151,7 +1174,7 @@ int gsr_renderer_view_image(GsrRenderer* r, uint32_t view, const void** rgba, co
     if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
     if (view >= r->views.size()) return fail(GSR_ERROR_INVALID_ARGUMENT, "view %u of %zu", view, r->views.size());
     const uint64_t base = r->views[view].pixel_base;
-    if (rgba) *rgba = r->image.as<unsigned char>() + base * 16;
+    if (rgba) *rgba = r->image.as<unsigned char>() + base * r->imageBytes();
     if (rgb8) *rgb8 = r->rgb8.p ? r->rgb8.as<unsigned char>() + base * 3 : nullptr;
     return GSR_OK;
 }
@@ -1162,8 +1185,25 @@ int gsr_read_view_image(GsrRenderer* r, uint32_t view, float* rgba, uint8_t* rgb
     GSR_CUDA(cudaDeviceSynchronize());
     const GsrViewLayout& v = r->views[view];
     const size_t pixels = size_t(v.width) * v.height;
-    if (rgba)
-        GSR_CUDA(cudaMemcpy(rgba, r->image.as<unsigned char>() + v.pixel_base * 16, pixels * 16, cudaMemcpyDeviceToHost));
+    if (rgba) {
+        const uint32_t bpp = r->imageBytes();
+        if (bpp == 16) {
+            GSR_CUDA(cudaMemcpy(rgba, r->image.as<unsigned char>() + v.pixel_base * 16, pixels * 16, cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<unsigned char> raw(pixels * bpp);
+            GSR_CUDA(cudaMemcpy(raw.data(), r->image.as<unsigned char>() + v.pixel_base * bpp, raw.size(),
+                                cudaMemcpyDeviceToHost));
+            for (size_t k = 0; k < pixels * 4; ++k) {
+                if (bpp == 8) {
+                    uint16_t h;
+                    std::memcpy(&h, &raw[k * 2], 2);
+                    rgba[k] = halfToFloat(h);
+                } else {
+                    rgba[k] = float(raw[k]) / 255.0f;
+                }
+            }
+        }
+    }
     if (rgb) {
         if (!r->rgb8.p) return fail(GSR_ERROR_INVALID_ARGUMENT, "rgb8 output is off");
         GSR_CUDA(cudaMemcpy(rgb, r->rgb8.as<unsigned char>() + v.pixel_base * 3, pixels * 3, cudaMemcpyDeviceToHost));

@@ -271,6 +271,7 @@ class Settings:
     raster_schedule: str = "auto"
     list_mode: str = "binning"
     render_splat: str = "full"
+    target: str = "rgba32f"  # the output image: rgba32f, rgba16f or rgba8 (rgb8 adds the 8-bit RGB image)
 
     def to_c(self) -> CSettings:
         s = CSettings()
@@ -281,7 +282,12 @@ class Settings:
         s.adaptive_list = int(self.adaptive_list)
         s.adaptive_initial_entries = self.adaptive_initial_entries
         s.max_sh_degree = self.max_sh_degree
-        s.output_format = 1 if self.rgb8 else 0
+        if self.target == "rgba8":
+            if self.rgb8:
+                raise ValueError("the rgba8 target has no separate rgb8 image")
+            s.output_format = 4
+        else:
+            s.output_format = {"rgba32f": 0, "rgba16f": 2}[self.target] + (1 if self.rgb8 else 0)
         s.frames_in_flight = self.frames_in_flight
         s.use_graph = int(self.use_graph)
         s.raster_schedule = RASTER_SCHEDULES[self.raster_schedule]

@@ -103,7 +103,17 @@ void gsr_scene_destroy(GsrScene* scene);
 /* ---- settings (SplatSettings src/render/splat_draw.h:31-37 + TileSettings
  *      src/render/splat_tile_renderer.h:96-114) ------------------------------------------ */
 typedef enum GsrTileBounds { GSR_BOUNDS_RECT = 0, GSR_BOUNDS_TIGHT = 1, GSR_BOUNDS_CUTOFF_ONLY = 2 } GsrTileBounds;
-typedef enum GsrOutputFormat { GSR_OUTPUT_RGBA32F = 0, GSR_OUTPUT_RGBA32F_AND_RGB8 = 1 } GsrOutputFormat;
+/* The rasterizer's output image (C, 1 - T) per pixel: the render target of SplatTargetFormat
+ * (splat_draw.h:26; the reference's default is rgba16f), optionally with the 8-bit RGB image
+ * lround(clamp(C, 0, 1) * 255) that the reference's PNG writer makes (image_io.cpp:55-56).
+ * RGBA16F stores each channel as fp16 rounded to nearest even; RGBA8 as lround(clamp(v, 0, 1) * 255). */
+typedef enum GsrOutputFormat {
+    GSR_OUTPUT_RGBA32F = 0,          /* float4 per pixel */
+    GSR_OUTPUT_RGBA32F_AND_RGB8 = 1, /* float4 + uint8 x 3 */
+    GSR_OUTPUT_RGBA16F = 2,          /* half4 per pixel */
+    GSR_OUTPUT_RGBA16F_AND_RGB8 = 3, /* half4 + uint8 x 3 */
+    GSR_OUTPUT_RGBA8 = 4             /* uint8 x 4 per pixel */
+} GsrOutputFormat;
 
 typedef struct GsrSettings {
     uint32_t bounds;                   /* GsrTileBounds; reference default tight (cli.h) */
@@ -228,11 +238,13 @@ int gsr_renderer_resize(GsrRenderer* r, uint32_t width, uint32_t height);
 int gsr_render(GsrRenderer* r, const GsrCamera* camera, void* stream);
 /* The same frame from a precomputed SplatCamera (tests that share one camera with the oracle). */
 int gsr_render_splat_camera(GsrRenderer* r, const GsrSplatCamera* camera, void* stream);
-/* Device pointers of the last frame's outputs: rgba = float4[W*H] (C, 1 - T), rgb8 = uint8[W*H*3]
- * (lround(clamp(C, 0, 1) * 255), NULL unless GSR_OUTPUT_RGBA32F_AND_RGB8). */
+/* Device pointers of the last frame's outputs: rgba = the output image (C, 1 - T) in the settings'
+ * format (float4, half4 or uint8 x 4 per pixel), rgb8 = uint8[W*H*3] (lround(clamp(C, 0, 1) *
+ * 255), NULL unless an _AND_RGB8 format). */
 int gsr_renderer_image(GsrRenderer* r, const void** rgba, const void** rgb8, uint32_t* width, uint32_t* height);
-/* The end-to-end call for host callers: render and copy the RGB8 (or RGBA32F when rgb8 output is
- * off) image into `host` (pinned or pageable; `bytes` must match), then synchronize `stream`. */
+/* The end-to-end call for host callers: render and copy the RGB8 image (or the output image in
+ * its format when rgb8 output is off) into `host` (pinned or pageable; `bytes` must match), then
+ * synchronize `stream`. */
 int gsr_render_to_host(GsrRenderer* r, const GsrCamera* camera, void* host, uint64_t bytes, void* stream);
 
 /* ---- batched views (no reference counterpart: the reference renders one camera per frame) ---
@@ -326,7 +338,9 @@ int gsr_autotune(const GsrSceneDesc* scene, const GsrSettings* settings, const G
                  const GsrSplatCamera* cameras, uint32_t count, const uint32_t* depths, uint32_t depth_count,
                  uint32_t frames, GsrTuneResult* out);
 
-/* Synchronizes and copies view `view`'s images to the host (either pointer may be NULL). */
+/* Synchronizes and copies view `view`'s images to the host (either pointer may be NULL); rgba
+ * receives float4 per pixel whatever the output format (fp16 and 8-bit values converted exactly:
+ * v / 255 for RGBA8). */
 int gsr_read_view_image(GsrRenderer* r, uint32_t view, float* rgba, uint8_t* rgb8);
 /* The end-to-end call for batched host callers: render the views and copy every view's RGB8
  * (or RGBA32F when rgb8 output is off) image into `host`, view after view at pixel_base
