@@ -168,7 +168,7 @@ __device__ __forceinline__ void shColour(const FrontArgs& a, uint32_t i, const C
 // the colour model or falls back to shColour.
 template <int GEOM, int COLOR, bool LEARNED>
 __device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, const DevCamera& cam, uint32_t i, DevSplat& s,
-                                                  TileRect& rect, ColourJob& job) {
+                                                  TileRect& rect, ColourJob& job, float4* ray) {
     const float4 pa = loadPosAlpha<GEOM>(a.scene, i);
     const float* v = cam.v;
     const float t[3] = {v[0] * pa.x + v[4] * pa.y + v[8] * pa.z + v[12], v[1] * pa.x + v[5] * pa.y + v[9] * pa.z + v[13],
@@ -205,6 +205,13 @@ __device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, const DevC
     s.conicC = conic[2];
     s.opacity = pa.w;
     s.radius = radius;
+    if (ray) {  // StopThePop: the ray-depth parameters of the visible gaussian
+        float4 rp[3];
+        rayDepthParams(sigma, q, t, cam, rp);
+        ray[0] = rp[0];
+        ray[1] = rp[1];
+        ray[2] = rp[2];
+    }
     return kCullVisible;
 }
 
@@ -289,9 +296,10 @@ __device__ __forceinline__ void writePackedSplat(const FrontArgs& a, size_t rec,
     a.depths[rec] = __float_as_uint(s.depth);
 }
 
-// PACKED: packed render records (p32 / p24, told apart at run time) instead of the 48-byte
-// record; a compile-time switch so that the default kernel carries none of their code.
-template <int GEOM, int COLOR, bool LEARNED, bool PACKED>
+// EXTRAS: the optional outputs, told apart at run time: packed render records (p32 / p24) instead
+// of the 48-byte record, and the StopThePop ray-depth parameters. A compile-time switch, so that
+// the default kernel carries none of their code.
+template <int GEOM, int COLOR, bool LEARNED, bool EXTRAS>
 __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __grid_constant__ FrontArgs a) {
     __shared__ DevCamera sCam;  // the view's camera, read once per block from its device copy
     __shared__ uint32_t sCull[kCullReasonCount];
@@ -323,7 +331,9 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
     DevSplat s;
     TileRect rect{0, 0, 0, 0};
     ColourJob job{};
-    if (i < a.count) reason = preprocessOne<GEOM, COLOR, LEARNED>(a, sCam, i, s, rect, job);
+    if (i < a.count)
+        reason = preprocessOne<GEOM, COLOR, LEARNED>(a, sCam, i, s, rect, job,
+                                                     EXTRAS && a.rayDepth ? a.rayDepth + rec * 3 : nullptr);
     if constexpr (LEARNED) learnedColour<COLOR>(a, *sl, i, reason == kCullVisible, job, s);  // warp-collective
     if (i < a.count) {
         uint32_t count = 0;
@@ -332,7 +342,7 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
             // them in fp16, so its tiles are counted with the decoded values
             float cA = s.conicA, cB = s.conicB, cC = s.conicC, cO = s.opacity;
             uint32_t p24w0 = 0, p24w1 = 0;
-            if (PACKED && a.renderSplat == kRenderSplatP24) {
+            if (EXTRAS && a.renderSplat == kRenderSplatP24) {
                 p24ConicWords(cA, cB, cC, cO, p24w0, p24w1);
                 p24DecodeConic(p24w0, p24w1, cA, cB, cC, cO);
             }
@@ -341,7 +351,7 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
             count = coverageCount(cv, g, a.binSize);
             if (a.bounds != kBoundsRect) a.hints[rec] = coverageHint(cv, g);
             s.cullReason = kCullVisible;
-            if (!PACKED) reinterpret_cast<DevSplat*>(a.splats)[rec] = s;
+            if (!EXTRAS || a.renderSplat == kRenderSplatFull) reinterpret_cast<DevSplat*>(a.splats)[rec] = s;
             else writePackedSplat(a, rec, s, rect, p24w0, p24w1);
             dmin = dmax = __float_as_uint(s.depth);  // positive: the bits order like the values
         }
@@ -561,12 +571,12 @@ cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capaci
 namespace {
 template <int GEOM, int COLOR>
 void launchPreprocess(const FrontArgs& a, dim3 blocks, cudaStream_t s) {
-    const bool packed = a.renderSplat != kRenderSplatFull;
+    const bool extras = a.renderSplat != kRenderSplatFull || a.rayDepth != nullptr;
     if (a.latents) {
-        if (packed) preprocessKernel<GEOM, COLOR, true, true><<<blocks, kFrontThreads, 0, s>>>(a);
+        if (extras) preprocessKernel<GEOM, COLOR, true, true><<<blocks, kFrontThreads, 0, s>>>(a);
         else preprocessKernel<GEOM, COLOR, true, false><<<blocks, kFrontThreads, 0, s>>>(a);
     } else {
-        if (packed) preprocessKernel<GEOM, COLOR, false, true><<<blocks, kFrontThreads, 0, s>>>(a);
+        if (extras) preprocessKernel<GEOM, COLOR, false, true><<<blocks, kFrontThreads, 0, s>>>(a);
         else preprocessKernel<GEOM, COLOR, false, false><<<blocks, kFrontThreads, 0, s>>>(a);
     }
 }

@@ -80,10 +80,105 @@ __device__ __forceinline__ uint32_t viewOfTile(const RenderArgs& a, uint32_t t) 
 }
 
 // The whole per-tile pass for frame tile `tile`; every thread of the block calls it.
+// StopThePop's per-pixel window (tile_render.comp:201-279): the pixel's K = a.sortWindow pending
+// splats ordered by their ray depth (nearest first, ties in list order), in CAP >= K register
+// slots. While fewer than K wait, a splat is inserted; once K wait, the nearest of the window and
+// the new splat is blended (the usual test-before-accept rule) and the other one takes its place.
+// The rest is blended nearest first at the end of the list. Every loop runs over the constant CAP
+// with K as a predicate, so the slots stay in registers for CAP <= 16.
+template <int CAP>
+struct SortWindow {
+    float d[CAP], al[CAP], r[CAP], g[CAP], b[CAP];
+    uint32_t count = 0;
+};
+__device__ __forceinline__ void blendOver(float alpha, float r, float g, float b, float& T, float& c0, float& c1,
+                                          float& c2, bool& done) {
+    const float testT = T * (1.0f - alpha);
+    if (testT < kMinTransmittance) {
+        done = true;
+        return;
+    }
+    const float w = alpha * T;
+    c0 += r * w;
+    c1 += g * w;
+    c2 += b * w;
+    T = testT;
+}
+template <int CAP>
+__device__ __forceinline__ void windowPush(SortWindow<CAP>& q, uint32_t K, float depth, float alpha, float4 col,
+                                           float& T, float& c0, float& c1, float& c2, bool& done) {
+    if (!(depth < 3.0e38f)) depth = 3.0e38f;  // finite (NaN / infinity of a degenerate splat)
+    if (q.count < K) {
+        // not full: insertion from the back
+        bool placed = false;
+#pragma unroll
+        for (int i = CAP - 1; i > 0; --i) {
+            if (uint32_t(i) < K && !placed) {
+                if (uint32_t(i - 1) < q.count && q.d[i - 1] > depth) {
+                    q.d[i] = q.d[i - 1];
+                    q.al[i] = q.al[i - 1];
+                    q.r[i] = q.r[i - 1];
+                    q.g[i] = q.g[i - 1];
+                    q.b[i] = q.b[i - 1];
+                } else if (uint32_t(i - 1) < q.count) {
+                    q.d[i] = depth;
+                    q.al[i] = alpha;
+                    q.r[i] = col.x;
+                    q.g[i] = col.y;
+                    q.b[i] = col.z;
+                    placed = true;
+                }
+            }
+        }
+        if (!placed) {
+            q.d[0] = depth;
+            q.al[0] = alpha;
+            q.r[0] = col.x;
+            q.g[0] = col.y;
+            q.b[0] = col.z;
+        }
+        ++q.count;
+        return;
+    }
+    // full: the nearest of the window and the new splat leaves it and is blended now
+    if (depth < q.d[0]) {
+        blendOver(alpha, col.x, col.y, col.z, T, c0, c1, c2, done);
+        return;
+    }
+    blendOver(q.al[0], q.r[0], q.g[0], q.b[0], T, c0, c1, c2, done);
+    // slots move left while they are not farther than the new splat; it takes the first other
+    // slot, or the last one (K - 1). (One loop: a separate "store at K - 1" loop is turned into an
+    // indexed store by the compiler, which moves the window to local memory.)
+    bool placed = false;
+#pragma unroll
+    for (int i = 0; i < CAP; ++i) {
+        if (!placed && uint32_t(i) < K) {
+            if (i + 1 < CAP && uint32_t(i + 1) < K && q.d[i + 1 < CAP ? i + 1 : i] <= depth) {
+                const int n = i + 1 < CAP ? i + 1 : i;
+                q.d[i] = q.d[n];
+                q.al[i] = q.al[n];
+                q.r[i] = q.r[n];
+                q.g[i] = q.g[n];
+                q.b[i] = q.b[n];
+            } else {
+                q.d[i] = depth;
+                q.al[i] = alpha;
+                q.r[i] = col.x;
+                q.g[i] = col.y;
+                q.b[i] = col.z;
+                placed = true;
+            }
+        }
+    }
+}
+
 // MODE: the record layout (kRenderSplatFull / P32 / P24), a compile-time parameter so that each
 // layout's kernel carries only its own gather and decode (a runtime switch measured 8 % slower).
-template <int MODE>
-__device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm, uint32_t tile) {
+// CAP: 0, or the StopThePop window's register capacity; `ray` is then the shared area of the
+// gathered ray-depth parameters (3 x 16 B per entry, double-buffered).
+template <int MODE, int CAP>
+__device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm, float4 (*ray)[3][kRenderThreads],
+                                           uint32_t tile) {
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t view = viewOfTile(a, tile);
     const DevView vw = a.views[view];
@@ -137,9 +232,23 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
                 cpAsync8(&dst[kRenderThreads + tid], rec + 1);
                 cpAsync8(&dst[2 * kRenderThreads + tid], rec + 2);
             }
+            if constexpr (CAP > 0) {
+                const float4* rp = a.rayDepth + (size_t(view) * a.count + g) * 3;
+                cpAsync16(&ray[buf][0][tid], rp);
+                cpAsync16(&ray[buf][1][tid], rp + 1);
+                cpAsync16(&ray[buf][2][tid], rp + 2);
+            }
         }
         cpAsyncCommit();
     };
+    // StopThePop: the pixel's ray t (vx, vy, 1) in camera space (pixel = f x / z + (size - 1) / 2)
+    SortWindow<(CAP > 0 ? CAP : 1)> window;
+    const uint32_t K = a.sortWindow;
+    float vx = 0.0f, vy = 0.0f;
+    if constexpr (CAP > 0) {
+        vx = (fx - 0.5f * (float(vw.width) - 1.0f)) / a.cam[view].focalX;
+        vy = (fy - 0.5f * (float(vw.height) - 1.0f)) / a.cam[view].focalY;
+    }
 
     int buf = 0;
     if (range.x < range.y) issue(range.x, 0);
@@ -216,6 +325,17 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
                 if (power2 > 0.0f) continue;
                 const float alpha = fminf(kMaxAlpha, co.w * fastExp2(power2));
                 if (alpha < (1.0f / 255.0f)) continue;
+                if constexpr (CAP > 0) {
+                    // the depth of the gaussian's maximum along the pixel ray: (v . b) / (v^T P v)
+                    const float4 pa = ray[buf][0][q], pb = ray[buf][1][q];
+                    const float pc = ray[buf][2][q].x;
+                    const float vPv = pa.x * vx * vx + 2.0f * pa.y * vx * vy + 2.0f * pa.z * vx + pa.w * vy * vy +
+                                      2.0f * pb.x * vy + pb.y;
+                    const float vb = pb.z * vx + pb.w * vy + pc;
+                    windowPush(window, K, vb / vPv, alpha, sm.color[q], T, c0, c1, c2, done);
+                    if (done) break;
+                    continue;
+                }
                 const float testT = T * (1.0f - alpha);
                 if (testT < kMinTransmittance) {
                     done = true;
@@ -229,6 +349,11 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
                 T = testT;
             }
         }
+    }
+    if constexpr (CAP > 0) {  // the end of the list: what waits is blended, nearest first
+#pragma unroll
+        for (int i = 0; i < CAP; ++i)
+            if (!done && uint32_t(i) < window.count) blendOver(window.al[i], window.r[i], window.g[i], window.b[i], T, c0, c1, c2, done);
     }
     cpAsyncWait<0>();
     if (!inside) return;
@@ -258,15 +383,25 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
 }
 
 // One block per frame tile.
-template <int MODE>
+// the shared area of a StopThePop kernel: the ray-depth parameters after RenderShared
+template <int CAP>
+constexpr size_t renderSmemBytes() {
+    return sizeof(RenderShared) + (CAP > 0 ? sizeof(float4) * 2 * 3 * kRenderThreads : 0);
+}
+__device__ __forceinline__ float4 (*rayArea(unsigned char* smem))[3][kRenderThreads] {
+    return reinterpret_cast<float4(*)[3][kRenderThreads]>(smem + sizeof(RenderShared));
+}
+
+template <int MODE, int CAP>
 __global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
-    renderTile<MODE>(a, *reinterpret_cast<RenderShared*>(smemRaw), blockIdx.x);
+    renderTile<MODE, CAP>(a, *reinterpret_cast<RenderShared*>(smemRaw), CAP > 0 ? rayArea(smemRaw) : nullptr,
+                          blockIdx.x);
 }
 
 // Persistent schedule: each block takes tiles from the frame's queue counter (reset by frame
 // begin) until the counter passes the last tile.
-template <int MODE>
+template <int MODE, int CAP>
 __global__ void __launch_bounds__(kRenderThreads) renderPersistentKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     RenderShared& sm = *reinterpret_cast<RenderShared*>(smemRaw);
@@ -275,20 +410,19 @@ __global__ void __launch_bounds__(kRenderThreads) renderPersistentKernel(const _
         __syncthreads();
         const uint32_t tile = sm.tile;
         if (tile >= a.totalTiles) break;
-        renderTile<MODE>(a, sm, tile);
+        renderTile<MODE, CAP>(a, sm, CAP > 0 ? rayArea(smemRaw) : nullptr, tile);
         __syncthreads();  // every thread has read sm.tile and left the tile's shared buffers
     }
 }
 
-template <int MODE>
+template <int MODE, int CAP>
 cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
+    constexpr size_t smem = renderSmemBytes<CAP>();
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(renderKernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             int(sizeof(RenderShared)));
+        cudaError_t e = cudaFuncSetAttribute(renderKernel<MODE, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(renderPersistentKernel<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(sizeof(RenderShared)));
+        e = cudaFuncSetAttribute(renderPersistentKernel<MODE, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
         configured = true;
     }
@@ -296,21 +430,29 @@ cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
         int sms = 148, dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const uint32_t grid = uint32_t(sms) * kPersistentBlocksPerSm;
-        renderPersistentKernel<MODE>
-            <<<grid < a.totalTiles ? grid : a.totalTiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
+        renderPersistentKernel<MODE, CAP><<<grid < a.totalTiles ? grid : a.totalTiles, kRenderThreads, smem, s>>>(a);
     } else {
-        renderKernel<MODE><<<a.totalTiles, kRenderThreads, sizeof(RenderShared), s>>>(a);
+        renderKernel<MODE, CAP><<<a.totalTiles, kRenderThreads, smem, s>>>(a);
     }
     return cudaGetLastError();
+}
+
+// the window capacity for K: 4, 16 or 64 register slots
+template <int MODE>
+cudaError_t launchRenderWindow(const RenderArgs& a, cudaStream_t s) {
+    if (a.sortWindow == 0) return launchRenderMode<MODE, 0>(a, s);
+    if (a.sortWindow <= 4) return launchRenderMode<MODE, 4>(a, s);
+    if (a.sortWindow <= 16) return launchRenderMode<MODE, 16>(a, s);
+    return launchRenderMode<MODE, 64>(a, s);
 }
 
 }  // namespace
 
 cudaError_t launchRender(const RenderArgs& a, cudaStream_t s) {
     if (a.totalTiles == 0) return cudaSuccess;
-    if (a.renderSplat == kRenderSplatP32) return launchRenderMode<kRenderSplatP32>(a, s);
-    if (a.renderSplat == kRenderSplatP24) return launchRenderMode<kRenderSplatP24>(a, s);
-    return launchRenderMode<kRenderSplatFull>(a, s);
+    if (a.renderSplat == kRenderSplatP32) return launchRenderWindow<kRenderSplatP32>(a, s);
+    if (a.renderSplat == kRenderSplatP24) return launchRenderWindow<kRenderSplatP24>(a, s);
+    return launchRenderWindow<kRenderSplatFull>(a, s);
 }
 
 }  // namespace gsr

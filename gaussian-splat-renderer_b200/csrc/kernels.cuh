@@ -63,6 +63,7 @@ struct FrontArgs {
     uint32_t renderSplat; // kRenderSplatFull / P32 / P24
     void* packed;         // packed render records [V * N] (8 or 6 words), P32 / P24
     uint2* rects;         // [V * N] packed tile rectangles, P32 / P24
+    float4* rayDepth;     // [V * N * 3] StopThePop ray-depth parameters of visible gaussians, or null
     uint32_t* depths;     // [V * N] depth bits, P32 / P24
     float4* hints;        // [V * N] cutoff-ellipse terms of visible gaussians (coverageHint), tight/cutoff bounds
     uint32_t* tileCounts; // [V * N]
@@ -126,6 +127,9 @@ struct RenderArgs {
     const void* splats;       // DevSplat[V * N] (full render records)
     uint32_t renderSplat;     // kRenderSplatFull / P32 / P24
     const void* packed;       // packed render records [V * N], P32 / P24
+    const float4* rayDepth;   // [V * N * 3] StopThePop ray-depth parameters (sortWindow > 0)
+    const DevCameraArgs* cam; // the frame's cameras [viewCount] (focal lengths of the pixel rays)
+    uint32_t sortWindow;      // StopThePop window K, 0 = off
     const uint32_t* values[2];
     const uint64_t* keys[2];
     uint32_t* ranges;         // uint2 per tile of the frame (all views)

@@ -230,6 +230,7 @@ struct GsrRenderer {
     // per gaussian
     DevBuf splats, hints, tileCounts, offsets, scanStatus;
     DevBuf packedSplats, rects, depths;  // packed render records (P32 / P24) and their side arrays
+    DevBuf rayDepth;                     // StopThePop ray-depth parameters (3 x float4 per record)
     // control + plan
     DevBuf control, plan;
     // binning mode: the records' depth words (ping-pong), their sort's look-back words and plan
@@ -377,6 +378,7 @@ struct GsrRenderer {
             GSR_CUDA(cudaMemset(depths.p, 0, depths.bytes));
         }
         GSR_CUDA(hints.alloc(n * 16));
+        if (settings.sort_window > 0) GSR_CUDA(rayDepth.alloc(n * 48));
         if (binning()) {
             for (auto& k : depthKeys) GSR_CUDA(k.alloc(n * 8));
             GSR_CUDA(depthStatus.alloc(size_t(kDepthSortPasses) * ((n + kDepthSortTile - 1) / kDepthSortTile) * 256 * 8));
@@ -622,6 +624,7 @@ struct GsrRenderer {
         fa.packed = packedSplats.p;
         fa.rects = rects.as<uint2>();
         fa.depths = depths.as<uint32_t>();
+        fa.rayDepth = settings.sort_window > 0 ? rayDepth.as<float4>() : nullptr;
         fa.hints = hints.as<float4>();
         fa.tileCounts = tileCounts.as<uint32_t>();
         fa.offsets = offsets.as<uint32_t>();
@@ -679,6 +682,9 @@ struct GsrRenderer {
         ra.splats = splats.p;
         ra.renderSplat = settings.render_splat;
         ra.packed = packedSplats.p;
+        ra.rayDepth = rayDepth.as<float4>();
+        ra.cam = slot.camDevice.as<DevCameraArgs>();
+        ra.sortWindow = settings.sort_window;
         for (int b = 0; b < 2; ++b) {
             ra.values[b] = l.values[b].as<uint32_t>();
             ra.keys[b] = l.keys[b].as<uint64_t>();
@@ -969,6 +975,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     rc = deviceTables(&r->logf);
     if (rc) return rc;
     if (settings->list_mode > GSR_LIST_GLOBAL) return fail(GSR_ERROR_INVALID_ARGUMENT, "list mode %u", settings->list_mode);
+    if (settings->sort_window > 64)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "sort window %u (at most 64)", settings->sort_window);
     if (settings->render_splat > GSR_RENDER_SPLAT_P24)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "render splat mode %u", settings->render_splat);
     if (settings->raster_schedule > GSR_RASTER_PERSISTENT)

@@ -140,6 +140,48 @@ __device__ __forceinline__ TileRect tileRect(float px, float py, float radius, u
     return t;
 }
 
+// computeRayDepthParams (splat_math.cpp:195-205) for the StopThePop window: with M = the upper-left
+// 3x3 of viewInria times quaternionToMatrix(q) (the gaussian's axes in camera space), s = sigma
+// clamped below at max(1e-4 max(sigma), 1e-12) and w = 1 / s^2, P = sum_k w_k M_k M_k^T (k = 0, 1,
+// 2 added to a zero matrix) and b = P tCam. The depth of the gaussian's maximum along the pixel
+// ray t (vx, vy, 1) is then (v . b) / (v^T P v). out: (P00, P01, P02, P11), (P12, P22, b0, b1),
+// (b2, 0, 0, 0).
+__device__ __forceinline__ void rayDepthParams(const float sigma[3], const float q[4], const float t[3],
+                                               const DevCamera& cam, float4 out[3]) {
+    const float r = q[0], x = q[1], y = q[2], z = q[3];
+    float R[9];  // R[c*3 + row], quaternionToMatrix
+    R[0] = 1.0f - 2.0f * (y * y + z * z); R[1] = 2.0f * (x * y + r * z); R[2] = 2.0f * (x * z - r * y);
+    R[3] = 2.0f * (x * y - r * z); R[4] = 1.0f - 2.0f * (x * x + z * z); R[5] = 2.0f * (y * z + r * x);
+    R[6] = 2.0f * (x * z + r * y); R[7] = 2.0f * (y * z - r * x); R[8] = 1.0f - 2.0f * (x * x + y * y);
+    float M[9];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int row = 0; row < 3; ++row)
+            M[c * 3 + row] = cam.v[0 * 4 + row] * R[c * 3 + 0] + cam.v[1 * 4 + row] * R[c * 3 + 1] + cam.v[2 * 4 + row] * R[c * 3 + 2];
+    const float sMax = smax(sigma[0], smax(sigma[1], sigma[2]));
+    const float floorS = smax(1e-4f * sMax, 1e-12f);
+    float w[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float sk = smax(sigma[k], floorS);
+        w[k] = 1.0f / (sk * sk);
+    }
+    float P[9] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int i = 0; i < 3; ++i)
+#pragma unroll
+            for (int j = 0; j < 3; ++j) P[i * 3 + j] = P[i * 3 + j] + w[k] * (M[k * 3 + j] * M[k * 3 + i]);
+    float b[3];
+#pragma unroll
+    for (int row = 0; row < 3; ++row) b[row] = P[0 * 3 + row] * t[0] + P[1 * 3 + row] * t[1] + P[2 * 3 + row] * t[2];
+    out[0] = make_float4(P[0], P[1], P[2], P[4]);
+    out[1] = make_float4(P[5], P[8], b[0], b[1]);
+    out[2] = make_float4(b[2], 0.0f, 0.0f, 0.0f);
+}
+
 // evalSH (splat_math.cpp:129-151) over 16 coefficient triplets sh[k*3 + c] (only the first
 // (degree+1)^2 are read).
 __device__ __forceinline__ void evalSH(int degree, const float* sh, float dx, float dy, float dz, float out[3]) {

@@ -78,7 +78,8 @@ class CSettings(C.Structure):
         ("bounds", C.c_uint32), ("tile_size", C.c_uint32), ("budget_mb", C.c_uint32), ("adaptive_list", C.c_uint32),
         ("adaptive_initial_entries", C.c_uint32), ("max_sh_degree", C.c_int32), ("output_format", C.c_uint32),
         ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("raster_schedule", C.c_uint32),
-        ("list_mode", C.c_uint32), ("render_splat", C.c_uint32), ("reserved", C.c_uint32 * 4),
+        ("list_mode", C.c_uint32), ("render_splat", C.c_uint32), ("sort_window", C.c_uint32),
+        ("reserved", C.c_uint32 * 3),
     ]
 
 
@@ -272,6 +273,7 @@ class Settings:
     list_mode: str = "binning"
     render_splat: str = "full"
     target: str = "rgba32f"  # the output image: rgba32f, rgba16f or rgba8 (rgb8 adds the 8-bit RGB image)
+    sort_window: int = 0  # StopThePop per-pixel window K (0 = off, at most 64)
 
     def to_c(self) -> CSettings:
         s = CSettings()
@@ -293,6 +295,7 @@ class Settings:
         s.raster_schedule = RASTER_SCHEDULES[self.raster_schedule]
         s.list_mode = LIST_MODES[self.list_mode]
         s.render_splat = RENDER_SPLATS[self.render_splat]
+        s.sort_window = self.sort_window
         return s
 
 

@@ -128,7 +128,9 @@ typedef struct GsrSettings {
     uint32_t raster_schedule;          /* GsrRasterSchedule (no reference counterpart) */
     uint32_t list_mode;                /* GsrListMode (TileSettings' sort mode, cli.h:28) */
     uint32_t render_splat;             /* GsrRenderSplat (TileSettings::renderSplat, cli.h:34) */
-    uint32_t reserved[4];
+    uint32_t sort_window;              /* StopThePop per-pixel window K (TileSettings::sortWindow, cli.h:46):
+                                          0 = off (the list's order), 1..64 */
+    uint32_t reserved[3];
 } GsrSettings;
 
 /* The per-entry record that key emission and the rasterizer read (RenderSplatMode,

@@ -641,7 +641,41 @@ uint32_t gsr_oracle_depth_sort(uint32_t n, const float* posAlpha, const float* V
     return m;
 }
 
-/* ---- renderReference (reference_renderer.cpp:41-234), StopThePop window off ------------- */
+/* ---- computeRayDepthParams (splat_math.cpp:195-205) and RayDepthParams::depthAt
+ *      (splat_math.h:134-141), the StopThePop window's per-gaussian ray depth ------------- */
+static void rayDepthParams(const float* sigma, const float* q, const float t[3], const float* V, float out[9]) {
+    const float r = q[0], x = q[1], y = q[2], z = q[3];
+    float R[9]; /* quaternionToMatrix, R[c*3 + row] */
+    R[0] = 1.0f - 2.0f * (y * y + z * z); R[1] = 2.0f * (x * y + r * z); R[2] = 2.0f * (x * z - r * y);
+    R[3] = 2.0f * (x * y - r * z); R[4] = 1.0f - 2.0f * (x * x + z * z); R[5] = 2.0f * (y * z + r * x);
+    R[6] = 2.0f * (x * z + r * y); R[7] = 2.0f * (y * z - r * x); R[8] = 1.0f - 2.0f * (x * x + y * y);
+    float M[9]; /* mat3(viewInria) * R */
+    for (int c = 0; c < 3; ++c)
+        for (int row = 0; row < 3; ++row)
+            M[c * 3 + row] = M4(V, 0, row) * R[c * 3 + 0] + M4(V, 1, row) * R[c * 3 + 1] + M4(V, 2, row) * R[c * 3 + 2];
+    const float sMax = smax(sigma[0], smax(sigma[1], sigma[2]));
+    const float floorS = smax(1e-4f * sMax, 1e-12f);
+    float w[3];
+    for (int k = 0; k < 3; ++k) {
+        const float sk = smax(sigma[k], floorS);
+        w[k] = 1.0f / (sk * sk);
+    }
+    float P[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < 3; ++k)
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) P[i * 3 + j] = P[i * 3 + j] + w[k] * (M[k * 3 + j] * M[k * 3 + i]);
+    float b[3];
+    for (int row = 0; row < 3; ++row) b[row] = P[0 * 3 + row] * t[0] + P[1 * 3 + row] * t[1] + P[2 * 3 + row] * t[2];
+    const float o[9] = {P[0], P[1], P[2], P[4], P[5], P[8], b[0], b[1], b[2]};
+    memcpy(out, o, sizeof(o));
+}
+static float rayDepthAt(const float* p, float vx, float vy) {
+    const float vPv = p[0] * vx * vx + 2.0f * p[1] * vx * vy + 2.0f * p[2] * vx + p[3] * vy * vy + 2.0f * p[4] * vy + p[5];
+    const float vb = p[6] * vx + p[7] * vy + p[8];
+    return vb / vPv;
+}
+
+/* ---- renderReference (reference_renderer.cpp:41-234), with the StopThePop window -------- */
 typedef struct {
     uint32_t n, K;
     int degree;
@@ -661,8 +695,90 @@ typedef struct {
     const uint32_t *tileStart, *tileLists;
     float* rgb;
     int earlyTermination;
+    uint32_t sortWindow;    /* 0: off; GSR_ORACLE_EXACT_PIXEL_SORT: every pixel sorts all its splats */
+    const float* rayDepth;  /* 9 floats per gaussian (rayDepthParams) */
     _Atomic uint64_t evaluated, blended, terminated;
 } RasterCtx;
+
+typedef struct {
+    float depth, alpha, color[3];
+} Pending;
+
+/* the reference's blend lambda (reference_renderer.cpp:150-159) */
+static void blendPending(const Pending* e, float* T, float* C, int* done, uint64_t* bl, uint64_t* te) {
+    const float testT = *T * (1.0f - e->alpha);
+    if (testT < kMinTransmittance) {
+        *done = 1;
+        ++*te;
+        return;
+    }
+    for (int ch = 0; ch < 3; ++ch) C[ch] = C[ch] + e->color[ch] * e->alpha * *T;
+    *T = testT;
+    ++*bl;
+}
+
+/* std::stable_sort by depth (a.depth < b.depth): a bottom-up merge sort */
+static void stableSortByDepth(Pending* a, size_t n) {
+    if (n < 2) return;
+    Pending* tmp = (Pending*)malloc(sizeof(Pending) * n);
+    for (size_t w = 1; w < n; w *= 2) {
+        for (size_t lo = 0; lo < n; lo += 2 * w) {
+            const size_t mid = lo + w < n ? lo + w : n, hi = lo + 2 * w < n ? lo + 2 * w : n;
+            size_t i = lo, j = mid, k = lo;
+            while (i < mid && j < hi) tmp[k++] = (a[j].depth < a[i].depth) ? a[j++] : a[i++];
+            while (i < mid) tmp[k++] = a[i++];
+            while (j < hi) tmp[k++] = a[j++];
+        }
+        memcpy(a, tmp, sizeof(Pending) * n);
+    }
+    free(tmp);
+}
+
+/* One pixel with the window (reference_renderer.cpp:143-196). */
+static void windowPixel(const RasterCtx* c, uint32_t s0, uint32_t s1, float px, float py, Pending* win, float* T,
+                        float* C, uint64_t* ev, uint64_t* bl, uint64_t* te) {
+    const GsrOracleCamera* cam = c->cam;
+    const float vx = (px - 0.5f * ((float)cam->width - 1.0f)) / cam->focalX;
+    const float vy = (py - 0.5f * ((float)cam->height - 1.0f)) / cam->focalY;
+    const int exact = c->sortWindow == GSR_ORACLE_EXACT_PIXEL_SORT;
+    const size_t K = c->sortWindow;
+    size_t wn = 0;
+    int done = 0;
+    for (uint32_t j = s0; j < s1 && !done; ++j) {
+        const uint32_t g = c->tileLists[j];
+        const GsrOracleSplat* s = &c->splats[g];
+        ++*ev;
+        const float dx = s->center[0] - px;
+        const float dy = s->center[1] - py;
+        const float* co = s->conicOpacity;
+        const float power = -0.5f * (co[0] * dx * dx + co[2] * dy * dy) - co[1] * dx * dy;
+        if (power > 0.0f) continue;
+        const float alpha = fminf(kMaxAlpha, co[3] * expf(power));
+        if (alpha < kMinAlpha) continue;
+        Pending e;
+        e.depth = rayDepthAt(c->rayDepth + (size_t)g * 9, vx, vy);
+        e.alpha = alpha;
+        memcpy(e.color, s->color, sizeof(e.color));
+        if (exact) {
+            win[wn++] = e;
+        } else if (wn == K) {
+            if (e.depth < win[0].depth) {
+                blendPending(&e, T, C, &done, bl, te);
+                continue;
+            }
+            blendPending(&win[0], T, C, &done, bl, te);
+            size_t i = 0;
+            for (; i + 1 < K && win[i + 1].depth <= e.depth; ++i) win[i] = win[i + 1];
+            win[i] = e;
+        } else {
+            size_t i = wn++;
+            for (; i > 0 && win[i - 1].depth > e.depth; --i) win[i] = win[i - 1];
+            win[i] = e;
+        }
+    }
+    if (exact) stableSortByDepth(win, wn);
+    for (size_t i = 0; i < wn && !done; ++i) blendPending(&win[i], T, C, &done, bl, te);
+}
 static void rasterTask(uint32_t tile, void* p) {
     RasterCtx* c = (RasterCtx*)p;
     const GsrOracleCamera* cam = c->cam;
@@ -672,10 +788,21 @@ static void rasterTask(uint32_t tile, void* p) {
     const uint32_t x0 = tx * kTileSize, y0 = ty * kTileSize;
     const uint32_t x1 = cam->width < x0 + kTileSize ? cam->width : x0 + kTileSize;
     const uint32_t y1 = cam->height < y0 + kTileSize ? cam->height : y0 + kTileSize;
+    Pending* win = NULL;
+    if (c->sortWindow > 0) {
+        const size_t cap = c->sortWindow == GSR_ORACLE_EXACT_PIXEL_SORT ? (size_t)(s1 - s0) : c->sortWindow;
+        win = (Pending*)malloc(sizeof(Pending) * (cap ? cap : 1));
+    }
     for (uint32_t y = y0; y < y1; ++y) {
         for (uint32_t x = x0; x < x1; ++x) {
             const float px = (float)x, py = (float)y;
             float T = 1.0f, C[3] = {0.0f, 0.0f, 0.0f};
+            if (win) {
+                windowPixel(c, s0, s1, px, py, win, &T, C, &ev, &bl, &te);
+                float* dst = &c->rgb[((size_t)y * cam->width + x) * 3];
+                for (int ch = 0; ch < 3; ++ch) dst[ch] = C[ch] + T * 0.0f;
+                continue;
+            }
             for (uint32_t j = s0; j < s1; ++j) {
                 const GsrOracleSplat* s = &c->splats[c->tileLists[j]];
                 ++ev;
@@ -701,6 +828,7 @@ static void rasterTask(uint32_t tile, void* p) {
             for (int ch = 0; ch < 3; ++ch) dst[ch] = C[ch] + T * 0.0f;
         }
     }
+    free(win);
     atomic_fetch_add(&c->evaluated, ev);
     atomic_fetch_add(&c->blended, bl);
     atomic_fetch_add(&c->terminated, te);
@@ -708,7 +836,7 @@ static void rasterTask(uint32_t tile, void* p) {
 
 int gsr_oracle_render(uint32_t n, int shDegree, const float* posAlpha, const float* scales, const float* rotations,
                       const float* sh, const GsrOracleCamera* cam, int maxShDegree, uint32_t bounds, uint32_t threads,
-                      int earlyTermination, float* rgb, GsrOracleRenderStats* stats) {
+                      int earlyTermination, uint32_t sortWindow, float* rgb, GsrOracleRenderStats* stats) {
     const double tStart = nowMs();
     const unsigned nt = threads ? threads : hardwareThreads();
     const uint32_t K = (uint32_t)((shDegree + 1) * (shDegree + 1));
@@ -727,6 +855,20 @@ int gsr_oracle_render(uint32_t n, int shDegree, const float* posAlpha, const flo
             case GSR_ORACLE_CULL_SINGULAR: st.culledSingular++; break;
             case GSR_ORACLE_CULL_OFFSCREEN: st.culledOffScreen++; break;
             default: break;
+        }
+    }
+    /* StopThePop: the ray-depth parameters of every visible gaussian (reference_renderer.cpp:60-70) */
+    float* rayDepth = NULL;
+    if (sortWindow > 0) {
+        rayDepth = (float*)calloc((size_t)(n ? n : 1) * 9, sizeof(float));
+        const float* V = cam->viewInria;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (splats[i].cullReason != GSR_ORACLE_CULL_VISIBLE) continue;
+            const float* pa = posAlpha + 4 * (size_t)i;
+            const float t[3] = {M4(V, 0, 0) * pa[0] + M4(V, 1, 0) * pa[1] + M4(V, 2, 0) * pa[2] + M4(V, 3, 0),
+                                M4(V, 0, 1) * pa[0] + M4(V, 1, 1) * pa[1] + M4(V, 2, 1) * pa[2] + M4(V, 3, 1),
+                                M4(V, 0, 2) * pa[0] + M4(V, 1, 2) * pa[1] + M4(V, 2, 2) * pa[2] + M4(V, 3, 2)};
+            rayDepthParams(scales + 4 * (size_t)i, rotations + 4 * (size_t)i, t, V, rayDepth + (size_t)i * 9);
         }
     }
     const double tPre = nowMs();
@@ -774,6 +916,8 @@ int gsr_oracle_render(uint32_t n, int shDegree, const float* posAlpha, const flo
             rc.tileLists = lists;
             rc.rgb = rgb;
             rc.earlyTermination = earlyTermination;
+            rc.sortWindow = sortWindow;
+            rc.rayDepth = rayDepth;
             atomic_init(&rc.evaluated, 0);
             atomic_init(&rc.blended, 0);
             atomic_init(&rc.terminated, 0);
@@ -791,6 +935,7 @@ int gsr_oracle_render(uint32_t n, int shDegree, const float* posAlpha, const flo
             free(lists);
         }
     }
+    free(rayDepth);
     free(tiles);
     free(tileStart);
     free(order);

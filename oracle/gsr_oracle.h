@@ -88,9 +88,13 @@ uint64_t gsr_oracle_tile_list(uint32_t n, const GsrOracleSplat* splats, const ui
                               uint32_t* keysLo, uint32_t* keysHi, uint32_t* values, uint32_t* ranges);
 
 /* renderReference (reference_renderer.cpp:41-234), image = W*H*3 floats, row 0 = top. */
+/* sortWindow: 0 = the list's order, K = StopThePop's per-pixel window of K splats, or
+ * GSR_ORACLE_EXACT_PIXEL_SORT = every pixel sorts all its splats by ray depth
+ * (ReferenceOptions::sortWindow, reference_renderer.h:41-46). */
+#define GSR_ORACLE_EXACT_PIXEL_SORT 0xFFFFFFFFu
 int gsr_oracle_render(uint32_t n, int shDegree, const float* posAlpha, const float* scales, const float* rotations,
                       const float* sh, const GsrOracleCamera* cam, int maxShDegree, uint32_t bounds, uint32_t threads,
-                      int earlyTermination, float* rgb, GsrOracleRenderStats* stats);
+                      int earlyTermination, uint32_t sortWindow, float* rgb, GsrOracleRenderStats* stats);
 
 /* DepthSorter (depth_sort.cpp). */
 uint32_t gsr_oracle_depth_sort(uint32_t n, const float* posAlpha, const float* viewInria, uint32_t* order,

@@ -35,6 +35,7 @@ assert SPLAT_DTYPE.itemsize == 48
 
 CULL_VISIBLE, CULL_NEAR, CULL_SINGULAR, CULL_OFFSCREEN, CULL_LOW_OPACITY = range(5)
 BOUNDS_RECT, BOUNDS_TIGHT, BOUNDS_CUTOFF = range(3)
+EXACT_PIXEL_SORT = 0xFFFFFFFF  # renderReference's kExactPixelSort
 
 
 class Camera(C.Structure):
@@ -209,13 +210,16 @@ class Oracle:
                 "ranges": ranges.reshape(tiles, 2)}
 
     # ---- whole frame -----------------------------------------------------------------
-    def render(self, scene, cam: Camera, max_sh_degree=3, bounds=BOUNDS_RECT, threads=0, early_termination=True):
+    def render(self, scene, cam: Camera, max_sh_degree=3, bounds=BOUNDS_RECT, threads=0, early_termination=True,
+               sort_window=0):
+        """renderReference; sort_window: 0 = the list's order, K = StopThePop's per-pixel window,
+        EXACT_PIXEL_SORT = every pixel sorts all its splats by ray depth."""
         rgb = np.zeros(cam.width * cam.height * 3, np.float32)
         st = RenderStats()
         rc = self._render(
             C.c_uint32(scene.count), C.c_int(scene.sh_degree), _p(scene.pos_alpha), _p(scene.scales),
             _p(scene.rotations), _p(scene.sh), C.byref(cam), C.c_int(max_sh_degree), C.c_uint32(bounds),
-            C.c_uint32(threads), C.c_int(int(early_termination)), _p(rgb), C.byref(st),
+            C.c_uint32(threads), C.c_int(int(early_termination)), C.c_uint32(sort_window), _p(rgb), C.byref(st),
         )
         if rc != 0:
             raise RuntimeError("oracle render failed")

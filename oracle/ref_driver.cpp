@@ -170,7 +170,7 @@ int gsr_ref_coverage_borderline(const void* splat, const RefCamera* camera, uint
 // renderReference (src/splat/reference_renderer.cpp:41-234): rgb = W*H*3 floats.
 int gsr_ref_render(uint32_t n, int shDegree, const float* posAlpha, const float* scales, const float* rotations,
                    const float* sh, const RefCamera* camera, int maxShDegree, uint32_t bounds, uint32_t threads,
-                   int earlyTermination, float* rgb, RefRenderStats* stats) {
+                   int earlyTermination, uint32_t sortWindow, float* rgb, RefRenderStats* stats) {
     try {
         const gsr::GaussianScene scene = makeScene(n, shDegree, posAlpha, scales, rotations, sh);
         gsr::ReferenceOptions o;
@@ -178,6 +178,7 @@ int gsr_ref_render(uint32_t n, int shDegree, const float* posAlpha, const float*
         o.bounds = gsr::TileBounds(bounds);
         o.threads = threads;
         o.earlyTermination = earlyTermination != 0;
+        o.sortWindow = sortWindow;
         const gsr::ReferenceImage img = gsr::renderReference(scene, toCamera(*camera), o);
         std::memcpy(rgb, img.rgb.data(), img.rgb.size() * sizeof(float));
         if (stats) {

@@ -1,6 +1,7 @@
 """Pins the C restatement (oracle/gsr_oracle.c) to the reference renderer's own CPU sources
 compiled in place (oracle/_ref), bit for bit: camera, preprocess, tight coverage (all three
-bounds modes, 16- and 8-px bins), the whole renderReference image and statistics, the depth
+bounds modes, 16- and 8-px bins), the whole renderReference image and statistics (also with the
+StopThePop window), the depth
 sort and radixSortPairs, half conversion, and every scene format's words and decode."""
 import numpy as np
 import pytest
@@ -60,6 +61,21 @@ def test_render_image_and_stats(port, ref, scenes_and_cams, bounds):
         for k in ("visible", "culledNear", "culledSingular", "culledOffScreen", "tileInstances", "evaluatedFragments",
                   "blendedFragments", "terminatedPixels"):
             assert sp[k] == sr[k], k
+
+
+@pytest.mark.parametrize("window", [1, 4, 16, 0xFFFFFFFF])
+def test_render_with_the_stopthepop_window(port, ref, scenes_and_cams, window):
+    """renderReference with ReferenceOptions::sortWindow (reference_renderer.cpp:143-196): the
+    per-pixel window of K splats ordered by ray depth, and the exact per-pixel sort."""
+    for scene, c in scenes_and_cams[:2]:
+        cp, cr = _cam_pair(port, ref, c)
+        ip, sp = port.render(scene, cp, bounds=1, threads=4, sort_window=window)
+        ir, sr = ref.render(scene, cr, bounds=1, threads=4, sort_window=window)
+        assert ip.tobytes() == ir.tobytes()
+        for k in ("evaluatedFragments", "blendedFragments", "terminatedPixels"):
+            assert sp[k] == sr[k], k
+        plain, _ = port.render(scene, cp, bounds=1, threads=4)
+        assert ip.tobytes() != plain.tobytes()  # the window reorders blends
 
 
 def test_gpu_culls_extend_the_cpu_preprocess(port, ref, scenes_and_cams):
