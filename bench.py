@@ -261,7 +261,8 @@ def run_b200(args, dist: Dist):
     scene, cams, fmt, layout = make_config(args.config)
     gs = G.GpuScene(scene, fmt, layout)
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, list_mode=args.list_mode,
-                                  render_splat=args.render_splat))
+                                  render_splat=args.render_splat, sort_window=args.sort_window,
+                                  tile_size=args.tile_size))
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     first = (dist.rank * 37) % len(cams)
@@ -405,7 +406,8 @@ def tune(args, G, gs, cams, first: int, model=None):
         return {"views_per_frame": args.batch, "raster_schedule": "auto", "table": None}
     probe = G.camera_array([cams[(first + k) % len(cams)] for k in range(32)])
     settings = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
-                          list_mode=args.list_mode, render_splat=args.render_splat)
+                          list_mode=args.list_mode, render_splat=args.render_splat, sort_window=args.sort_window,
+                          tile_size=args.tile_size)
     return G.autotune(gs, settings, probe, depths=(1, 2, 4, 8, 16), frames=4, model=model)
 
 
@@ -423,7 +425,8 @@ def run_batched(args, dist: Dist, G, gs, cams, first: int, stream, plain_rendere
     nframes = len(frames)
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
                                   raster_schedule=tuned["raster_schedule"], list_mode=args.list_mode,
-                                  render_splat=args.render_splat))
+                                  render_splat=args.render_splat, sort_window=args.sort_window,
+                                  tile_size=args.tile_size))
     if model is not None:
         r.set_color_model(model)
     # warm-up: at least the requested views, then until the adaptive list keeps its capacity for
@@ -510,6 +513,8 @@ def main():
                     help="list construction: one (tile, depth) sort, or depth sort + emission + tile sort")
     ap.add_argument("--render-splat", default="full", choices=["full", "p32", "p24"],
                     help="the per-entry record of emission and render: 48 B, or packed 32 / 24 B")
+    ap.add_argument("--sort-window", type=int, default=0, help="StopThePop per-pixel window K (0: off)")
+    ap.add_argument("--tile-size", type=int, default=16, choices=[8, 16], help="binning / render tile in pixels")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")

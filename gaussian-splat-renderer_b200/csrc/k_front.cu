@@ -325,7 +325,8 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
     __syncthreads();
     const uint32_t i = blockIdx.x * kFrontThreads + tid;
     const size_t rec = size_t(view) * a.count + i;
-    const int gx = int(sCam.tilesX) * (16 / a.binSize), gy = int(sCam.tilesY) * (16 / a.binSize);
+    // the binning grid: ceil(size / S) bins (INRIA's rectangles stay on the 16-px tiles)
+    const int gx = (int(sCam.width) + a.binSize - 1) / a.binSize, gy = (int(sCam.height) + a.binSize - 1) / a.binSize;
     uint32_t reason = kCullReasonCount;  // threads past the end
     uint32_t dmin = 0xFFFFFFFFu, dmax = 0;
     DevSplat s;
@@ -424,7 +425,7 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
         const KeyLayout lay = keyLayout(a.ctl, sentinel, a.count, BINNING);
         const uint32_t offset = a.offsets[slot];
         const DevView vw = a.views[view];
-        const int gx = int(vw.tilesX) * (16 / a.binSize), gy = int(vw.tilesY) * (16 / a.binSize);
+        const int gx = int(vw.tilesX), gy = int(vw.tilesY);  // the view's binning grid
         // centre, conic, rectangle and depth from the record (full) or the packed arrays
         float cx, cy, cA, cB, cC;
         TileRect rect;
@@ -436,7 +437,7 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
             cA = s.conicA;
             cB = s.conicB;
             cC = s.conicC;
-            rect = tileRect(s.cx, s.cy, s.radius, vw.tilesX, vw.tilesY);
+            rect = tileRect(s.cx, s.cy, s.radius, (vw.width + 15) / 16, (vw.height + 15) / 16);
             depthBits = __float_as_uint(s.depth);
         } else {
             rect = unpackRect(a.rects[rec]);

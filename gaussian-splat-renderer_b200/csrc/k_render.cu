@@ -57,15 +57,17 @@ __device__ __forceinline__ float fastExp2(float x) {
     return y;
 }
 
+// N = the batch (one entry per thread of the tile's block)
+template <int N>
 struct RenderShared {
-    // gathered records, double-buffered: full 3 x 16 B, p32 2 x 16 B, p24 3 x 8 B (as uint2 in the
-    // first half of each row)
-    float4 raw[2][3][kRenderThreads];
-    float4 conic[kRenderThreads];      // a', b', c' (pre-scaled), opacity
-    float4 box[kRenderThreads];        // x0, x1, y0, y1 of the cutoff ellipse (pixels)
-    float4 color[kRenderThreads];      // r, g, b, -
-    float2 center[kRenderThreads];
-    uint32_t tile;                     // persistent schedule: the block's current tile
+    // gathered records, double-buffered: full 3 x 16 B, p32 2 x 16 B, p24 3 x 8 B (as uint2 rows of
+    // N in the first half of the area)
+    float4 raw[2][3][N];
+    float4 conic[N];      // a', b', c' (pre-scaled), opacity
+    float4 box[N];        // x0, x1, y0, y1 of the cutoff ellipse (pixels)
+    float4 color[N];      // r, g, b, -
+    float2 center[N];
+    uint32_t tile;        // persistent schedule: the block's current tile
 };
 
 // The view holding frame tile t: the last view whose tileBase <= t (views are in tile order).
@@ -176,15 +178,19 @@ __device__ __forceinline__ void windowPush(SortWindow<CAP>& q, uint32_t K, float
 // layout's kernel carries only its own gather and decode (a runtime switch measured 8 % slower).
 // CAP: 0, or the StopThePop window's register capacity; `ray` is then the shared area of the
 // gathered ray-depth parameters (3 x 16 B per entry, double-buffered).
-template <int MODE, int CAP>
-__device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm, float4 (*ray)[3][kRenderThreads],
-                                           uint32_t tile) {
+// TILE: the tile's edge, 16 (INRIA's tiles) or 8 pixels; one thread per pixel, batches of TILE^2
+// entries, and each warp owns 32 / TILE rows of the tile (its strip).
+template <int MODE, int CAP, int TILE>
+__device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TILE * TILE>& sm,
+                                           float4 (*ray)[3][TILE * TILE], uint32_t tile) {
+    constexpr uint32_t kThreads = TILE * TILE, kRows = 32 / TILE;
+    static_assert(kThreads <= kRenderThreads && kRows * TILE == 32, "tile shape");
     const uint32_t tid = threadIdx.x, warp = tid >> 5;
     const uint32_t view = viewOfTile(a, tile);
     const DevView vw = a.views[view];
     const uint32_t local = tile - vw.tileBase;
     const uint32_t tx = local % vw.tilesX, ty = local / vw.tilesX;
-    const uint32_t px = tx * 16 + (tid & 15), py = ty * 16 + (tid >> 4);
+    const uint32_t px = tx * TILE + (tid % TILE), py = ty * TILE + (tid / TILE);
     const bool inside = px < vw.width && py < vw.height;
     uint2 range = reinterpret_cast<const uint2*>(a.ranges)[tile];
     // a frame whose look-back gave up (GSR_CONTROL_TIMEOUT) has meaningless ranges: every index
@@ -203,8 +209,8 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
     constexpr int mode = MODE;
     const float fx = float(px), fy = float(py);
     // this warp's pixel strip
-    const float wx0 = float(tx * 16), wx1 = float(tx * 16 + 15);
-    const float wy0 = float(ty * 16 + 2 * warp), wy1 = wy0 + 1.0f;
+    const float wx0 = float(tx * TILE), wx1 = float(tx * TILE + TILE - 1);
+    const float wy0 = float(ty * TILE + kRows * warp), wy1 = wy0 + float(kRows - 1);
     float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
     bool done = !inside;
 
@@ -229,8 +235,8 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
                 const uint2* rec = records24 + size_t(g) * 3;
                 uint2* dst = reinterpret_cast<uint2*>(&sm.raw[buf][0][0]);
                 cpAsync8(&dst[tid], rec);
-                cpAsync8(&dst[kRenderThreads + tid], rec + 1);
-                cpAsync8(&dst[2 * kRenderThreads + tid], rec + 2);
+                cpAsync8(&dst[kThreads + tid], rec + 1);
+                cpAsync8(&dst[2 * kThreads + tid], rec + 2);
             }
             if constexpr (CAP > 0) {
                 const float4* rp = a.rayDepth + (size_t(view) * a.count + g) * 3;
@@ -252,10 +258,10 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
 
     int buf = 0;
     if (range.x < range.y) issue(range.x, 0);
-    for (uint32_t start = range.x; start < range.y; start += kRenderThreads, buf ^= 1) {
-        if (__syncthreads_count(done) == kRenderThreads) break;
+    for (uint32_t start = range.x; start < range.y; start += kThreads, buf ^= 1) {
+        if (__syncthreads_count(done) == int(kThreads)) break;
         // prefetch the next batch while this one is prepared and blended
-        const uint32_t next = start + kRenderThreads;
+        const uint32_t next = start + kThreads;
         if (next < range.y) issue(next, buf ^ 1);
         else cpAsyncCommit();
         cpAsyncWait<1>();
@@ -285,7 +291,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
                 r2 = make_float4(halfLoF(rg), halfHiF(rg), halfLoF(bw), 0.0f);
             } else {
                 const uint2* w = reinterpret_cast<const uint2*>(&sm.raw[buf][0][0]);
-                const uint2 w0 = w[tid], w1 = w[kRenderThreads + tid], w2 = w[2 * kRenderThreads + tid];
+                const uint2 w0 = w[tid], w1 = w[kThreads + tid], w2 = w[2 * kThreads + tid];
                 r0 = make_float2(__uint_as_float(w0.x), __uint_as_float(w0.y));
                 p24DecodeConic(w1.x, w1.y, A, B, C, o);
                 r2 = make_float4(halfLoF(w2.x), halfHiF(w2.x), halfLoF(w2.y), 0.0f);
@@ -312,7 +318,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
             sm.center[tid] = make_float2(r0.x, r0.y);
         }
         __syncthreads();
-        const uint32_t n = range.y - start < uint32_t(kRenderThreads) ? range.y - start : uint32_t(kRenderThreads);
+        const uint32_t n = range.y - start < kThreads ? range.y - start : kThreads;
         if (!done) {
             for (uint32_t q = 0; q < n; ++q) {
                 const float4 bx = sm.box[q];
@@ -383,76 +389,85 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared& sm
 }
 
 // One block per frame tile.
-// the shared area of a StopThePop kernel: the ray-depth parameters after RenderShared
-template <int CAP>
+// the shared area of a block: RenderShared, then for a StopThePop kernel the ray-depth parameters
+template <int CAP, int N>
 constexpr size_t renderSmemBytes() {
-    return sizeof(RenderShared) + (CAP > 0 ? sizeof(float4) * 2 * 3 * kRenderThreads : 0);
+    return sizeof(RenderShared<N>) + (CAP > 0 ? sizeof(float4) * 2 * 3 * N : 0);
 }
-__device__ __forceinline__ float4 (*rayArea(unsigned char* smem))[3][kRenderThreads] {
-    return reinterpret_cast<float4(*)[3][kRenderThreads]>(smem + sizeof(RenderShared));
+template <int N>
+__device__ __forceinline__ float4 (*rayArea(unsigned char* smem))[3][N] {
+    return reinterpret_cast<float4(*)[3][N]>(smem + sizeof(RenderShared<N>));
 }
 
-template <int MODE, int CAP>
-__global__ void __launch_bounds__(kRenderThreads) renderKernel(const __grid_constant__ RenderArgs a) {
+template <int MODE, int CAP, int TILE>
+__global__ void __launch_bounds__(TILE * TILE) renderKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
-    renderTile<MODE, CAP>(a, *reinterpret_cast<RenderShared*>(smemRaw), CAP > 0 ? rayArea(smemRaw) : nullptr,
-                          blockIdx.x);
+    renderTile<MODE, CAP, TILE>(a, *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw),
+                                CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, blockIdx.x);
 }
 
 // Persistent schedule: each block takes tiles from the frame's queue counter (reset by frame
 // begin) until the counter passes the last tile.
-template <int MODE, int CAP>
-__global__ void __launch_bounds__(kRenderThreads) renderPersistentKernel(const __grid_constant__ RenderArgs a) {
+template <int MODE, int CAP, int TILE>
+__global__ void __launch_bounds__(TILE * TILE) renderPersistentKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
-    RenderShared& sm = *reinterpret_cast<RenderShared*>(smemRaw);
+    RenderShared<TILE * TILE>& sm = *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw);
     for (;;) {
         if (threadIdx.x == 0) sm.tile = atomicAdd(&a.ctl->tickets[kRenderQueueTicket], 1u);
         __syncthreads();
         const uint32_t tile = sm.tile;
         if (tile >= a.totalTiles) break;
-        renderTile<MODE, CAP>(a, sm, CAP > 0 ? rayArea(smemRaw) : nullptr, tile);
+        renderTile<MODE, CAP, TILE>(a, sm, CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, tile);
         __syncthreads();  // every thread has read sm.tile and left the tile's shared buffers
     }
 }
 
-template <int MODE, int CAP>
+template <int MODE, int CAP, int TILE>
 cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
-    constexpr size_t smem = renderSmemBytes<CAP>();
+    constexpr size_t smem = renderSmemBytes<CAP, TILE * TILE>();
+    constexpr uint32_t threads = TILE * TILE;
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(renderKernel<MODE, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaError_t e =
+            cudaFuncSetAttribute(renderKernel<MODE, CAP, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(renderPersistentKernel<MODE, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        e = cudaFuncSetAttribute(renderPersistentKernel<MODE, CAP, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(smem));
         if (e != cudaSuccess) return e;
         configured = true;
     }
     if (a.persistent) {
         int sms = 148, dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const uint32_t grid = uint32_t(sms) * kPersistentBlocksPerSm;
-        renderPersistentKernel<MODE, CAP><<<grid < a.totalTiles ? grid : a.totalTiles, kRenderThreads, smem, s>>>(a);
+        // as many resident threads per SM for either tile size
+        const uint32_t grid = uint32_t(sms) * kPersistentBlocksPerSm * (kRenderThreads / threads);
+        renderPersistentKernel<MODE, CAP, TILE><<<grid < a.totalTiles ? grid : a.totalTiles, threads, smem, s>>>(a);
     } else {
-        renderKernel<MODE, CAP><<<a.totalTiles, kRenderThreads, smem, s>>>(a);
+        renderKernel<MODE, CAP, TILE><<<a.totalTiles, threads, smem, s>>>(a);
     }
     return cudaGetLastError();
 }
 
 // the window capacity for K: 4, 16 or 64 register slots
-template <int MODE>
+template <int MODE, int TILE>
 cudaError_t launchRenderWindow(const RenderArgs& a, cudaStream_t s) {
-    if (a.sortWindow == 0) return launchRenderMode<MODE, 0>(a, s);
-    if (a.sortWindow <= 4) return launchRenderMode<MODE, 4>(a, s);
-    if (a.sortWindow <= 16) return launchRenderMode<MODE, 16>(a, s);
-    return launchRenderMode<MODE, 64>(a, s);
+    if (a.sortWindow == 0) return launchRenderMode<MODE, 0, TILE>(a, s);
+    if (a.sortWindow <= 4) return launchRenderMode<MODE, 4, TILE>(a, s);
+    if (a.sortWindow <= 16) return launchRenderMode<MODE, 16, TILE>(a, s);
+    return launchRenderMode<MODE, 64, TILE>(a, s);
+}
+template <int MODE>
+cudaError_t launchRenderTile(const RenderArgs& a, cudaStream_t s) {
+    return a.tileSize == 8 ? launchRenderWindow<MODE, 8>(a, s) : launchRenderWindow<MODE, 16>(a, s);
 }
 
 }  // namespace
 
 cudaError_t launchRender(const RenderArgs& a, cudaStream_t s) {
     if (a.totalTiles == 0) return cudaSuccess;
-    if (a.renderSplat == kRenderSplatP32) return launchRenderWindow<kRenderSplatP32>(a, s);
-    if (a.renderSplat == kRenderSplatP24) return launchRenderWindow<kRenderSplatP24>(a, s);
-    return launchRenderWindow<kRenderSplatFull>(a, s);
+    if (a.renderSplat == kRenderSplatP32) return launchRenderTile<kRenderSplatP32>(a, s);
+    if (a.renderSplat == kRenderSplatP24) return launchRenderTile<kRenderSplatP24>(a, s);
+    return launchRenderTile<kRenderSplatFull>(a, s);
 }
 
 }  // namespace gsr

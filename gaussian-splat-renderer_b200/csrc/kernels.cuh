@@ -24,7 +24,7 @@ struct DevCameraArgs {  // = DevCamera (splat_math.cuh)
 // image buffers. Per-gaussian arrays (records, tile counts, offsets) are indexed v * N + g.
 struct DevView {
     uint32_t tileBase;
-    uint32_t tilesX, tilesY;
+    uint32_t tilesX, tilesY;  // the binning / render tiles of the view (tile_size pixels)
     uint32_t width, height;
     uint32_t pad;
     uint64_t pixelBase;
@@ -130,6 +130,7 @@ struct RenderArgs {
     const float4* rayDepth;   // [V * N * 3] StopThePop ray-depth parameters (sortWindow > 0)
     const DevCameraArgs* cam; // the frame's cameras [viewCount] (focal lengths of the pixel rays)
     uint32_t sortWindow;      // StopThePop window K, 0 = off
+    uint32_t tileSize;        // the render tile: 16 (INRIA) or 8 pixels
     const uint32_t* values[2];
     const uint64_t* keys[2];
     uint32_t* ranges;         // uint2 per tile of the frame (all views)

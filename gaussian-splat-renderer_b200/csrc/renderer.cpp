@@ -411,7 +411,8 @@ struct GsrRenderer {
             if (w[i] == 0 || h[i] == 0 || w[i] > 32768 || h[i] > 32768)
                 return fail(GSR_ERROR_INVALID_ARGUMENT, "render size %ux%u", w[i], h[i]);
             if (same && (views[i].width != w[i] || views[i].height != h[i])) same = false;
-            tiles += uint64_t((w[i] + 15) / 16) * ((h[i] + 15) / 16);
+            const uint32_t S = settings.tile_size;  // the binning / render tiles
+            tiles += uint64_t((w[i] + S - 1) / S) * ((h[i] + S - 1) / S);
             pixels += uint64_t(w[i]) * h[i];
         }
         if (same) return GSR_OK;
@@ -427,8 +428,8 @@ struct GsrRenderer {
             GsrViewLayout& L = views[i];
             L.width = w[i];
             L.height = h[i];
-            L.tiles_x = (w[i] + 15) / 16;
-            L.tiles_y = (h[i] + 15) / 16;
+            L.tiles_x = (w[i] + settings.tile_size - 1) / settings.tile_size;
+            L.tiles_y = (h[i] + settings.tile_size - 1) / settings.tile_size;
             L.tile_base = tileBase;
             L.pixel_base = pixelBase;
             dv[i] = DevView{L.tile_base, L.tiles_x, L.tiles_y, L.width, L.height, 0, L.pixel_base};
@@ -534,7 +535,7 @@ struct GsrRenderer {
             if (rc) return rc;
         }
         for (uint32_t i = 0; i < v; ++i)
-            if (cams[i].tiles_x != views[i].tiles_x || cams[i].tiles_y != views[i].tiles_y)
+            if (cams[i].tiles_x != (views[i].width + 15) / 16 || cams[i].tiles_y != (views[i].height + 15) / 16)
                 return fail(GSR_ERROR_INVALID_ARGUMENT, "camera %u: tiles %ux%u for a %ux%u image", i, cams[i].tiles_x,
                             cams[i].tiles_y, cams[i].width, cams[i].height);
         if (slots.empty()) return fail(GSR_ERROR_INVALID_ARGUMENT, "renderer not initialised");
@@ -685,6 +686,7 @@ struct GsrRenderer {
         ra.rayDepth = rayDepth.as<float4>();
         ra.cam = slot.camDevice.as<DevCameraArgs>();
         ra.sortWindow = settings.sort_window;
+        ra.tileSize = settings.tile_size;
         for (int b = 0; b < 2; ++b) {
             ra.values[b] = l.values[b].as<uint32_t>();
             ra.keys[b] = l.keys[b].as<uint64_t>();
@@ -959,9 +961,7 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     *out = nullptr;
     int rc = validateScene(*scene);
     if (rc) return rc;
-    if (settings->tile_size == 8)
-        return fail(GSR_ERROR_UNSUPPORTED, "--tile-size 8 is not implemented by this build (16 only)");
-    if (settings->tile_size != 16)
+    if (settings->tile_size != 8 && settings->tile_size != 16)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "--tile-size must be 8 or 16 (a divisor of INRIA's 16-px tiles)");
     if (settings->bounds > GSR_BOUNDS_CUTOFF_ONLY) return fail(GSR_ERROR_INVALID_ARGUMENT, "bounds %u", settings->bounds);
     if (settings->output_format > GSR_OUTPUT_RGBA8)
