@@ -178,6 +178,9 @@ __global__ void encodeKernel(const __grid_constant__ EncodeArgs a, const uint8_t
                     const uint32_t h = floatToHalf(shValue(a, i, kept, k, ch));
                     c[hi / 2] = (hi & 1u) ? ((c[hi / 2] & 0x0000FFFFu) | (h << 16)) : ((c[hi / 2] & 0xFFFF0000u) | h);
                 }
+        } else if (a.color == GSR_COLOR_CODEBOOK) {  // DC + the codebook entry (scene_compression.cpp:309-314)
+            c[0] = packHalf2(shValue(a, i, kept, 0, 0), shValue(a, i, kept, 0, 1));
+            c[1] = uint32_t(floatToHalf(shValue(a, i, kept, 0, 2))) | ((a.cbIndex ? a.cbIndex[i] : 0u) << 16);
         } else {  // q8
             c[0] = packHalf2(shValue(a, i, kept, 0, 0), shValue(a, i, kept, 0, 1));
             uint16_t bandScale[4] = {0, 0, 0, 0};
@@ -196,21 +199,21 @@ __global__ void encodeKernel(const __grid_constant__ EncodeArgs a, const uint8_t
             const uint32_t restDims = (a.K - 1) * 3;
             for (uint32_t j = 0; j < restDims; ++j) c[3 + j / 4] |= uint32_t(uint8_t(q[j])) << (8 * (j % 4));
         }
+        // variable degree: the degree in word 7, plus the compacted colour offset in the split
+        // layout (scene_compression.cpp:320-337); cb records stay fixed-size (degree only)
+        const bool compact = a.variable && a.layout == GSR_LAYOUT_SPLIT && a.color != GSR_COLOR_CODEBOOK;
         uint32_t colorWords = a.colorWords;
-        if (a.variable) {
-            if (a.layout == GSR_LAYOUT_SPLIT) {
-                g[7] = (d << 30) | offsets[i];
-                colorWords = colorWordsFor(a.color, kept);
-            } else {
-                g[7] = d << 30;
-            }
+        if (compact) {
+            g[7] = (d << 30) | offsets[i];
+            colorWords = colorWordsFor(a.color, kept);
+        } else if (a.variable) {
+            g[7] = d << 30;
         }
         uint32_t* gdst;
         uint32_t* cdst;
         if (a.layout == GSR_LAYOUT_SPLIT) {
             gdst = reinterpret_cast<uint32_t*>(a.out[0]) + size_t(i) * a.geomWords;
-            cdst = reinterpret_cast<uint32_t*>(a.out[1]) +
-                   (a.variable ? size_t(offsets[i]) * 4 : size_t(i) * a.colorWords);
+            cdst = reinterpret_cast<uint32_t*>(a.out[1]) + (compact ? size_t(offsets[i]) * 4 : size_t(i) * a.colorWords);
         } else {
             uint32_t* rec = reinterpret_cast<uint32_t*>(a.out[0]) + size_t(i) * (a.geomWords + a.colorWords);
             gdst = rec;
@@ -226,6 +229,88 @@ uint32_t gridFor(uint32_t n) {
     return b < 1 ? 1 : (b > 148 * 32 ? 148 * 32 : b);
 }
 
+// ---- the cb codebook's k-means (kmeans.cpp) --------------------------------------------------
+__global__ void codebookPointsKernel(const __grid_constant__ EncodeArgs a, const uint8_t* degrees, float* points) {
+    const uint32_t dims = (a.K - 1) * 3;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const uint32_t d = degrees[i];
+        const uint32_t kept = a.variable ? (d + 1) * (d + 1) : a.K;
+        for (uint32_t k = 1; k < a.K; ++k)
+            for (uint32_t c = 0; c < 3; ++c) {
+                const float v = shValue(a, i, kept, k, c);
+                points[size_t(i) * dims + (k - 1) * 3 + c] = isfinite(v) ? v : 0.0f;
+            }
+    }
+}
+
+__global__ void codebookGatherKernel(const float* points, uint32_t dims, const uint32_t* index, uint32_t count,
+                                     float* out) {
+    const size_t total = size_t(count) * dims;
+    for (size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x; e < total; e += size_t(gridDim.x) * blockDim.x)
+        out[e] = points[size_t(index[e / dims]) * dims + e % dims];
+}
+
+// nearestAvx2 (kmeans.cpp:153-190) per point: x.c_j accumulated over the dimensions in order with
+// one fused multiply-add per dimension, the distance |c_j|^2 - 2 x.c_j fused as well, the first
+// smallest distance wins; then max(0, |x|^2 + best) with |x|^2 summed in double (assignAll,
+// :196-223). A block's 256 threads take 256 points; the centroids pass through shared memory in
+// tiles of 64, transposed so that one 16-byte load feeds four centroids' chains.
+constexpr int kCentroidTile = 64;
+template <int DIMS>
+__global__ void __launch_bounds__(256) nearestCentroidKernel(const float* __restrict__ points, uint32_t count,
+                                                             const float* __restrict__ centroids,
+                                                             const float* __restrict__ norm2, uint32_t k,
+                                                             uint32_t* assignment, float* sqDist) {
+    __shared__ __align__(16) float sC[DIMS][kCentroidTile];
+    __shared__ float sN[kCentroidTile];
+    const uint32_t i = blockIdx.x * 256 + threadIdx.x;
+    const bool valid = i < count;
+    float x[DIMS];
+    double x2 = 0.0;
+#pragma unroll
+    for (int d = 0; d < DIMS; ++d) x[d] = valid ? points[size_t(i) * DIMS + d] : 0.0f;
+#pragma unroll
+    for (int d = 0; d < DIMS; ++d) x2 += double(x[d]) * double(x[d]);
+    float best = __uint_as_float(0x7F800000u);
+    uint32_t bestIndex = 0;
+    for (uint32_t t0 = 0; t0 < k; t0 += kCentroidTile) {
+        __syncthreads();
+        for (uint32_t e = threadIdx.x; e < uint32_t(DIMS * kCentroidTile); e += 256) {
+            const uint32_t j = e / DIMS, d = e % DIMS;
+            sC[d][j] = t0 + j < k ? centroids[size_t(t0 + j) * DIMS + d] : 0.0f;
+        }
+        if (threadIdx.x < uint32_t(kCentroidTile))
+            sN[threadIdx.x] = t0 + threadIdx.x < k ? norm2[t0 + threadIdx.x] : __uint_as_float(0x7F800000u);
+        __syncthreads();
+        const uint32_t m = k - t0 < uint32_t(kCentroidTile) ? k - t0 : uint32_t(kCentroidTile);
+        for (uint32_t j = 0; j < m; j += 4) {  // slots past m: c = 0, |c|^2 = +inf, never chosen
+            float a0 = 0.0f, a1 = 0.0f, a2 = 0.0f, a3 = 0.0f;
+#pragma unroll
+            for (int d = 0; d < DIMS; ++d) {
+                const float4 c = *reinterpret_cast<const float4*>(&sC[d][j]);
+                a0 = fmaf(x[d], c.x, a0);
+                a1 = fmaf(x[d], c.y, a1);
+                a2 = fmaf(x[d], c.z, a2);
+                a3 = fmaf(x[d], c.w, a3);
+            }
+            const float acc[4] = {a0, a1, a2, a3};
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+                const float dist = fmaf(-2.0f, acc[l], sN[j + l]);
+                if (dist < best) {
+                    best = dist;
+                    bestIndex = t0 + j + uint32_t(l);
+                }
+            }
+        }
+    }
+    if (valid) {
+        assignment[i] = bestIndex;
+        const float v = float(x2) + best;
+        sqDist[i] = (0.0f < v) ? v : 0.0f;  // std::max(0.0f, v)
+    }
+}
+
 }  // namespace
 
 cudaError_t launchEncodeDegrees(const EncodeArgs& a, uint8_t* degrees, uint32_t* sizes, cudaStream_t s) {
@@ -235,6 +320,32 @@ cudaError_t launchEncodeDegrees(const EncodeArgs& a, uint8_t* degrees, uint32_t*
 
 cudaError_t launchEncodeRecords(const EncodeArgs& a, const uint8_t* degrees, const uint32_t* offsets, cudaStream_t s) {
     encodeKernel<<<gridFor(a.n), 256, 0, s>>>(a, degrees, offsets);
+    return cudaGetLastError();
+}
+
+cudaError_t launchCodebookPoints(const EncodeArgs& a, const uint8_t* degrees, float* points, cudaStream_t s) {
+    codebookPointsKernel<<<gridFor(a.n), 256, 0, s>>>(a, degrees, points);
+    return cudaGetLastError();
+}
+
+cudaError_t launchCodebookGather(const float* points, uint32_t dims, const uint32_t* index, uint32_t count, float* out,
+                                 cudaStream_t s) {
+    const uint64_t total = uint64_t(count) * dims;
+    const uint32_t blocks = uint32_t(total / 256 + 1 < 148 * 32 ? total / 256 + 1 : 148 * 32);
+    codebookGatherKernel<<<blocks, 256, 0, s>>>(points, dims, index, count, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launchNearestCentroid(const float* points, uint32_t count, uint32_t dims, const float* centroids,
+                                  const float* norm2, uint32_t k, uint32_t* assignment, float* sqDist, cudaStream_t s) {
+    if (count == 0) return cudaSuccess;
+    const uint32_t blocks = (count + 255) / 256;
+    switch (dims) {
+        case 9: nearestCentroidKernel<9><<<blocks, 256, 0, s>>>(points, count, centroids, norm2, k, assignment, sqDist); break;
+        case 24: nearestCentroidKernel<24><<<blocks, 256, 0, s>>>(points, count, centroids, norm2, k, assignment, sqDist); break;
+        case 45: nearestCentroidKernel<45><<<blocks, 256, 0, s>>>(points, count, centroids, norm2, k, assignment, sqDist); break;
+        default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 

@@ -118,6 +118,34 @@ __device__ __forceinline__ void loadSH(const SceneArgs& s, uint32_t i, uint32_t 
                 }
             }
         }
+    } else if (COLOR == GSR_COLOR_CODEBOOK) {
+        // CB record (h(dc.r, dc.g), h(dc.b) | index << 16), two per 16 bytes when the colour stride
+        // is 0 (split); the rest from codebook entry `index`, fp32 (scene_decode.glsl:96-103, 177-188)
+        uint2 r;
+        if (s.colorStride == 0) {
+            const uint4 v = __ldg(&s.b1[i >> 1]);
+            r = (i & 1u) ? make_uint2(v.z, v.w) : make_uint2(v.x, v.y);
+        } else {
+            const uint4 v = __ldg(&s.b1[size_t(i) * s.colorStride + s.colorOffset]);
+            r = make_uint2(v.x, v.y);
+        }
+        sh[0] = halfLo(r.x);
+        sh[1] = halfHi(r.x);
+        sh[2] = halfLo(r.y);
+        if (used > 1 && K > 1) {
+            const size_t entry = size_t(min(r.y >> 16, s.codebookLast)) * s.codebookStride;
+#pragma unroll
+            for (int v = 0; v < 12; ++v) {
+                if (uint32_t(v) * 4 < (K - 1) * 3 && uint32_t(v) * 4 < (used - 1) * 3) {
+                    const uint4 w = __ldg(&s.b2[entry + v]);
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int k = 3 + v * 4 + j;  // rest word v*4+j -> sh[3 + v*4 + j]
+                        if (k < 48) sh[k] = __uint_as_float(word(w, j));
+                    }
+                }
+            }
+        }
     } else {  // Q8: w0 = h(dc.r, dc.g), w1 = h(dc.b, s1), w2 = h(s2, s3), int8 rest from byte 12
         uint4 w[4];
 #pragma unroll
@@ -599,6 +627,8 @@ cudaError_t launchShDecode(const SceneArgs& scene, uint32_t geometry, uint32_t c
         launchShDecodeT<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16>(scene, count, evalDegree, out, degrees, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_Q8)
         launchShDecodeT<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8>(scene, count, evalDegree, out, degrees, s);
+    else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_CODEBOOK)
+        launchShDecodeT<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_CODEBOOK>(scene, count, evalDegree, out, degrees, s);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
@@ -615,6 +645,8 @@ cudaError_t launchFrontBinningKeys(const FrontArgs& a, uint32_t geometry, uint32
         launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16>(a, blocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_Q8)
         launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8>(a, blocks, s);
+    else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_CODEBOOK)
+        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_CODEBOOK>(a, blocks, s);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
@@ -645,6 +677,8 @@ cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, c
         launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16>(a, blocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_Q8)
         launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8>(a, blocks, s);
+    else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_CODEBOOK)
+        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_CODEBOOK>(a, blocks, s);
     else
         return cudaErrorInvalidValue;
     cudaError_t e = cudaGetLastError();

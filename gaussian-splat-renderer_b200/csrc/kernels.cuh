@@ -44,6 +44,8 @@ struct SceneArgs {
     const float* shSoa;  // soa sh float[]
     uint32_t geometryStride, colorStride, colorOffset;
     uint32_t storedCoeffs;  // K
+    uint32_t codebookStride;  // cb: 16-byte units per codebook entry (b2 = the codebook)
+    uint32_t codebookLast;    // cb: the last entry the codebook buffer holds (indices clamp to it)
     uint32_t variableSh;    // GsrVariableSh
 };
 

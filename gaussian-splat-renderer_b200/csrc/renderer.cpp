@@ -17,7 +17,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <numeric>
+#include <random>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -196,6 +199,9 @@ SceneArgs sceneArgs(const GsrSceneDesc& scene) {
     s.colorStride = scene.color_stride;
     s.colorOffset = scene.color_offset;
     s.storedCoeffs = scene.sh_coeffs;
+    s.codebookStride = scene.codebook_stride;
+    const uint64_t entryBytes = uint64_t(scene.codebook_stride) * 16;
+    s.codebookLast = entryBytes && scene.buffer_bytes[2] >= entryBytes ? uint32_t(scene.buffer_bytes[2] / entryBytes - 1) : 0u;
     s.variableSh = scene.variable_sh;
     return s;
 }
@@ -215,7 +221,142 @@ struct GsrColorModel {
 struct GsrScene {
     GsrSceneDesc desc{};
     DevBuf buffers[4];
+    GsrCodebookStats codebook{};
 };
+
+namespace {
+
+double msSince(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// The k-means of the cb codebook (kmeans.cpp:193-300, KMeansOptions seed 0x5EED5EED): the host
+// draws the training sample and the initial centroids with the same generator and bound, runs the
+// Lloyd updates (sequential double sums in sample order) and the re-seeding of empty clusters;
+// the nearest-centroid searches (the sample's each iteration and every point's at the end) run on
+// the GPU in the AVX2 kernel's arithmetic. `points` (device, n x dims) are the SH-rest vectors;
+// `assignment` (device, n) receives every gaussian's entry; `centroids` the codebook (k x dims).
+int trainCodebook(const float* points, uint32_t n, uint32_t dims, uint32_t kRequested, uint32_t iterations,
+                  uint32_t samples, uint32_t* assignment, std::vector<float>& centroids, GsrCodebookStats& st) {
+    const auto start = std::chrono::steady_clock::now();
+    st = GsrCodebookStats{};
+    st.dimensions = dims;
+    if (n == 0 || dims == 0) return GSR_OK;
+    const uint32_t k = std::max(1u, std::min(kRequested, n));
+    st.entries = k;
+    // 1. training sample (sorted indices)
+    const uint32_t S = std::min(n, samples ? std::max(samples, k) : uint32_t(std::min<uint64_t>(n, 32ull * k)));
+    std::mt19937_64 rng(0x5EED5EEDull);
+    auto uniformBelow = [&](uint32_t bound) { return uint32_t((rng() >> 32) * bound >> 32); };
+    std::vector<uint32_t> sample;
+    if (S == n) {
+        sample.resize(n);
+        std::iota(sample.begin(), sample.end(), 0u);
+    } else {
+        std::vector<uint32_t> perm(n);
+        std::iota(perm.begin(), perm.end(), 0u);
+        for (uint32_t i = 0; i < S; ++i) std::swap(perm[i], perm[i + uniformBelow(n - i)]);  // partial Fisher-Yates
+        sample.assign(perm.begin(), perm.begin() + S);
+        std::sort(sample.begin(), sample.end());
+    }
+    st.samples = S;
+    DevBuf dSample, dSamplePts, dCent, dNorm, dAssign, dDist, dFullDist;
+    GSR_CUDA(dSample.alloc(size_t(S) * 4));
+    GSR_CUDA(cudaMemcpy(dSample.p, sample.data(), size_t(S) * 4, cudaMemcpyHostToDevice));
+    GSR_CUDA(dSamplePts.alloc(size_t(S) * dims * 4));
+    GSR_CUDA(launchCodebookGather(points, dims, dSample.as<uint32_t>(), S, dSamplePts.as<float>(), nullptr));
+    std::vector<float> x(size_t(S) * dims);  // the sample's points, in sample order
+    GSR_CUDA(cudaMemcpy(x.data(), dSamplePts.p, x.size() * 4, cudaMemcpyDeviceToHost));
+    // 2. initial centroids: k distinct sample points
+    std::vector<uint32_t> pick(S);
+    std::iota(pick.begin(), pick.end(), 0u);
+    for (uint32_t i = 0; i < k; ++i) std::swap(pick[i], pick[i + uniformBelow(S - i)]);
+    centroids.assign(size_t(k) * dims, 0.0f);
+    for (uint32_t j = 0; j < k; ++j) std::copy_n(&x[size_t(pick[j]) * dims], dims, &centroids[size_t(j) * dims]);
+    GSR_CUDA(dCent.alloc(size_t(k) * dims * 4));
+    GSR_CUDA(dNorm.alloc(size_t(k) * 4));
+    GSR_CUDA(dAssign.alloc(size_t(S) * 4));
+    GSR_CUDA(dDist.alloc(size_t(S) * 4));
+    std::vector<float> norm2(k);
+    auto upload = [&]() -> int {  // CentroidTable::build: |c|^2 summed in double
+        for (uint32_t j = 0; j < k; ++j) {
+            double s = 0.0;
+            for (uint32_t d = 0; d < dims; ++d) {
+                const float v = centroids[size_t(j) * dims + d];
+                s += double(v) * v;
+            }
+            norm2[j] = float(s);
+        }
+        GSR_CUDA(cudaMemcpy(dCent.p, centroids.data(), centroids.size() * 4, cudaMemcpyHostToDevice));
+        GSR_CUDA(cudaMemcpy(dNorm.p, norm2.data(), size_t(k) * 4, cudaMemcpyHostToDevice));
+        return GSR_OK;
+    };
+    // 3. Lloyd iterations on the sample
+    std::vector<uint32_t> assign(S, 0u), previous(S, ~0u);
+    std::vector<float> dist(S, 0.0f);
+    std::vector<double> sums(size_t(k) * dims);
+    std::vector<uint32_t> counts(k);
+    for (uint32_t it = 0; it < iterations; ++it) {
+        int rc = upload();
+        if (rc) return rc;
+        GSR_CUDA(launchNearestCentroid(dSamplePts.as<float>(), S, dims, dCent.as<float>(), dNorm.as<float>(), k,
+                                       dAssign.as<uint32_t>(), dDist.as<float>(), nullptr));
+        GSR_CUDA(cudaMemcpy(assign.data(), dAssign.p, size_t(S) * 4, cudaMemcpyDeviceToHost));
+        GSR_CUDA(cudaMemcpy(dist.data(), dDist.p, size_t(S) * 4, cudaMemcpyDeviceToHost));
+        st.iterations = it + 1;
+        const bool converged = assign == previous;
+        previous = assign;
+        // update, sequential in sample order
+        std::fill(sums.begin(), sums.end(), 0.0);
+        std::fill(counts.begin(), counts.end(), 0u);
+        for (uint32_t s = 0; s < S; ++s) {
+            const float* xs = &x[size_t(s) * dims];
+            double* sum = &sums[size_t(assign[s]) * dims];
+            for (uint32_t d = 0; d < dims; ++d) sum[d] += xs[d];
+            ++counts[assign[s]];
+        }
+        // empty clusters take the sample points farthest from their centroid
+        std::vector<uint32_t> empty;
+        for (uint32_t j = 0; j < k; ++j)
+            if (counts[j] == 0) empty.push_back(j);
+        if (!empty.empty()) {
+            std::vector<uint32_t> far(S);
+            std::iota(far.begin(), far.end(), 0u);
+            const size_t m = std::min(empty.size(), far.size());
+            std::partial_sort(far.begin(), far.begin() + std::ptrdiff_t(m), far.end(), [&](uint32_t a, uint32_t b) {
+                return dist[a] != dist[b] ? dist[a] > dist[b] : a < b;
+            });
+            for (size_t e = 0; e < m; ++e) std::copy_n(&x[size_t(far[e]) * dims], dims, &centroids[size_t(empty[e]) * dims]);
+            st.empty_reseeded += uint32_t(m);
+        }
+        for (uint32_t j = 0; j < k; ++j) {
+            if (counts[j] == 0) continue;
+            for (uint32_t d = 0; d < dims; ++d)
+                centroids[size_t(j) * dims + d] = float(sums[size_t(j) * dims + d] / double(counts[j]));
+        }
+        if (converged) break;
+    }
+    st.train_ms = msSince(start);
+    // 4. every point's entry under the trained centroids, and the errors
+    int rc = upload();
+    if (rc) return rc;
+    const auto tf = std::chrono::steady_clock::now();
+    GSR_CUDA(dFullDist.alloc(size_t(n) * 4));
+    GSR_CUDA(launchNearestCentroid(points, n, dims, dCent.as<float>(), dNorm.as<float>(), k, assignment,
+                                   dFullDist.as<float>(), nullptr));
+    std::vector<float> fullDist(n);
+    GSR_CUDA(cudaMemcpy(fullDist.data(), dFullDist.p, size_t(n) * 4, cudaMemcpyDeviceToHost));
+    st.assign_ms = msSince(tf);
+    double sampleErr = 0.0, fullErr = 0.0;
+    for (uint32_t s = 0; s < S; ++s) sampleErr += fullDist[sample[s]];
+    for (uint32_t i = 0; i < n; ++i) fullErr += fullDist[i];
+    st.sample_mse = sampleErr / (double(S) * dims);
+    st.full_mse = fullErr / (double(n) * dims);
+    st.total_ms = msSince(start);
+    return GSR_OK;
+}
+
+}  // namespace
 
 // ====================================================================================== renderer
 struct GsrRenderer {
@@ -724,9 +865,12 @@ int validateScene(const GsrSceneDesc& s) {
     const bool f32 = s.geometry == GSR_GEOMETRY_RECORD_F32 && s.color == GSR_COLOR_RECORD_F32;
     const bool f16 = s.geometry == GSR_GEOMETRY_RECORD_F16 && s.color == GSR_COLOR_RECORD_F16;
     const bool q8 = s.geometry == GSR_GEOMETRY_RECORD_F16 && s.color == GSR_COLOR_Q8;
-    if (s.color == GSR_COLOR_CODEBOOK)
-        return fail(GSR_ERROR_UNSUPPORTED, "the codebook (cb) scene format is not implemented by this build");
-    if (!(soa || f32 || f16 || q8))
+    const bool cb = s.geometry == GSR_GEOMETRY_RECORD_F16 && s.color == GSR_COLOR_CODEBOOK;
+    if (cb && (!s.buffers[2] || s.codebook_stride == 0 || s.buffer_bytes[2] < uint64_t(s.codebook_stride) * 16))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "a codebook scene needs the codebook buffer and its stride");
+    if (cb && s.variable_sh == GSR_VARIABLE_SH_COMPACT)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "cb colour records are fixed-size (no compacted variable SH)");
+    if (!(soa || f32 || f16 || q8 || cb))
         return fail(GSR_ERROR_INVALID_ARGUMENT, "geometry encoding %u with colour encoding %u", s.geometry, s.color);
     if (s.variable_sh > GSR_VARIABLE_SH_COMPACT) return fail(GSR_ERROR_INVALID_ARGUMENT, "variable_sh %u", s.variable_sh);
     if (soa && (!s.buffers[0] || !s.buffers[1] || !s.buffers[2] || !s.buffers[3]))
@@ -830,8 +974,7 @@ int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, Gs
         !host->rotations || !host->sh)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "host scene (count %u, degree %d)", host->count, host->sh_degree);
     const uint32_t fmt = options->format, layout = options->layout;
-    if (fmt == GSR_FORMAT_CB) return fail(GSR_ERROR_UNSUPPORTED, "the codebook (cb) scene format is not implemented");
-    if (fmt > GSR_FORMAT_Q8 || layout > GSR_LAYOUT_AOS) return fail(GSR_ERROR_INVALID_ARGUMENT, "format %u layout %u", fmt, layout);
+    if (fmt > GSR_FORMAT_CB || layout > GSR_LAYOUT_AOS) return fail(GSR_ERROR_INVALID_ARGUMENT, "format %u layout %u", fmt, layout);
     if (fmt != GSR_FORMAT_F32 && layout == GSR_LAYOUT_SOA)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "scene layout 'soa' exists only for the f32 format (use split or aos)");
     const uint32_t n = host->count;
@@ -875,16 +1018,21 @@ int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, Gs
         ea.color = GSR_COLOR_SOA_F32;
     } else {
         ea.geometry = fmt == GSR_FORMAT_F32 ? GSR_GEOMETRY_RECORD_F32 : GSR_GEOMETRY_RECORD_F16;
-        ea.color = fmt == GSR_FORMAT_F32 ? GSR_COLOR_RECORD_F32 : fmt == GSR_FORMAT_F16 ? GSR_COLOR_RECORD_F16 : GSR_COLOR_Q8;
+        ea.color = fmt == GSR_FORMAT_F32   ? GSR_COLOR_RECORD_F32
+                   : fmt == GSR_FORMAT_F16 ? GSR_COLOR_RECORD_F16
+                   : fmt == GSR_FORMAT_Q8  ? GSR_COLOR_Q8
+                                           : GSR_COLOR_CODEBOOK;
     }
+    const bool cb = ea.color == GSR_COLOR_CODEBOOK;
     auto vec4sFor = [](uint32_t bytes) { return (bytes + 15u) / 16u; };
     ea.geomWords = ea.geometry == GSR_GEOMETRY_RECORD_F16 ? 8u : 12u;
     ea.colorWords = ea.color == GSR_COLOR_RECORD_F32   ? vec4sFor(K * 12) * 4
                     : ea.color == GSR_COLOR_RECORD_F16 ? vec4sFor(K * 6) * 4
                     : ea.color == GSR_COLOR_Q8         ? vec4sFor(12 + (K - 1) * 3) * 4
+                    : cb                               ? (layout == GSR_LAYOUT_SPLIT ? 2u : 4u)  // two 8-byte records per uvec4 (split)
                                                        : 0;
     GSR_CUDA(degrees.alloc(n));
-    const bool compact = variable && (layout == GSR_LAYOUT_SOA || layout == GSR_LAYOUT_SPLIT);
+    const bool compact = variable && !cb && (layout == GSR_LAYOUT_SOA || layout == GSR_LAYOUT_SPLIT);
     uint64_t compactTotal = 0;
     if (compact) {
         GSR_CUDA(sizes.alloc(size_t(n) * 4));
@@ -901,6 +1049,21 @@ int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, Gs
         compactTotal = t;
         if (compactTotal >= (1ull << 30)) return fail(GSR_ERROR_INVALID_ARGUMENT, "variable SH: compacted data exceeds 2^30");
     }
+    // cb: the k-means codebook of the SH-rest vectors, and every gaussian's entry
+    DevBuf cbPoints, cbAssign;
+    std::vector<float> centroids;
+    const uint32_t restDims = (K - 1) * 3;
+    if (cb && restDims > 0) {
+        GSR_CUDA(cbPoints.alloc(size_t(n) * restDims * 4));
+        GSR_CUDA(cbAssign.alloc(size_t(n) * 4));
+        GSR_CUDA(launchCodebookPoints(ea, degrees.as<uint8_t>(), cbPoints.as<float>(), 0));
+        const uint32_t size = std::clamp(options->codebook_size ? options->codebook_size : 4096u, 1u, 65536u);
+        const uint32_t iters = options->codebook_iterations ? options->codebook_iterations : 10u;
+        int rc = trainCodebook(cbPoints.as<float>(), n, restDims, size, iters, options->codebook_samples,
+                               cbAssign.as<uint32_t>(), centroids, scene->codebook);
+        if (rc) return rc;
+        ea.cbIndex = cbAssign.as<uint32_t>();
+    }
     size_t bytes[4] = {0, 0, 0, 0};
     if (layout == GSR_LAYOUT_SOA) {
         bytes[0] = bytes[1] = bytes[2] = size_t(n) * 16;
@@ -914,8 +1077,8 @@ int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, Gs
         d.geometry = ea.geometry;
         d.color = ea.color;
         d.geometry_stride = ea.geomWords / 4;
-        d.color_stride = ea.colorWords / 4;
-        d.variable_sh = variable ? GSR_VARIABLE_SH_COMPACT : GSR_VARIABLE_SH_OFF;
+        d.color_stride = cb ? 0u : ea.colorWords / 4;  // cb: records packed two per 16 bytes
+        d.variable_sh = !variable ? GSR_VARIABLE_SH_OFF : compact ? GSR_VARIABLE_SH_COMPACT : GSR_VARIABLE_SH_DEGREE_ONLY;
     } else {
         bytes[0] = size_t(n) * (ea.geomWords + ea.colorWords) * 4;
         d.geometry = ea.geometry;
@@ -925,6 +1088,16 @@ int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, Gs
         d.color_offset = ea.geomWords / 4;
         d.variable_sh = variable ? GSR_VARIABLE_SH_DEGREE_ONLY : GSR_VARIABLE_SH_OFF;
     }
+    std::vector<uint32_t> codebookWords;
+    if (cb) {  // entries of (K - 1) * 3 fp32 words padded to 16 bytes (at least one entry)
+        const uint32_t entryWords = std::max(4u, vec4sFor(restDims * 4) * 4);
+        d.codebook_stride = entryWords / 4;
+        const uint32_t entries = scene->codebook.entries;
+        codebookWords.assign(size_t(std::max(entries, 1u)) * entryWords, 0u);
+        for (uint32_t c = 0; c < entries; ++c)
+            std::memcpy(&codebookWords[size_t(c) * entryWords], &centroids[size_t(c) * restDims], size_t(restDims) * 4);
+        bytes[2] = codebookWords.size() * 4;
+    }
     for (int b = 0; b < 4; ++b) {
         if (!bytes[b]) continue;
         GSR_CUDA(scene->buffers[b].alloc(bytes[b]));
@@ -933,10 +1106,28 @@ int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, Gs
         d.buffers[b] = scene->buffers[b].p;
         d.buffer_bytes[b] = bytes[b];
     }
+    if (cb) GSR_CUDA(cudaMemcpy(scene->buffers[2].p, codebookWords.data(), bytes[2], cudaMemcpyHostToDevice));
     GSR_CUDA(launchEncodeRecords(ea, degrees.as<uint8_t>(), compact ? offs.as<uint32_t>() : nullptr, 0));
     GSR_CUDA(cudaDeviceSynchronize());
     *out = scene.release();
     return GSR_OK;
+}
+
+int gsr_scene_codebook_stats(const GsrScene* scene, GsrCodebookStats* out) {
+    if (!scene || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = scene->codebook;
+    return GSR_OK;
+}
+
+void gsr_compression_default(GsrCompression* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->format = GSR_FORMAT_F32;
+    c->layout = GSR_LAYOUT_SOA;
+    c->max_sh_degree = 3;
+    c->sh_threshold = -1.0f;
+    c->codebook_size = 4096;
+    c->codebook_iterations = 10;
 }
 
 int gsr_scene_get_desc(const GsrScene* scene, GsrSceneDesc* out) {

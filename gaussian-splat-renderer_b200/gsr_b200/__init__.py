@@ -70,7 +70,15 @@ class HostScene(C.Structure):
 
 
 class Compression(C.Structure):
-    _fields_ = [("format", C.c_uint32), ("layout", C.c_uint32), ("max_sh_degree", C.c_int32), ("sh_threshold", C.c_float)]
+    _fields_ = [("format", C.c_uint32), ("layout", C.c_uint32), ("max_sh_degree", C.c_int32), ("sh_threshold", C.c_float),
+                ("codebook_size", C.c_uint32), ("codebook_iterations", C.c_uint32), ("codebook_samples", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class CodebookStats(C.Structure):
+    _fields_ = [("entries", C.c_uint32), ("dimensions", C.c_uint32), ("samples", C.c_uint32), ("iterations", C.c_uint32),
+                ("empty_reseeded", C.c_uint32), ("pad", C.c_uint32), ("train_ms", C.c_double), ("assign_ms", C.c_double),
+                ("total_ms", C.c_double), ("sample_mse", C.c_double), ("full_mse", C.c_double)]
 
 
 class CSettings(C.Structure):
@@ -180,6 +188,8 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_scene_create": (C.c_int, [C.POINTER(HostScene), C.POINTER(Compression), C.POINTER(vp)]),
         "gsr_scene_get_desc": (C.c_int, [vp, C.POINTER(SceneDesc)]),
         "gsr_scene_read_buffer": (C.c_int, [vp, u32, vp, u64]),
+        "gsr_scene_codebook_stats": (C.c_int, [vp, vp]),
+        "gsr_compression_default": (None, [vp]),
         "gsr_scene_destroy": (None, [vp]),
         "gsr_renderer_create": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(CSettings), C.POINTER(vp)]),
         "gsr_renderer_resize": (C.c_int, [vp, u32, u32]),
@@ -302,17 +312,24 @@ class Settings:
 class GpuScene:
     """gsr::GpuScene: the scene encoded (on the GPU) and resident in device memory."""
 
-    def __init__(self, scene, fmt: str = "f32", layout: str = "soa", max_sh_degree: int = 3, sh_threshold: float = -1.0):
+    def __init__(self, scene, fmt: str = "f32", layout: str = "soa", max_sh_degree: int = 3, sh_threshold: float = -1.0,
+                 codebook_size: int = 4096, codebook_iterations: int = 10, codebook_samples: int = 0):
         lib = load()
         self._arrays = [np.ascontiguousarray(a, np.float32) for a in (scene.pos_alpha, scene.scales, scene.rotations, scene.sh)]
         hs = HostScene(scene.count, scene.sh_degree, *[a.ctypes.data for a in self._arrays])
-        comp = Compression(FORMATS[fmt], LAYOUTS[layout], max_sh_degree, sh_threshold)
+        comp = Compression(FORMATS[fmt], LAYOUTS[layout], max_sh_degree, sh_threshold, codebook_size, codebook_iterations,
+                           codebook_samples, 0)
         h = C.c_void_p()
         check(lib.gsr_scene_create(C.byref(hs), C.byref(comp), C.byref(h)))
         self._h = h
         self._arrays = None
         self.desc = SceneDesc()
         check(lib.gsr_scene_get_desc(self._h, C.byref(self.desc)))
+
+    def codebook_stats(self) -> dict:
+        st = CodebookStats()
+        check(load().gsr_scene_codebook_stats(self._h, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in CodebookStats._fields_ if f != "pad"}
 
     def buffer(self, b: int) -> np.ndarray:
         n = int(self.desc.buffer_bytes[b])

@@ -64,7 +64,7 @@ typedef struct GsrSceneDesc {
     uint32_t geometry_stride;  /* uvec4 per geometry record (0 for soa) */
     uint32_t color_stride;     /* uvec4 per colour record */
     uint32_t color_offset;     /* uvec4 offset of the colour record (aos) */
-    uint32_t codebook_stride;  /* uvec4 per codebook entry (cb; unsupported) */
+    uint32_t codebook_stride;  /* uvec4 per codebook entry (cb) */
     uint32_t variable_sh;      /* GsrVariableSh */
     const void* buffers[4];    /* device pointers, 16-byte aligned */
     uint64_t buffer_bytes[4];
@@ -80,13 +80,33 @@ typedef struct GsrHostScene {
     const float* sh;         /* float[N * K * 3] */
 } GsrHostScene;
 
-/* gsr::CompressionOptions subset (src/scene/scene_compression.h:76-86). */
+/* gsr::CompressionOptions (src/scene/scene_compression.h:76-86). The codebook fields configure
+ * the cb format's k-means; 0 selects the reference's default (4096 entries, 10 iterations). */
 typedef struct GsrCompression {
-    uint32_t format;        /* GsrSceneFormat (f32, f16, q8) */
-    uint32_t layout;        /* GsrSceneLayout (soa only with f32) */
-    int32_t max_sh_degree;  /* drop stored bands above this */
-    float sh_threshold;     /* per-gaussian SH degree threshold in 1/255 (< 0: off) */
+    uint32_t format;              /* GsrSceneFormat (f32, f16, q8, cb) */
+    uint32_t layout;              /* GsrSceneLayout (soa only with f32) */
+    int32_t max_sh_degree;        /* drop stored bands above this */
+    float sh_threshold;           /* per-gaussian SH degree threshold in 1/255 (< 0: off) */
+    uint32_t codebook_size;       /* cb: codebook entries (1..65536; 0 = 4096) */
+    uint32_t codebook_iterations; /* cb: Lloyd iterations on the training sample (0 = 10) */
+    uint32_t codebook_samples;    /* cb: training sample size (0 = min(N, 32 x entries)) */
+    uint32_t reserved;
 } GsrCompression;
+/* The reference's defaults: f32, soa, degree 3, threshold off, 4096 entries, 10 iterations. */
+void gsr_compression_default(GsrCompression* options);
+
+/* CodebookStats (scene_compression.h:91-101) of a cb scene's k-means (entries 0 for other formats).
+ * The assignment passes run on the GPU; the update and the statistics on the host. */
+typedef struct GsrCodebookStats {
+    uint32_t entries;        /* codebook size used (<= requested, <= N) */
+    uint32_t dimensions;     /* (K - 1) * 3 */
+    uint32_t samples;        /* training sample size */
+    uint32_t iterations;     /* Lloyd iterations run */
+    uint32_t empty_reseeded; /* empty clusters re-seeded over all iterations */
+    uint32_t pad;
+    double train_ms, assign_ms, total_ms;
+    double sample_mse, full_mse; /* mean squared error per coefficient (sample, all gaussians) */
+} GsrCodebookStats;
 
 typedef struct GsrScene GsrScene;
 
@@ -94,6 +114,14 @@ typedef struct GsrScene GsrScene;
  * src/scene/scene_compression.cpp:150-380, f32/f16/q8 in soa/split/aos, variable SH degree)
  * and keeps the encoded buffers in device memory owned by the handle. */
 int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, GsrScene** out);
+/* The cb format (encodeScene's codebook path, scene_compression.cpp:250-273, 309-314, 340-377):
+ * fp16 geometry records, an 8-byte colour record (h(dc.r, dc.g), h(dc.b) | index << 16; two per
+ * 16 bytes in the split layout) and the codebook of SH-rest vectors (fp32, entries padded to 16
+ * bytes) from the reference's k-means (kmeans.cpp): the same sample, initial centroids, Lloyd
+ * updates, re-seeding and final assignment, with the nearest-centroid searches computed on the
+ * GPU in the reference's own arithmetic (the AVX2 kernel's fused multiply-adds), so the codebook
+ * and the indices equal the reference's on a host with AVX2 and FMA. */
+int gsr_scene_codebook_stats(const GsrScene* scene, GsrCodebookStats* out);
 /* The descriptor of a GsrScene, to pass to gsr_renderer_create. */
 int gsr_scene_get_desc(const GsrScene* scene, GsrSceneDesc* out);
 /* Copies encoded buffer b (0..3) to host memory (tests): bytes = buffer_bytes[b]. */

@@ -1236,7 +1236,7 @@ int gsr_oracle_encode(uint32_t n, int shDegreeIn, const float* posAlpha, const f
     return 0;
 }
 
-/* decodeGaussian (scene_compression.cpp:382-460), f32/f16/q8. */
+/* decodeGaussian (scene_compression.cpp:382-460), f32/f16/q8/cb. */
 void gsr_oracle_decode(uint32_t n, const uint32_t* desc, const uint64_t* sizes, void* const* buffers, float* posAlpha,
                        float* scales, float* rotations, float* shOut) {
     (void)sizes;
@@ -1314,8 +1314,14 @@ void gsr_oracle_decode(uint32_t n, const uint32_t* desc, const uint64_t* sizes, 
                     const int8_t q = (int8_t)(uint8_t)(c[3 + j / 4] >> (8 * (j % 4)));
                     sh[k * 3 + ch] = (float)q * scale[bandOf(k)];
                 }
+        } else if (color == COL_CB) {  /* DC in the record, the rest from entry c[1] >> 16 of the codebook */
+            sh[0] = unpackLo(c[0]);
+            sh[1] = unpackHi(c[0]);
+            sh[2] = unpackLo(c[1]);
+            const uint32_t* entry = b2 + (size_t)(c[1] >> 16) * desc[5] * 4;
+            for (uint32_t k = 1; k < K; ++k)
+                for (uint32_t ch = 0; ch < 3; ++ch) sh[k * 3 + ch] = bitsf(entry[(k - 1) * 3 + ch]);
         }
-        (void)b2;
     }
 }
 

@@ -125,6 +125,7 @@ class Oracle:
             f("ply_comment", C.c_char_p, [C.c_void_p, C.c_uint32])
             f("ply_warning", C.c_char_p, [C.c_void_p, C.c_uint32])
             f("ply_free", None, [C.c_void_p])
+            f("encode_codebook", C.c_int, None)
         if kind == "port":
             f("look_at", None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p])
             f("perspective", None, [C.c_float, C.c_float, C.c_float, C.c_float, C.c_void_p])
@@ -255,6 +256,27 @@ class Oracle:
         if self._encode(*args, ptrs) != 0:
             raise ValueError("encode failed")
         return {"desc": desc, "buffers": bufs}
+
+    def encode_codebook(self, scene, layout: int, codebook_size: int, iterations: int, samples: int = 0,
+                        max_sh_degree: int = 3, sh_threshold: float = -1.0):
+        """encodeScene in the cb format (the reference build only): desc, buffers and the k-means
+        stats {entries, samples, iterations, empty_reseeded, simd}."""
+        desc = np.zeros(11, np.uint32)
+        sizes = np.zeros(4, np.uint64)
+        stats = np.zeros(5, np.uint32)
+        args = [
+            C.c_uint32(scene.count), C.c_int(scene.sh_degree), _p(scene.pos_alpha), _p(scene.scales),
+            _p(scene.rotations), _p(scene.sh), C.c_uint32(layout), C.c_int(max_sh_degree), C.c_float(sh_threshold),
+            C.c_uint32(codebook_size), C.c_uint32(iterations), C.c_uint32(samples), _p(desc), _p(sizes),
+        ]
+        if self._encode_codebook(*args, None, None) != 0:
+            raise ValueError("invalid layout for the cb format")
+        bufs = [np.zeros(int(s) // 4, np.uint32) for s in sizes]
+        ptrs = (C.c_void_p * 4)(*[b.ctypes.data if b.size else None for b in bufs])
+        if self._encode_codebook(*args, ptrs, _p(stats)) != 0:
+            raise ValueError("encode failed")
+        names = ("entries", "samples", "iterations", "empty_reseeded", "simd")
+        return {"desc": desc, "buffers": bufs, "stats": {k: int(v) for k, v in zip(names, stats)}}
 
     def decode(self, enc, count: int):
         desc = np.ascontiguousarray(enc["desc"], np.uint32)

@@ -257,6 +257,54 @@ int gsr_ref_encode(uint32_t n, int shDegree, const float* posAlpha, const float*
     }
 }
 
+// encodeScene with the codebook options (the cb format's k-means): codebookSize, iterations,
+// samples as CompressionOptions; otherwise as gsr_ref_encode. stats: entries, samples, iterations,
+// emptyReseeded, simd (the AVX2 kernel was used).
+int gsr_ref_encode_codebook(uint32_t n, int shDegree, const float* posAlpha, const float* scales, const float* rotations,
+                            const float* sh, uint32_t layout, int maxShDegree, float shThreshold, uint32_t codebookSize,
+                            uint32_t iterations, uint32_t samples, uint32_t* desc, uint64_t* sizes, void** buffers,
+                            uint32_t* stats) {
+    try {
+        const gsr::GaussianScene scene = makeScene(n, shDegree, posAlpha, scales, rotations, sh);
+        gsr::CompressionOptions o;
+        o.format = gsr::SceneFormat::Codebook;
+        o.layout = gsr::SceneLayout(layout);
+        o.maxShDegree = maxShDegree;
+        o.shThreshold = shThreshold;
+        o.codebookSize = codebookSize;
+        o.codebookIterations = iterations;
+        o.codebookSamples = samples;
+        o.threads = 0;
+        const gsr::EncodedScene e = gsr::encodeScene(scene, o);
+        desc[0] = uint32_t(e.geometry);
+        desc[1] = uint32_t(e.color);
+        desc[2] = e.geometryStride;
+        desc[3] = e.colorStride;
+        desc[4] = e.colorOffset;
+        desc[5] = e.codebookStride;
+        desc[6] = uint32_t(e.variableSh);
+        desc[7] = uint32_t(e.shDegree);
+        desc[8] = e.shCoeffs;
+        desc[9] = uint32_t(e.format);
+        desc[10] = uint32_t(e.layout);
+        for (int b = 0; b < 4; ++b) {
+            const size_t bytes = b < int(e.buffers.size()) ? e.buffers[b].size() * 4 : 0;
+            sizes[b] = bytes;
+            if (buffers && buffers[b] && bytes) std::memcpy(buffers[b], e.buffers[b].data(), bytes);
+        }
+        if (stats) {
+            stats[0] = e.codebook.entries;
+            stats[1] = e.codebook.samples;
+            stats[2] = e.codebook.iterations;
+            stats[3] = e.codebook.emptyReseeded;
+            stats[4] = e.codebook.simd ? 1u : 0u;
+        }
+        return 0;
+    } catch (const std::exception&) {
+        return -1;
+    }
+}
+
 // decodeGaussian (src/scene/scene_compression.cpp:382-460) for gaussians [0, n) of an encoded
 // scene given as (desc, buffers) like gsr_ref_encode; writes posAlpha, sigma (vec4, w = 0),
 // rotation and K = desc[8] SH triplets per gaussian.

@@ -63,13 +63,6 @@ def test_encode_words_and_frame(gpu, port, scene, fmt, layout, threshold):
     assert psnr(r.read_back_image()[..., :3], ref) > 60.0
 
 
-def test_codebook_format_is_rejected(gpu):
-    scene = tile_raster_scene(1000, 1)
-    with pytest.raises(gpu.GsrError) as e:
-        gpu.GpuScene(scene, "cb", "split")
-    assert e.value.status == 2
-
-
 def test_soa_layout_only_for_f32(gpu):
     scene = tile_raster_scene(1000, 1)
     with pytest.raises(gpu.GsrError) as e:

@@ -155,3 +155,15 @@ def test_invalid_format_combinations(port, ref, scenes_and_cams):
     for o in (port, ref):
         with pytest.raises(ValueError):
             o.encode(scene, 1, 0)  # f16 has no soa layout
+
+
+@pytest.mark.parametrize("layout", [1, 2])
+@pytest.mark.parametrize("max_deg,threshold", [(3, -1.0), (2, -1.0), (3, 2.0), (0, -1.0)])
+def test_codebook_decode(port, ref, scenes_and_cams, layout, max_deg, threshold):
+    """The port's decode of cb scenes (DC from the record, the rest from the codebook entry the
+    record names) equals decodeGaussian on the reference's own cb encoding."""
+    scene = scenes_and_cams[2][0]
+    enc = ref.encode_codebook(scene, layout, 128, 5, 0, max_deg, threshold)
+    assert enc["stats"]["entries"] == (0 if max_deg == 0 else 128)
+    for x, y in zip(port.decode(enc, scene.count), ref.decode(enc, scene.count)):
+        np.testing.assert_array_equal(x.view(np.uint32), y.view(np.uint32))
