@@ -57,6 +57,32 @@ __device__ __forceinline__ float fastExp2(float x) {
     return y;
 }
 
+__device__ __forceinline__ float approxSqrt(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// Whether a record's cutoff ellipse q(d) = A dx^2 + 2B dx dy + C dy^2 <= t meets any pixel centre
+// of a warp's strip: ROWS rows from y0, columns [x0, x1]. Row y holds the run
+// |px - (cx + (B/A) dy)| <= sqrt((t - (D/A) dy^2) / A), dy = cy - y; the row test inflates t by
+// 0.2 %, moves the row 0.05 px towards the centre and widens the run by 0.1 % + 0.05 px (the
+// margins of the tile-coverage box), and any NaN keeps the record.
+template <uint32_t ROWS>
+__device__ __forceinline__ bool stripHit(float2 c, float4 k, float x0, float x1, float y0) {
+    bool hit = false;
+#pragma unroll
+    for (uint32_t r = 0; r < ROWS; ++r) {
+        const float dy = c.y - (y0 + float(r));
+        const float dyIn = copysignf(fmaxf(fabsf(dy) - 0.05f, 0.0f), dy);
+        const float s = fmaf(-k.y * dyIn, dyIn, k.w * 1.002f);
+        const float hw = fmaf(approxSqrt(fmaxf(s, 0.0f) * k.z), 1.001f, 0.05f);
+        const float xc = fmaf(k.x, dy, c.x);
+        hit |= !(s < 0.0f) && !(xc - hw > x1) && !(xc + hw < x0);
+    }
+    return hit;
+}
+
 // N = the batch (one entry per thread of the tile's block)
 template <int N>
 struct RenderShared {
@@ -64,7 +90,7 @@ struct RenderShared {
     // N in the first half of the area)
     float4 raw[2][3][N];
     float4 conic[N];      // a', b', c' (pre-scaled), opacity
-    float4 box[N];        // x0, x1, y0, y1 of the cutoff ellipse (pixels)
+    float4 cull[N];       // B/A, D/A, 1/A, t: the cutoff ellipse's row extents (stripHit)
     float4 color[N];      // r, g, b, -
     float2 center[N];
     uint32_t tile;        // persistent schedule: the block's current tile
@@ -210,7 +236,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
     const float fx = float(px), fy = float(py);
     // this warp's pixel strip
     const float wx0 = float(tx * TILE), wx1 = float(tx * TILE + TILE - 1);
-    const float wy0 = float(ty * TILE + kRows * warp), wy1 = wy0 + float(kRows - 1);
+    const float wy0 = float(ty * TILE + kRows * warp);
     float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
     bool done = !inside;
 
@@ -296,33 +322,37 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
                 p24DecodeConic(w1.x, w1.y, A, B, C, o);
                 r2 = make_float4(halfLoF(w2.x), halfHiF(w2.x), halfLoF(w2.y), 0.0f);
             }
-            // cutoff ellipse box (makeCutoffEllipse's threshold, wider margin)
-            float4 box = make_float4(-3.0e38f, 3.0e38f, -3.0e38f, 3.0e38f);
+            // the cutoff ellipse for the strip tests (makeCutoffEllipse's threshold, wider margin):
+            // t < 0 misses every row (opacity below 1/255), an invalid conic meets every row
+            float4 cull = make_float4(0.0f, 0.0f, 1.0f, 3.0e38f);
             const float D = A * C - B * B;
             if (!(o >= 1.0f / 255.0f)) {
-                box = make_float4(3.0e38f, -3.0e38f, 3.0e38f, -3.0e38f);  // never reaches 1/255: skip everywhere
+                cull.w = -3.0e38f;
             } else if (A > 0.0f && C > 0.0f && D > 0.0f) {
                 const float qmax = 2.0f * __logf(255.0f * o) + 1e-3f;
                 const float rho = fabsf(B) * rsqrtf(A * C);
                 const float K = 2.0f / fmaxf(1.0f - rho, 1e-30f);
                 const float t = qmax + (2e-3f + 4e-5f * K) * fmaxf(qmax, 1.0f) + 4e-3f;
                 if (t < 1e30f) {
-                    const float ex = sqrtf(t * C / D) * 1.001f + 0.05f;
-                    const float ey = sqrtf(t * A / D) * 1.001f + 0.05f;
-                    box = make_float4(r0.x - ex, r0.x + ex, r0.y - ey, r0.y + ey);
+                    const float ia = 1.0f / A;
+                    cull = make_float4(B * ia, D * ia, ia, t);
                 }
             }
-            sm.box[tid] = box;
+            sm.cull[tid] = cull;
             sm.conic[tid] = make_float4(-0.5f * kLog2e * A, -kLog2e * B, -0.5f * kLog2e * C, o);
             sm.color[tid] = r2;
             sm.center[tid] = make_float2(r0.x, r0.y);
         }
         __syncthreads();
         const uint32_t n = range.y - start < kThreads ? range.y - start : kThreads;
-        if (!done) {
-            for (uint32_t q = 0; q < n; ++q) {
-                const float4 bx = sm.box[q];
-                if (bx.y < wx0 || bx.x > wx1 || bx.w < wy0 || bx.z > wy1) continue;  // warp-uniform
+        // the warp tests 32 records at a time against its strip, one per lane, and visits the
+        // hits in list order
+        for (uint32_t q0 = 0; q0 < n && !__all_sync(0xffffffffu, done); q0 += 32) {
+            const uint32_t ql = q0 + (tid & 31u);
+            const bool hit = ql < n && stripHit<kRows>(sm.center[ql], sm.cull[ql], wx0, wx1, wy0);
+            for (uint32_t m = __ballot_sync(0xffffffffu, hit); m != 0u; m &= m - 1u) {
+                const uint32_t q = q0 + uint32_t(__ffs(m)) - 1u;
+                if (done) continue;
                 const float2 c = sm.center[q];
                 const float4 co = sm.conic[q];
                 const float dx = c.x - fx;
@@ -339,13 +369,12 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
                                       2.0f * pb.x * vy + pb.y;
                     const float vb = pb.z * vx + pb.w * vy + pc;
                     windowPush(window, K, vb / vPv, alpha, sm.color[q], T, c0, c1, c2, done);
-                    if (done) break;
                     continue;
                 }
                 const float testT = T * (1.0f - alpha);
                 if (testT < kMinTransmittance) {
                     done = true;
-                    break;
+                    continue;
                 }
                 const float4 col = sm.color[q];
                 const float w = alpha * T;
