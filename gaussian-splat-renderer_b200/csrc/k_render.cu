@@ -205,18 +205,20 @@ __device__ __forceinline__ void windowPush(SortWindow<CAP>& q, uint32_t K, float
 // CAP: 0, or the StopThePop window's register capacity; `ray` is then the shared area of the
 // gathered ray-depth parameters (3 x 16 B per entry, double-buffered).
 // TILE: the tile's edge, 16 (INRIA's tiles) or 8 pixels; one thread per pixel, batches of TILE^2
-// entries, and each warp owns 32 / TILE rows of the tile (its strip).
+// entries, and each warp owns an 8 x 4 pixel block of the tile (its strip: a squarer footprint
+// meets fewer ellipses than a 16 x 2 row pair).
 template <int MODE, int CAP, int TILE>
 __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TILE * TILE>& sm,
                                            float4 (*ray)[3][TILE * TILE], uint32_t tile) {
-    constexpr uint32_t kThreads = TILE * TILE, kRows = 32 / TILE;
-    static_assert(kThreads <= kRenderThreads && kRows * TILE == 32, "tile shape");
-    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    constexpr uint32_t kThreads = TILE * TILE, kStripW = 8, kRows = 4, kStripsX = TILE / kStripW;
+    static_assert(kThreads <= kRenderThreads && kStripW * kRows == 32 && TILE % kStripW == 0, "tile shape");
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t sx = (warp % kStripsX) * kStripW, sy = (warp / kStripsX) * kRows;
     const uint32_t view = viewOfTile(a, tile);
     const DevView vw = a.views[view];
     const uint32_t local = tile - vw.tileBase;
     const uint32_t tx = local % vw.tilesX, ty = local / vw.tilesX;
-    const uint32_t px = tx * TILE + (tid % TILE), py = ty * TILE + (tid / TILE);
+    const uint32_t px = tx * TILE + sx + (lane % kStripW), py = ty * TILE + sy + (lane / kStripW);
     const bool inside = px < vw.width && py < vw.height;
     uint2 range = reinterpret_cast<const uint2*>(a.ranges)[tile];
     // a frame whose look-back gave up (GSR_CONTROL_TIMEOUT) has meaningless ranges: every index
@@ -235,8 +237,8 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
     constexpr int mode = MODE;
     const float fx = float(px), fy = float(py);
     // this warp's pixel strip
-    const float wx0 = float(tx * TILE), wx1 = float(tx * TILE + TILE - 1);
-    const float wy0 = float(ty * TILE + kRows * warp);
+    const float wx0 = float(tx * TILE + sx), wx1 = wx0 + float(kStripW - 1);
+    const float wy0 = float(ty * TILE + sy);
     float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
     bool done = !inside;
 
@@ -348,7 +350,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
         // the warp tests 32 records at a time against its strip, one per lane, and visits the
         // hits in list order
         for (uint32_t q0 = 0; q0 < n && !__all_sync(0xffffffffu, done); q0 += 32) {
-            const uint32_t ql = q0 + (tid & 31u);
+            const uint32_t ql = q0 + lane;
             const bool hit = ql < n && stripHit<kRows>(sm.center[ql], sm.cull[ql], wx0, wx1, wy0);
             for (uint32_t m = __ballot_sync(0xffffffffu, hit); m != 0u; m &= m - 1u) {
                 const uint32_t q = q0 + uint32_t(__ffs(m)) - 1u;
