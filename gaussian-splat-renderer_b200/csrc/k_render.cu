@@ -354,15 +354,14 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
             const bool hit = ql < n && stripHit<kRows>(sm.center[ql], sm.cull[ql], wx0, wx1, wy0);
             for (uint32_t m = __ballot_sync(0xffffffffu, hit); m != 0u; m &= m - 1u) {
                 const uint32_t q = q0 + uint32_t(__ffs(m)) - 1u;
-                if (done) continue;
                 const float2 c = sm.center[q];
                 const float4 co = sm.conic[q];
                 const float dx = c.x - fx;
                 const float dy = c.y - fy;
                 const float power2 = co.x * dx * dx + co.z * dy * dy + co.y * dx * dy;
-                if (power2 > 0.0f) continue;
                 const float alpha = fminf(kMaxAlpha, co.w * fastExp2(power2));
-                if (alpha < (1.0f / 255.0f)) continue;
+                // skipped: a finished pixel, power > 0, alpha below 1/255 (one predicate)
+                if (done || power2 > 0.0f || alpha < (1.0f / 255.0f)) continue;
                 if constexpr (CAP > 0) {
                     // the depth of the gaussian's maximum along the pixel ray: (v . b) / (v^T P v)
                     const float4 pa = ray[buf][0][q], pb = ray[buf][1][q];
