@@ -179,11 +179,58 @@ struct ColourJob {
     float dir[3];  // normalize(mean - camera position), glm::normalize's order
 };
 
+// Staged SH (soa scenes with 16 stored coefficients and no per-gaussian degree): at block start
+// one thread copies the block's 256 x 192 bytes of SH into shared memory with one bulk copy
+// (cp.async.bulk, completed on an mbarrier), so the coefficients arrive while the geometry is
+// computed and the colour reads them from shared memory. Every wait is bounded: on expiry the
+// frame records GSR_CONTROL_TIMEOUT (kWaitShStage) and the thread reads global memory instead.
+__shared__ alignas(8) uint64_t gShBarrier;
+extern __shared__ float4 gShStage[];  // [kFrontThreads * 12]
+
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ bool shStageReady() {
+    uint32_t done = 0;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done) : "r"(smemAddr(&gShBarrier)) : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ bool waitShStage(DeviceControl* ctl) {
+    for (uint32_t spins = 0; spins < kSpinLimit; ++spins)
+        if (shStageReady()) return true;
+    reportTimeout(ctl, kWaitShStage);
+    return false;
+}
+
+// Thread 0, after the barrier's init is visible: the block's SH range [i0, i0 + n).
+__device__ __forceinline__ void issueShStage(const SceneArgs& s, uint32_t i0, uint32_t n) {
+    const uint32_t bytes = n * 192u;
+    const float* src = s.shSoa + size_t(i0) * 48;
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smemAddr(&gShBarrier)), "r"(bytes)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smemAddr(gShStage)), "l"(src), "r"(bytes), "r"(smemAddr(&gShBarrier)) : "memory");
+}
+
 // The plain colour: the gaussian's SH coefficients, evaluated in the view direction.
 template <int COLOR>
 __device__ __forceinline__ void shColour(const FrontArgs& a, uint32_t i, const ColourJob& job, DevSplat& s) {
     float sh[48];
-    loadSH<COLOR>(a.scene, i, (job.degree + 1) * (job.degree + 1), job.meta, sh);
+    const uint32_t used = (job.degree + 1) * (job.degree + 1);
+    if (COLOR == GSR_COLOR_SOA_F32 && a.shStaged && waitShStage(a.ctl)) {
+        const float4* p = gShStage + threadIdx.x * 12;
+#pragma unroll
+        for (int v = 0; v < 12; ++v) {
+            if (uint32_t(v) * 4 < used * 3) {
+                const float4 f = p[v];
+                sh[v * 4 + 0] = f.x; sh[v * 4 + 1] = f.y; sh[v * 4 + 2] = f.z; sh[v * 4 + 3] = f.w;
+            }
+        }
+    } else {
+        loadSH<COLOR>(a.scene, i, used, job.meta, sh);
+    }
     float color[3];
     evalSH(int(job.degree), sh, job.dir[0], job.dir[1], job.dir[2], color);
     s.r = color[0];
@@ -342,6 +389,14 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
     static_assert(sizeof(DevCamera) == sizeof(DevCameraArgs) && sizeof(DevCamera) % 4 == 0, "camera layout");
     if (tid < sizeof(DevCamera) / 4)
         reinterpret_cast<uint32_t*>(&sCam)[tid] = reinterpret_cast<const uint32_t*>(a.cam + view)[tid];
+    const bool staged = COLOR == GSR_COLOR_SOA_F32 && a.shStaged;
+    if (staged && tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smemAddr(&gShBarrier)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint32_t i0 = blockIdx.x * kFrontThreads;
+        issueShStage(a.scene, i0, a.count - i0 < kFrontThreads ? a.count - i0 : kFrontThreads);
+    }
     LearnedShared* sl = nullptr;
     if constexpr (LEARNED) {
         __shared__ LearnedShared sLearned;
@@ -403,6 +458,8 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
         atomicMax(&sDepthMax, dmax);
     }
     __syncthreads();
+    // the bulk copy must have landed before the block's shared memory is released
+    if (staged && tid == 0 && !shStageReady()) waitShStage(a.ctl);
     if (tid < kCullReasonCount && sCull[tid]) atomicAdd(&a.ctl->c.cull_counts[tid], sCull[tid]);
     if (tid == 0 && sDepthMin <= sDepthMax) {
         atomicMin(&a.ctl->c.depth_min_bits, sDepthMin);
@@ -598,15 +655,32 @@ cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capaci
 }
 
 namespace {
+constexpr int kShStageBytes = kFrontThreads * 192;
+template <int GEOM, int COLOR, bool LEARNED, bool EXTRAS>
+void launchPreprocessT(const FrontArgs& a, dim3 blocks, cudaStream_t s) {
+    static bool configured = false;
+    if (COLOR == GSR_COLOR_SOA_F32 && !configured) {
+        cudaFuncSetAttribute(preprocessKernel<GEOM, COLOR, LEARNED, EXTRAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kShStageBytes);
+        configured = true;
+    }
+    preprocessKernel<GEOM, COLOR, LEARNED, EXTRAS><<<blocks, kFrontThreads, a.shStaged ? kShStageBytes : 0, s>>>(a);
+}
 template <int GEOM, int COLOR>
 void launchPreprocess(const FrontArgs& a, dim3 blocks, cudaStream_t s) {
     const bool extras = a.renderSplat != kRenderSplatFull || a.rayDepth != nullptr;
+    FrontArgs b = a;
+    // staging: soa with 16 stored coefficients and no per-gaussian degree (192 bytes a gaussian,
+    // so every block's range starts on a 16-byte boundary); not with the learned colour, which
+    // reads SH only for its fallback gaussians
+    b.shStaged = COLOR == GSR_COLOR_SOA_F32 && !a.latents && a.scene.storedCoeffs == 16 &&
+                 a.scene.variableSh == GSR_VARIABLE_SH_OFF && (reinterpret_cast<uintptr_t>(a.scene.shSoa) & 15u) == 0;
     if (a.latents) {
-        if (extras) preprocessKernel<GEOM, COLOR, true, true><<<blocks, kFrontThreads, 0, s>>>(a);
-        else preprocessKernel<GEOM, COLOR, true, false><<<blocks, kFrontThreads, 0, s>>>(a);
+        if (extras) launchPreprocessT<GEOM, COLOR, true, true>(b, blocks, s);
+        else launchPreprocessT<GEOM, COLOR, true, false>(b, blocks, s);
     } else {
-        if (extras) preprocessKernel<GEOM, COLOR, false, true><<<blocks, kFrontThreads, 0, s>>>(a);
-        else preprocessKernel<GEOM, COLOR, false, false><<<blocks, kFrontThreads, 0, s>>>(a);
+        if (extras) launchPreprocessT<GEOM, COLOR, false, true>(b, blocks, s);
+        else launchPreprocessT<GEOM, COLOR, false, false>(b, blocks, s);
     }
 }
 template <int GEOM, int COLOR>

@@ -76,6 +76,7 @@ struct FrontArgs {
     // binning mode (the reference's default list construction): the records ordered by
     // (depth, record index), a packed word per record, sorted on the device
     uint32_t binning;
+    uint32_t shStaged;                    // soa SH3 scenes: each block's SH copied to shared memory by one bulk copy
     uint64_t* depthKeys[2];               // [V * N] (depth mod 2^W, or the no-tile sentinel) << recordBits | record
     const struct SortPlan* depthPlan;     // its sort's plan (which buffer holds the result)
     uint32_t recordBits;                  // bits of a record index (V * N - 1)
