@@ -197,9 +197,17 @@ __device__ __forceinline__ bool shStageReady() {
     return done != 0;
 }
 
-__device__ __forceinline__ bool waitShStage(DeviceControl* ctl) {
-    for (uint32_t spins = 0; spins < kSpinLimit; ++spins)
+// honorForce: the test hook (DeviceControl::forceTimeout) makes the wait see no completion for
+// that many spins and give up; the wait before the block exits ignores it.
+__device__ __forceinline__ bool waitShStage(DeviceControl* ctl, bool honorForce) {
+    const uint32_t forced = honorForce ? ctl->forceTimeout : 0u;
+    for (uint32_t spins = 0; spins < kSpinLimit; ++spins) {
+        if (forced) {
+            if (spins >= forced) break;
+            continue;
+        }
         if (shStageReady()) return true;
+    }
     reportTimeout(ctl, kWaitShStage);
     return false;
 }
@@ -219,7 +227,7 @@ template <int COLOR>
 __device__ __forceinline__ void shColour(const FrontArgs& a, uint32_t i, const ColourJob& job, DevSplat& s) {
     float sh[48];
     const uint32_t used = (job.degree + 1) * (job.degree + 1);
-    if (COLOR == GSR_COLOR_SOA_F32 && a.shStaged && waitShStage(a.ctl)) {
+    if (COLOR == GSR_COLOR_SOA_F32 && a.shStaged && waitShStage(a.ctl, true)) {
         const float4* p = gShStage + threadIdx.x * 12;
 #pragma unroll
         for (int v = 0; v < 12; ++v) {
@@ -459,7 +467,7 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
     }
     __syncthreads();
     // the bulk copy must have landed before the block's shared memory is released
-    if (staged && tid == 0 && !shStageReady()) waitShStage(a.ctl);
+    if (staged && tid == 0 && !shStageReady()) waitShStage(a.ctl, false);
     if (tid < kCullReasonCount && sCull[tid]) atomicAdd(&a.ctl->c.cull_counts[tid], sCull[tid]);
     if (tid == 0 && sDepthMin <= sDepthMax) {
         atomicMin(&a.ctl->c.depth_min_bits, sDepthMin);

@@ -407,8 +407,10 @@ int gsr_renderer_pass_times(GsrRenderer* r, float* ms, const char** names, uint3
 int gsr_renderer_capacity(GsrRenderer* r, uint32_t* capacity, uint32_t* max_capacity, uint32_t* resizes);
 /* Kernels of this library that gsr_render has launched on this renderer so far. */
 int gsr_renderer_kernel_launches(GsrRenderer* r, uint64_t* count);
-/* Test hook: forces the look-back waits of the next frame to see no predecessor, so that
- * they run into their iteration limit and report GSR_CONTROL_TIMEOUT (iterations = limit). */
+/* Test hook: forces the look-back waits of the next frame to see no predecessor, and the
+ * preprocess's waits for its staged SH to see no completion (those read the SH from global
+ * memory instead), so that they run into their iteration limit and report GSR_CONTROL_TIMEOUT
+ * (iterations = limit; timeout_where 1 scan, 2 sort, 4 SH staging). */
 int gsr_renderer_debug_force_timeout(GsrRenderer* r, uint32_t iterations);
 void gsr_renderer_destroy(GsrRenderer* r);
 

@@ -32,7 +32,7 @@ def test_forced_lookback_timeout_is_reported_and_recoverable(gpu, port, setup):
     r.render(cam)
     c = r.read_control()
     assert c.status & gpu.CONTROL_TIMEOUT
-    assert c.timeout_where in (1, 2)
+    assert c.timeout_where in (1, 2, 4)
     st = gpu.load().gsr_read_control(r.handle, gpu.C.byref(gpu.Control()))
     assert st == 5  # GSR_ERROR_DEVICE_TIMEOUT
     r.render(cam)  # the next frame is valid again
@@ -40,6 +40,26 @@ def test_forced_lookback_timeout_is_reported_and_recoverable(gpu, port, setup):
     assert again[4].status == 0
     for a, b in zip(good[:4], again[:4]):
         np.testing.assert_array_equal(a, b)
+
+
+def test_forced_sh_stage_timeout_falls_back_to_global_reads(gpu, port, setup):
+    """The preprocess of an soa SH3 scene stages each block's SH in shared memory; a forced
+    expiry of that wait reads the coefficients from global memory: the splat records equal the
+    staged frame's bit for bit and the frame reports the timeout."""
+    scene, cam = setup
+    gs = gpu.GpuScene(scene)
+    r = gpu.Renderer(gs, gpu.Settings(adaptive_list=False))
+    r.render(cam)
+    good, _ = r.read_back_splats(scene.count)
+    r.force_timeout(64)
+    r.render(cam)
+    c = r.read_control()
+    assert c.status & gpu.CONTROL_TIMEOUT
+    forced, _ = r.read_back_splats(scene.count)
+    vis = good["cullReason"] == 0
+    assert vis.sum() > 1000 and forced[vis].tobytes() == good[vis].tobytes()
+    r.render(cam)
+    assert r.read_control().status == 0
 
 
 def test_adaptive_list_grows_after_overflow(gpu, port, setup):
