@@ -5,15 +5,18 @@
 
 Workload (default): the plain forward render at 1920x1080 of 1,240,000 synthetic gaussians
 (means uniform in a ball of radius 8, SH degree 3, fp32 SoA scene), on the 300-frame 360-degree
-orbit of radius 14 at height 2; tight tile bounds, adaptive list, global 64-bit key sort. A step
-renders one view of the orbit (view k = frame k mod 300, ranks start at different frames).
+orbit of radius 14 at height 2; tight tile bounds, adaptive list, binning list construction (depth
+sort of the visible splats, emission in depth order, stable sort by tile). A step renders one view
+of the orbit (view k = frame k mod 300, ranks start at different frames). The line's `value` is
+the batched + learned-colour form (the metric's subject); the plain form is in `forms.plain`.
 
 value        views/s over all ranks, scene and camera parameters resident on the device: CUDA
-             events around K consecutive gsr_render calls on one stream (barrier + synchronize
-             on both sides, max over ranks).
-e2e          the same metric through gsr_render_to_host, the call a host application makes:
-             each step passes the camera from host memory and copies the 8-bit RGB image into
-             pinned host memory, then synchronizes. The scene upload is an init-time step
+             events around the timed steps on one stream (gsr_render_views frames of D views for
+             the batched forms, K gsr_render calls for the plain form; barrier + synchronize on
+             both sides, max over ranks).
+e2e          the same metric through gsr_render_views_to_host / gsr_render_to_host, the calls a
+             host application makes: each step passes the cameras from host memory and copies the
+             8-bit RGB images into pinned host memory, then synchronizes. The scene upload is an init-time step
              (GpuScene::upload in the reference) and is not part of a step.
 roofline     the front kernel (preprocess + count + scan + key emission) against the measured
              HBM copy bandwidth: algorithmic bytes per frame / its CUDA-event duration.
@@ -188,7 +191,7 @@ def front_bytes(scene_format: str, ctl, n: int, list_mode: str = "global") -> fl
 FRONT_TRAFFIC_PLAIN_1080P = {
     "global": (296.7 + 61.3 + 5.0 + 89.3 + 8.4) * 1e6,
     # preprocess, depth histogram, 4 depth passes, gathered scan, emission in depth order
-    "binning": (302.1 + 73.5 + 10.0 + 39.7 + 14.9 + 152.6 + 29.0) * 1e6,
+    "binning": (299.3 + 72.5 + 10.0 + 39.7 + 14.9 + 150.8 + 28.6) * 1e6,
 }
 
 
