@@ -440,8 +440,20 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
             }
             const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, cA, cB, cC, cO, a.logf);
             const RowGeom g = rowGeom(cv);
-            count = coverageCount(cv, g, a.binSize);
-            if (a.bounds != kBoundsRect) a.hints[rec] = coverageHint(cv, g);
+            if (a.bounds != kBoundsRect) {
+                uint32_t* hintWords = reinterpret_cast<uint32_t*>(a.hints + rec);
+                int r0, rows;
+                bool spanForm;
+                count = coverageCountSpans(cv, g, a.binSize, gx, hintWords, reinterpret_cast<uint32_t*>(a.spanRows + rec),
+                                           r0, rows, spanForm);
+                if (spanForm) {
+                    hintWords[0] = kSpanMarker | uint32_t(r0) | (uint32_t(rows) << 16);
+                } else {
+                    a.hints[rec] = coverageHint(cv, g);
+                }
+            } else {
+                count = coverageCount(cv, g, a.binSize);
+            }
             s.cullReason = kCullVisible;
             if (!EXTRAS || a.renderSplat == kRenderSplatFull) reinterpret_cast<DevSplat*>(a.splats)[rec] = s;
             else writePackedSplat(a, rec, s, rect, p24w0, p24w1);
@@ -519,6 +531,63 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
         const uint32_t offset = a.offsets[slot];
         const DevView vw = a.views[view];
         const int gx = int(vw.tilesX), gy = int(vw.tilesY);  // the view's binning grid
+        const float4 hint = a.bounds != kBoundsRect ? a.hints[rec] : make_float4(-2.0f, 0.0f, 0.0f, 0.0f);
+        if (isSpanHint(hint)) {
+            // the runs the count was made of: no record, no ellipse (binning keys need no depth)
+            const uint32_t head = __float_as_uint(hint.x);
+            const int r0 = int(head & 0xFFFFu), rows = int((head >> 16) & 0x7u);
+            uint32_t span[kSpanRows] = {__float_as_uint(hint.y), __float_as_uint(hint.z), __float_as_uint(hint.w),
+                                        0u, 0u, 0u, 0u};
+            if (rows > 3) {
+                const uint4 more = a.spanRows[rec];
+                span[3] = more.x;
+                span[4] = more.y;
+                span[5] = more.z;
+                span[6] = more.w;
+            }
+            uint64_t depthBits = 0;
+            if (!BINNING || !lay.packed)
+                depthBits = a.renderSplat == kRenderSplatFull ? __float_as_uint(reinterpret_cast<const DevSplat*>(a.splats)[rec].depth)
+                                                              : a.depths[rec];
+            const uint64_t packedBase =
+                ((lay.lowBits >= 32 ? depthBits : (depthBits & ((1ull << lay.lowBits) - 1ull))) << lay.indexBits) | i;
+            const uint32_t tileShift = lay.lowBits + lay.indexBits;
+            uint32_t k = offset, written = 0, tileMax = 0;
+#pragma unroll
+            for (int r = 0; r < kSpanRows; ++r) {
+                if (r < rows) {
+                    const uint32_t x0 = span[r] & 0xFFFFu, x1 = span[r] >> 16;
+                    const uint32_t rowBase = vw.tileBase + uint32_t(r0 + r) * uint32_t(gx);
+                    for (uint32_t x = x0; x < x1 && written < count; ++x, ++written, ++k) {
+                        const uint32_t tile = rowBase + x;
+                        tileMax = tile > tileMax ? tile : tileMax;
+                        if (k < a.capacity) {
+                            if (lay.packed) {
+                                a.keys[k] = (uint64_t(tile) << tileShift) | packedBase;
+                            } else {
+                                a.keys[k] = (uint64_t(tile) << 32) | depthBits;
+                                a.values[k] = i;
+                            }
+                        }
+                    }
+                }
+            }
+            if (written != count) {  // the runs hold the count's tiles: never, but treated as below
+                atomicAdd(&sMismatch, 1u);
+                tileMax = sentinel;
+                for (; written < count; ++written, ++k) {
+                    if (k >= a.capacity) continue;
+                    if (lay.packed) {
+                        a.keys[k] = (uint64_t(sentinel) << tileShift) | packedBase;
+                    } else {
+                        a.keys[k] = (uint64_t(sentinel) << 32) | depthBits;
+                        a.values[k] = i;
+                    }
+                }
+            }
+            atomicMax(&sTileMax, tileMax);
+            sAny = 1;
+        } else {
         // centre, conic, rectangle and depth from the record (full) or the packed arrays
         float cx, cy, cA, cB, cC;
         TileRect rect;
@@ -552,7 +621,6 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
             }
         }
         RowGeom g;
-        const float4 hint = a.bounds != kBoundsRect ? a.hints[rec] : make_float4(-2.0f, 0.0f, 0.0f, 0.0f);
         const Coverage cv = coverageFromHint(a.bounds, rect, a.binSize, gx, gy, cx, cy, cA, cB, cC, hint, g);
         // packed: (((tile << W) | depth mod 2^W) << indexBits) | index; the tile part added per entry
         const uint64_t packedBase =
@@ -589,6 +657,7 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
         }
         atomicMax(&sTileMax, tileMax);
         sAny = 1;
+        }
     }
     __syncthreads();
     if (tid == 0 && sAny) {

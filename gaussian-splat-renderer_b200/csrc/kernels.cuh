@@ -67,7 +67,9 @@ struct FrontArgs {
     uint2* rects;         // [V * N] packed tile rectangles, P32 / P24
     float4* rayDepth;     // [V * N * 3] StopThePop ray-depth parameters of visible gaussians, or null
     uint32_t* depths;     // [V * N] depth bits, P32 / P24
-    float4* hints;        // [V * N] cutoff-ellipse terms of visible gaussians (coverageHint), tight/cutoff bounds
+    float4* hints;        // [V * N] cutoff-ellipse terms of visible gaussians (coverageHint), tight/cutoff bounds,
+                          // or rows 0-3 of their runs (span hints)
+    uint4* spanRows;      // [V * N] rows 3-6 of span hints with more than 3 rows
     uint32_t* tileCounts; // [V * N]
     uint32_t* offsets;    // [V * N] exclusive scan of tileCounts
     uint64_t* keys;       // [capacity] (tile << 32 | depth bits), view-major index order

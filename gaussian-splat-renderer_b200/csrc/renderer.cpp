@@ -369,7 +369,7 @@ struct GsrRenderer {
     const DecoderWeights* colorDecoder = nullptr;
 
     // per gaussian
-    DevBuf splats, hints, tileCounts, offsets, scanStatus;
+    DevBuf splats, hints, spanRows, tileCounts, offsets, scanStatus;
     DevBuf packedSplats, rects, depths;  // packed render records (P32 / P24) and their side arrays
     DevBuf rayDepth;                     // StopThePop ray-depth parameters (3 x float4 per record)
     // control + plan
@@ -519,6 +519,7 @@ struct GsrRenderer {
             GSR_CUDA(cudaMemset(depths.p, 0, depths.bytes));
         }
         GSR_CUDA(hints.alloc(n * 16));
+        GSR_CUDA(spanRows.alloc(n * 16));
         if (settings.sort_window > 0) GSR_CUDA(rayDepth.alloc(n * 48));
         if (binning()) {
             for (auto& k : depthKeys) GSR_CUDA(k.alloc(n * 8));
@@ -768,6 +769,7 @@ struct GsrRenderer {
         fa.depths = depths.as<uint32_t>();
         fa.rayDepth = settings.sort_window > 0 ? rayDepth.as<float4>() : nullptr;
         fa.hints = hints.as<float4>();
+        fa.spanRows = spanRows.as<uint4>();
         fa.tileCounts = tileCounts.as<uint32_t>();
         fa.offsets = offsets.as<uint32_t>();
         fa.keys = l.keys[0].as<uint64_t>();

@@ -376,6 +376,42 @@ __device__ __forceinline__ uint32_t coverageCount(const Coverage& cv, const RowG
     return n;
 }
 
+// Span hints: the coverage of a visible gaussian as its rows' runs, kept by the preprocess (which
+// computes them for the count anyway) when it has at most kSpanRows rows and fewer than 65536
+// bins a row, so that the emission needs neither the record nor the ellipse's square roots and
+// quotients. Word x of the hint is a quiet NaN carrying r0 (16 bits) and the row count (3 bits),
+// which no float hint has (their x is t: finite, or -2); words y, z, w hold rows 0-2 as
+// x0 | x1 << 16, the second array's four words rows 3-6.
+constexpr int kSpanRows = 7;
+constexpr uint32_t kSpanMarker = 0x7FC00000u;
+__device__ __forceinline__ bool isSpanHint(const float4& h) {
+    return (__float_as_uint(h.x) & 0xFFC00000u) == kSpanMarker;
+}
+
+// coverageCount that also stores the rows' runs of a span hint (spanForm: rows <= kSpanRows and
+// the grid's width below 65536) into `hint` (rows 0-2, words 1-3) and `more` (rows 3-6).
+__device__ __forceinline__ uint32_t coverageCountSpans(const Coverage& cv, const RowGeom& g, int S, int gx,
+                                                       uint32_t* hint, uint32_t* more, int& r0, int& rows,
+                                                       bool& spanForm) {
+    int r1;
+    coverageRows(cv, S, r0, r1);
+    rows = r1 - r0;
+    spanForm = r1 - r0 <= kSpanRows && gx < 65536 && r0 >= 0 && r0 < 65536;
+    uint32_t n = 0;
+    for (int r = r0; r < r1; ++r) {
+        int x0, x1;
+        coverageRowSpan(cv, g, r, S, x0, x1);
+        n += uint32_t(x1 - x0);
+        if (spanForm) {
+            const int k = r - r0;
+            const uint32_t w = uint32_t(x0) | (uint32_t(x1) << 16);
+            if (k < 3) hint[1 + k] = w;
+            else more[k - 3] = w;
+        }
+    }
+    return n;
+}
+
 // What the key emission needs of a visible gaussian's coverage beyond its record, kept by the
 // preprocess so that the emission does not evaluate the logarithm, the square roots and the
 // quotients of the cutoff ellipse again: (t, ex, ey, eyRight0), t = -2 for an invalid ellipse.
