@@ -376,40 +376,53 @@ __global__ void __launch_bounds__(kSortThreads, 4) depthPassKernel(const __grid_
     sortPassTiles<false, kDepthSortItems>(a, p, smem, sOff, sScan, sTile);
 }
 
-// The gaussian index and the tile of sorted entry k in either layout.
-__device__ __forceinline__ uint32_t entryTile(const uint64_t* keys, uint32_t k, const SortPlan* plan) {
-    const uint64_t key = keys[k];
-    return plan->packed ? uint32_t(key >> (plan->indexBits + plan->lowBits)) : uint32_t(key >> 32);
-}
-
 // ---- tile ranges (tile_ranges.comp:22-44) -----------------------------------------------------
-__global__ void rangesKernel(const __grid_constant__ RenderArgs a) {
+// Each thread takes 8 consecutive sorted entries (four 16-byte loads) and the entry before them,
+// so the loads stream at the copy's width; a range starts where the tile changes and ends where
+// the next one starts (or at the list's end).
+constexpr uint32_t kRangeItems = 8;
+__global__ void __launch_bounds__(256) rangesKernel(const __grid_constant__ RenderArgs a) {
     const DeviceControl* ctl = a.ctl;
     const uint32_t n = ctl->c.entries;
     const uint64_t* keys = a.keys[ctl->c.sorted_buffer & 1u];
     const uint32_t tileCount = a.totalTiles;  // every view's tiles; the sentinel is this id
     uint2* ranges = reinterpret_cast<uint2*>(a.ranges);
-    const SortPlan* plan = a.plan;
-    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const uint32_t tile = entryTile(keys, k, plan);
-        if (tile >= tileCount) {
-            // the sentinel tile (sorted last) closes the last real tile's range
-            if (k > 0) {
-                const uint32_t prev = entryTile(keys, k - 1, plan);
-                if (prev < tileCount) ranges[prev].y = k;
+    const uint32_t shift = a.plan->packed ? a.plan->indexBits + a.plan->lowBits : 32u;
+    const uint32_t stride = gridDim.x * blockDim.x * kRangeItems;
+    for (uint32_t base = (blockIdx.x * blockDim.x + threadIdx.x) * kRangeItems; base < n; base += stride) {
+        uint32_t t[kRangeItems];
+        if (base + kRangeItems <= n) {
+            const uint4* v = reinterpret_cast<const uint4*>(keys + base);
+#pragma unroll
+            for (uint32_t j = 0; j < kRangeItems / 2; ++j) {
+                const uint4 w = __ldg(&v[j]);
+                t[2 * j] = uint32_t(((uint64_t(w.y) << 32) | w.x) >> shift);
+                t[2 * j + 1] = uint32_t(((uint64_t(w.w) << 32) | w.z) >> shift);
             }
-            continue;
-        }
-        if (k == 0) {
-            ranges[tile].x = 0;
         } else {
-            const uint32_t prev = entryTile(keys, k - 1, plan);
-            if (prev != tile) {
-                if (prev < tileCount) ranges[prev].y = k;
-                ranges[tile].x = k;
-            }
+#pragma unroll
+            for (uint32_t j = 0; j < kRangeItems; ++j) t[j] = base + j < n ? uint32_t(keys[base + j] >> shift) : 0u;
         }
-        if (k == n - 1) ranges[tile].y = n;
+        uint32_t prev = base > 0 ? uint32_t(keys[base - 1] >> shift) : 0u;
+#pragma unroll
+        for (uint32_t j = 0; j < kRangeItems; ++j) {
+            const uint32_t k = base + j;
+            if (k >= n) break;
+            const uint32_t tile = t[j];
+            if (tile >= tileCount) {
+                // the sentinel tile (sorted last) closes the last real tile's range
+                if (k > 0 && prev < tileCount) ranges[prev].y = k;
+            } else {
+                if (k == 0) {
+                    ranges[tile].x = 0;
+                } else if (prev != tile) {
+                    if (prev < tileCount) ranges[prev].y = k;
+                    ranges[tile].x = k;
+                }
+                if (k == n - 1) ranges[tile].y = n;
+            }
+            prev = tile;
+        }
     }
 }
 
@@ -526,7 +539,7 @@ cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s) {
 }
 
 cudaError_t launchRanges(const RenderArgs& a, uint32_t capacity, cudaStream_t s) {
-    rangesKernel<<<gridFor(capacity, 256, 148 * 16), 256, 0, s>>>(a);
+    rangesKernel<<<gridFor((capacity + kRangeItems - 1) / kRangeItems, 256, 148 * 16), 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
