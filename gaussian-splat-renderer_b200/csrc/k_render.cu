@@ -63,24 +63,39 @@ __device__ __forceinline__ float approxSqrt(float x) {
     return y;
 }
 
-// Whether a record's cutoff ellipse q(d) = A dx^2 + 2B dx dy + C dy^2 <= t meets any pixel centre
-// of a warp's strip: ROWS rows from y0, columns [x0, x1]. Row y holds the run
-// |px - (cx + (B/A) dy)| <= sqrt((t - (D/A) dy^2) / A), dy = cy - y; the row test inflates t by
-// 0.2 %, moves the row 0.05 px towards the centre and widens the run by 0.1 % + 0.05 px (the
-// margins of the tile-coverage box), and any NaN keeps the record.
-template <uint32_t ROWS>
-__device__ __forceinline__ bool stripHit(float2 c, float4 k, float x0, float x1, float y0) {
-    bool hit = false;
+// The warp strips (8 x 4 pixel blocks of a TILE x TILE tile; bit w = warp w's) that a record's
+// cutoff ellipse q(d) = A dx^2 + 2B dx dy + C dy^2 <= t meets, computed once per record. At
+// distance dy = cy - y from the centre the ellipse's run is cx + (B/A) dy -/+ sqrt((t - (D/A) dy^2)
+// / A); over a strip row's y-range its right edge (concave in dy) peaks at the ellipse's
+// rightmost point dy = B sqrt(t / (C D)) clamped into the range, its left edge at the mirror
+// point. The test keeps the margins of the tile-coverage box: t + 0.2 %, the y-range widened by
+// 0.05 px, the run by 0.1 % + 0.05 px, over a continuous y-range (a superset of the pixel rows),
+// so a strip holding a pixel with alpha >= 1/255 is always set; a NaN sets the strip.
+template <uint32_t TILE>
+__device__ __forceinline__ uint32_t stripMask(float cx, float cy, float A, float B, float C, float D, float t,
+                                              float tileX, float tileY) {
+    constexpr uint32_t kStripsX = TILE / 8, kGroups = TILE / 4;
+    const float tt = t * 1.002f;
+    const float ia = 1.0f / A, bA = B * ia, dA = D * ia;
+    const float ey = approxSqrt(tt / dA);
+    const float dyR = B * approxSqrt(tt / (C * D));
+    uint32_t mask = 0;
 #pragma unroll
-    for (uint32_t r = 0; r < ROWS; ++r) {
-        const float dy = c.y - (y0 + float(r));
-        const float dyIn = copysignf(fmaxf(fabsf(dy) - 0.05f, 0.0f), dy);
-        const float s = fmaf(-k.y * dyIn, dyIn, k.w * 1.002f);
-        const float hw = fmaf(approxSqrt(fmaxf(s, 0.0f) * k.z), 1.001f, 0.05f);
-        const float xc = fmaf(k.x, dy, c.x);
-        hit |= !(s < 0.0f) && !(xc - hw > x1) && !(xc + hw < x0);
+    for (uint32_t g = 0; g < kGroups; ++g) {
+        const float ya = tileY + float(4 * g) - 0.05f, yb = tileY + float(4 * g + 3) + 0.05f;
+        const float lo = fmaxf(cy - yb, -ey), hi = fminf(cy - ya, ey);  // dy range inside the ellipse
+        if (lo > hi) continue;
+        const float dr = fminf(fmaxf(dyR, lo), hi), dl = fminf(fmaxf(-dyR, lo), hi);
+        const float hr = fmaf(approxSqrt(fmaxf(fmaf(-dA * dr, dr, tt), 0.0f) * ia), 1.001f, 0.05f);
+        const float hl = fmaf(approxSqrt(fmaxf(fmaf(-dA * dl, dl, tt), 0.0f) * ia), 1.001f, 0.05f);
+        const float right = fmaf(bA, dr, cx) + hr, left = fmaf(bA, dl, cx) - hl;
+#pragma unroll
+        for (uint32_t c = 0; c < kStripsX; ++c) {
+            const float x0 = tileX + float(8 * c), x1 = x0 + 7.0f;
+            if (!(right < x0) && !(left > x1)) mask |= 1u << (g * kStripsX + c);
+        }
     }
-    return hit;
+    return mask;
 }
 
 // N = the batch (one entry per thread of the tile's block)
@@ -90,7 +105,7 @@ struct RenderShared {
     // N in the first half of the area)
     float4 raw[2][3][N];
     float4 conic[N];      // a', b', c' (pre-scaled), opacity
-    float4 cull[N];       // B/A, D/A, 1/A, t: the cutoff ellipse's row extents (stripHit)
+    uint32_t strips[N];   // the warp strips the cutoff ellipse meets (stripMask)
     float4 color[N];      // r, g, b, -
     float2 center[N];
     uint32_t tile;        // persistent schedule: the block's current tile
@@ -237,8 +252,6 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
     constexpr int mode = MODE;
     const float fx = float(px), fy = float(py);
     // this warp's pixel strip
-    const float wx0 = float(tx * TILE + sx), wx1 = wx0 + float(kStripW - 1);
-    const float wy0 = float(ty * TILE + sy);
     float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
     bool done = !inside;
 
@@ -324,34 +337,31 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
                 p24DecodeConic(w1.x, w1.y, A, B, C, o);
                 r2 = make_float4(halfLoF(w2.x), halfHiF(w2.x), halfLoF(w2.y), 0.0f);
             }
-            // the cutoff ellipse for the strip tests (makeCutoffEllipse's threshold, wider margin):
-            // t < 0 misses every row (opacity below 1/255), an invalid conic meets every row
-            float4 cull = make_float4(0.0f, 0.0f, 1.0f, 3.0e38f);
+            // the strips the cutoff ellipse meets (makeCutoffEllipse's threshold, wider margin):
+            // none below opacity 1/255, all for an invalid conic
+            uint32_t strips = (1u << (kThreads / 32)) - 1u;
             const float D = A * C - B * B;
             if (!(o >= 1.0f / 255.0f)) {
-                cull.w = -3.0e38f;
+                strips = 0u;
             } else if (A > 0.0f && C > 0.0f && D > 0.0f) {
                 const float qmax = 2.0f * __logf(255.0f * o) + 1e-3f;
                 const float rho = fabsf(B) * rsqrtf(A * C);
                 const float K = 2.0f / fmaxf(1.0f - rho, 1e-30f);
                 const float t = qmax + (2e-3f + 4e-5f * K) * fmaxf(qmax, 1.0f) + 4e-3f;
-                if (t < 1e30f) {
-                    const float ia = 1.0f / A;
-                    cull = make_float4(B * ia, D * ia, ia, t);
-                }
+                if (t < 1e30f) strips = stripMask<TILE>(r0.x, r0.y, A, B, C, D, t, float(tx * TILE), float(ty * TILE));
             }
-            sm.cull[tid] = cull;
+            sm.strips[tid] = strips;
             sm.conic[tid] = make_float4(-0.5f * kLog2e * A, -kLog2e * B, -0.5f * kLog2e * C, o);
             sm.color[tid] = r2;
             sm.center[tid] = make_float2(r0.x, r0.y);
         }
         __syncthreads();
         const uint32_t n = range.y - start < kThreads ? range.y - start : kThreads;
-        // the warp tests 32 records at a time against its strip, one per lane, and visits the
-        // hits in list order
+        // the warp takes 32 records at a time, one per lane, and visits those that meet its strip
+        // in list order
         for (uint32_t q0 = 0; q0 < n && !__all_sync(0xffffffffu, done); q0 += 32) {
             const uint32_t ql = q0 + lane;
-            const bool hit = ql < n && stripHit<kRows>(sm.center[ql], sm.cull[ql], wx0, wx1, wy0);
+            const bool hit = ql < n && ((sm.strips[ql] >> warp) & 1u) != 0u;
             for (uint32_t m = __ballot_sync(0xffffffffu, hit); m != 0u; m &= m - 1u) {
                 const uint32_t q = q0 + uint32_t(__ffs(m)) - 1u;
                 const float2 c = sm.center[q];
@@ -429,8 +439,10 @@ __device__ __forceinline__ float4 (*rayArea(unsigned char* smem))[3][N] {
     return reinterpret_cast<float4(*)[3][N]>(smem + sizeof(RenderShared<N>));
 }
 
+// Without the window: five 256-thread blocks (or the same threads in 8-px tiles) per SM, 48
+// registers a thread (the strip masks would take 61, four blocks, 5 % slower).
 template <int MODE, int CAP, int TILE>
-__global__ void __launch_bounds__(TILE * TILE) renderKernel(const __grid_constant__ RenderArgs a) {
+__global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1) renderKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     renderTile<MODE, CAP, TILE>(a, *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw),
                                 CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, blockIdx.x);
@@ -439,7 +451,7 @@ __global__ void __launch_bounds__(TILE * TILE) renderKernel(const __grid_constan
 // Persistent schedule: each block takes tiles from the frame's queue counter (reset by frame
 // begin) until the counter passes the last tile.
 template <int MODE, int CAP, int TILE>
-__global__ void __launch_bounds__(TILE * TILE) renderPersistentKernel(const __grid_constant__ RenderArgs a) {
+__global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1) renderPersistentKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     RenderShared<TILE * TILE>& sm = *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw);
     for (;;) {
