@@ -736,10 +736,9 @@ constexpr int kShStageBytes = kFrontThreads * 192;
 template <int GEOM, int COLOR, bool LEARNED, bool EXTRAS>
 void launchPreprocessT(const FrontArgs& a, dim3 blocks, cudaStream_t s) {
     static bool configured = false;
-    if (COLOR == GSR_COLOR_SOA_F32 && !configured) {
-        cudaFuncSetAttribute(preprocessKernel<GEOM, COLOR, LEARNED, EXTRAS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             kShStageBytes);
-        configured = true;
+    if (COLOR == GSR_COLOR_SOA_F32 && !configured) {  // (a failure here fails the staged launch below)
+        configured = cudaFuncSetAttribute(preprocessKernel<GEOM, COLOR, LEARNED, EXTRAS>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, kShStageBytes) == cudaSuccess;
     }
     preprocessKernel<GEOM, COLOR, LEARNED, EXTRAS><<<blocks, kFrontThreads, a.shStaged ? kShStageBytes : 0, s>>>(a);
 }
