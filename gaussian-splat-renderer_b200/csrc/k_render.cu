@@ -445,7 +445,7 @@ template <int MODE, int CAP, int TILE>
 __global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1) renderKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     renderTile<MODE, CAP, TILE>(a, *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw),
-                                CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, blockIdx.x);
+                                CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, blockIdx.x + a.tileOffset);
 }
 
 // Persistent schedule: each block takes tiles from the frame's queue counter (reset by frame
@@ -485,7 +485,7 @@ cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
         const uint32_t grid = uint32_t(sms) * kPersistentBlocksPerSm * (kRenderThreads / threads);
         renderPersistentKernel<MODE, CAP, TILE><<<grid < a.totalTiles ? grid : a.totalTiles, threads, smem, s>>>(a);
     } else {
-        renderKernel<MODE, CAP, TILE><<<a.totalTiles, threads, smem, s>>>(a);
+        renderKernel<MODE, CAP, TILE><<<a.tileLaunch ? a.tileLaunch : a.totalTiles, threads, smem, s>>>(a);
     }
     return cudaGetLastError();
 }

@@ -146,6 +146,8 @@ struct RenderArgs {
     uint32_t viewCount;
     uint32_t totalTiles;
     uint32_t persistent;      // 1: a fixed grid takes (view, tile) work items from a queue
+    uint32_t tileOffset;      // per-tile schedule: the launch's first frame tile
+    uint32_t tileLaunch;      // per-tile schedule: the launch's tiles (0: every tile of the frame)
     uint32_t count;           // N: gaussian indices read from the list are checked against it
     DeviceControl* ctl;
     const SortPlan* plan;     // the entry layout (packed words or key/value arrays)

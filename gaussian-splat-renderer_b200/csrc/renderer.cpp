@@ -434,8 +434,10 @@ struct GsrRenderer {
         cudaGraphExec_t graph = nullptr;
         const void* graphList = nullptr;   // the list / layout the graph was captured with
         uint64_t graphLayout = ~0ull;
+        std::vector<cudaEvent_t> viewDone;  // view-by-view frames: each view's image is complete
         ~Slot() {
             if (graph) cudaGraphExecDestroy(graph);
+            for (cudaEvent_t e : viewDone) cudaEventDestroy(e);
         }
     };
     std::vector<std::unique_ptr<Slot>> slots;
@@ -457,6 +459,12 @@ struct GsrRenderer {
     }
 
     cudaStream_t captureStream = nullptr;  // graphs are captured here (never the legacy stream)
+    // gsr_render_views_to_host: the frame's views are rasterized one launch each, and each view's
+    // image goes to the host on copyStream as soon as it is complete (hostCopies asks for it,
+    // lastSplit / lastSlot tell how the last frame ran)
+    bool hostCopies = false, lastSplit = false, splitViews = false;
+    Slot* lastSlot = nullptr;
+    cudaStream_t copyStream = nullptr;
 
     ~GsrRenderer() {
         for (auto& s : slots) {
@@ -467,6 +475,13 @@ struct GsrRenderer {
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         if (captureStream) cudaStreamDestroy(captureStream);
+        if (copyStream) cudaStreamDestroy(copyStream);
+    }
+
+    // the (view, tile) queue rasterizer: asked for, or chosen by the auto schedule for batches
+    bool persistentRaster(uint32_t viewCount) const {
+        return settings.raster_schedule == GSR_RASTER_PERSISTENT ||
+               (settings.raster_schedule == GSR_RASTER_AUTO && viewCount > 1);
     }
 
     uint32_t passesFor(uint32_t tileCount) const {
@@ -692,7 +707,17 @@ struct GsrRenderer {
         // the slot's previous frame has completed: its pinned cameras may be overwritten
         static_assert(sizeof(DevCameraArgs) == sizeof(GsrSplatCamera), "camera layout");
         std::memcpy(slot.camHost, cams, sizeof(GsrSplatCamera) * v);
-        const bool graphed = settings.use_graph && !timing && forceTimeout == 0;
+        // view by view: several per-tile views with their images wanted on the host (not graphed)
+        const bool split = hostCopies && v > 1 && !persistentRaster(v);
+        while (split && slot.viewDone.size() < v) {
+            cudaEvent_t e = nullptr;
+            GSR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            slot.viewDone.push_back(e);
+        }
+        splitViews = split;
+        lastSplit = split;
+        lastSlot = &slot;
+        const bool graphed = settings.use_graph && !timing && forceTimeout == 0 && !split;
         if (graphed) {
             if (!slot.graph || slot.graphList != list.get() || slot.graphLayout != layoutVersion) {
                 if (slot.graph) cudaGraphExecDestroy(slot.graph);
@@ -729,7 +754,7 @@ struct GsrRenderer {
         // frameBegin, preprocess, scan, duplicate, histogram, one per pass, ranges, render
         // binning: frameBegin, preprocess, depth histogram + passes, scan, duplicate, list
         // histogram + passes, ranges, render
-        kernelLaunches += binning() ? 8 + kDepthSortPasses + list->passes : 7 + list->passes;
+        kernelLaunches += (binning() ? 8 + kDepthSortPasses + list->passes : 7 + list->passes) + (split ? v - 1 : 0);
         timed = timing;
         ++frameIndex;
         return GSR_OK;
@@ -841,14 +866,22 @@ struct GsrRenderer {
         ra.views = viewsDevice.as<DevView>();
         ra.viewCount = viewCount;
         ra.totalTiles = tileCount;
-        ra.persistent = settings.raster_schedule == GSR_RASTER_PERSISTENT ||
-                        (settings.raster_schedule == GSR_RASTER_AUTO && viewCount > 1);
+        ra.persistent = persistentRaster(viewCount);
         ra.count = scene.count;
         ra.ctl = ctl;
         ra.plan = sortPlan;
         GSR_CUDA(launchRanges(ra, l.capacity, stream));
         mark(stream);
-        GSR_CUDA(launchRender(ra, stream));
+        if (splitViews) {
+            for (uint32_t j = 0; j < viewCount; ++j) {
+                ra.tileOffset = views[j].tile_base;
+                ra.tileLaunch = views[j].tiles_x * views[j].tiles_y;
+                GSR_CUDA(launchRender(ra, stream));
+                GSR_CUDA(cudaEventRecord(slot.viewDone[j], stream));
+            }
+        } else {
+            GSR_CUDA(launchRender(ra, stream));
+        }
         mark(stream);
 
         GSR_CUDA(cudaMemcpyAsync(slot.host, &ctl->c, sizeof(GsrControl), cudaMemcpyDeviceToHost, stream));
@@ -1349,14 +1382,30 @@ int gsr_render_views(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t vie
 int gsr_render_views_to_host(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* host, uint64_t bytes,
                              void* stream) {
     if (!r || !cameras || !host) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    r->hostCopies = true;
     int rc = gsr_render_views(r, cameras, views, stream);
+    r->hostCopies = false;
     if (rc) return rc;
     const bool rgb = r->rgb8.p != nullptr;
     const uint64_t need = r->totalPixels * (rgb ? 3 : r->imageBytes());
     if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, the views need %llu",
                                    (unsigned long long)bytes, (unsigned long long)need);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    GSR_CUDA(cudaMemcpyAsync(host, rgb ? r->rgb8.p : r->image.p, need, cudaMemcpyDeviceToHost, s));
+    const size_t bpp = rgb ? 3 : r->imageBytes();
+    const unsigned char* src = rgb ? r->rgb8.as<unsigned char>() : r->image.as<unsigned char>();
+    if (r->lastSplit) {  // each view's image as soon as its rasterizer launch is done
+        if (!r->copyStream) GSR_CUDA(cudaStreamCreateWithFlags(&r->copyStream, cudaStreamNonBlocking));
+        for (size_t j = 0; j < r->views.size(); ++j) {
+            const GsrViewLayout& L = r->views[j];
+            const size_t off = size_t(L.pixel_base) * bpp, len = size_t(L.width) * L.height * bpp;
+            GSR_CUDA(cudaStreamWaitEvent(r->copyStream, r->lastSlot->viewDone[j], 0));
+            GSR_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(host) + off, src + off, len, cudaMemcpyDeviceToHost,
+                                     r->copyStream));
+        }
+        GSR_CUDA(cudaStreamSynchronize(r->copyStream));
+    } else {
+        GSR_CUDA(cudaMemcpyAsync(host, src, need, cudaMemcpyDeviceToHost, s));
+    }
     GSR_CUDA(cudaStreamSynchronize(s));
     return GSR_OK;
 }

@@ -108,3 +108,38 @@ def test_view_layout_and_limits(gpu):
     assert len(r.view_layouts()) == 1
     img = r.read_back_image()
     assert img.shape == (cams[1].height, cams[1].width, 4)
+
+
+@pytest.mark.parametrize("schedule,target", [("per-tile", "rgba32f"), ("per-tile", "rgba16f"), ("persistent", "rgba32f")])
+@pytest.mark.parametrize("rgb8", [True, False])
+def test_views_to_host_equal_the_device_images(gpu, schedule, target, rgb8):
+    """gsr_render_views_to_host: with the per-tile schedule the views are rasterized one launch
+    each and each view's image is copied while the next is rasterized; the host buffer must hold
+    every view's image as the device has it (RGB8 when the renderer keeps it, else the target),
+    over consecutive frames of changing cameras."""
+    from gsr_b200 import scenes
+
+    gs = gpu.GpuScene(_scene(gpu), "f32", "soa")
+    r = gpu.Renderer(gs, gpu.Settings(budget_mb=1024, adaptive_list=False, rgb8=rgb8, raster_schedule=schedule,
+                                      target=target))
+    for frame in range(3):
+        cams = scenes.batched_cameras(4, seed=20 + frame)
+        cams[1] = scenes.viewer_camera((0.5, 1.0, 9.0 + frame), (0.0, 0.0, 0.0), 200, 120)
+        pixels = sum(c.width * c.height for c in cams)
+        if rgb8:
+            out = np.zeros(pixels * 3, np.uint8)
+        else:
+            out = np.zeros(pixels * 4, np.float32 if target == "rgba32f" else np.float16)
+        r.render_views_to_host(cams, out)
+        base = 0
+        for v, c in enumerate(cams):
+            n = c.width * c.height
+            if rgb8:
+                want = r.read_view_image(v, rgb8=True)[1].reshape(-1)
+                got = out[base * 3:(base + n) * 3]
+            else:
+                want = r.read_view_image(v).reshape(-1)
+                got = out[base * 4:(base + n) * 4].astype(np.float32)
+            np.testing.assert_array_equal(got, want, err_msg=f"frame {frame} view {v}")
+            base += n
+        assert r.read_control().status == 0
