@@ -265,7 +265,7 @@ def run_b200(args, dist: Dist):
     gs = G.GpuScene(scene, fmt, layout)
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, list_mode=args.list_mode,
                                   render_splat=args.render_splat, sort_window=args.sort_window,
-                                  tile_size=args.tile_size))
+                                  tile_size=args.tile_size, use_graph=args.use_graph))
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     first = (dist.rank * 37) % len(cams)
@@ -372,6 +372,7 @@ def run_b200(args, dist: Dist):
                    "scene_format": f"{fmt}/{layout}", "bounds": "tight", "list": "adaptive", "sort": SORT_FORMS[args.list_mode],
                    "form": form, "step": "one view", "views": "300-frame orbit r=14 h=2",
                    "l2": "inputs larger than L2 (scene 298 MB fp32), no flush",
+                   "cuda_graph": bool(args.use_graph),
                    "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "1 GPU"},
         "forms": {"plain": plain, "batched": {k: v for k, v in batched.items() if k != "clocks"},
                   "batched+mlp": ({k: v for k, v in learned.items() if k != "clocks"} if learned else None)},
@@ -410,7 +411,7 @@ def tune(args, G, gs, cams, first: int, model=None):
     probe = G.camera_array([cams[(first + k) % len(cams)] for k in range(32)])
     settings = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
                           list_mode=args.list_mode, render_splat=args.render_splat, sort_window=args.sort_window,
-                          tile_size=args.tile_size)
+                          tile_size=args.tile_size, use_graph=args.use_graph)
     return G.autotune(gs, settings, probe, depths=(1, 2, 4, 8, 16), frames=4, model=model)
 
 
@@ -429,7 +430,7 @@ def run_batched(args, dist: Dist, G, gs, cams, first: int, stream, plain_rendere
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
                                   raster_schedule=tuned["raster_schedule"], list_mode=args.list_mode,
                                   render_splat=args.render_splat, sort_window=args.sort_window,
-                                  tile_size=args.tile_size))
+                                  tile_size=args.tile_size, use_graph=args.use_graph))
     if model is not None:
         r.set_color_model(model)
     # warm-up: at least the requested views, then until the adaptive list keeps its capacity for
@@ -512,6 +513,8 @@ def main():
     ap.add_argument("--no-mlp", action="store_true", help="skip the batched + learned colour form")
     ap.add_argument("--plain-only", action="store_true", help="the plain form only (profiling runs)")
     ap.add_argument("--mlp-steps", type=int, default=2000)
+    ap.add_argument("--use-graph", type=int, default=1, choices=[0, 1],
+                    help="1 (default): each frame launched as one captured CUDA graph (GsrSettings.use_graph)")
     ap.add_argument("--list-mode", default="binning", choices=["binning", "global"],
                     help="list construction: one (tile, depth) sort, or depth sort + emission + tile sort")
     ap.add_argument("--render-splat", default="full", choices=["full", "p32", "p24"],
