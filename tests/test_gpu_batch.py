@@ -110,18 +110,19 @@ def test_view_layout_and_limits(gpu):
     assert img.shape == (cams[1].height, cams[1].width, 4)
 
 
-@pytest.mark.parametrize("schedule,target", [("per-tile", "rgba32f"), ("per-tile", "rgba16f"), ("persistent", "rgba32f")])
+@pytest.mark.parametrize("schedule,target,tile", [("per-tile", "rgba32f", 16), ("per-tile", "rgba16f", 16),
+                                                  ("persistent", "rgba32f", 16), ("per-tile", "rgba32f", 8)])
 @pytest.mark.parametrize("rgb8", [True, False])
-def test_views_to_host_equal_the_device_images(gpu, schedule, target, rgb8):
+def test_views_to_host_equal_the_device_images(gpu, schedule, target, tile, rgb8):
     """gsr_render_views_to_host: with the per-tile schedule the views are rasterized one launch
     each and each view's image is copied while the next is rasterized; the host buffer must hold
     every view's image as the device has it (RGB8 when the renderer keeps it, else the target),
-    over consecutive frames of changing cameras."""
+    over consecutive frames of changing cameras, with 16- and 8-px tiles."""
     from gsr_b200 import scenes
 
     gs = gpu.GpuScene(_scene(gpu), "f32", "soa")
     r = gpu.Renderer(gs, gpu.Settings(budget_mb=1024, adaptive_list=False, rgb8=rgb8, raster_schedule=schedule,
-                                      target=target))
+                                      target=target, tile_size=tile))
     for frame in range(3):
         cams = scenes.batched_cameras(4, seed=20 + frame)
         cams[1] = scenes.viewer_camera((0.5, 1.0, 9.0 + frame), (0.0, 0.0, 0.0), 200, 120)
