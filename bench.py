@@ -163,8 +163,9 @@ def front_bytes(scene_format: str, ctl, n: int, list_mode: str = "global") -> fl
     frame's counts. Preprocess: posAlpha of every gaussian, scale + rotation of those past the
     near/opacity culls, SH of the visible ones; writes the tile counts, the 48-byte records and
     16-byte coverage hints of the visible ones. Scan: counts in, offsets out. Emission: counts of
-    every gaussian, offset + record + hint of the visible ones, and the entries (8 B packed, 12 B
-    as key/value pairs).
+    every gaussian, offset + hint of the visible ones (the span hint holds a splat's tile runs;
+    the few splats beyond its 7 rows also need their record: not counted) plus their depth in
+    global mode, and the entries (8 B packed, 12 B as key/value pairs).
     Binning mode adds the 8-byte depth word of every gaussian (written by the preprocess), its
     depth sort (histogram read + a read and a write of every word per pass), and walks the sorted
     words in the scan and the emission (8 B each, with the counts and offsets gathered)."""
@@ -179,19 +180,19 @@ def front_bytes(scene_format: str, ctl, n: int, list_mode: str = "global") -> fl
         b += 8 * n  # depth words
         b += 8 * n + 16 * n * depth_sort_passes(ctl)  # depth sort
         b += 8 * n + 4 * n + 4 * n  # gathered scan: sorted words, counts, offsets
-        b += 8 * n + 4 * n + 4 * n + 64 * vis + 8 * ctl.entries  # emission in depth order
+        b += 8 * n + 4 * n + 4 * n + 16 * vis + 8 * ctl.entries  # emission in depth order
         return float(b)
     b += 8 * n  # scan
-    b += 4 * n + 68 * vis + (8 if ctl.packed_entries else 12) * ctl.entries  # emission
+    b += 4 * n + 20 * vis + (8 if ctl.packed_entries else 12) * ctl.entries  # emission
     return float(b)
 
 
 # DRAM bytes of the front per frame of the default workload, from one ncu capture
 # (profiles/kernels_plain_1080p.md: preprocess + scan + duplicate, read + write).
 FRONT_TRAFFIC_PLAIN_1080P = {
-    "global": (296.7 + 61.3 + 5.0 + 89.3 + 8.4) * 1e6,
+    "global": None,  # not captured since the span hints changed the emission
     # preprocess, depth histogram, 4 depth passes, gathered scan, emission in depth order
-    "binning": (299.3 + 72.5 + 10.0 + 39.7 + 14.9 + 150.8 + 28.6) * 1e6,
+    "binning": (320.7 + 77.5 + 10.0 + 39.6 + 14.9 + 47.9 + 2.7) * 1e6,
 }
 
 
