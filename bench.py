@@ -54,6 +54,21 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+# warp instructions of one plain 1080p render pass (ncu smsp__inst_issued, profiles/kernels_plain_1080p.md)
+RENDER_WARP_INSTRUCTIONS_1080P = 228.0e6
+
+
+def render_issue(passes: dict, clocks: dict, config: str):
+    ms = passes.get("render tiles")
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
+    if config != "plain_1080p" or not ms or not mhz:
+        return None
+    achieved = RENDER_WARP_INSTRUCTIONS_1080P / (ms * 1e-3) / 1e12
+    peak = 148 * 4 * mhz * 1e6 / 1e12
+    return {"bound": "issue", "achieved": round(achieved, 4), "peak": round(peak, 4), "unit": "T warp-instr/s",
+            "frac": round(achieved / peak, 4), "instructions_source": "ncu issued instructions, one frame"}
+
+
 # ---- configurations ---------------------------------------------------------------------
 def make_config(name: str):
     from gsr_b200 import scenes
@@ -390,6 +405,10 @@ def run_b200(args, dist: Dist):
                      "traffic_source": "ncu dram__bytes_read+write, one frame (profiles/kernels_plain_1080p.md)",
                      "peak_kind": peak_kind, "algorithmic_bytes": int(fb)},
         "passes_ms": {k: round(v, 4) for k, v in passes.items()},
+        # the rasterizer (41 % of the frame) is bound by instruction issue, not by HBM or the
+        # tensor cores: its warp instructions per 1080p frame (ncu, profiles/) over its live
+        # pass time, against 148 SMs x 4 schedulers x the SM clock seen under load
+        "render_issue": render_issue(passes, clocks.summary(), args.config),
         "sort": {"bytes": int(sb), "ms": round(sort_ms, 4), "GB/s": round(sb / (sort_ms * 1e-3) / 1e9, 1),
                  "passes": ctl.sort_passes, "key_bits": ctl.key_bits},
         "frame": {"visible": ctl.visible, "entries": ctl.entries, "duplicates": ctl.duplicates,
