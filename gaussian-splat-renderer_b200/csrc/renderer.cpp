@@ -434,6 +434,7 @@ struct GsrRenderer {
         cudaGraphExec_t graph = nullptr;
         const void* graphList = nullptr;   // the list / layout the graph was captured with
         uint64_t graphLayout = ~0ull;
+        bool graphSplit = false;           // ... and whether it rasterizes view by view
         std::vector<cudaEvent_t> viewDone;  // view-by-view frames: each view's image is complete
         ~Slot() {
             if (graph) cudaGraphExecDestroy(graph);
@@ -707,7 +708,7 @@ struct GsrRenderer {
         // the slot's previous frame has completed: its pinned cameras may be overwritten
         static_assert(sizeof(DevCameraArgs) == sizeof(GsrSplatCamera), "camera layout");
         std::memcpy(slot.camHost, cams, sizeof(GsrSplatCamera) * v);
-        // view by view: several per-tile views with their images wanted on the host (not graphed)
+        // view by view: several per-tile views with their images wanted on the host
         const bool split = hostCopies && v > 1 && !persistentRaster(v);
         while (split && slot.viewDone.size() < v) {
             cudaEvent_t e = nullptr;
@@ -717,9 +718,10 @@ struct GsrRenderer {
         splitViews = split;
         lastSplit = split;
         lastSlot = &slot;
-        const bool graphed = settings.use_graph && !timing && forceTimeout == 0 && !split;
+        const bool graphed = settings.use_graph && !timing && forceTimeout == 0;
         if (graphed) {
-            if (!slot.graph || slot.graphList != list.get() || slot.graphLayout != layoutVersion) {
+            if (!slot.graph || slot.graphList != list.get() || slot.graphLayout != layoutVersion ||
+                slot.graphSplit != split) {
                 if (slot.graph) cudaGraphExecDestroy(slot.graph);
                 slot.graph = nullptr;
                 if (!captureStream) GSR_CUDA(cudaStreamCreateWithFlags(&captureStream, cudaStreamNonBlocking));
@@ -737,6 +739,7 @@ struct GsrRenderer {
                 if (ie != cudaSuccess) return cudaFail(ie, "cudaGraphInstantiate");
                 slot.graphList = list.get();
                 slot.graphLayout = layoutVersion;
+                slot.graphSplit = split;
             }
             GSR_CUDA(cudaGraphLaunch(slot.graph, stream));
         } else {
@@ -873,11 +876,16 @@ struct GsrRenderer {
         GSR_CUDA(launchRanges(ra, l.capacity, stream));
         mark(stream);
         if (splitViews) {
+            // inside a capture the view events become external event nodes (recorded by each
+            // launch of the graph); outside one they are plain records
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            GSR_CUDA(cudaStreamIsCapturing(stream, &cs));
+            const unsigned recordFlags = cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
             for (uint32_t j = 0; j < viewCount; ++j) {
                 ra.tileOffset = views[j].tile_base;
                 ra.tileLaunch = views[j].tiles_x * views[j].tiles_y;
                 GSR_CUDA(launchRender(ra, stream));
-                GSR_CUDA(cudaEventRecord(slot.viewDone[j], stream));
+                GSR_CUDA(cudaEventRecordWithFlags(slot.viewDone[j], stream, recordFlags));
             }
         } else {
             GSR_CUDA(launchRender(ra, stream));

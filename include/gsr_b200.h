@@ -375,9 +375,10 @@ int gsr_read_view_image(GsrRenderer* r, uint32_t view, float* rgba, uint8_t* rgb
 /* The end-to-end call for batched host callers: render the views and copy every view's RGB8
  * (or, when rgb8 output is off, the output format's) image into `host`, view after view at
  * pixel_base (`bytes` must match), then synchronize `stream`. With the per-tile raster schedule
- * and more than one view the frame rasterizes the views one launch each, not as a CUDA graph,
- * and copies each view's image on a renderer-owned stream as soon as that view is done, so the
- * copies overlap the rasterization of the following views; the images are the same. */
+ * and more than one view the frame rasterizes the views one launch each (in its own CUDA graph
+ * when use_graph is on) and copies each view's image on a renderer-owned stream as soon as that
+ * view is done, so the copies overlap the rasterization of the following views; the images are
+ * the same. */
 int gsr_render_views_to_host(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* host, uint64_t bytes,
                              void* stream);
 

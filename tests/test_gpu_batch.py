@@ -112,19 +112,21 @@ def test_view_layout_and_limits(gpu):
 
 @pytest.mark.parametrize("schedule,target,tile", [("per-tile", "rgba32f", 16), ("per-tile", "rgba16f", 16),
                                                   ("persistent", "rgba32f", 16), ("per-tile", "rgba32f", 8)])
-@pytest.mark.parametrize("rgb8", [True, False])
-def test_views_to_host_equal_the_device_images(gpu, schedule, target, tile, rgb8):
+@pytest.mark.parametrize("rgb8,graph", [(True, False), (False, False), (True, True)])
+def test_views_to_host_equal_the_device_images(gpu, schedule, target, tile, rgb8, graph):
     """gsr_render_views_to_host: with the per-tile schedule the views are rasterized one launch
     each and each view's image is copied while the next is rasterized; the host buffer must hold
     every view's image as the device has it (RGB8 when the renderer keeps it, else the target),
-    over consecutive frames of changing cameras, with 16- and 8-px tiles."""
+    over consecutive frames of changing cameras, with 16- and 8-px tiles, also when the frame is a
+    CUDA graph (its view events are external event nodes)."""
     from gsr_b200 import scenes
 
     gs = gpu.GpuScene(_scene(gpu), "f32", "soa")
     r = gpu.Renderer(gs, gpu.Settings(budget_mb=1024, adaptive_list=False, rgb8=rgb8, raster_schedule=schedule,
-                                      target=target, tile_size=tile))
-    for frame in range(3):
-        cams = scenes.batched_cameras(4, seed=20 + frame)
+                                      target=target, tile_size=tile, use_graph=graph))
+    fixed = scenes.batched_cameras(4, seed=20)
+    for frame in range(4):  # the same sizes (a graph is reused), one camera moving
+        cams = list(fixed)
         cams[1] = scenes.viewer_camera((0.5, 1.0, 9.0 + frame), (0.0, 0.0, 0.0), 200, 120)
         pixels = sum(c.width * c.height for c in cams)
         if rgb8:
