@@ -285,7 +285,6 @@ def run_b200(args, dist: Dist):
     stream = torch.cuda.Stream(device=dev)
     sptr = stream.cuda_stream
     first = (dist.rank * 37) % len(cams)
-    view = lambda k: cams[(first + k) % len(cams)]  # noqa: E731
     c_cams = [G.to_c_camera(c) for c in cams]  # the GsrCamera structs a host application passes
     scam = lambda k: c_cams[(first + k) % len(cams)]  # noqa: E731
 
@@ -318,14 +317,14 @@ def run_b200(args, dist: Dist):
         torch.empty((cams[0].height, cams[0].width, 3), dtype=torch.uint8).pin_memory()
     out = img.numpy()
     for k in range(min(args.warmup, 5)):
-        r.render_to_host(view(k), out, sptr)
+        r.render_to_host(scam(k), out, sptr)
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     e0.record(stream)
     for k in range(args.steps):
-        r.render_to_host(view(args.warmup + k), out, sptr)
+        r.render_to_host(scam(args.warmup + k), out, sptr)
     e1.record(stream)
     e1.synchronize()
     wall = time.perf_counter() - t0

@@ -462,9 +462,21 @@ struct GsrRenderer {
     cudaStream_t captureStream = nullptr;  // graphs are captured here (never the legacy stream)
     // gsr_render_views_to_host: the frame's views are rasterized one launch each, and each view's
     // image goes to the host on copyStream as soon as it is complete (hostCopies asks for it,
-    // lastSplit / lastSlot tell how the last frame ran)
+    // lastSplit / lastSlot tell how the last frame ran; row bands of a single view measured no
+    // faster, so one-view frames stay whole)
     bool hostCopies = false, lastSplit = false, splitViews = false;
     Slot* lastSlot = nullptr;
+    // the parts of such a frame: one per view (its tiles and its pixels)
+    struct RenderPart {
+        uint32_t tileOffset, tiles;
+        uint64_t pixelOffset, pixels;
+    };
+    std::vector<RenderPart> parts;
+    void planParts() {
+        parts.clear();
+        for (const GsrViewLayout& L : views)
+            parts.push_back(RenderPart{L.tile_base, L.tiles_x * L.tiles_y, L.pixel_base, uint64_t(L.width) * L.height});
+    }
     cudaStream_t copyStream = nullptr;
 
     ~GsrRenderer() {
@@ -710,7 +722,8 @@ struct GsrRenderer {
         std::memcpy(slot.camHost, cams, sizeof(GsrSplatCamera) * v);
         // view by view: several per-tile views with their images wanted on the host
         const bool split = hostCopies && v > 1 && !persistentRaster(v);
-        while (split && slot.viewDone.size() < v) {
+        if (split) planParts();
+        while (split && slot.viewDone.size() < parts.size()) {
             cudaEvent_t e = nullptr;
             GSR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             slot.viewDone.push_back(e);
@@ -757,7 +770,7 @@ struct GsrRenderer {
         // frameBegin, preprocess, scan, duplicate, histogram, one per pass, ranges, render
         // binning: frameBegin, preprocess, depth histogram + passes, scan, duplicate, list
         // histogram + passes, ranges, render
-        kernelLaunches += (binning() ? 8 + kDepthSortPasses + list->passes : 7 + list->passes) + (split ? v - 1 : 0);
+        kernelLaunches += (binning() ? 8 + kDepthSortPasses + list->passes : 7 + list->passes) + (split ? uint32_t(parts.size()) - 1 : 0);
         timed = timing;
         ++frameIndex;
         return GSR_OK;
@@ -881,9 +894,9 @@ struct GsrRenderer {
             cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
             GSR_CUDA(cudaStreamIsCapturing(stream, &cs));
             const unsigned recordFlags = cs == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : cudaEventRecordDefault;
-            for (uint32_t j = 0; j < viewCount; ++j) {
-                ra.tileOffset = views[j].tile_base;
-                ra.tileLaunch = views[j].tiles_x * views[j].tiles_y;
+            for (size_t j = 0; j < parts.size(); ++j) {
+                ra.tileOffset = parts[j].tileOffset;
+                ra.tileLaunch = parts[j].tiles;
                 GSR_CUDA(launchRender(ra, stream));
                 GSR_CUDA(cudaEventRecordWithFlags(slot.viewDone[j], stream, recordFlags));
             }
@@ -1261,18 +1274,42 @@ int gsr_renderer_image(GsrRenderer* r, const void** rgba, const void** rgb8, uin
     return GSR_OK;
 }
 
+namespace {
+// The frame's images to `host` (RGB8 when kept, else the output format): part by part on the
+// renderer's copy stream after each part's rasterizer launch when the frame ran in parts, else
+// one copy on `s`; then both streams are synchronized.
+int copyFrameToHost(GsrRenderer* r, void* host, uint64_t need, cudaStream_t s) {
+    const bool rgb = r->rgb8.p != nullptr;
+    const size_t bpp = rgb ? 3 : r->imageBytes();
+    const unsigned char* src = rgb ? r->rgb8.as<unsigned char>() : r->image.as<unsigned char>();
+    if (r->lastSplit) {
+        if (!r->copyStream) GSR_CUDA(cudaStreamCreateWithFlags(&r->copyStream, cudaStreamNonBlocking));
+        for (size_t j = 0; j < r->parts.size(); ++j) {
+            const size_t off = size_t(r->parts[j].pixelOffset) * bpp, len = size_t(r->parts[j].pixels) * bpp;
+            GSR_CUDA(cudaStreamWaitEvent(r->copyStream, r->lastSlot->viewDone[j], 0));
+            GSR_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(host) + off, src + off, len, cudaMemcpyDeviceToHost,
+                                     r->copyStream));
+        }
+        GSR_CUDA(cudaStreamSynchronize(r->copyStream));
+    } else {
+        GSR_CUDA(cudaMemcpyAsync(host, src, need, cudaMemcpyDeviceToHost, s));
+    }
+    GSR_CUDA(cudaStreamSynchronize(s));
+    return GSR_OK;
+}
+}  // namespace
+
 int gsr_render_to_host(GsrRenderer* r, const GsrCamera* camera, void* host, uint64_t bytes, void* stream) {
     if (!r || !camera || !host) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    r->hostCopies = true;
     int rc = gsr_render(r, camera, stream);
+    r->hostCopies = false;
     if (rc) return rc;
     const bool rgb = r->rgb8.p != nullptr;
     const uint64_t need = uint64_t(r->width) * r->height * (rgb ? 3 : r->imageBytes());
     if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, image needs %llu",
                                    (unsigned long long)bytes, (unsigned long long)need);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    GSR_CUDA(cudaMemcpyAsync(host, rgb ? r->rgb8.p : r->image.p, need, cudaMemcpyDeviceToHost, s));
-    GSR_CUDA(cudaStreamSynchronize(s));
-    return GSR_OK;
+    return copyFrameToHost(r, host, need, static_cast<cudaStream_t>(stream));
 }
 
 int gsr_renderer_last_stats(GsrRenderer* r, GsrControl* out, uint64_t* frameIndex) {
@@ -1398,24 +1435,7 @@ int gsr_render_views_to_host(GsrRenderer* r, const GsrSplatCamera* cameras, uint
     const uint64_t need = r->totalPixels * (rgb ? 3 : r->imageBytes());
     if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, the views need %llu",
                                    (unsigned long long)bytes, (unsigned long long)need);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    const size_t bpp = rgb ? 3 : r->imageBytes();
-    const unsigned char* src = rgb ? r->rgb8.as<unsigned char>() : r->image.as<unsigned char>();
-    if (r->lastSplit) {  // each view's image as soon as its rasterizer launch is done
-        if (!r->copyStream) GSR_CUDA(cudaStreamCreateWithFlags(&r->copyStream, cudaStreamNonBlocking));
-        for (size_t j = 0; j < r->views.size(); ++j) {
-            const GsrViewLayout& L = r->views[j];
-            const size_t off = size_t(L.pixel_base) * bpp, len = size_t(L.width) * L.height * bpp;
-            GSR_CUDA(cudaStreamWaitEvent(r->copyStream, r->lastSlot->viewDone[j], 0));
-            GSR_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(host) + off, src + off, len, cudaMemcpyDeviceToHost,
-                                     r->copyStream));
-        }
-        GSR_CUDA(cudaStreamSynchronize(r->copyStream));
-    } else {
-        GSR_CUDA(cudaMemcpyAsync(host, src, need, cudaMemcpyDeviceToHost, s));
-    }
-    GSR_CUDA(cudaStreamSynchronize(s));
-    return GSR_OK;
+    return copyFrameToHost(r, host, need, static_cast<cudaStream_t>(stream));
 }
 
 int gsr_renderer_view_layout(GsrRenderer* r, uint32_t view, GsrViewLayout* out, uint32_t* views) {

@@ -430,8 +430,10 @@ class Renderer:
             self.width, self.height = camera.width, camera.height
 
     def render_to_host(self, camera, out: np.ndarray, stream: int = 0):
-        check(load().gsr_render_to_host(self._h, C.byref(to_c_camera(camera)), out.ctypes.data, out.nbytes,
-                                        C.c_void_p(stream)))
+        """camera: scenes.ViewerCamera or a GsrCamera struct (to_c_camera, built once per camera)."""
+        cam = camera if isinstance(camera, CCamera) else to_c_camera(camera)
+        check(load().gsr_render_to_host(self._h, C.byref(cam), out.ctypes.data, out.nbytes, C.c_void_p(stream)))
+        self.width, self.height = camera.width, camera.height
 
     def image_pointers(self):
         rgba, rgb = C.c_void_p(), C.c_void_p()
@@ -530,6 +532,10 @@ class Renderer:
         return sp, counts
 
     def read_back_image(self, rgb8: bool = False):
+        # the first view's size as the renderer has it (whichever call rendered the frame)
+        w, h = C.c_uint32(), C.c_uint32()
+        check(load().gsr_renderer_image(self._h, None, None, C.byref(w), C.byref(h)))
+        self.width, self.height = w.value, h.value
         rgba = np.zeros((self.height, self.width, 4), np.float32)
         out8 = np.zeros((self.height, self.width, 3), np.uint8) if rgb8 else None
         check(load().gsr_read_image(self._h, rgba.ctypes.data, out8.ctypes.data if rgb8 else None))

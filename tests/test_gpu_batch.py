@@ -146,3 +146,23 @@ def test_views_to_host_equal_the_device_images(gpu, schedule, target, tile, rgb8
             np.testing.assert_array_equal(got, want, err_msg=f"frame {frame} view {v}")
             base += n
         assert r.read_control().status == 0
+
+
+@pytest.mark.parametrize("graph", [False, True])
+@pytest.mark.parametrize("rgb8,target", [(True, "rgba32f"), (False, "rgba16f")])
+def test_single_view_to_host(gpu, graph, rgb8, target):
+    """gsr_render_to_host: the host image equals the device image, frame after frame (graph
+    reused)."""
+    from gsr_b200 import scenes
+
+    gs = gpu.GpuScene(_scene(gpu), "f32", "soa")
+    r = gpu.Renderer(gs, gpu.Settings(budget_mb=1024, adaptive_list=False, rgb8=rgb8, target=target, use_graph=graph))
+    for frame in range(4):
+        cam = scenes.viewer_camera((0.5, 1.0 + 0.3 * frame, 9.0), (0.0, 0.0, 0.0), 1000, 570)
+        px = cam.width * cam.height
+        out = np.zeros(px * 3, np.uint8) if rgb8 else np.zeros(px * 4, np.float16)
+        r.render_to_host(cam, out)
+        if rgb8:
+            np.testing.assert_array_equal(out, r.read_back_image(rgb8=True)[1].reshape(-1), err_msg=f"frame {frame}")
+        else:
+            np.testing.assert_array_equal(out.astype(np.float32), r.read_back_image().reshape(-1), err_msg=f"frame {frame}")
