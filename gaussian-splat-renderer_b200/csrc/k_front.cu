@@ -225,22 +225,17 @@ __device__ __forceinline__ void issueShStage(const SceneArgs& s, uint32_t i0, ui
 // The plain colour: the gaussian's SH coefficients, evaluated in the view direction.
 template <int COLOR>
 __device__ __forceinline__ void shColour(const FrontArgs& a, uint32_t i, const ColourJob& job, DevSplat& s) {
-    float sh[48];
-    const uint32_t used = (job.degree + 1) * (job.degree + 1);
-    if (COLOR == GSR_COLOR_SOA_F32 && a.shStaged && waitShStage(a.ctl, true)) {
-        const float4* p = gShStage + threadIdx.x * 12;
-#pragma unroll
-        for (int v = 0; v < 12; ++v) {
-            if (uint32_t(v) * 4 < used * 3) {
-                const float4 f = p[v];
-                sh[v * 4 + 0] = f.x; sh[v * 4 + 1] = f.y; sh[v * 4 + 2] = f.z; sh[v * 4 + 3] = f.w;
-            }
-        }
-    } else {
-        loadSH<COLOR>(a.scene, i, used, job.meta, sh);
-    }
     float color[3];
-    evalSH(int(job.degree), sh, job.dir[0], job.dir[1], job.dir[2], color);
+    if (COLOR == GSR_COLOR_SOA_F32 && a.shStaged && waitShStage(a.ctl, true)) {
+        // straight from the staged copy: the coefficients are read as the bands need them, with
+        // no 48-register array (evalSH reads the first (degree + 1)^2 triplets)
+        evalSH(int(job.degree), reinterpret_cast<const float*>(gShStage + threadIdx.x * 12), job.dir[0], job.dir[1],
+               job.dir[2], color);
+    } else {
+        float sh[48];
+        loadSH<COLOR>(a.scene, i, (job.degree + 1) * (job.degree + 1), job.meta, sh);
+        evalSH(int(job.degree), sh, job.dir[0], job.dir[1], job.dir[2], color);
+    }
     s.r = color[0];
     s.g = color[1];
     s.b = color[2];
