@@ -207,7 +207,7 @@ def front_bytes(scene_format: str, ctl, n: int, list_mode: str = "global") -> fl
 FRONT_TRAFFIC_PLAIN_1080P = {
     "global": None,  # not captured since the span hints changed the emission
     # preprocess, depth histogram, 4 depth passes, gathered scan, emission in depth order
-    "binning": (320.7 + 77.5 + 10.0 + 39.6 + 14.9 + 47.9 + 2.7) * 1e6,
+    "binning": (314.4 + 70.7 + 10.0 + 39.6 + 14.9 + 47.9 + 2.9) * 1e6,
 }
 
 
