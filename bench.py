@@ -130,7 +130,7 @@ class ClockSampler:
                "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
                "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-               "--format=csv,noheader,nounits", "-lms", "100"]
+               "--format=csv,noheader,nounits", "-lms", "50"]
         try:
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
