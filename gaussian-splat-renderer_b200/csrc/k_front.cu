@@ -730,7 +730,8 @@ namespace {
 constexpr int kShStageBytes = kFrontThreads * 192;
 template <int GEOM, int COLOR, bool LEARNED, bool EXTRAS>
 void launchPreprocessT(const FrontArgs& a, dim3 blocks, cudaStream_t s) {
-    static bool configured = false;
+    static bool configuredOn[64] = {};
+    bool& configured = perDevice(configuredOn);
     if (COLOR == GSR_COLOR_SOA_F32 && !configured) {  // (a failure here fails the staged launch below)
         configured = cudaFuncSetAttribute(preprocessKernel<GEOM, COLOR, LEARNED, EXTRAS>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, kShStageBytes) == cudaSuccess;

@@ -512,7 +512,9 @@ uint32_t gridFor(uint32_t n, uint32_t perBlock, uint32_t cap) {
 }  // namespace
 
 cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s) {
-    static int passGrid = 0, depthGrid = 0;
+    static int passGrids[64] = {}, depthGrids[64] = {};
+    int& passGrid = perDevice(passGrids);
+    int& depthGrid = perDevice(depthGrids);
     constexpr int kListSmem = PassShape<false>::kSmemBytes, kDepthSmem = PassShape<false, kDepthSortItems>::kSmemBytes;
     if (!passGrid) {
         cudaError_t e = cudaFuncSetAttribute(sortPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kListSmem);

@@ -10,6 +10,15 @@
 
 namespace gsr {
 
+// One-time launch set-up (function attributes, grid sizes) is per device: the slot of the
+// current device in a launcher's table.
+template <class T>
+inline T& perDevice(T (&table)[64]) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return table[dev & 63];
+}
+
 struct DevCameraArgs {  // = DevCamera (splat_math.cuh)
     float v[16];
     float pos[3];
