@@ -33,10 +33,15 @@ struct DeviceControl {
     uint32_t pad[5];
 };
 
+// Items of one block of the exclusive scan (scanKernel: 256 threads x kScanItems); the scan's
+// grid, its look-back words and the static scratch below are all sized by it.
+constexpr uint32_t kScanBlockItems = 2048;
+
 // Layout of the static scratch of gsr_scan_static: the control block, then one look-back word
-// per 2048-item scan block of the largest accepted count.
+// per scan block of the largest accepted count.
 constexpr size_t kStaticScanCtlBytes = 512;
-constexpr size_t kStaticScanScratchBytes = kStaticScanCtlBytes + size_t(GSR_SCAN_STATIC_MAX_COUNT / 2048) * 8;
+constexpr size_t kStaticScanScratchBytes =
+    kStaticScanCtlBytes + size_t((GSR_SCAN_STATIC_MAX_COUNT + kScanBlockItems - 1) / kScanBlockItems) * 8;
 static_assert(sizeof(DeviceControl) <= kStaticScanCtlBytes, "the control block fits its slot");
 static_assert(kStaticScanScratchBytes == 66048, "the size the header states");
 

@@ -473,7 +473,9 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
         atomicMax(&sDepthMax, dmax);
     }
     __syncthreads();
-    // the bulk copy must have landed before the block's shared memory is released
+    // the bulk copy must have landed before the block's shared memory is released; if this
+    // bounded wait expires the copy may still be writing after the block ends, so the frame is
+    // marked GSR_CONTROL_TIMEOUT (its records untrusted; the host reports a failed frame)
     if (staged && tid == 0 && !shStageReady()) waitShStage(a.ctl, false);
     if (tid < kCullReasonCount && sCull[tid]) atomicAdd(&a.ctl->c.cull_counts[tid], sCull[tid]);
     if (tid == 0 && sDepthMin <= sDepthMax) {
@@ -715,6 +717,11 @@ __global__ void logfTableKernel(float* out, LogfFixups t) {
 
 }  // namespace
 
+cudaError_t loadFrameBeginKernel() {
+    cudaFuncAttributes attr;
+    return cudaFuncGetAttributes(&attr, frameBeginKernel);
+}
+
 cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint32_t* ranges,
                              uint32_t rangeWords, SortPlan* plan, uint32_t forceTimeout, cudaStream_t s,
                              SortPlan* plan2) {
@@ -730,8 +737,8 @@ namespace {
 constexpr int kShStageBytes = kFrontThreads * 192;
 template <int GEOM, int COLOR, bool LEARNED, bool EXTRAS>
 void launchPreprocessT(const FrontArgs& a, dim3 blocks, cudaStream_t s) {
-    static bool configuredOn[64] = {};
-    bool& configured = perDevice(configuredOn);
+    static std::atomic<bool> configuredOn[64] = {};
+    std::atomic<bool>& configured = perDevice(configuredOn);
     if (COLOR == GSR_COLOR_SOA_F32 && !configured) {  // (a failure here fails the staged launch below)
         configured = cudaFuncSetAttribute(preprocessKernel<GEOM, COLOR, LEARNED, EXTRAS>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, kShStageBytes) == cudaSuccess;

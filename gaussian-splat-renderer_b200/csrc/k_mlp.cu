@@ -342,8 +342,8 @@ __global__ void __launch_bounds__(kGateWarps * 32) gateKernel(const __grid_const
 cudaError_t launchColorTrainStep(const float* sh, const uint8_t* degrees, uint32_t count, uint32_t dirs, uint32_t seed,
                                  uint32_t batch, float* params, float* m, float* v, float* partials, uint32_t* step,
                                  float lr, float* lossOut, uint32_t maxSteps, cudaStream_t s) {
-    static bool configuredOn[64] = {};
-    bool& configured = perDevice(configuredOn);
+    static std::atomic<bool> configuredOn[64] = {};
+    std::atomic<bool>& configured = perDevice(configuredOn);
     const int smem = kTrainSmemFloats * 4;
     if (!configured) {
         const cudaError_t e = cudaFuncSetAttribute(trainStepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

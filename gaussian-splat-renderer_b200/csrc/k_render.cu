@@ -468,8 +468,8 @@ template <int MODE, int CAP, int TILE>
 cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
     constexpr size_t smem = renderSmemBytes<CAP, TILE * TILE>();
     constexpr uint32_t threads = TILE * TILE;
-    static bool configuredOn[64] = {};
-    bool& configured = perDevice(configuredOn);
+    static std::atomic<bool> configuredOn[64] = {};
+    std::atomic<bool>& configured = perDevice(configuredOn);
     if (!configured) {
         cudaError_t e =
             cudaFuncSetAttribute(renderKernel<MODE, CAP, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));

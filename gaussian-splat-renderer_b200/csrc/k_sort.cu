@@ -427,7 +427,8 @@ __global__ void __launch_bounds__(256) rangesKernel(const __grid_constant__ Rend
 }
 
 // ---- standalone exclusive scan (GpuScan plain / kNonZero / kGather) ---------------------------
-constexpr int kScanItems = 8;
+constexpr int kScanItems = int(kScanBlockItems / 256);
+static_assert(256 * kScanItems == int(kScanBlockItems), "one scan block = 256 threads x kScanItems");
 __global__ void __launch_bounds__(256) scanKernel(const uint32_t* __restrict__ in, const uint32_t* __restrict__ index,
                                                   uint32_t* __restrict__ out, uint32_t* total, uint32_t count,
                                                   uint32_t mode, uint64_t* status, DeviceControl* ctl,
@@ -512,9 +513,9 @@ uint32_t gridFor(uint32_t n, uint32_t perBlock, uint32_t cap) {
 }  // namespace
 
 cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s) {
-    static int passGrids[64] = {}, depthGrids[64] = {};
-    int& passGrid = perDevice(passGrids);
-    int& depthGrid = perDevice(depthGrids);
+    static std::atomic<int> passGrids[64] = {}, depthGrids[64] = {};
+    std::atomic<int>& passGrid = perDevice(passGrids);
+    std::atomic<int>& depthGrid = perDevice(depthGrids);
     constexpr int kListSmem = PassShape<false>::kSmemBytes, kDepthSmem = PassShape<false, kDepthSortItems>::kSmemBytes;
     if (!passGrid) {
         cudaError_t e = cudaFuncSetAttribute(sortPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kListSmem);
@@ -548,7 +549,7 @@ cudaError_t launchRanges(const RenderArgs& a, uint32_t capacity, cudaStream_t s)
 cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
                        uint32_t mode, uint64_t* status, DeviceControl* ctl, cudaStream_t s, uint32_t setupCapacity,
                        uint32_t waitSite, const ScanGather* gather) {
-    const uint32_t blocks = (count + 256 * kScanItems - 1) / (256 * kScanItems);
+    const uint32_t blocks = (count + kScanBlockItems - 1) / kScanBlockItems;
     if (blocks == 0) {
         if (total) return cudaMemsetAsync(total, 0, 4, s);
         return cudaSuccess;
@@ -564,6 +565,13 @@ cudaError_t launchScan(const uint32_t* in, const uint32_t* index, uint32_t* out,
 static __device__ __align__(256) unsigned char gStaticScanScratch[kStaticScanScratchBytes];
 
 cudaError_t staticScanScratch(void** base) { return cudaGetSymbolAddress(base, gStaticScanScratch); }
+
+// Loads the scan kernel's code on the current device now (with lazy module loading a kernel is
+// loaded, and may allocate device memory, at its first launch).
+cudaError_t loadScanKernel() {
+    cudaFuncAttributes attr;
+    return cudaFuncGetAttributes(&attr, scanKernel);
+}
 
 cudaError_t launchPack64(const uint32_t* lo, const uint32_t* hi, uint64_t* out, uint32_t n, cudaStream_t s) {
     if (!n) return cudaSuccess;

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 
 #include "gsr_types.h"
@@ -11,9 +12,10 @@
 namespace gsr {
 
 // One-time launch set-up (function attributes, grid sizes) is per device: the slot of the
-// current device in a launcher's table.
+// current device in a launcher's table. The slots are atomics, so host threads that render on
+// the same device at once may both do the set-up (it is idempotent) without a data race.
 template <class T>
-inline T& perDevice(T (&table)[64]) {
+inline std::atomic<T>& perDevice(std::atomic<T> (&table)[64]) {
     int dev = 0;
     cudaGetDevice(&dev);
     return table[dev & 63];
@@ -208,6 +210,9 @@ cudaError_t launchColorGate(const float* sh, const uint8_t* degrees, uint32_t co
 // Device address of the static scratch of gsr_scan_static (kStaticScanScratchBytes) on the
 // current device.
 cudaError_t staticScanScratch(void** base);
+// Load the code of the kernels gsr_scan_static launches on the current device (cudaFuncGetAttributes).
+cudaError_t loadScanKernel();
+cudaError_t loadFrameBeginKernel();
 cudaError_t launchPack64(const uint32_t* lo, const uint32_t* hi, uint64_t* out, uint32_t n, cudaStream_t s);
 cudaError_t launchUnpack64(const uint64_t* in, uint32_t* lo, uint32_t* hi, uint32_t n, cudaStream_t s);
 cudaError_t launchSetEntries(DeviceControl* ctl, uint32_t count, cudaStream_t s);

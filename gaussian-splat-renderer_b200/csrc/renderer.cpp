@@ -128,6 +128,34 @@ int deviceTables(LogfFixups* out) {
     return GSR_OK;
 }
 
+// ---- the static scratch of gsr_scan_static, made ready once per device -----------------------
+// gsr_scan_static is for callers that must not allocate device memory: recovery code running
+// after an allocation failed (the device's memory is held by a resident scene), hooks of a
+// caching allocator that must not re-enter it, and streams that must not stall behind cudaFree
+// (it synchronizes the whole device). Under CUDA's lazy module loading a module's device arrays
+// and a kernel's code are loaded on first use, and loading can allocate. So the array's address
+// is looked up and the two kernels the call launches are loaded here, once per device, by every
+// set-up call of this library on a device (scene and renderer creation, gsr_scan,
+// gsr_sort_pairs) and by gsr_scan_static itself (count 0 does nothing else).
+std::mutex g_staticScanMutex;
+void* g_staticScanBase[64] = {};
+
+int staticScanReady(void** base) {
+    int dev = 0;
+    GSR_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(GSR_ERROR_UNSUPPORTED, "device index %d", dev);
+    std::lock_guard<std::mutex> lock(g_staticScanMutex);
+    if (!g_staticScanBase[dev]) {
+        void* p = nullptr;
+        GSR_CUDA(staticScanScratch(&p));
+        GSR_CUDA(loadScanKernel());
+        GSR_CUDA(loadFrameBeginKernel());
+        g_staticScanBase[dev] = p;
+    }
+    if (base) *base = g_staticScanBase[dev];
+    return GSR_OK;
+}
+
 // ---- camera (splat_math.cpp:9-42), host, same evaluation order as the device and the oracle --
 void mul4(const float* a, const float* b, float* r) {
     for (int c = 0; c < 4; ++c)
@@ -1033,6 +1061,8 @@ int gsr_scene_create(const GsrHostScene* host, const GsrCompression* options, Gs
     if (fmt > GSR_FORMAT_CB || layout > GSR_LAYOUT_AOS) return fail(GSR_ERROR_INVALID_ARGUMENT, "format %u layout %u", fmt, layout);
     if (fmt != GSR_FORMAT_F32 && layout == GSR_LAYOUT_SOA)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "scene layout 'soa' exists only for the f32 format (use split or aos)");
+    const int ready = staticScanReady(nullptr);  // gsr_scan_static's scratch and kernels on this device
+    if (ready) return ready;
     const uint32_t n = host->count;
     const uint32_t srcK = uint32_t((host->sh_degree + 1) * (host->sh_degree + 1));
     const int degree = std::clamp(std::min(host->sh_degree, options->max_sh_degree), 0, 3);
@@ -1220,6 +1250,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     r->settings.frames_in_flight = std::max(settings->frames_in_flight, 1u);
     r->evalDegree = std::min(scene->sh_degree, r->settings.max_sh_degree);
     rc = deviceTables(&r->logf);
+    if (rc) return rc;
+    rc = staticScanReady(nullptr);  // gsr_scan_static's scratch and kernels on this device
     if (rc) return rc;
     if (settings->list_mode > GSR_LIST_GLOBAL) return fail(GSR_ERROR_INVALID_ARGUMENT, "list mode %u", settings->list_mode);
     if (settings->sort_window > 64)
@@ -1775,9 +1807,11 @@ int gsr_scan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t*
              void* stream) {
     if (mode > GSR_SCAN_GATHER || (count && (!in || !out)) || (mode == GSR_SCAN_GATHER && count && !index))
         return fail(GSR_ERROR_INVALID_ARGUMENT, "scan arguments");
+    int rc = staticScanReady(nullptr);
+    if (rc) return rc;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     DevBuf ctl, status;
-    const uint32_t blocks = (count + 2047) / 2048;
+    const uint32_t blocks = (count + kScanBlockItems - 1) / kScanBlockItems;
     GSR_CUDA(ctl.alloc(sizeof(DeviceControl)));
     GSR_CUDA(cudaMemsetAsync(ctl.p, 0, sizeof(DeviceControl), s));
     GSR_CUDA(status.alloc(size_t(std::max(blocks, 1u)) * 8));
@@ -1791,18 +1825,6 @@ int gsr_scan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t*
     return GSR_OK;
 }
 
-// gsr_scan without allocation, for callers that must not allocate device memory: recovery code
-// running after an allocation failed (the device's memory is held by a resident scene), hooks of
-// a caching allocator that must not re-enter it, and streams that must not stall behind cudaFree
-// (it synchronizes the whole device). The scratch is the static array of k_sort.cu; its address
-// is looked up once per device and kept. Overlapping calls on one device share that array and
-// race (the header tells the caller to serialize them).
-namespace {
-constexpr int kMaxStaticScanDevices = 64;
-std::mutex g_staticScanMutex;
-void* g_staticScanBase[kMaxStaticScanDevices] = {};
-}  // namespace
-
 int gsr_scan_static(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
                     uint32_t mode, void* stream) {
     if (mode > GSR_SCAN_GATHER || (count && (!in || !out)) || (mode == GSR_SCAN_GATHER && count && !index))
@@ -1810,21 +1832,18 @@ int gsr_scan_static(const uint32_t* in, const uint32_t* index, uint32_t* out, ui
     if (count > GSR_SCAN_STATIC_MAX_COUNT)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "gsr_scan_static: count %u exceeds the static scratch limit of %u items",
                     count, GSR_SCAN_STATIC_MAX_COUNT);
-    int dev = 0;
-    GSR_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxStaticScanDevices) return fail(GSR_ERROR_INVALID_ARGUMENT, "device ordinal %d", dev);
     void* base = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_staticScanMutex);
-        if (!g_staticScanBase[dev]) GSR_CUDA(staticScanScratch(&g_staticScanBase[dev]));
-        base = g_staticScanBase[dev];
-    }
+    int rc = staticScanReady(&base);
+    if (rc) return rc;
+    if (count == 0) return GSR_OK;  // the set-up call: the scratch and the kernels are ready
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     DeviceControl* ctl = static_cast<DeviceControl*>(base);
     uint64_t* status = reinterpret_cast<uint64_t*>(static_cast<unsigned char*>(base) + kStaticScanCtlBytes);
-    const uint32_t blocks = (count + 2047) / 2048;
+    const uint32_t blocks = (count + kScanBlockItems - 1) / kScanBlockItems;
+    static_assert(kStaticScanCtlBytes + size_t((GSR_SCAN_STATIC_MAX_COUNT + kScanBlockItems - 1) / kScanBlockItems) * 8 <=
+                      kStaticScanScratchBytes, "the look-back words of the largest count fit the array");
     // what must start at zero: the look-back words here, the block tickets in frame begin
-    if (blocks) GSR_CUDA(cudaMemsetAsync(status, 0, size_t(blocks) * 8, s));
+    GSR_CUDA(cudaMemsetAsync(status, 0, size_t(blocks) * 8, s));
     GSR_CUDA(launchFrameBegin(ctl, count, 0, nullptr, 0, nullptr, 0, s));
     GSR_CUDA(launchScan(in, index, out, total, count, mode, status, ctl, s));
     uint32_t st = 0;
@@ -1838,6 +1857,8 @@ int gsr_sort_pairs(uint32_t* keysLo, uint32_t* keysHi, uint32_t* values, uint32_
     if (keyBits == 0 || keyBits > 64 || (!keysHi && keyBits > 32)) return fail(GSR_ERROR_INVALID_ARGUMENT, "key_bits %u", keyBits);
     if (count == 0) return GSR_OK;
     if (!keysLo || !values) return fail(GSR_ERROR_INVALID_ARGUMENT, "null keys/values");
+    const int ready = staticScanReady(nullptr);
+    if (ready) return ready;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const uint32_t passes = (keyBits + 7) / 8;
     const uint32_t maxTiles = (count + kSortTile - 1) / kSortTile;

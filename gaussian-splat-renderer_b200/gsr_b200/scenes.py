@@ -13,7 +13,9 @@ Named workloads (sizes as the benchmark configurations state them):
 * ``plain_1080p``     1,240,000 gaussians, ball radius 8, 1920x1080, 300-frame orbit of
                       radius 14 at height 2
 * ``batched_64``      559,000 gaussians, ball radius 6, 64 cameras of mixed resolution, seed 2
-* ``scale_4k``        6,000,000 gaussians, ball radius 20, 16 views at 3840x2160, seed 3
+* ``scale_4k``        6,000,000 gaussians, ball radius 20, per-gaussian SH degree drawn
+                      uniformly from 0-3 (the bands above it zero), 16 views at 3840x2160 on a
+                      ring of radius 30 at height 3, seed 3
 """
 from __future__ import annotations
 
@@ -57,9 +59,14 @@ class Scene:
         )
 
 
-def make_scene(count: int, seed: int, ball_radius: float, sh_degree: int = 3, name: str = "") -> Scene:
+def make_scene(count: int, seed: int, ball_radius: float, sh_degree: int = 3, name: str = "",
+               random_degrees: bool = False) -> Scene:
     """Means uniform in a ball, log-scales N(-3.5, 0.7), uniform rotations,
-    opacity = sigmoid(N(0, 1)), SH DC ~ N(0, 0.5), higher bands ~ N(0, 0.1)."""
+    opacity = sigmoid(N(0, 1)), SH DC ~ N(0, 0.5), higher bands ~ N(0, 0.1).
+    random_degrees: each gaussian's SH degree is drawn uniformly from 0..sh_degree (from a
+    stream of its own, so every other value is the same as without it) and its bands above that
+    degree are zero; an encoder with a per-gaussian degree threshold of 0 then stores exactly
+    that degree (meta["degrees"] holds it)."""
     rng = np.random.default_rng(seed)
     n = int(count)
     d = rng.standard_normal((n, 3))
@@ -86,7 +93,13 @@ def make_scene(count: int, seed: int, ball_radius: float, sh_degree: int = 3, na
     pos_alpha[:, 3] = alpha
     scales = np.zeros((n, 4), np.float32)
     scales[:, :3] = sigma
-    return Scene(pos_alpha, scales, np.ascontiguousarray(q, np.float32), sh.reshape(-1), sh_degree, name)
+    meta = {}
+    if random_degrees and K > 1:
+        deg = np.random.default_rng([seed, 1]).integers(0, sh_degree + 1, n).astype(np.uint8)
+        for d in range(sh_degree):
+            sh[deg == d, (d + 1) ** 2:, :] = 0.0
+        meta["degrees"] = deg
+    return Scene(pos_alpha, scales, np.ascontiguousarray(q, np.float32), sh.reshape(-1), sh_degree, name, meta)
 
 
 # ---- cameras ---------------------------------------------------------------------------
@@ -196,7 +209,7 @@ def batched_64():
 
 
 def scale_4k():
-    scene = make_scene(6_000_000, seed=3, ball_radius=20.0, name="scale_4k")
+    scene = make_scene(6_000_000, seed=3, ball_radius=20.0, name="scale_4k", random_degrees=True)
     cams = []
     for k in range(16):
         a = 2.0 * math.pi * k / 16

@@ -220,7 +220,11 @@ void gsr_perspective_vk(float fovy_radians, float aspect, float z_near, float z_
 /* ---- the control block (TileControl, splat_tile_renderer.h:117-128 + extensions) -------- */
 typedef enum GsrControlStatus {
     GSR_CONTROL_OK = 0,
-    GSR_CONTROL_TIMEOUT = 1,         /* a look-back wait hit its iteration limit */
+    GSR_CONTROL_TIMEOUT = 1,         /* a bounded device-side wait hit its iteration limit (a look-back,
+                                        or a preprocess block's wait for its staged SH, which can leave
+                                        that bulk copy writing shared memory after the block ended):
+                                        the frame's records, list and image are untrusted, and
+                                        gsr_read_control reports GSR_ERROR_DEVICE_TIMEOUT */
     GSR_CONTROL_BOUNDS = 2,          /* an index check failed; the access was skipped */
     GSR_CONTROL_KEY_RANGE = 4        /* the sort key did not fit the planned bits */
 } GsrControlStatus;
@@ -427,29 +431,35 @@ typedef enum GsrScanMode { GSR_SCAN_PLAIN = 0, GSR_SCAN_NONZERO = 1, GSR_SCAN_GA
  * returns after the scan has finished on `stream`. */
 int gsr_scan(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
              uint32_t mode, void* stream);
-/* Largest count gsr_scan_static accepts. */
-#define GSR_SCAN_STATIC_MAX_COUNT 16777216u
-/* gsr_scan without any allocation. NO COUNTERPART IN THE REFERENCE (its GpuScan, gpu_scan.h,
- * owns scratch buffers that it creates itself); added for callers that must not allocate
- * device memory: recovery code that runs after an allocation failed (device memory held by a
- * resident scene), hooks of a caching allocator that must not re-enter it, and streams that
- * must not stall behind cudaFree, which synchronizes the whole device.
- * Same arguments, results and errors as gsr_scan. The scratch (a 512-byte control block and
- * one look-back word per 2048 items) is a fixed 66,048-byte static device array of this
- * library; count above GSR_SCAN_STATIC_MAX_COUNT (2^24) is rejected with
- * GSR_ERROR_INVALID_ARGUMENT before anything is launched. The call clears what must start at
- * zero (the block tickets and the look-back words) on `stream` and returns after the scan
- * has finished there. Calls that overlap in time on one device (two streams or two host
- * threads) share the array and race: the caller serializes them. The first call on each
- * device looks the array up (cudaGetSymbolAddress) and should come before any stream
- * capture begins on that device. */
-int gsr_scan_static(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
-                    uint32_t mode, void* stream);
 /* Stable LSD sort of (key, value) pairs by the low key_bits of the key, in place (device
  * pointers). keys_hi may be NULL (32-bit keys); with it the key is (keys_hi << 32 | keys_lo).
  * Bit-for-bit the order of a stable sort (DepthSorter::radixSortPairs for 32-bit keys). */
 int gsr_sort_pairs(uint32_t* keys_lo, uint32_t* keys_hi, uint32_t* values, uint32_t count, uint32_t key_bits,
                    void* stream);
+
+/* ---- allocation-free scan (no counterpart in the reference) ---------------------------- */
+/* Largest count gsr_scan_static accepts. */
+#define GSR_SCAN_STATIC_MAX_COUNT 16777216u
+/* gsr_scan without any allocation, for callers that must not allocate device memory: recovery
+ * code that runs after an allocation failed (device memory held by a resident scene), hooks of
+ * a caching allocator that must not re-enter it, and streams that must not stall behind
+ * cudaFree, which synchronizes the whole device.
+ * Same arguments, results and errors as gsr_scan. The scratch (a 512-byte control block and
+ * one look-back word per 2048 items) is a fixed 66,048-byte static device array of this
+ * library, held on every device that loads it until the process exits; count above
+ * GSR_SCAN_STATIC_MAX_COUNT (2^24) is rejected with GSR_ERROR_INVALID_ARGUMENT before anything
+ * is launched. The call clears what must start at zero (the block tickets and the look-back
+ * words) on `stream` and returns after the scan has finished there. Calls that overlap in time
+ * on one device (two streams or two host threads) share the array and race: the caller
+ * serializes them.
+ * Set-up: with CUDA's lazy module loading, the array and the scan's kernels are loaded on a
+ * device when first used, which can allocate device memory. This library does that loading
+ * (and looks up the array's address) in every set-up call on a device: gsr_scene_create,
+ * gsr_renderer_create, gsr_scan and gsr_sort_pairs; a caller that makes none of those first
+ * calls gsr_scan_static once with count 0, which does only that. Make that first call before
+ * any stream capture begins on the device. */
+int gsr_scan_static(const uint32_t* in, const uint32_t* index, uint32_t* out, uint32_t* total, uint32_t count,
+                    uint32_t mode, void* stream);
 
 /* ---- scene input: 3DGS PLY files (src/scene/ply_loader.h:1-120) --------------------------
  * Host-side: the file is validated exactly as loadGaussianPly does (same accepted files, the

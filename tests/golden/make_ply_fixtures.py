@@ -1,7 +1,7 @@
 """Generates the PLY loader fixtures under tests/golden/ply/ with the reference's own synthetic
 file generator (tools/gen_synthetic_ply.py of the reference tree, imported from REF):
 
-    python tests/golden/make_ply_fixtures.py [REF]        (REF defaults to /root/reference)
+    python tests/golden/make_ply_fixtures.py REF          (REF = the reference checkout, or $REF)
 
 It writes the small files of the generator's standard set (single, grid 512, random 2000 without
 normals, overlap, shdir) plus a 300-gaussian degree-1 random cloud in place of the set's 10k and
@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import importlib.util
 import json
+import os
 import sys
 from pathlib import Path
 
@@ -50,4 +51,7 @@ def main(ref: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("REF")
+    if not ref:
+        raise SystemExit("usage: make_ply_fixtures.py REF (the reference checkout; or set $REF)")
+    main(Path(ref))

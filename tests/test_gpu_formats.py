@@ -16,9 +16,9 @@ FORMATS = [("f32", "soa"), ("f32", "split"), ("f32", "aos"), ("f16", "split"), (
 def scene():
     from gsr_b200 import scenes
 
-    s = scenes.make_scene(60_000, seed=11, ball_radius=4.0)
-    # a copy with degree 1 and some zero bands so that the per-gaussian degree varies
-    return s
+    # per-gaussian degrees 0..3 (the bands above each gaussian's degree are zero), so that with a
+    # threshold the stored degree varies from gaussian to gaussian
+    return scenes.make_scene(60_000, seed=11, ball_radius=4.0, random_degrees=True)
 
 
 @pytest.mark.parametrize("fmt,layout", FORMATS)

@@ -1,7 +1,10 @@
-"""gsr_scan_static, the allocation-free exclusive scan (no counterpart in the reference): on two
-calls in a row it gives exactly what gsr_scan gives on the same inputs, and a count above its
-static limit is refused before anything runs. Collected last (the file name), so it also runs
-after every other GPU test has used the device."""
+"""gsr_scan_static, the allocation-free exclusive scan (no counterpart in the reference), for
+callers that must not allocate device memory (recovery after a failed allocation, allocator
+hooks, streams that must not wait behind cudaFree). On two calls in a row it gives exactly what
+gsr_scan gives on the same inputs and what a numpy exclusive sum in uint32 gives; its set-up
+call (count 0) does nothing visible; a count above its static limit is refused before anything
+runs. Collected last (the file name), so it also runs after every other GPU test has used the
+device, and it passes alone in a fresh process as well."""
 import numpy as np
 import pytest
 
@@ -28,6 +31,8 @@ def test_static_scan_equals_scan_on_two_calls_in_a_row(gpu):
     idx = rng.integers(0, cap, cap).astype(np.uint32)
     d_in = torch.from_numpy(vals.view(np.int32)).cuda()
     d_idx = torch.from_numpy(idx.view(np.int32)).cuda()
+    # the set-up call: count 0 loads the scratch and the kernels and touches no buffer
+    gpu.scan_static(0, None, 0, None, 0, 0)
     # two calls in a row with different counts and modes: the second must not see the first's
     # tickets or look-back words
     for n, mode in [(3_000_017, 0), (1_048_577, 2)]:
@@ -36,6 +41,8 @@ def test_static_scan_equals_scan_on_two_calls_in_a_row(gpu):
         np.testing.assert_array_equal(got, want, err_msg=f"n {n} mode {mode}")
         np.testing.assert_array_equal(got_tot, want_tot)
         v = vals[idx[:n]] if mode == 2 else vals[:n]
+        excl = np.concatenate([[0], np.cumsum(v, dtype=np.uint64)[:-1]]).astype(np.uint32)
+        np.testing.assert_array_equal(got[:n], excl, err_msg=f"numpy exclusive sum, n {n} mode {mode}")
         assert got_tot[0] == np.uint32(v.sum(dtype=np.uint64))
         assert np.all(got[n:] == np.uint32(0xDEADBEEF))
 
