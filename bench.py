@@ -1,28 +1,46 @@
 """Benchmark of the B200 splat-tiles frame path (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--config plain_1080p|plain_1080p_f16|plain_720p]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config all|<workload>]
     python bench.py --impl reference ...    # the reference's own CPU renderer on this host
 
-Workload (default): the plain forward render at 1920x1080 of 1,240,000 synthetic gaussians
-(means uniform in a ball of radius 8, SH degree 3, fp32 SoA scene), on the 300-frame 360-degree
-orbit of radius 14 at height 2; tight tile bounds, adaptive list, binning list construction (depth
-sort of the visible splats, emission in depth order, stable sort by tile). A step renders one view
-of the orbit (view k = frame k mod 300, ranks start at different frames). The line's `value` is
-the batched + learned-colour form (the metric's subject); the plain form is in `forms.plain`.
+Workloads (seeded synthetic scenes with the distributions the benchmark configurations state;
+the reference's real INRIA scenes are not available):
 
-value        views/s over all ranks, scene and camera parameters resident on the device: CUDA
-             events around the timed steps on one stream (gsr_render_views frames of D views for
-             the batched forms, K gsr_render calls for the plain form; barrier + synchronize on
-             both sides, max over ranks).
-e2e          the same metric through gsr_render_views_to_host / gsr_render_to_host, the calls a
-             host application makes: each step passes the cameras from host memory and copies the
-             8-bit RGB images into pinned host memory, then synchronizes. The scene upload is an init-time step
-             (GpuScene::upload in the reference) and is not part of a step.
-roofline     the front kernel (preprocess + count + scan + key emission) against the measured
-             HBM copy bandwidth: algorithmic bytes per frame / its CUDA-event duration.
-cpu_baseline the reference's own CPU renderer (renderReference compiled from its sources, else
-             the C restatement), rank 0, all host threads, a bounded sample of the orbit.
-L2           the scene (298 MB fp32) is larger than the 126 MB L2, so no flush between steps.
+  plain_720p       100,000 gaussians, fp32 soa, SH3, one camera at (0, 0, 10), 1280x720
+  plain_1080p      1,240,000 gaussians (ball radius 8), fp32 soa, SH3, 1920x1080, the 300-view
+                   360-degree orbit of radius 14 at height 2 (the headline workload)
+  plain_1080p_f16  the same scene in the fp16 split format
+  learned_1080p    the plain_1080p scene with the learned colour stage (fp16 latent + BF16 MLP
+                   decoder, 2,000 Adam steps of 65,536 (gaussian, direction) pairs, seed 1, SH
+                   fallback above 2/255), and the same decoder forced on for every gaussian
+  batched_64       559,000 gaussians (ball radius 6), 64 cameras of mixed size in one frame
+  scale_4k         6,000,000 gaussians (ball radius 20), fp16 split, per-gaussian SH degree
+                   drawn from 0-3, 16 views at 3840x2160, learned colour with SH fallback
+
+`--config all` (the default) measures every workload; the line's headline `value` is the batched
++ learned-colour form of learned_1080p (the metric's subject), `configs` holds each workload.
+
+step         one pass over a workload's views: the 300-view orbit, the 64 batched views, the 16
+             4K views. K steps are timed after W warm-up steps (at least until the adaptive
+             list has kept its capacity for three frames).
+value        views/s over all ranks, scene and cameras resident on the device: CUDA events on
+             the launching stream around the K steps (barrier + synchronize on both sides, the
+             max over ranks).
+e2e          the same views through the calls a host application makes (gsr_render_to_host,
+             gsr_render_views_to_host): cameras from host memory, every view's RGB8 image
+             copied into pinned host memory, synchronized every call.
+parity       per workload (the CPU leg, rank 0), one view (or one per resolution): the list
+             (keys, values, tile ranges) bit for bit against the oracle's construction, the
+             float image's PSNR and the 8-bit image's PSNR and largest difference against the
+             reference's own renderReference; forms that must equal another form say so.
+roofline     preprocess + sort (preprocess, depth sort, scan + emission, tile sort, ranges)
+             against the measured HBM copy bandwidth: algorithmic bytes per frame over the
+             summed CUDA-event pass times; each kernel's fraction in `kernels`.
+multi-GPU    one process per GPU. The orbit workloads run as replicas (each rank renders the
+             whole orbit: weak scaling); batched_64 and scale_4k split their views across the
+             ranks, balanced by pixel count, and gather per-view checksums on rank 0.
+L2           every scene (>= 67 MB) plus its per-frame lists exceeds the 126 MB L2 over a
+             step; no flush between steps.
 """
 from __future__ import annotations
 
@@ -30,6 +48,7 @@ import argparse
 import json
 import math
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -44,6 +63,7 @@ sys.path.insert(0, str(REPO / "gaussian-splat-renderer_b200"))
 
 METRIC = "1080p views/s at 1.24M gaussians: batched+MLP colour vs plain, PSNR>=45 dB"
 UNIT = "views/s"
+WORKLOADS = ("plain_1080p", "learned_1080p", "plain_1080p_f16", "batched_64", "scale_4k", "plain_720p")
 
 
 def load_peaks():
@@ -54,33 +74,83 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
-# warp instructions of one plain 1080p render pass (ncu smsp__inst_issued, profiles/kernels_plain_1080p.md)
-RENDER_WARP_INSTRUCTIONS_1080P = 228.0e6
+# ---- clocks and device memory sampled during the timed regions (NVML, read-only) ------------
+class Sampler:
+    """A thread reading the SM clock, its maximum, the clock event reasons, power and the used
+    device memory every 20 ms while it is open (nothing is set)."""
 
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4,
+               "hw_power_brake_slowdown": 0x80}
 
-def render_issue(passes: dict, clocks: dict, config: str):
-    ms = passes.get("render tiles")
-    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
-    if config != "plain_1080p" or not ms or not mhz:
-        return None
-    achieved = RENDER_WARP_INSTRUCTIONS_1080P / (ms * 1e-3) / 1e12
-    peak = 148 * 4 * mhz * 1e6 / 1e12
-    return {"bound": "issue", "achieved": round(achieved, 4), "peak": round(peak, 4), "unit": "T warp-instr/s",
-            "frac": round(achieved / peak, 4), "instructions_source": "ncu issued instructions, one frame"}
+    def __init__(self, device_index: int):
+        self.rows, self.mem_peak, self.error = [], 0, None
+        self._stop = threading.Event()
+        self.handle = None
+        try:
+            import pynvml as N
 
+            N.nvmlInit()
+            self.N = N
+            self.handle = self._handle(device_index)
+        except Exception as e:  # noqa: BLE001
+            self.error = f"NVML unavailable: {e}"
 
-# ---- configurations ---------------------------------------------------------------------
-def make_config(name: str):
-    from gsr_b200 import scenes
+    def _handle(self, index: int):
+        N = self.N
+        try:
+            import torch
 
-    if name in ("plain_1080p", "plain_1080p_f16"):
-        scene, cams = scenes.plain_1080p(300)
-        fmt, layout = ("f16", "split") if name.endswith("f16") else ("f32", "soa")
-        return scene, cams, fmt, layout
-    if name == "plain_720p":
-        scene, cams = scenes.plain_720p()
-        return scene, cams, "f32", "soa"
-    raise SystemExit(f"unknown config {name}")
+            uuid = str(torch.cuda.get_device_properties(index).uuid)
+            return N.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU-") else uuid)
+        except Exception:  # noqa: BLE001
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [v for v in vis.split(",") if v.strip()]
+            idx = int(ids[index]) if index < len(ids) and ids[index].strip().isdigit() else index
+            return N.nvmlDeviceGetHandleByIndex(idx)
+
+    def memory_used(self) -> int:
+        if self.handle is None:
+            return 0
+        return int(self.N.nvmlDeviceGetMemoryInfo(self.handle).used)
+
+    def _run(self):
+        N = self.N
+        reasons_fn = getattr(N, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            N.nvmlDeviceGetCurrentClocksThrottleReasons
+        while not self._stop.is_set():
+            try:
+                sm = N.nvmlDeviceGetClockInfo(self.handle, N.NVML_CLOCK_SM)
+                mx = N.nvmlDeviceGetMaxClockInfo(self.handle, N.NVML_CLOCK_SM)
+                rs = int(reasons_fn(self.handle))
+                pw = N.nvmlDeviceGetPowerUsage(self.handle) / 1000.0
+                mem = self.memory_used()
+                self.mem_peak = max(self.mem_peak, mem)
+                self.rows.append((sm, mx, rs, pw))
+            except Exception as e:  # noqa: BLE001
+                self.error = f"NVML query failed: {e}"
+                return
+            self._stop.wait(0.02)
+
+    def __enter__(self):
+        self.rows = []
+        self._stop.clear()
+        if self.handle is not None:
+            self.thread = threading.Thread(target=self._run, daemon=True)
+            self.thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        if self.handle is not None:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "no samples"], "samples": 0}
+        reasons = sorted({k for _, _, rs, _ in self.rows for k, bit in self.REASONS.items() if rs & bit})
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": max(r[1] for r in self.rows),
+                "reasons": reasons, "samples": len(self.rows),
+                "power_w_median": round(statistics.median(r[3] for r in self.rows), 1)}
 
 
 # ---- distributed plumbing (one process per GPU) -------------------------------------------
@@ -96,180 +166,725 @@ class Dist:
             import torch.distributed as dist
 
             os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
             self.pg = dist
+
+    def _dev(self):
+        return "cuda" if self.pg.get_backend() == "nccl" else "cpu"
 
     def barrier(self):
         if self.pg:
-            self.pg.barrier()
+            if self.pg.get_backend() == "nccl":
+                import torch
+
+                self.pg.barrier(device_ids=[torch.cuda.current_device()])
+            else:
+                self.pg.barrier()
 
     def max(self, value: float) -> float:
         if not self.pg:
             return value
         import torch
 
-        dev = "cuda" if self.pg.get_backend() == "nccl" else "cpu"
-        t = torch.tensor([value], dtype=torch.float64, device=dev)
+        t = torch.tensor([value], dtype=torch.float64, device=self._dev())
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
+
+    def sum(self, value: float) -> float:
+        if not self.pg:
+            return value
+        import torch
+
+        t = torch.tensor([value], dtype=torch.float64, device=self._dev())
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def gather_view_results(self, views: list[int], values: list[float], total: int) -> np.ndarray:
+        """Every rank's per-view results into one array of `total` slots on every rank (an
+        all-reduce of a zero-filled vector: each view is owned by exactly one rank)."""
+        out = np.zeros(total, np.float64)
+        out[np.asarray(views, np.int64)] = values
+        if not self.pg:
+            return out
+        import torch
+
+        t = torch.from_numpy(out).to(self._dev())
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return t.cpu().numpy()
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
 
 
-# ---- clocks sampled during the timed region ---------------------------------------------
-class ClockSampler:
-    def __init__(self, index: int):
-        self.index = index
-        self.rows = []
-        self.proc = None
-
-    def __enter__(self):
-        cmd = ["nvidia-smi", f"--id={self.index}",
-               "--query-gpu=clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-               "--format=csv,noheader,nounits", "-lms", "50"]
-        try:
-            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
-        return self
-
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) >= 8:
-                self.rows.append(parts)
-
-    def __exit__(self, *exc):
-        if self.proc:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
-
-    def summary(self):
-        if not self.rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clocks not sampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+def partition_views(pixels, ranks: int) -> list[list[int]]:
+    """Views split across ranks, balanced by pixel count: largest view first onto the rank with
+    the fewest pixels so far (ties: lower rank, lower view index); each rank's views in order."""
+    order = sorted(range(len(pixels)), key=lambda v: (-pixels[v], v))
+    load = [0] * ranks
+    parts = [[] for _ in range(ranks)]
+    for v in order:
+        r = min(range(ranks), key=lambda k: (load[k], k))
+        parts[r].append(v)
+        load[r] += pixels[v]
+    return [sorted(p) for p in parts]
 
 
-# ---- algorithmic bytes of the front kernel (preprocess + scan + key emission) -------------
+def free_port() -> int:
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def launch_ranks(argv: list[str], gpus: int) -> int:
+    """`--gpus N` without a launcher: start N ranks (one process per GPU) with torch's launcher
+    on this host and return its exit status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={free_port()}", str(Path(__file__).resolve()), *argv]
+    return subprocess.call(cmd)
+
+
+# ---- workloads ----------------------------------------------------------------------------
+_SCENES = {}
+
+
+def workload(name: str):
+    """(scene, cameras, scene format, layout, SH threshold) of a workload; scenes are cached."""
+    from gsr_b200 import scenes
+
+    if name in ("plain_1080p", "plain_1080p_f16", "learned_1080p"):
+        if "1080p" not in _SCENES:
+            _SCENES["1080p"] = scenes.plain_1080p(300)
+        scene, cams = _SCENES["1080p"]
+        fmt, layout = ("f16", "split") if name.endswith("f16") else ("f32", "soa")
+        return scene, cams, fmt, layout, -1.0
+    if name == "plain_720p":
+        scene, cams = scenes.plain_720p()
+        return scene, cams, "f32", "soa", -1.0
+    if name == "batched_64":
+        scene, cams = scenes.batched_64()
+        return scene, cams, "f32", "soa", -1.0
+    if name == "scale_4k":
+        scene, cams = scenes.scale_4k()
+        return scene, cams, "f16", "split", 0.0  # threshold 0: each gaussian keeps its drawn degree
+    raise SystemExit(f"unknown workload {name}")
+
+
+# ---- algorithmic bytes of the passes (binning list mode) ------------------------------------
 def depth_sort_passes(ctl) -> int:
-    """Digit passes of binning mode's depth sort: the depth bits that vary over the frame plus the
-    bit that puts the splats with no tiles last, 8 bits a pass."""
+    """Digit passes of the depth sort: the depth bits that vary over the frame plus the bit
+    that puts the records without tiles last, 8 bits a pass."""
     lo, hi = ctl.depth_min_bits, ctl.depth_max_bits
     w = (lo ^ hi).bit_length() if lo <= hi else 0
     return (w + 1 + 7) // 8
 
 
-def front_bytes(scene_format: str, ctl, n: int, list_mode: str = "global") -> float:
-    """Bytes the front (preprocess + scan + key emission) must move for one frame, from the
-    frame's counts. Preprocess: posAlpha of every gaussian, scale + rotation of those past the
-    near/opacity culls, SH of the visible ones; writes the tile counts, the 48-byte records and
-    16-byte coverage hints of the visible ones. Scan: counts in, offsets out. Emission: counts of
-    every gaussian, offset + hint of the visible ones (the span hint holds a splat's tile runs;
-    the few splats beyond its 7 rows also need their record: not counted) plus their depth in
-    global mode, and the entries (8 B packed, 12 B as key/value pairs).
-    Binning mode adds the 8-byte depth word of every gaussian (written by the preprocess), its
-    depth sort (histogram read + a read and a write of every word per pass), and walks the sorted
-    words in the scan and the emission (8 B each, with the counts and offsets gathered)."""
+def pass_bytes(scene_format: str, ctl, n: int, tiles: int) -> dict:
+    """Bytes each pass must move for one frame, from the frame's counts.
+    preprocess: posAlpha of every gaussian, scale + rotation of those past the near/opacity
+      culls, SH of the visible ones (fp32 soa 16 + 32 + 192 B; fp16 split 16 + 16 + 96 B); writes
+      the tile count and depth word of every gaussian, the 48-byte record and 16-byte coverage
+      hint of the visible ones.
+    depth sort: the histogram reads every depth word, each pass reads and writes it.
+    scan + emission: the sorted words, counts and offsets (scan); the sorted words, counts,
+      offsets and span hints again and 8 bytes per list entry (emission).
+    tile sort: histogram read + a read and a write of every entry per active pass.
+    ranges: every entry read, 8 bytes per tile written."""
     past_cull = n - ctl.cull_counts[1] - ctl.cull_counts[4]
     vis = ctl.cull_counts[0]
+    m = ctl.entries
     if scene_format == "f32":
-        b = 16 * n + 32 * past_cull + 192 * vis
-    else:  # f16 split: G16 record 32 B (posAlpha in the first 16 B), colour 96 B
-        b = 16 * n + 16 * past_cull + 96 * vis
-    b += 4 * n + 64 * vis  # preprocess writes
-    if list_mode == "binning":
-        b += 8 * n  # depth words
-        b += 8 * n + 16 * n * depth_sort_passes(ctl)  # depth sort
-        b += 8 * n + 4 * n + 4 * n  # gathered scan: sorted words, counts, offsets
-        b += 8 * n + 4 * n + 4 * n + 16 * vis + 8 * ctl.entries  # emission in depth order
-        return float(b)
-    b += 8 * n  # scan
-    b += 4 * n + 20 * vis + (8 if ctl.packed_entries else 12) * ctl.entries  # emission
-    return float(b)
+        pre = 16 * n + 32 * past_cull + 192 * vis
+    else:
+        pre = 16 * n + 16 * past_cull + 96 * vis
+    pre += 4 * n + 8 * n + 64 * vis
+    per_entry = 16 if ctl.packed_entries else 24
+    return {
+        "preprocess": float(pre),
+        "depth sort": float(8 * n + 16 * n * depth_sort_passes(ctl)),
+        "scan + emission": float((8 + 4 + 4) * n + (8 + 4 + 4) * n + 16 * vis + 8 * m),
+        "tile sort": float(8 * m + per_entry * m * ctl.sort_passes),
+        "ranges": float(8 * m + 8 * tiles),
+    }
 
 
-# DRAM bytes of the front per frame of the default workload, from one ncu capture
-# (profiles/kernels_plain_1080p.md: preprocess + scan + duplicate, read + write).
-FRONT_TRAFFIC_PLAIN_1080P = {
-    "global": None,  # not captured since the span hints changed the emission
-    # preprocess, depth histogram, 4 depth passes, gathered scan, emission in depth order
-    "binning": (314.4 + 70.7 + 10.0 + 39.6 + 14.9 + 47.9 + 2.9) * 1e6,
-}
+PASS_NAMES = {"preprocess": "reset + preprocess (depth keys)", "depth sort": "depth sort (total)",
+              "scan + emission": "scan + duplicate (depth order)", "tile sort": "tile sort (total)",
+              "ranges": "tile ranges"}
+
+# DRAM bytes of the same passes for one frame of plain_1080p, from one ncu capture of this
+# build (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot read the counters itself
+TRAFFIC_PLAIN_1080P_CAPTURE = (314.4 + 70.7 + 10.0 + 39.6 + 14.9 + 47.9 + 2.9) * 1e6
 
 
-SORT_FORMS = {"binning": "binning: depth sort of the visible splats + stable onesweep sort by tile",
-              "global": "global: one onesweep sort of (tile, depth) keys"}
+# ---- the CPU leg: the reference's renderer as the baseline and as the checker of the GPU's views
+def quantize(rgb):
+    """lround(clamp(v, 0, 1) * 255), the reference's PNG writer (src/app/image_io.cpp:55-56)."""
+    v = np.clip(rgb.astype(np.float32), 0.0, 1.0) * np.float32(255.0)
+    return np.floor(v.astype(np.float64) + 0.5).astype(np.uint8)
 
 
-def sort_bytes(ctl) -> float:
-    """Histogram read (8 B/entry) + per active pass the read and write of every entry: 16 B for
-    packed 64-bit entries, 24 B for (key, value) pairs."""
-    per_pass = 16 if ctl.packed_entries else 24
-    return float(8 * ctl.entries + per_pass * ctl.entries * ctl.sort_passes)
+def psnr(a, b, peak=1.0) -> float:
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    mse = float(np.mean((a - b) ** 2))
+    return 999.0 if mse == 0.0 else round(10.0 * math.log10(peak * peak / mse), 2)
 
 
-# ---- the CPU baseline ----------------------------------------------------------------------
-def cpu_reference_run(scene, cams, max_frames: int, time_budget_s: float, warmup: int = 1):
-    sys.path.insert(0, str(REPO / "oracle"))
-    import oracle as O
+class CpuLeg:
+    """Rank 0's CPU work: renderReference (the reference's own CPU renderer compiled from its
+    sources, else the C restatement) timed on a bounded sample of the orbit as the baseline, and
+    the same CPU code as the checker of one GPU view per workload (the list against the
+    restatement's construction bit for bit, the images against renderReference). None of it is
+    inside a timed GPU region."""
 
-    kind = "reference" if O.reference_available() else "port"
-    orc = O.Oracle(kind)
-    threads = os.cpu_count() or 1
-    for c in cams[:warmup]:
-        cam = orc.camera_from_viewer(c.view, c.proj, c.model, c.width, c.height)
-        orc.render(scene, cam, bounds=1, threads=threads)
-    done, t0 = 0, time.perf_counter()
-    step = max(1, len(cams) // max(1, max_frames))
-    frames = []
-    for k in range(0, len(cams), step):
-        if done >= max_frames or time.perf_counter() - t0 > time_budget_s:
-            break
-        c = cams[k]
-        cam = orc.camera_from_viewer(c.view, c.proj, c.model, c.width, c.height)
-        orc.render(scene, cam, bounds=1, threads=threads)
-        frames.append(k)
-        done += 1
-    dt = time.perf_counter() - t0
-    return {"value": done / dt if dt > 0 else 0.0, "unit": UNIT, "cores": threads, "kind": kind,
-            "sample": f"{done} views of the 300-frame orbit (every {step}th frame), tight bounds, "
-                      f"renderReference with {threads} threads, {dt:.1f} s"}
+    def __init__(self):
+        sys.path.insert(0, str(REPO / "oracle"))
+        import oracle as O
+
+        self.port = O.Oracle("port")
+        self.kind = "reference" if O.reference_available() else "port"
+        self.ref = O.Oracle("reference") if self.kind == "reference" else self.port
+        self.threads = os.cpu_count() or 1
+
+    def decoded(self, scene, fmt: str, layout: str, threshold: float):
+        """The floats the GPU reads: the scene itself (fp32) or the decode of its encoding."""
+        if fmt == "f32":
+            return scene
+        from gsr_b200 import scenes
+
+        enc = self.port.encode(scene, {"f16": 1, "q8": 2}[fmt], {"split": 1, "aos": 2}[layout], 3, threshold)
+        pa, sc, ro, sh = self.port.decode(enc, scene.count)
+        return scenes.Scene(pa, sc, ro, sh, int(enc["desc"][7]))
+
+    def check_view(self, G, gs, dec_scene, cam, stream, tile_size: int = 16) -> dict:
+        """One view on the GPU (list capacity large enough for it) against the CPU code."""
+        r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=False, budget_mb=4096, rgb8=True,
+                                      tile_size=tile_size))
+        r.render(cam, stream)
+        lo, hi, val, ranges, ctl = r.read_back()
+        rgba, rgb8 = r.read_back_image(rgb8=True)
+        r.close()
+        port = self.port
+        ocam = port.camera_from_viewer(cam.view, cam.proj, cam.model, cam.width, cam.height)
+        osp = port.preprocess(dec_scene, ocam, dec_scene.sh_degree, gpu_rules=True)
+        ocounts = port.coverage_counts(osp, ocam, 1, tile_size)
+        olist = port.tile_list(osp, ocounts, ocam, 1, tile_size)
+        same = (len(hi) == len(olist["keys_hi"]) and np.array_equal(hi, olist["keys_hi"]) and
+                np.array_equal(lo, olist["keys_lo"]) and np.array_equal(val, olist["values"]) and
+                np.array_equal(ranges, olist["ranges"]))
+        rcam = self.ref.camera_from_viewer(cam.view, cam.proj, cam.model, cam.width, cam.height)
+        img, _ = self.ref.render(dec_scene, rcam, bounds=1, threads=self.threads)
+        want8 = quantize(img)
+        diff8 = int(np.abs(rgb8.astype(np.int16) - want8.astype(np.int16)).max())
+        return {"list_bit_exact": bool(same), "entries": int(ctl.entries), "oracle_entries": int(olist["duplicates"]),
+                "overflow": int(ctl.overflow),
+                "psnr_float_db": psnr(np.clip(rgba[..., :3], 0, 1), np.clip(img, 0, 1)),
+                "psnr_8bit_db": psnr(rgb8, want8, 255.0), "max_8bit_diff": diff8, "image_oracle": self.kind,
+                "view": f"{cam.width}x{cam.height}"}
+
+    def baseline(self, scene, cams, max_frames: int, time_budget_s: float, warmup: int = 1) -> dict:
+        """renderReference on all host threads over a bounded, evenly spaced sample of the cameras."""
+        orc = self.ref
+        for c in cams[:warmup]:
+            orc.render(scene, orc.camera_from_viewer(c.view, c.proj, c.model, c.width, c.height), bounds=1,
+                       threads=self.threads)
+        step = max(1, len(cams) // max(1, max_frames))
+        done, t0 = 0, time.perf_counter()
+        for k in range(0, len(cams), step):
+            if done >= max_frames or time.perf_counter() - t0 > time_budget_s:
+                break
+            c = cams[k]
+            orc.render(scene, orc.camera_from_viewer(c.view, c.proj, c.model, c.width, c.height), bounds=1,
+                       threads=self.threads)
+            done += 1
+        dt = time.perf_counter() - t0
+        return {"value": round(done / dt, 4) if dt > 0 else 0.0, "unit": UNIT, "cores": self.threads, "kind": self.kind,
+                "sample": f"{done} of {len(cams)} views (every {step}th), tight bounds, renderReference with "
+                          f"{self.threads} threads, {dt:.1f} s"}
 
 
+_CPU = {}
+
+
+def cpu_leg(args, dist) -> "CpuLeg | None":
+    """The CPU leg on rank 0 (None elsewhere, or with --no-cpu-baseline)."""
+    if dist.rank != 0 or args.no_cpu_baseline:
+        return None
+    if "leg" not in _CPU:
+        _CPU["leg"] = CpuLeg()
+    return _CPU["leg"]
+
+
+# ---- timing of one form ------------------------------------------------------------------------
+class Frames:
+    """The calls of one form over a workload's views: `frames` lists what each call renders
+    (a GsrCamera for a one-view call, a SplatCamera array for a batched frame); one step is
+    every call once."""
+
+    def __init__(self, G, cams, views_per_frame: int, order=None):
+        self.G = G
+        order = list(range(len(cams))) if order is None else list(order)
+        self.views = order
+        self.d = views_per_frame
+        if views_per_frame == 1:
+            self.calls = [G.to_c_camera(cams[v]) for v in order]
+            self.sizes = [[(cams[v].width, cams[v].height)] for v in order]
+        else:
+            self.calls, self.sizes = [], []
+            for k in range(0, len(order), views_per_frame):
+                chunk = [cams[order[(k + j) % len(order)]] for j in range(views_per_frame)]
+                self.calls.append(G.camera_array(chunk))
+                self.sizes.append([(c.width, c.height) for c in chunk])
+        self.views_per_step = len(self.calls) * views_per_frame
+
+
+def render_call(r, frames: Frames, k: int, stream: int):
+    call = frames.calls[k % len(frames.calls)]
+    if frames.d == 1:
+        r.render(call, stream)
+    else:
+        r.render_views(call, stream)
+
+
+def to_host_call(r, frames: Frames, k: int, host: dict, stream: int):
+    call = frames.calls[k % len(frames.calls)]
+    px = sum(w * h for w, h in frames.sizes[k % len(frames.sizes)])
+    buf = host[px]
+    if frames.d == 1:
+        r.render_to_host(call, buf, stream)
+    else:
+        r.render_views_to_host(call, buf, stream)
+
+
+def time_form(r, frames: Frames, args, dist: Dist, sampler: Sampler, stream_obj):
+    """W warm-up steps (and until the adaptive list is stable), then K timed steps on the device
+    and K timed steps end to end. Returns the form's numbers (max over ranks)."""
+    import torch
+
+    stream = stream_obj.cuda_stream
+    calls = len(frames.calls)
+    with torch.cuda.stream(stream_obj):
+        stable, last, k = 0, -1, 0
+        limit = args.warmup * calls + 64
+        while k < limit and (k < args.warmup * calls or stable < 3):
+            render_call(r, frames, k, stream)
+            if k >= args.warmup * calls - 6 or k % 16 == 0:
+                stream_obj.synchronize()
+                cap = r.capacity()[0]
+                stable, last = (stable + 1 if cap == last else 0), cap
+            k += 1
+    stream_obj.synchronize()
+    n_calls = args.steps * calls
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches0 = r.kernel_launches()
+    resizes0 = r.capacity()[2]
+    dist.barrier()
+    torch.cuda.synchronize()
+    with sampler:
+        start.record(stream_obj)
+        for j in range(n_calls):
+            render_call(r, frames, j, stream)
+        end.record(stream_obj)
+        end.synchronize()
+    torch.cuda.synchronize()
+    dist.barrier()
+    ms = dist.max(start.elapsed_time(end))
+    clocks = sampler.summary()
+    launches = r.kernel_launches() - launches0
+    resizes = r.capacity()[2] - resizes0
+    # end to end: pinned host buffers per frame size
+    host = {}
+    for sz in frames.sizes:
+        px = sum(w * h for w, h in sz)
+        if px not in host:
+            host[px] = torch.empty((px * 3,), dtype=torch.uint8).pin_memory().numpy()
+    for j in range(min(calls, 3)):
+        to_host_call(r, frames, j, host, stream)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record(stream_obj)
+    for j in range(n_calls):
+        to_host_call(r, frames, j, host, stream)
+    e1.record(stream_obj)
+    e1.synchronize()
+    e2e_ms = dist.max(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3))
+    views = n_calls * frames.d
+    views_all = dist.sum(views)
+    d2h = sum(sum(w * h for w, h in sz) * 3 for sz in frames.sizes)
+    return {"views_per_frame": frames.d, "views_timed": int(views_all), "steps": args.steps,
+            "views_per_s": round(views_all / (ms / 1e3), 3), "e2e_views_per_s": round(views_all / (e2e_ms / 1e3), 3),
+            "ms_per_view": round(ms / views, 4), "ms_per_step": round(ms / args.steps, 3),
+            "e2e_ms_per_step": round(e2e_ms / args.steps, 3), "gpu_launches": int(launches),
+            "list_resizes_timed": int(resizes),
+            # GsrCamera (200 B) per one-view call, GsrSplatCamera (108 B) per view of a batched call
+            "h2d_bytes_per_step": int(frames.views_per_step * (200 if frames.d == 1 else 108)),
+            "d2h_bytes_per_step": int(d2h),
+            "clocks": clocks}
+
+
+def pass_profile(r, frames: Frames, stream_obj, n: int = 20) -> tuple[dict, object]:
+    """Per-pass device times (CUDA events between the passes, graphs off for these frames)."""
+    stream = stream_obj.cuda_stream
+    r.set_timing(True)
+    passes = {}
+    for k in range(n):
+        render_call(r, frames, k, stream)
+        stream_obj.synchronize()
+        for name, t in r.pass_times().items():
+            passes[name] = passes.get(name, 0.0) + t / n
+    r.set_timing(False)
+    return {k: round(v, 4) for k, v in passes.items()}, r.read_control()
+
+
+def roofline(passes: dict, ctl, fmt: str, n: int, tiles: int, peak: float, peak_kind: str) -> dict:
+    b = pass_bytes(fmt, ctl, n, tiles)
+    kernels, tot_b, tot_ms = {}, 0.0, 0.0
+    for k, nb in b.items():
+        ms = passes.get(PASS_NAMES[k])
+        if not ms:
+            continue
+        gbs = nb / (ms * 1e-3) / 1e9
+        kernels[k] = {"bytes": int(nb), "ms": ms, "GB/s": round(gbs, 1), "frac": round(gbs / peak, 4)}
+        tot_b += nb
+        tot_ms += ms
+    achieved = tot_b / (tot_ms * 1e-3) / 1e9 if tot_ms else 0.0
+    return {"bound": "hbm", "kernel": "preprocess + sort (preprocess, depth sort, scan + emission, tile sort, "
+                                      "ranges), plain form, one 1080p frame",
+            "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+            "peak_kind": peak_kind, "algorithmic_bytes": int(tot_b), "ms": round(tot_ms, 4), "kernels": kernels}
+
+
+def render_issue(passes: dict, clocks: dict, instructions: float | None):
+    ms = passes.get("render tiles")
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
+    if not ms or not mhz or not instructions:
+        return None
+    achieved = instructions / (ms * 1e-3) / 1e12
+    peak = 148 * 4 * mhz * 1e6 / 1e12
+    return {"bound": "issue", "achieved": round(achieved, 4), "peak": round(peak, 4), "unit": "T warp-instr/s",
+            "frac": round(achieved / peak, 4), "instructions_source": "ncu smsp__inst_issued.sum of one frame"}
+
+
+# warp instructions of one plain 1080p render pass, from an ncu capture of this build
+RENDER_WARP_INSTRUCTIONS_1080P = 228.0e6
+
+
+def settle_and_tune(G, gs, cams, args, model=None, depths=(1, 2, 4, 8, 16), tile_sizes=None, probe=32):
+    """The autotuner's pick (views per frame, raster schedule, tile size) on the first `probe`
+    cameras; --batch fixes the views per frame instead."""
+    if args.batch > 0:
+        return {"views_per_frame": args.batch, "raster_schedule": "auto", "tile_size": 16, "table": None}
+    sel = [cams[k % len(cams)] for k in range(max(probe, max(depths)))]
+    st = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.budget_mb, use_graph=True)
+    return G.autotune(gs, st, G.camera_array(sel), depths=depths, frames=3, model=model, tile_sizes=tile_sizes)
+
+
+def renderer_for(G, gs, args, tuned=None, model=None):
+    t = tuned or {}
+    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.budget_mb,
+                                  raster_schedule=t.get("raster_schedule", "auto"), tile_size=t.get("tile_size", 16),
+                                  use_graph=True))
+    if model is not None:
+        r.set_color_model(model)
+    return r
+
+
+def frame_images(r, frames: Frames, stream_obj, k: int = 0) -> list:
+    """The RGB8 images of call k's views."""
+    render_call(r, frames, k, stream_obj.cuda_stream)
+    stream_obj.synchronize()
+    if frames.d == 1:
+        return [r.read_back_image(rgb8=True)[1]]
+    return [r.read_view_image(j, rgb8=True)[1] for j in range(frames.d)]
+
+
+def min_psnr8(a: list, b: list) -> float:
+    return min(psnr(x, y, 255.0) for x, y in zip(a, b))
+
+
+# ---- the workloads --------------------------------------------------------------------------------
+def run_1080p(G, args, dist, sampler, stream_obj, peak):
+    """plain_1080p (plain and batched forms) and learned_1080p (gated and forced decode)."""
+    scene, cams, fmt, layout, thr = workload("plain_1080p")
+    first = (dist.rank * 37) % len(cams)
+    order = [(first + k) % len(cams) for k in range(len(cams))]
+    gs = G.GpuScene(scene, fmt, layout)
+    out = {}
+    # plain form: one view per frame, gsr_render
+    plain_frames = Frames(G, cams, 1, order)
+    r = renderer_for(G, gs, args)
+    plain = time_form(r, plain_frames, args, dist, sampler, stream_obj)
+    passes, ctl = pass_profile(r, plain_frames, stream_obj)
+    tiles = ((1920 + 15) // 16) * ((1080 + 15) // 16)
+    roof = roofline(passes, ctl, fmt, scene.count, tiles, peak[0], peak[1])
+    roof["traffic"] = int(TRAFFIC_PLAIN_1080P_CAPTURE)
+    roof["traffic_kind"] = "from_capture"
+    plain.update({"passes_ms": passes, "frame": {"visible": ctl.visible, "entries": ctl.entries,
+                                                 "duplicates": ctl.duplicates, "overflow": ctl.overflow,
+                                                 "sort_passes": ctl.sort_passes, "key_bits": ctl.key_bits}})
+    r.close()
+    # batched form: the autotuner's views per frame and schedule
+    tuned = settle_and_tune(G, gs, [cams[v] for v in order], args)
+    bframes = Frames(G, cams, tuned["views_per_frame"], order)
+    rb = renderer_for(G, gs, args, tuned)
+    batched = time_form(rb, bframes, args, dist, sampler, stream_obj)
+    bimgs = frame_images(rb, bframes, stream_obj)
+    rp = renderer_for(G, gs, args)
+    pimgs = [frame_images(rp, Frames(G, cams, 1, [order[j]]), stream_obj)[0] for j in range(bframes.d)]
+    rp.close()
+    batched.update({"raster": tuned["raster_schedule"], "autotune": tuned["table"],
+                    "images_identical_to_plain": all(np.array_equal(a, b) for a, b in zip(bimgs, pimgs))})
+    rb.close()
+    out["plain_1080p"] = {"plain": plain, "batched": batched}
+    # parity of view 0 against the oracle (list bit for bit, images against renderReference)
+    leg = cpu_leg(args, dist)
+    if leg:
+        out["plain_1080p"]["parity"] = leg.check_view(G, gs, scene, cams[order[0]], stream_obj.cuda_stream)
+    # learned colour: the configs' recipe, gated at 2/255, then the same training forced on
+    learned = {}
+    for label, gate in (("gated", 2.0 / 255.0), ("forced", 1e30)):
+        model = G.ColorModel(gs, steps=args.mlp_steps, batch=65536, directions=64, seed=1, gate=gate)
+        stats = model.stats()
+        rl = renderer_for(G, gs, args, tuned, model)
+        form = time_form(rl, bframes, args, dist, sampler, stream_obj)
+        limgs = frame_images(rl, bframes, stream_obj)
+        form["psnr_vs_plain_sh_db"] = min_psnr8(limgs, bimgs)
+        form["images_identical_to_plain"] = all(np.array_equal(a, b) for a, b in zip(limgs, bimgs))
+        # the preprocess time the decode adds (pass times of a one-view frame)
+        r1 = renderer_for(G, gs, args, None, model)
+        lp, _ = pass_profile(r1, plain_frames, stream_obj)
+        r1.close()
+        form["passes_ms_one_view"] = lp
+        form["gate"] = "2/255" if label == "gated" else "off (decode forced for every gaussian)"
+        form["color_model"] = {k: (round(v, 6) if isinstance(v, float) else v) for k, v in stats.items()}
+        form["fallback_share"] = round(stats["fallback"] / max(stats["gaussians"], 1), 4)
+        rl.close()
+        model.close()
+        learned[label] = form
+    out["learned_1080p"] = learned
+    gs.close()
+    return out, scene, cams, order, roof
+
+
+def run_1080p_f16(G, args, dist, sampler, stream_obj, tuned_depth: int, raster: str):
+    scene, cams, fmt, layout, thr = workload("plain_1080p_f16")
+    first = (dist.rank * 37) % len(cams)
+    order = [(first + k) % len(cams) for k in range(len(cams))]
+    gs = G.GpuScene(scene, fmt, layout, 3, thr)
+    r = renderer_for(G, gs, args)
+    plain_frames = Frames(G, cams, 1, order)
+    plain = time_form(r, plain_frames, args, dist, sampler, stream_obj)
+    passes, ctl = pass_profile(r, plain_frames, stream_obj)
+    plain["passes_ms"] = passes
+    r.close()
+    tuned = {"views_per_frame": tuned_depth, "raster_schedule": raster}
+    rb = renderer_for(G, gs, args, tuned)
+    batched = time_form(rb, Frames(G, cams, tuned_depth, order), args, dist, sampler, stream_obj)
+    rb.close()
+    out = {"plain": plain, "batched": batched}
+    leg = cpu_leg(args, dist)
+    if leg:
+        out["parity"] = leg.check_view(G, gs, leg.decoded(scene, fmt, layout, thr), cams[order[0]],
+                                       stream_obj.cuda_stream)
+    gs.close()
+    return out
+
+
+def sharded(cams, dist) -> list[int]:
+    parts = partition_views([c.width * c.height for c in cams], dist.world)
+    return parts[dist.rank]
+
+
+def view_checksums(r, frames: Frames, stream_obj) -> list[float]:
+    """Per-view checksums of one step's RGB8 images (the per-view results gathered on rank 0)."""
+    sums = []
+    for k in range(len(frames.calls)):
+        for img in frame_images(r, frames, stream_obj, k):
+            sums.append(float(img.astype(np.uint64).sum()) + 1.0)
+    return sums[:len(frames.views)]
+
+
+def run_batched_64(G, args, dist, sampler, stream_obj):
+    """the 64 views one by one on the plain path (one renderer per resolution, so
+    no view changes a renderer's layout) against all of them in one frame."""
+    scene, cams, fmt, layout, thr = workload("batched_64")
+    mine = sharded(cams, dist)
+    gs = G.GpuScene(scene, fmt, layout)
+    out = {"views": len(cams), "views_this_rank": len(mine)}
+    # one by one: per resolution a renderer; a step renders every view of this rank once
+    import torch
+
+    by_res = {}
+    for v in mine:
+        by_res.setdefault((cams[v].width, cams[v].height), []).append(v)
+    rs = {res: renderer_for(G, gs, args) for res in by_res}
+    stream = stream_obj.cuda_stream
+    ccams = {v: G.to_c_camera(cams[v]) for v in mine}
+    for _ in range(max(args.warmup, 3)):
+        for v in mine:
+            rs[(cams[v].width, cams[v].height)].render(ccams[v], stream)
+    stream_obj.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize()
+    with sampler:
+        e0.record(stream_obj)
+        for _ in range(args.steps):
+            for v in mine:
+                rs[(cams[v].width, cams[v].height)].render(ccams[v], stream)
+        e1.record(stream_obj)
+        e1.synchronize()
+    ms = dist.max(e0.elapsed_time(e1))
+    one_by_one = {"views_per_s": round(len(cams) * args.steps / (ms / 1e3), 3), "ms_per_step": round(ms / args.steps, 3),
+                  "views_timed": len(cams) * args.steps, "clocks": sampler.summary()}
+    plain_imgs = {}
+    for v in mine:
+        rr = rs[(cams[v].width, cams[v].height)]
+        rr.render(ccams[v], stream)
+        stream_obj.synchronize()
+        plain_imgs[v] = rr.read_back_image(rgb8=True)[1]
+    for rr in rs.values():
+        rr.close()
+    # batched: this rank's views in one frame; tile size and schedule autotuned
+    d = len(mine)
+    tuned = settle_and_tune(G, gs, [cams[v] for v in mine], args, depths=(d,), tile_sizes=(16, 8), probe=d)
+    rb = renderer_for(G, gs, args, tuned)
+    bframes = Frames(G, cams, d, mine)
+    batched = time_form(rb, bframes, args, dist, sampler, stream_obj)
+    bimgs = frame_images(rb, bframes, stream_obj)
+    same = all(np.array_equal(bimgs[j], plain_imgs[v]) for j, v in enumerate(mine))
+    sums = dist.gather_view_results(mine, view_checksums(rb, bframes, stream_obj), len(cams))
+    rb.close()
+    batched.update({"tile_size": tuned["tile_size"], "raster": tuned["raster_schedule"], "autotune": tuned["table"],
+                    "images_identical_to_one_by_one": bool(same),
+                    "psnr_vs_one_by_one_db": min(psnr(bimgs[j], plain_imgs[v], 255.0) for j, v in enumerate(mine)),
+                    "views_gathered": int(np.count_nonzero(sums))})
+    out.update({"one_by_one": one_by_one, "batched": batched,
+                "speedup_vs_one_by_one": round(batched["views_per_s"] / one_by_one["views_per_s"], 4)})
+    leg = cpu_leg(args, dist)
+    if leg:  # one view of each resolution
+        seen, par = set(), []
+        for v in range(len(cams)):
+            res = (cams[v].width, cams[v].height)
+            if res not in seen:
+                seen.add(res)
+                par.append(leg.check_view(G, gs, scene, cams[v], stream))
+        out["parity"] = par
+    gs.close()
+    return out
+
+
+def run_scale_4k(G, args, dist, sampler, stream_obj, base_mem: int):
+    """16 4K views of 6M gaussians (fp16, per-gaussian degree), one by one and
+    batched, plain SH and learned colour with SH fallback; peak device memory."""
+    scene, cams, fmt, layout, thr = workload("scale_4k")
+    mine = sharded(cams, dist)
+    mem = [sampler.memory_used()]
+    gs = G.GpuScene(scene, fmt, layout, 3, thr)
+    mem.append(sampler.memory_used())
+    out = {"views": len(cams), "views_this_rank": len(mine), "scene_bytes": int(sum(gs.desc.buffer_bytes))}
+    r = renderer_for(G, gs, args)
+    plain_frames = Frames(G, cams, 1, mine)
+    plain = time_form(r, plain_frames, args, dist, sampler, stream_obj)
+    passes, ctl = pass_profile(r, plain_frames, stream_obj, n=4)
+    plain["passes_ms"] = passes
+    plain["frame"] = {"visible": ctl.visible, "entries": ctl.entries, "overflow": ctl.overflow}
+    plain_imgs = [frame_images(r, Frames(G, cams, 1, [v]), stream_obj)[0] for v in mine]
+    mem.append(sampler.memory_used())
+    r.close()
+    depths = tuple(x for x in (2, 4, 8, 16) if x <= len(mine)) or (len(mine),)
+    tuned = settle_and_tune(G, gs, [cams[v] for v in mine], args, depths=depths, probe=len(mine))
+    rb = renderer_for(G, gs, args, tuned)
+    bframes = Frames(G, cams, tuned["views_per_frame"], mine)
+    batched = time_form(rb, bframes, args, dist, sampler, stream_obj)
+    mem.append(max(sampler.memory_used(), sampler.mem_peak))
+    bimgs = frame_images(rb, bframes, stream_obj)
+    batched.update({"raster": tuned["raster_schedule"], "autotune": tuned["table"],
+                    "images_identical_to_plain": all(np.array_equal(a, b) for a, b in zip(bimgs, plain_imgs))})
+    rb.close()
+    model = G.ColorModel(gs, steps=args.mlp_steps, batch=65536, directions=64, seed=1, gate=2.0 / 255.0)
+    stats = model.stats()
+    rl = renderer_for(G, gs, args, tuned, model)
+    learned = time_form(rl, bframes, args, dist, sampler, stream_obj)
+    mem.append(max(sampler.memory_used(), sampler.mem_peak))
+    limgs = frame_images(rl, bframes, stream_obj)
+    sums = dist.gather_view_results(mine, view_checksums(rl, bframes, stream_obj), len(cams))
+    learned.update({"psnr_vs_plain_sh_db": min_psnr8(limgs, bimgs),
+                    "color_model": {k: (round(v, 6) if isinstance(v, float) else v) for k, v in stats.items()},
+                    "fallback_share": round(stats["fallback"] / max(stats["gaussians"], 1), 4),
+                    "views_gathered": int(np.count_nonzero(sums))})
+    rl.close()
+    model.close()
+    out.update({"plain": plain, "batched": batched, "batched+mlp": learned,
+                "peak_hbm_bytes": int(max(mem) - base_mem), "peak_hbm_note":
+                "device memory in use (NVML) above the level before the scene upload, sampled between "
+                "and during the forms"})
+    leg = cpu_leg(args, dist)
+    if leg:
+        out["parity"] = leg.check_view(G, gs, leg.decoded(scene, fmt, layout, thr), cams[0], stream_obj.cuda_stream)
+    gs.close()
+    return out
+
+
+def run_720p(G, args, dist, sampler, stream_obj):
+    scene, cams, fmt, layout, thr = workload("plain_720p")
+    gs = G.GpuScene(scene, fmt, layout)
+    r = renderer_for(G, gs, args)
+    a = argparse.Namespace(**vars(args))
+    a.steps = max(args.steps, 1) * 30  # one view a step: 30 per outer step keep the timed region measurable
+    plain = time_form(r, Frames(G, cams, 1), a, dist, sampler, stream_obj)
+    r.close()
+    out = {"plain": plain}
+    leg = cpu_leg(args, dist)
+    if leg:
+        out["parity"] = leg.check_view(G, gs, scene, cams[0], stream_obj.cuda_stream)
+    gs.close()
+    return out
+
+
+def check_launch(args, dist: Dist):
+    """The distributed plumbing alone, without a GPU: every rank takes its part of batched_64's
+    views, reports per-view results for them, and rank 0 prints what was gathered."""
+    from gsr_b200 import scenes
+
+    cams = scenes.batched_cameras(64, seed=2)
+    mine = sharded(cams, dist)
+    dist.barrier()
+    got = dist.gather_view_results(mine, [float(v + 1) for v in mine], len(cams))
+    slowest = dist.max(float(dist.rank))
+    views = dist.sum(len(mine))
+    if dist.rank == 0:
+        print(json.dumps({"check": "launch", "n_gpus": dist.world, "views": int(views),
+                          "views_gathered": int(np.count_nonzero(got)),
+                          "gathered_in_order": bool(np.array_equal(got, np.arange(1, 65, dtype=np.float64))),
+                          "max_rank": slowest}), flush=True)
+
+
+# ---- the reference arm ------------------------------------------------------------------------
 def run_reference_arm(args):
     # under torchrun only rank 0 runs the CPU reference; the other ranks exit without work
     if int(os.environ.get("RANK", "0")) != 0:
         return
-    scene, cams, fmt, layout = make_config(args.config)
-    budget = 90.0
-    res = cpu_reference_run(scene, cams, max_frames=max(1, args.steps), time_budget_s=budget, warmup=min(args.warmup, 1))
+    scene, cams, fmt, layout, thr = workload("plain_1080p")
+    # a step = one view of the orbit (evenly spaced); warm-up 1 view
+    res = CpuLeg().baseline(scene, cams, max_frames=max(1, args.steps), time_budget_s=150.0, warmup=1)
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(res["value"], 4), "unit": UNIT, "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": res["value"], "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.config, "gaussians": scene.count, "resolution": "1920x1080",
-                   "scene_format": fmt, "bounds": "tight", "form": "plain"},
+        "config": {"workload": "plain_1080p", "gaussians": scene.count, "resolution": "1920x1080",
+                   "scene_format": fmt, "bounds": "tight", "form": "plain (renderReference)",
+                   "step": "one view of the 300-view orbit"},
         "cpu_baseline": res,
-        "e2e": {"value": round(res["value"], 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
 
-# ---- the B200 arm -----------------------------------------------------------------------
+# ---- the B200 arm ---------------------------------------------------------------------------------
 def run_b200(args, dist: Dist):
     import torch
 
@@ -277,278 +892,100 @@ def run_b200(args, dist: Dist):
 
     torch.cuda.set_device(dist.local_rank)
     dev = torch.device("cuda", dist.local_rank)
-    scene, cams, fmt, layout = make_config(args.config)
-    gs = G.GpuScene(scene, fmt, layout)
-    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, list_mode=args.list_mode,
-                                  render_splat=args.render_splat, sort_window=args.sort_window,
-                                  tile_size=args.tile_size, use_graph=args.use_graph))
-    stream = torch.cuda.Stream(device=dev)
-    sptr = stream.cuda_stream
-    first = (dist.rank * 37) % len(cams)
-    c_cams = [G.to_c_camera(c) for c in cams]  # the GsrCamera structs a host application passes
-    scam = lambda k: c_cams[(first + k) % len(cams)]  # noqa: E731
+    stream_obj = torch.cuda.Stream(device=dev)
+    sampler = Sampler(dist.local_rank)
+    base_mem = sampler.memory_used()
+    peak = load_peaks()
+    which = WORKLOADS if args.config == "all" else (args.config,)
+    configs = {}
+    t_start = time.perf_counter()
+    head_roof, scene, cams, order = None, None, None, None
+    tuned_depth, raster = 8, "per-tile"
+    if any(w in which for w in ("plain_1080p", "learned_1080p")):
+        res, scene, cams, order, head_roof = run_1080p(G, args, dist, sampler, stream_obj, peak)
+        configs.update(res)
+        tuned_depth = res["plain_1080p"]["batched"]["views_per_frame"]
+        raster = res["plain_1080p"]["batched"]["raster"]
+    if "plain_1080p_f16" in which:
+        configs["plain_1080p_f16"] = run_1080p_f16(G, args, dist, sampler, stream_obj, tuned_depth, raster)
+    if "batched_64" in which:
+        configs["batched_64"] = run_batched_64(G, args, dist, sampler, stream_obj)
+    if "scale_4k" in which:
+        configs["scale_4k"] = run_scale_4k(G, args, dist, sampler, stream_obj, base_mem)
+    if "plain_720p" in which:
+        configs["plain_720p"] = run_720p(G, args, dist, sampler, stream_obj)
 
-    # warm-up (also lets the adaptive list settle)
-    with torch.cuda.stream(stream):
-        for k in range(args.warmup):
-            r.render(scam(k), sptr)
-    stream.synchronize()
-
-    # device-resident timed region
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = r.kernel_launches()
-    dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(dist.local_rank) as clocks:
-        start.record(stream)
-        for k in range(args.steps):
-            r.render(scam(args.warmup + k), sptr)
-        end.record(stream)
-        end.synchronize()
-    torch.cuda.synchronize()
-    dist.barrier()
-    ms = start.elapsed_time(end)
-    launches = r.kernel_launches() - launches0
-    ms_max = dist.max(ms)
-    value = dist.world * args.steps / (ms_max / 1e3)
-
-    # end to end through gsr_render_to_host (camera in, RGB8 image out, synchronized)
-    img = torch.empty((1080, 1920, 3), dtype=torch.uint8).pin_memory() if args.config.startswith("plain_1080p") else \
-        torch.empty((cams[0].height, cams[0].width, 3), dtype=torch.uint8).pin_memory()
-    out = img.numpy()
-    for k in range(min(args.warmup, 5)):
-        r.render_to_host(scam(k), out, sptr)
-    dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t0 = time.perf_counter()
-    e0.record(stream)
-    for k in range(args.steps):
-        r.render_to_host(scam(args.warmup + k), out, sptr)
-    e1.record(stream)
-    e1.synchronize()
-    wall = time.perf_counter() - t0
-    e2e_ms = max(e0.elapsed_time(e1), wall * 1e3)
-    e2e_ms = dist.max(e2e_ms)
-    e2e_value = dist.world * args.steps / (e2e_ms / 1e3)
-
-    # per-pass times (CUDA events between the kernels, a separate run) and the roofline
-    r.set_timing(True)
-    passes = {}
-    nt = 20
-    for k in range(nt):
-        r.render(scam(k), sptr)
-        stream.synchronize()
-        for name, t in r.pass_times().items():
-            passes[name] = passes.get(name, 0.0) + t / nt
-    r.set_timing(False)
-    ctl = r.read_control()
-    capacity = r.capacity()[0]
-    peak, peak_kind = load_peaks()
-    fb = front_bytes(fmt, ctl, scene.count, args.list_mode)
-    if args.list_mode == "binning":
-        front_ms = sum(passes.get(k, float("nan")) for k in
-                       ("reset + preprocess (depth keys)", "depth sort (total)", "scan + duplicate (depth order)"))
-    else:
-        front_ms = passes.get("reset + preprocess + scan + duplicate", float("nan"))
-    sort_ms = passes.get("tile sort (total)", float("nan"))
-    achieved = fb / (front_ms * 1e-3) / 1e9
-    sb = sort_bytes(ctl)
-
-    if args.plain_only:  # profiling runs: the plain form alone
-        if dist.rank == 0:
-            print(json.dumps({"metric": METRIC, "value": round(value, 3), "unit": UNIT, "form": "plain only",
-                              "passes_ms": passes}), flush=True)
-        r.close()
-        gs.close()
-        return
-    # the batched form: D consecutive views of the orbit per frame (one sort over all of them)
-    batched = run_batched(args, dist, G, gs, cams, first, stream, r)
-    plain = {"views_per_s": round(value, 3), "e2e_views_per_s": round(e2e_value, 3),
-             "ms_per_view": round(ms_max / args.steps, 4), "gpu_launches": int(launches)}
-    # the batched + learned colour form: the colour model trained on this scene (2000 Adam steps of
-    # 65,536 (gaussian, direction) pairs, 64 directions per gaussian, seed 1, 2/255 gate)
-    learned, model_stats = None, None
-    if not args.no_mlp:
-        model = G.ColorModel(gs, steps=args.mlp_steps, batch=65536, directions=64, seed=1, gate=2.0 / 255.0)
-        model_stats = model.stats()
-        learned = run_batched(args, dist, G, gs, cams, first, stream, r, model=model)
-        model.close()
-    head = learned or batched
-    best = head
-    form = (f"batched ({head['views_per_frame']} views per frame) + learned colour (fp16 latent, BF16 MLP, "
-            f"{model_stats['fallback'] / model_stats['gaussians']:.1%} SH fallback)" if learned
-            else f"batched ({head['views_per_frame']} views per frame, SH colour)")
+    if "learned_1080p" in configs:
+        head = configs["learned_1080p"]["gated"]
+        form = (f"batched ({head['views_per_frame']} views per frame) + learned colour (fp16 latent, BF16 MLP, "
+                f"{head['fallback_share']:.1%} SH fallback at the 2/255 gate)")
+        workload_name = "learned_1080p"
+    else:  # a single workload: its main form
+        c = configs[which[0]]
+        head = c.get("batched") or c.get("plain")
+        form = f"{which[0]}: {'batched' if 'batched' in c else 'plain'}"
+        workload_name = which[0]
     line = {
-        "metric": METRIC, "value": round(best["views_per_s"], 3), "unit": UNIT, "n_gpus": dist.world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(best["ms_per_view"], 4),
+        "metric": METRIC, "value": head["views_per_s"], "unit": UNIT, "n_gpus": dist.world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": args.config, "gaussians": scene.count, "resolution": f"{cams[0].width}x{cams[0].height}",
-                   "scene_format": f"{fmt}/{layout}", "bounds": "tight", "list": "adaptive", "sort": SORT_FORMS[args.list_mode],
-                   "form": form, "step": "one view", "views": "300-frame orbit r=14 h=2",
-                   "l2": "inputs larger than L2 (scene 298 MB fp32), no flush",
-                   "cuda_graph": bool(args.use_graph),
-                   "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "1 GPU"},
-        "forms": {"plain": plain, "batched": {k: v for k, v in batched.items() if k != "clocks"},
-                  "batched+mlp": ({k: v for k, v in learned.items() if k != "clocks"} if learned else None)},
-        "color_model": ({k: (round(v, 6) if isinstance(v, float) else v) for k, v in model_stats.items()}
-                        if model_stats else None),
-        "speedup_vs_plain": round(best["views_per_s"] / value, 4),
-        "e2e": {"value": round(best["e2e_views_per_s"], 3), "unit": UNIT, "h2d_bytes_per_step": 200,
-                "d2h_bytes_per_step": int(out.nbytes)},
-        "gpu_launches": int(best["gpu_launches"]),
-        "roofline": {"bound": "hbm", "kernel": "front (preprocess+count+scan+emit), plain form",
-                     "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "traffic": (int(FRONT_TRAFFIC_PLAIN_1080P[args.list_mode])
-                                 if args.config == "plain_1080p" and FRONT_TRAFFIC_PLAIN_1080P[args.list_mode] else None),
-                     "traffic_source": "ncu dram__bytes_read+write, one frame (profiles/kernels_plain_1080p.md)",
-                     "peak_kind": peak_kind, "algorithmic_bytes": int(fb)},
-        "passes_ms": {k: round(v, 4) for k, v in passes.items()},
-        # the rasterizer (41 % of the frame) is bound by instruction issue, not by HBM or the
-        # tensor cores: its warp instructions per 1080p frame (ncu, profiles/) over its live
-        # pass time, against 148 SMs x 4 schedulers x the SM clock seen under load
-        "render_issue": render_issue(passes, clocks.summary(), args.config),
-        "sort": {"bytes": int(sb), "ms": round(sort_ms, 4), "GB/s": round(sb / (sort_ms * 1e-3) / 1e9, 1),
-                 "passes": ctl.sort_passes, "key_bits": ctl.key_bits},
-        "frame": {"visible": ctl.visible, "entries": ctl.entries, "duplicates": ctl.duplicates,
-                  "overflow": ctl.overflow, "capacity": capacity},
-        "clocks": best["clocks"],
-        "clocks_plain": clocks.summary(),
+        "config": {"workload": workload_name, "gaussians": 1_240_000, "resolution": "1920x1080",
+                   "scene_format": "f32/soa", "bounds": "tight", "list": "adaptive, binning (depth sort + tile sort)",
+                   "form": form, "step": "one pass over the 300-view orbit (r=14, h=2)",
+                   "l2": "inputs larger than L2 (scene 298 MB), no flush", "cuda_graph": True,
+                   "parallelism": f"replicas x{dist.world} (orbit workloads); views split by pixel count "
+                                  f"(batched_64, scale_4k)" if dist.world > 1 else "1 GPU"},
+        "views_timed": head["views_timed"],
+        "e2e": {"value": head["e2e_views_per_s"], "unit": UNIT, "h2d_bytes_per_step": head["h2d_bytes_per_step"],
+                "d2h_bytes_per_step": head["d2h_bytes_per_step"]},
+        "gpu_launches": head["gpu_launches"],
+        "clocks": head["clocks"],
     }
-    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_reference_run(scene, cams, max_frames=args.cpu_frames, time_budget_s=30.0)
+    if "plain_1080p" in configs:
+        plain = configs["plain_1080p"]["plain"]
+        line["speedup_vs_plain"] = round(head["views_per_s"] / plain["views_per_s"], 4)
+        line["roofline"] = head_roof
+        line["render_issue"] = render_issue(plain["passes_ms"], plain["clocks"], RENDER_WARP_INSTRUCTIONS_1080P)
+        line["parity"] = configs["plain_1080p"].get("parity")
+    line["configs"] = configs
+    leg = cpu_leg(args, dist)
+    if leg and dist.world == 1 and scene is not None:
+        line["cpu_baseline"] = leg.baseline(scene, [cams[v] for v in order], max_frames=args.cpu_frames,
+                                            time_budget_s=30.0)
+    line["wall_s"] = round(time.perf_counter() - t_start, 1)
     if dist.rank == 0:
         print(json.dumps(line), flush=True)
-    r.close()
-    gs.close()
-
-
-def tune(args, G, gs, cams, first: int, model=None):
-    """views per frame and rasterizer schedule: --batch, or the autotuner's pick on 32 orbit views."""
-    if args.batch > 0:
-        return {"views_per_frame": args.batch, "raster_schedule": "auto", "table": None}
-    probe = G.camera_array([cams[(first + k) % len(cams)] for k in range(32)])
-    settings = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
-                          list_mode=args.list_mode, render_splat=args.render_splat, sort_window=args.sort_window,
-                          tile_size=args.tile_size, use_graph=args.use_graph)
-    return G.autotune(gs, settings, probe, depths=(1, 2, 4, 8, 16), frames=4, model=model)
-
-
-def run_batched(args, dist: Dist, G, gs, cams, first: int, stream, plain_renderer, model=None):
-    """The batched form on the same scene and orbit: frames of D consecutive views; a step is
-    still one view. Checks each view of one frame against the plain render of the same camera
-    (PSNR of the 8-bit images; equal images give inf)."""
-    import torch
-
-    tuned = tune(args, G, gs, cams, first, model)
-    d = tuned["views_per_frame"]
-    nviews = len(cams)
-    sptr = stream.cuda_stream
-    frames = [G.camera_array([cams[(first + k * d + j) % nviews] for j in range(d)]) for k in range(nviews // d + 1)]
-    nframes = len(frames)
-    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.batch_budget_mb,
-                                  raster_schedule=tuned["raster_schedule"], list_mode=args.list_mode,
-                                  render_splat=args.render_splat, sort_window=args.sort_window,
-                                  tile_size=args.tile_size, use_graph=args.use_graph))
-    if model is not None:
-        r.set_color_model(model)
-    # warm-up: at least the requested views, then until the adaptive list keeps its capacity for
-    # three frames (its statistics arrive two frames late), so that no list re-allocation falls
-    # into the timed region
-    with torch.cuda.stream(stream):
-        stable, last, k = 0, -1, 0
-        while k < 64 and (k * d < args.warmup or stable < 3):
-            r.render_views(frames[k % nframes], sptr)
-            stream.synchronize()
-            cap = r.capacity()[0]
-            stable, last, k = (stable + 1 if cap == last else 0), cap, k + 1
-    stream.synchronize()
-    steps = max(1, args.steps // d)
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches0 = r.kernel_launches()
-    dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(dist.local_rank) as clocks:
-        start.record(stream)
-        for k in range(steps):
-            r.render_views(frames[k % nframes], sptr)
-        end.record(stream)
-        end.synchronize()
-    torch.cuda.synchronize()
-    dist.barrier()
-    ms = dist.max(start.elapsed_time(end))
-    launches = r.kernel_launches() - launches0
-    value = dist.world * steps * d / (ms / 1e3)
-    # end to end: cameras from host memory, every view's RGB8 image into pinned host memory
-    total_px = sum(c.width * c.height for c in frames[0])
-    host = torch.empty((total_px * 3,), dtype=torch.uint8).pin_memory().numpy()
-    for k in range(3):
-        r.render_views_to_host(frames[k % nframes], host, sptr)
-    dist.barrier()
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    t0 = time.perf_counter()
-    e0.record(stream)
-    for k in range(steps):
-        r.render_views_to_host(frames[k % nframes], host, sptr)
-    e1.record(stream)
-    e1.synchronize()
-    e2e_ms = dist.max(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3))
-    # image check of one frame against the plain renders of its views
-    r.render_views(frames[0], sptr)
-    stream.synchronize()
-    psnrs = []
-    for j in range(d):
-        got = r.read_view_image(j, rgb8=True)[1].astype(np.float64)
-        plain_renderer.render(frames[0][j], sptr)
-        stream.synchronize()
-        ref = plain_renderer.read_back_image(rgb8=True)[1].astype(np.float64)
-        mse = float(np.mean((got - ref) ** 2))
-        psnrs.append(float("inf") if mse == 0 else 10 * math.log10(255.0 ** 2 / mse))
-    ctl = r.read_control()
-    out = {"views_per_frame": d, "views_per_s": value, "e2e_views_per_s": dist.world * steps * d / (e2e_ms / 1e3),
-           "ms_per_view": ms / (steps * d), "ms_per_frame": ms / steps, "gpu_launches": int(launches),
-           "psnr_vs_plain_db": None if math.isinf(min(psnrs)) else round(min(psnrs), 2),
-           "images_identical_to_plain": bool(math.isinf(min(psnrs))),
-           "entries_per_frame": ctl.entries, "sort_passes": ctl.sort_passes,
-           "packed_entries": ctl.packed_entries, "raster": tuned["raster_schedule"], "autotune": tuned["table"],
-           "colour": "learned (MLP, SH fallback)" if model is not None else "SH",
-           "clocks": clocks.summary()}
-    r.close()
-    return out
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
-    ap.add_argument("--warmup", type=int, default=35)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--config", default="plain_1080p")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--config", default="all", choices=["all", *WORKLOADS])
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU leg (the baseline and the checks of the GPU views; profiling runs)")
     ap.add_argument("--cpu-frames", type=int, default=10)
     ap.add_argument("--batch", type=int, default=0, help="views per frame of the batched forms (0: autotuned)")
-    ap.add_argument("--batch-budget-mb", type=int, default=8192)
-    ap.add_argument("--no-mlp", action="store_true", help="skip the batched + learned colour form")
-    ap.add_argument("--plain-only", action="store_true", help="the plain form only (profiling runs)")
+    ap.add_argument("--budget-mb", type=int, default=16384)
     ap.add_argument("--mlp-steps", type=int, default=2000)
-    ap.add_argument("--use-graph", type=int, default=1, choices=[0, 1],
-                    help="1 (default): each frame launched as one captured CUDA graph (GsrSettings.use_graph)")
-    ap.add_argument("--list-mode", default="binning", choices=["binning", "global"],
-                    help="list construction: one (tile, depth) sort, or depth sort + emission + tile sort")
-    ap.add_argument("--render-splat", default="full", choices=["full", "p32", "p24"],
-                    help="the per-entry record of emission and render: 48 B, or packed 32 / 24 B")
-    ap.add_argument("--sort-window", type=int, default=0, help="StopThePop per-pixel window K (0: off)")
-    ap.add_argument("--tile-size", type=int, default=16, choices=[8, 16], help="binning / render tile in pixels")
+    ap.add_argument("--check-launch", action="store_true",
+                    help="plumbing self-check: ranks, view partition and gather, no GPU work, no timing")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be >= 3")
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        raise SystemExit(launch_ranks(sys.argv[1:], args.gpus))
     if args.impl == "reference":
         run_reference_arm(args)
         return
-    dist = Dist(os.environ.get("GSR_BENCH_BACKEND", "nccl"))
+    dist = Dist(os.environ.get("GSR_BENCH_BACKEND", "gloo" if args.check_launch else "nccl"))
     try:
-        run_b200(args, dist)
+        if args.check_launch:
+            check_launch(args, dist)
+        else:
+            run_b200(args, dist)
     finally:
         dist.close()
 

@@ -1260,6 +1260,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
         return fail(GSR_ERROR_INVALID_ARGUMENT, "render splat mode %u", settings->render_splat);
     if (settings->raster_schedule > GSR_RASTER_PERSISTENT)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "raster schedule %u", settings->raster_schedule);
+    if (settings->sort_digit_bits != 0 && settings->sort_digit_bits != 8)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "sort digit bits %u (8)", settings->sort_digit_bits);
     GSR_CUDA(r->control.alloc(sizeof(DeviceControl)));
     GSR_CUDA(cudaMemset(r->control.p, 0, sizeof(DeviceControl)));
     GSR_CUDA(r->plan.alloc(sizeof(SortPlan)));
@@ -1738,68 +1740,98 @@ void gsr_color_model_destroy(GsrColorModel* model) {
 }
 
 // ---- autotuner ------------------------------------------------------------------------------
-int gsr_autotune(const GsrSceneDesc* scene, const GsrSettings* settings, const GsrColorModel* model,
-                 const GsrSplatCamera* cameras, uint32_t count, const uint32_t* depths, uint32_t depthCount,
-                 uint32_t frames, GsrTuneResult* out) {
-    if (!scene || !settings || !cameras || !depths || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
-    if (count == 0 || depthCount == 0 || frames == 0) return fail(GSR_ERROR_INVALID_ARGUMENT, "nothing to tune");
+int gsr_autotune_space(const GsrSceneDesc* scene, const GsrSettings* settings, const GsrColorModel* model,
+                       const GsrSplatCamera* cameras, uint32_t count, const GsrTuneSpace* space, uint32_t frames,
+                       GsrTuneResult* out) {
+    if (!scene || !settings || !cameras || !space || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    if (count == 0 || frames == 0 || !space->views_per_frame || space->views_per_frame_count == 0)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "nothing to tune");
     std::memset(out, 0, sizeof(*out));
-    const uint32_t schedules[2] = {GSR_RASTER_PER_TILE, GSR_RASTER_PERSISTENT};
+    // the knobs' value lists (a missing list keeps the settings' value; both schedules by default)
+    auto listOf = [](const uint32_t* v, uint32_t n, std::vector<uint32_t> fallback) {
+        return v && n ? std::vector<uint32_t>(v, v + n) : fallback;
+    };
+    const std::vector<uint32_t> depths = listOf(space->views_per_frame, space->views_per_frame_count, {});
+    const std::vector<uint32_t> schedules =
+        listOf(space->raster_schedules, space->raster_schedule_count, {GSR_RASTER_PER_TILE, GSR_RASTER_PERSISTENT});
+    const std::vector<uint32_t> tiles = listOf(space->tile_sizes, space->tile_size_count, {settings->tile_size});
+    const std::vector<uint32_t> digits =
+        listOf(space->sort_digit_bits, space->sort_digit_bits_count, {settings->sort_digit_bits});
+    if (uint64_t(depths.size()) * schedules.size() * tiles.size() * digits.size() > GSR_TUNE_MAX_CANDIDATES)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "more than %u candidates", GSR_TUNE_MAX_CANDIDATES);
+    for (uint32_t d : depths)
+        if (d == 0 || d > count || d > GSR_MAX_VIEWS)
+            return fail(GSR_ERROR_INVALID_ARGUMENT, "views per frame %u (1..%u)", d, std::min(count, GSR_MAX_VIEWS));
+    for (uint32_t sc : schedules)
+        if (sc != GSR_RASTER_PER_TILE && sc != GSR_RASTER_PERSISTENT)
+            return fail(GSR_ERROR_INVALID_ARGUMENT, "raster schedule %u", sc);
     cudaStream_t s = nullptr;
     GSR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int rc = GSR_OK;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rc = fail(GSR_ERROR_CUDA, "events");
-    for (uint32_t di = 0; rc == GSR_OK && di < depthCount; ++di) {
-        const uint32_t d = depths[di];
-        if (d == 0 || d > count || d > GSR_MAX_VIEWS) {
-            rc = fail(GSR_ERROR_INVALID_ARGUMENT, "views per frame %u (1..%u)", d, std::min(count, GSR_MAX_VIEWS));
-            break;
-        }
-        for (uint32_t sc : schedules) {
-            if (out->candidates >= GSR_TUNE_MAX_CANDIDATES) break;
-            GsrSettings st = *settings;
-            st.raster_schedule = sc;
-            GsrRenderer* r = nullptr;
-            rc = gsr_renderer_create(scene, &st, &r);
-            if (rc) break;
-            if (model) rc = gsr_renderer_set_color_model(r, model);
-            const uint32_t frameCount = count / d;  // whole frames of consecutive cameras
-            auto frame = [&](uint32_t k) { return r->renderViews(cameras + size_t(k % frameCount) * d, d, s); };
-            // warm-up: the layout, then frames until the adaptive list has kept its capacity for
-            // three frames (its statistics arrive frames_in_flight frames late)
-            uint32_t stable = 0, last = 0, k = 0;
-            for (; rc == GSR_OK && k < 24 && stable < 3; ++k) {
-                rc = frame(k);
-                if (rc == GSR_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(GSR_ERROR_CUDA, "warm-up");
-                const uint32_t cap = r->list ? r->list->capacity : 0;
-                stable = cap == last ? stable + 1 : 0;
-                last = cap;
-            }
-            if (rc == GSR_OK && cudaEventRecord(e0, s) != cudaSuccess) rc = fail(GSR_ERROR_CUDA, "event");
-            for (uint32_t j = 0; rc == GSR_OK && j < frames; ++j) rc = frame(k + j);
-            float ms = 0.0f;
-            if (rc == GSR_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-                                 cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
-                rc = fail(GSR_ERROR_CUDA, "timing");
-            gsr_renderer_destroy(r);
-            if (rc) break;
-            GsrTuneCandidate& c = out->table[out->candidates++];
-            c.views_per_frame = d;
-            c.raster_schedule = sc;
-            c.ms_per_frame = ms / float(frames);
-            c.views_per_s = ms > 0.0f ? float(frames) * float(d) / (ms * 1e-3f) : 0.0f;
-            if (c.views_per_s > out->views_per_s) {
-                out->views_per_s = c.views_per_s;
-                out->views_per_frame = d;
-                out->raster_schedule = sc;
-            }
-        }
-    }
+    for (uint32_t tile : tiles)
+        for (uint32_t bits : digits)
+            for (uint32_t d : depths)
+                for (uint32_t sc : schedules) {
+                    if (rc) break;
+                    GsrSettings st = *settings;
+                    st.raster_schedule = sc;
+                    st.tile_size = tile;
+                    st.sort_digit_bits = bits;
+                    GsrRenderer* r = nullptr;
+                    rc = gsr_renderer_create(scene, &st, &r);
+                    if (rc) break;
+                    if (model) rc = gsr_renderer_set_color_model(r, model);
+                    const uint32_t frameCount = count / d;  // whole frames of consecutive cameras
+                    auto frame = [&](uint32_t k) { return r->renderViews(cameras + size_t(k % frameCount) * d, d, s); };
+                    // warm-up: the layout, then frames until the adaptive list has kept its
+                    // capacity for three frames (its statistics arrive frames_in_flight frames late)
+                    uint32_t stable = 0, last = 0, k = 0;
+                    for (; rc == GSR_OK && k < 24 && stable < 3; ++k) {
+                        rc = frame(k);
+                        if (rc == GSR_OK && cudaStreamSynchronize(s) != cudaSuccess) rc = fail(GSR_ERROR_CUDA, "warm-up");
+                        const uint32_t cap = r->list ? r->list->capacity : 0;
+                        stable = cap == last ? stable + 1 : 0;
+                        last = cap;
+                    }
+                    if (rc == GSR_OK && cudaEventRecord(e0, s) != cudaSuccess) rc = fail(GSR_ERROR_CUDA, "event");
+                    for (uint32_t j = 0; rc == GSR_OK && j < frames; ++j) rc = frame(k + j);
+                    float ms = 0.0f;
+                    if (rc == GSR_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                                         cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                        rc = fail(GSR_ERROR_CUDA, "timing");
+                    gsr_renderer_destroy(r);
+                    if (rc) break;
+                    GsrTuneCandidate& c = out->table[out->candidates++];
+                    c.views_per_frame = d;
+                    c.raster_schedule = sc;
+                    c.tile_size = tile;
+                    c.sort_digit_bits = bits ? bits : 8u;
+                    c.ms_per_frame = ms / float(frames);
+                    c.views_per_s = ms > 0.0f ? float(frames) * float(d) / (ms * 1e-3f) : 0.0f;
+                    if (c.views_per_s > out->views_per_s) {
+                        out->views_per_s = c.views_per_s;
+                        out->views_per_frame = d;
+                        out->raster_schedule = sc;
+                        out->tile_size = tile;
+                        out->sort_digit_bits = c.sort_digit_bits;
+                    }
+                }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaStreamDestroy(s);
     return rc;
+}
+
+int gsr_autotune(const GsrSceneDesc* scene, const GsrSettings* settings, const GsrColorModel* model,
+                 const GsrSplatCamera* cameras, uint32_t count, const uint32_t* depths, uint32_t depthCount,
+                 uint32_t frames, GsrTuneResult* out) {
+    if (!depths || depthCount == 0) return fail(GSR_ERROR_INVALID_ARGUMENT, "nothing to tune");
+    GsrTuneSpace space{};
+    space.views_per_frame = depths;
+    space.views_per_frame_count = depthCount;
+    return gsr_autotune_space(scene, settings, model, cameras, count, &space, frames, out);
 }
 
 // ---- primitives ----------------------------------------------------------------------------

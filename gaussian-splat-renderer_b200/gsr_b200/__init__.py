@@ -87,7 +87,7 @@ class CSettings(C.Structure):
         ("adaptive_initial_entries", C.c_uint32), ("max_sh_degree", C.c_int32), ("output_format", C.c_uint32),
         ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("raster_schedule", C.c_uint32),
         ("list_mode", C.c_uint32), ("render_splat", C.c_uint32), ("sort_window", C.c_uint32),
-        ("reserved", C.c_uint32 * 3),
+        ("sort_digit_bits", C.c_uint32), ("reserved", C.c_uint32 * 2),
     ]
 
 
@@ -123,14 +123,25 @@ class ColorModelStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
+TUNE_MAX_CANDIDATES = 64
+
+
 class TuneCandidate(C.Structure):
     _fields_ = [("views_per_frame", C.c_uint32), ("raster_schedule", C.c_uint32), ("views_per_s", C.c_float),
-                ("ms_per_frame", C.c_float)]
+                ("ms_per_frame", C.c_float), ("tile_size", C.c_uint32), ("sort_digit_bits", C.c_uint32)]
 
 
 class TuneResult(C.Structure):
     _fields_ = [("views_per_frame", C.c_uint32), ("raster_schedule", C.c_uint32), ("views_per_s", C.c_float),
-                ("candidates", C.c_uint32), ("table", TuneCandidate * 32)]
+                ("candidates", C.c_uint32), ("tile_size", C.c_uint32), ("sort_digit_bits", C.c_uint32),
+                ("table", TuneCandidate * TUNE_MAX_CANDIDATES)]
+
+
+class TuneSpace(C.Structure):
+    _fields_ = [("views_per_frame", C.POINTER(C.c_uint32)), ("views_per_frame_count", C.c_uint32),
+                ("raster_schedules", C.POINTER(C.c_uint32)), ("raster_schedule_count", C.c_uint32),
+                ("tile_sizes", C.POINTER(C.c_uint32)), ("tile_size_count", C.c_uint32),
+                ("sort_digit_bits", C.POINTER(C.c_uint32)), ("sort_digit_bits_count", C.c_uint32)]
 
 
 class Control(C.Structure):
@@ -222,6 +233,8 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_color_model_destroy": (None, [vp]),
         "gsr_autotune": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(CSettings), vp, C.POINTER(SplatCamera), u32,
                                    C.POINTER(u32), u32, u32, C.POINTER(TuneResult)]),
+        "gsr_autotune_space": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(CSettings), vp, C.POINTER(SplatCamera), u32,
+                                         C.POINTER(TuneSpace), u32, C.POINTER(TuneResult)]),
         "gsr_scan": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_scan_static": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_sort_pairs": (C.c_int, [vp, vp, vp, u32, u32, vp]),
@@ -284,6 +297,7 @@ class Settings:
     render_splat: str = "full"
     target: str = "rgba32f"  # the output image: rgba32f, rgba16f or rgba8 (rgb8 adds the 8-bit RGB image)
     sort_window: int = 0  # StopThePop per-pixel window K (0 = off, at most 64)
+    sort_digit_bits: int = 0  # radix digit width of the list sort (0 = 8)
 
     def to_c(self) -> CSettings:
         s = CSettings()
@@ -306,6 +320,7 @@ class Settings:
         s.list_mode = LIST_MODES[self.list_mode]
         s.render_splat = RENDER_SPLATS[self.render_splat]
         s.sort_window = self.sort_window
+        s.sort_digit_bits = self.sort_digit_bits
         return s
 
 
@@ -580,17 +595,30 @@ class Renderer:
 
 
 def autotune(scene: GpuScene, settings: Settings, cameras, depths=(1, 2, 4, 8, 16), frames: int = 4,
-             model: "ColorModel | None" = None) -> dict:
-    """gsr_autotune: the fastest (views per frame, rasterizer schedule) on these cameras."""
+             model: "ColorModel | None" = None, schedules=None, tile_sizes=None, sort_digit_bits=None) -> dict:
+    """gsr_autotune_space: the fastest (views per frame, rasterizer schedule, tile size, digit
+    width) on these cameras. A knob given as None keeps the settings' value (both schedules)."""
     cams = cameras if isinstance(cameras, C.Array) else camera_array(cameras)
-    dep = (C.c_uint32 * len(depths))(*depths)
+
+    def arr(v):
+        return ((C.c_uint32 * len(v))(*v), len(v)) if v else (None, 0)
+
+    keep = []
+    fields = []
+    for v in (depths, [RASTER_SCHEDULES[x] if isinstance(x, str) else x for x in schedules] if schedules else None,
+              tile_sizes, sort_digit_bits):
+        a, n = arr(list(v) if v else None)
+        keep.append(a)
+        fields += [C.cast(a, C.POINTER(C.c_uint32)) if a is not None else None, n]
+    space = TuneSpace(*fields)
     res = TuneResult()
-    check(load().gsr_autotune(C.byref(scene.desc), C.byref(settings.to_c()), model.handle if model else None, cams,
-                              len(cams), dep, len(depths), frames, C.byref(res)))
+    check(load().gsr_autotune_space(C.byref(scene.desc), C.byref(settings.to_c()), model.handle if model else None,
+                                    cams, len(cams), C.byref(space), frames, C.byref(res)))
     names = {v: k for k, v in RASTER_SCHEDULES.items()}
     return {"views_per_frame": res.views_per_frame, "raster_schedule": names[res.raster_schedule],
-            "views_per_s": res.views_per_s,
+            "tile_size": res.tile_size, "sort_digit_bits": res.sort_digit_bits, "views_per_s": res.views_per_s,
             "table": [{"views_per_frame": c.views_per_frame, "raster_schedule": names[c.raster_schedule],
+                       "tile_size": c.tile_size, "sort_digit_bits": c.sort_digit_bits,
                        "views_per_s": round(c.views_per_s, 2), "ms_per_frame": round(c.ms_per_frame, 4)}
                       for c in res.table[:res.candidates]]}
 

@@ -158,7 +158,9 @@ typedef struct GsrSettings {
     uint32_t render_splat;             /* GsrRenderSplat (TileSettings::renderSplat, cli.h:34) */
     uint32_t sort_window;              /* StopThePop per-pixel window K (TileSettings::sortWindow, cli.h:46):
                                           0 = off (the list's order), 1..64 */
-    uint32_t reserved[3];
+    uint32_t sort_digit_bits;          /* radix digit width of the list sort; 0 = 8 (the reference's
+                                          GpuRadixSort digits, gpu_radix_sort.h:38-122) */
+    uint32_t reserved[2];
 } GsrSettings;
 
 /* The per-entry record that key emission and the rasterizer read (RenderSplatMode,
@@ -348,26 +350,49 @@ int gsr_renderer_set_color_model(GsrRenderer* r, const GsrColorModel* model);
 void gsr_color_model_destroy(GsrColorModel* model);
 
 /* ---- autotuner (no reference counterpart) -------------------------------------------------
- * Times each candidate (views per frame x rasterizer schedule) on the caller's cameras with a
- * renderer of the given settings (and colour model, or NULL) and returns the fastest. Tile shape
- * (16 x 16, the reference's) and radix digit width (8 bits) are fixed in this build and not among
- * the knobs. Synchronous; allocates and frees its own renderers. */
-#define GSR_TUNE_MAX_CANDIDATES 32u
+ * Times each candidate of a search space on the caller's cameras with renderers of the given
+ * settings (and colour model, or NULL) and returns the fastest. The knobs: views per frame, the
+ * rasterizer schedule (one block per tile, or a persistent (view, tile) queue), the tile shape
+ * (16 x 16, the reference's tiles, or 8 x 8) and the radix digit width of the list sort.
+ * Synchronous; allocates and frees its own renderers. */
+#define GSR_TUNE_MAX_CANDIDATES 64u
 typedef struct GsrTuneCandidate {
     uint32_t views_per_frame;
     uint32_t raster_schedule;  /* GSR_RASTER_PER_TILE or GSR_RASTER_PERSISTENT */
     float views_per_s;         /* device time over whole frames of consecutive cameras */
     float ms_per_frame;
+    uint32_t tile_size;        /* binning / render tile edge in pixels */
+    uint32_t sort_digit_bits;  /* digit width of the list's radix sort */
 } GsrTuneCandidate;
 typedef struct GsrTuneResult {
     uint32_t views_per_frame;  /* the fastest candidate */
     uint32_t raster_schedule;
     float views_per_s;
     uint32_t candidates;       /* entries of table */
+    uint32_t tile_size;
+    uint32_t sort_digit_bits;
     GsrTuneCandidate table[GSR_TUNE_MAX_CANDIDATES];
 } GsrTuneResult;
-/* depths: the candidate views per frame (each <= count); cameras[0..count) are rendered in frames
- * of that many consecutive cameras, `frames` timed frames per candidate after 2 warm-up frames. */
+/* The search space: a NULL list (or a zero count) keeps the settings' value for that knob, except
+ * raster_schedules, where it means both schedules. Candidates beyond GSR_TUNE_MAX_CANDIDATES are
+ * refused (GSR_ERROR_INVALID_ARGUMENT). */
+typedef struct GsrTuneSpace {
+    const uint32_t* views_per_frame;  /* each 1..min(count, GSR_MAX_VIEWS) */
+    uint32_t views_per_frame_count;
+    const uint32_t* raster_schedules; /* GSR_RASTER_PER_TILE / GSR_RASTER_PERSISTENT */
+    uint32_t raster_schedule_count;
+    const uint32_t* tile_sizes;       /* 16 or 8 */
+    uint32_t tile_size_count;
+    const uint32_t* sort_digit_bits;  /* see GsrSettings.sort_digit_bits */
+    uint32_t sort_digit_bits_count;
+} GsrTuneSpace;
+/* cameras[0..count) are rendered in frames of `views_per_frame` consecutive cameras; each
+ * candidate gets warm-up frames until the adaptive list keeps its capacity, then `frames` timed
+ * frames. */
+int gsr_autotune_space(const GsrSceneDesc* scene, const GsrSettings* settings, const GsrColorModel* model,
+                       const GsrSplatCamera* cameras, uint32_t count, const GsrTuneSpace* space, uint32_t frames,
+                       GsrTuneResult* out);
+/* gsr_autotune_space over views per frame x both schedules, the settings' tile size and digit width. */
 int gsr_autotune(const GsrSceneDesc* scene, const GsrSettings* settings, const GsrColorModel* model,
                  const GsrSplatCamera* cameras, uint32_t count, const uint32_t* depths, uint32_t depth_count,
                  uint32_t frames, GsrTuneResult* out);

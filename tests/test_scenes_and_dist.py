@@ -1,6 +1,7 @@
 """Host logic without a GPU: the synthetic workloads (seeded, the stated distributions and
 sizes) and the multi-rank plumbing of bench.py (one process per GPU; max over ranks and
 barriers), run as two gloo ranks on the CPU."""
+import json
 import os
 import socket
 import subprocess
@@ -85,3 +86,33 @@ def test_reference_arm_on_other_ranks_exits_without_work():
     r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "3"],
                        env=env, capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_partition_views_balances_pixels_and_covers_every_view():
+    import bench
+    from gsr_b200 import scenes
+
+    pixels = [c.width * c.height for c in scenes.batched_cameras(64, seed=2)]
+    for ranks in (1, 2, 3, 4, 8):
+        parts = bench.partition_views(pixels, ranks)
+        flat = sorted(v for p in parts for v in p)
+        assert flat == list(range(64))  # every view exactly once
+        loads = [sum(pixels[v] for v in p) for p in parts]
+        # greedy largest-first: no rank exceeds the mean by more than the largest view
+        assert max(loads) - sum(loads) / ranks <= max(pixels)
+        assert all(p == sorted(p) for p in parts)
+    assert bench.partition_views([5, 1, 1, 1, 1, 1], 2) == [[0], [1, 2, 3, 4, 5]]
+
+
+@pytest.mark.timeout(300)
+def test_bench_gpus_2_launches_two_ranks_and_gathers_views():
+    """`bench.py --gpus 2` without a launcher starts two ranks itself (torch's launcher, gloo
+    here); the views of batched_64 are split between them and gathered on rank 0."""
+    env = dict(os.environ, GSR_BENCH_BACKEND="gloo")
+    env.pop("WORLD_SIZE", None)
+    r = subprocess.run([sys.executable, str(REPO / "bench.py"), "--gpus", "2", "--check-launch"], env=env,
+                       capture_output=True, text=True, timeout=280)
+    assert r.returncode == 0, r.stdout + r.stderr
+    line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+    assert line["n_gpus"] == 2 and line["views"] == 64 and line["views_gathered"] == 64
+    assert line["gathered_in_order"] and line["max_rank"] == 1.0
