@@ -357,8 +357,9 @@ class CpuLeg:
         pa, sc, ro, sh = self.port.decode(enc, scene.count)
         return scenes.Scene(pa, sc, ro, sh, int(enc["desc"][7]))
 
-    def check_view(self, G, gs, dec_scene, cam, stream, tile_size: int = 16) -> dict:
-        """One view on the GPU (list capacity large enough for it) against the CPU code."""
+    def check_view(self, G, gs, dec_scene, cam, stream, tile_size: int = 16, fp64: bool = False) -> dict:
+        """One view on the GPU (list capacity large enough for it) against the CPU code; with fp64
+        also the float images' largest error against the FP64 build of renderReference."""
         r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=False, budget_mb=4096, rgb8=True,
                                       tile_size=tile_size))
         r.render(cam, stream)
@@ -377,11 +378,20 @@ class CpuLeg:
         img, _ = self.ref.render(dec_scene, rcam, bounds=1, threads=self.threads)
         want8 = quantize(img)
         diff8 = int(np.abs(rgb8.astype(np.int16) - want8.astype(np.int16)).max())
-        return {"list_bit_exact": bool(same), "entries": int(ctl.entries), "oracle_entries": int(olist["duplicates"]),
-                "overflow": int(ctl.overflow),
-                "psnr_float_db": psnr(np.clip(rgba[..., :3], 0, 1), np.clip(img, 0, 1)),
-                "psnr_8bit_db": psnr(rgb8, want8, 255.0), "max_8bit_diff": diff8, "image_oracle": self.kind,
-                "view": f"{cam.width}x{cam.height}"}
+        out = {"list_bit_exact": bool(same), "entries": int(ctl.entries), "oracle_entries": int(olist["duplicates"]),
+               "overflow": int(ctl.overflow),
+               "psnr_float_db": psnr(np.clip(rgba[..., :3], 0, 1), np.clip(img, 0, 1)),
+               "psnr_8bit_db": psnr(rgb8, want8, 255.0), "max_8bit_diff": diff8, "image_oracle": self.kind,
+               "view": f"{cam.width}x{cam.height}"}
+        if fp64:
+            f64, _ = self.port.render_precision(dec_scene, cam, 64, bounds=1, threads=self.threads)
+            gpu_err = np.abs(rgba[..., :3].astype(np.float64) - f64)
+            cpu_err = np.abs(img.astype(np.float64) - f64)
+            out["vs_fp64"] = {"max_float_err": float(gpu_err.max()), "mean_float_err": float(gpu_err.mean()),
+                              "psnr_db": psnr(rgba[..., :3], f64),
+                              "cpu_reference_max_float_err": float(cpu_err.max()),
+                              "cpu_reference_psnr_db": psnr(img, f64)}
+        return out
 
     def baseline(self, scene, cams, max_frames: int, time_budget_s: float, warmup: int = 1) -> dict:
         """renderReference on all host threads over a bounded, evenly spaced sample of the cameras."""
@@ -642,7 +652,7 @@ def run_1080p(G, args, dist, sampler, stream_obj, peak):
     # parity of view 0 against the oracle (list bit for bit, images against renderReference)
     leg = cpu_leg(args, dist)
     if leg:
-        out["plain_1080p"]["parity"] = leg.check_view(G, gs, scene, cams[order[0]], stream_obj.cuda_stream)
+        out["plain_1080p"]["parity"] = leg.check_view(G, gs, scene, cams[order[0]], stream_obj.cuda_stream, fp64=True)
     # learned colour: the configs' recipe, gated at 2/255, then the same training forced on
     learned = {}
     for label, gate in (("gated", 2.0 / 255.0), ("forced", 1e30)):
@@ -840,7 +850,7 @@ def run_720p(G, args, dist, sampler, stream_obj):
     out = {"plain": plain}
     leg = cpu_leg(args, dist)
     if leg:
-        out["parity"] = leg.check_view(G, gs, scene, cams[0], stream_obj.cuda_stream)
+        out["parity"] = leg.check_view(G, gs, scene, cams[0], stream_obj.cuda_stream, fp64=True)
     gs.close()
     return out
 

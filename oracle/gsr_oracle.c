@@ -1337,3 +1337,19 @@ void gsr_oracle_quantize_rgb8(uint32_t pixels, const float* rgb, uint32_t srcStr
 void gsr_oracle_logf_range(uint32_t first_bits, uint32_t count, float* out) {
     for (uint32_t j = 0; j < count; ++j) out[j] = logf(bitsf(first_bits + j));
 }
+
+/* ---- renderReference over a scalar type (frame_generic.h): the float instance restates the
+ *      functions above once more and must equal them bit for bit; the double instance is the
+ *      FP64 build the float images are measured against. <tgmath.h> picks each math
+ *      function's precision from its argument. ------------------------------------------ */
+#include <tgmath.h>
+#define REAL float
+#define FN(x) x##_f32
+#include "frame_generic.h"
+#undef REAL
+#undef FN
+#define REAL double
+#define FN(x) x##_f64
+#include "frame_generic.h"
+#undef REAL
+#undef FN

@@ -122,6 +122,19 @@ void gsr_oracle_logf_range(uint32_t first_bits, uint32_t count, float* out);
  * lround(clamp(v, 0, 1) * 255)), and PSNR with peak 1.0 (tools/imgdiff.cpp:127). */
 void gsr_oracle_quantize_rgb8(uint32_t pixels, const float* rgb, uint32_t srcStride, uint8_t* out);
 
+/* renderReference (reference_renderer.cpp:41-234, list order, no window) written once over a
+ * scalar type (frame_generic.h), from the viewer matrices: _f32 in float (equal to
+ * gsr_oracle_render bit for bit), _f64 the same operations in double (the FP64 build). rgb:
+ * width x height x 3 of the instance's type. */
+int gsr_oracle_render_f32(uint32_t n, int shDegree, const float* posAlpha, const float* scales, const float* rotations,
+                          const float* sh, const float* view, const float* proj, const float* model, uint32_t width,
+                          uint32_t height, int maxShDegree, uint32_t bounds, uint32_t threads, float* rgb,
+                          GsrOracleRenderStats* stats);
+int gsr_oracle_render_f64(uint32_t n, int shDegree, const float* posAlpha, const float* scales, const float* rotations,
+                          const float* sh, const float* view, const float* proj, const float* model, uint32_t width,
+                          uint32_t height, int maxShDegree, uint32_t bounds, uint32_t threads, double* rgb,
+                          GsrOracleRenderStats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -80,7 +80,7 @@ class RenderStats(C.Structure):
 
 def build_port() -> Path:
     """Compile the C restatement (gcc) if its library is missing or stale."""
-    src = [HERE / "gsr_oracle.c", HERE / "gsr_oracle.h"]
+    src = [HERE / "gsr_oracle.c", HERE / "gsr_oracle.h", HERE / "frame_generic.h"]
     if not PORT_LIB.exists() or any(s.stat().st_mtime > PORT_LIB.stat().st_mtime for s in src):
         subprocess.run(["make", "-s", "-C", str(HERE), "oracle"], check=True)
     return PORT_LIB
@@ -132,6 +132,8 @@ class Oracle:
             f("tile_list", C.c_uint64, None)
             f("preprocess_degrees", None, None)
             f("logf_range", None, [C.c_uint32, C.c_uint32, C.c_void_p])
+            f("render_f32", C.c_int, None)
+            f("render_f64", C.c_int, None)
 
     def _f(self, name, restype, argtypes):
         fn = getattr(self.lib, self.prefix + name)
@@ -225,6 +227,26 @@ class Oracle:
         if rc != 0:
             raise RuntimeError("oracle render failed")
         return rgb.reshape(cam.height, cam.width, 3), st.as_dict()
+
+    def render_precision(self, scene, viewer_cam, bits: int = 64, max_sh_degree=3, bounds=BOUNDS_TIGHT, threads=0):
+        """renderReference (list order) written once over a scalar type, in float (bits 32, equal to
+        render() bit for bit) or double (bits 64, the FP64 build), from the viewer camera's
+        matrices. Returns (rgb (H, W, 3) float32 or float64, stats)."""
+        w, h = viewer_cam.width, viewer_cam.height
+        rgb = np.zeros(w * h * 3, np.float64 if bits == 64 else np.float32)
+        st = RenderStats()
+        v, p, m = (np.ascontiguousarray(x, np.float32).reshape(16) for x in (viewer_cam.view, viewer_cam.proj,
+                                                                             viewer_cam.model))
+        fn = self._render_f64 if bits == 64 else self._render_f32
+        rc = fn(C.c_uint32(scene.count), C.c_int(scene.sh_degree), _p(scene.pos_alpha), _p(scene.scales),
+                _p(scene.rotations), _p(scene.sh), _p(v), _p(p), _p(m), C.c_uint32(w), C.c_uint32(h),
+                C.c_int(max_sh_degree), C.c_uint32(bounds), C.c_uint32(threads), _p(rgb), C.byref(st))
+        if rc != 0:
+            raise RuntimeError("oracle render failed")
+        d = st.as_dict()
+        for k in ("preprocessMs", "sortMs", "binMs", "rasterMs", "totalMs"):
+            d.pop(k, None)
+        return rgb.reshape(h, w, 3), d
 
     def depth_sort(self, pos_alpha, view_inria):
         n = len(pos_alpha)
