@@ -567,6 +567,34 @@ def roofline(passes: dict, ctl, fmt: str, n: int, tiles: int, peak: float, peak_
             "peak_kind": peak_kind, "algorithmic_bytes": int(tot_b), "ms": round(tot_ms, 4), "kernels": kernels}
 
 
+def render_flops(G, gs, args, frames: Frames, stream_obj, passes: dict, clocks: dict, n: int = 20):
+    """The rasterizer against the FP32 pipe: the stats build counts, over the same frames as the
+    pass times, the (pixel, splat) pairs the reference's loop evaluates (entries a pixel visits
+    until it terminates) and the pairs this kernel tests; each pair is ~20 FP32 operations and
+    one exp (the tile loop's power, alpha and blend). The peak is 148 SMs x 128 FP32 lanes x 2
+    (FMA) at the SM clock sampled under load (nominal, not measured)."""
+    r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.budget_mb,
+                                  tile_stats=True))
+    ev = te = 0
+    for k in range(n):
+        render_call(r, frames, k, stream_obj.cuda_stream)
+        stream_obj.synchronize()
+        st, tested = r.read_tile_stats()
+        ev += int(st[:, 2].sum())
+        te += int(tested)
+    r.close()
+    ms = passes.get("render tiles")
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+    ev, te = ev / n, te / n
+    return {"bound": "fp32", "flops_per_pair": 20, "evaluated_pairs": int(ev), "tested_pairs": int(te),
+            "algorithmic_tflops": round(20 * ev / (ms * 1e-3) / 1e12, 3),
+            "kernel_tflops": round(20 * te / (ms * 1e-3) / 1e12, 3), "peak_tflops": round(peak, 2),
+            "frac_algorithmic": round(20 * ev / (ms * 1e-3) / 1e12 / peak, 4),
+            "frac_kernel": round(20 * te / (ms * 1e-3) / 1e12 / peak, 4), "render_ms": ms,
+            "peak_kind": "nominal (148 x 128 FP32 lanes x 2 at the sampled SM clock)"}
+
+
 def render_issue(passes: dict, clocks: dict, instructions: float | None):
     ms = passes.get("render tiles")
     mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
@@ -632,6 +660,7 @@ def run_1080p(G, args, dist, sampler, stream_obj, peak):
     roof = roofline(passes, ctl, fmt, scene.count, tiles, peak[0], peak[1])
     roof["traffic"] = int(TRAFFIC_PLAIN_1080P_CAPTURE)
     roof["traffic_kind"] = "from_capture"
+    plain["render_flops"] = render_flops(G, gs, args, plain_frames, stream_obj, passes, plain["clocks"])
     plain.update({"passes_ms": passes, "frame": {"visible": ctl.visible, "entries": ctl.entries,
                                                  "duplicates": ctl.duplicates, "overflow": ctl.overflow,
                                                  "sort_passes": ctl.sort_passes, "key_bits": ctl.key_bits}})
@@ -956,6 +985,7 @@ def run_b200(args, dist: Dist):
         line["speedup_vs_plain"] = round(head["views_per_s"] / plain["views_per_s"], 4)
         line["roofline"] = head_roof
         line["render_issue"] = render_issue(plain["passes_ms"], plain["clocks"], RENDER_WARP_INSTRUCTIONS_1080P)
+        line["render_flops"] = plain.get("render_flops")
         line["parity"] = configs["plain_1080p"].get("parity")
     line["configs"] = configs
     leg = cpu_leg(args, dist)

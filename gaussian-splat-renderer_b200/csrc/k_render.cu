@@ -222,7 +222,13 @@ __device__ __forceinline__ void windowPush(SortWindow<CAP>& q, uint32_t K, float
 // TILE: the tile's edge, 16 (INRIA's tiles) or 8 pixels; one thread per pixel, batches of TILE^2
 // entries, and each warp owns an 8 x 4 pixel block of the tile (its strip: a squarer footprint
 // meets fewer ellipses than a 16 x 2 row pair).
-template <int MODE, int CAP, int TILE>
+// STATS: the instrumented build (TileSettings::stats, tile_render.comp's GSR_TILE_STATS): the
+// kTileStatCount words of the tile (list length, fetched, evaluated, blended, terminated, lane
+// slots, max depth, pixels) and the frame's count of the pairs this kernel tested. "Evaluated"
+// keeps the reference's meaning, the list entries a pixel visits until it terminates (all of
+// them when it does not); "tested" are the pairs this kernel computed alpha for (a pixel still
+// blending and a record whose cutoff ellipse meets the pixel's warp strip).
+template <int MODE, int CAP, int TILE, bool STATS>
 __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TILE * TILE>& sm,
                                            float4 (*ray)[3][TILE * TILE], uint32_t tile) {
     constexpr uint32_t kThreads = TILE * TILE, kStripW = 8, kRows = 4, kStripsX = TILE / kStripW;
@@ -297,10 +303,15 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
         vy = (fy - 0.5f * (float(vw.height) - 1.0f)) / a.cam[view].focalY;
     }
 
+    // STATS counters (per thread; stIters is uniform over the warp)
+    uint32_t stEval = 0, stBlend = 0, stIters = 0, stFetched = 0, stTested = 0;
+    bool stTerm = false;
+
     int buf = 0;
     if (range.x < range.y) issue(range.x, 0);
     for (uint32_t start = range.x; start < range.y; start += kThreads, buf ^= 1) {
         if (__syncthreads_count(done) == int(kThreads)) break;
+        if constexpr (STATS) stFetched += range.y - start < kThreads ? range.y - start : kThreads;
         // prefetch the next batch while this one is prepared and blended
         const uint32_t next = start + kThreads;
         if (next < range.y) issue(next, buf ^ 1);
@@ -364,6 +375,10 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
             const bool hit = ql < n && ((sm.strips[ql] >> warp) & 1u) != 0u;
             for (uint32_t m = __ballot_sync(0xffffffffu, hit); m != 0u; m &= m - 1u) {
                 const uint32_t q = q0 + uint32_t(__ffs(m)) - 1u;
+                if constexpr (STATS) {
+                    ++stIters;
+                    stTested += done ? 0u : 1u;
+                }
                 const float2 c = sm.center[q];
                 const float4 co = sm.conic[q];
                 const float dx = c.x - fx;
@@ -385,6 +400,10 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
                 const float testT = T * (1.0f - alpha);
                 if (testT < kMinTransmittance) {
                     done = true;
+                    if constexpr (STATS) {
+                        stTerm = true;
+                        stEval = start + q - range.x + 1u;  // the entries visited, the terminating one included
+                    }
                     continue;
                 }
                 const float4 col = sm.color[q];
@@ -393,6 +412,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
                 c1 += col.y * w;
                 c2 += col.z * w;
                 T = testT;
+                if constexpr (STATS) ++stBlend;
             }
         }
     }
@@ -402,6 +422,31 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
             if (!done && uint32_t(i) < window.count) blendOver(window.al[i], window.r[i], window.g[i], window.b[i], T, c0, c1, c2, done);
     }
     cpAsyncWait<0>();
+    if constexpr (STATS) {
+        if (!stTerm) stEval = inside ? range.y - range.x : 0u;
+        __shared__ uint32_t sStat[kTileStatWords];
+        if (tid < kTileStatWords) sStat[tid] = 0u;
+        __syncthreads();
+        const uint32_t eSum = __reduce_add_sync(0xffffffffu, stEval), bSum = __reduce_add_sync(0xffffffffu, stBlend);
+        const uint32_t tSum = __popc(__ballot_sync(0xffffffffu, stTerm)), pSum = __popc(__ballot_sync(0xffffffffu, inside));
+        const uint32_t eMax = __reduce_max_sync(0xffffffffu, stEval), tested = __reduce_add_sync(0xffffffffu, stTested);
+        if (lane == 0) {
+            atomicAdd(&sStat[kTileStatEvaluated], eSum);
+            atomicAdd(&sStat[kTileStatBlended], bSum);
+            atomicAdd(&sStat[kTileStatTerminated], tSum);
+            atomicAdd(&sStat[kTileStatLaneSlots], stIters * 32u);
+            atomicMax(&sStat[kTileStatMaxDepth], eMax);
+            atomicAdd(&sStat[kTileStatPixels], pSum);
+            atomicAdd(a.testedPairs, (unsigned long long)tested);
+        }
+        __syncthreads();
+        if (tid == 0) {
+            sStat[kTileStatListLength] = range.y - range.x;
+            sStat[kTileStatFetched] = stFetched;
+        }
+        __syncthreads();
+        if (tid < kTileStatWords) a.tileStats[size_t(tile) * kTileStatWords + tid] = sStat[tid];
+    }
     if (!inside) return;
     const size_t p = vw.pixelBase + size_t(py) * vw.width + px;
     if (a.imageFormat == 0) {
@@ -441,16 +486,16 @@ __device__ __forceinline__ float4 (*rayArea(unsigned char* smem))[3][N] {
 
 // Without the window: five 256-thread blocks (or the same threads in 8-px tiles) per SM, 48
 // registers a thread (the strip masks would take 61, four blocks, 5 % slower).
-template <int MODE, int CAP, int TILE>
+template <int MODE, int CAP, int TILE, bool STATS>
 __global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1) renderKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
-    renderTile<MODE, CAP, TILE>(a, *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw),
-                                CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, blockIdx.x + a.tileOffset);
+    renderTile<MODE, CAP, TILE, STATS>(a, *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw),
+                                       CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, blockIdx.x + a.tileOffset);
 }
 
 // Persistent schedule: each block takes tiles from the frame's queue counter (reset by frame
 // begin) until the counter passes the last tile.
-template <int MODE, int CAP, int TILE>
+template <int MODE, int CAP, int TILE, bool STATS>
 __global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1) renderPersistentKernel(const __grid_constant__ RenderArgs a) {
     extern __shared__ __align__(16) unsigned char smemRaw[];
     RenderShared<TILE * TILE>& sm = *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw);
@@ -459,12 +504,12 @@ __global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE
         __syncthreads();
         const uint32_t tile = sm.tile;
         if (tile >= a.totalTiles) break;
-        renderTile<MODE, CAP, TILE>(a, sm, CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, tile);
+        renderTile<MODE, CAP, TILE, STATS>(a, sm, CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, tile);
         __syncthreads();  // every thread has read sm.tile and left the tile's shared buffers
     }
 }
 
-template <int MODE, int CAP, int TILE>
+template <int MODE, int CAP, int TILE, bool STATS = false>
 cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
     constexpr size_t smem = renderSmemBytes<CAP, TILE * TILE>();
     constexpr uint32_t threads = TILE * TILE;
@@ -472,9 +517,9 @@ cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
     std::atomic<bool>& configured = perDevice(configuredOn);
     if (!configured) {
         cudaError_t e =
-            cudaFuncSetAttribute(renderKernel<MODE, CAP, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+            cudaFuncSetAttribute(renderKernel<MODE, CAP, TILE, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(renderPersistentKernel<MODE, CAP, TILE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(renderPersistentKernel<MODE, CAP, TILE, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(smem));
         if (e != cudaSuccess) return e;
         configured = true;
@@ -484,9 +529,9 @@ cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         // as many resident threads per SM for either tile size
         const uint32_t grid = uint32_t(sms) * kPersistentBlocksPerSm * (kRenderThreads / threads);
-        renderPersistentKernel<MODE, CAP, TILE><<<grid < a.totalTiles ? grid : a.totalTiles, threads, smem, s>>>(a);
+        renderPersistentKernel<MODE, CAP, TILE, STATS><<<grid < a.totalTiles ? grid : a.totalTiles, threads, smem, s>>>(a);
     } else {
-        renderKernel<MODE, CAP, TILE><<<a.tileLaunch ? a.tileLaunch : a.totalTiles, threads, smem, s>>>(a);
+        renderKernel<MODE, CAP, TILE, STATS><<<a.tileLaunch ? a.tileLaunch : a.totalTiles, threads, smem, s>>>(a);
     }
     return cudaGetLastError();
 }
@@ -494,6 +539,7 @@ cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
 // the window capacity for K: 4, 16 or 64 register slots
 template <int MODE, int TILE>
 cudaError_t launchRenderWindow(const RenderArgs& a, cudaStream_t s) {
+    if (a.tileStats) return launchRenderMode<MODE, 0, TILE, true>(a, s);  // the stats build has no window
     if (a.sortWindow == 0) return launchRenderMode<MODE, 0, TILE>(a, s);
     if (a.sortWindow <= 4) return launchRenderMode<MODE, 4, TILE>(a, s);
     if (a.sortWindow <= 16) return launchRenderMode<MODE, 16, TILE>(a, s);

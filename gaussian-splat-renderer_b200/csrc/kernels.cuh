@@ -162,7 +162,14 @@ struct RenderArgs {
     uint32_t count;           // N: gaussian indices read from the list are checked against it
     DeviceControl* ctl;
     const SortPlan* plan;     // the entry layout (packed words or key/value arrays)
+    uint32_t* tileStats;      // the stats build: kTileStatWords per frame tile (null: the plain build)
+    unsigned long long* testedPairs;  // the stats build: pairs the kernel tested, summed over the frame
 };
+
+// The stats build's words per tile (TileStat, splat_tile_renderer.h:131-141).
+constexpr uint32_t kTileStatListLength = 0, kTileStatFetched = 1, kTileStatEvaluated = 2, kTileStatBlended = 3,
+                   kTileStatTerminated = 4, kTileStatLaneSlots = 5, kTileStatMaxDepth = 6, kTileStatPixels = 7,
+                   kTileStatWords = 8;
 
 // ---- launchers (return cudaGetLastError()) ---------------------------------------------------
 cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint32_t* ranges,

@@ -25,40 +25,28 @@ namespace {
 using Clock = std::chrono::steady_clock;
 double msSince(Clock::time_point t0) { return std::chrono::duration<double, std::milli>(Clock::now() - t0).count(); }
 
-// Headers of real files are about 1.5 KB; a longer one is not a 3DGS file.
+// A header is read from at most this many bytes (3DGS headers are a few KB).
 constexpr size_t kMaxHeaderBytes = size_t(1) << 20;
 
-bool scalarFromName(std::string_view s, PlyScalar& t) {
-    // the classic PLY names and their sized aliases
-    static const struct {
-        const char* name;
-        PlyScalar type;
-    } kNames[] = {{"char", PlyScalar::Int8},      {"int8", PlyScalar::Int8},       {"uchar", PlyScalar::UInt8},
-                  {"uint8", PlyScalar::UInt8},    {"short", PlyScalar::Int16},     {"int16", PlyScalar::Int16},
-                  {"ushort", PlyScalar::UInt16},  {"uint16", PlyScalar::UInt16},   {"int", PlyScalar::Int32},
-                  {"int32", PlyScalar::Int32},    {"uint", PlyScalar::UInt32},     {"uint32", PlyScalar::UInt32},
-                  {"float", PlyScalar::Float32},  {"float32", PlyScalar::Float32}, {"double", PlyScalar::Float64},
-                  {"float64", PlyScalar::Float64}};
-    for (const auto& e : kNames)
-        if (s == e.name) {
-            t = e.type;
-            return true;
-        }
-    return false;
-}
+// ---- scalars -----------------------------------------------------------------------------------
+struct ScalarName {
+    std::string_view name;
+    PlyScalar type;
+};
+// the PLY specification's type names and their sized spellings
+constexpr ScalarName kScalarNames[] = {
+    {"char", PlyScalar::Int8},      {"uchar", PlyScalar::UInt8},    {"short", PlyScalar::Int16},
+    {"ushort", PlyScalar::UInt16},  {"int", PlyScalar::Int32},      {"uint", PlyScalar::UInt32},
+    {"float", PlyScalar::Float32},  {"double", PlyScalar::Float64}, {"int8", PlyScalar::Int8},
+    {"uint8", PlyScalar::UInt8},    {"int16", PlyScalar::Int16},    {"uint16", PlyScalar::UInt16},
+    {"int32", PlyScalar::Int32},    {"uint32", PlyScalar::UInt32},  {"float32", PlyScalar::Float32},
+    {"float64", PlyScalar::Float64}};
 
-// whitespace (space, tab) separated words of one header line
-std::vector<std::string_view> words(std::string_view line) {
-    std::vector<std::string_view> out;
-    size_t i = 0;
-    while (i < line.size()) {
-        while (i < line.size() && (line[i] == ' ' || line[i] == '\t')) ++i;
-        size_t j = i;
-        while (j < line.size() && line[j] != ' ' && line[j] != '\t') ++j;
-        if (j > i) out.push_back(line.substr(i, j - i));
-        i = j;
-    }
-    return out;
+std::optional<PlyScalar> scalarNamed(std::string_view s) {
+    const auto it = std::find_if(std::begin(kScalarNames), std::end(kScalarNames),
+                                 [&](const ScalarName& n) { return n.name == s; });
+    if (it == std::end(kScalarNames)) return std::nullopt;
+    return it->type;
 }
 
 template <typename T>
@@ -95,132 +83,191 @@ inline bool nonFinite(float v) {
     return (b & 0x7F800000u) == 0x7F800000u;
 }
 
+bool startsWith(std::string_view s, std::string_view prefix) { return s.substr(0, prefix.size()) == prefix; }
+
+// ---- the 3DGS vertex schema ---------------------------------------------------------------------
+// The attributes the renderer reads from a vertex record, in the order a missing one is reported.
+enum Attr : int { kPosX = 0, kDcR = 3, kOpacity = 6, kScale0 = 7, kRotW = 10, kAttrCount = 14 };
+constexpr std::string_view kAttrNames[kAttrCount] = {"x",       "y",       "z",       "f_dc_0", "f_dc_1",
+                                                     "f_dc_2",  "opacity", "scale_0", "scale_1", "scale_2",
+                                                     "rot_0",   "rot_1",   "rot_2",   "rot_3"};
+constexpr std::string_view kShRestPrefix = "f_rest_";
+
 struct Field {
     uint32_t offset = 0;
     PlyScalar type = PlyScalar::Float32;
 };
 
-// What the header says about the vertex records once the 3DGS checks have passed.
-struct VertexPlan {
-    Field pos[3], dc[3], opacity, scale[3], rot[4];
-    std::vector<Field> rest;  // f_rest_0 .. f_rest_{n-1} in file (channel-major) order
-    uint32_t stride = 0;
-    bool allFloat = true;
+// Where a file's 3DGS records are and how one of them is read.
+struct VertexSource {
+    uint64_t first = 0;         // file offset of record 0
+    uint64_t records = 0;
+    uint32_t recordBytes = 0;
+    Field attr[kAttrCount];
+    std::vector<Field> shRest;  // f_rest_0 .. in index (channel-major) order
     int shDegree = 0;
-    uint64_t count = 0;
-    uint64_t vertexOffset = 0;   // file offset of the first vertex record
-    uint64_t trailingBytes = 0;  // list-free elements after `vertex`
-    bool trailingUnknown = false;
-    std::vector<std::string> warnings;
+    bool float32Only = true;    // every field the decode reads is float32
+    uint64_t bytesAfter = 0;    // bytes of the list-free elements that follow the vertex records
+    bool listsAfter = false;    // an element with list properties follows (its size is unknown)
+    std::vector<std::string> notes;  // one warning per skipped element
 };
 
-// planVertexDecode (ply_loader.cpp:300-401). `fileSize` bounds the elements stored before
-// `vertex` (UINT64_MAX while a stream's size is unknown).
-VertexPlan planVertices(const PlyHeader& h, const std::string& file, uint64_t fileSize) {
-    if (h.format == PlyFormat::Ascii)
-        throw FormatError(file + ": ASCII PLY is not supported (3DGS files are binary_little_endian; "
-                                 "re-export as binary)");
-    if (h.format == PlyFormat::BinaryBigEndian)
-        throw FormatError(file + ": binary_big_endian PLY is not supported (expected binary_little_endian)");
-    for (const PlyElement& e : h.elements) {
-        bool quantized = e.name == "chunk";
-        for (const PlyProperty& p : e.properties) quantized = quantized || p.name.compare(0, 7, "packed_") == 0;
-        if (quantized)
-            throw FormatError(file + ": this is a PlayCanvas compressed PLY (element 'chunk' / packed_* properties), "
-                                     "not a standard 3DGS PLY. Decompress it first (e.g. @playcanvas/splat-transform).");
-    }
-    VertexPlan plan;
-    plan.vertexOffset = h.headerBytes;
-    const PlyElement* vertex = nullptr;
-    for (const PlyElement& e : h.elements) {
+// ---- what the element list says, before any judgement ------------------------------------------
+struct ElementSurvey {
+    const PlyElement* vertex = nullptr;        // the element the records are read with
+    size_t firstVertex = SIZE_MAX;             // index of the first element named 'vertex'
+    const PlyElement* listBefore = nullptr;    // the first element with lists stored before the records
+    const PlyElement* overrunBefore = nullptr; // the first element before the records longer than the file
+    uint64_t recordsAt = 0;
+    uint64_t bytesAfter = 0;
+    bool listsAfter = false;
+    bool compressed = false;                   // PlayCanvas quantized layout
+    std::vector<std::string> skipped;
+};
+
+ElementSurvey surveyElements(const PlyHeader& h, uint64_t fileSize) {
+    ElementSurvey v;
+    v.recordsAt = h.headerBytes;
+    for (size_t i = 0; i < h.elements.size(); ++i) {
+        const PlyElement& e = h.elements[i];
+        v.compressed = v.compressed || e.name == "chunk" ||
+                       std::any_of(e.properties.begin(), e.properties.end(),
+                                   [](const PlyProperty& p) { return startsWith(p.name, "packed_"); });
         if (e.name == "vertex") {
-            vertex = &e;
+            v.vertex = &e;  // a later 'vertex' element is the one the records are read with
+            v.firstVertex = std::min(v.firstVertex, i);
             continue;
         }
-        if (!vertex) {
-            if (e.hasList) throw FormatError(file + ": element '" + e.name + "' with list properties precedes 'vertex'");
-            const uint64_t left = fileSize - std::min<uint64_t>(plan.vertexOffset, fileSize);
-            if (e.stride != 0 && e.count > left / e.stride)
-                throw FormatError(file + ": file is truncated inside element '" + e.name + "'");
-            plan.vertexOffset += e.count * e.stride;
-        } else if (e.hasList) {
-            plan.trailingUnknown = true;
-        } else {
-            plan.trailingBytes += e.count * e.stride;
+        v.skipped.push_back("skipped element '" + e.name + "' (" + std::to_string(e.count) + " records)");
+        if (v.firstVertex != SIZE_MAX) {  // stored after the vertex records
+            if (e.hasList) v.listsAfter = true;
+            else v.bytesAfter += e.count * e.stride;
+            continue;
         }
-        plan.warnings.push_back("skipped element '" + e.name + "' (" + std::to_string(e.count) + " records)");
+        if (v.listBefore || v.overrunBefore) continue;  // the first offender decides
+        if (e.hasList) {
+            v.listBefore = &e;
+            continue;
+        }
+        const uint64_t room = fileSize - std::min<uint64_t>(v.recordsAt, fileSize);
+        if (e.stride != 0 && e.count > room / e.stride) {  // (count x stride would overflow first)
+            v.overrunBefore = &e;
+            continue;
+        }
+        v.recordsAt += e.count * e.stride;
     }
-    if (!vertex) throw FormatError(file + ": no 'vertex' element");
-    if (vertex->hasList) throw FormatError(file + ": 'vertex' element has list properties (not a 3DGS file)");
-    if (vertex->count == 0) throw FormatError(file + ": 'vertex' element is empty (0 gaussians)");
-    if (vertex->count > UINT32_MAX) throw FormatError(file + ": too many gaussians");
-    plan.count = vertex->count;
-    plan.stride = vertex->stride;
+    return v;
+}
 
-    auto need = [&](const char* name) {
-        const PlyProperty* p = vertex->find(name);
-        if (!p) throw FormatError(file + ": missing required property '" + name + "'");
-        plan.allFloat = plan.allFloat && p->type == PlyScalar::Float32;
-        return Field{p->offset, p->type};
-    };
-    static const char* const kPos[3] = {"x", "y", "z"}, *const kDc[3] = {"f_dc_0", "f_dc_1", "f_dc_2"};
-    static const char* const kScale[3] = {"scale_0", "scale_1", "scale_2"};
-    static const char* const kRot[4] = {"rot_0", "rot_1", "rot_2", "rot_3"};
-    for (int c = 0; c < 3; ++c) plan.pos[c] = need(kPos[c]);
-    for (int c = 0; c < 3; ++c) plan.dc[c] = need(kDc[c]);
-    plan.opacity = need("opacity");
-    for (int c = 0; c < 3; ++c) plan.scale[c] = need(kScale[c]);
-    for (int c = 0; c < 4; ++c) plan.rot[c] = need(kRot[c]);
+// ---- the acceptance rules, in the order they are checked ----------------------------------------
+struct HeaderRule {
+    bool (*broken)(const PlyHeader&, const ElementSurvey&);
+    std::string (*explain)(const ElementSurvey&);
+};
+const HeaderRule kHeaderRules[] = {
+    {[](const PlyHeader& h, const ElementSurvey&) { return h.format == PlyFormat::Ascii; },
+     [](const ElementSurvey&) -> std::string {
+         return "ASCII PLY is not supported (3DGS files are binary_little_endian; re-export as binary)";
+     }},
+    {[](const PlyHeader& h, const ElementSurvey&) { return h.format == PlyFormat::BinaryBigEndian; },
+     [](const ElementSurvey&) -> std::string {
+         return "binary_big_endian PLY is not supported (expected binary_little_endian)";
+     }},
+    {[](const PlyHeader&, const ElementSurvey& v) { return v.compressed; },
+     [](const ElementSurvey&) -> std::string {
+         return "this is a PlayCanvas compressed PLY (element 'chunk' / packed_* properties), not a standard "
+                "3DGS PLY. Decompress it first (e.g. @playcanvas/splat-transform).";
+     }},
+    {[](const PlyHeader&, const ElementSurvey& v) { return v.listBefore != nullptr; },
+     [](const ElementSurvey& v) { return "element '" + v.listBefore->name + "' with list properties precedes 'vertex'"; }},
+    {[](const PlyHeader&, const ElementSurvey& v) { return v.overrunBefore != nullptr; },
+     [](const ElementSurvey& v) { return "file is truncated inside element '" + v.overrunBefore->name + "'"; }},
+    {[](const PlyHeader&, const ElementSurvey& v) { return v.vertex == nullptr; },
+     [](const ElementSurvey&) -> std::string { return "no 'vertex' element"; }},
+    {[](const PlyHeader&, const ElementSurvey& v) { return v.vertex->hasList; },
+     [](const ElementSurvey&) -> std::string { return "'vertex' element has list properties (not a 3DGS file)"; }},
+    {[](const PlyHeader&, const ElementSurvey& v) { return v.vertex->count == 0; },
+     [](const ElementSurvey&) -> std::string { return "'vertex' element is empty (0 gaussians)"; }},
+    {[](const PlyHeader&, const ElementSurvey& v) { return v.vertex->count > UINT32_MAX; },
+     [](const ElementSurvey&) -> std::string { return "too many gaussians"; }},
+};
 
-    // f_rest_<j>: the count sets the degree; the indices must be exactly 0..n-1
-    std::vector<const PlyProperty*> rest;
-    for (const PlyProperty& p : vertex->properties) {
-        if (p.name.compare(0, 7, "f_rest_") != 0) continue;
+// Binds the schema's attributes and the SH-rest properties of the vertex element.
+void bindAttributes(const PlyElement& vertex, const std::string& file, VertexSource& src) {
+    for (int a = 0; a < kAttrCount; ++a) {
+        const PlyProperty* p = vertex.find(kAttrNames[a]);
+        if (!p) throw FormatError(file + ": missing required property '" + std::string(kAttrNames[a]) + "'");
+        src.attr[a] = Field{p->offset, p->type};
+        src.float32Only = src.float32Only && p->type == PlyScalar::Float32;
+    }
+    // f_rest_<j>: indices 0..n-1 exactly once each; n sets the degree
+    std::vector<std::pair<size_t, const PlyProperty*>> rest;
+    for (const PlyProperty& p : vertex.properties) {
+        if (!startsWith(p.name, kShRestPrefix)) continue;
         size_t j = 0;
-        if (!parseWhole(std::string_view(p.name).substr(7), j))
+        if (!parseWhole(std::string_view(p.name).substr(kShRestPrefix.size()), j))
             throw FormatError(file + ": bad SH property name '" + p.name + "'");
-        if (j >= rest.size()) rest.resize(j + 1, nullptr);
-        if (rest[j]) throw FormatError(file + ": duplicate property '" + p.name + "'");
-        rest[j] = &p;
+        if (std::any_of(rest.begin(), rest.end(), [&](const auto& r) { return r.first == j; }))
+            throw FormatError(file + ": duplicate property '" + p.name + "'");
+        rest.emplace_back(j, &p);
     }
-    size_t present = 0;
-    for (const PlyProperty* p : rest) present += p != nullptr;
-    if (present != rest.size())
-        throw FormatError(file + ": f_rest_* indices are not contiguous (highest index " + std::to_string(rest.size() - 1) +
-                          ", but only " + std::to_string(present) + " present)");
-    plan.shDegree = shDegreeForRestCount(present);
-    if (plan.shDegree < 0)
-        throw FormatError(file + ": unexpected number of f_rest_* properties: " + std::to_string(present) +
+    std::sort(rest.begin(), rest.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    const size_t highest = rest.empty() ? 0 : rest.back().first;
+    if (!rest.empty() && highest + 1 != rest.size())
+        throw FormatError(file + ": f_rest_* indices are not contiguous (highest index " + std::to_string(highest) +
+                          ", but only " + std::to_string(rest.size()) + " present)");
+    src.shDegree = shDegreeForRestCount(rest.size());
+    if (src.shDegree < 0)
+        throw FormatError(file + ": unexpected number of f_rest_* properties: " + std::to_string(rest.size()) +
                           " (expected 0, 9, 24 or 45 for SH degree 0..3)");
-    for (const PlyProperty* p : rest) {
-        plan.rest.push_back({p->offset, p->type});
-        plan.allFloat = plan.allFloat && p->type == PlyScalar::Float32;
+    for (const auto& r : rest) {
+        src.shRest.push_back(Field{r.second->offset, r.second->type});
+        src.float32Only = src.float32Only && r.second->type == PlyScalar::Float32;
     }
-    return plan;
 }
 
-// checkPayloadSize (ply_loader.cpp:405-422)
-void checkPayload(const VertexPlan& plan, uint64_t fileSize, const std::string& file, std::vector<std::string>& warnings) {
-    const uint64_t avail = fileSize > plan.vertexOffset ? fileSize - plan.vertexOffset : 0;
-    const uint64_t need = plan.count * plan.stride;
-    if (avail < need)
-        throw FormatError(file + ": file is truncated: header declares " + std::to_string(plan.count) + " gaussians x " +
-                          std::to_string(plan.stride) + " bytes = " + std::to_string(need) +
-                          " bytes of vertex data, but only " + std::to_string(avail) + " bytes follow the header (" +
-                          std::to_string(avail / plan.stride) + " complete records)");
-    if (!plan.trailingUnknown && avail > need + plan.trailingBytes)
-        warnings.push_back(std::to_string(avail - need - plan.trailingBytes) +
-                           " unexpected trailing bytes after the last element");
-    if (!plan.trailingUnknown && avail < need + plan.trailingBytes)
-        warnings.push_back("elements after 'vertex' are truncated (ignored)");
+// The header judged for 3DGS use (loadGaussianPly's checks, ply_loader.cpp:300-401: the same
+// files are accepted and the same texts name the first problem). `fileSize` is UINT64_MAX while a
+// stream's size is unknown.
+VertexSource locateVertices(const PlyHeader& h, const std::string& file, uint64_t fileSize) {
+    const ElementSurvey survey = surveyElements(h, fileSize);
+    for (const HeaderRule& rule : kHeaderRules)
+        if (rule.broken(h, survey)) throw FormatError(file + ": " + rule.explain(survey));
+    VertexSource src;
+    src.first = survey.recordsAt;
+    src.records = survey.vertex->count;
+    src.recordBytes = survey.vertex->stride;
+    src.bytesAfter = survey.bytesAfter;
+    src.listsAfter = survey.listsAfter;
+    src.notes = survey.skipped;
+    bindAttributes(*survey.vertex, file, src);
+    return src;
 }
 
-void valueWarnings(HostScene& s, bool allFloat) {
+// The payload against the header (checkPayloadSize, ply_loader.cpp:405-422): too few bytes for
+// the records is an error; bytes that the elements after the records do not explain are warnings.
+void checkPayload(const VertexSource& src, uint64_t fileSize, const std::string& file,
+                  std::vector<std::string>& warnings) {
+    const uint64_t follow = fileSize > src.first ? fileSize - src.first : 0;
+    const uint64_t wanted = src.records * src.recordBytes;
+    if (follow < wanted)
+        throw FormatError(file + ": file is truncated: header declares " + std::to_string(src.records) +
+                          " gaussians x " + std::to_string(src.recordBytes) + " bytes = " + std::to_string(wanted) +
+                          " bytes of vertex data, but only " + std::to_string(follow) +
+                          " bytes follow the header (" + std::to_string(follow / src.recordBytes) +
+                          " complete records)");
+    if (src.listsAfter) return;  // the size of what follows is unknown: nothing to compare
+    const uint64_t explained = wanted + src.bytesAfter;
+    if (follow > explained) warnings.push_back(std::to_string(follow - explained) + " unexpected trailing bytes after the last element");
+    if (follow < explained) warnings.push_back("elements after 'vertex' are truncated (ignored)");
+}
+
+void valueWarnings(HostScene& s, bool float32Only) {
     if (s.stats.nonFiniteValues)
         s.warnings.push_back(std::to_string(s.stats.nonFiniteValues) + " NaN/Inf values in the file");
     if (s.stats.zeroQuaternions)
         s.warnings.push_back(std::to_string(s.stats.zeroQuaternions) + " zero-length quaternions replaced by identity");
-    if (!allFloat) s.warnings.push_back("non-float32 properties converted to float");
+    if (!float32Only) s.warnings.push_back("non-float32 properties converted to float");
 }
 
 struct DecodeCounters {
@@ -233,22 +280,22 @@ struct DecodeCounters {
 // reference evaluates them (ply_loader.cpp:127-150), and the SH transpose from the file's
 // channel-major f_rest[c (K-1) + k-1] to RGB triplets sh[k][c].
 template <bool kAllFloat>
-void decodeRecords(const VertexPlan& plan, const uint8_t* records, size_t n, HostScene& s, size_t first,
+void decodeRecords(const VertexSource& src, const uint8_t* records, size_t n, HostScene& s, size_t first,
                    DecodeCounters& ctr) {
     const uint32_t K = s.coeffsPerChannel();
     for (size_t r = 0; r < n; ++r) {
-        const uint8_t* rec = records + r * plan.stride;
+        const uint8_t* rec = records + r * src.recordBytes;
         auto get = [&](const Field& f) {
             const float v = kAllFloat ? readAs<float>(rec + f.offset) : toFloat(rec + f.offset, f.type);
             ctr.nonFinite += nonFinite(v) ? 1u : 0u;
             return v;
         };
         const size_t i = first + r;
-        const float px = get(plan.pos[0]), py = get(plan.pos[1]), pz = get(plan.pos[2]);
-        const float op = get(plan.opacity);
+        const float px = get(src.attr[kPosX]), py = get(src.attr[kPosX + 1]), pz = get(src.attr[kPosX + 2]);
+        const float op = get(src.attr[kOpacity]);
         float ls[3], q[4];
-        for (int c = 0; c < 3; ++c) ls[c] = get(plan.scale[c]);
-        for (int c = 0; c < 4; ++c) q[c] = get(plan.rot[c]);
+        for (int c = 0; c < 3; ++c) ls[c] = get(src.attr[kScale0 + c]);
+        for (int c = 0; c < 4; ++c) q[c] = get(src.attr[kRotW + c]);
         s.rawOpacity[i] = op;
         for (int c = 0; c < 3; ++c) s.rawLogScale[i * 3 + c] = ls[c];
         for (int c = 0; c < 4; ++c) s.rawRotation[i * 4 + c] = q[c];
@@ -275,15 +322,15 @@ void decodeRecords(const VertexPlan& plan, const uint8_t* records, size_t n, Hos
             ++ctr.zeroQuats;
         }
         float* out = &s.sh[i * K * 3];
-        for (int c = 0; c < 3; ++c) out[c] = get(plan.dc[c]);
+        for (int c = 0; c < 3; ++c) out[c] = get(src.attr[kDcR + c]);
         for (uint32_t k = 1; k < K; ++k)
-            for (uint32_t c = 0; c < 3; ++c) out[k * 3 + c] = get(plan.rest[c * (K - 1) + (k - 1)]);
+            for (uint32_t c = 0; c < 3; ++c) out[k * 3 + c] = get(src.shRest[c * (K - 1) + (k - 1)]);
     }
 }
 
-void decode(const VertexPlan& plan, const uint8_t* records, size_t n, HostScene& s, size_t first, DecodeCounters& ctr) {
-    if (plan.allFloat) decodeRecords<true>(plan, records, n, s, first, ctr);
-    else decodeRecords<false>(plan, records, n, s, first, ctr);
+void decode(const VertexSource& src, const uint8_t* records, size_t n, HostScene& s, size_t first, DecodeCounters& ctr) {
+    if (src.float32Only) decodeRecords<true>(src, records, n, s, first, ctr);
+    else decodeRecords<false>(src, records, n, s, first, ctr);
 }
 
 uint32_t hostThreads() { return std::max(1u, std::thread::hardware_concurrency()); }
@@ -363,74 +410,117 @@ int shDegreeForRestCount(size_t restCount) {
     return -1;
 }
 
-std::optional<PlyHeader> parsePlyHeader(std::string_view bytes, bool final) {
-    PlyHeader h;
-    const std::string_view window = bytes.substr(0, std::min(bytes.size(), kMaxHeaderBytes));
-    size_t pos = 0, lineNo = 0;
+namespace {
+
+// One header line split into its words (spaces and tabs separate them).
+struct HeaderLine {
+    std::string_view text;  // without the line end
+    std::vector<std::string_view> word;
+    std::string where;      // "PLY header line <n>: ", the prefix of a syntax error on it
+};
+
+void splitWords(HeaderLine& l) {
+    constexpr std::string_view kBlank = " \t";
+    for (size_t b = l.text.find_first_not_of(kBlank); b != std::string_view::npos;
+         b = l.text.find_first_not_of(kBlank, b)) {
+        const size_t e = std::min(l.text.find_first_of(kBlank, b), l.text.size());
+        l.word.push_back(l.text.substr(b, e - b));
+        b = e;
+    }
+}
+
+// What the header lines build.
+struct HeaderBuilder {
+    PlyHeader header;
     bool haveFormat = false;
-    for (;;) {
-        const size_t eol = window.find('\n', pos);
+};
+
+void onComment(HeaderBuilder& b, const HeaderLine& l) {
+    const size_t skip = l.word[0].size() + 1;  // the keyword and one separator
+    b.header.comments.emplace_back(l.text.size() > skip ? l.text.substr(skip) : std::string_view());
+}
+
+void onFormat(HeaderBuilder& b, const HeaderLine& l) {
+    static const std::pair<std::string_view, PlyFormat> kFormats[] = {
+        {"binary_little_endian", PlyFormat::BinaryLittleEndian},
+        {"binary_big_endian", PlyFormat::BinaryBigEndian},
+        {"ascii", PlyFormat::Ascii}};
+    if (l.word.size() < 2) throw FormatError(l.where + "malformed 'format' line");
+    const auto it = std::find_if(std::begin(kFormats), std::end(kFormats), [&](const auto& f) { return f.first == l.word[1]; });
+    if (it == std::end(kFormats)) throw FormatError(l.where + "unknown format '" + std::string(l.word[1]) + "'");
+    b.header.format = it->second;
+    b.haveFormat = true;
+}
+
+void onElement(HeaderBuilder& b, const HeaderLine& l) {
+    if (l.word.size() != 3) throw FormatError(l.where + "malformed 'element' line");
+    PlyElement e;
+    e.name = std::string(l.word[1]);
+    if (!parseWhole(l.word[2], e.count)) throw FormatError(l.where + "bad element count '" + std::string(l.word[2]) + "'");
+    b.header.elements.push_back(std::move(e));
+}
+
+void onProperty(HeaderBuilder& b, const HeaderLine& l) {
+    if (b.header.elements.empty()) throw FormatError(l.where + "'property' before any 'element'");
+    PlyElement& e = b.header.elements.back();
+    PlyProperty p;
+    const size_t n = l.word.size();
+    if (n == 5 && l.word[1] == "list") {  // property list <count type> <item type> <name>
+        if (!scalarNamed(l.word[2]) || !scalarNamed(l.word[3])) throw FormatError(l.where + "unknown list types");
+        p.list = true;
+        e.hasList = true;
+    } else if (n == 3) {  // property <type> <name>; every scalar counts towards the record, named or not
+        const std::optional<PlyScalar> t = scalarNamed(l.word[1]);
+        if (!t) throw FormatError(l.where + "unknown property type '" + std::string(l.word[1]) + "'");
+        p.type = *t;
+        p.offset = e.stride;
+        e.stride += scalarBytes(p.type);
+    } else {
+        throw FormatError(l.where + "malformed 'property' line");
+    }
+    p.name = std::string(l.word[n - 1]);
+    e.properties.push_back(std::move(p));
+}
+
+using LineHandler = void (*)(HeaderBuilder&, const HeaderLine&);
+const std::pair<std::string_view, LineHandler> kHeaderKeywords[] = {
+    {"comment", onComment}, {"obj_info", onComment}, {"format", onFormat},
+    {"element", onElement}, {"property", onProperty}};
+
+}  // namespace
+
+std::optional<PlyHeader> parsePlyHeader(std::string_view bytes, bool final) {
+    // lines are searched for in the first kMaxHeaderBytes bytes only
+    const std::string_view window = bytes.substr(0, std::min(bytes.size(), kMaxHeaderBytes));
+    HeaderBuilder b;
+    size_t next = 0;
+    for (size_t lineNo = 1;; ++lineNo) {
+        const size_t eol = window.find('\n', next);
         if (eol == std::string_view::npos) {
             if (!final && bytes.size() < kMaxHeaderBytes) return std::nullopt;  // more bytes to come
-            throw FormatError(lineNo == 0 ? "not a PLY file (empty or no header)"
+            throw FormatError(lineNo == 1 ? "not a PLY file (empty or no header)"
                                           : "PLY header has no 'end_header' line (file truncated or not a PLY)");
         }
-        std::string_view line = bytes.substr(pos, eol - pos);
-        if (!line.empty() && line.back() == '\r') line.remove_suffix(1);  // CRLF headers
-        pos = eol + 1;
-        ++lineNo;
-        const std::string at = "PLY header line " + std::to_string(lineNo) + ": ";
+        HeaderLine l;
+        l.text = bytes.substr(next, eol - next);
+        if (!l.text.empty() && l.text.back() == '\r') l.text.remove_suffix(1);  // CRLF line ends
+        next = eol + 1;
         if (lineNo == 1) {
-            if (line != "ply") throw FormatError("not a PLY file (first line is not 'ply')");
+            if (l.text != "ply") throw FormatError("not a PLY file (first line is not 'ply')");
             continue;
         }
-        const std::vector<std::string_view> w = words(line);
-        if (w.empty()) continue;
-        const std::string_view key = w[0];
-        if (key == "end_header") {
-            if (!haveFormat) throw FormatError("PLY header has no 'format' line");
-            h.headerBytes = pos;
-            return h;
+        l.where = "PLY header line " + std::to_string(lineNo) + ": ";
+        splitWords(l);
+        if (l.word.empty()) continue;
+        if (l.word[0] == "end_header") {
+            if (!b.haveFormat) throw FormatError("PLY header has no 'format' line");
+            b.header.headerBytes = next;
+            return std::move(b.header);
         }
-        if (key == "comment" || key == "obj_info") {
-            h.comments.emplace_back(line.size() > key.size() + 1 ? line.substr(key.size() + 1) : std::string_view());
-        } else if (key == "format") {
-            if (w.size() < 2) throw FormatError(at + "malformed 'format' line");
-            if (w[1] == "binary_little_endian") h.format = PlyFormat::BinaryLittleEndian;
-            else if (w[1] == "binary_big_endian") h.format = PlyFormat::BinaryBigEndian;
-            else if (w[1] == "ascii") h.format = PlyFormat::Ascii;
-            else throw FormatError(at + "unknown format '" + std::string(w[1]) + "'");
-            haveFormat = true;
-        } else if (key == "element") {
-            if (w.size() != 3) throw FormatError(at + "malformed 'element' line");
-            PlyElement e;
-            e.name = std::string(w[1]);
-            if (!parseWhole(w[2], e.count)) throw FormatError(at + "bad element count '" + std::string(w[2]) + "'");
-            h.elements.push_back(std::move(e));
-        } else if (key == "property") {
-            if (h.elements.empty()) throw FormatError(at + "'property' before any 'element'");
-            PlyElement& e = h.elements.back();
-            PlyProperty p;
-            if (w.size() == 5 && w[1] == "list") {
-                PlyScalar countType, itemType;
-                if (!scalarFromName(w[2], countType) || !scalarFromName(w[3], itemType))
-                    throw FormatError(at + "unknown list types");
-                p.list = true;
-                p.name = std::string(w[4]);
-                e.hasList = true;
-            } else if (w.size() == 3) {
-                if (!scalarFromName(w[1], p.type))
-                    throw FormatError(at + "unknown property type '" + std::string(w[1]) + "'");
-                p.name = std::string(w[2]);
-                p.offset = e.stride;  // unknown names count towards the record size too
-                e.stride += scalarBytes(p.type);
-            } else {
-                throw FormatError(at + "malformed 'property' line");
-            }
-            e.properties.push_back(std::move(p));
-        } else {
-            throw FormatError(at + "unknown keyword '" + std::string(key) + "'");
-        }
+        const auto h = std::find_if(std::begin(kHeaderKeywords), std::end(kHeaderKeywords),
+                                    [&](const auto& k) { return k.first == l.word[0]; });
+        if (h == std::end(kHeaderKeywords)) throw FormatError(l.where + "unknown keyword '" + std::string(l.word[0]) + "'");
+        h->second(b, l);
     }
 }
 
@@ -527,26 +617,26 @@ HostScene loadPly(const uint8_t* bytes, size_t size, const std::string& file) {
         throw FormatError(file + ": " + e.what());
     }
     scene.comments = header->comments;
-    const VertexPlan plan = planVertices(*header, file, size);
-    scene.warnings = plan.warnings;
-    checkPayload(plan, size, file, scene.warnings);
-    scene.shDegree = plan.shDegree;
+    const VertexSource src = locateVertices(*header, file, size);
+    scene.warnings = src.notes;
+    checkPayload(src, size, file, scene.warnings);
+    scene.shDegree = src.shDegree;
     scene.timings.headerMs = msSince(tHeader);
 
     const auto tDecode = Clock::now();
-    const size_t n = size_t(plan.count);
+    const size_t n = size_t(src.records);
     scene.resize(n);
-    const uint8_t* records = bytes + plan.vertexOffset;
+    const uint8_t* records = bytes + src.first;
     // contiguous ranges, one per host thread (16384 records at least per thread)
     const size_t threads = std::clamp<size_t>(n / 16384, 1, hostThreads());
     std::vector<DecodeCounters> ctr(threads);
     if (threads == 1) {
-        decode(plan, records, n, scene, 0, ctr[0]);
+        decode(src, records, n, scene, 0, ctr[0]);
     } else {
         std::vector<std::thread> pool;
         for (size_t t = 0; t < threads; ++t) {
             const size_t b = n * t / threads, e = n * (t + 1) / threads;
-            pool.emplace_back([&, t, b, e] { decode(plan, records + b * plan.stride, e - b, scene, b, ctr[t]); });
+            pool.emplace_back([&, t, b, e] { decode(src, records + b * src.recordBytes, e - b, scene, b, ctr[t]); });
         }
         for (auto& th : pool) th.join();
     }
@@ -558,7 +648,7 @@ HostScene loadPly(const uint8_t* bytes, size_t size, const std::string& file) {
         scene.stats.nonFiniteValues += c.nonFinite;
         scene.stats.zeroQuaternions += c.zeroQuats;
     }
-    valueWarnings(scene, plan.allFloat);
+    valueWarnings(scene, src.float32Only);
     scene.timings.statsMs = msSince(tStats);
     scene.timings.totalMs = msSince(t0);
     return scene;
@@ -586,7 +676,7 @@ struct PlyStream::State {
     std::string headerText;  // the first bytes, until the header parses
     bool headerDone = false, done = false, failed = false;
     PlyHeader header;
-    VertexPlan plan;
+    VertexSource src;
     uint64_t vertexEnd = 0;
     std::vector<uint8_t> pending;  // whole records waiting for a batch decode
     size_t pendingBytes = 0;
@@ -600,25 +690,25 @@ struct PlyStream::State {
         headerDone = true;
         info.comments = header.comments;
         // with the total size known, a truncated file fails before any record is decoded
-        plan = planVertices(header, file, totalBytes ? totalBytes : UINT64_MAX);
+        src = locateVertices(header, file, totalBytes ? totalBytes : UINT64_MAX);
         if (totalBytes) {
             std::vector<std::string> later;  // reported by finish()
-            checkPayload(plan, totalBytes, file, later);
+            checkPayload(src, totalBytes, file, later);
         }
-        const uint64_t vertexBytes = plan.count * plan.stride;
-        vertexEnd = plan.vertexOffset > UINT64_MAX - vertexBytes ? UINT64_MAX : plan.vertexOffset + vertexBytes;
-        info.count = uint32_t(plan.count);
-        info.shDegree = plan.shDegree;
+        const uint64_t vertexBytes = src.records * src.recordBytes;
+        vertexEnd = src.first > UINT64_MAX - vertexBytes ? UINT64_MAX : src.first + vertexBytes;
+        info.count = uint32_t(src.records);
+        info.shDegree = src.shDegree;
         info.timings.headerMs = msSince(start);
-        pending.resize(size_t(std::min<uint64_t>(plan.count, batchCapacity)) * plan.stride);
-        batch.shDegree = plan.shDegree;
+        pending.resize(size_t(std::min<uint64_t>(src.records, batchCapacity)) * src.recordBytes);
+        batch.shDegree = src.shDegree;
         batch.comments = header.comments;
         if (onHeader) onHeader(info);
     }
 
     // the bytes [fileOffset, fileOffset + size) of the file; only vertex records are kept
     void payload(const uint8_t* data, size_t size, uint64_t fileOffset) {
-        const uint64_t b = std::max<uint64_t>(fileOffset, plan.vertexOffset);
+        const uint64_t b = std::max<uint64_t>(fileOffset, src.first);
         const uint64_t e = std::min<uint64_t>(fileOffset + size, vertexEnd);
         for (uint64_t at = b; at < e;) {
             const size_t take = size_t(std::min<uint64_t>(e - at, pending.size() - pendingBytes));
@@ -631,10 +721,10 @@ struct PlyStream::State {
     }
 
     void flush() {
-        const size_t m = pendingBytes / plan.stride;
+        const size_t m = pendingBytes / src.recordBytes;
         const auto t0 = Clock::now();
         batch.resize(m);
-        decode(plan, pending.data(), m, batch, 0, counters);
+        decode(src, pending.data(), m, batch, 0, counters);
         decodeMs += msSince(t0);
         if (onBatch) onBatch(uint32_t(decoded), batch);
         decoded += m;
@@ -713,12 +803,12 @@ void PlyStream::finish() {
             throw std::runtime_error(s.file + ": stream ended after " + std::to_string(s.received) + " of " +
                                      std::to_string(s.totalBytes) + " bytes");
         // the whole-file checks with the real size: the same errors and warnings
-        s.plan = planVertices(s.header, s.file, s.received);
-        s.info.warnings = s.plan.warnings;
-        checkPayload(s.plan, s.received, s.file, s.info.warnings);
+        s.src = locateVertices(s.header, s.file, s.received);
+        s.info.warnings = s.src.notes;
+        checkPayload(s.src, s.received, s.file, s.info.warnings);
         s.info.stats.nonFiniteValues = s.counters.nonFinite;
         s.info.stats.zeroQuaternions = s.counters.zeroQuats;
-        valueWarnings(s.info, s.plan.allFloat);
+        valueWarnings(s.info, s.src.float32Only);
         s.info.timings.decodeMs = s.decodeMs;
         s.info.timings.totalMs = msSince(s.start);
         s.done = true;

@@ -449,6 +449,7 @@ struct GsrRenderer {
     uint32_t width = 0, height = 0, tilesX = 0, tilesY = 0;
     uint32_t passesUpper = 0;
     DevBuf ranges, image, rgb8;
+    DevBuf tileStats, testedPairs;  // the stats build: kTileStatWords per frame tile, one 64-bit total
     // readback slots (2 frames late)
     // Per frame slot: the control readback, the camera (pinned, copied to the slot's device
     // copy by the frame itself), and the frame captured as a CUDA graph.
@@ -645,6 +646,11 @@ struct GsrRenderer {
         const uint32_t tileCount = totalTiles;
         GSR_CUDA(ranges.alloc(size_t(tileCount) * 8));
         GSR_CUDA(cudaMemset(ranges.p, 0, ranges.bytes));
+        if (settings.tile_stats) {
+            GSR_CUDA(tileStats.alloc(size_t(tileCount) * kTileStatWords * 4));
+            GSR_CUDA(cudaMemset(tileStats.p, 0, tileStats.bytes));
+            GSR_CUDA(testedPairs.alloc(8));
+        }
         GSR_CUDA(image.alloc(size_t(pixels) * imageBytes()));
         if (withRgb8()) GSR_CUDA(rgb8.alloc(size_t(pixels) * 3));
         else rgb8.release();
@@ -914,6 +920,11 @@ struct GsrRenderer {
         ra.count = scene.count;
         ra.ctl = ctl;
         ra.plan = sortPlan;
+        if (settings.tile_stats) {
+            ra.tileStats = tileStats.as<uint32_t>();
+            ra.testedPairs = testedPairs.as<unsigned long long>();
+            GSR_CUDA(cudaMemsetAsync(testedPairs.p, 0, 8, stream));
+        }
         GSR_CUDA(launchRanges(ra, l.capacity, stream));
         mark(stream);
         if (splitViews) {
@@ -1260,6 +1271,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
         return fail(GSR_ERROR_INVALID_ARGUMENT, "render splat mode %u", settings->render_splat);
     if (settings->raster_schedule > GSR_RASTER_PERSISTENT)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "raster schedule %u", settings->raster_schedule);
+    if (settings->tile_stats > 1 || (settings->tile_stats && settings->sort_window > 0))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "tile_stats %u (0 or 1, not with sort_window)", settings->tile_stats);
     if (settings->sort_digit_bits != 0 && settings->sort_digit_bits != 8)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "sort digit bits %u (8)", settings->sort_digit_bits);
     GSR_CUDA(r->control.alloc(sizeof(DeviceControl)));
@@ -1452,6 +1465,16 @@ int gsr_read_packed_splats(GsrRenderer* r, uint32_t* words, uint32_t* rectsOut, 
 }
 
 int gsr_read_image(GsrRenderer* r, float* rgba, uint8_t* rgb) { return gsr_read_view_image(r, 0, rgba, rgb); }
+
+int gsr_read_tile_stats(GsrRenderer* r, uint32_t* stats, uint32_t tiles, uint64_t* testedPairs) {
+    if (!r || !stats) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    if (!r->settings.tile_stats || !r->tileStats.p) return fail(GSR_ERROR_INVALID_ARGUMENT, "renderer built without tile_stats");
+    if (tiles != r->totalTiles) return fail(GSR_ERROR_INVALID_ARGUMENT, "tiles %u != the frame's %u", tiles, r->totalTiles);
+    GSR_CUDA(cudaDeviceSynchronize());
+    GSR_CUDA(cudaMemcpy(stats, r->tileStats.p, size_t(tiles) * kTileStatWords * 4, cudaMemcpyDeviceToHost));
+    if (testedPairs) GSR_CUDA(cudaMemcpy(testedPairs, r->testedPairs.p, 8, cudaMemcpyDeviceToHost));
+    return GSR_OK;
+}
 
 int gsr_render_views(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* stream) {
     if (!r || !cameras) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");

@@ -87,7 +87,7 @@ class CSettings(C.Structure):
         ("adaptive_initial_entries", C.c_uint32), ("max_sh_degree", C.c_int32), ("output_format", C.c_uint32),
         ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("raster_schedule", C.c_uint32),
         ("list_mode", C.c_uint32), ("render_splat", C.c_uint32), ("sort_window", C.c_uint32),
-        ("sort_digit_bits", C.c_uint32), ("reserved", C.c_uint32 * 2),
+        ("sort_digit_bits", C.c_uint32), ("tile_stats", C.c_uint32), ("reserved", C.c_uint32 * 1),
     ]
 
 
@@ -235,6 +235,7 @@ def load(build_if_missing: bool = True) -> C.CDLL:
                                    C.POINTER(u32), u32, u32, C.POINTER(TuneResult)]),
         "gsr_autotune_space": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(CSettings), vp, C.POINTER(SplatCamera), u32,
                                          C.POINTER(TuneSpace), u32, C.POINTER(TuneResult)]),
+        "gsr_read_tile_stats": (C.c_int, [vp, vp, u32, C.POINTER(C.c_uint64)]),
         "gsr_scan": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_scan_static": (C.c_int, [vp, vp, vp, vp, u32, u32, vp]),
         "gsr_sort_pairs": (C.c_int, [vp, vp, vp, u32, u32, vp]),
@@ -298,6 +299,7 @@ class Settings:
     target: str = "rgba32f"  # the output image: rgba32f, rgba16f or rgba8 (rgb8 adds the 8-bit RGB image)
     sort_window: int = 0  # StopThePop per-pixel window K (0 = off, at most 64)
     sort_digit_bits: int = 0  # radix digit width of the list sort (0 = 8)
+    tile_stats: bool = False  # the instrumented rasterizer with per-tile statistics (read_tile_stats)
 
     def to_c(self) -> CSettings:
         s = CSettings()
@@ -321,6 +323,7 @@ class Settings:
         s.render_splat = RENDER_SPLATS[self.render_splat]
         s.sort_window = self.sort_window
         s.sort_digit_bits = self.sort_digit_bits
+        s.tile_stats = int(self.tile_stats)
         return s
 
 
@@ -555,6 +558,16 @@ class Renderer:
         out8 = np.zeros((self.height, self.width, 3), np.uint8) if rgb8 else None
         check(load().gsr_read_image(self._h, rgba.ctypes.data, out8.ctypes.data if rgb8 else None))
         return (rgba, out8) if rgb8 else rgba
+
+    TILE_STATS = ("list_length", "fetched", "evaluated", "blended", "terminated", "lane_slots", "max_depth", "pixels")
+
+    def read_tile_stats(self):
+        """The last frame's per-tile counters (tiles, 8) in TileStat order and the pairs tested."""
+        tiles = sum(L.tiles_x * L.tiles_y for L in self.view_layouts())
+        out = np.zeros((tiles, 8), np.uint32)
+        tested = C.c_uint64()
+        check(load().gsr_read_tile_stats(self._h, out.ctypes.data, tiles, C.byref(tested)))
+        return out, tested.value
 
     def set_timing(self, enabled: bool):
         check(load().gsr_renderer_set_timing(self._h, int(enabled)))

@@ -160,7 +160,10 @@ typedef struct GsrSettings {
                                           0 = off (the list's order), 1..64 */
     uint32_t sort_digit_bits;          /* radix digit width of the list sort; 0 = 8 (the reference's
                                           GpuRadixSort digits, gpu_radix_sort.h:38-122) */
-    uint32_t reserved[2];
+    uint32_t tile_stats;               /* 1: the instrumented rasterizer with per-tile statistics
+                                          (TileSettings::stats, splat_tile_renderer.h:102); not with
+                                          sort_window; read with gsr_read_tile_stats */
+    uint32_t reserved[1];
 } GsrSettings;
 
 /* The per-entry record that key emission and the rasterizer read (RenderSplatMode,
@@ -432,6 +435,17 @@ int gsr_read_packed_splats(GsrRenderer* r, uint32_t* words, uint32_t* rects, uin
                            uint32_t n);
 /* readBackImage (splat_tile_renderer.h:194): rgba float4[W*H] and/or rgb8 uint8[W*H*3]. */
 int gsr_read_image(GsrRenderer* r, float* rgba, uint8_t* rgb8);
+/* The per-tile counters of the last frame of a renderer created with tile_stats = 1, in the
+ * reference's TileStat order (splat_tile_renderer.h:131-141), GSR_TILE_STAT_COUNT words per frame
+ * tile: list length, entries fetched before the tile stopped, (pixel, splat) pairs evaluated
+ * (entries a pixel visits until it terminates, all of them when it does not), pairs blended,
+ * pixels terminated (T < 1e-4), lane slots of the blend loop (its warp iterations x 32), the
+ * largest evaluated count of a pixel, pixels inside the image. tested_pairs (may be NULL)
+ * receives the pairs this rasterizer computed alpha for (a pixel still blending and a record
+ * whose cutoff ellipse meets that pixel's warp strip). Synchronizes; `tiles` must be the
+ * frame's tile count over all views. */
+#define GSR_TILE_STAT_COUNT 8u
+int gsr_read_tile_stats(GsrRenderer* r, uint32_t* stats, uint32_t tiles, uint64_t* tested_pairs);
 /* Per-pass device time of the last frame in ms (GpuProfiler scopes), when timing is on: 5 passes
  * in global mode, 7 in binning mode (its front as preprocess, depth sort, scan + emission). */
 int gsr_renderer_set_timing(GsrRenderer* r, int enabled);

@@ -222,6 +222,34 @@ def error_cases():
          "bad element count"),
         ("no format line", b"ply\nelement vertex 1\nend_header\n", "no 'format' line"),
         ("empty file", b"", "not a PLY"),
+        # several problems in one file: the first check in the loader's order names it
+        ("list element before an oversized one",
+         ("ply\nformat binary_little_endian 1.0\nelement face 1\nproperty list uchar int idx\n"
+          "element big 99999999\nproperty double a\n" + deg0_header(1)[36:]).encode() + deg0_record(), "precedes"),
+        ("oversized element before a list element",
+         ("ply\nformat binary_little_endian 1.0\nelement big 99999999\nproperty double a\n"
+          "element face 1\nproperty list uchar int idx\n" + deg0_header(1)[36:]).encode() + deg0_record(),
+         "truncated inside element 'big'"),
+        ("list element and no vertex", b"ply\nformat ascii 1.0\nelement face 1\nproperty list uchar int i\nend_header\n",
+         "ASCII"),
+        ("list element without any vertex",
+         b"ply\nformat binary_little_endian 1.0\nelement face 1\nproperty list uchar int i\nend_header\n", "precedes"),
+        ("compressed and big endian",
+         b"ply\nformat binary_big_endian 1.0\nelement chunk 1\nproperty float a\nend_header\n", "big_endian"),
+        ("missing property and a bad f_rest count",
+         (no_opacity.replace("end_header\n", "property float f_rest_0\nend_header\n")).encode() + bytes(14 * 4),
+         "'opacity'"),
+        ("bad f_rest name before a duplicate",
+         ("ply\nformat binary_little_endian 1.0\nelement vertex 1\n" + DEG0_PROPS
+          + "property float f_rest_x\nproperty float f_rest_0\nproperty float f_rest_0\nend_header\n").encode(),
+         "bad SH property name 'f_rest_x'"),
+        ("duplicate before a bad f_rest name",
+         ("ply\nformat binary_little_endian 1.0\nelement vertex 1\n" + DEG0_PROPS
+          + "property float f_rest_1\nproperty float f_rest_1\nproperty float f_rest_\nend_header\n").encode(),
+         "duplicate"),
+        ("empty vertex in a list-free file with trailing data",
+         ("ply\nformat binary_little_endian 1.0\nelement vertex 0\n" + DEG0_PROPS
+          + "element extra 2\nproperty float a\nend_header\n").encode() + bytes(8), "empty"),
     ]
 
 
@@ -279,6 +307,14 @@ def test_hand_written_identical_to_reference_loader(io, ref, tmp_path):
     vals[::67, 7] = np.float32(-90.0)
     vals[::61, 2] = np.float32("nan")
     cases["random.ply"] = deg0_header(n).encode() + vals.tobytes()
+    # elements around the vertex records: list-free before, lists after, a second 'vertex'
+    # element (the records are read at the first one's place with the last one's layout)
+    pre = "element pre 2\nproperty short a\nproperty uchar b\n"
+    cases["around.ply"] = (("ply\nformat binary_little_endian 1.0\ncomment two vertex elements\n" + pre
+                            + deg0_header(3)[36:-11] + "element post 1\nproperty list uchar int i\n"
+                            + deg0_header(2)[36:]).encode() + bytes(6) + vals[:3].tobytes() + bytes(9))
+    cases["trailing.ply"] = (deg0_header(2)[:-11] + "element tail 3\nproperty float t\nend_header\n").encode() \
+        + vals[:2].tobytes() + bytes(12 + 5)
     for name, data in cases.items():
         p = tmp_path / name
         p.write_bytes(data)
@@ -335,11 +371,22 @@ def test_stream_equals_whole_file(io, name, chunk, total_known, capacity):
     assert info.stats["zero_quaternions"] == whole.stats["zero_quaternions"]
 
 
+# A stream of unknown size cannot tell that an element before the records overruns the file
+# until the stream ends, so it names the next problem of the header instead (the reference's
+# stream decoder runs the same check with an unknown size).
+SIZE_DEPENDENT = {"oversized element before a list element"}
+
+
 @pytest.mark.parametrize("case", range(len(error_cases())))
 def test_stream_errors_match_whole_file(io, case):
     what, data, _ = error_cases()[case]
     with pytest.raises(io.PlyError) as whole:
         io.load_ply_bytes(data, "bad.ply")
+    if what in SIZE_DEPENDENT:
+        with pytest.raises(io.PlyError) as e:
+            io.PlyStream("bad.ply", 0).push(data)
+        assert "precedes 'vertex'" in str(e.value)
+        return
     for chunk in (1, 64, 1 << 30):
         with pytest.raises(io.PlyError) as e:
             st = io.PlyStream("bad.ply", 0)
