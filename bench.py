@@ -620,11 +620,11 @@ def settle_and_tune(G, gs, cams, args, model=None, depths=(1, 2, 4, 8, 16), tile
     return G.autotune(gs, st, G.camera_array(sel), depths=depths, frames=3, model=model, tile_sizes=tile_sizes)
 
 
-def renderer_for(G, gs, args, tuned=None, model=None):
+def renderer_for(G, gs, args, tuned=None, model=None, gather=None):
     t = tuned or {}
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.budget_mb,
                                   raster_schedule=t.get("raster_schedule", "auto"), tile_size=t.get("tile_size", 16),
-                                  use_graph=True))
+                                  use_graph=True, raster_gather=gather or args.gather))
     if model is not None:
         r.set_color_model(model)
     return r
@@ -656,6 +656,14 @@ def run_1080p(G, args, dist, sampler, stream_obj, peak):
     r = renderer_for(G, gs, args)
     plain = time_form(r, plain_frames, args, dist, sampler, stream_obj)
     passes, ctl = pass_profile(r, plain_frames, stream_obj)
+    # the rasterizer's two batch gathers on the same frames (pass times; the images are equal)
+    ab = {}
+    for gather in ("cp.async", "tma"):
+        rg = renderer_for(G, gs, args, gather=gather)
+        gp, _ = pass_profile(rg, plain_frames, stream_obj)
+        rg.close()
+        ab[gather] = gp.get("render tiles")
+    plain["render_ms_by_gather"] = ab
     tiles = ((1920 + 15) // 16) * ((1080 + 15) // 16)
     roof = roofline(passes, ctl, fmt, scene.count, tiles, peak[0], peak[1])
     roof["traffic"] = int(TRAFFIC_PLAIN_1080P_CAPTURE)
@@ -1010,6 +1018,8 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="views per frame of the batched forms (0: autotuned)")
     ap.add_argument("--budget-mb", type=int, default=16384)
     ap.add_argument("--mlp-steps", type=int, default=2000)
+    ap.add_argument("--gather", default="default", choices=["default", "cp.async", "tma"],
+                    help="how the rasterizer stages each batch of records (GsrSettings.raster_gather)")
     ap.add_argument("--check-launch", action="store_true",
                     help="plumbing self-check: ranks, view partition and gather, no GPU work, no timing")
     args = ap.parse_args()

@@ -25,6 +25,8 @@
 // FMA contraction and the hardware exp2 make the float image differ from the CPU reference's
 // in the last bits (and, for pairs within an ulp of the 1/255 or 1e-4 thresholds, by one such
 // pair's contribution); tests bound it: float PSNR > 60 dB and the 8-bit image within 1/255.
+#include <cuda.h>  // CUtensorMap (the type only; maps are encoded by the host)
+
 #include "gsr_device.cuh"
 #include "kernels.cuh"
 #include "render_splat.cuh"
@@ -98,18 +100,66 @@ __device__ __forceinline__ uint32_t stripMask(float cx, float cy, float A, float
     return mask;
 }
 
-// N = the batch (one entry per thread of the tile's block)
-template <int N>
-struct RenderShared {
-    // gathered records, double-buffered: full 3 x 16 B, p32 2 x 16 B, p24 3 x 8 B (as uint2 rows of
-    // N in the first half of the area)
+// How a batch's records reach shared memory.
+constexpr int kGatherCpAsync = 0;  // every thread copies its record with 16-byte cp.async
+constexpr int kGatherTma = 1;      // one warp gathers four records per cp.async.bulk.tensor tile::gather4
+
+// The staging area of a batch (double-buffered). cp.async: full 3 x 16 B, p32 2 x 16 B, p24
+// 3 x 8 B per record (as uint2 rows of N in the first half of the area). TMA: quads of four
+// 48-byte records as gather4 writes them, each quad in a 256-byte slot so that every
+// destination is 128-byte aligned; one mbarrier per buffer and its completed uses (the phase).
+template <int N, int GATHER>
+struct StageArea {
     float4 raw[2][3][N];
+};
+template <int N>
+struct StageArea<N, kGatherTma> {
+    alignas(128) unsigned char quad[2][N / 4][256];
+    uint64_t bar[2];
+    uint32_t uses[2];
+};
+
+// N = the batch (one entry per thread of the tile's block)
+template <int N, int GATHER = kGatherCpAsync>
+struct RenderShared {
+    StageArea<N, GATHER> st;
     float4 conic[N];      // a', b', c' (pre-scaled), opacity
     uint32_t strips[N];   // the warp strips the cutoff ellipse meets (stripMask)
     float4 color[N];      // r, g, b, -
     float2 center[N];
     uint32_t tile;        // persistent schedule: the block's current tile
 };
+
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+// Four records (rows of the 2-D tensor map over the frame's record array: 12 fp32 columns, one
+// row per record) into 192 contiguous bytes at dst, completed on bar. Column 0 is the only
+// x coordinate used (16-byte aligned); the box is one row high.
+__device__ __forceinline__ void tmaGather4(void* dst, const CUtensorMap* map, const uint32_t (&row)[4], uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile::gather4.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+        :: "r"(smemAddr(dst)), "l"(map), "r"(0), "r"(row[0]), "r"(row[1]), "r"(row[2]), "r"(row[3]), "r"(smemAddr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbarDone(uint64_t* bar, uint32_t parity) {
+    uint32_t done = 0;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+                 : "=r"(done) : "r"(smemAddr(bar)), "r"(parity) : "memory");
+    return done != 0;
+}
+
+// Bounded wait for a buffer's gathers; on expiry the frame is marked GSR_CONTROL_TIMEOUT (site
+// kWaitGather) and its image is untrusted.
+__device__ __forceinline__ void mbarWaitBounded(uint64_t* bar, uint32_t parity, DeviceControl* ctl) {
+    for (uint32_t spins = 0; !mbarDone(bar, parity); ++spins) {
+        if (spins >= kSpinLimit) {
+            if ((threadIdx.x & 31) == 0) reportTimeout(ctl, kWaitGather);
+            return;
+        }
+    }
+}
 
 // The view holding frame tile t: the last view whose tileBase <= t (views are in tile order).
 __device__ __forceinline__ uint32_t viewOfTile(const RenderArgs& a, uint32_t t) {
@@ -228,9 +278,12 @@ __device__ __forceinline__ void windowPush(SortWindow<CAP>& q, uint32_t K, float
 // keeps the reference's meaning, the list entries a pixel visits until it terminates (all of
 // them when it does not); "tested" are the pairs this kernel computed alpha for (a pixel still
 // blending and a record whose cutoff ellipse meets the pixel's warp strip).
-template <int MODE, int CAP, int TILE, bool STATS>
-__device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TILE * TILE>& sm,
-                                           float4 (*ray)[3][TILE * TILE], uint32_t tile) {
+// GATHER: how the batch reaches shared memory (kGatherCpAsync or kGatherTma; TMA only with the
+// full records, no window and no statistics); map = the tensor map of the record array (TMA).
+template <int MODE, int CAP, int TILE, bool STATS, int GATHER>
+__device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TILE * TILE, GATHER>& sm,
+                                           float4 (*ray)[3][TILE * TILE], uint32_t tile, const CUtensorMap* map) {
+    static_assert(GATHER == kGatherCpAsync || (MODE == kRenderSplatFull && CAP == 0 && !STATS), "the TMA gather");
     constexpr uint32_t kThreads = TILE * TILE, kStripW = 8, kRows = 4, kStripsX = TILE / kStripW;
     static_assert(kThreads <= kRenderThreads && kStripW * kRows == 32 && TILE % kStripW == 0, "tile shape");
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
@@ -261,38 +314,78 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
     float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
     bool done = !inside;
 
+    // TMA: the buffers' mbarrier phases, the same in every thread (each thread counts the uses)
+    uint32_t phase0 = 0, phase1 = 0;
+    if constexpr (GATHER == kGatherTma) {
+        phase0 = sm.st.uses[0];
+        phase1 = sm.st.uses[1];
+    }
     auto issue = [&](uint32_t start, int buf) {
-        const uint32_t j = start + tid;
-        if (j < range.y) {
-            uint32_t g = packed ? uint32_t(__ldg(&packedKeys[j]) & indexMask) : __ldg(&values[j]);
-            if (g >= a.count) {
-                atomicOr(&a.ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
-                g = 0;
+        if constexpr (GATHER == kGatherTma) {
+            // warp 0 reads the batch's gaussian indices and gathers the records four at a time
+            if (warp != 0) return;
+            const uint32_t n = range.y - start < kThreads ? range.y - start : kThreads;
+            const uint32_t quads = (n + 3u) / 4u;
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(smemAddr(&sm.st.bar[buf])),
+                             "r"(quads * 192u) : "memory");
+            __syncwarp();
+            for (uint32_t q = lane; q < quads; q += 32u) {
+                uint32_t row[4];
+#pragma unroll
+                for (uint32_t r = 0; r < 4; ++r) {
+                    const uint32_t slot = 4u * q + r;
+                    const uint32_t j = start + (slot < n ? slot : n - 1u);  // a short last quad repeats its last record
+                    uint32_t g = packed ? uint32_t(__ldg(&packedKeys[j]) & indexMask) : __ldg(&values[j]);
+                    if (g >= a.count) {
+                        atomicOr(&a.ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
+                        g = 0;
+                    }
+                    row[r] = view * a.count + g;  // the host uses TMA only while V N < 2^31
+                }
+                tmaGather4(&sm.st.quad[buf][q][0], map, row, &sm.st.bar[buf]);
             }
-            if constexpr (mode == kRenderSplatFull) {
-                const float4* rec = records + size_t(g) * 3;
-                cpAsync16(&sm.raw[buf][0][tid], rec);
-                cpAsync16(&sm.raw[buf][1][tid], rec + 1);
-                cpAsync16(&sm.raw[buf][2][tid], rec + 2);
-            } else if constexpr (mode == kRenderSplatP32) {
-                const uint4* rec = records32 + size_t(g) * 2;
-                cpAsync16(&sm.raw[buf][0][tid], rec);
-                cpAsync16(&sm.raw[buf][1][tid], rec + 1);
-            } else {  // 24-byte records start on 8-byte boundaries
-                const uint2* rec = records24 + size_t(g) * 3;
-                uint2* dst = reinterpret_cast<uint2*>(&sm.raw[buf][0][0]);
-                cpAsync8(&dst[tid], rec);
-                cpAsync8(&dst[kThreads + tid], rec + 1);
-                cpAsync8(&dst[2 * kThreads + tid], rec + 2);
+        } else {
+            const uint32_t j = start + tid;
+            if (j < range.y) {
+                uint32_t g = packed ? uint32_t(__ldg(&packedKeys[j]) & indexMask) : __ldg(&values[j]);
+                if (g >= a.count) {
+                    atomicOr(&a.ctl->c.status, uint32_t(GSR_CONTROL_BOUNDS));
+                    g = 0;
+                }
+                if constexpr (mode == kRenderSplatFull) {
+                    const float4* rec = records + size_t(g) * 3;
+                    cpAsync16(&sm.st.raw[buf][0][tid], rec);
+                    cpAsync16(&sm.st.raw[buf][1][tid], rec + 1);
+                    cpAsync16(&sm.st.raw[buf][2][tid], rec + 2);
+                } else if constexpr (mode == kRenderSplatP32) {
+                    const uint4* rec = records32 + size_t(g) * 2;
+                    cpAsync16(&sm.st.raw[buf][0][tid], rec);
+                    cpAsync16(&sm.st.raw[buf][1][tid], rec + 1);
+                } else {  // 24-byte records start on 8-byte boundaries
+                    const uint2* rec = records24 + size_t(g) * 3;
+                    uint2* dst = reinterpret_cast<uint2*>(&sm.st.raw[buf][0][0]);
+                    cpAsync8(&dst[tid], rec);
+                    cpAsync8(&dst[kThreads + tid], rec + 1);
+                    cpAsync8(&dst[2 * kThreads + tid], rec + 2);
+                }
+                if constexpr (CAP > 0) {
+                    const float4* rp = a.rayDepth + (size_t(view) * a.count + g) * 3;
+                    cpAsync16(&ray[buf][0][tid], rp);
+                    cpAsync16(&ray[buf][1][tid], rp + 1);
+                    cpAsync16(&ray[buf][2][tid], rp + 2);
+                }
             }
-            if constexpr (CAP > 0) {
-                const float4* rp = a.rayDepth + (size_t(view) * a.count + g) * 3;
-                cpAsync16(&ray[buf][0][tid], rp);
-                cpAsync16(&ray[buf][1][tid], rp + 1);
-                cpAsync16(&ray[buf][2][tid], rp + 2);
-            }
+            cpAsyncCommit();
         }
-        cpAsyncCommit();
+    };
+    // TMA: every thread waits for the buffer's gathers (bounded) and counts the use
+    auto waitTma = [&](int buf) {
+        if constexpr (GATHER == kGatherTma) {
+            mbarWaitBounded(&sm.st.bar[buf], buf ? phase1 : phase0, a.ctl);
+            if (buf) phase1 ^= 1u;
+            else phase0 ^= 1u;
+        }
     };
     // StopThePop: the pixel's ray t (vx, vy, 1) in camera space (pixel = f x / z + (size - 1) / 2)
     SortWindow<(CAP > 0 ? CAP : 1)> window;
@@ -308,32 +401,50 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
     bool stTerm = false;
 
     int buf = 0;
-    if (range.x < range.y) issue(range.x, 0);
+    bool inFlight = false;  // TMA: the batch at `start` was issued and not yet waited for
+    if (range.x < range.y) {
+        issue(range.x, 0);
+        inFlight = true;
+    }
     for (uint32_t start = range.x; start < range.y; start += kThreads, buf ^= 1) {
         if (__syncthreads_count(done) == int(kThreads)) break;
         if constexpr (STATS) stFetched += range.y - start < kThreads ? range.y - start : kThreads;
         // prefetch the next batch while this one is prepared and blended
         const uint32_t next = start + kThreads;
-        if (next < range.y) issue(next, buf ^ 1);
-        else cpAsyncCommit();
-        cpAsyncWait<1>();
+        if constexpr (GATHER == kGatherTma) {
+            if (next < range.y) issue(next, buf ^ 1);
+            waitTma(buf);
+            inFlight = next < range.y;
+        } else {
+            if (next < range.y) issue(next, buf ^ 1);
+            else cpAsyncCommit();
+            cpAsyncWait<1>();
+        }
         __syncthreads();
         if (start + tid < range.y) {
             float2 r0;  // cx, cy
             float A, B, C, o;
             float4 r2;  // r, g, b, -
             if constexpr (mode == kRenderSplatFull) {
-                const float4 w0 = sm.raw[buf][0][tid];  // cx, cy, depth, cull
-                const float4 w1 = sm.raw[buf][1][tid];  // A, B, C, opacity
+                float4 w0, w1;
+                if constexpr (GATHER == kGatherTma) {
+                    const float4* rec = reinterpret_cast<const float4*>(&sm.st.quad[buf][tid >> 2][(tid & 3u) * 48u]);
+                    w0 = rec[0];
+                    w1 = rec[1];
+                    r2 = rec[2];
+                } else {
+                    w0 = sm.st.raw[buf][0][tid];  // cx, cy, depth, cull
+                    w1 = sm.st.raw[buf][1][tid];  // A, B, C, opacity
+                    r2 = sm.st.raw[buf][2][tid];  // r, g, b, radius
+                }
                 r0 = make_float2(w0.x, w0.y);
                 A = w1.x;
                 B = w1.y;
                 C = w1.z;
                 o = w1.w;
-                r2 = sm.raw[buf][2][tid];  // r, g, b, radius
             } else if constexpr (mode == kRenderSplatP32) {
-                const float4 w0 = sm.raw[buf][0][tid];  // cx, cy, A, B
-                const float4 w1 = sm.raw[buf][1][tid];  // C, opacity, h(r, g), h(b) | radius
+                const float4 w0 = sm.st.raw[buf][0][tid];  // cx, cy, A, B
+                const float4 w1 = sm.st.raw[buf][1][tid];  // C, opacity, h(r, g), h(b) | radius
                 r0 = make_float2(w0.x, w0.y);
                 A = w0.z;
                 B = w0.w;
@@ -342,7 +453,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
                 const uint32_t rg = __float_as_uint(w1.z), bw = __float_as_uint(w1.w);
                 r2 = make_float4(halfLoF(rg), halfHiF(rg), halfLoF(bw), 0.0f);
             } else {
-                const uint2* w = reinterpret_cast<const uint2*>(&sm.raw[buf][0][0]);
+                const uint2* w = reinterpret_cast<const uint2*>(&sm.st.raw[buf][0][0]);
                 const uint2 w0 = w[tid], w1 = w[kThreads + tid], w2 = w[2 * kThreads + tid];
                 r0 = make_float2(__uint_as_float(w0.x), __uint_as_float(w0.y));
                 p24DecodeConic(w1.x, w1.y, A, B, C, o);
@@ -421,7 +532,18 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
         for (int i = 0; i < CAP; ++i)
             if (!done && uint32_t(i) < window.count) blendOver(window.al[i], window.r[i], window.g[i], window.b[i], T, c0, c1, c2, done);
     }
-    cpAsyncWait<0>();
+    if constexpr (GATHER == kGatherTma) {
+        // a tile that ended early still has its next batch in flight: it lands before the
+        // buffers are reused (or the block exits); the phases are kept for the next tile
+        if (inFlight) waitTma(buf);
+        __syncthreads();
+        if (tid == 0) {
+            sm.st.uses[0] = phase0;
+            sm.st.uses[1] = phase1;
+        }
+    } else {
+        cpAsyncWait<0>();
+    }
     if constexpr (STATS) {
         if (!stTerm) stEval = inside ? range.y - range.x : 0u;
         __shared__ uint32_t sStat[kTileStatWords];
@@ -475,63 +597,87 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
 
 // One block per frame tile.
 // the shared area of a block: RenderShared, then for a StopThePop kernel the ray-depth parameters
-template <int CAP, int N>
+template <int CAP, int N, int GATHER>
 constexpr size_t renderSmemBytes() {
-    return sizeof(RenderShared<N>) + (CAP > 0 ? sizeof(float4) * 2 * 3 * N : 0);
+    return sizeof(RenderShared<N, GATHER>) + (CAP > 0 ? sizeof(float4) * 2 * 3 * N : 0);
 }
-template <int N>
+template <int N, int GATHER>
 __device__ __forceinline__ float4 (*rayArea(unsigned char* smem))[3][N] {
-    return reinterpret_cast<float4(*)[3][N]>(smem + sizeof(RenderShared<N>));
+    return reinterpret_cast<float4(*)[3][N]>(smem + sizeof(RenderShared<N, GATHER>));
+}
+
+// TMA: the buffers' mbarriers, initialized once per block (their phases then run across tiles)
+template <int N, int GATHER>
+__device__ __forceinline__ void initStage(RenderShared<N, GATHER>& sm) {
+    if constexpr (GATHER == kGatherTma) {
+        if (threadIdx.x == 0) {
+            for (int b = 0; b < 2; ++b) {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smemAddr(&sm.st.bar[b])) : "memory");
+                sm.st.uses[b] = 0;
+            }
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+    }
 }
 
 // Without the window: five 256-thread blocks (or the same threads in 8-px tiles) per SM, 48
 // registers a thread (the strip masks would take 61, four blocks, 5 % slower).
-template <int MODE, int CAP, int TILE, bool STATS>
-__global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1) renderKernel(const __grid_constant__ RenderArgs a) {
-    extern __shared__ __align__(16) unsigned char smemRaw[];
-    renderTile<MODE, CAP, TILE, STATS>(a, *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw),
-                                       CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, blockIdx.x + a.tileOffset);
+template <int MODE, int CAP, int TILE, bool STATS, int GATHER>
+__global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1)
+    renderKernel(const __grid_constant__ RenderArgs a, const __grid_constant__ CUtensorMap map) {
+    extern __shared__ __align__(128) unsigned char smemRaw[];
+    RenderShared<TILE * TILE, GATHER>& sm = *reinterpret_cast<RenderShared<TILE * TILE, GATHER>*>(smemRaw);
+    initStage(sm);
+    renderTile<MODE, CAP, TILE, STATS, GATHER>(a, sm, CAP > 0 ? rayArea<TILE * TILE, GATHER>(smemRaw) : nullptr,
+                                               blockIdx.x + a.tileOffset, &map);
 }
 
 // Persistent schedule: each block takes tiles from the frame's queue counter (reset by frame
 // begin) until the counter passes the last tile.
-template <int MODE, int CAP, int TILE, bool STATS>
-__global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1) renderPersistentKernel(const __grid_constant__ RenderArgs a) {
-    extern __shared__ __align__(16) unsigned char smemRaw[];
-    RenderShared<TILE * TILE>& sm = *reinterpret_cast<RenderShared<TILE * TILE>*>(smemRaw);
+template <int MODE, int CAP, int TILE, bool STATS, int GATHER>
+__global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1)
+    renderPersistentKernel(const __grid_constant__ RenderArgs a, const __grid_constant__ CUtensorMap map) {
+    extern __shared__ __align__(128) unsigned char smemRaw[];
+    RenderShared<TILE * TILE, GATHER>& sm = *reinterpret_cast<RenderShared<TILE * TILE, GATHER>*>(smemRaw);
+    initStage(sm);
     for (;;) {
         if (threadIdx.x == 0) sm.tile = atomicAdd(&a.ctl->tickets[kRenderQueueTicket], 1u);
         __syncthreads();
         const uint32_t tile = sm.tile;
         if (tile >= a.totalTiles) break;
-        renderTile<MODE, CAP, TILE, STATS>(a, sm, CAP > 0 ? rayArea<TILE * TILE>(smemRaw) : nullptr, tile);
+        renderTile<MODE, CAP, TILE, STATS, GATHER>(a, sm, CAP > 0 ? rayArea<TILE * TILE, GATHER>(smemRaw) : nullptr,
+                                                   tile, &map);
         __syncthreads();  // every thread has read sm.tile and left the tile's shared buffers
     }
 }
 
-template <int MODE, int CAP, int TILE, bool STATS = false>
+template <int MODE, int CAP, int TILE, bool STATS = false, int GATHER = kGatherCpAsync>
 cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
-    constexpr size_t smem = renderSmemBytes<CAP, TILE * TILE>();
+    constexpr size_t smem = renderSmemBytes<CAP, TILE * TILE, GATHER>();
     constexpr uint32_t threads = TILE * TILE;
     static std::atomic<bool> configuredOn[64] = {};
     std::atomic<bool>& configured = perDevice(configuredOn);
     if (!configured) {
-        cudaError_t e =
-            cudaFuncSetAttribute(renderKernel<MODE, CAP, TILE, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaError_t e = cudaFuncSetAttribute(renderKernel<MODE, CAP, TILE, STATS, GATHER>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(renderPersistentKernel<MODE, CAP, TILE, STATS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 int(smem));
+        e = cudaFuncSetAttribute(renderPersistentKernel<MODE, CAP, TILE, STATS, GATHER>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return e;
         configured = true;
     }
+    CUtensorMap map{};  // read by the TMA kernels only
+    if constexpr (GATHER == kGatherTma) map = *static_cast<const CUtensorMap*>(a.splatMap);
     if (a.persistent) {
         int sms = 148, dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         // as many resident threads per SM for either tile size
         const uint32_t grid = uint32_t(sms) * kPersistentBlocksPerSm * (kRenderThreads / threads);
-        renderPersistentKernel<MODE, CAP, TILE, STATS><<<grid < a.totalTiles ? grid : a.totalTiles, threads, smem, s>>>(a);
+        renderPersistentKernel<MODE, CAP, TILE, STATS, GATHER>
+            <<<grid < a.totalTiles ? grid : a.totalTiles, threads, smem, s>>>(a, map);
     } else {
-        renderKernel<MODE, CAP, TILE, STATS><<<a.tileLaunch ? a.tileLaunch : a.totalTiles, threads, smem, s>>>(a);
+        renderKernel<MODE, CAP, TILE, STATS, GATHER><<<a.tileLaunch ? a.tileLaunch : a.totalTiles, threads, smem, s>>>(a, map);
     }
     return cudaGetLastError();
 }
@@ -540,6 +686,9 @@ cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
 template <int MODE, int TILE>
 cudaError_t launchRenderWindow(const RenderArgs& a, cudaStream_t s) {
     if (a.tileStats) return launchRenderMode<MODE, 0, TILE, true>(a, s);  // the stats build has no window
+    if constexpr (MODE == kRenderSplatFull) {
+        if (a.sortWindow == 0 && a.splatMap) return launchRenderMode<MODE, 0, TILE, false, kGatherTma>(a, s);
+    }
     if (a.sortWindow == 0) return launchRenderMode<MODE, 0, TILE>(a, s);
     if (a.sortWindow <= 4) return launchRenderMode<MODE, 4, TILE>(a, s);
     if (a.sortWindow <= 16) return launchRenderMode<MODE, 16, TILE>(a, s);

@@ -162,6 +162,7 @@ struct RenderArgs {
     uint32_t count;           // N: gaussian indices read from the list are checked against it
     DeviceControl* ctl;
     const SortPlan* plan;     // the entry layout (packed words or key/value arrays)
+    const void* splatMap;     // host copy of the CUtensorMap over the full records: the TMA gather (null: cp.async)
     uint32_t* tileStats;      // the stats build: kTileStatWords per frame tile (null: the plain build)
     unsigned long long* testedPairs;  // the stats build: pairs the kernel tested, summed over the frame
 };

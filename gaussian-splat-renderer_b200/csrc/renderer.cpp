@@ -14,6 +14,8 @@
 // Counts (V, M, entries) exist only on the device; grids over the list are sized for the
 // capacity and read the entry count from the control block, as the reference's indirect
 // dispatches do. The adaptive list (splat_tile_renderer.cpp:444-486) follows the measured M.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -126,6 +128,34 @@ int deviceTables(LogfFixups* out) {
     out->last = gsr_logf_fixup_last;
     out->count = gsr_logf_fixup_count;
     return GSR_OK;
+}
+
+// ---- TMA tensor maps (the rasterizer's gather) -------------------------------------------------
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the library links no libcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tensorMapEncoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }();
+    return fn;
+}
+
+// The full records as a 2-D tensor for tile::gather4: rows = records (48 bytes apart), 12 fp32
+// columns, a box of one row of 12 columns (48 bytes, a multiple of 16), no swizzle, zero fill.
+bool encodeRecordMap(CUtensorMap* map, void* records, uint64_t rows) {
+    PFN_cuTensorMapEncodeTiled_v12000 encode = tensorMapEncoder();
+    if (!encode || !records || rows == 0 || rows >= (1ull << 31) || reinterpret_cast<uintptr_t>(records) % 16) return false;
+    const cuuint64_t dims[2] = {12, rows};
+    const cuuint64_t strides[1] = {48};
+    const cuuint32_t box[2] = {12, 1};
+    const cuuint32_t elemStrides[2] = {1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, records, dims, strides, box, elemStrides,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 // ---- the static scratch of gsr_scan_static, made ready once per device -----------------------
@@ -450,6 +480,13 @@ struct GsrRenderer {
     uint32_t passesUpper = 0;
     DevBuf ranges, image, rgb8;
     DevBuf tileStats, testedPairs;  // the stats build: kTileStatWords per frame tile, one 64-bit total
+    // the TMA gather: the tensor map over `splats` (valid while splatMapOk)
+    alignas(64) CUtensorMap splatMap{};
+    bool splatMapOk = false;
+    bool tmaGather() const {
+        return settings.raster_gather == GSR_GATHER_TMA && settings.render_splat == GSR_RENDER_SPLAT_FULL &&
+               settings.sort_window == 0 && !settings.tile_stats;
+    }
     // readback slots (2 frames late)
     // Per frame slot: the control readback, the camera (pinned, copied to the slot's device
     // copy by the frame itself), and the frame captured as a CUDA graph.
@@ -567,6 +604,7 @@ struct GsrRenderer {
         if (settings.render_splat == GSR_RENDER_SPLAT_FULL) {
             GSR_CUDA(splats.alloc(n * 48));
             GSR_CUDA(cudaMemset(splats.p, 0, splats.bytes));
+            splatMapOk = tmaGather() && encodeRecordMap(&splatMap, splats.p, n);
         } else {
             GSR_CUDA(packedSplats.alloc(n * packedWords() * 4));
             GSR_CUDA(cudaMemset(packedSplats.p, 0, packedSplats.bytes));
@@ -920,6 +958,7 @@ struct GsrRenderer {
         ra.count = scene.count;
         ra.ctl = ctl;
         ra.plan = sortPlan;
+        ra.splatMap = splatMapOk && tmaGather() ? &splatMap : nullptr;
         if (settings.tile_stats) {
             ra.tileStats = tileStats.as<uint32_t>();
             ra.testedPairs = testedPairs.as<unsigned long long>();
@@ -1271,6 +1310,11 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
         return fail(GSR_ERROR_INVALID_ARGUMENT, "render splat mode %u", settings->render_splat);
     if (settings->raster_schedule > GSR_RASTER_PERSISTENT)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "raster schedule %u", settings->raster_schedule);
+    if (settings->raster_gather > GSR_GATHER_TMA ||
+        (settings->raster_gather == GSR_GATHER_TMA &&
+         (settings->render_splat != GSR_RENDER_SPLAT_FULL || settings->sort_window > 0 || settings->tile_stats)))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "raster gather %u (TMA: full records, no sort window, no tile stats)",
+                    settings->raster_gather);
     if (settings->tile_stats > 1 || (settings->tile_stats && settings->sort_window > 0))
         return fail(GSR_ERROR_INVALID_ARGUMENT, "tile_stats %u (0 or 1, not with sort_window)", settings->tile_stats);
     if (settings->sort_digit_bits != 0 && settings->sort_digit_bits != 8)

@@ -35,6 +35,7 @@ BOUNDS = {"rect": 0, "tight": 1, "cutoff-only": 2}
 RASTER_SCHEDULES = {"auto": 0, "per-tile": 1, "persistent": 2}
 LIST_MODES = {"binning": 0, "global": 1}
 RENDER_SPLATS = {"full": 0, "p32": 1, "p24": 2}
+RASTER_GATHERS = {"default": 0, "cp.async": 1, "tma": 2}
 CONTROL_TIMEOUT, CONTROL_BOUNDS, CONTROL_KEY_RANGE = 1, 2, 4
 
 SPLAT_DTYPE = np.dtype(
@@ -87,7 +88,7 @@ class CSettings(C.Structure):
         ("adaptive_initial_entries", C.c_uint32), ("max_sh_degree", C.c_int32), ("output_format", C.c_uint32),
         ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("raster_schedule", C.c_uint32),
         ("list_mode", C.c_uint32), ("render_splat", C.c_uint32), ("sort_window", C.c_uint32),
-        ("sort_digit_bits", C.c_uint32), ("tile_stats", C.c_uint32), ("reserved", C.c_uint32 * 1),
+        ("sort_digit_bits", C.c_uint32), ("tile_stats", C.c_uint32), ("raster_gather", C.c_uint32),
     ]
 
 
@@ -300,6 +301,7 @@ class Settings:
     sort_window: int = 0  # StopThePop per-pixel window K (0 = off, at most 64)
     sort_digit_bits: int = 0  # radix digit width of the list sort (0 = 8)
     tile_stats: bool = False  # the instrumented rasterizer with per-tile statistics (read_tile_stats)
+    raster_gather: str = "default"  # how batches reach shared memory: default, cp.async or tma
 
     def to_c(self) -> CSettings:
         s = CSettings()
@@ -324,6 +326,7 @@ class Settings:
         s.sort_window = self.sort_window
         s.sort_digit_bits = self.sort_digit_bits
         s.tile_stats = int(self.tile_stats)
+        s.raster_gather = RASTER_GATHERS[self.raster_gather]
         return s
 
 

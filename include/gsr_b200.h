@@ -22,7 +22,7 @@
 extern "C" {
 #endif
 
-#define GSR_ABI_VERSION 1
+#define GSR_ABI_VERSION 2
 
 typedef enum GsrStatus {
     GSR_OK = 0,
@@ -163,8 +163,20 @@ typedef struct GsrSettings {
     uint32_t tile_stats;               /* 1: the instrumented rasterizer with per-tile statistics
                                           (TileSettings::stats, splat_tile_renderer.h:102); not with
                                           sort_window; read with gsr_read_tile_stats */
-    uint32_t reserved[1];
+    uint32_t raster_gather;            /* GsrRasterGather: how the rasterizer stages each batch of records */
 } GsrSettings;
+
+/* How the rasterizer brings a batch of records into shared memory (no reference counterpart; the
+ * reference's workgroup fetches them cooperatively, tile_render.comp:281-400). The images are
+ * the same either way. */
+typedef enum GsrRasterGather {
+    GSR_GATHER_DEFAULT = 0, /* the build's default (GSR_GATHER_CP_ASYNC) */
+    GSR_GATHER_CP_ASYNC = 1, /* every thread copies its record with 16-byte cp.async */
+    GSR_GATHER_TMA = 2       /* one warp gathers four records per TMA instruction (cp.async.bulk.tensor
+                                tile::gather4 over a 2-D tensor map of the record array), completed on
+                                an mbarrier; full records, no sort window, no tile statistics, and
+                                fewer than 2^31 records (else the cp.async gather runs) */
+} GsrRasterGather;
 
 /* The per-entry record that key emission and the rasterizer read (RenderSplatMode,
  * splat_tile_renderer.h:87-92; layouts of shaders/render_splat.glsl). Packed records keep the

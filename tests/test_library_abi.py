@@ -33,7 +33,7 @@ def test_exports_every_declared_symbol(gsr):
 
 def test_abi_version_and_error_strings(gsr):
     lib = gsr.load()
-    assert lib.gsr_abi_version() == 1
+    assert lib.gsr_abi_version() == 2
     names = [lib.gsr_error_string(i).decode() for i in range(9)]
     assert names[0] == "ok" and len(set(names)) == 9
 
@@ -118,3 +118,23 @@ def test_invalid_arguments_are_reported(gsr):
     assert "null" in lib.gsr_last_error_message().decode()
     assert lib.gsr_sort_pairs(None, None, None, 10, 0, None) == 1
     assert lib.gsr_scan(None, None, None, None, 5, 9, None) == 1
+
+
+def test_struct_sizes_match_the_header(gsr, tmp_path):
+    """The ctypes mirrors have the sizes the C compiler gives the header's structs."""
+    import ctypes as C
+    import shutil
+    import subprocess
+
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    src = tmp_path / "sizes.c"
+    names = ["GsrSettings", "GsrTuneResult", "GsrTuneSpace", "GsrControl", "GsrSceneDesc", "GsrSplatCamera",
+             "GsrCamera"]
+    src.write_text('#include <stdio.h>\n#include "gsr_b200.h"\nint main(void) {\n' +
+                   "".join(f'    printf("%zu\\n", sizeof({n}));\n' for n in names) + "    return 0;\n}\n")
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", f"-I{REPO / 'include'}", str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    mirrors = [gsr.CSettings, gsr.TuneResult, gsr.TuneSpace, gsr.Control, gsr.SceneDesc, gsr.SplatCamera, gsr.CCamera]
+    assert got == [C.sizeof(m) for m in mirrors], dict(zip(names, got))
