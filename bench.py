@@ -476,10 +476,13 @@ def time_form(r, frames: Frames, args, dist: Dist, sampler: Sampler, stream_obj)
     calls = len(frames.calls)
     with torch.cuda.stream(stream_obj):
         stable, last, k = 0, -1, 0
-        limit = args.warmup * calls + 64
-        while k < limit and (k < args.warmup * calls or stable < 3):
+        # at least 128 calls: the adaptive list shrinks after 120 readbacks below 40 % of its
+        # capacity (splat_tile_renderer.cpp:444-486), which must happen before the timed steps
+        least = max(args.warmup * calls, 128)
+        limit = least + 64
+        while k < limit and (k < least or stable < 3):
             render_call(r, frames, k, stream)
-            if k >= args.warmup * calls - 6 or k % 16 == 0:
+            if k >= least - 6 or k % 16 == 0:
                 stream_obj.synchronize()
                 cap = r.capacity()[0]
                 stable, last = (stable + 1 if cap == last else 0), cap
@@ -910,6 +913,23 @@ def check_launch(args, dist: Dist):
                           "max_rank": slowest}), flush=True)
 
 
+def run_plain_only(G, args, dist, sampler, stream_obj):
+    """Profiling runs: the plain form of one orbit workload alone (no autotuning, no learned
+    colour, no CPU leg), with its pass times."""
+    name = args.config if args.config in ("plain_1080p", "plain_1080p_f16", "plain_720p") else "plain_1080p"
+    scene, cams, fmt, layout, thr = workload(name)
+    gs = G.GpuScene(scene, fmt, layout, 3, thr)
+    r = renderer_for(G, gs, args)
+    frames = Frames(G, cams, 1)
+    form = time_form(r, frames, args, dist, sampler, stream_obj)
+    form["passes_ms"], _ = pass_profile(r, frames, stream_obj)
+    r.close()
+    gs.close()
+    if dist.rank == 0:
+        print(json.dumps({"metric": METRIC, "form": f"{name} plain only (profiling)", "gather": args.gather, **form}),
+              flush=True)
+
+
 # ---- the reference arm ------------------------------------------------------------------------
 def run_reference_arm(args):
     # under torchrun only rank 0 runs the CPU reference; the other ranks exit without work
@@ -943,6 +963,9 @@ def run_b200(args, dist: Dist):
     sampler = Sampler(dist.local_rank)
     base_mem = sampler.memory_used()
     peak = load_peaks()
+    if args.plain_only:
+        run_plain_only(G, args, dist, sampler, stream_obj)
+        return
     which = WORKLOADS if args.config == "all" else (args.config,)
     configs = {}
     t_start = time.perf_counter()
@@ -1020,6 +1043,7 @@ def main():
     ap.add_argument("--mlp-steps", type=int, default=2000)
     ap.add_argument("--gather", default="default", choices=["default", "cp.async", "tma"],
                     help="how the rasterizer stages each batch of records (GsrSettings.raster_gather)")
+    ap.add_argument("--plain-only", action="store_true", help="profiling runs: the plain form of one workload")
     ap.add_argument("--check-launch", action="store_true",
                     help="plumbing self-check: ranks, view partition and gather, no GPU work, no timing")
     args = ap.parse_args()

@@ -6,10 +6,14 @@
 // point on the sphere from a hash of (g, j), the same in training and in the gate. A training
 // step draws `batch` pairs from a hash of (seed, step, k), so the run is reproducible bit for bit.
 //
-//   trainStep   one thread per sample: forward (BF16-rounded weights and decoder activations, the
-//               latent rounded to fp16 then BF16, as the tensor-core decode sees them), loss,
-//               backward (straight through the roundings); then the block's weight gradients
-//               over its 64 samples, written as the block's partial sums (no atomics)
+//   trainStep   on the tensor cores: a 128-thread block takes 512 samples in chunks of 64, each
+//               warp 16 of them. Forward (BF16 weights and activations, FP32 accumulation, the
+//               latent rounded to fp16 then BF16 as the tensor-core decode sees it), loss and
+//               backward (straight through the roundings) are mma.sync.m16n8k16 products whose
+//               fragments come from shared memory by ldmatrix; the weight gradients are products
+//               over the chunk's samples (activations transposed by ldmatrix.trans), kept in
+//               registers across the chunks and written once as the block's partial sums (no
+//               atomics: the run is reproducible bit for bit)
 //   adamStep    one thread per parameter: the batch gradient from the partial sums, Adam
 //   encode      latents of every gaussian (fp32 encoder, stored fp16)
 //   gate        per gaussian, the tensor-core decode on its directions against the SH colour;
@@ -22,14 +26,24 @@ namespace gsr {
 
 namespace {
 
-constexpr int kTrainThreads = 64;
-constexpr int kActStride = kTrainThreads + 1;  // per-sample vectors stored [element][sample], padded
-// per-sample vectors kept for the weight gradients
-constexpr int kOffX = 0, kOffH = kOffX + kEncIn, kOffIn = kOffH + kEncHidden, kOffA1 = kOffIn + kMlpIn,
-              kOffA2 = kOffA1 + kMlpHidden, kOffDH = kOffA2 + kMlpHidden, kOffDZ = kOffDH + kEncHidden,
-              kOffDA1 = kOffDZ + kMlpLatent, kOffDA2 = kOffDA1 + kMlpHidden, kOffDO = kOffDA2 + kMlpHidden,
-              kActRows = kOffDO + kMlpOut;
-constexpr int kTrainSmemFloats = MlpLayout::kCount + 1 + kActRows * kActStride;
+// The tensor-core training step: blocks of 4 warps, chunks of 64 samples (16 per warp), 8
+// chunks (512 samples) a block. Row strides of the shared-memory matrices are K + 8 BF16 so
+// that the 8 rows an ldmatrix reads fall into distinct banks.
+constexpr int kTcWarps = 4, kTcThreads = kTcWarps * 32, kTcChunk = kTcWarps * 16, kTcChunks = 8;
+constexpr int kTcBlockSamples = kTcChunk * kTcChunks;
+constexpr int S48 = kEncIn + 8, S64 = kEncHidden + 8, S32 = kMlpHidden + 8, S16 = 16 + 8;
+
+struct alignas(16) TrainSmem {
+    // forward operands [n][k] (the weight matrices transposed), backward operands [n][k] = W[in][out]
+    __nv_bfloat16 wt1e[kEncHidden][S48], wt2e[8][S64], wt1d[kMlpHidden][S16], wt2d[kMlpHidden][S32], wt3d[8][S32];
+    __nv_bfloat16 wb3[kMlpHidden][S16], wb2[kMlpHidden][S32], wb1[kMlpLatent][S32], wb2e[kEncHidden][S16];
+    // the chunk's activations and gradients, one row per sample
+    __nv_bfloat16 x[kTcChunk][S48], h[kTcChunk][S64], in[kTcChunk][S16], a1[kTcChunk][S32], a2[kTcChunk][S32];
+    __nv_bfloat16 dO[kTcChunk][S16], dA2[kTcChunk][S32], dA1[kTcChunk][S32], dZ[kTcChunk][S16], dH[kTcChunk][S64];
+    float b1e[kEncHidden], b2e[8], b1d[kMlpHidden], b2d[kMlpHidden], b3d[8];
+    float tgt[kTcChunk][4];
+    float lossWarp[kTcWarps];
+};
 
 __device__ __forceinline__ uint32_t mix32(uint32_t x) {
     x ^= x >> 16;
@@ -67,112 +81,327 @@ struct TrainArgs {
     const uint32_t* step;    // current step (device counter, advanced by adamStep)
 };
 
-__global__ void __launch_bounds__(kTrainThreads) trainStepKernel(const __grid_constant__ TrainArgs a) {
-    extern __shared__ float sm[];
-    float* W = sm;                                   // BF16-rounded weights (encoder fp32)
-    float* act = sm + MlpLayout::kCount + 1;         // [kActRows][kActStride]
-    const uint32_t s = threadIdx.x;
-    using L = MlpLayout;
-    for (int p = s; p < L::kCount; p += kTrainThreads)
-        W[p] = p >= L::kDecW1 ? bf16Round(a.params[p]) : a.params[p];
-    __syncthreads();
-    auto A = [&](int row) -> float& { return act[row * kActStride + s]; };
-    const uint32_t step = *a.step;
-    const uint32_t k = blockIdx.x * kTrainThreads + s;
-    const uint32_t h = hash3(a.seed, step, k);
-    const uint32_t g = uint32_t((uint64_t(h) * a.count) >> 32);
-    const uint32_t j = hash3(a.seed ^ 0x5bd1e995u, step, k) % a.dirs;
-    float dir[3];
-    sampleDirection(g, j, dir);
-    float target[3];
-    const float* shg = a.sh + size_t(g) * kEncIn;
-    evalSH(int(a.degrees[g]), shg, dir[0], dir[1], dir[2], target);
-    // ---- forward
-    for (int i = 0; i < kEncIn; ++i) A(kOffX + i) = shg[i];
-    for (int o = 0; o < kEncHidden; ++o) {
-        float v = W[L::kEncB1 + o];
-        for (int i = 0; i < kEncIn; ++i) v += A(kOffX + i) * W[L::kEncW1 + i * kEncHidden + o];
-        A(kOffH + o) = fmaxf(v, 0.0f);
-    }
-    for (int o = 0; o < kMlpLatent; ++o) {
-        float v = W[L::kEncB2 + o];
-        for (int i = 0; i < kEncHidden; ++i) v += A(kOffH + i) * W[L::kEncW2 + i * kMlpLatent + o];
-        A(kOffIn + o) = latentRound(v);
-    }
-    for (int c = 0; c < 3; ++c) A(kOffIn + kMlpLatent + c) = bf16Round(dir[c]);
-    for (int o = 0; o < kMlpHidden; ++o) {
-        float v = W[L::kDecB1 + o];
-        for (int i = 0; i < kMlpIn; ++i) v += A(kOffIn + i) * W[L::kDecW1 + i * kMlpHidden + o];
-        A(kOffA1 + o) = bf16Round(fmaxf(v, 0.0f));
-    }
-    for (int o = 0; o < kMlpHidden; ++o) {
-        float v = W[L::kDecB2 + o];
-        for (int i = 0; i < kMlpHidden; ++i) v += A(kOffA1 + i) * W[L::kDecW2 + i * kMlpHidden + o];
-        A(kOffA2 + o) = bf16Round(fmaxf(v, 0.0f));
-    }
-    float loss = 0.0f;
-    for (int o = 0; o < kMlpOut; ++o) {
-        float v = W[L::kDecB3 + o];
-        for (int i = 0; i < kMlpHidden; ++i) v += A(kOffA2 + i) * W[L::kDecW3 + i * kMlpOut + o];
-        const float y = 1.0f / (1.0f + expf(-v));
-        const float e = y - target[o];
-        loss += e * e;
-        A(kOffDO + o) = 2.0f * e * y * (1.0f - y);  // d loss / d pre-sigmoid
-    }
-    // ---- backward (activations are post-ReLU: > 0 means the unit was active)
-    for (int i = 0; i < kMlpHidden; ++i) {
-        float v = 0.0f;
-        for (int o = 0; o < kMlpOut; ++o) v += W[L::kDecW3 + i * kMlpOut + o] * A(kOffDO + o);
-        A(kOffDA2 + i) = A(kOffA2 + i) > 0.0f ? v : 0.0f;
-    }
-    for (int i = 0; i < kMlpHidden; ++i) {
-        float v = 0.0f;
-        for (int o = 0; o < kMlpHidden; ++o) v += W[L::kDecW2 + i * kMlpHidden + o] * A(kOffDA2 + o);
-        A(kOffDA1 + i) = A(kOffA1 + i) > 0.0f ? v : 0.0f;
-    }
-    for (int i = 0; i < kMlpLatent; ++i) {
-        float v = 0.0f;
-        for (int o = 0; o < kMlpHidden; ++o) v += W[L::kDecW1 + i * kMlpHidden + o] * A(kOffDA1 + o);
-        A(kOffDZ + i) = v;  // straight through the fp16/BF16 roundings of the latent
-    }
-    for (int i = 0; i < kEncHidden; ++i) {
-        float v = 0.0f;
-        for (int o = 0; o < kMlpLatent; ++o) v += W[L::kEncW2 + i * kMlpLatent + o] * A(kOffDZ + o);
-        A(kOffDH + i) = A(kOffH + i) > 0.0f ? v : 0.0f;
-    }
-    // the block's loss sum
-    for (int o = 16; o; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
-    __syncthreads();
-    float* part = a.partials + size_t(blockIdx.x) * (L::kCount + 1);
-    if ((s & 31) == 0) atomicAdd(&part[L::kCount], loss);  // two warps; the slot is zeroed below first
-    // ---- weight gradients of the block: parameter p sums over the block's samples
-    for (int p = s; p < L::kCount; p += kTrainThreads) {
-        int u = -1, v = -1;  // rows of the two factors (u = -1: a bias, the factor is 1)
-        if (p < L::kEncB1) { u = kOffX + (p - L::kEncW1) / kEncHidden; v = kOffDH + (p - L::kEncW1) % kEncHidden; }
-        else if (p < L::kEncW2) { v = kOffDH + (p - L::kEncB1); }
-        else if (p < L::kEncB2) { u = kOffH + (p - L::kEncW2) / kMlpLatent; v = kOffDZ + (p - L::kEncW2) % kMlpLatent; }
-        else if (p < L::kDecW1) { v = kOffDZ + (p - L::kEncB2); }
-        else if (p < L::kDecB1) { u = kOffIn + (p - L::kDecW1) / kMlpHidden; v = kOffDA1 + (p - L::kDecW1) % kMlpHidden; }
-        else if (p < L::kDecW2) { v = kOffDA1 + (p - L::kDecB1); }
-        else if (p < L::kDecB2) { u = kOffA1 + (p - L::kDecW2) / kMlpHidden; v = kOffDA2 + (p - L::kDecW2) % kMlpHidden; }
-        else if (p < L::kDecW3) { v = kOffDA2 + (p - L::kDecB2); }
-        else if (p < L::kDecB3) { u = kOffA2 + (p - L::kDecW3) / kMlpOut; v = kOffDO + (p - L::kDecW3) % kMlpOut; }
-        else { v = kOffDO + (p - L::kDecB3); }
-        float sum = 0.0f;
-        const float* vr = act + v * kActStride;
-        if (u < 0) {
-            for (int t = 0; t < kTrainThreads; ++t) sum += vr[t];
-        } else {
-            const float* ur = act + u * kActStride;
-            for (int t = 0; t < kTrainThreads; ++t) sum += ur[t] * vr[t];
+__device__ __forceinline__ uint32_t smemAddr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
+
+__device__ __forceinline__ void ldsm4(uint32_t (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(smemAddr(p)));
+}
+__device__ __forceinline__ void ldsm4t(uint32_t (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(smemAddr(p)));
+}
+__device__ __forceinline__ void ldsm2(uint32_t& r0, uint32_t& r1, const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0, %1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(smemAddr(p)));
+}
+__device__ __forceinline__ void ldsm2t(uint32_t& r0, uint32_t& r1, const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0, %1}, [%2];" : "=r"(r0), "=r"(r1) : "r"(smemAddr(p)));
+}
+
+// One warp's 16 rows (rb..rb+15) of act (row-major, stride SA) times B ([n][k], stride SB):
+// c[nt] += rows x B for n-tiles nt (columns 8 nt .. 8 nt + 7), K = 16 KSTEPS.
+template <int KSTEPS, int NTILES, int SA, int SB>
+__device__ __forceinline__ void rowsTimes(float (&c)[NTILES][4], const __nv_bfloat16 (*act)[SA], int rb,
+                                          const __nv_bfloat16 (*B)[SB]) {
+    const int lane = threadIdx.x & 31, j = lane >> 3, i = lane & 7;
+#pragma unroll
+    for (int ks = 0; ks < KSTEPS; ++ks) {
+        uint32_t a[4];
+        ldsm4(a, &act[rb + (j & 1) * 8 + i][ks * 16 + (j >> 1) * 8]);
+#pragma unroll
+        for (int nt = 0; nt < NTILES; ++nt) {
+            uint32_t b0, b1;
+            ldsm2(b0, b1, &B[nt * 8 + i][ks * 16 + (j & 1) * 8]);
+            mmaBf16(c[nt], a, b0, b1);
         }
-        part[p] = sum;
     }
 }
 
-__global__ void zeroLossSlotsKernel(float* partials, uint32_t blocks) {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b < blocks) partials[size_t(b) * (MlpLayout::kCount + 1) + MlpLayout::kCount] = 0.0f;
+// c (16 x 8 tile) -> BF16 rows of out; op applied per element with its column
+template <int S, typename Op>
+__device__ __forceinline__ void storeTile(__nv_bfloat16 (*out)[S], int rb, int n0, const float (&c)[4], Op op) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, col = n0 + (lane & 3) * 2;
+    *reinterpret_cast<uint32_t*>(&out[rb + g][col]) = packBf16(op(c[0], rb + g, col), op(c[1], rb + g, col + 1));
+    *reinterpret_cast<uint32_t*>(&out[rb + g + 8][col]) = packBf16(op(c[2], rb + g + 8, col), op(c[3], rb + g + 8, col + 1));
+}
+
+// The chunk's weight-gradient tiles (16 x 8 each): dW1e 48 x 64 (3 x 8 tiles), dW2e 64 x 8
+// (4 x 1), dW1d 16 x 32 (1 x 4; rows 11..15 are padding), dW2d 32 x 32 (2 x 4), dW3d 32 x 8
+// (2 x 1); tile t goes to warp t mod 4.
+constexpr int kGradTiles = 24 + 4 + 4 + 8 + 2;
+constexpr int kTilesPerWarp = (kGradTiles + kTcWarps - 1) / kTcWarps;
+struct GradTile {
+    int mat, m0, n0;
+};
+__device__ __forceinline__ GradTile gradTile(int t) {
+    if (t < 24) return {0, (t / 8) * 16, (t % 8) * 8};
+    t -= 24;
+    if (t < 4) return {1, t * 16, 0};
+    t -= 4;
+    if (t < 4) return {2, 0, t * 8};
+    t -= 4;
+    if (t < 8) return {3, (t / 4) * 16, (t % 4) * 8};
+    t -= 8;
+    return {4, t * 16, 0};
+}
+
+// acc += act^T (rows m0.., the chunk's samples as K) x grad (columns n0..n0+7)
+template <int SA, int SG>
+__device__ __forceinline__ void gradTimes(float (&acc)[4], const __nv_bfloat16 (*act)[SA], int m0,
+                                          const __nv_bfloat16 (*grad)[SG], int n0) {
+    const int lane = threadIdx.x & 31, j = lane >> 3, i = lane & 7;
+#pragma unroll
+    for (int ks = 0; ks < kTcChunk / 16; ++ks) {
+        uint32_t a[4], b0, b1;
+        ldsm4t(a, &act[ks * 16 + (j >> 1) * 8 + i][m0 + (j & 1) * 8]);
+        ldsm2t(b0, b1, &grad[ks * 16 + (j & 1) * 8 + i][n0]);
+        mmaBf16(acc, a, b0, b1);
+    }
+}
+
+__global__ void __launch_bounds__(kTcThreads) trainStepKernel(const __grid_constant__ TrainArgs a) {
+    extern __shared__ __align__(16) unsigned char smemRaw[];
+    TrainSmem& S = *reinterpret_cast<TrainSmem*>(smemRaw);
+    using L = MlpLayout;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, g = lane >> 2, tig = lane & 3;
+    const float* P = a.params;
+    auto bf = [](float v) { return __float2bfloat16_rn(v); };
+    // weights in both layouts (padding zero), biases, and the constant zero columns
+    for (int e = tid; e < kEncHidden * S48; e += kTcThreads) {
+        const int o = e / S48, i = e % S48;
+        S.wt1e[o][i] = bf(i < kEncIn ? P[L::kEncW1 + i * kEncHidden + o] : 0.0f);
+    }
+    for (int e = tid; e < 8 * S64; e += kTcThreads) {
+        const int o = e / S64, i = e % S64;
+        S.wt2e[o][i] = bf(i < kEncHidden ? P[L::kEncW2 + i * kMlpLatent + o] : 0.0f);
+    }
+    for (int e = tid; e < kMlpHidden * S16; e += kTcThreads) {
+        const int o = e / S16, i = e % S16;
+        S.wt1d[o][i] = bf(i < kMlpIn ? P[L::kDecW1 + i * kMlpHidden + o] : 0.0f);
+        S.wb3[o][i] = bf(i < kMlpOut ? P[L::kDecW3 + o * kMlpOut + i] : 0.0f);
+    }
+    for (int e = tid; e < kMlpHidden * S32; e += kTcThreads) {
+        const int r = e / S32, c = e % S32;
+        S.wt2d[r][c] = bf(c < kMlpHidden ? P[L::kDecW2 + c * kMlpHidden + r] : 0.0f);
+        S.wb2[r][c] = bf(c < kMlpHidden ? P[L::kDecW2 + r * kMlpHidden + c] : 0.0f);
+    }
+    for (int e = tid; e < 8 * S32; e += kTcThreads) {
+        const int r = e / S32, c = e % S32;
+        S.wt3d[r][c] = bf(r < kMlpOut && c < kMlpHidden ? P[L::kDecW3 + c * kMlpOut + r] : 0.0f);
+        S.wb1[r][c] = bf(c < kMlpHidden ? P[L::kDecW1 + r * kMlpHidden + c] : 0.0f);  // the latent rows of W1d
+    }
+    for (int e = tid; e < kEncHidden * S16; e += kTcThreads) {
+        const int r = e / S16, c = e % S16;
+        S.wb2e[r][c] = bf(c < kMlpLatent ? P[L::kEncW2 + r * kMlpLatent + c] : 0.0f);
+    }
+    for (int e = tid; e < kEncHidden; e += kTcThreads) S.b1e[e] = P[L::kEncB1 + e];
+    for (int e = tid; e < kMlpHidden; e += kTcThreads) {
+        S.b1d[e] = P[L::kDecB1 + e];
+        S.b2d[e] = P[L::kDecB2 + e];
+    }
+    if (tid < 8) {
+        S.b2e[tid] = P[L::kEncB2 + tid];
+        S.b3d[tid] = tid < kMlpOut ? P[L::kDecB3 + tid] : 0.0f;
+    }
+    for (int e = tid; e < kTcChunk * 8; e += kTcThreads) {
+        const int r = e / 8, c = 8 + e % 8;
+        S.in[r][c] = bf(0.0f);  // columns 11..15 stay zero (8..10 are rewritten per chunk)
+        S.dO[r][c] = bf(0.0f);
+        S.dZ[r][c] = bf(0.0f);
+    }
+    __syncthreads();
+
+    const uint32_t step = *a.step;
+    const int rb = warp * 16;
+    float acc[kTilesPerWarp][4];
+#pragma unroll
+    for (int q = 0; q < kTilesPerWarp; ++q) acc[q][0] = acc[q][1] = acc[q][2] = acc[q][3] = 0.0f;
+    float bsum[2] = {0.0f, 0.0f};  // bias gradients of columns tid and tid + 128 of [dH | dZ | dA1 | dA2 | dO]
+    float loss = 0.0f;
+    for (int chunk = 0; chunk < kTcChunks; ++chunk) {
+        // ---- the chunk's samples: (gaussian, direction), SH coefficients and the SH colour
+        if (tid < kTcChunk) {
+            const uint32_t k = blockIdx.x * kTcBlockSamples + chunk * kTcChunk + tid;
+            const uint32_t gs = uint32_t((uint64_t(hash3(a.seed, step, k)) * a.count) >> 32);
+            const uint32_t jd = hash3(a.seed ^ 0x5bd1e995u, step, k) % a.dirs;
+            float dir[3], target[3];
+            sampleDirection(gs, jd, dir);
+            const float* shg = a.sh + size_t(gs) * kEncIn;
+            evalSH(int(a.degrees[gs]), shg, dir[0], dir[1], dir[2], target);
+            const float4* sh4 = reinterpret_cast<const float4*>(shg);
+#pragma unroll
+            for (int q = 0; q < kEncIn / 4; ++q) {
+                const float4 v = __ldg(&sh4[q]);
+                *reinterpret_cast<uint32_t*>(&S.x[tid][4 * q]) = packBf16(v.x, v.y);
+                *reinterpret_cast<uint32_t*>(&S.x[tid][4 * q + 2]) = packBf16(v.z, v.w);
+            }
+            for (int c = 0; c < 3; ++c) {
+                S.in[tid][kMlpLatent + c] = bf(dir[c]);
+                S.tgt[tid][c] = target[c];
+            }
+        }
+        __syncthreads();
+        // ---- forward, each warp its 16 rows
+        {
+            float c[8][4];
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int col = nt * 8 + tig * 2;
+                c[nt][0] = c[nt][2] = S.b1e[col];
+                c[nt][1] = c[nt][3] = S.b1e[col + 1];
+            }
+            rowsTimes<3, 8>(c, S.x, rb, S.wt1e);
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) storeTile(S.h, rb, nt * 8, c[nt], [](float v, int, int) { return fmaxf(v, 0.0f); });
+        }
+        __syncwarp();
+        {
+            float c[1][4];
+            c[0][0] = c[0][2] = S.b2e[tig * 2];
+            c[0][1] = c[0][3] = S.b2e[tig * 2 + 1];
+            rowsTimes<4, 1>(c, S.h, rb, S.wt2e);
+            storeTile(S.in, rb, 0, c[0], [](float v, int, int) { return latentRound(v); });
+        }
+        __syncwarp();
+        {
+            float c[4][4];
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int col = nt * 8 + tig * 2;
+                c[nt][0] = c[nt][2] = S.b1d[col];
+                c[nt][1] = c[nt][3] = S.b1d[col + 1];
+            }
+            rowsTimes<1, 4>(c, S.in, rb, S.wt1d);
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) storeTile(S.a1, rb, nt * 8, c[nt], [](float v, int, int) { return fmaxf(v, 0.0f); });
+        }
+        __syncwarp();
+        {
+            float c[4][4];
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int col = nt * 8 + tig * 2;
+                c[nt][0] = c[nt][2] = S.b2d[col];
+                c[nt][1] = c[nt][3] = S.b2d[col + 1];
+            }
+            rowsTimes<2, 4>(c, S.a1, rb, S.wt2d);
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) storeTile(S.a2, rb, nt * 8, c[nt], [](float v, int, int) { return fmaxf(v, 0.0f); });
+        }
+        __syncwarp();
+        {
+            float c[1][4];
+            c[0][0] = c[0][2] = S.b3d[tig * 2];
+            c[0][1] = c[0][3] = S.b3d[tig * 2 + 1];
+            rowsTimes<2, 1>(c, S.a2, rb, S.wt3d);
+            // sigmoid, squared error against the SH colour, d loss / d pre-sigmoid
+            storeTile(S.dO, rb, 0, c[0], [&](float v, int row, int col) {
+                if (col >= kMlpOut) return 0.0f;
+                const float y = 1.0f / (1.0f + expf(-v));
+                const float e = y - S.tgt[row - 0][col];
+                loss += e * e;
+                return 2.0f * e * y * (1.0f - y);
+            });
+        }
+        __syncwarp();
+        // ---- backward (activations are post-ReLU: > 0 means the unit was active)
+        auto activeIn = [](const __nv_bfloat16(*act)[S32]) {
+            return [act](float v, int row, int col) { return __bfloat162float(act[row][col]) > 0.0f ? v : 0.0f; };
+        };
+        {
+            float c[4][4] = {};
+            rowsTimes<1, 4>(c, S.dO, rb, S.wb3);
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) storeTile(S.dA2, rb, nt * 8, c[nt], activeIn(S.a2));
+        }
+        __syncwarp();
+        {
+            float c[4][4] = {};
+            rowsTimes<2, 4>(c, S.dA2, rb, S.wb2);
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) storeTile(S.dA1, rb, nt * 8, c[nt], activeIn(S.a1));
+        }
+        __syncwarp();
+        {
+            float c[1][4] = {};
+            rowsTimes<2, 1>(c, S.dA1, rb, S.wb1);  // straight through the latent's roundings
+            storeTile(S.dZ, rb, 0, c[0], [](float v, int, int) { return v; });
+        }
+        __syncwarp();
+        {
+            float c[8][4] = {};
+            rowsTimes<1, 8>(c, S.dZ, rb, S.wb2e);
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt)
+                storeTile(S.dH, rb, nt * 8, c[nt],
+                          [&](float v, int row, int col) { return __bfloat162float(S.h[row][col]) > 0.0f ? v : 0.0f; });
+        }
+        __syncthreads();
+        // ---- the chunk's weight gradients (tiles of this warp) and bias gradients
+#pragma unroll
+        for (int q = 0; q < kTilesPerWarp; ++q) {
+            const int t = warp + q * kTcWarps;
+            if (t >= kGradTiles) break;
+            const GradTile gt = gradTile(t);
+            switch (gt.mat) {
+                case 0: gradTimes(acc[q], S.x, gt.m0, S.dH, gt.n0); break;
+                case 1: gradTimes(acc[q], S.h, gt.m0, S.dZ, gt.n0); break;
+                case 2: gradTimes(acc[q], S.in, gt.m0, S.dA1, gt.n0); break;
+                case 3: gradTimes(acc[q], S.a1, gt.m0, S.dA2, gt.n0); break;
+                default: gradTimes(acc[q], S.a2, gt.m0, S.dO, gt.n0); break;
+            }
+        }
+#pragma unroll
+        for (int h2 = 0; h2 < 2; ++h2) {
+            const int col = tid + h2 * kTcThreads;
+            float sum = 0.0f;
+            for (int r = 0; r < kTcChunk; ++r) {
+                const __nv_bfloat16 v = col < 64    ? S.dH[r][col]
+                                        : col < 72  ? S.dZ[r][col - 64]
+                                        : col < 104 ? S.dA1[r][col - 72]
+                                        : col < 136 ? S.dA2[r][col - 104]
+                                        : col < 139 ? S.dO[r][col - 136]
+                                                    : __float2bfloat16_rn(0.0f);
+                sum += __bfloat162float(v);
+            }
+            bsum[h2] += sum;
+        }
+        __syncthreads();  // the next chunk overwrites the rows
+    }
+    // ---- the block's partial sums
+    float* part = a.partials + size_t(blockIdx.x) * (L::kCount + 1);
+#pragma unroll
+    for (int q = 0; q < kTilesPerWarp; ++q) {
+        const int t = warp + q * kTcWarps;
+        if (t >= kGradTiles) break;
+        const GradTile gt = gradTile(t);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int m = gt.m0 + g + (e >> 1) * 8, n = gt.n0 + tig * 2 + (e & 1);
+            int p = -1;
+            if (gt.mat == 0) p = L::kEncW1 + m * kEncHidden + n;
+            else if (gt.mat == 1) p = L::kEncW2 + m * kMlpLatent + n;
+            else if (gt.mat == 2) p = m < kMlpIn ? L::kDecW1 + m * kMlpHidden + n : -1;
+            else if (gt.mat == 3) p = L::kDecW2 + m * kMlpHidden + n;
+            else p = n < kMlpOut ? L::kDecW3 + m * kMlpOut + n : -1;
+            if (p >= 0) part[p] = acc[q][e];
+        }
+    }
+#pragma unroll
+    for (int h2 = 0; h2 < 2; ++h2) {
+        const int col = tid + h2 * kTcThreads;
+        const int p = col < 64 ? L::kEncB1 + col : col < 72 ? L::kEncB2 + col - 64 : col < 104 ? L::kDecB1 + col - 72
+                      : col < 136 ? L::kDecB2 + col - 104 : col < 139 ? L::kDecB3 + col - 136 : -1;
+        if (p >= 0) part[p] = bsum[h2];
+    }
+    for (int o = 16; o; o >>= 1) loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
+    if (lane == 0) S.lossWarp[warp] = loss;
+    __syncthreads();
+    if (tid == 0) {
+        float sum = 0.0f;
+        for (int w = 0; w < kTcWarps; ++w) sum += S.lossWarp[w];
+        part[L::kCount] = sum;
+    }
 }
 
 struct AdamArgs {
@@ -222,23 +451,25 @@ __global__ void adamStepKernel(const __grid_constant__ AdamArgs a) {
     }
 }
 
-// Latents of every gaussian: the fp32 encoder (one thread per gaussian), stored as fp16.
+// Latents of every gaussian (one thread per gaussian), stored as fp16: the encoder with the
+// training's roundings (BF16 coefficients, weights and hidden units, FP32 sums).
 __global__ void __launch_bounds__(128) encodeLatentsKernel(const float* __restrict__ sh, const float* __restrict__ params,
                                                            uint4* __restrict__ latents, uint32_t count) {
     __shared__ float W[MlpLayout::kDecW1];  // the encoder part
-    for (int p = threadIdx.x; p < MlpLayout::kDecW1; p += blockDim.x) W[p] = params[p];
+    for (int p = threadIdx.x; p < MlpLayout::kDecW1; p += blockDim.x)
+        W[p] = (p >= MlpLayout::kEncB1 && p < MlpLayout::kEncW2) || p >= MlpLayout::kEncB2 ? params[p] : bf16Round(params[p]);
     __syncthreads();
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= count) return;
     using L = MlpLayout;
     float x[kEncIn];
-    for (int i = 0; i < kEncIn; ++i) x[i] = sh[size_t(g) * kEncIn + i];
+    for (int i = 0; i < kEncIn; ++i) x[i] = bf16Round(sh[size_t(g) * kEncIn + i]);
     float z[kMlpLatent];
     for (int o = 0; o < kMlpLatent; ++o) z[o] = W[L::kEncB2 + o];
     for (int hdn = 0; hdn < kEncHidden; ++hdn) {
         float v = W[L::kEncB1 + hdn];
         for (int i = 0; i < kEncIn; ++i) v += x[i] * W[L::kEncW1 + i * kEncHidden + hdn];
-        v = fmaxf(v, 0.0f);
+        v = bf16Round(fmaxf(v, 0.0f));
         for (int o = 0; o < kMlpLatent; ++o) z[o] += v * W[L::kEncW2 + hdn * kMlpLatent + o];
     }
     uint32_t w[4];
@@ -344,16 +575,15 @@ cudaError_t launchColorTrainStep(const float* sh, const uint8_t* degrees, uint32
                                  float lr, float* lossOut, uint32_t maxSteps, cudaStream_t s) {
     static std::atomic<bool> configuredOn[64] = {};
     std::atomic<bool>& configured = perDevice(configuredOn);
-    const int smem = kTrainSmemFloats * 4;
+    const int smem = int(sizeof(TrainSmem));
     if (!configured) {
         const cudaError_t e = cudaFuncSetAttribute(trainStepKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    const uint32_t blocks = batch / kTrainThreads;
-    zeroLossSlotsKernel<<<(blocks + 255) / 256, 256, 0, s>>>(partials, blocks);
+    const uint32_t blocks = batch / kTcBlockSamples;
     TrainArgs ta{sh, degrees, count, dirs, seed, params, partials, step};
-    trainStepKernel<<<blocks, kTrainThreads, smem, s>>>(ta);
+    trainStepKernel<<<blocks, kTcThreads, smem, s>>>(ta);
     AdamArgs aa{params, m, v, partials, blocks, 1.0f / float(batch), lr, 0.9f, 0.999f, 1e-8f, step, lossOut, maxSteps};
     adamStepKernel<<<(MlpLayout::kCount + 1 + 255) / 256, 256, 0, s>>>(aa);
     return cudaGetLastError();
@@ -374,6 +604,6 @@ cudaError_t launchColorGate(const float* sh, const uint8_t* degrees, uint32_t co
     return cudaGetLastError();
 }
 
-uint32_t colorTrainBatchMultiple() { return kTrainThreads; }
+uint32_t colorTrainBatchMultiple() { return kTcBlockSamples; }
 
 }  // namespace gsr
