@@ -271,15 +271,15 @@ def workload(name: str):
 
 
 # ---- algorithmic bytes of the passes (binning list mode) ------------------------------------
-def depth_sort_passes(ctl) -> int:
+def depth_sort_passes(ctl, bits: int = 8) -> int:
     """Digit passes of the depth sort: the depth bits that vary over the frame plus the bit
-    that puts the records without tiles last, 8 bits a pass."""
+    that puts the records without tiles last, `bits` a pass."""
     lo, hi = ctl.depth_min_bits, ctl.depth_max_bits
     w = (lo ^ hi).bit_length() if lo <= hi else 0
-    return (w + 1 + 7) // 8
+    return (w + 1 + bits - 1) // bits
 
 
-def pass_bytes(scene_format: str, ctl, n: int, tiles: int) -> dict:
+def pass_bytes(scene_format: str, ctl, n: int, tiles: int, bits: int = 8) -> dict:
     """Bytes each pass must move for one frame, from the frame's counts.
     preprocess: posAlpha of every gaussian, scale + rotation of those past the near/opacity
       culls, SH of the visible ones (fp32 soa 16 + 32 + 192 B; fp16 split 16 + 16 + 96 B); writes
@@ -301,7 +301,7 @@ def pass_bytes(scene_format: str, ctl, n: int, tiles: int) -> dict:
     per_entry = 16 if ctl.packed_entries else 24
     return {
         "preprocess": float(pre),
-        "depth sort": float(8 * n + 16 * n * depth_sort_passes(ctl)),
+        "depth sort": float(8 * n + 16 * n * depth_sort_passes(ctl, bits)),
         "scan + emission": float((8 + 4 + 4) * n + (8 + 4 + 4) * n + 16 * vis + 8 * m),
         "tile sort": float(8 * m + per_entry * m * ctl.sort_passes),
         "ranges": float(8 * m + 8 * tiles),
@@ -552,8 +552,8 @@ def pass_profile(r, frames: Frames, stream_obj, n: int = 20) -> tuple[dict, obje
     return {k: round(v, 4) for k, v in passes.items()}, r.read_control()
 
 
-def roofline(passes: dict, ctl, fmt: str, n: int, tiles: int, peak: float, peak_kind: str) -> dict:
-    b = pass_bytes(fmt, ctl, n, tiles)
+def roofline(passes: dict, ctl, fmt: str, n: int, tiles: int, peak: float, peak_kind: str, bits: int = 8) -> dict:
+    b = pass_bytes(fmt, ctl, n, tiles, bits)
     kernels, tot_b, tot_ms = {}, 0.0, 0.0
     for k, nb in b.items():
         ms = passes.get(PASS_NAMES[k])
@@ -619,15 +619,18 @@ def settle_and_tune(G, gs, cams, args, model=None, depths=(1, 2, 4, 8, 16), tile
     if args.batch > 0:
         return {"views_per_frame": args.batch, "raster_schedule": "auto", "tile_size": 16, "table": None}
     sel = [cams[k % len(cams)] for k in range(max(probe, max(depths)))]
-    st = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.budget_mb, use_graph=True)
-    return G.autotune(gs, st, G.camera_array(sel), depths=depths, frames=3, model=model, tile_sizes=tile_sizes)
+    st = G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.budget_mb, use_graph=True,
+                    raster_gather=args.gather)
+    return G.autotune(gs, st, G.camera_array(sel), depths=depths, frames=3, model=model, tile_sizes=tile_sizes,
+                      sort_digit_bits=(8, 9))
 
 
 def renderer_for(G, gs, args, tuned=None, model=None, gather=None):
     t = tuned or {}
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.budget_mb,
                                   raster_schedule=t.get("raster_schedule", "auto"), tile_size=t.get("tile_size", 16),
-                                  use_graph=True, raster_gather=gather or args.gather))
+                                  use_graph=True, raster_gather=gather or args.gather,
+                                  sort_digit_bits=t.get("sort_digit_bits", args.digit_bits)))
     if model is not None:
         r.set_color_model(model)
     return r
@@ -668,7 +671,7 @@ def run_1080p(G, args, dist, sampler, stream_obj, peak):
         ab[gather] = gp.get("render tiles")
     plain["render_ms_by_gather"] = ab
     tiles = ((1920 + 15) // 16) * ((1080 + 15) // 16)
-    roof = roofline(passes, ctl, fmt, scene.count, tiles, peak[0], peak[1])
+    roof = roofline(passes, ctl, fmt, scene.count, tiles, peak[0], peak[1], args.digit_bits or 8)
     roof["traffic"] = int(TRAFFIC_PLAIN_1080P_CAPTURE)
     roof["traffic_kind"] = "from_capture"
     plain["render_flops"] = render_flops(G, gs, args, plain_frames, stream_obj, passes, plain["clocks"])
@@ -685,7 +688,8 @@ def run_1080p(G, args, dist, sampler, stream_obj, peak):
     rp = renderer_for(G, gs, args)
     pimgs = [frame_images(rp, Frames(G, cams, 1, [order[j]]), stream_obj)[0] for j in range(bframes.d)]
     rp.close()
-    batched.update({"raster": tuned["raster_schedule"], "autotune": tuned["table"],
+    batched.update({"raster": tuned["raster_schedule"], "sort_digit_bits": tuned.get("sort_digit_bits"),
+                    "autotune": tuned["table"],
                     "images_identical_to_plain": all(np.array_equal(a, b) for a, b in zip(bimgs, pimgs))})
     rb.close()
     out["plain_1080p"] = {"plain": plain, "batched": batched}
@@ -719,7 +723,7 @@ def run_1080p(G, args, dist, sampler, stream_obj, peak):
     return out, scene, cams, order, roof
 
 
-def run_1080p_f16(G, args, dist, sampler, stream_obj, tuned_depth: int, raster: str):
+def run_1080p_f16(G, args, dist, sampler, stream_obj, tuned_depth: int, raster: str, bits: int = 0):
     scene, cams, fmt, layout, thr = workload("plain_1080p_f16")
     first = (dist.rank * 37) % len(cams)
     order = [(first + k) % len(cams) for k in range(len(cams))]
@@ -730,7 +734,7 @@ def run_1080p_f16(G, args, dist, sampler, stream_obj, tuned_depth: int, raster: 
     passes, ctl = pass_profile(r, plain_frames, stream_obj)
     plain["passes_ms"] = passes
     r.close()
-    tuned = {"views_per_frame": tuned_depth, "raster_schedule": raster}
+    tuned = {"views_per_frame": tuned_depth, "raster_schedule": raster, "sort_digit_bits": bits}
     rb = renderer_for(G, gs, args, tuned)
     batched = time_form(rb, Frames(G, cams, tuned_depth, order), args, dist, sampler, stream_obj)
     rb.close()
@@ -970,14 +974,15 @@ def run_b200(args, dist: Dist):
     configs = {}
     t_start = time.perf_counter()
     head_roof, scene, cams, order = None, None, None, None
-    tuned_depth, raster = 8, "per-tile"
+    tuned_depth, raster, bits = 8, "per-tile", 0
     if any(w in which for w in ("plain_1080p", "learned_1080p")):
         res, scene, cams, order, head_roof = run_1080p(G, args, dist, sampler, stream_obj, peak)
         configs.update(res)
         tuned_depth = res["plain_1080p"]["batched"]["views_per_frame"]
         raster = res["plain_1080p"]["batched"]["raster"]
+        bits = res["plain_1080p"]["batched"].get("sort_digit_bits") or 0
     if "plain_1080p_f16" in which:
-        configs["plain_1080p_f16"] = run_1080p_f16(G, args, dist, sampler, stream_obj, tuned_depth, raster)
+        configs["plain_1080p_f16"] = run_1080p_f16(G, args, dist, sampler, stream_obj, tuned_depth, raster, bits)
     if "batched_64" in which:
         configs["batched_64"] = run_batched_64(G, args, dist, sampler, stream_obj)
     if "scale_4k" in which:
@@ -1041,6 +1046,8 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="views per frame of the batched forms (0: autotuned)")
     ap.add_argument("--budget-mb", type=int, default=16384)
     ap.add_argument("--mlp-steps", type=int, default=2000)
+    ap.add_argument("--digit-bits", type=int, default=0, choices=[0, 7, 8, 9],
+                    help="radix digit width of the plain form's sorts (0: the default, 8)")
     ap.add_argument("--gather", default="default", choices=["default", "cp.async", "tma"],
                     help="how the rasterizer stages each batch of records (GsrSettings.raster_gather)")
     ap.add_argument("--plain-only", action="store_true", help="profiling runs: the plain form of one workload")

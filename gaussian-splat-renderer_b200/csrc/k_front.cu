@@ -676,7 +676,7 @@ __global__ void frameBeginKernel(DeviceControl* ctl, uint32_t count, uint32_t ca
     for (int k = 0; k < 2; ++k) {
         if (!plans[k]) continue;
         uint32_t* h = &plans[k]->hist[0][0];
-        for (uint32_t j = threadIdx.x; j < kMaxSortPasses * 256; j += blockDim.x) h[j] = 0;
+        for (uint32_t j = threadIdx.x; j < kMaxSortPasses * kMaxSortBins; j += blockDim.x) h[j] = 0;
     }
     if (threadIdx.x == 0) {
         GsrControl& c = ctl->c;

@@ -69,10 +69,39 @@ __device__ __forceinline__ uint32_t blockExclusiveScan256(uint32_t v, uint32_t* 
     return base + incl - v;
 }
 
+// Digits of BITS bits (7, 8 or 9): kBins digit values; in the per-digit phases thread tid owns
+// digits tid * kPerThread .. tid * kPerThread + kPerThread - 1 (those below kBins).
+template <int BITS>
+struct Digits {
+    static constexpr int kBins = 1 << BITS;
+    static constexpr int kPerThread = kBins > 256 ? kBins / 256 : 1;
+    static constexpr uint32_t kMask = uint32_t(kBins - 1);
+    static_assert(kBins <= kMaxSortBins, "the plan's digit arrays");
+    __device__ static uint32_t of(uint32_t q) { return threadIdx.x * kPerThread + q; }
+};
+
+// Exclusive scan over the kBins digits in digit order, v and excl in each thread's own digits.
+template <int BITS>
+__device__ __forceinline__ void blockScanDigits(const uint32_t (&v)[Digits<BITS>::kPerThread],
+                                                uint32_t (&excl)[Digits<BITS>::kPerThread], uint32_t* sWarp) {
+    uint32_t sum = 0;
+#pragma unroll
+    for (int q = 0; q < Digits<BITS>::kPerThread; ++q) {
+        excl[q] = sum;
+        sum += v[q];
+    }
+    uint32_t total;
+    const uint32_t base = blockExclusiveScan256(sum, sWarp, &total);
+#pragma unroll
+    for (int q = 0; q < Digits<BITS>::kPerThread; ++q) excl[q] += base;
+}
+
 // ---- histogram of every pass's digit + the plan ---------------------------------------------
 constexpr int kHistItems = 16;
+template <int BITS>
 __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ SortArgs a) {
-    __shared__ uint32_t sHist[kMaxSortPasses][256];
+    using D = Digits<BITS>;
+    __shared__ uint32_t sHist[kMaxSortPasses][D::kBins];
     __shared__ uint32_t sWarp[8];
     __shared__ uint32_t sLast;
     __shared__ uint32_t sAny;
@@ -95,13 +124,13 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
         lowBits = a.fixedLowBits;
         keyBits = a.fixedKeyBits;
     }
-    uint32_t passes = entries ? (keyBits + 7) / 8 : 0;
+    uint32_t passes = entries ? (keyBits + BITS - 1) / BITS : 0;
     if (passes > a.passesLaunched) {  // planned for fewer bits than the keys carry: report
         if (threadIdx.x == 0 && blockIdx.x == 0) atomicOr(&ctl->c.status, uint32_t(GSR_CONTROL_KEY_RANGE));
         passes = a.passesLaunched;
     }
     const uint64_t keyMask = maskOf(keyBits);
-    for (uint32_t j = threadIdx.x; j < kMaxSortPasses * 256; j += 256) (&sHist[0][0])[j] = 0;
+    for (uint32_t j = threadIdx.x; j < kMaxSortPasses * D::kBins; j += 256) (&sHist[0][0])[j] = 0;
     __syncthreads();
     const uint64_t* keys = a.keys[0];
     // kHistItems independent loads per thread in flight before the counting
@@ -117,15 +146,16 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
         for (int j = 0; j < kHistItems; ++j) {
             if (base + j * 256 + threadIdx.x < entries) {
                 const uint64_t v = packed ? (k[j] >> indexBits) : virtualKey(k[j], lowBits, keyMask);
-                for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][uint32_t(v >> (8 * p)) & 0xFFu], 1u);
+                for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][uint32_t(v >> (BITS * p)) & D::kMask], 1u);
             }
         }
     }
     __syncthreads();
-    for (uint32_t p = 0; p < passes; ++p) {
-        const uint32_t c = sHist[p][threadIdx.x];
-        if (c) atomicAdd(&a.plan->hist[p][threadIdx.x], c);
-    }
+    for (uint32_t p = 0; p < passes; ++p)
+        for (uint32_t d = threadIdx.x; d < uint32_t(D::kBins); d += 256) {
+            const uint32_t c = sHist[p][d];
+            if (c) atomicAdd(&a.plan->hist[p][d], c);
+        }
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) sLast = atomicAdd(&ctl->histDone[a.frameMode == 2 ? 1 : 0], 1u) == gridDim.x - 1;
@@ -136,15 +166,24 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     SortPlan* plan = a.plan;
     uint32_t activeCount = 0;
     for (uint32_t p = 0; p < kMaxSortPasses; ++p) {
-        const uint32_t c = p < passes ? ldAcquire32(&plan->hist[p][threadIdx.x]) : 0;
+        uint32_t c[D::kPerThread];
+#pragma unroll
+        for (int q = 0; q < D::kPerThread; ++q) {
+            const uint32_t d = D::of(q);
+            c[q] = p < passes && d < uint32_t(D::kBins) ? ldAcquire32(&plan->hist[p][d]) : 0u;
+        }
         if (threadIdx.x == 0) sAny = 0;
         __syncthreads();
-        if (p < passes && c == entries) sAny = 1;  // one digit holds every key: constant
+#pragma unroll
+        for (int q = 0; q < D::kPerThread; ++q)
+            if (p < passes && D::of(q) < uint32_t(D::kBins) && c[q] == entries) sAny = 1;  // one digit holds every key
         __syncthreads();
         const bool active = p < passes && !sAny;
-        uint32_t total;
-        const uint32_t excl = blockExclusiveScan256(c, sWarp, &total);
-        plan->digitBase[p][threadIdx.x] = excl;
+        uint32_t excl[D::kPerThread];
+        blockScanDigits<BITS>(c, excl, sWarp);
+#pragma unroll
+        for (int q = 0; q < D::kPerThread; ++q)
+            if (D::of(q) < uint32_t(D::kBins)) plan->digitBase[p][D::of(q)] = excl[q];
         if (threadIdx.x == 0) {
             plan->active[p] = active ? 1u : 0u;
             plan->inBuffer[p] = activeCount & 1u;
@@ -158,6 +197,7 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
         plan->keyBits = keyBits;
         plan->packed = packed;
         plan->indexBits = indexBits;
+        plan->digitBits = BITS;
         plan->sortedBuffer = activeCount & 1u;
         if (a.frameMode == 2) return;  // the list's own plan fills the control block
         ctl->c.packed_entries = packed;
@@ -171,10 +211,12 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
 }
 
 // ---- one onesweep pass ------------------------------------------------------------------------
-// Decoupled look-back of digit d for tile t: the sum of the digit's counts over tiles 0..t-1.
-// Eight predecessors are read per round trip; a word that is not yet published (or carries an
-// older frame's epoch) stops the window and is re-read after a short sleep. Waits are bounded
-// by kSpinLimit (then the timeout is reported and the partial sum returned).
+// Decoupled look-back of digit d for tile t: the sum of the digit's counts over tiles 0..t-1
+// (status words [tile][BINS]). Eight predecessors are read per round trip; a word that is not
+// yet published (or carries an older frame's epoch) stops the window and is re-read after a
+// short sleep. Waits are bounded by kSpinLimit (then the timeout is reported and the partial
+// sum returned).
+template <int BINS>
 __device__ __forceinline__ uint32_t digitLookback(const uint64_t* status, uint32_t t, uint32_t d, uint32_t epoch,
                                                   DeviceControl* ctl) {
     constexpr int kWindow = 8;
@@ -185,7 +227,7 @@ __device__ __forceinline__ uint32_t digitLookback(const uint64_t* status, uint32
         uint64_t w[kWindow];
 #pragma unroll
         for (int j = 0; j < kWindow; ++j)
-            w[j] = q - j >= 0 ? ldRelaxed(&status[size_t(q - j) * 256 + d]) : packStatus(epoch, kFlagInclusive, 0);
+            w[j] = q - j >= 0 ? ldRelaxed(&status[size_t(q - j) * BINS + d]) : packStatus(epoch, kFlagInclusive, 0);
         int used = 0;
         bool found = false;
 #pragma unroll
@@ -214,40 +256,42 @@ __device__ __forceinline__ uint32_t digitLookback(const uint64_t* status, uint32
 // One pass over 256-thread tiles of kItems keys per thread. PAIRS = false: the entries are
 // single words (vkey << indexBits | index), 24 per thread; PAIRS = true: (tile << 32 | depth)
 // keys with a 32-bit value array, 16 per thread. The frame launches both and the one that does
-// not match the plan's layout returns at once. Three blocks per SM.
+// not match the plan's layout returns at once. BITS: the digit width.
 //   1) load; per-warp digit counts -> the tile's counts, published at once (aggregate, or
 //      inclusive for tile 0), and the tile's digit starts;
 //   2) ranks: peer masks of each warp step, a warp-private running count per digit; every key
 //      goes straight to its place in the tile's stable order in shared memory;
-//   3) the look-back of digit tid gives the global offset of the tile's run of that digit;
+//   3) the look-back of each digit a thread owns gives the global offset of the tile's run of
+//      that digit;
 //   4) the runs are written out, coalesced.
 // Items past the end of the list are loaded as all-ones keys: their digit is the largest one
 // the key width allows, they rank after every real key of the tile and are never stored.
-template <bool PAIRS, int ITEMS = PAIRS ? 16 : 24>
+template <bool PAIRS, int ITEMS, int BITS>
 struct PassShape {
     static constexpr int kItems = ITEMS;
     static constexpr int kTile = kSortThreads * kItems;
-    // keys, values, per-warp running counts [8][256], per-warp peer masks [8][2][256]
-    static constexpr int kSmemBytes = kTile * 8 + (PAIRS ? kTile * 4 : 0) + 8 * 256 * 4 * 3;
+    static constexpr int kBins = 1 << BITS;
+    // keys, values, per-warp running counts [8][kBins], per-warp peer masks [8][2][kBins]
+    static constexpr int kSmemBytes = kTile * 8 + (PAIRS ? kTile * 4 : 0) + 8 * kBins * 4 * 3;
 };
-static_assert(kSortThreads == 256, "one digit per thread");
-static_assert(PassShape<true>::kTile == kSortTile, "the status array is sized by the smaller tile");
-
-static_assert(PassShape<true>::kSmemBytes == PassShape<false>::kSmemBytes, "one launch serves both layouts");
-static_assert(PassShape<false, kDepthSortItems>::kTile == kDepthSortTile, "the depth status array is sized by this tile");
+static_assert(kSortThreads == 256, "256 threads own the digits");
+static_assert(PassShape<true, 16, 8>::kTile == kSortTile, "the status array is sized by the smaller tile");
+static_assert(PassShape<true, 16, 9>::kSmemBytes == PassShape<false, 24, 9>::kSmemBytes, "one launch serves both layouts");
+static_assert(PassShape<false, kDepthSortItems, 8>::kTile == kDepthSortTile, "the depth status array is sized by this tile");
 
 // The blocks of a pass are persistent: each takes tiles by ticket (the tile order of the
 // look-back) until the list is done, so a pass launches a fixed grid of blocks that all stay
 // resident (blocks only ever wait on tiles already taken by running blocks).
-template <bool PAIRS, int ITEMS = PAIRS ? 16 : 24>
+template <bool PAIRS, int ITEMS, int BITS>
 __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, unsigned char* smem, uint32_t* sOff,
                                               uint32_t* sScan, uint32_t& sTile) {
-    using S = PassShape<PAIRS, ITEMS>;
-    constexpr int kItems = S::kItems, kTile = S::kTile;
+    using S = PassShape<PAIRS, ITEMS, BITS>;
+    using D = Digits<BITS>;
+    constexpr int kItems = S::kItems, kTile = S::kTile, kBins = D::kBins, P = D::kPerThread;
     uint64_t* sKeys = reinterpret_cast<uint64_t*>(smem);
     uint32_t* sVals = reinterpret_cast<uint32_t*>(smem + kTile * 8);
-    uint32_t* sWarpCnt = reinterpret_cast<uint32_t*>(smem + kTile * (PAIRS ? 12 : 8));  // [8][256]
-    uint32_t* sMask = sWarpCnt + 8 * 256;                                                // [8][2][256]
+    uint32_t* sWarpCnt = reinterpret_cast<uint32_t*>(smem + kTile * (PAIRS ? 12 : 8));  // [8][kBins]
+    uint32_t* sMask = sWarpCnt + 8 * kBins;                                             // [8][2][kBins]
     const SortPlan* plan = a.plan;
     DeviceControl* ctl = a.ctl;
     const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -256,7 +300,7 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
     for (;;) {
     if (tid == 0) sTile = atomicAdd(&ctl->tickets[ticket], 1u);
 #pragma unroll
-    for (int j = 0; j < 24; ++j) sWarpCnt[j * 256 + tid] = 0;
+    for (int j = 0; j < 24 * kBins / 256; ++j) sWarpCnt[j * 256 + tid] = 0;
     __syncthreads();
     const uint32_t t = sTile;
     const uint32_t tileBase = t * kTile;
@@ -268,9 +312,9 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
     uint32_t* valsOut = a.values[in ^ 1u];
     const uint32_t lowBits = plan->lowBits;
     const uint64_t keyMask = maskOf(plan->keyBits);
-    const uint32_t shift = 8 * p + (PAIRS ? 0u : plan->indexBits);
+    const uint32_t shift = BITS * p + (PAIRS ? 0u : plan->indexBits);
     auto digit = [&](uint64_t k) -> uint32_t {
-        return PAIRS ? uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & 0xFFu : uint32_t(k >> shift) & 0xFFu;
+        return PAIRS ? uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & D::kMask : uint32_t(k >> shift) & D::kMask;
     };
 
     // 1) load, count, publish
@@ -283,26 +327,36 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
         key[j] = idx < entries ? __ldg(&keysIn[idx]) : ~0ull;
         if (PAIRS) val[PAIRS ? j : 0] = idx < entries ? __ldg(&valsIn[idx]) : 0u;
     }
-    uint32_t* wc = sWarpCnt + warp * 256;
+    uint32_t* wc = sWarpCnt + warp * kBins;
 #pragma unroll
     for (int j = 0; j < kItems; ++j)
         if (itemBase + j * 32 < entries) atomicAdd(&wc[digit(key[j])], 1u);
     __syncthreads();
-    const uint32_t d = tid;
     const uint32_t epoch = ctl->c.epoch;
-    uint64_t* status = a.status + (size_t(p) * a.maxTiles) * 256;
-    uint32_t blockCount = 0;
+    uint64_t* status = a.status + (size_t(p) * a.maxTiles) * kBins;
+    uint32_t blockCount[P];
 #pragma unroll
-    for (int w = 0; w < 8; ++w) {  // warp offsets of digit d, exclusive over the warps
-        const uint32_t c = sWarpCnt[w * 256 + d];
-        sWarpCnt[w * 256 + d] = blockCount;
-        blockCount += c;
+    for (int q = 0; q < P; ++q) {
+        const uint32_t d = D::of(q);
+        blockCount[q] = 0;
+        if (d >= uint32_t(kBins)) continue;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {  // warp offsets of digit d, exclusive over the warps
+            const uint32_t c = sWarpCnt[w * kBins + d];
+            sWarpCnt[w * kBins + d] = blockCount[q];
+            blockCount[q] += c;
+        }
+        stRelaxed(&status[size_t(t) * kBins + d], packStatus(epoch, t == 0 ? kFlagInclusive : kFlagAggregate, blockCount[q]));
     }
-    stRelaxed(&status[size_t(t) * 256 + d], packStatus(epoch, t == 0 ? kFlagInclusive : kFlagAggregate, blockCount));
-    uint32_t total;
-    const uint32_t blockStart = blockExclusiveScan256(blockCount, sScan, &total);
+    uint32_t blockStart[P];
+    blockScanDigits<BITS>(blockCount, blockStart, sScan);
 #pragma unroll
-    for (int w = 0; w < 8; ++w) sWarpCnt[w * 256 + d] += blockStart;
+    for (int q = 0; q < P; ++q) {
+        const uint32_t d = D::of(q);
+        if (d >= uint32_t(kBins)) continue;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) sWarpCnt[w * kBins + d] += blockStart[q];
+    }
     __syncthreads();
 
     // 2) ranks and the local stable order
@@ -311,13 +365,13 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
         const uint32_t dj = digit(key[j]);
-        uint32_t* mask = sMask + (warp * 2 + (j & 1)) * 256;
+        uint32_t* mask = sMask + (warp * 2 + (j & 1)) * kBins;
         atomicOr(&mask[dj], 1u << lane);
         __syncwarp();
         const uint32_t peers = mask[dj];
         const uint32_t run = wc[dj];  // the digit's running position in this warp's order
         // the previous step's masks were read by every lane before the last __syncwarp
-        if (j > 0 && prevLeader) sMask[(warp * 2 + ((j & 1) ^ 1)) * 256 + prevDigit] = 0;
+        if (j > 0 && prevLeader) sMask[(warp * 2 + ((j & 1) ^ 1)) * kBins + prevDigit] = 0;
         const uint32_t below = peers & ltMask;
         prevDigit = dj;
         prevLeader = below == 0;
@@ -330,13 +384,18 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
         if (below == 0) wc[dj] = run + __popc(peers);
     }
 
-    // 3) global offset of digit d's run
-    uint32_t exclusive = 0;
-    if (t > 0) {
-        exclusive = digitLookback(status, t, d, epoch, ctl);
-        stRelaxed(&status[size_t(t) * 256 + d], packStatus(epoch, kFlagInclusive, exclusive + blockCount));
+    // 3) global offsets of this thread's digits' runs
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+        const uint32_t d = D::of(q);
+        if (d >= uint32_t(kBins)) continue;
+        uint32_t exclusive = 0;
+        if (t > 0) {
+            exclusive = digitLookback<kBins>(status, t, d, epoch, ctl);
+            stRelaxed(&status[size_t(t) * kBins + d], packStatus(epoch, kFlagInclusive, exclusive + blockCount[q]));
+        }
+        sOff[d] = plan->digitBase[p][d] + exclusive - blockStart[q];
     }
-    sOff[d] = plan->digitBase[p][d] + exclusive - blockStart;
     __syncthreads();
 
     // 4) write-out
@@ -357,23 +416,27 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
 }
 
 // One pass in the layout the plan chose on the device (a skipped pass returns at once).
-__global__ void __launch_bounds__(kSortThreads, 3) sortPassKernel(const __grid_constant__ SortArgs a, uint32_t p) {
+template <int BITS>
+__global__ void __launch_bounds__(kSortThreads, BITS == 9 ? 2 : 3) sortPassKernel(const __grid_constant__ SortArgs a,
+                                                                                 uint32_t p) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ uint32_t sOff[256], sScan[8], sTile;
+    __shared__ uint32_t sOff[1 << BITS], sScan[8], sTile;
     const SortPlan* plan = a.plan;
     if (!plan->active[p]) return;
-    if (plan->packed) sortPassTiles<false>(a, p, smem, sOff, sScan, sTile);
-    else sortPassTiles<true>(a, p, smem, sOff, sScan, sTile);
+    if (plan->packed) sortPassTiles<false, 24, BITS>(a, p, smem, sOff, sScan, sTile);
+    else sortPassTiles<true, 16, BITS>(a, p, smem, sOff, sScan, sTile);
 }
 
 // One pass of binning mode's depth sort: always single words, 4096-key tiles (N / 4096 tiles, one
-// wave at N ~ 1M). Measured on B200 at N = 1.24M, 4 passes: 16 keys per thread 86 us, 12: 86,
-// 24 (the list sort's tile): 92, 8: 94, 4: 120.
-__global__ void __launch_bounds__(kSortThreads, 4) depthPassKernel(const __grid_constant__ SortArgs a, uint32_t p) {
+// wave at N ~ 1M). Measured on B200 at N = 1.24M, 4 passes of 8 bits: 16 keys per thread 86 us,
+// 12: 86, 24 (the list sort's tile): 92, 8: 94, 4: 120.
+template <int BITS>
+__global__ void __launch_bounds__(kSortThreads, BITS == 9 ? 2 : 4) depthPassKernel(const __grid_constant__ SortArgs a,
+                                                                                  uint32_t p) {
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ uint32_t sOff[256], sScan[8], sTile;
+    __shared__ uint32_t sOff[1 << BITS], sScan[8], sTile;
     if (!a.plan->active[p]) return;
-    sortPassTiles<false, kDepthSortItems>(a, p, smem, sOff, sScan, sTile);
+    sortPassTiles<false, kDepthSortItems, BITS>(a, p, smem, sOff, sScan, sTile);
 }
 
 // ---- tile ranges (tile_ranges.comp:22-44) -----------------------------------------------------
@@ -512,33 +575,49 @@ uint32_t gridFor(uint32_t n, uint32_t perBlock, uint32_t cap) {
 
 }  // namespace
 
-cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s) {
+namespace {
+template <int BITS>
+cudaError_t launchSortBits(const SortArgs& a, uint32_t histBlocks, cudaStream_t s) {
     static std::atomic<int> passGrids[64] = {}, depthGrids[64] = {};
     std::atomic<int>& passGrid = perDevice(passGrids);
     std::atomic<int>& depthGrid = perDevice(depthGrids);
-    constexpr int kListSmem = PassShape<false>::kSmemBytes, kDepthSmem = PassShape<false, kDepthSortItems>::kSmemBytes;
+    constexpr int kListSmem = PassShape<false, 24, BITS>::kSmemBytes;
+    constexpr int kDepthSmem = PassShape<false, kDepthSortItems, BITS>::kSmemBytes;
     if (!passGrid) {
-        cudaError_t e = cudaFuncSetAttribute(sortPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kListSmem);
+        cudaError_t e = cudaFuncSetAttribute(sortPassKernel<BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, kListSmem);
         if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(depthPassKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepthSmem);
+            e = cudaFuncSetAttribute(depthPassKernel<BITS>, cudaFuncAttributeMaxDynamicSharedMemorySize, kDepthSmem);
         if (e != cudaSuccess) return e;
         int dev = 0, sms = 148, perSm = 3, depthPerSm = 4;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, sortPassKernel, kSortThreads, kListSmem);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&depthPerSm, depthPassKernel, kSortThreads, kDepthSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, sortPassKernel<BITS>, kSortThreads, kListSmem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&depthPerSm, depthPassKernel<BITS>, kSortThreads, kDepthSmem);
         depthGrid = sms * (depthPerSm > 0 ? depthPerSm : 1);
         passGrid = sms * (perSm > 0 ? perSm : 1);
     }
-    sortHistKernel<<<histBlocks < 1 ? 1 : histBlocks, 256, 0, s>>>(a);
+    sortHistKernel<BITS><<<histBlocks < 1 ? 1 : histBlocks, 256, 0, s>>>(a);
     const bool depth = a.frameMode == 2;
     const uint32_t tiles = a.maxTiles < 1 ? 1 : a.maxTiles;
     const uint32_t limit = uint32_t(depth ? depthGrid : passGrid);
     const uint32_t grid = tiles < limit ? tiles : limit;
     for (uint32_t p = 0; p < a.passesLaunched; ++p) {
-        if (depth) depthPassKernel<<<grid, kSortThreads, kDepthSmem, s>>>(a, p);
-        else sortPassKernel<<<grid, kSortThreads, kListSmem, s>>>(a, p);
+        if (depth) depthPassKernel<BITS><<<grid, kSortThreads, kDepthSmem, s>>>(a, p);
+        else sortPassKernel<BITS><<<grid, kSortThreads, kListSmem, s>>>(a, p);
     }
     return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s) {
+    if (a.passesLaunched > uint32_t(kMaxSortPasses)) return cudaErrorInvalidValue;
+    switch (a.digitBits) {
+        case 7: return launchSortBits<7>(a, histBlocks, s);
+        case 9: return launchSortBits<9>(a, histBlocks, s);
+        case 0:
+        case 8: return launchSortBits<8>(a, histBlocks, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t launchRanges(const RenderArgs& a, uint32_t capacity, cudaStream_t s) {

@@ -100,7 +100,8 @@ struct FrontArgs {
 };
 
 // Sort plan written by the histogram kernel's last block.
-constexpr int kMaxSortPasses = 8;
+constexpr int kMaxSortPasses = 10;  // 64 key bits in 7-bit digits
+constexpr int kMaxSortBins = 512;   // digits of up to 9 bits
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
@@ -115,15 +116,16 @@ struct SortPlan {
     uint32_t indexBits;
     uint32_t active[kMaxSortPasses];
     uint32_t inBuffer[kMaxSortPasses];
-    uint32_t digitBase[kMaxSortPasses][256];
-    uint32_t hist[kMaxSortPasses][256];
+    uint32_t digitBits;     // digit width of the passes (7, 8 or 9)
+    uint32_t digitBase[kMaxSortPasses][kMaxSortBins];
+    uint32_t hist[kMaxSortPasses][kMaxSortBins];
     uint32_t sortedBuffer;  // the buffer that holds the result (active passes mod 2)
 };
 
 struct SortArgs {
     uint64_t* keys[2];
     uint32_t* values[2];
-    uint64_t* status;      // [kMaxSortPasses][maxTiles][256]
+    uint64_t* status;      // [passes][maxTiles][1 << digitBits]
     uint32_t maxTiles;     // ceil(capacity / kSortTile); the depth sort: ceil(count / kDepthSortTile)
     SortPlan* plan;
     DeviceControl* ctl;
@@ -137,6 +139,7 @@ struct SortArgs {
     uint32_t tileCount, count;  // frame mode: the grid's tiles and N (for the entry layout)
     uint32_t binning;
     uint32_t indexBits;         // frameMode 2: bits of the record index
+    uint32_t digitBits;         // 7, 8 or 9 bits a pass
 };
 
 struct RenderArgs {

@@ -434,8 +434,12 @@ struct GsrRenderer {
     DevBuf control, plan;
     // binning mode: the records' depth words (ping-pong), their sort's look-back words and plan
     DevBuf depthKeys[2], depthStatus, depthPlan;
-    static constexpr uint32_t kDepthSortPasses = 4;  // 32 depth bits
     bool binning() const { return settings.list_mode == GSR_LIST_BINNING; }
+    // the radix digit width of both sorts, and the depth sort's passes: its keys are the varying
+    // depth bits and the no-tile bit, at most 32 bits (depths are positive floats)
+    uint32_t digitBits() const { return settings.sort_digit_bits ? settings.sort_digit_bits : 8u; }
+    uint32_t depthPasses() const { return (32u + digitBits() - 1u) / digitBits(); }
+    size_t statusWordsPerTile() const { return size_t(1) << digitBits(); }
     // the output image: bytes per pixel, the kernel's format code, and the RGB8 companion
     uint32_t imageBytes() const {
         const uint32_t f = settings.output_format;
@@ -567,13 +571,14 @@ struct GsrRenderer {
         // the largest key: tile ids < tileCount + 1 (sentinel) above up to 32 depth bits (global)
         // or alone (binning)
         const uint32_t keyBits = bitWidth(tileCount) + (binning() ? 0u : 32u);
-        return (keyBits + 7) / 8;
+        return (keyBits + digitBits() - 1) / digitBits();
     }
 
     double bytesPerEntry() const {
         // keys (8 B) + values (4 B), each ping-ponged (binning: the one-word entries alone), + the
         // look-back words of the passes
-        return (binning() ? 16.0 : 24.0) + 0.5 * double(std::max<uint32_t>(passesUpper, 6));
+        const double statusPerPass = double(statusWordsPerTile()) * 8.0 / double(kSortTile);
+        return (binning() ? 16.0 : 24.0) + statusPerPass * double(std::max<uint32_t>(passesUpper, 6));
     }
 
     uint32_t capacityForBytes(double bytes) const {
@@ -590,7 +595,7 @@ struct GsrRenderer {
             GSR_CUDA(l->keys[b].alloc(size_t(capacity) * 8));
             if (!binning()) GSR_CUDA(l->values[b].alloc(size_t(capacity) * 4));  // binning entries are one word
         }
-        GSR_CUDA(l->status.alloc(size_t(l->passes) * l->maxTiles * 256 * 8));
+        GSR_CUDA(l->status.alloc(size_t(l->passes) * l->maxTiles * statusWordsPerTile() * 8));
         GSR_CUDA(cudaMemset(l->status.p, 0, l->status.bytes));
         GSR_CUDA(cudaEventCreateWithFlags(&l->lastUse, cudaEventDisableTiming));
         out = std::move(l);
@@ -618,7 +623,8 @@ struct GsrRenderer {
         if (settings.sort_window > 0) GSR_CUDA(rayDepth.alloc(n * 48));
         if (binning()) {
             for (auto& k : depthKeys) GSR_CUDA(k.alloc(n * 8));
-            GSR_CUDA(depthStatus.alloc(size_t(kDepthSortPasses) * ((n + kDepthSortTile - 1) / kDepthSortTile) * 256 * 8));
+            GSR_CUDA(depthStatus.alloc(size_t(depthPasses()) * ((n + kDepthSortTile - 1) / kDepthSortTile) *
+                                       statusWordsPerTile() * 8));
             GSR_CUDA(cudaMemset(depthStatus.p, 0, depthStatus.bytes));
         }
         GSR_CUDA(tileCounts.alloc(n * 4));
@@ -842,7 +848,7 @@ struct GsrRenderer {
         // frameBegin, preprocess, scan, duplicate, histogram, one per pass, ranges, render
         // binning: frameBegin, preprocess, depth histogram + passes, scan, duplicate, list
         // histogram + passes, ranges, render
-        kernelLaunches += (binning() ? 8 + kDepthSortPasses + list->passes : 7 + list->passes) + (split ? uint32_t(parts.size()) - 1 : 0);
+        kernelLaunches += (binning() ? 8 + depthPasses() + list->passes : 7 + list->passes) + (split ? uint32_t(parts.size()) - 1 : 0);
         timed = timing;
         ++frameIndex;
         return GSR_OK;
@@ -906,7 +912,8 @@ struct GsrRenderer {
             sd.maxTiles = uint32_t((size_t(scene.count) * viewCount + kDepthSortTile - 1) / kDepthSortTile);
             sd.plan = depthPlan.as<SortPlan>();
             sd.ctl = ctl;
-            sd.passesLaunched = kDepthSortPasses;
+            sd.passesLaunched = depthPasses();
+            sd.digitBits = digitBits();
             sd.frameMode = 2;
             sd.count = scene.count * viewCount;
             sd.indexBits = fa.recordBits;
@@ -928,6 +935,7 @@ struct GsrRenderer {
         sa.plan = sortPlan;
         sa.ctl = ctl;
         sa.passesLaunched = l.passes;
+        sa.digitBits = digitBits();
         sa.frameMode = 1;
         sa.binning = binning() ? 1u : 0u;
         sa.tileCount = tileCount;
@@ -1317,8 +1325,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
                     settings->raster_gather);
     if (settings->tile_stats > 1 || (settings->tile_stats && settings->sort_window > 0))
         return fail(GSR_ERROR_INVALID_ARGUMENT, "tile_stats %u (0 or 1, not with sort_window)", settings->tile_stats);
-    if (settings->sort_digit_bits != 0 && settings->sort_digit_bits != 8)
-        return fail(GSR_ERROR_INVALID_ARGUMENT, "sort digit bits %u (8)", settings->sort_digit_bits);
+    if (settings->sort_digit_bits != 0 && (settings->sort_digit_bits < 7 || settings->sort_digit_bits > 9))
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "sort digit bits %u (7, 8 or 9)", settings->sort_digit_bits);
     GSR_CUDA(r->control.alloc(sizeof(DeviceControl)));
     GSR_CUDA(cudaMemset(r->control.p, 0, sizeof(DeviceControl)));
     GSR_CUDA(r->plan.alloc(sizeof(SortPlan)));

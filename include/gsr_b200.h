@@ -158,8 +158,10 @@ typedef struct GsrSettings {
     uint32_t render_splat;             /* GsrRenderSplat (TileSettings::renderSplat, cli.h:34) */
     uint32_t sort_window;              /* StopThePop per-pixel window K (TileSettings::sortWindow, cli.h:46):
                                           0 = off (the list's order), 1..64 */
-    uint32_t sort_digit_bits;          /* radix digit width of the list sort; 0 = 8 (the reference's
-                                          GpuRadixSort digits, gpu_radix_sort.h:38-122) */
+    uint32_t sort_digit_bits;          /* radix digit width of the depth and list sorts: 7, 8 or 9 bits
+                                          a pass; 0 = 8 (the reference's GpuRadixSort digits,
+                                          gpu_radix_sort.h:38-122). 9 bits sort a 1080p frame's
+                                          25-bit depth keys in 3 passes instead of 4 */
     uint32_t tile_stats;               /* 1: the instrumented rasterizer with per-tile statistics
                                           (TileSettings::stats, splat_tile_renderer.h:102); not with
                                           sort_window; read with gsr_read_tile_stats */
