@@ -413,7 +413,8 @@ struct AdamArgs {
     float invBatch;
     float lr, beta1, beta2, eps;
     uint32_t* step;    // advanced here (t = step + 1 in the bias corrections)
-    float* lossOut;    // [steps] mean squared error per pair of each step
+    float* lossOut;    // mean squared error per pair of steps lossBase .. maxSteps - 1
+    uint32_t lossBase;
     uint32_t maxSteps;
 };
 
@@ -425,7 +426,7 @@ __global__ void adamStepKernel(const __grid_constant__ AdamArgs a) {
         for (uint32_t b = 0; b < a.blocks; ++b) g += a.partials[size_t(b) * (MlpLayout::kCount + 1) + p];
         g *= a.invBatch;
         if (p == uint32_t(MlpLayout::kCount)) {
-            if (step < a.maxSteps) a.lossOut[step] = g / 3.0f;  // per channel
+            if (step >= a.lossBase && step < a.maxSteps) a.lossOut[step - a.lossBase] = g / 3.0f;  // per channel
         } else {
             const float t = float(step + 1);
             const float m = a.beta1 * a.m[p] + (1.0f - a.beta1) * g;
@@ -572,7 +573,7 @@ __global__ void __launch_bounds__(kGateWarps * 32) gateKernel(const __grid_const
 
 cudaError_t launchColorTrainStep(const float* sh, const uint8_t* degrees, uint32_t count, uint32_t dirs, uint32_t seed,
                                  uint32_t batch, float* params, float* m, float* v, float* partials, uint32_t* step,
-                                 float lr, float* lossOut, uint32_t maxSteps, cudaStream_t s) {
+                                 float lr, float* lossOut, uint32_t lossBase, uint32_t maxSteps, cudaStream_t s) {
     static std::atomic<bool> configuredOn[64] = {};
     std::atomic<bool>& configured = perDevice(configuredOn);
     const int smem = int(sizeof(TrainSmem));
@@ -584,7 +585,8 @@ cudaError_t launchColorTrainStep(const float* sh, const uint8_t* degrees, uint32
     const uint32_t blocks = batch / kTcBlockSamples;
     TrainArgs ta{sh, degrees, count, dirs, seed, params, partials, step};
     trainStepKernel<<<blocks, kTcThreads, smem, s>>>(ta);
-    AdamArgs aa{params, m, v, partials, blocks, 1.0f / float(batch), lr, 0.9f, 0.999f, 1e-8f, step, lossOut, maxSteps};
+    AdamArgs aa{params, m, v, partials, blocks, 1.0f / float(batch), lr, 0.9f, 0.999f, 1e-8f, step, lossOut, lossBase,
+                maxSteps};
     adamStepKernel<<<(MlpLayout::kCount + 1 + 255) / 256, 256, 0, s>>>(aa);
     return cudaGetLastError();
 }
@@ -592,6 +594,11 @@ cudaError_t launchColorTrainStep(const float* sh, const uint8_t* degrees, uint32
 cudaError_t launchColorEncode(const float* sh, const float* params, uint4* latents, DecoderWeights* decoder,
                               uint32_t count, cudaStream_t s) {
     encodeLatentsKernel<<<(count + 127) / 128, 128, 0, s>>>(sh, params, latents, count);
+    packDecoderKernel<<<1, 256, 0, s>>>(params, decoder);
+    return cudaGetLastError();
+}
+
+cudaError_t launchPackDecoder(const float* params, DecoderWeights* decoder, cudaStream_t s) {
     packDecoderKernel<<<1, 256, 0, s>>>(params, decoder);
     return cudaGetLastError();
 }

@@ -208,7 +208,9 @@ cudaError_t launchShDecode(const SceneArgs& scene, uint32_t geometry, uint32_t c
 // partial sums, then Adam; step = {step counter, scratch counter} advanced on the device.
 cudaError_t launchColorTrainStep(const float* sh, const uint8_t* degrees, uint32_t count, uint32_t dirs, uint32_t seed,
                                  uint32_t batch, float* params, float* m, float* v, float* partials, uint32_t* step,
-                                 float lr, float* lossOut, uint32_t maxSteps, cudaStream_t s);
+                                 float lr, float* lossOut, uint32_t lossBase, uint32_t maxSteps, cudaStream_t s);
+// The tensor-core decoder packed from the fp32 parameters.
+cudaError_t launchPackDecoder(const float* params, struct DecoderWeights* decoder, cudaStream_t s);
 uint32_t colorTrainBatchMultiple();
 // Latents of every gaussian and the packed decoder from the trained parameters.
 cudaError_t launchColorEncode(const float* sh, const float* params, uint4* latents, struct DecoderWeights* decoder,

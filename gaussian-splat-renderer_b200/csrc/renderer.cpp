@@ -271,8 +271,12 @@ struct GsrColorModel {
     uint32_t count = 0;
     int degree = 3;
     GsrColorModelStats stats{};
-    std::vector<float> loss;
-    DevBuf params, latents, decoder;
+    GsrColorModelOptions options{};
+    uint32_t step = 0;        // Adam steps taken
+    std::vector<float> loss;  // of every step taken
+    // fp32 parameters, latents, packed decoder; Adam's moments and the device step counter
+    // ({step, scratch}) stay with the model so that training can resume from it
+    DevBuf params, latents, decoder, mom, vel, stepDev;
 };
 
 // ====================================================================================== scene
@@ -1688,6 +1692,77 @@ void initColorParams(uint32_t seed, std::vector<float>& p) {
 }
 }  // namespace
 
+namespace {
+// `steps` more Adam steps of the model on the scene's SH colour (from the model's state), then
+// the latents of every gaussian and the gate; the statistics cover every step taken so far.
+int trainColorModel(const GsrSceneDesc& scene, GsrColorModel& m, uint32_t steps) {
+    const GsrColorModelOptions& o = m.options;
+    const uint32_t n = scene.count, blocks = o.batch / colorTrainBatchMultiple();
+    DevBuf sh, degrees, partials, lossDev, counters;
+    GSR_CUDA(sh.alloc(size_t(n) * 48 * 4));
+    GSR_CUDA(degrees.alloc(n));
+    GSR_CUDA(partials.alloc(size_t(blocks) * (kColorModelParams + 1) * 4));
+    GSR_CUDA(lossDev.alloc(size_t(std::max(steps, 1u)) * 4));
+    GSR_CUDA(counters.alloc(8));
+    GSR_CUDA(cudaMemset(counters.p, 0, 8));
+    cudaStream_t s = nullptr;
+    GSR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    auto cleanup = [&]() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (s) cudaStreamDestroy(s);
+    };
+    cudaError_t ce = cudaEventCreate(&e0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e0, s);
+    if (ce == cudaSuccess)
+        ce = launchShDecode(sceneArgs(scene), scene.geometry, scene.color, n, m.degree, sh.as<float>(), degrees.as<uint8_t>(), s);
+    for (uint32_t k = 0; ce == cudaSuccess && k < steps; ++k)
+        ce = launchColorTrainStep(sh.as<float>(), degrees.as<uint8_t>(), n, o.directions, o.seed, o.batch,
+                                  m.params.as<float>(), m.mom.as<float>(), m.vel.as<float>(), partials.as<float>(),
+                                  m.stepDev.as<uint32_t>(), o.learning_rate, lossDev.as<float>(), m.step, m.step + steps, s);
+    if (ce == cudaSuccess)
+        ce = launchColorEncode(sh.as<float>(), m.params.as<float>(), m.latents.as<uint4>(), m.decoder.as<DecoderWeights>(), n, s);
+    if (ce == cudaSuccess)
+        ce = launchColorGate(sh.as<float>(), degrees.as<uint8_t>(), n, o.directions, m.decoder.as<DecoderWeights>(),
+                             m.latents.as<uint4>(), o.gate, counters.as<uint32_t>(), counters.as<uint32_t>() + 1, s);
+    if (ce == cudaSuccess) ce = cudaEventRecord(e1, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    float ms = 0.0f;
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
+    cleanup();
+    if (ce != cudaSuccess) return cudaFail(ce, "colour model training");
+    const size_t before = m.loss.size();
+    m.loss.resize(before + steps);
+    if (steps) GSR_CUDA(cudaMemcpy(m.loss.data() + before, lossDev.p, size_t(steps) * 4, cudaMemcpyDeviceToHost));
+    m.step += steps;
+    uint32_t cnt[2];
+    GSR_CUDA(cudaMemcpy(cnt, counters.p, 8, cudaMemcpyDeviceToHost));
+    GsrColorModelStats& st = m.stats;
+    st.gaussians = n;
+    st.fallback = cnt[0];
+    std::memcpy(&st.max_error_kept, &cnt[1], 4);
+    st.steps = m.step;
+    st.sh_degree = m.degree;
+    st.first_loss = m.loss.empty() ? 0.0f : m.loss.front();
+    st.final_loss = m.loss.empty() ? 0.0f : m.loss.back();
+    st.train_ms = ms;
+    return GSR_OK;
+}
+
+// The model's device buffers for n gaussians.
+int allocColorModel(GsrColorModel& m, uint32_t n) {
+    GSR_CUDA(m.params.alloc(size_t(kColorModelParams) * 4));
+    GSR_CUDA(m.mom.alloc(size_t(kColorModelParams) * 4));
+    GSR_CUDA(m.vel.alloc(size_t(kColorModelParams) * 4));
+    GSR_CUDA(m.stepDev.alloc(8));
+    GSR_CUDA(m.latents.alloc(size_t(n) * 16));
+    GSR_CUDA(m.decoder.alloc(kDecoderWeightsBytes));
+    return GSR_OK;
+}
+}  // namespace
+
 int gsr_color_model_train(const GsrSceneDesc* scene, const GsrColorModelOptions* options, GsrColorModel** out) {
     if (!scene || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
@@ -1702,74 +1777,97 @@ int gsr_color_model_train(const GsrSceneDesc* scene, const GsrColorModelOptions*
         return fail(GSR_ERROR_INVALID_ARGUMENT, "batch %u (a multiple of %u, at most 2^24)", o.batch, mult);
     if (o.steps == 0 || !(o.learning_rate > 0.0f) || !(o.gate >= 0.0f))
         return fail(GSR_ERROR_INVALID_ARGUMENT, "steps %u, learning rate %g, gate %g", o.steps, o.learning_rate, o.gate);
-    const int degree = o.sh_degree < 0 ? scene->sh_degree : std::min(o.sh_degree, scene->sh_degree);
     auto m = std::make_unique<GsrColorModel>();
-    const uint32_t n = scene->count;
-    m->count = n;
-    m->degree = degree;
-    const uint32_t blocks = o.batch / mult;
-    DevBuf sh, degrees, mom, vel, partials, step, lossDev, counters;
-    GSR_CUDA(sh.alloc(size_t(n) * 48 * 4));
-    GSR_CUDA(degrees.alloc(n));
-    GSR_CUDA(m->params.alloc(size_t(kColorModelParams) * 4));
-    GSR_CUDA(mom.alloc(size_t(kColorModelParams) * 4));
-    GSR_CUDA(vel.alloc(size_t(kColorModelParams) * 4));
-    GSR_CUDA(partials.alloc(size_t(blocks) * (kColorModelParams + 1) * 4));
-    GSR_CUDA(step.alloc(8));
-    GSR_CUDA(lossDev.alloc(size_t(o.steps) * 4));
-    GSR_CUDA(counters.alloc(8));
-    GSR_CUDA(m->latents.alloc(size_t(n) * 16));
-    GSR_CUDA(m->decoder.alloc(kDecoderWeightsBytes));
+    m->count = scene->count;
+    m->degree = o.sh_degree < 0 ? scene->sh_degree : std::min(o.sh_degree, scene->sh_degree);
+    m->options = o;
+    rc = allocColorModel(*m, scene->count);
+    if (rc) return rc;
     std::vector<float> p0;
     initColorParams(o.seed, p0);
     GSR_CUDA(cudaMemcpy(m->params.p, p0.data(), p0.size() * 4, cudaMemcpyHostToDevice));
-    GSR_CUDA(cudaMemset(mom.p, 0, mom.bytes));
-    GSR_CUDA(cudaMemset(vel.p, 0, vel.bytes));
-    GSR_CUDA(cudaMemset(step.p, 0, 8));
-    GSR_CUDA(cudaMemset(counters.p, 0, 8));
-    cudaStream_t s = nullptr;
-    GSR_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
-    auto cleanup = [&]() {
-        if (e0) cudaEventDestroy(e0);
-        if (e1) cudaEventDestroy(e1);
-        if (s) cudaStreamDestroy(s);
-    };
-    cudaError_t ce = cudaEventCreate(&e0);
-    if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
-    if (ce == cudaSuccess) ce = cudaEventRecord(e0, s);
-    if (ce == cudaSuccess)
-        ce = launchShDecode(sceneArgs(*scene), scene->geometry, scene->color, n, degree, sh.as<float>(), degrees.as<uint8_t>(), s);
-    for (uint32_t k = 0; ce == cudaSuccess && k < o.steps; ++k)
-        ce = launchColorTrainStep(sh.as<float>(), degrees.as<uint8_t>(), n, o.directions, o.seed, o.batch,
-                                  m->params.as<float>(), mom.as<float>(), vel.as<float>(), partials.as<float>(),
-                                  step.as<uint32_t>(), o.learning_rate, lossDev.as<float>(), o.steps, s);
-    if (ce == cudaSuccess)
-        ce = launchColorEncode(sh.as<float>(), m->params.as<float>(), m->latents.as<uint4>(),
-                               m->decoder.as<DecoderWeights>(), n, s);
-    if (ce == cudaSuccess)
-        ce = launchColorGate(sh.as<float>(), degrees.as<uint8_t>(), n, o.directions, m->decoder.as<DecoderWeights>(),
-                             m->latents.as<uint4>(), o.gate, counters.as<uint32_t>(), counters.as<uint32_t>() + 1, s);
-    if (ce == cudaSuccess) ce = cudaEventRecord(e1, s);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-    float ms = 0.0f;
-    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e0, e1);
-    cleanup();
-    if (ce != cudaSuccess) return cudaFail(ce, "colour model training");
-    m->loss.resize(o.steps);
-    GSR_CUDA(cudaMemcpy(m->loss.data(), lossDev.p, size_t(o.steps) * 4, cudaMemcpyDeviceToHost));
-    uint32_t cnt[2];
-    GSR_CUDA(cudaMemcpy(cnt, counters.p, 8, cudaMemcpyDeviceToHost));
-    GsrColorModelStats& st = m->stats;
-    st.gaussians = n;
-    st.fallback = cnt[0];
-    std::memcpy(&st.max_error_kept, &cnt[1], 4);
-    st.steps = o.steps;
-    st.sh_degree = degree;
-    st.first_loss = m->loss.front();
-    st.final_loss = m->loss.back();
-    st.train_ms = ms;
+    GSR_CUDA(cudaMemset(m->mom.p, 0, m->mom.bytes));
+    GSR_CUDA(cudaMemset(m->vel.p, 0, m->vel.bytes));
+    GSR_CUDA(cudaMemset(m->stepDev.p, 0, 8));
+    rc = trainColorModel(*scene, *m, o.steps);
+    if (rc) return rc;
     *out = m.release();
+    return GSR_OK;
+}
+
+int gsr_color_model_resume(const GsrSceneDesc* scene, GsrColorModel* model, uint32_t steps) {
+    if (!scene || !model) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    int rc = validateScene(*scene);
+    if (rc) return rc;
+    if (scene->count != model->count || model->degree > scene->sh_degree)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "colour model of %u gaussians (degree %d) for a scene of %u (degree %d)",
+                    model->count, model->degree, scene->count, scene->sh_degree);
+    GSR_CUDA(cudaDeviceSynchronize());  // renderers using the model finish their frames first
+    return trainColorModel(*scene, *model, steps);
+}
+
+int gsr_color_model_save(const GsrColorModel* model, const char* path) {
+    if (!model || !path) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    GSR_CUDA(cudaDeviceSynchronize());
+    std::vector<float> params(kColorModelParams), m(kColorModelParams), v(kColorModelParams);
+    std::vector<uint16_t> latents(size_t(model->count) * 8);
+    GSR_CUDA(cudaMemcpy(params.data(), model->params.p, params.size() * 4, cudaMemcpyDeviceToHost));
+    GSR_CUDA(cudaMemcpy(m.data(), model->mom.p, m.size() * 4, cudaMemcpyDeviceToHost));
+    GSR_CUDA(cudaMemcpy(v.data(), model->vel.p, v.size() * 4, cudaMemcpyDeviceToHost));
+    GSR_CUDA(cudaMemcpy(latents.data(), model->latents.p, latents.size() * 2, cudaMemcpyDeviceToHost));
+    GsrColorModelCheckpoint ck{};
+    ck.count = model->count;
+    ck.sh_degree = model->degree;
+    ck.step = model->step;
+    ck.loss_count = uint32_t(model->loss.size());
+    ck.options = model->options;
+    ck.stats = model->stats;
+    ck.params = params.data();
+    ck.adam_m = m.data();
+    ck.adam_v = v.data();
+    ck.loss = const_cast<float*>(model->loss.data());
+    ck.latents = latents.data();
+    return gsr_color_model_file_write(path, &ck);
+}
+
+int gsr_color_model_load(const GsrSceneDesc* scene, const char* path, GsrColorModel** out) {
+    if (!scene || !path || !out) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    int rc = validateScene(*scene);
+    if (rc) return rc;
+    GsrColorModelCheckpoint ck{};
+    rc = gsr_color_model_file_read(path, &ck);  // the sizes
+    if (rc) return rc;
+    if (ck.count != scene->count || ck.sh_degree < 0 || ck.sh_degree > scene->sh_degree)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "%s: a model of %u gaussians (degree %d) for a scene of %u (degree %d)", path,
+                    ck.count, ck.sh_degree, scene->count, scene->sh_degree);
+    std::vector<float> params(kColorModelParams), m(kColorModelParams), v(kColorModelParams), loss(ck.loss_count);
+    std::vector<uint16_t> latents(size_t(ck.count) * 8);
+    ck.params = params.data();
+    ck.adam_m = m.data();
+    ck.adam_v = v.data();
+    ck.loss = loss.data();
+    ck.latents = latents.data();
+    rc = gsr_color_model_file_read(path, &ck);
+    if (rc) return rc;
+    auto model = std::make_unique<GsrColorModel>();
+    model->count = ck.count;
+    model->degree = ck.sh_degree;
+    model->options = ck.options;
+    model->stats = ck.stats;
+    model->step = ck.step;
+    model->loss = std::move(loss);
+    rc = allocColorModel(*model, ck.count);
+    if (rc) return rc;
+    const uint32_t stepWords[2] = {ck.step, 0u};
+    GSR_CUDA(cudaMemcpy(model->params.p, params.data(), params.size() * 4, cudaMemcpyHostToDevice));
+    GSR_CUDA(cudaMemcpy(model->mom.p, m.data(), m.size() * 4, cudaMemcpyHostToDevice));
+    GSR_CUDA(cudaMemcpy(model->vel.p, v.data(), v.size() * 4, cudaMemcpyHostToDevice));
+    GSR_CUDA(cudaMemcpy(model->stepDev.p, stepWords, 8, cudaMemcpyHostToDevice));
+    GSR_CUDA(cudaMemcpy(model->latents.p, latents.data(), latents.size() * 2, cudaMemcpyHostToDevice));
+    GSR_CUDA(launchPackDecoder(model->params.as<float>(), model->decoder.as<DecoderWeights>(), nullptr));
+    GSR_CUDA(cudaDeviceSynchronize());
+    *out = model.release();
     return GSR_OK;
 }
 

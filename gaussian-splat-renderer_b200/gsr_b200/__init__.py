@@ -124,6 +124,12 @@ class ColorModelStats(C.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_ if name != "reserved"}
 
 
+class ColorModelCheckpoint(C.Structure):
+    _fields_ = [("count", C.c_uint32), ("sh_degree", C.c_int32), ("step", C.c_uint32), ("loss_count", C.c_uint32),
+                ("options", ColorModelOptions), ("stats", ColorModelStats), ("params", C.c_void_p),
+                ("adam_m", C.c_void_p), ("adam_v", C.c_void_p), ("loss", C.c_void_p), ("latents", C.c_void_p)]
+
+
 TUNE_MAX_CANDIDATES = 64
 
 
@@ -230,6 +236,11 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_color_model_train": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(ColorModelOptions), C.POINTER(vp)]),
         "gsr_color_model_stats": (C.c_int, [vp, C.POINTER(ColorModelStats)]),
         "gsr_color_model_read": (C.c_int, [vp, vp, vp, vp]),
+        "gsr_color_model_save": (C.c_int, [vp, C.c_char_p]),
+        "gsr_color_model_load": (C.c_int, [C.POINTER(SceneDesc), C.c_char_p, C.POINTER(vp)]),
+        "gsr_color_model_resume": (C.c_int, [C.POINTER(SceneDesc), vp, u32]),
+        "gsr_color_model_file_write": (C.c_int, [C.c_char_p, C.POINTER(ColorModelCheckpoint)]),
+        "gsr_color_model_file_read": (C.c_int, [C.c_char_p, C.POINTER(ColorModelCheckpoint)]),
         "gsr_renderer_set_color_model": (C.c_int, [vp, vp]),
         "gsr_color_model_destroy": (None, [vp]),
         "gsr_autotune": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(CSettings), vp, C.POINTER(SplatCamera), u32,
@@ -379,18 +390,39 @@ class ColorModel:
     BF16 MLP decoder; gaussians beyond the gate keep their SH colour."""
 
     def __init__(self, scene: GpuScene, steps: int = 2000, batch: int = 65536, directions: int = 64,
-                 learning_rate: float = 1e-3, seed: int = 1, gate: float = 2.0 / 255.0, sh_degree: int = -1):
+                 learning_rate: float = 1e-3, seed: int = 1, gate: float = 2.0 / 255.0, sh_degree: int = -1,
+                 _handle=None):
         lib = load()
+        self.scene = scene
+        self.count = int(scene.desc.count)
+        if _handle is not None:  # a loaded checkpoint
+            self._h = _handle
+            return
         o = ColorModelOptions()
         lib.gsr_color_model_options_default(C.byref(o))
         o.steps, o.batch, o.directions, o.learning_rate, o.seed, o.gate, o.sh_degree = (
             steps, batch, directions, learning_rate, seed, gate, sh_degree)
-        self.scene = scene
-        self.count = int(scene.desc.count)
-        self.steps = steps
         h = C.c_void_p()
         check(lib.gsr_color_model_train(C.byref(scene.desc), C.byref(o), C.byref(h)))
         self._h = h
+
+    @classmethod
+    def load(cls, scene: GpuScene, path) -> "ColorModel":
+        """gsr_color_model_load: a model from a checkpoint file, for `scene`."""
+        h = C.c_void_p()
+        check(load().gsr_color_model_load(C.byref(scene.desc), str(path).encode(), C.byref(h)))
+        return cls(scene, _handle=h)
+
+    def save(self, path):
+        check(load().gsr_color_model_save(self._h, str(path).encode()))
+
+    def resume(self, steps: int):
+        """gsr_color_model_resume: `steps` more Adam steps from the model's state."""
+        check(load().gsr_color_model_resume(C.byref(self.scene.desc), self._h, steps))
+
+    @property
+    def steps(self) -> int:
+        return int(self.stats()["steps"])
 
     @property
     def handle(self):
@@ -405,9 +437,9 @@ class ColorModel:
         """(latents uint16 [N, 8] fp16 bits, params float32 [5195], loss per step)."""
         lat = np.zeros((self.count, 8), np.uint16)
         par = np.zeros(COLOR_MODEL_PARAMS, np.float32)
-        loss = np.zeros(self.steps, np.float32)
+        loss = np.zeros(max(self.steps, 1), np.float32)
         check(load().gsr_color_model_read(self._h, lat.ctypes.data, par.ctypes.data, loss.ctypes.data))
-        return lat, par, loss
+        return lat, par, loss[:self.steps]
 
     def close(self):
         if getattr(self, "_h", None):
@@ -637,6 +669,40 @@ def autotune(scene: GpuScene, settings: Settings, cameras, depths=(1, 2, 4, 8, 1
                        "tile_size": c.tile_size, "sort_digit_bits": c.sort_digit_bits,
                        "views_per_s": round(c.views_per_s, 2), "ms_per_frame": round(c.ms_per_frame, 4)}
                       for c in res.table[:res.candidates]]}
+
+
+def read_color_checkpoint(path) -> dict:
+    """gsr_color_model_file_read (host only): the checkpoint's header fields and arrays."""
+    lib = load()
+    ck = ColorModelCheckpoint()
+    check(lib.gsr_color_model_file_read(str(path).encode(), C.byref(ck)))
+    arrays = {"params": np.zeros(COLOR_MODEL_PARAMS, np.float32), "adam_m": np.zeros(COLOR_MODEL_PARAMS, np.float32),
+              "adam_v": np.zeros(COLOR_MODEL_PARAMS, np.float32), "loss": np.zeros(ck.loss_count, np.float32),
+              "latents": np.zeros((ck.count, 8), np.uint16)}
+    for k, a in arrays.items():
+        setattr(ck, k, a.ctypes.data if a.size else None)
+    check(lib.gsr_color_model_file_read(str(path).encode(), C.byref(ck)))
+    return {"count": ck.count, "sh_degree": ck.sh_degree, "step": ck.step,
+            "options": {f: getattr(ck.options, f) for f, _ in ColorModelOptions._fields_ if f != "reserved"},
+            "stats": ck.stats.as_dict(), **arrays}
+
+
+def write_color_checkpoint(path, ck: dict):
+    """gsr_color_model_file_write (host only) from the fields read_color_checkpoint returns."""
+    lib = load()
+    c = ColorModelCheckpoint()
+    c.count, c.sh_degree, c.step = ck["count"], ck["sh_degree"], ck["step"]
+    lib.gsr_color_model_options_default(C.byref(c.options))
+    for f, v in ck.get("options", {}).items():
+        setattr(c.options, f, v)
+    for f, v in ck.get("stats", {}).items():
+        setattr(c.stats, f, v)
+    keep = {k: np.ascontiguousarray(ck[k], np.float32) for k in ("params", "adam_m", "adam_v", "loss")}
+    keep["latents"] = np.ascontiguousarray(ck["latents"], np.uint16)
+    c.loss_count = keep["loss"].size
+    for k, a in keep.items():
+        setattr(c, k, a.ctypes.data if a.size else None)
+    check(lib.gsr_color_model_file_write(str(path).encode(), C.byref(c)))
 
 
 def scan(in_ptr: int, index_ptr: int | None, out_ptr: int, total_ptr: int | None, count: int, mode: int, stream: int = 0):

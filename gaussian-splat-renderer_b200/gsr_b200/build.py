@@ -34,7 +34,7 @@ NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contr
 # (the rasterizer's image is held to a tolerance instead and uses FMA and the hardware exp2)
 EXACT_UNITS = {"k_front.cu", "k_encode.cu"}
 CU_UNITS = ["k_front.cu", "k_sort.cu", "k_render.cu", "k_encode.cu", "k_mlp.cu"]
-HOST_UNITS = ["renderer.cpp", "ply_loader.cpp", "training_cameras.cpp", "scene_io_abi.cpp"]
+HOST_UNITS = ["renderer.cpp", "ply_loader.cpp", "training_cameras.cpp", "scene_io_abi.cpp", "color_checkpoint.cpp"]
 
 
 def _run(cmd, verbose=False):

@@ -366,6 +366,48 @@ int gsr_color_model_read(const GsrColorModel* model, uint16_t* latents, float* p
 int gsr_renderer_set_color_model(GsrRenderer* r, const GsrColorModel* model);
 void gsr_color_model_destroy(GsrColorModel* model);
 
+/* ---- colour model checkpoints (no reference counterpart: its renderer keeps no trained state) --
+ * A checkpoint file holds everything a training run has made: the fp32 parameters, Adam's first
+ * and second moments, the steps taken, the options (seed, learning rate, batch, directions,
+ * gate), the statistics, the loss of every step and the per-gaussian latents (fp16 bits, NaN in
+ * the last half for the gaussians kept on SH). Layout, little-endian, version 1:
+ *   "GSRCLRM\0" | u32 version | u32 count | i32 sh_degree | u32 step | u32 loss_count | u32 params
+ *   | GsrColorModelOptions (48 B) | GsrColorModelStats (48 B) | f32 params[params] | f32 m[params]
+ *   | f32 v[params] | f32 loss[loss_count] | u16 latents[count * 8] | u32 CRC-32 (IEEE, of every
+ *   byte before it).
+ * Reading checks the magic, the version, the sizes against the file length and the CRC, and
+ * reports GSR_ERROR_FORMAT for a file that fails any of them, GSR_ERROR_IO when it cannot be
+ * read or written. */
+#define GSR_COLOR_MODEL_PARAMS 5195u
+#define GSR_COLOR_MODEL_FILE_VERSION 1u
+typedef struct GsrColorModelCheckpoint {
+    uint32_t count;               /* gaussians */
+    int32_t sh_degree;            /* the SH degree the model learned */
+    uint32_t step;                /* Adam steps taken */
+    uint32_t loss_count;          /* entries of loss */
+    GsrColorModelOptions options;
+    GsrColorModelStats stats;
+    float* params;                /* [GSR_COLOR_MODEL_PARAMS], in gsr_color_model_read's order */
+    float* adam_m;                /* [GSR_COLOR_MODEL_PARAMS] */
+    float* adam_v;                /* [GSR_COLOR_MODEL_PARAMS] */
+    float* loss;                  /* [loss_count] mean squared error per channel of each step */
+    uint16_t* latents;            /* [count * 8] */
+} GsrColorModelCheckpoint;
+/* Host only (no device needed): writes / reads a checkpoint file. Reading with NULL arrays
+ * fills the sizes and the header fields only, so the caller can size the arrays. */
+int gsr_color_model_file_write(const char* path, const GsrColorModelCheckpoint* checkpoint);
+int gsr_color_model_file_read(const char* path, GsrColorModelCheckpoint* checkpoint);
+/* Saves a trained model to a checkpoint file. */
+int gsr_color_model_save(const GsrColorModel* model, const char* path);
+/* A model from a checkpoint file for `scene` (the count and the learned degree must match);
+ * the decoder is packed from the parameters, the latents are the file's. */
+int gsr_color_model_load(const GsrSceneDesc* scene, const char* path, GsrColorModel** out);
+/* Continues training for `steps` more Adam steps from the model's parameters, moments and step
+ * counter with its options, then encodes the latents and applies the gate again. A run cut into
+ * pieces this way (with save and load between them) gives the same model bit for bit as one run
+ * of all the steps. */
+int gsr_color_model_resume(const GsrSceneDesc* scene, GsrColorModel* model, uint32_t steps);
+
 /* ---- autotuner (no reference counterpart) -------------------------------------------------
  * Times each candidate of a search space on the caller's cameras with renderers of the given
  * settings (and colour model, or NULL) and returns the fastest. The knobs: views per frame, the
