@@ -804,7 +804,7 @@ def run_batched_64(G, args, dist, sampler, stream_obj):
         rr.close()
     # batched: this rank's views in one frame; tile size and schedule autotuned
     d = len(mine)
-    tuned = settle_and_tune(G, gs, [cams[v] for v in mine], args, depths=(d,), tile_sizes=(16, 8), probe=d)
+    tuned = settle_and_tune(G, gs, [cams[v] for v in mine], args, depths=(d,), tile_sizes=(16, 8, 32), probe=d)
     rb = renderer_for(G, gs, args, tuned)
     bframes = Frames(G, cams, d, mine)
     batched = time_form(rb, bframes, args, dist, sampler, stream_obj)

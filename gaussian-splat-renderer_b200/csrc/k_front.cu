@@ -411,8 +411,9 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
     __syncthreads();
     const uint32_t i = blockIdx.x * kFrontThreads + tid;
     const size_t rec = size_t(view) * a.count + i;
-    // the binning grid: ceil(size / S) bins (INRIA's rectangles stay on the 16-px tiles)
-    const int gx = (int(sCam.width) + a.binSize - 1) / a.binSize, gy = (int(sCam.height) + a.binSize - 1) / a.binSize;
+    // the binning grid: ceil(size / bin) bins (INRIA's rectangles stay on the 16-px tiles)
+    const BinShape bs = binShapeOf(a.binSize);
+    const int gx = (int(sCam.width) + bs.sx - 1) >> bs.lx, gy = (int(sCam.height) + bs.sy - 1) >> bs.ly;
     uint32_t reason = kCullReasonCount;  // threads past the end
     uint32_t dmin = 0xFFFFFFFFu, dmax = 0;
     DevSplat s;
@@ -433,13 +434,13 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
                 p24ConicWords(cA, cB, cC, cO, p24w0, p24w1);
                 p24DecodeConic(p24w0, p24w1, cA, cB, cC, cO);
             }
-            const Coverage cv = makeCoverage(a.bounds, rect, a.binSize, gx, gy, s.cx, s.cy, cA, cB, cC, cO, a.logf);
+            const Coverage cv = makeCoverage(a.bounds, rect, bs, gx, gy, s.cx, s.cy, cA, cB, cC, cO, a.logf);
             const RowGeom g = rowGeom(cv);
             if (a.bounds != kBoundsRect) {
                 uint32_t* hintWords = reinterpret_cast<uint32_t*>(a.hints + rec);
                 int r0, rows;
                 bool spanForm;
-                count = coverageCountSpans(cv, g, a.binSize, gx, hintWords, reinterpret_cast<uint32_t*>(a.spanRows + rec),
+                count = coverageCountSpans(cv, g, bs, gx, hintWords, reinterpret_cast<uint32_t*>(a.spanRows + rec),
                                            r0, rows, spanForm);
                 if (spanForm) {
                     hintWords[0] = kSpanMarker | uint32_t(r0) | (uint32_t(rows) << 16);
@@ -447,7 +448,7 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
                     a.hints[rec] = coverageHint(cv, g);
                 }
             } else {
-                count = coverageCount(cv, g, a.binSize);
+                count = coverageCount(cv, g, bs);
             }
             s.cullReason = kCullVisible;
             if (!EXTRAS || a.renderSplat == kRenderSplatFull) reinterpret_cast<DevSplat*>(a.splats)[rec] = s;
@@ -618,7 +619,8 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
             }
         }
         RowGeom g;
-        const Coverage cv = coverageFromHint(a.bounds, rect, a.binSize, gx, gy, cx, cy, cA, cB, cC, hint, g);
+        const BinShape S = binShapeOf(a.binSize);
+        const Coverage cv = coverageFromHint(a.bounds, rect, S, gx, gy, cx, cy, cA, cB, cC, hint, g);
         // packed: (((tile << W) | depth mod 2^W) << indexBits) | index; the tile part added per entry
         const uint64_t packedBase =
             ((lay.lowBits >= 32 ? depthBits : (depthBits & ((1ull << lay.lowBits) - 1ull))) << lay.indexBits) | i;
@@ -631,7 +633,6 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
                 a.values[k] = i;
             }
         };
-        const int S = a.binSize;
         int r0, r1;
         coverageRows(cv, S, r0, r1);
         uint32_t written = 0;

@@ -65,7 +65,12 @@ __device__ __forceinline__ float approxSqrt(float x) {
     return y;
 }
 
-// The warp strips (8 x 4 pixel blocks of a TILE x TILE tile; bit w = warp w's) that a record's
+// Render tiles by their code: 16 (16 x 16, INRIA's), 8 (8 x 8) or 32 (32 x 8).
+__host__ __device__ constexpr int tileW(int code) { return code; }
+__host__ __device__ constexpr int tileH(int code) { return code == 32 ? 8 : code; }
+__host__ __device__ constexpr int tilePixels(int code) { return tileW(code) * tileH(code); }
+
+// The warp strips (8 x 4 pixel blocks of a tile; bit w = warp w's) that a record's
 // cutoff ellipse q(d) = A dx^2 + 2B dx dy + C dy^2 <= t meets, computed once per record. At
 // distance dy = cy - y from the centre the ellipse's run is cx + (B/A) dy -/+ sqrt((t - (D/A) dy^2)
 // / A); over a strip row's y-range its right edge (concave in dy) peaks at the ellipse's
@@ -73,10 +78,10 @@ __device__ __forceinline__ float approxSqrt(float x) {
 // point. The test keeps the margins of the tile-coverage box: t + 0.2 %, the y-range widened by
 // 0.05 px, the run by 0.1 % + 0.05 px, over a continuous y-range (a superset of the pixel rows),
 // so a strip holding a pixel with alpha >= 1/255 is always set; a NaN sets the strip.
-template <uint32_t TILE>
+template <int TILE>
 __device__ __forceinline__ uint32_t stripMask(float cx, float cy, float A, float B, float C, float D, float t,
                                               float tileX, float tileY) {
-    constexpr uint32_t kStripsX = TILE / 8, kGroups = TILE / 4;
+    constexpr uint32_t kStripsX = tileW(TILE) / 8, kGroups = tileH(TILE) / 4;
     const float tt = t * 1.002f;
     const float ia = 1.0f / A, bA = B * ia, dA = D * ia;
     const float ey = approxSqrt(tt / dA);
@@ -269,7 +274,8 @@ __device__ __forceinline__ void windowPush(SortWindow<CAP>& q, uint32_t K, float
 // layout's kernel carries only its own gather and decode (a runtime switch measured 8 % slower).
 // CAP: 0, or the StopThePop window's register capacity; `ray` is then the shared area of the
 // gathered ray-depth parameters (3 x 16 B per entry, double-buffered).
-// TILE: the tile's edge, 16 (INRIA's tiles) or 8 pixels; one thread per pixel, batches of TILE^2
+// TILE: the tile's code, 16 (INRIA's 16 x 16 tiles), 8 (8 x 8) or 32 (32 x 8); one thread per pixel, batches of
+// a tile's pixel count
 // entries, and each warp owns an 8 x 4 pixel block of the tile (its strip: a squarer footprint
 // meets fewer ellipses than a 16 x 2 row pair).
 // STATS: the instrumented build (TileSettings::stats, tile_render.comp's GSR_TILE_STATS): the
@@ -281,18 +287,20 @@ __device__ __forceinline__ void windowPush(SortWindow<CAP>& q, uint32_t K, float
 // GATHER: how the batch reaches shared memory (kGatherCpAsync or kGatherTma; TMA only with the
 // full records, no window and no statistics); map = the tensor map of the record array (TMA).
 template <int MODE, int CAP, int TILE, bool STATS, int GATHER>
-__device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TILE * TILE, GATHER>& sm,
-                                           float4 (*ray)[3][TILE * TILE], uint32_t tile, const CUtensorMap* map) {
+__device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<tilePixels(TILE), GATHER>& sm,
+                                           float4 (*ray)[3][tilePixels(TILE)], uint32_t tile, const CUtensorMap* map) {
     static_assert(GATHER == kGatherCpAsync || (MODE == kRenderSplatFull && CAP == 0 && !STATS), "the TMA gather");
-    constexpr uint32_t kThreads = TILE * TILE, kStripW = 8, kRows = 4, kStripsX = TILE / kStripW;
-    static_assert(kThreads <= kRenderThreads && kStripW * kRows == 32 && TILE % kStripW == 0, "tile shape");
+    constexpr uint32_t kTW = tileW(TILE), kTH = tileH(TILE);
+    constexpr uint32_t kThreads = kTW * kTH, kStripW = 8, kRows = 4, kStripsX = kTW / kStripW;
+    static_assert(kThreads <= kRenderThreads && kStripW * kRows == 32 && kTW % kStripW == 0 && kTH % kRows == 0,
+                  "tile shape");
     const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
     const uint32_t sx = (warp % kStripsX) * kStripW, sy = (warp / kStripsX) * kRows;
     const uint32_t view = viewOfTile(a, tile);
     const DevView vw = a.views[view];
     const uint32_t local = tile - vw.tileBase;
     const uint32_t tx = local % vw.tilesX, ty = local / vw.tilesX;
-    const uint32_t px = tx * TILE + sx + (lane % kStripW), py = ty * TILE + sy + (lane / kStripW);
+    const uint32_t px = tx * kTW + sx + (lane % kStripW), py = ty * kTH + sy + (lane / kStripW);
     const bool inside = px < vw.width && py < vw.height;
     uint2 range = reinterpret_cast<const uint2*>(a.ranges)[tile];
     // a frame whose look-back gave up (GSR_CONTROL_TIMEOUT) has meaningless ranges: every index
@@ -470,7 +478,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<TIL
                 const float rho = fabsf(B) * rsqrtf(A * C);
                 const float K = 2.0f / fmaxf(1.0f - rho, 1e-30f);
                 const float t = qmax + (2e-3f + 4e-5f * K) * fmaxf(qmax, 1.0f) + 4e-3f;
-                if (t < 1e30f) strips = stripMask<TILE>(r0.x, r0.y, A, B, C, D, t, float(tx * TILE), float(ty * TILE));
+                if (t < 1e30f) strips = stripMask<TILE>(r0.x, r0.y, A, B, C, D, t, float(tx * kTW), float(ty * kTH));
             }
             sm.strips[tid] = strips;
             sm.conic[tid] = make_float4(-0.5f * kLog2e * A, -kLog2e * B, -0.5f * kLog2e * C, o);
@@ -624,29 +632,29 @@ __device__ __forceinline__ void initStage(RenderShared<N, GATHER>& sm) {
 // Without the window: five 256-thread blocks (or the same threads in 8-px tiles) per SM, 48
 // registers a thread (the strip masks would take 61, four blocks, 5 % slower).
 template <int MODE, int CAP, int TILE, bool STATS, int GATHER>
-__global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1)
+__global__ void __launch_bounds__(tilePixels(TILE), CAP == 0 ? 5 * 256 / (tilePixels(TILE)) : 1)
     renderKernel(const __grid_constant__ RenderArgs a, const __grid_constant__ CUtensorMap map) {
     extern __shared__ __align__(128) unsigned char smemRaw[];
-    RenderShared<TILE * TILE, GATHER>& sm = *reinterpret_cast<RenderShared<TILE * TILE, GATHER>*>(smemRaw);
+    RenderShared<tilePixels(TILE), GATHER>& sm = *reinterpret_cast<RenderShared<tilePixels(TILE), GATHER>*>(smemRaw);
     initStage(sm);
-    renderTile<MODE, CAP, TILE, STATS, GATHER>(a, sm, CAP > 0 ? rayArea<TILE * TILE, GATHER>(smemRaw) : nullptr,
+    renderTile<MODE, CAP, TILE, STATS, GATHER>(a, sm, CAP > 0 ? rayArea<tilePixels(TILE), GATHER>(smemRaw) : nullptr,
                                                blockIdx.x + a.tileOffset, &map);
 }
 
 // Persistent schedule: each block takes tiles from the frame's queue counter (reset by frame
 // begin) until the counter passes the last tile.
 template <int MODE, int CAP, int TILE, bool STATS, int GATHER>
-__global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE) : 1)
+__global__ void __launch_bounds__(tilePixels(TILE), CAP == 0 ? 5 * 256 / (tilePixels(TILE)) : 1)
     renderPersistentKernel(const __grid_constant__ RenderArgs a, const __grid_constant__ CUtensorMap map) {
     extern __shared__ __align__(128) unsigned char smemRaw[];
-    RenderShared<TILE * TILE, GATHER>& sm = *reinterpret_cast<RenderShared<TILE * TILE, GATHER>*>(smemRaw);
+    RenderShared<tilePixels(TILE), GATHER>& sm = *reinterpret_cast<RenderShared<tilePixels(TILE), GATHER>*>(smemRaw);
     initStage(sm);
     for (;;) {
         if (threadIdx.x == 0) sm.tile = atomicAdd(&a.ctl->tickets[kRenderQueueTicket], 1u);
         __syncthreads();
         const uint32_t tile = sm.tile;
         if (tile >= a.totalTiles) break;
-        renderTile<MODE, CAP, TILE, STATS, GATHER>(a, sm, CAP > 0 ? rayArea<TILE * TILE, GATHER>(smemRaw) : nullptr,
+        renderTile<MODE, CAP, TILE, STATS, GATHER>(a, sm, CAP > 0 ? rayArea<tilePixels(TILE), GATHER>(smemRaw) : nullptr,
                                                    tile, &map);
         __syncthreads();  // every thread has read sm.tile and left the tile's shared buffers
     }
@@ -654,8 +662,8 @@ __global__ void __launch_bounds__(TILE * TILE, CAP == 0 ? 5 * 256 / (TILE * TILE
 
 template <int MODE, int CAP, int TILE, bool STATS = false, int GATHER = kGatherCpAsync>
 cudaError_t launchRenderMode(const RenderArgs& a, cudaStream_t s) {
-    constexpr size_t smem = renderSmemBytes<CAP, TILE * TILE, GATHER>();
-    constexpr uint32_t threads = TILE * TILE;
+    constexpr size_t smem = renderSmemBytes<CAP, tilePixels(TILE), GATHER>();
+    constexpr uint32_t threads = tilePixels(TILE);
     static std::atomic<bool> configuredOn[64] = {};
     std::atomic<bool>& configured = perDevice(configuredOn);
     if (!configured) {
@@ -696,7 +704,9 @@ cudaError_t launchRenderWindow(const RenderArgs& a, cudaStream_t s) {
 }
 template <int MODE>
 cudaError_t launchRenderTile(const RenderArgs& a, cudaStream_t s) {
-    return a.tileSize == 8 ? launchRenderWindow<MODE, 8>(a, s) : launchRenderWindow<MODE, 16>(a, s);
+    if (a.tileSize == 8) return launchRenderWindow<MODE, 8>(a, s);
+    if (a.tileSize == 32) return launchRenderWindow<MODE, 32>(a, s);
+    return launchRenderWindow<MODE, 16>(a, s);
 }
 
 }  // namespace

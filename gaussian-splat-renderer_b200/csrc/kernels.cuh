@@ -70,7 +70,7 @@ struct FrontArgs {
     uint32_t count;       // N
     int evalDegree;       // min(stored degree, max_sh_degree)
     uint32_t bounds;      // GsrTileBounds
-    int binSize;          // S (16)
+    int binSize;          // the bins: 16 or 8 (S x S), 32 (32 x 8)
     uint32_t capacity;    // list entries
     void* splats;         // DevSplat[V * N] (full render records)
     uint32_t renderSplat; // kRenderSplatFull / P32 / P24

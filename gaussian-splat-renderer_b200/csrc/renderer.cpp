@@ -442,6 +442,9 @@ struct GsrRenderer {
     // the radix digit width of both sorts, and the depth sort's passes: its keys are the varying
     // depth bits and the no-tile bit, at most 32 bits (depths are positive floats)
     uint32_t digitBits() const { return settings.sort_digit_bits ? settings.sort_digit_bits : 8u; }
+    // the binning / render tiles: tile_size 16 or 8 (square), 32 (32 x 8)
+    uint32_t tileW() const { return settings.tile_size; }
+    uint32_t tileH() const { return settings.tile_size == 32 ? 8u : settings.tile_size; }
     uint32_t depthPasses() const { return (32u + digitBits() - 1u) / digitBits(); }
     size_t statusWordsPerTile() const { return size_t(1) << digitBits(); }
     // the output image: bytes per pixel, the kernel's format code, and the RGB8 companion
@@ -658,8 +661,7 @@ struct GsrRenderer {
             if (w[i] == 0 || h[i] == 0 || w[i] > 32768 || h[i] > 32768)
                 return fail(GSR_ERROR_INVALID_ARGUMENT, "render size %ux%u", w[i], h[i]);
             if (same && (views[i].width != w[i] || views[i].height != h[i])) same = false;
-            const uint32_t S = settings.tile_size;  // the binning / render tiles
-            tiles += uint64_t((w[i] + S - 1) / S) * ((h[i] + S - 1) / S);
+            tiles += uint64_t((w[i] + tileW() - 1) / tileW()) * ((h[i] + tileH() - 1) / tileH());
             pixels += uint64_t(w[i]) * h[i];
         }
         if (same) return GSR_OK;
@@ -675,8 +677,8 @@ struct GsrRenderer {
             GsrViewLayout& L = views[i];
             L.width = w[i];
             L.height = h[i];
-            L.tiles_x = (w[i] + settings.tile_size - 1) / settings.tile_size;
-            L.tiles_y = (h[i] + settings.tile_size - 1) / settings.tile_size;
+            L.tiles_x = (w[i] + tileW() - 1) / tileW();
+            L.tiles_y = (h[i] + tileH() - 1) / tileH();
             L.tile_base = tileBase;
             L.pixel_base = pixelBase;
             dv[i] = DevView{L.tile_base, L.tiles_x, L.tiles_y, L.width, L.height, 0, L.pixel_base};
@@ -1300,8 +1302,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     *out = nullptr;
     int rc = validateScene(*scene);
     if (rc) return rc;
-    if (settings->tile_size != 8 && settings->tile_size != 16)
-        return fail(GSR_ERROR_INVALID_ARGUMENT, "--tile-size must be 8 or 16 (a divisor of INRIA's 16-px tiles)");
+    if (settings->tile_size != 8 && settings->tile_size != 16 && settings->tile_size != 32)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "--tile-size must be 8, 16 or 32 (8 x 8, 16 x 16 or 32 x 8 tiles)");
     if (settings->bounds > GSR_BOUNDS_CUTOFF_ONLY) return fail(GSR_ERROR_INVALID_ARGUMENT, "bounds %u", settings->bounds);
     if (settings->output_format > GSR_OUTPUT_RGBA8)
         return fail(GSR_ERROR_INVALID_ARGUMENT, "output format %u", settings->output_format);

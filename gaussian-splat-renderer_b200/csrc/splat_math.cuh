@@ -262,23 +262,35 @@ __device__ __forceinline__ Ellipse makeEllipse(float cx, float cy, float A, floa
     return e;
 }
 
-// floorDivClamped (tile_coverage.cpp:54). S is 16 or 8: dividing by a power of two is exactly
+// The bins of the binning grid, sx x sy pixels (lx, ly their base-2 logarithms). The reference's
+// bins are square, S x S with S = 16 or 8 (tile_coverage.cpp); code 32 names 32 x 8 bins, as many
+// pixels as a 16 x 16 tile. With sx = sy = S every expression below is the reference's.
+struct BinShape {
+    int sx, sy, lx, ly;
+};
+__device__ __forceinline__ BinShape binShapeOf(int code) {
+    const int sy = code == 32 ? 8 : code;
+    return BinShape{code, sy, code == 32 ? 5 : (code == 16 ? 4 : 3), sy == 16 ? 4 : 3};
+}
+
+// floorDivClamped (tile_coverage.cpp:54). S is 32, 16 or 8: dividing by a power of two is exactly
 // multiplying by its reciprocal (both give the exact quotient, or round the same exact value),
 // so the quotient is the reference's without a division sequence.
 __device__ __forceinline__ int floorDivClamped(float v, int S) {
-    const float inv = S == 16 ? 0.0625f : (S == 8 ? 0.125f : 0.0f);
+    const float inv = S == 16 ? 0.0625f : (S == 8 ? 0.125f : (S == 32 ? 0.03125f : 0.0f));
     const float c = sclamp(v, -65536.0f, 1048576.0f);
     return ftoi(floorf(inv != 0.0f ? c * inv : c / float(S)));
 }
 
-// rectToBins (tile_coverage.cpp:102-105).
-__device__ __forceinline__ BinRect rectToBins(const TileRect& r, int S, int gx, int gy) {
-    const int f = 16 / S;
-    return {r.minX * f, r.minY * f, imin(r.maxX * f, gx), imin(r.maxY * f, gy)};
+// rectToBins (tile_coverage.cpp:102-105): the bins holding the 16-px rectangle's pixels (its
+// first bin rounds down, its end up; for bins that divide 16 this is the reference's r * 16 / S).
+__device__ __forceinline__ BinRect rectToBins(const TileRect& r, const BinShape& bs, int gx, int gy) {
+    return {(r.minX << 4) >> bs.lx, (r.minY << 4) >> bs.ly, imin(((r.maxX << 4) + bs.sx - 1) >> bs.lx, gx),
+            imin(((r.maxY << 4) + bs.sy - 1) >> bs.ly, gy)};
 }
 
 // makeCoverage (tile_coverage.cpp:107-117).
-__device__ __forceinline__ Coverage makeCoverage(uint32_t mode, const TileRect& rect16, int S, int gx, int gy,
+__device__ __forceinline__ Coverage makeCoverage(uint32_t mode, const TileRect& rect16, const BinShape& S, int gx, int gy,
                                                  float cx, float cy, float A, float B, float C, float opacity,
                                                  const LogfFixups& logf) {
     Coverage cv;
@@ -295,7 +307,7 @@ __device__ __forceinline__ Coverage makeCoverage(uint32_t mode, const TileRect& 
 }
 
 // coverageRows (tile_coverage.cpp:119-122) with ellipseRows (56-63).
-__device__ __forceinline__ void coverageRows(const Coverage& cv, int S, int& r0, int& r1) {
+__device__ __forceinline__ void coverageRows(const Coverage& cv, const BinShape& S, int& r0, int& r1) {
     if (!cv.useEllipse) {
         r0 = cv.bins.y0;
         r1 = imax(cv.bins.y0, cv.bins.y1);
@@ -309,8 +321,8 @@ __device__ __forceinline__ void coverageRows(const Coverage& cv, int S, int& r0,
     }
     const float y0 = ceilf(e.cy - e.eyPad);
     const float y1 = floorf(e.cy + e.eyPad);
-    const int lo = imax(cv.bins.y0, floorDivClamped(y0, S));
-    const int hi = imin(cv.bins.y1, floorDivClamped(y1, S) + 1);
+    const int lo = imax(cv.bins.y0, floorDivClamped(y0, S.sy));
+    const int hi = imin(cv.bins.y1, floorDivClamped(y1, S.sy) + 1);
     r0 = lo;
     r1 = imax(lo, hi);
 }
@@ -334,15 +346,16 @@ __device__ __forceinline__ RowGeom rowGeom(const Coverage& cv) {
 }
 
 // coverageRowSpan (tile_coverage.cpp:124-127) with ellipseRowBounds/ellipseRowSpan (70-96).
-__device__ __forceinline__ void coverageRowSpan(const Coverage& cv, const RowGeom& g, int row, int S, int& x0, int& x1) {
+__device__ __forceinline__ void coverageRowSpan(const Coverage& cv, const RowGeom& g, int row, const BinShape& S, int& x0,
+                                                int& x1) {
     if (!cv.useEllipse) {
         x0 = cv.bins.x0;
         x1 = imax(cv.bins.x0, cv.bins.x1);
         return;
     }
     const Ellipse& e = cv.e;
-    const float ey0 = float(row * S) - e.cy;
-    const float ey1 = float(row * S + S - 1) - e.cy;
+    const float ey0 = float(row * S.sy) - e.cy;
+    const float ey1 = float(row * S.sy + S.sy - 1) - e.cy;
     const float lo = smax(ey0, -e.eyPad);
     const float hi = smin(ey1, e.eyPad);
     if (!(lo <= hi)) {
@@ -356,14 +369,14 @@ __device__ __forceinline__ void coverageRowSpan(const Coverage& cv, const RowGeo
     const float xLeft = (-e.B * eyLeft - sqrtf(smax(0.0f, g.At - e.D * eyLeft * eyLeft))) / e.A;
     const float fx0 = e.cx + xLeft - g.pad;
     const float fx1 = e.cx + xRight + g.pad;
-    const int a = imax(cv.bins.x0, floorDivClamped(ceilf(fx0), S));
-    const int c = imin(cv.bins.x1, floorDivClamped(floorf(fx1), S) + 1);
+    const int a = imax(cv.bins.x0, floorDivClamped(ceilf(fx0), S.sx));
+    const int c = imin(cv.bins.x1, floorDivClamped(floorf(fx1), S.sx) + 1);
     x0 = a;
     x1 = imax(a, c);
 }
 
 // coverageCount (tile_coverage.cpp:129-138).
-__device__ __forceinline__ uint32_t coverageCount(const Coverage& cv, const RowGeom& g, int S) {
+__device__ __forceinline__ uint32_t coverageCount(const Coverage& cv, const RowGeom& g, const BinShape& S) {
     int r0, r1;
     coverageRows(cv, S, r0, r1);
     if (!cv.useEllipse) return uint32_t(imax(0, cv.bins.x1 - cv.bins.x0) * (r1 - r0));
@@ -390,7 +403,7 @@ __device__ __forceinline__ bool isSpanHint(const float4& h) {
 
 // coverageCount that also stores the rows' runs of a span hint (spanForm: rows <= kSpanRows and
 // the grid's width below 65536) into `hint` (rows 0-2, words 1-3) and `more` (rows 3-6).
-__device__ __forceinline__ uint32_t coverageCountSpans(const Coverage& cv, const RowGeom& g, int S, int gx,
+__device__ __forceinline__ uint32_t coverageCountSpans(const Coverage& cv, const RowGeom& g, const BinShape& S, int gx,
                                                        uint32_t* hint, uint32_t* more, int& r0, int& rows,
                                                        bool& spanForm) {
     int r1;
@@ -424,7 +437,7 @@ __device__ __forceinline__ float4 coverageHint(const Coverage& cv, const RowGeom
     return make_float4(e.t, g.exTrue, sqrtf(e.t * e.A / e.D), g.eyRight0);
 }
 
-__device__ __forceinline__ Coverage coverageFromHint(uint32_t mode, const TileRect& rect16, int S, int gx, int gy,
+__device__ __forceinline__ Coverage coverageFromHint(uint32_t mode, const TileRect& rect16, const BinShape& S, int gx, int gy,
                                                      float cx, float cy, float A, float B, float C, const float4& h,
                                                      RowGeom& g) {
     Coverage cv;

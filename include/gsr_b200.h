@@ -145,7 +145,9 @@ typedef enum GsrOutputFormat {
 
 typedef struct GsrSettings {
     uint32_t bounds;                   /* GsrTileBounds; reference default tight (cli.h) */
-    uint32_t tile_size;                /* 16 (INRIA tiles) */
+    uint32_t tile_size;                /* the binning and render tiles: 16 (INRIA's 16 x 16, the
+                                          reference's default), 8 (8 x 8) or 32 (32 x 8, as many
+                                          pixels as 16 x 16 in a wider, lower tile) */
     uint32_t budget_mb;                /* list memory incl. sort scratch; default 256 */
     uint32_t adaptive_list;            /* 1: capacity follows the measured entry count */
     uint32_t adaptive_initial_entries; /* 0: max(4 N, 1 M) */
@@ -420,7 +422,7 @@ typedef struct GsrTuneCandidate {
     uint32_t raster_schedule;  /* GSR_RASTER_PER_TILE or GSR_RASTER_PERSISTENT */
     float views_per_s;         /* device time over whole frames of consecutive cameras */
     float ms_per_frame;
-    uint32_t tile_size;        /* binning / render tile edge in pixels */
+    uint32_t tile_size;        /* binning / render tiles: 16, 8 or 32 (32 x 8) */
     uint32_t sort_digit_bits;  /* digit width of the list's radix sort */
 } GsrTuneCandidate;
 typedef struct GsrTuneResult {

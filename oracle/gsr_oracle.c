@@ -368,8 +368,18 @@ static Ellipse makeEllipse(const float c[2], const float conic[3], float opacity
 /* floorDivClamped (tile_coverage.cpp:54). */
 static int floorDivClamped(float v, int S) { return ftoi(floorf(sclamp(v, -65536.0f, 1048576.0f) / (float)S)); }
 
+/* The bins of the binning grid: sx x sy pixels. The reference's bins are square, S x S with
+ * S = 16 or 8 (tile_coverage.cpp); S = 32 here names 32 x 8 bins (wide bins of 256 pixels, as
+ * many as a 16 x 16 tile), for which every S below is the bin's width along x and its height
+ * along y. With sx = sy = S every expression is the reference's. */
+typedef struct { int sx, sy; } BinShape;
+static BinShape binShape(int S) {
+    BinShape b = {S, S == 32 ? 8 : S};
+    return b;
+}
+
 /* ellipseRows (tile_coverage.cpp:56-63). */
-static void ellipseRows(const Ellipse* e, int S, const BinRect* b, int* lo, int* hi) {
+static void ellipseRows(const Ellipse* e, BinShape bs, const BinRect* b, int* lo, int* hi) {
     if (e->t < 0.0f) {
         *lo = 0;
         *hi = 0;
@@ -377,16 +387,16 @@ static void ellipseRows(const Ellipse* e, int S, const BinRect* b, int* lo, int*
     }
     const float y0 = ceilf(e->cy - e->eyPad);
     const float y1 = floorf(e->cy + e->eyPad);
-    const int l = imax(b->y0, floorDivClamped(y0, S));
-    const int h = imin(b->y1, floorDivClamped(y1, S) + 1);
+    const int l = imax(b->y0, floorDivClamped(y0, bs.sy));
+    const int h = imin(b->y1, floorDivClamped(y1, bs.sy) + 1);
     *lo = l;
     *hi = imax(l, h);
 }
 
 /* ellipseRowBounds (tile_coverage.cpp:70-88). Returns 0 if the strip is empty. */
-static int rowBounds(const Ellipse* e, int row, int S, float* x0, float* x1) {
-    const float ey0 = (float)(row * S) - e->cy;
-    const float ey1 = (float)(row * S + S - 1) - e->cy;
+static int rowBounds(const Ellipse* e, int row, BinShape bs, float* x0, float* x1) {
+    const float ey0 = (float)(row * bs.sy) - e->cy;
+    const float ey1 = (float)(row * bs.sy + bs.sy - 1) - e->cy;
     const float lo = smax(ey0, -e->eyPad);
     const float hi = smin(ey1, e->eyPad);
     if (!(lo <= hi)) return 0;
@@ -403,28 +413,29 @@ static int rowBounds(const Ellipse* e, int row, int S, float* x0, float* x1) {
 }
 
 /* ellipseRowSpan (tile_coverage.cpp:90-96). */
-static void ellipseRowSpan(const Ellipse* e, int row, int S, const BinRect* b, int* x0, int* x1) {
+static void ellipseRowSpan(const Ellipse* e, int row, BinShape bs, const BinRect* b, int* x0, int* x1) {
     float fx0, fx1;
-    if (!rowBounds(e, row, S, &fx0, &fx1)) {
+    if (!rowBounds(e, row, bs, &fx0, &fx1)) {
         *x0 = b->x0;
         *x1 = b->x0;
         return;
     }
-    const int a = imax(b->x0, floorDivClamped(ceilf(fx0), S));
-    const int c = imin(b->x1, floorDivClamped(floorf(fx1), S) + 1);
+    const int a = imax(b->x0, floorDivClamped(ceilf(fx0), bs.sx));
+    const int c = imin(b->x1, floorDivClamped(floorf(fx1), bs.sx) + 1);
     *x0 = a;
     *x1 = imax(a, c);
 }
 
-/* rectToBins (tile_coverage.cpp:102-105). */
-static BinRect rectToBins(TileRect r, int S, int gx, int gy) {
-    const int f = 16 / S;
-    BinRect b = {r.minX * f, r.minY * f, imin(r.maxX * f, gx), imin(r.maxY * f, gy)};
+/* rectToBins (tile_coverage.cpp:102-105): the bins holding the 16-px rectangle's pixels (its
+ * first bin rounds down, its end up; for bins that divide 16 this is the reference's r * 16 / S). */
+static BinRect rectToBins(TileRect r, BinShape bs, int gx, int gy) {
+    BinRect b = {r.minX * 16 / bs.sx, r.minY * 16 / bs.sy, imin((r.maxX * 16 + bs.sx - 1) / bs.sx, gx),
+                 imin((r.maxY * 16 + bs.sy - 1) / bs.sy, gy)};
     return b;
 }
 
 /* makeCoverage (tile_coverage.cpp:107-117). */
-static Coverage makeCoverage(uint32_t mode, TileRect rect16, int S, int gx, int gy, const float center[2],
+static Coverage makeCoverage(uint32_t mode, TileRect rect16, BinShape bs, int gx, int gy, const float center[2],
                              const float conic[3], float opacity) {
     Coverage cv;
     memset(&cv, 0, sizeof(cv));
@@ -432,54 +443,54 @@ static Coverage makeCoverage(uint32_t mode, TileRect rect16, int S, int gx, int 
         BinRect all = {0, 0, gx, gy};
         cv.bins = all;
     } else {
-        cv.bins = rectToBins(rect16, S, gx, gy);
+        cv.bins = rectToBins(rect16, bs, gx, gy);
     }
     cv.e.t = -1.0f;
     if (mode != GSR_ORACLE_BOUNDS_RECT) {
         cv.e = makeEllipse(center, conic, opacity);
         cv.useEllipse = cv.e.valid;
-        if (!cv.e.valid && mode == GSR_ORACLE_BOUNDS_CUTOFF) cv.bins = rectToBins(rect16, S, gx, gy);
+        if (!cv.e.valid && mode == GSR_ORACLE_BOUNDS_CUTOFF) cv.bins = rectToBins(rect16, bs, gx, gy);
     }
     return cv;
 }
 
 /* coverageRows / coverageRowSpan (tile_coverage.cpp:119-127). */
-static void coverageRows(const Coverage* cv, int S, int* r0, int* r1) {
+static void coverageRows(const Coverage* cv, BinShape bs, int* r0, int* r1) {
     if (!cv->useEllipse) {
         *r0 = cv->bins.y0;
         *r1 = imax(cv->bins.y0, cv->bins.y1);
         return;
     }
-    ellipseRows(&cv->e, S, &cv->bins, r0, r1);
+    ellipseRows(&cv->e, bs, &cv->bins, r0, r1);
 }
-static void coverageRowSpan(const Coverage* cv, int row, int S, int* x0, int* x1) {
+static void coverageRowSpan(const Coverage* cv, int row, BinShape bs, int* x0, int* x1) {
     if (!cv->useEllipse) {
         *x0 = cv->bins.x0;
         *x1 = imax(cv->bins.x0, cv->bins.x1);
         return;
     }
-    ellipseRowSpan(&cv->e, row, S, &cv->bins, x0, x1);
+    ellipseRowSpan(&cv->e, row, bs, &cv->bins, x0, x1);
 }
 
 /* coverageCount (tile_coverage.cpp:129-138). */
-static uint32_t coverageCount(const Coverage* cv, int S) {
+static uint32_t coverageCount(const Coverage* cv, BinShape bs) {
     int r0, r1;
-    coverageRows(cv, S, &r0, &r1);
+    coverageRows(cv, bs, &r0, &r1);
     if (!cv->useEllipse) return (uint32_t)(imax(0, cv->bins.x1 - cv->bins.x0) * (r1 - r0));
     uint32_t n = 0;
     for (int r = r0; r < r1; ++r) {
         int x0, x1;
-        ellipseRowSpan(&cv->e, r, S, &cv->bins, &x0, &x1);
+        ellipseRowSpan(&cv->e, r, bs, &cv->bins, &x0, &x1);
         n += (uint32_t)(x1 - x0);
     }
     return n;
 }
 
 /* splatCoverage (tile_coverage.cpp:140-144). */
-static Coverage splatCoverage(uint32_t mode, const GsrOracleSplat* s, const GsrOracleCamera* cam, int S) {
-    const int gx = (int)((cam->width + S - 1) / S), gy = (int)((cam->height + S - 1) / S);
+static Coverage splatCoverage(uint32_t mode, const GsrOracleSplat* s, const GsrOracleCamera* cam, BinShape bs) {
+    const int gx = (int)((cam->width + bs.sx - 1) / bs.sx), gy = (int)((cam->height + bs.sy - 1) / bs.sy);
     const TileRect rect = tileRect(s->center, s->radius, cam->tilesX, cam->tilesY);
-    return makeCoverage(mode, rect, S, gx, gy, s->center, s->conicOpacity, s->conicOpacity[3]);
+    return makeCoverage(mode, rect, bs, gx, gy, s->center, s->conicOpacity, s->conicOpacity[3]);
 }
 
 void gsr_oracle_coverage_counts(uint32_t n, const GsrOracleSplat* splats, const GsrOracleCamera* cam, uint32_t bounds,
@@ -489,21 +500,22 @@ void gsr_oracle_coverage_counts(uint32_t n, const GsrOracleSplat* splats, const 
             counts[i] = 0;
             continue;
         }
-        const Coverage cv = splatCoverage(bounds, &splats[i], cam, S);
-        counts[i] = coverageCount(&cv, S);
+        const Coverage cv = splatCoverage(bounds, &splats[i], cam, binShape(S));
+        counts[i] = coverageCount(&cv, binShape(S));
     }
 }
 
 uint32_t gsr_oracle_coverage_tiles(const GsrOracleSplat* s, const GsrOracleCamera* cam, uint32_t bounds, int S,
                                    uint32_t* tiles, uint32_t cap) {
-    const int gx = (int)((cam->width + S - 1) / S);
-    const Coverage cv = splatCoverage(bounds, s, cam, S);
+    const BinShape bs = binShape(S);
+    const int gx = (int)((cam->width + bs.sx - 1) / bs.sx);
+    const Coverage cv = splatCoverage(bounds, s, cam, bs);
     int r0, r1;
-    coverageRows(&cv, S, &r0, &r1);
+    coverageRows(&cv, bs, &r0, &r1);
     uint32_t k = 0;
     for (int r = r0; r < r1; ++r) {
         int x0, x1;
-        coverageRowSpan(&cv, r, S, &x0, &x1);
+        coverageRowSpan(&cv, r, bs, &x0, &x1);
         for (int x = x0; x < x1; ++x) {
             if (k < cap) tiles[k] = (uint32_t)(r * gx + x);
             ++k;
@@ -517,19 +529,20 @@ static int nearInteger(float v, float eps) { return fabsf(v - roundf(v)) < eps; 
 /* coverageIsBorderline (tile_coverage.cpp:146-164). */
 int gsr_oracle_coverage_borderline(const GsrOracleSplat* s, const GsrOracleCamera* cam, uint32_t bounds, int S,
                                    float eps) {
-    const Coverage cv = splatCoverage(bounds, s, cam, S);
+    const BinShape bs = binShape(S);
+    const Coverage cv = splatCoverage(bounds, s, cam, bs);
     if (!cv.useEllipse || cv.e.t < 0.0f) return 0;
     const float rho = fabsf(cv.e.B) / sqrtf(cv.e.A * cv.e.C);
     const float K = 2.0f / smax(1.0f - rho, 1e-30f);
     eps += (1e-7f * K + 1e-12f * K * K) * (cv.e.exPad + cv.e.eyPad);
     if (nearInteger(cv.e.cy - cv.e.eyPad, eps) || nearInteger(cv.e.cy + cv.e.eyPad, eps)) return 1;
     int r0, r1;
-    coverageRows(&cv, S, &r0, &r1);
+    coverageRows(&cv, bs, &r0, &r1);
     for (int r = r0; r < r1; ++r) {
         float x0, x1;
-        if (!rowBounds(&cv.e, r, S, &x0, &x1)) continue;
+        if (!rowBounds(&cv.e, r, bs, &x0, &x1)) continue;
         if (nearInteger(x0, eps) || nearInteger(x1, eps)) return 1;
-        const float ey0 = (float)(r * S) - cv.e.cy, ey1 = (float)(r * S + S - 1) - cv.e.cy;
+        const float ey0 = (float)(r * bs.sy) - cv.e.cy, ey1 = (float)(r * bs.sy + bs.sy - 1) - cv.e.cy;
         if (fabsf(ey1 + cv.e.eyPad) < eps || fabsf(ey0 - cv.e.eyPad) < eps) return 1;
     }
     return 0;
@@ -563,7 +576,8 @@ uint64_t gsr_oracle_tile_list(uint32_t n, const GsrOracleSplat* splats, const ui
         }
         const uint32_t m = gsr_oracle_coverage_tiles(&splats[i], cam, bounds, S, tiles, tilesCap);
         for (uint32_t j = 0; j < counts[i] && k < kept; ++j, ++k) {
-            e[k].tile = j < m ? tiles[j] : ((cam->width + S - 1) / S) * ((cam->height + S - 1) / S);
+            e[k].tile = j < m ? tiles[j] : ((cam->width + binShape(S).sx - 1) / binShape(S).sx) *
+                                               ((cam->height + binShape(S).sy - 1) / binShape(S).sy);
             e[k].depth = fbits(splats[i].depth);
             e[k].value = i;
             e[k].pos = (uint32_t)k;
@@ -571,7 +585,7 @@ uint64_t gsr_oracle_tile_list(uint32_t n, const GsrOracleSplat* splats, const ui
     }
     free(tiles);
     qsort(e, (size_t)kept, sizeof(Entry), entryCmp);
-    const uint32_t T = ((cam->width + S - 1) / S) * ((cam->height + S - 1) / S);
+    const uint32_t T = ((cam->width + binShape(S).sx - 1) / binShape(S).sx) * ((cam->height + binShape(S).sy - 1) / binShape(S).sy);
     if (ranges) memset(ranges, 0, sizeof(uint32_t) * 2 * T);
     for (uint64_t j = 0; j < kept; ++j) {
         if (keysLo) keysLo[j] = e[j].depth;
@@ -895,8 +909,8 @@ int gsr_oracle_render(uint32_t n, int shDegree, const float* posAlpha, const flo
             const uint32_t idx = order[j];
             const GsrOracleSplat* s = &splats[idx];
             if (s->cullReason != GSR_ORACLE_CULL_VISIBLE) continue;
-            const Coverage cv = splatCoverage(bounds, s, cam, kTileSize);
-            const uint32_t cnt = coverageCount(&cv, kTileSize);
+            const Coverage cv = splatCoverage(bounds, s, cam, binShape(kTileSize));
+            const uint32_t cnt = coverageCount(&cv, binShape(kTileSize));
             if (cnt > tilesCap) {
                 tilesCap = cnt;
                 tiles = (uint32_t*)realloc(tiles, sizeof(uint32_t) * tilesCap);

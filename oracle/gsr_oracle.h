@@ -70,7 +70,8 @@ void gsr_oracle_preprocess_degrees(uint32_t n, const float* posAlpha, const floa
                                    const GsrOracleCamera* cam, int gpuRules, GsrOracleSplat* out);
 
 /* Tight coverage (tile_coverage.cpp): counts of visible splats (0 otherwise), and the tiles
- * of one splat in enumeration order (returns the count; writes at most cap). */
+ * of one splat in enumeration order (returns the count; writes at most cap). S names the bins:
+ * 16 or 8 (the reference's S x S bins) or 32 (32 x 8 bins). */
 void gsr_oracle_coverage_counts(uint32_t n, const GsrOracleSplat* splats, const GsrOracleCamera* cam, uint32_t bounds,
                                 int S, uint32_t* counts);
 uint32_t gsr_oracle_coverage_tiles(const GsrOracleSplat* splat, const GsrOracleCamera* cam, uint32_t bounds, int S,

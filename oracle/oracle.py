@@ -200,7 +200,8 @@ class Oracle:
         total = int(np.asarray(counts, np.uint64).sum())
         kept = min(total, capacity)
         lo, hi, val = (np.zeros(max(kept, 1), np.uint32) for _ in range(3))
-        tiles = ((cam.width + S - 1) // S) * ((cam.height + S - 1) // S)
+        sy = 8 if S == 32 else S  # S = 32 names 32 x 8 bins
+        tiles = ((cam.width + S - 1) // S) * ((cam.height + sy - 1) // sy)
         ranges = np.zeros(2 * tiles, np.uint32)
         c = np.ascontiguousarray(counts, np.uint32)
         self._tile_list.restype = C.c_uint64

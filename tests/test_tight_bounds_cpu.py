@@ -119,3 +119,23 @@ def test_tight_renders_identical_to_rect(port):
     assert a.tobytes() == b.tobytes()
     assert sa["blendedFragments"] == sb["blendedFragments"] and sa["terminatedPixels"] == sb["terminatedPixels"]
     assert sb["tileInstances"] < sa["tileInstances"]
+
+
+def test_32x8_bins_cover_what_the_8px_bins_cover(port):
+    """The 32 x 8 bins' rows are the 8-px bins' rows and the same cutoff ellipse decides each row's
+    x-extent, so the pixels of a splat's 32 x 8 bins contain the pixels of its 8 x 8 bins (and both
+    the pixels its alpha reaches)."""
+    from helpers import tile_raster_camera, tile_raster_scene
+
+    scene = tile_raster_scene(4000, seed=17, needles=True)
+    cam_v = tile_raster_camera(333, 190)
+    cam = port.camera_from_viewer(cam_v.view, cam_v.proj, cam_v.model, cam_v.width, cam_v.height)
+    sp = port.preprocess(scene, cam, 1, gpu_rules=True)
+    gx8, gx32 = (333 + 7) // 8, (333 + 31) // 32
+    for bounds in (0, 1, 2):
+        for i in np.flatnonzero(sp["cullReason"] == 0)[:1500]:
+            t8 = port.coverage_tiles(sp[i], cam, bounds, 8)
+            t32 = set(int(t) for t in port.coverage_tiles(sp[i], cam, bounds, 32))
+            for t in t8:
+                row, col = divmod(int(t), gx8)
+                assert row * gx32 + col // 4 in t32, (bounds, i, t)
