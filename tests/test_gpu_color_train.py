@@ -42,8 +42,9 @@ def init_params(seed):
     """The initial weights (uniform, He/Glorot bounds) from the library's 64-bit LCG; biases zero."""
     st = (0x9E3779B97F4A7C15 ^ ((seed * 0xD1B54A32D192ED03) & (2**64 - 1))) & (2**64 - 1)
     p = np.zeros(5195, np.float32)
-    layers = [(0, 48, 64, True), (48 * 64 + 64, 64, 8, False), (3648, 11, 32, True), (4032, 32, 32, True),
-              (5088, 32, 3, False)]
+    # encoder W1 [48][64] + b1 [64], W2 [64][8] + b2 [8]; decoder W1 [11][32] + b1, W2 [32][32] + b2, W3 [32][3]
+    layers = [(0, 48, 64, True), (3136, 64, 8, False), (3656, 11, 32, True), (4040, 32, 32, True),
+              (5096, 32, 3, False)]
     for off, n_in, n_out, relu in layers:
         b = np.float32(np.sqrt(np.float32(6.0 if relu else 3.0) / np.float32(n_in)))
         for e in range(n_in * n_out):
