@@ -35,7 +35,9 @@ parity       per workload (the CPU leg, rank 0), one view (or one per resolution
              reference's own renderReference; forms that must equal another form say so.
 roofline     preprocess + sort (preprocess, depth sort, scan + emission, tile sort, ranges)
              against the measured HBM copy bandwidth: algorithmic bytes per frame over the
-             summed CUDA-event pass times; each kernel's fraction in `kernels`.
+             summed CUDA-event pass times; each kernel's fraction in `kernels`. Measured on the
+             headline's own frame (the batched form, its views per frame); `plain_view` holds
+             the same for a one-view frame.
 multi-GPU    one process per GPU. The orbit workloads run as replicas (each rank renders the
              whole orbit: weak scaling); batched_64 and scale_4k split their views across the
              ranks, balanced by pixel count, and gather per-view checksums on rank 0.
@@ -279,7 +281,7 @@ def depth_sort_passes(ctl, bits: int = 8) -> int:
     return (w + 1 + bits - 1) // bits
 
 
-def pass_bytes(scene_format: str, ctl, n: int, tiles: int, bits: int = 8) -> dict:
+def pass_bytes(scene_format: str, ctl, n: int, tiles: int, bits: int = 8, views: int = 1) -> dict:
     """Bytes each pass must move for one frame, from the frame's counts.
     preprocess: posAlpha of every gaussian, scale + rotation of those past the near/opacity
       culls, SH of the visible ones (fp32 soa 16 + 32 + 192 B; fp16 split 16 + 16 + 96 B); writes
@@ -289,14 +291,18 @@ def pass_bytes(scene_format: str, ctl, n: int, tiles: int, bits: int = 8) -> dic
     scan + emission: the sorted words, counts and offsets (scan); the sorted words, counts,
       offsets and span hints again and 8 bytes per list entry (emission).
     tile sort: histogram read + a read and a write of every entry per active pass.
-    ranges: every entry read, 8 bytes per tile written."""
+    ranges: every entry read, 8 bytes per tile written.
+    A frame of several views (n = views x the scene's gaussians records) reads the scene once:
+    every gaussian's position, shape and SH (the union of the views' reads), then the writes of
+    every record."""
     past_cull = n - ctl.cull_counts[1] - ctl.cull_counts[4]
     vis = ctl.cull_counts[0]
     m = ctl.entries
-    if scene_format == "f32":
-        pre = 16 * n + 32 * past_cull + 192 * vis
+    per_g = (16, 32, 192) if scene_format == "f32" else (16, 16, 96)
+    if views == 1:
+        pre = per_g[0] * n + per_g[1] * past_cull + per_g[2] * vis
     else:
-        pre = 16 * n + 16 * past_cull + 96 * vis
+        pre = sum(per_g) * (n // views)
     pre += 4 * n + 8 * n + 64 * vis
     per_entry = 16 if ctl.packed_entries else 24
     return {
@@ -315,6 +321,10 @@ PASS_NAMES = {"preprocess": "reset + preprocess (depth keys)", "depth sort": "de
 # DRAM bytes of the same passes for one frame of plain_1080p, from one ncu capture of this
 # build (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot read the counters itself
 TRAFFIC_PLAIN_1080P_CAPTURE = (314.4 + 70.7 + 10.0 + 39.6 + 14.9 + 47.9 + 2.9) * 1e6
+# the same for one batched frame of 8 views (preprocess, depth sort, scan, emission, tile sort,
+# ranges; the second tile-sort pass taken equal to the first, which the capture did not reach)
+TRAFFIC_BATCHED_1080P_CAPTURE: dict = {8: (469.7 + 747.5 + 79.6 + 4 * 79.4 + 121.7 + 135.4 + 675.5 + 332.2 +
+                                           2 * (332.3 + 290.6) + 335.9) * 1e6}
 
 
 # ---- the CPU leg: the reference's renderer as the baseline and as the checker of the GPU's views
@@ -552,8 +562,9 @@ def pass_profile(r, frames: Frames, stream_obj, n: int = 20) -> tuple[dict, obje
     return {k: round(v, 4) for k, v in passes.items()}, r.read_control()
 
 
-def roofline(passes: dict, ctl, fmt: str, n: int, tiles: int, peak: float, peak_kind: str, bits: int = 8) -> dict:
-    b = pass_bytes(fmt, ctl, n, tiles, bits)
+def roofline(passes: dict, ctl, fmt: str, n: int, tiles: int, peak: float, peak_kind: str, bits: int = 8,
+             form: str = "plain form, one 1080p frame", views: int = 1) -> dict:
+    b = pass_bytes(fmt, ctl, n, tiles, bits, views)
     kernels, tot_b, tot_ms = {}, 0.0, 0.0
     for k, nb in b.items():
         ms = passes.get(PASS_NAMES[k])
@@ -565,7 +576,7 @@ def roofline(passes: dict, ctl, fmt: str, n: int, tiles: int, peak: float, peak_
         tot_ms += ms
     achieved = tot_b / (tot_ms * 1e-3) / 1e9 if tot_ms else 0.0
     return {"bound": "hbm", "kernel": "preprocess + sort (preprocess, depth sort, scan + emission, tile sort, "
-                                      "ranges), plain form, one 1080p frame",
+                                      "ranges), " + form,
             "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
             "peak_kind": peak_kind, "algorithmic_bytes": int(tot_b), "ms": round(tot_ms, 4), "kernels": kernels}
 
@@ -625,12 +636,12 @@ def settle_and_tune(G, gs, cams, args, model=None, depths=(1, 2, 4, 8, 16), tile
                       sort_digit_bits=(8, 9))
 
 
-def renderer_for(G, gs, args, tuned=None, model=None, gather=None):
+def renderer_for(G, gs, args, tuned=None, model=None, gather=None, decode="default"):
     t = tuned or {}
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.budget_mb,
                                   raster_schedule=t.get("raster_schedule", "auto"), tile_size=t.get("tile_size", 16),
                                   use_graph=True, raster_gather=gather or args.gather,
-                                  sort_digit_bits=t.get("sort_digit_bits", args.digit_bits)))
+                                  sort_digit_bits=t.get("sort_digit_bits", args.digit_bits), color_decode=decode))
     if model is not None:
         r.set_color_model(model)
     return r
@@ -684,6 +695,17 @@ def run_1080p(G, args, dist, sampler, stream_obj, peak):
     bframes = Frames(G, cams, tuned["views_per_frame"], order)
     rb = renderer_for(G, gs, args, tuned)
     batched = time_form(rb, bframes, args, dist, sampler, stream_obj)
+    # the same byte model over the batched frame: d views of the scene's gaussians and tiles
+    bpasses, bctl = pass_profile(rb, bframes, stream_obj)
+    d = bframes.d
+    broof = roofline(bpasses, bctl, fmt, scene.count * d, tiles * d, peak[0], peak[1],
+                     tuned.get("sort_digit_bits") or args.digit_bits or 8,
+                     form=f"batched form, one frame of {d} 1080p views", views=d)
+    broof["traffic"] = int(TRAFFIC_BATCHED_1080P_CAPTURE.get(d, 0)) or None
+    broof["traffic_kind"] = "from_capture" if broof["traffic"] else "not captured at this views-per-frame"
+    batched["passes_ms"] = bpasses
+    batched["frame"] = {"visible": bctl.visible, "entries": bctl.entries, "sort_passes": bctl.sort_passes,
+                        "key_bits": bctl.key_bits}
     bimgs = frame_images(rb, bframes, stream_obj)
     rp = renderer_for(G, gs, args)
     pimgs = [frame_images(rp, Frames(G, cams, 1, [order[j]]), stream_obj)[0] for j in range(bframes.d)]
@@ -712,6 +734,19 @@ def run_1080p(G, args, dist, sampler, stream_obj, peak):
         lp, _ = pass_profile(r1, plain_frames, stream_obj)
         r1.close()
         form["passes_ms_one_view"] = lp
+        if label == "forced":
+            # the same decode as a tcgen05 pre-pass (tensor memory accumulators) against the fused
+            # mma.sync decode inside the preprocess
+            rt = renderer_for(G, gs, args, tuned, model, decode="tcgen05")
+            tform = time_form(rt, bframes, args, dist, sampler, stream_obj)
+            timgs = frame_images(rt, bframes, stream_obj)
+            rt.close()
+            r1 = renderer_for(G, gs, args, None, model, decode="tcgen05")
+            tp, _ = pass_profile(r1, plain_frames, stream_obj)
+            r1.close()
+            form["tcgen05_decode"] = {"views_per_s": tform["views_per_s"], "e2e_views_per_s": tform["e2e_views_per_s"],
+                                      "passes_ms_one_view": tp, "psnr_vs_fused_db": min_psnr8(timgs, limgs),
+                                      "gpu_launches": tform["gpu_launches"], "clocks": tform["clocks"]}
         form["gate"] = "2/255" if label == "gated" else "off (decode forced for every gaussian)"
         form["color_model"] = {k: (round(v, 6) if isinstance(v, float) else v) for k, v in stats.items()}
         form["fallback_share"] = round(stats["fallback"] / max(stats["gaussians"], 1), 4)
@@ -720,7 +755,10 @@ def run_1080p(G, args, dist, sampler, stream_obj, peak):
         learned[label] = form
     out["learned_1080p"] = learned
     gs.close()
-    return out, scene, cams, order, roof
+    # the headline's roofline is its own frame's (the batched form; the learned form's frames are
+    # the same kernels when the gate keeps no gaussian), the plain view's beside it
+    broof["plain_view"] = roof
+    return out, scene, cams, order, broof
 
 
 def run_1080p_f16(G, args, dist, sampler, stream_obj, tuned_depth: int, raster: str, bits: int = 0):
@@ -808,6 +846,10 @@ def run_batched_64(G, args, dist, sampler, stream_obj):
     rb = renderer_for(G, gs, args, tuned)
     bframes = Frames(G, cams, d, mine)
     batched = time_form(rb, bframes, args, dist, sampler, stream_obj)
+    bpasses, bctl = pass_profile(rb, bframes, stream_obj)
+    batched["passes_ms"] = bpasses
+    batched["frame"] = {"visible": bctl.visible, "entries": bctl.entries, "sort_passes": bctl.sort_passes,
+                        "key_bits": bctl.key_bits}
     bimgs = frame_images(rb, bframes, stream_obj)
     same = all(np.array_equal(bimgs[j], plain_imgs[v]) for j, v in enumerate(mine))
     sums = dist.gather_view_results(mine, view_checksums(rb, bframes, stream_obj), len(cams))
@@ -923,15 +965,16 @@ def run_plain_only(G, args, dist, sampler, stream_obj):
     name = args.config if args.config in ("plain_1080p", "plain_1080p_f16", "plain_720p") else "plain_1080p"
     scene, cams, fmt, layout, thr = workload(name)
     gs = G.GpuScene(scene, fmt, layout, 3, thr)
-    r = renderer_for(G, gs, args)
-    frames = Frames(G, cams, 1)
+    d = max(args.batch, 1)
+    r = renderer_for(G, gs, args, {"views_per_frame": d, "raster_schedule": "per-tile"} if d > 1 else None)
+    frames = Frames(G, cams, d)
     form = time_form(r, frames, args, dist, sampler, stream_obj)
     form["passes_ms"], _ = pass_profile(r, frames, stream_obj)
     r.close()
     gs.close()
+    label = f"{name} plain only (profiling)" if d == 1 else f"{name} batched, {d} views per frame (profiling)"
     if dist.rank == 0:
-        print(json.dumps({"metric": METRIC, "form": f"{name} plain only (profiling)", "gather": args.gather, **form}),
-              flush=True)
+        print(json.dumps({"metric": METRIC, "form": label, "gather": args.gather, **form}), flush=True)
 
 
 # ---- the reference arm ------------------------------------------------------------------------

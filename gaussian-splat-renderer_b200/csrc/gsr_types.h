@@ -16,7 +16,14 @@ constexpr uint32_t kBoundsRect = 0, kBoundsTight = 1, kBoundsCutoff = 2;
 // Iteration limit of every device-side wait; on expiry the kernel records
 // GSR_CONTROL_TIMEOUT + where, stops waiting and finishes (the frame is then invalid).
 constexpr uint32_t kSpinLimit = 1u << 22;
-enum WaitSite : uint32_t { kWaitScan = 1, kWaitSort = 2, kWaitStandaloneScan = 3, kWaitShStage = 4, kWaitGather = 5 };
+enum WaitSite : uint32_t {
+    kWaitScan = 1,
+    kWaitSort = 2,
+    kWaitStandaloneScan = 3,
+    kWaitShStage = 4,
+    kWaitGather = 5,
+    kWaitDecode = 6,  // the tensor-core colour decode's MMA completions
+};
 
 constexpr int kControlTickets = 32;
 constexpr uint32_t kListSortTickets = 1, kDepthSortTickets = 16;

@@ -15,6 +15,7 @@
 #include "kernels.cuh"
 #include "mlp.cuh"
 #include "splat_math.cuh"
+#include "tcgen05.cuh"
 
 namespace gsr {
 
@@ -173,6 +174,16 @@ __device__ __forceinline__ uint32_t gaussianDegree(const SceneArgs& s, uint32_t 
     return s.variableSh == GSR_VARIABLE_SH_OFF ? 3u : (meta >> 30);
 }
 
+// normalize(mean - camera position), glm::normalize's order (the SH colour's direction and the
+// learned colour's direction input).
+__device__ __forceinline__ void viewDirection(const float4& pa, const float (&camPos)[3], float (&dir)[3]) {
+    const float d0 = pa.x - camPos[0], d1 = pa.y - camPos[1], d2 = pa.z - camPos[2];
+    const float inv = 1.0f / sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+    dir[0] = d0 * inv;
+    dir[1] = d1 * inv;
+    dir[2] = d2 * inv;
+}
+
 // What the colour of a visible gaussian needs once its geometry is done.
 struct ColourJob {
     uint32_t meta, degree;
@@ -272,11 +283,7 @@ __device__ __forceinline__ uint32_t preprocessOne(const FrontArgs& a, const DevC
     const uint32_t gdeg = gaussianDegree(a.scene, meta);
     job.meta = meta;
     job.degree = uint32_t(a.evalDegree) < gdeg ? uint32_t(a.evalDegree) : gdeg;
-    const float d0 = pa.x - cam.pos[0], d1 = pa.y - cam.pos[1], d2 = pa.z - cam.pos[2];
-    const float inv = 1.0f / sqrtf(d0 * d0 + d1 * d1 + d2 * d2);  // glm::normalize
-    job.dir[0] = d0 * inv;
-    job.dir[1] = d1 * inv;
-    job.dir[2] = d2 * inv;
+    viewDirection(pa, cam.pos, job.dir);
     if (!LEARNED) shColour<COLOR>(a, i, job, s);
     s.conicA = conic[0];
     s.conicB = conic[1];
@@ -301,8 +308,21 @@ struct LearnedShared {
     float out4[kFrontThreads / 32][32][4];
 };
 template <int COLOR>
-__device__ __forceinline__ void learnedColour(const FrontArgs& a, LearnedShared& sl, uint32_t i, bool visible,
-                                              const ColourJob& job, DevSplat& s) {
+__device__ __forceinline__ void learnedColour(const FrontArgs& a, LearnedShared& sl, uint32_t i, size_t rec,
+                                              bool visible, const ColourJob& job, DevSplat& s) {
+    if (a.decoded) {  // decoded by the tensor-core pre-pass
+        if (visible) {
+            if (!latentIsFallback(__ldg(&a.latents[i]))) {
+                const float4 c = __ldg(&a.decoded[rec]);
+                s.r = c.x;
+                s.g = c.y;
+                s.b = c.z;
+            } else {
+                shColour<COLOR>(a, i, job, s);
+            }
+        }
+        return;
+    }
     bool mlp = false;
     float feat[kMlpIn];
 #pragma unroll
@@ -383,7 +403,9 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
     __shared__ uint32_t sCull[kCullReasonCount];
     __shared__ uint32_t sDepthMin, sDepthMax;
     const uint32_t tid = threadIdx.x, lane = tid & 31;
-    const uint32_t view = blockIdx.y;
+    // the views vary fastest along the grid: the blocks of one gaussian range for every view run
+    // side by side, so one of them reads the range's scene data from DRAM and the others from L2
+    const uint32_t view = blockIdx.x % a.viewCount, i0 = blockIdx.x / a.viewCount * kFrontThreads;
     if (tid < kCullReasonCount) sCull[tid] = 0;
     if (tid == 0) {
         sDepthMin = 0xFFFFFFFFu;
@@ -397,19 +419,19 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smemAddr(&gShBarrier)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const uint32_t i0 = blockIdx.x * kFrontThreads;
         issueShStage(a.scene, i0, a.count - i0 < kFrontThreads ? a.count - i0 : kFrontThreads);
     }
     LearnedShared* sl = nullptr;
     if constexpr (LEARNED) {
         __shared__ LearnedShared sLearned;
         static_assert(sizeof(DecoderWeights) % 4 == 0, "decoder layout");
-        for (uint32_t e = tid; e < sizeof(DecoderWeights) / 4; e += kFrontThreads)
-            reinterpret_cast<uint32_t*>(&sLearned.w)[e] = reinterpret_cast<const uint32_t*>(a.decoder)[e];
+        if (!a.decoded)
+            for (uint32_t e = tid; e < sizeof(DecoderWeights) / 4; e += kFrontThreads)
+                reinterpret_cast<uint32_t*>(&sLearned.w)[e] = reinterpret_cast<const uint32_t*>(a.decoder)[e];
         sl = &sLearned;
     }
     __syncthreads();
-    const uint32_t i = blockIdx.x * kFrontThreads + tid;
+    const uint32_t i = i0 + tid;
     const size_t rec = size_t(view) * a.count + i;
     // the binning grid: ceil(size / bin) bins (INRIA's rectangles stay on the 16-px tiles)
     const BinShape bs = binShapeOf(a.binSize);
@@ -422,7 +444,7 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
     if (i < a.count)
         reason = preprocessOne<GEOM, COLOR, LEARNED>(a, sCam, i, s, rect, job,
                                                      EXTRAS && a.rayDepth ? a.rayDepth + rec * 3 : nullptr);
-    if constexpr (LEARNED) learnedColour<COLOR>(a, *sl, i, reason == kCullVisible, job, s);  // warp-collective
+    if constexpr (LEARNED) learnedColour<COLOR>(a, *sl, i, rec, reason == kCullVisible, job, s);  // warp-collective
     if (i < a.count) {
         uint32_t count = 0;
         if (reason == kCullVisible) {
@@ -457,9 +479,13 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
         }
         a.tileCounts[rec] = count;
         // binning mode: the record's depth word, depth bits above the record index; records that
-        // emit no tile get all-ones depth bits and sort after every real depth (positive floats)
+        // emit no tile get all-ones depth bits and sort after every real depth (positive floats).
+        // Frames of several views put the view above the depth bits: the depth sort then orders
+        // by (view, depth, record), so the emission walks one view's records at a time (each
+        // tile's entries come from one view, so the list is the same)
         if (a.binning)
-            a.depthKeys[0][rec] = (uint64_t(count ? __float_as_uint(s.depth) : 0xFFFFFFFFu) << a.recordBits) | rec;
+            a.depthKeys[0][rec] = (a.depthViewShift ? uint64_t(view) << a.depthViewShift : 0ull) |
+                                  (uint64_t(count ? __float_as_uint(s.depth) : 0xFFFFFFFFu) << a.recordBits) | rec;
     }
 #pragma unroll
     for (uint32_t r = 0; r < kCullReasonCount; ++r) {
@@ -734,6 +760,186 @@ cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capaci
     return cudaGetLastError();
 }
 
+// ---- the learned colour's decode on the tcgen05 tensor cores (GSR_DECODE_TCGEN05) ----------------
+// A pre-pass before the preprocess. Persistent 128-thread blocks take 128-gaussian tiles of one
+// view at a time (the views of one gaussian range side by side, so the latents and positions are
+// read from DRAM once). Thread t builds row t of the decoder input (the fp16 latent and the view
+// direction as BF16, zero-padded to K = 16) in shared memory; one thread issues each layer as
+// tcgen05.mma products of M = 128 rows (the tile's gaussians) with FP32 accumulators in tensor
+// memory: 16 -> 32 (1 MMA), 32 -> 32 (2 MMAs of K = 16), 32 -> 16 (2 MMAs; 3 outputs used),
+// each completion signalled through tcgen05.commit on an mbarrier. After each layer every warp
+// reads its 32 rows back (tcgen05.ld, thread t = row t = TMEM lane t), adds the bias and applies
+// ReLU (sigmoid at the output), and writes the next layer's BF16 operand. The colours of the
+// kept gaussians go to decoded[view][g]. The rounding points are the in-preprocess decode's
+// (BF16 inputs, weights and hidden units, FP32 accumulation); the bias is added after the
+// products instead of seeding the accumulator, so colours can differ in the last bits of FP32.
+constexpr uint32_t kDecodeTcThreads = 128, kDecodeTcCols = 128;
+struct alignas(128) DecodeTcSmem {
+    alignas(128) unsigned char a1[128 * 16 * 2];  // layer inputs, M = 128 rows, K-major no swizzle
+    alignas(128) unsigned char a2[128 * 32 * 2];
+    alignas(128) unsigned char a3[128 * 32 * 2];
+    alignas(128) unsigned char b1[32 * 16 * 2];   // weights [n][k]: N = 32, 32, 16 (rows 3..15 zero)
+    alignas(128) unsigned char b2[32 * 32 * 2];
+    alignas(128) unsigned char b3[16 * 32 * 2];
+    float bias1[32], bias2[32], bias3[4];
+    uint64_t mbar;
+    uint32_t tmem;
+};
+// 56 KB a block: at most 4 blocks per SM, so the blocks' TMEM (128 columns each) always fits
+// the SM's 512 columns and no allocation waits.
+constexpr uint32_t kDecodeTcSmem = 56 * 1024;
+static_assert(sizeof(DecodeTcSmem) + 128 <= kDecodeTcSmem, "the decode's shared memory");
+
+// Eight floats as BF16 into one 16-byte row chunk of an operand.
+__device__ __forceinline__ void storeRowChunk(unsigned char* base, uint32_t off, const float* v) {
+    *reinterpret_cast<uint4*>(base + off) =
+        make_uint4(packBf16(v[0], v[1]), packBf16(v[2], v[3]), packBf16(v[4], v[5]), packBf16(v[6], v[7]));
+}
+
+template <int GEOM>
+__global__ void __launch_bounds__(kDecodeTcThreads) decodeColoursTcKernel(const __grid_constant__ FrontArgs a) {
+    extern __shared__ __align__(128) unsigned char decodeRaw[];
+    DecodeTcSmem& S = *reinterpret_cast<DecodeTcSmem*>(decodeRaw + ((128u - (tc::smem32(decodeRaw) & 127u)) & 127u));
+    const uint32_t tid = threadIdx.x, warp = tid >> 5;
+    const DecoderWeights& W = *a.decoder;
+    // the weights in the operand layout, the biases, the barrier and the tensor memory
+    if (tid < 64) {
+        const uint32_t n = tid >> 1, c = tid & 1;
+        *reinterpret_cast<uint4*>(S.b1 + tc::operandOffset(n, 8 * c, 16)) = *reinterpret_cast<const uint4*>(&W.w1[n][8 * c]);
+    }
+    {
+        const uint32_t n = tid >> 2, c = tid & 3;
+        *reinterpret_cast<uint4*>(S.b2 + tc::operandOffset(n, 8 * c, 32)) = *reinterpret_cast<const uint4*>(&W.w2[n][8 * c]);
+    }
+    if (tid < 64) {
+        const uint32_t n = tid >> 2, c = tid & 3;
+        *reinterpret_cast<uint4*>(S.b3 + tc::operandOffset(n, 8 * c, 32)) =
+            n < 8 ? *reinterpret_cast<const uint4*>(&W.w3[n][8 * c]) : make_uint4(0, 0, 0, 0);
+    }
+    if (tid < 32) {
+        S.bias1[tid] = W.b1[tid];
+        S.bias2[tid] = W.b2[tid];
+    }
+    if (tid < 4) S.bias3[tid] = W.b3[tid];
+    if (tid == 0) tc::mbarInit(&S.mbar, 1);
+    if (warp == 0) tc::tmemAlloc(&S.tmem, kDecodeTcCols);
+    tc::fenceProxyAsync();
+    tc::fenceBeforeSync();
+    __syncthreads();
+    tc::fenceAfterSync();
+    const uint32_t tmem = S.tmem, lane0 = (warp * 32u) << 16;
+    const uint32_t a1 = tc::smem32(S.a1), a2 = tc::smem32(S.a2), a3 = tc::smem32(S.a3);
+    const uint32_t b1 = tc::smem32(S.b1), b2 = tc::smem32(S.b2), b3 = tc::smem32(S.b3);
+    const uint32_t tiles = (a.count + 127u) / 128u * a.viewCount;
+    uint32_t phase = 0;
+    bool failed = false;
+    // every thread waits for the layer's commit; a wait that runs out stops the whole block
+    auto layerDone = [&]() -> bool {
+        const bool ok = tc::mbarWait(&S.mbar, phase, kSpinLimit);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            return false;
+        }
+        tc::fenceAfterSync();
+        return true;
+    };
+    for (uint32_t tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
+        const uint32_t view = tile % a.viewCount, g = tile / a.viewCount * 128u + tid;
+        float f[16];
+#pragma unroll
+        for (int k = 0; k < 16; ++k) f[k] = 0.0f;
+        bool kept = false;
+        if (g < a.count) {
+            const uint4 q = __ldg(&a.latents[g]);
+            kept = !latentIsFallback(q);
+            if (kept) {
+                const uint32_t qw[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int k = 0; k < kMlpLatent; ++k) f[k] = __half2float(__ushort_as_half(uint16_t(qw[k >> 1] >> (16 * (k & 1)))));
+                const float4 pa = loadPosAlpha<GEOM>(a.scene, g);
+                const float camPos[3] = {a.cam[view].pos[0], a.cam[view].pos[1], a.cam[view].pos[2]};
+                float dir[3];
+                viewDirection(pa, camPos, dir);
+                f[8] = dir[0];
+                f[9] = dir[1];
+                f[10] = dir[2];
+            }
+        }
+        storeRowChunk(S.a1, tc::operandOffset(tid, 0, 16), f);
+        storeRowChunk(S.a1, tc::operandOffset(tid, 8, 16), f + 8);
+        tc::fenceProxyAsync();
+        tc::fenceBeforeSync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fenceAfterSync();
+            tc::mma(tmem, tc::operandDescriptor(a1, 0, 16), tc::operandDescriptor(b1, 0, 16), tc::instrDescriptorBf16(128, 32),
+                    false);
+            tc::commit(&S.mbar);
+        }
+        if (!layerDone()) break;
+        uint32_t acc[32];
+        tc::ld32(tmem + lane0, acc);
+        tc::waitLd();
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float h[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) h[e] = fmaxf(__uint_as_float(acc[8 * c + e]) + S.bias1[8 * c + e], 0.0f);
+            storeRowChunk(S.a2, tc::operandOffset(tid, 8 * c, 32), h);
+        }
+        tc::fenceProxyAsync();
+        tc::fenceBeforeSync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fenceAfterSync();
+            for (uint32_t ks = 0; ks < 2; ++ks)
+                tc::mma(tmem + 32, tc::operandDescriptor(a2, ks, 32), tc::operandDescriptor(b2, ks, 32),
+                        tc::instrDescriptorBf16(128, 32), ks > 0);
+            tc::commit(&S.mbar);
+        }
+        if (!layerDone()) break;
+        tc::ld32(tmem + lane0 + 32, acc);
+        tc::waitLd();
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float h[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) h[e] = fmaxf(__uint_as_float(acc[8 * c + e]) + S.bias2[8 * c + e], 0.0f);
+            storeRowChunk(S.a3, tc::operandOffset(tid, 8 * c, 32), h);
+        }
+        tc::fenceProxyAsync();
+        tc::fenceBeforeSync();
+        __syncthreads();
+        if (tid == 0) {
+            tc::fenceAfterSync();
+            for (uint32_t ks = 0; ks < 2; ++ks)
+                tc::mma(tmem + 64, tc::operandDescriptor(a3, ks, 32), tc::operandDescriptor(b3, ks, 32),
+                        tc::instrDescriptorBf16(128, 16), ks > 0);
+            tc::commit(&S.mbar);
+        }
+        if (!layerDone()) break;
+        uint32_t out[16];
+        tc::ld16(tmem + lane0 + 64, out);
+        tc::waitLd();
+        if (kept)
+            a.decoded[size_t(view) * a.count + g] =
+                make_float4(sigmoidF(__uint_as_float(out[0]) + S.bias3[0]), sigmoidF(__uint_as_float(out[1]) + S.bias3[1]),
+                            sigmoidF(__uint_as_float(out[2]) + S.bias3[2]), 0.0f);
+        tc::fenceBeforeSync();  // this tile's TMEM reads before the next tile's products
+    }
+    if (failed && tid == 0) {
+        reportTimeout(a.ctl, kWaitDecode);
+        tc::mbarWait(&S.mbar, phase ^ 1u, kSpinLimit);  // the products in flight, once more (bounded)
+    }
+    tc::fenceBeforeSync();
+    __syncthreads();
+    if (warp == 0) {
+        tc::fenceAfterSync();
+        tc::tmemFree(tmem, kDecodeTcCols);
+    }
+}
+
 namespace {
 constexpr int kShStageBytes = kFrontThreads * 192;
 template <int GEOM, int COLOR, bool LEARNED, bool EXTRAS>
@@ -788,9 +994,13 @@ cudaError_t launchShDecode(const SceneArgs& scene, uint32_t geometry, uint32_t c
     return cudaGetLastError();
 }
 
+// The preprocess grid: one block per (gaussian block, view), the view fastest (records = count x
+// views fit 32 bits, so the block count stays below 2^24).
+static dim3 preprocessGrid(const FrontArgs& a) { return dim3((a.count + kFrontThreads - 1) / kFrontThreads * a.viewCount); }
+
 cudaError_t launchFrontBinningKeys(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s) {
-    const dim3 blocks((a.count + kFrontThreads - 1) / kFrontThreads, a.viewCount);
-    if (blocks.x == 0 || blocks.y == 0) return cudaSuccess;
+    const dim3 blocks = preprocessGrid(a);
+    if (blocks.x == 0) return cudaSuccess;
     if (geometry == GSR_GEOMETRY_SOA_F32 && color == GSR_COLOR_SOA_F32)
         launchPreprocess<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32>(a, blocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F32 && color == GSR_COLOR_RECORD_F32)
@@ -819,20 +1029,49 @@ cudaError_t launchFrontBinningEmit(const FrontArgs& a, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+namespace {
+template <int GEOM>
+cudaError_t launchDecodeTcT(const FrontArgs& a, cudaStream_t s) {
+    static std::atomic<int> grids[64] = {};
+    std::atomic<int>& grid = perDevice(grids);
+    if (!grid) {
+        cudaError_t e = cudaFuncSetAttribute(decodeColoursTcKernel<GEOM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(kDecodeTcSmem));
+        if (e != cudaSuccess) return e;
+        int dev = 0, sms = 148, perSm = 4;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, decodeColoursTcKernel<GEOM>, kDecodeTcThreads, kDecodeTcSmem);
+        grid = sms * (perSm > 0 ? (perSm < 4 ? perSm : 4) : 1);
+    }
+    const uint32_t tiles = (a.count + 127u) / 128u * a.viewCount;
+    const uint32_t blocks = tiles < uint32_t(grid) ? tiles : uint32_t(grid);
+    decodeColoursTcKernel<GEOM><<<blocks, kDecodeTcThreads, kDecodeTcSmem, s>>>(a);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launchDecodeColoursTc(const FrontArgs& a, uint32_t geometry, cudaStream_t s) {
+    if (a.count == 0 || a.viewCount == 0 || !a.latents || !a.decoder || !a.decoded) return cudaSuccess;
+    if (geometry == GSR_GEOMETRY_SOA_F32) return launchDecodeTcT<GSR_GEOMETRY_SOA_F32>(a, s);
+    if (geometry == GSR_GEOMETRY_RECORD_F32) return launchDecodeTcT<GSR_GEOMETRY_RECORD_F32>(a, s);
+    if (geometry == GSR_GEOMETRY_RECORD_F16) return launchDecodeTcT<GSR_GEOMETRY_RECORD_F16>(a, s);
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s) {
-    const dim3 blocks((a.count + kFrontThreads - 1) / kFrontThreads, a.viewCount);
+    const dim3 blocks((a.count + kFrontThreads - 1) / kFrontThreads, a.viewCount), pblocks = preprocessGrid(a);
     if (blocks.x == 0 || blocks.y == 0) return cudaSuccess;
-    // 1) preprocess + count, grid (gaussian blocks, views)
+    // 1) preprocess + count, one block per (gaussian block, view)
     if (geometry == GSR_GEOMETRY_SOA_F32 && color == GSR_COLOR_SOA_F32)
-        launchPreprocess<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32>(a, blocks, s);
+        launchPreprocess<GSR_GEOMETRY_SOA_F32, GSR_COLOR_SOA_F32>(a, pblocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F32 && color == GSR_COLOR_RECORD_F32)
-        launchPreprocess<GSR_GEOMETRY_RECORD_F32, GSR_COLOR_RECORD_F32>(a, blocks, s);
+        launchPreprocess<GSR_GEOMETRY_RECORD_F32, GSR_COLOR_RECORD_F32>(a, pblocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_RECORD_F16)
-        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16>(a, blocks, s);
+        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_RECORD_F16>(a, pblocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_Q8)
-        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8>(a, blocks, s);
+        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_Q8>(a, pblocks, s);
     else if (geometry == GSR_GEOMETRY_RECORD_F16 && color == GSR_COLOR_CODEBOOK)
-        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_CODEBOOK>(a, blocks, s);
+        launchPreprocess<GSR_GEOMETRY_RECORD_F16, GSR_COLOR_CODEBOOK>(a, pblocks, s);
     else
         return cudaErrorInvalidValue;
     cudaError_t e = cudaGetLastError();

@@ -105,6 +105,24 @@ __device__ __forceinline__ uint32_t stripMask(float cx, float cy, float A, float
     return mask;
 }
 
+// 32 x 8 tiles: the strips (bit g * 4 + c: columns 8c .. 8c + 7 of the tile, either row group)
+// inside the splat's 16-px tile rectangle along x, [16 minX, 16 maxX) with the preprocess's
+// tileRect arithmetic (its upper clamp to the grid only removes pixels past the image). The
+// rectangle's edges are multiples of 16 and the strips' multiples of 8, so a strip is wholly in
+// or out. (Along y the tile's 8 rows always lie inside or outside the rectangle's 16-px rows.)
+__device__ __forceinline__ uint32_t rectStrips32(float cx, float radius, uint32_t tileX) {
+    const float fr = float(ftoi(radius));
+    const int x0 = 16 * imax(0, ftoi((cx - fr) / float(kTileSize)));
+    const int x1 = 16 * imax(0, ftoi((cx + fr + float(kTileSize - 1)) / float(kTileSize)));
+    uint32_t m = 0;
+#pragma unroll
+    for (uint32_t c = 0; c < 4; ++c) {
+        const int s = int(tileX + 8 * c);
+        if (s >= x0 && s < x1) m |= 0x11u << c;
+    }
+    return m;
+}
+
 // How a batch's records reach shared memory.
 constexpr int kGatherCpAsync = 0;  // every thread copies its record with 16-byte cp.async
 constexpr int kGatherTma = 1;      // one warp gathers four records per cp.async.bulk.tensor tile::gather4
@@ -433,6 +451,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
             float2 r0;  // cx, cy
             float A, B, C, o;
             float4 r2;  // r, g, b, -
+            float radius = 0.0f;  // as the preprocess's 16-px rectangle read it (truncated)
             if constexpr (mode == kRenderSplatFull) {
                 float4 w0, w1;
                 if constexpr (GATHER == kGatherTma) {
@@ -450,6 +469,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
                 B = w1.y;
                 C = w1.z;
                 o = w1.w;
+                radius = r2.w;
             } else if constexpr (mode == kRenderSplatP32) {
                 const float4 w0 = sm.st.raw[buf][0][tid];  // cx, cy, A, B
                 const float4 w1 = sm.st.raw[buf][1][tid];  // C, opacity, h(r, g), h(b) | radius
@@ -460,26 +480,34 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
                 o = w1.y;
                 const uint32_t rg = __float_as_uint(w1.z), bw = __float_as_uint(w1.w);
                 r2 = make_float4(halfLoF(rg), halfHiF(rg), halfLoF(bw), 0.0f);
+                radius = float(bw >> 16);
             } else {
                 const uint2* w = reinterpret_cast<const uint2*>(&sm.st.raw[buf][0][0]);
                 const uint2 w0 = w[tid], w1 = w[kThreads + tid], w2 = w[2 * kThreads + tid];
                 r0 = make_float2(__uint_as_float(w0.x), __uint_as_float(w0.y));
                 p24DecodeConic(w1.x, w1.y, A, B, C, o);
                 r2 = make_float4(halfLoF(w2.x), halfHiF(w2.x), halfLoF(w2.y), 0.0f);
+                radius = float(w2.y >> 16);
             }
             // the strips the cutoff ellipse meets (makeCutoffEllipse's threshold, wider margin):
             // none below opacity 1/255, all for an invalid conic
             uint32_t strips = (1u << (kThreads / 32)) - 1u;
             const float D = A * C - B * B;
+            const bool ellipse = A > 0.0f && C > 0.0f && D > 0.0f;
             if (!(o >= 1.0f / 255.0f)) {
                 strips = 0u;
-            } else if (A > 0.0f && C > 0.0f && D > 0.0f) {
+            } else if (ellipse) {
                 const float qmax = 2.0f * __logf(255.0f * o) + 1e-3f;
                 const float rho = fabsf(B) * rsqrtf(A * C);
                 const float K = 2.0f / fmaxf(1.0f - rho, 1e-30f);
                 const float t = qmax + (2e-3f + 4e-5f * K) * fmaxf(qmax, 1.0f) + 4e-3f;
                 if (t < 1e30f) strips = stripMask<TILE>(r0.x, r0.y, A, B, C, D, t, float(tx * kTW), float(ty * kTH));
             }
+            // 32 x 8 tiles: a bin's 32 columns can reach 16 px past the splat's 16-px rectangle,
+            // which bounds the splat's pixels wherever the coverage used it (rect and tight
+            // bounds, and cutoff-only bounds for a splat without an ellipse)
+            if constexpr (TILE == 32)
+                if (a.bounds != kBoundsCutoff || !ellipse) strips &= rectStrips32(r0.x, radius, tx * kTW);
             sm.strips[tid] = strips;
             sm.conic[tid] = make_float4(-0.5f * kLog2e * A, -kLog2e * B, -0.5f * kLog2e * C, o);
             sm.color[tid] = r2;

@@ -39,6 +39,15 @@ __device__ __forceinline__ uint64_t virtualKey(uint64_t key, uint32_t lowBits, u
 
 __device__ __forceinline__ uint64_t maskOf(uint32_t bits) { return bits >= 64 ? ~0ull : ((1ull << bits) - 1ull); }
 
+// The depth sort's key of a depth word: the varying depth bits (and the sentinel bit) above the
+// record index, with the view (the word's field at viewShift, when there is one) right above
+// them, so that (view, depth) costs no digit pass on the depth bits every real depth shares.
+__device__ __forceinline__ uint64_t depthVirtualKey(uint64_t word, uint32_t indexBits, uint32_t depthBits,
+                                                    uint32_t viewShift) {
+    const uint64_t depth = (word >> indexBits) & maskOf(depthBits);
+    return viewShift ? ((word >> viewShift) << depthBits) | depth : depth;
+}
+
 __device__ __forceinline__ uint32_t laneMaskLt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
@@ -107,19 +116,21 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     __shared__ uint32_t sAny;
     DeviceControl* ctl = a.ctl;
     const uint32_t entries = a.frameMode == 2 ? a.count : ctl->c.entries;
-    uint32_t lowBits, keyBits, packed = 0, indexBits = 0;
+    uint32_t lowBits, keyBits, packed = 0, indexBits = 0, depthBits = 0, viewShift = 0;
     if (a.frameMode == 1) {
         const KeyLayout lay = keyLayout(ctl, a.tileCount, a.count, a.binning != 0);
         lowBits = lay.lowBits;
         packed = lay.packed;
         indexBits = lay.indexBits;
         keyBits = bitWidth(ctl->c.tile_max) + lowBits;
-    } else if (a.frameMode == 2) {  // binning mode's depth keys: W depth bits + the sentinel bit
+    } else if (a.frameMode == 2) {  // binning mode's depth keys: W depth bits + the sentinel bit (+ the view)
         const uint32_t dmin = ctl->c.depth_min_bits, dmax = ctl->c.depth_max_bits;
         lowBits = 0;
         packed = 1;
         indexBits = a.indexBits;
-        keyBits = (dmin > dmax ? 0u : bitWidth(dmin ^ dmax)) + 1u;
+        depthBits = (dmin > dmax ? 0u : bitWidth(dmin ^ dmax)) + 1u;
+        viewShift = a.viewBits ? a.indexBits + 32u : 0u;
+        keyBits = depthBits + a.viewBits;
     } else {
         lowBits = a.fixedLowBits;
         keyBits = a.fixedKeyBits;
@@ -145,7 +156,9 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
 #pragma unroll
         for (int j = 0; j < kHistItems; ++j) {
             if (base + j * 256 + threadIdx.x < entries) {
-                const uint64_t v = packed ? (k[j] >> indexBits) : virtualKey(k[j], lowBits, keyMask);
+                const uint64_t v = a.frameMode == 2 ? depthVirtualKey(k[j], indexBits, depthBits, viewShift)
+                                   : packed          ? (k[j] >> indexBits)
+                                                     : virtualKey(k[j], lowBits, keyMask);
                 for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][uint32_t(v >> (BITS * p)) & D::kMask], 1u);
             }
         }
@@ -198,6 +211,8 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
         plan->packed = packed;
         plan->indexBits = indexBits;
         plan->digitBits = BITS;
+        plan->depthBits = depthBits;
+        plan->viewShift = viewShift;
         plan->sortedBuffer = activeCount & 1u;
         if (a.frameMode == 2) return;  // the list's own plan fills the control block
         ctl->c.packed_entries = packed;
@@ -282,7 +297,7 @@ static_assert(PassShape<false, kDepthSortItems, 8>::kTile == kDepthSortTile, "th
 // The blocks of a pass are persistent: each takes tiles by ticket (the tile order of the
 // look-back) until the list is done, so a pass launches a fixed grid of blocks that all stay
 // resident (blocks only ever wait on tiles already taken by running blocks).
-template <bool PAIRS, int ITEMS, int BITS>
+template <bool PAIRS, int ITEMS, int BITS, bool DEPTH = false>
 __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, unsigned char* smem, uint32_t* sOff,
                                               uint32_t* sScan, uint32_t& sTile) {
     using S = PassShape<PAIRS, ITEMS, BITS>;
@@ -312,8 +327,10 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
     uint32_t* valsOut = a.values[in ^ 1u];
     const uint32_t lowBits = plan->lowBits;
     const uint64_t keyMask = maskOf(plan->keyBits);
-    const uint32_t shift = BITS * p + (PAIRS ? 0u : plan->indexBits);
+    const uint32_t shift = BITS * p + (PAIRS || DEPTH ? 0u : plan->indexBits);
+    const uint32_t indexBits = plan->indexBits, depthBits = plan->depthBits, viewShift = plan->viewShift;
     auto digit = [&](uint64_t k) -> uint32_t {
+        if constexpr (DEPTH) return uint32_t(depthVirtualKey(k, indexBits, depthBits, viewShift) >> shift) & D::kMask;
         return PAIRS ? uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & D::kMask : uint32_t(k >> shift) & D::kMask;
     };
 
@@ -436,7 +453,7 @@ __global__ void __launch_bounds__(kSortThreads, BITS == 9 ? 2 : 4) depthPassKern
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ uint32_t sOff[1 << BITS], sScan[8], sTile;
     if (!a.plan->active[p]) return;
-    sortPassTiles<false, kDepthSortItems, BITS>(a, p, smem, sOff, sScan, sTile);
+    sortPassTiles<false, kDepthSortItems, BITS, true>(a, p, smem, sOff, sScan, sTile);
 }
 
 // ---- tile ranges (tile_ranges.comp:22-44) -----------------------------------------------------

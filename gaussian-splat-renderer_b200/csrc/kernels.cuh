@@ -93,8 +93,12 @@ struct FrontArgs {
     uint64_t* depthKeys[2];               // [V * N] (depth mod 2^W, or the no-tile sentinel) << recordBits | record
     const struct SortPlan* depthPlan;     // its sort's plan (which buffer holds the result)
     uint32_t recordBits;                  // bits of a record index (V * N - 1)
+    uint32_t depthViewShift;              // the view's field in the depth words, above the depth bits
+                                          // (0: none; the depth sort then orders all views together)
     const uint4* latents;                 // learned colour: fp16 latents [N] (null: SH colour)
     const struct DecoderWeights* decoder; // learned colour: the tensor-core decoder (mlp.cuh)
+    float4* decoded;                      // tcgen05 decode: kept gaussians' colours [viewCount][N]
+                                          // (null: the preprocess decodes with mma.sync)
     DeviceControl* ctl;
     LogfFixups logf;
 };
@@ -117,6 +121,8 @@ struct SortPlan {
     uint32_t active[kMaxSortPasses];
     uint32_t inBuffer[kMaxSortPasses];
     uint32_t digitBits;     // digit width of the passes (7, 8 or 9)
+    uint32_t depthBits;     // the depth sort: varying depth bits + the sentinel bit of its virtual key
+    uint32_t viewShift;     // the depth sort: position of the view field in the words (0: none)
     uint32_t digitBase[kMaxSortPasses][kMaxSortBins];
     uint32_t hist[kMaxSortPasses][kMaxSortBins];
     uint32_t sortedBuffer;  // the buffer that holds the result (active passes mod 2)
@@ -140,6 +146,7 @@ struct SortArgs {
     uint32_t binning;
     uint32_t indexBits;         // frameMode 2: bits of the record index
     uint32_t digitBits;         // 7, 8 or 9 bits a pass
+    uint32_t viewBits;          // frameMode 2: bits of the view field above the depth bits (0: none)
 };
 
 struct RenderArgs {
@@ -149,7 +156,8 @@ struct RenderArgs {
     const float4* rayDepth;   // [V * N * 3] StopThePop ray-depth parameters (sortWindow > 0)
     const DevCameraArgs* cam; // the frame's cameras [viewCount] (focal lengths of the pixel rays)
     uint32_t sortWindow;      // StopThePop window K, 0 = off
-    uint32_t tileSize;        // the render tile: 16 (INRIA) or 8 pixels
+    uint32_t tileSize;        // the render tile: 16 (INRIA), 8 or 32 (32 x 8) pixels
+    uint32_t bounds;          // GsrTileBounds of the list (32 x 8 tiles clip splats to their 16-px rectangle)
     const uint32_t* values[2];
     const uint64_t* keys[2];
     uint32_t* ranges;         // uint2 per tile of the frame (all views)
@@ -184,6 +192,9 @@ cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, c
 // the depth keys) the scan of the counts in depth order and the emission in that order.
 cudaError_t launchFrontBinningKeys(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s);
 cudaError_t launchFrontBinningEmit(const FrontArgs& a, cudaStream_t s);
+// The learned colour's decode as a pre-pass on the tcgen05 tensor cores: every kept gaussian's
+// colour for every view of the frame into a.decoded (before the preprocess, which reads them).
+cudaError_t launchDecodeColoursTc(const FrontArgs& a, uint32_t geometry, cudaStream_t s);
 cudaError_t launchSort(const SortArgs& a, uint32_t histBlocks, cudaStream_t s);
 cudaError_t launchRanges(const RenderArgs& a, uint32_t capacity, cudaStream_t s);
 cudaError_t launchRender(const RenderArgs& a, cudaStream_t s);

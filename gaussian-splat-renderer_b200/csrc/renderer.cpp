@@ -432,6 +432,7 @@ struct GsrRenderer {
 
     // per gaussian
     DevBuf splats, hints, spanRows, tileCounts, offsets, scanStatus;
+    DevBuf decodedColours;  // GSR_DECODE_TCGEN05: the pre-pass's colours, 16 B per (view, gaussian)
     DevBuf packedSplats, rects, depths;  // packed render records (P32 / P24) and their side arrays
     DevBuf rayDepth;                     // StopThePop ray-depth parameters (3 x float4 per record)
     // control + plan
@@ -445,7 +446,19 @@ struct GsrRenderer {
     // the binning / render tiles: tile_size 16 or 8 (square), 32 (32 x 8)
     uint32_t tileW() const { return settings.tile_size; }
     uint32_t tileH() const { return settings.tile_size == 32 ? 8u : settings.tile_size; }
-    uint32_t depthPasses() const { return (32u + digitBits() - 1u) / digitBits(); }
+    // The depth words of a frame of v views carry the view above the depth bits when the word
+    // has room (record bits + 32 depth bits + view bits <= 64): the depth sort then orders by
+    // (view, depth), one view's records after another's. 0: no view field (one view, or no room).
+    uint32_t depthViewBits(size_t v) const {
+        if (v <= 1) return 0u;
+        const uint64_t n = uint64_t(scene.count) * v;
+        const uint32_t rb = n > 1 ? bitWidth(uint32_t(n - 1)) : 1u, vb = bitWidth(uint32_t(v - 1));
+        return rb + 32u + vb <= 64u ? vb : 0u;
+    }
+    // Passes launched for the depth sort: the depth word's 32 bits and the view bits (the plan
+    // skips the ones the frame's depth range does not need)
+    uint32_t depthPasses(size_t v) const { return (32u + depthViewBits(v) + digitBits() - 1u) / digitBits(); }
+    uint32_t depthPasses() const { return depthPasses(std::max<size_t>(views.size(), 1)); }
     size_t statusWordsPerTile() const { return size_t(1) << digitBits(); }
     // the output image: bytes per pixel, the kernel's format code, and the RGB8 companion
     uint32_t imageBytes() const {
@@ -494,6 +507,7 @@ struct GsrRenderer {
     // the TMA gather: the tensor map over `splats` (valid while splatMapOk)
     alignas(64) CUtensorMap splatMap{};
     bool splatMapOk = false;
+    bool tcDecode() const { return settings.color_decode == GSR_DECODE_TCGEN05; }
     bool tmaGather() const {
         return settings.raster_gather == GSR_GATHER_TMA && settings.render_splat == GSR_RENDER_SPLAT_FULL &&
                settings.sort_window == 0 && !settings.tile_stats;
@@ -628,9 +642,10 @@ struct GsrRenderer {
         GSR_CUDA(hints.alloc(n * 16));
         GSR_CUDA(spanRows.alloc(n * 16));
         if (settings.sort_window > 0) GSR_CUDA(rayDepth.alloc(n * 48));
+        if (tcDecode()) GSR_CUDA(decodedColours.alloc(n * 16));
         if (binning()) {
             for (auto& k : depthKeys) GSR_CUDA(k.alloc(n * 8));
-            GSR_CUDA(depthStatus.alloc(size_t(depthPasses()) * ((n + kDepthSortTile - 1) / kDepthSortTile) *
+            GSR_CUDA(depthStatus.alloc(size_t(depthPasses(v)) * ((n + kDepthSortTile - 1) / kDepthSortTile) *
                                        statusWordsPerTile() * 8));
             GSR_CUDA(cudaMemset(depthStatus.p, 0, depthStatus.bytes));
         }
@@ -854,7 +869,8 @@ struct GsrRenderer {
         // frameBegin, preprocess, scan, duplicate, histogram, one per pass, ranges, render
         // binning: frameBegin, preprocess, depth histogram + passes, scan, duplicate, list
         // histogram + passes, ranges, render
-        kernelLaunches += (binning() ? 8 + depthPasses() + list->passes : 7 + list->passes) + (split ? uint32_t(parts.size()) - 1 : 0);
+        kernelLaunches += (binning() ? 8 + depthPasses() + list->passes : 7 + list->passes) + (split ? uint32_t(parts.size()) - 1 : 0) +
+                          (colorLatents && tcDecode() ? 1u : 0u);
         timed = timing;
         ++frameIndex;
         return GSR_OK;
@@ -882,6 +898,7 @@ struct GsrRenderer {
         fa.scene = sceneArgs(scene);
         fa.latents = colorLatents;
         fa.decoder = colorDecoder;
+        fa.decoded = colorLatents && tcDecode() ? decodedColours.as<float4>() : nullptr;
         fa.count = scene.count;
         fa.evalDegree = evalDegree;
         fa.bounds = settings.bounds;
@@ -902,12 +919,15 @@ struct GsrRenderer {
         fa.scanStatus = scanStatus.as<uint64_t>();
         fa.ctl = ctl;
         fa.logf = logf;
+        if (fa.decoded) GSR_CUDA(launchDecodeColoursTc(fa, scene.geometry, stream));  // timed with the preprocess
         if (binning()) {
             fa.binning = 1;
             fa.depthKeys[0] = depthKeys[0].as<uint64_t>();
             fa.depthKeys[1] = depthKeys[1].as<uint64_t>();
             fa.depthPlan = depthPlan.as<SortPlan>();
             fa.recordBits = recordBits();
+            const uint32_t viewBits = depthViewBits(viewCount);
+            fa.depthViewShift = viewBits ? fa.recordBits + 32u : 0u;
             GSR_CUDA(launchFrontBinningKeys(fa, scene.geometry, scene.color, stream));
             mark(stream);
             // the records by (depth, record index): 32 depth bits above the record index
@@ -923,6 +943,7 @@ struct GsrRenderer {
             sd.frameMode = 2;
             sd.count = scene.count * viewCount;
             sd.indexBits = fa.recordBits;
+            sd.viewBits = viewBits;
             GSR_CUDA(launchSort(sd, 148 * 2, stream));
             mark(stream);
             GSR_CUDA(launchFrontBinningEmit(fa, stream));
@@ -957,6 +978,7 @@ struct GsrRenderer {
         ra.cam = slot.camDevice.as<DevCameraArgs>();
         ra.sortWindow = settings.sort_window;
         ra.tileSize = settings.tile_size;
+        ra.bounds = settings.bounds;
         for (int b = 0; b < 2; ++b) {
             ra.values[b] = l.values[b].as<uint32_t>();
             ra.keys[b] = l.keys[b].as<uint64_t>();
@@ -1333,6 +1355,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
         return fail(GSR_ERROR_INVALID_ARGUMENT, "tile_stats %u (0 or 1, not with sort_window)", settings->tile_stats);
     if (settings->sort_digit_bits != 0 && (settings->sort_digit_bits < 7 || settings->sort_digit_bits > 9))
         return fail(GSR_ERROR_INVALID_ARGUMENT, "sort digit bits %u (7, 8 or 9)", settings->sort_digit_bits);
+    if (settings->color_decode > GSR_DECODE_TCGEN05)
+        return fail(GSR_ERROR_INVALID_ARGUMENT, "colour decode %u", settings->color_decode);
     GSR_CUDA(r->control.alloc(sizeof(DeviceControl)));
     GSR_CUDA(cudaMemset(r->control.p, 0, sizeof(DeviceControl)));
     GSR_CUDA(r->plan.alloc(sizeof(SortPlan)));

@@ -36,6 +36,7 @@ RASTER_SCHEDULES = {"auto": 0, "per-tile": 1, "persistent": 2}
 LIST_MODES = {"binning": 0, "global": 1}
 RENDER_SPLATS = {"full": 0, "p32": 1, "p24": 2}
 RASTER_GATHERS = {"default": 0, "cp.async": 1, "tma": 2}
+COLOR_DECODES = {"default": 0, "fused": 1, "tcgen05": 2}
 CONTROL_TIMEOUT, CONTROL_BOUNDS, CONTROL_KEY_RANGE = 1, 2, 4
 
 SPLAT_DTYPE = np.dtype(
@@ -89,6 +90,7 @@ class CSettings(C.Structure):
         ("frames_in_flight", C.c_uint32), ("use_graph", C.c_uint32), ("raster_schedule", C.c_uint32),
         ("list_mode", C.c_uint32), ("render_splat", C.c_uint32), ("sort_window", C.c_uint32),
         ("sort_digit_bits", C.c_uint32), ("tile_stats", C.c_uint32), ("raster_gather", C.c_uint32),
+        ("color_decode", C.c_uint32),
     ]
 
 
@@ -313,6 +315,7 @@ class Settings:
     sort_digit_bits: int = 0  # radix digit width of the list sort (0 = 8)
     tile_stats: bool = False  # the instrumented rasterizer with per-tile statistics (read_tile_stats)
     raster_gather: str = "default"  # how batches reach shared memory: default, cp.async or tma
+    color_decode: str = "default"  # the learned colour's decoder: default, fused (mma.sync) or tcgen05
 
     def to_c(self) -> CSettings:
         s = CSettings()
@@ -338,6 +341,7 @@ class Settings:
         s.sort_digit_bits = self.sort_digit_bits
         s.tile_stats = int(self.tile_stats)
         s.raster_gather = RASTER_GATHERS[self.raster_gather]
+        s.color_decode = COLOR_DECODES[self.color_decode]
         return s
 
 

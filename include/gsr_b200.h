@@ -168,7 +168,20 @@ typedef struct GsrSettings {
                                           (TileSettings::stats, splat_tile_renderer.h:102); not with
                                           sort_window; read with gsr_read_tile_stats */
     uint32_t raster_gather;            /* GsrRasterGather: how the rasterizer stages each batch of records */
+    uint32_t color_decode;             /* GsrColorDecode: where the learned colour's decoder runs */
 } GsrSettings;
+
+/* Where the learned colour stage decodes (latent, view direction) -> RGB (no reference
+ * counterpart). The images agree to the last bits of FP32 (the bias is added after the
+ * products in the tcgen05 pre-pass, into the accumulator before them in the fused decode). */
+typedef enum GsrColorDecode {
+    GSR_DECODE_DEFAULT = 0, /* the build's default (GSR_DECODE_FUSED) */
+    GSR_DECODE_FUSED = 1,   /* inside the preprocess: each warp decodes its 32 gaussians with chained
+                               mma.sync.m16n8k16 BF16 products in registers */
+    GSR_DECODE_TCGEN05 = 2  /* a pre-pass kernel on the fifth-generation tensor cores: tcgen05.mma over
+                               128-gaussian tiles with FP32 accumulators in tensor memory; the colours
+                               (16 B per view and gaussian) are read by the preprocess */
+} GsrColorDecode;
 
 /* How the rasterizer brings a batch of records into shared memory (no reference counterpart; the
  * reference's workgroup fetches them cooperatively, tile_render.comp:281-400). The images are

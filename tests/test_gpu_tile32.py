@@ -1,9 +1,10 @@
 """32 x 8 tiles (`tile_size` 32: bins and render tiles of 32 x 8 pixels, as many pixels as INRIA's
 16 x 16 tile; no reference counterpart, its bins are square). The lists equal the oracle's
 construction on 32 x 8 bins in every bounds mode and both list modes, on sizes that are not
-multiples of the bins; with tight or cutoff-only bounds the images equal the 16-px images bit for
-bit (the cutoff ellipse decides which pixels take a splat, whatever the bins). With INRIA's
-rectangles the wide bins reach pixels beyond a splat's 16-px rectangle, so that image may differ."""
+multiples of the bins; in every bounds mode the images equal the 16-px images bit for bit: the
+cutoff ellipse decides which pixels take a splat whatever the bins, and where the coverage is
+bounded by the splat's 16-px INRIA rectangle (rect and tight bounds), the rasterizer clips the
+32-px-wide bins, which can reach 16 px past that rectangle, back to it."""
 import numpy as np
 import pytest
 
@@ -39,9 +40,8 @@ def test_lists_and_image_at_32x8(gpu, port, bounds, list_mode, size):
     np.testing.assert_array_equal(ranges, want["ranges"])
     layout = r32.view_layouts()[0]
     assert (layout.tiles_x, layout.tiles_y) == ((size[0] + 31) // 32, (size[1] + 7) // 8)
-    if bounds != "rect":
-        r16 = render(gpu, gs, cam, 16, bounds=bounds, list_mode=list_mode)
-        assert r32.read_back_image().tobytes() == r16.read_back_image().tobytes()
+    r16 = render(gpu, gs, cam, 16, bounds=bounds, list_mode=list_mode)
+    assert r32.read_back_image().tobytes() == r16.read_back_image().tobytes()
 
 
 def test_32x8_batched_views_gathers_and_stats(gpu):

@@ -116,3 +116,27 @@ def test_bench_gpus_2_launches_two_ranks_and_gathers_views():
     line = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
     assert line["n_gpus"] == 2 and line["views"] == 64 and line["views_gathered"] == 64
     assert line["gathered_in_order"] and line["max_rank"] == 1.0
+
+
+def test_pass_bytes_model():
+    """The roofline's byte model: a one-view frame counts the scene data its culls let through
+    (16 B position, 32 B shape past the culls, 192 B SH of the visible); a frame of several views
+    counts the whole scene once and every record's writes."""
+    import types
+
+    import bench
+
+    n, vis, entries = 1000, 900, 5000
+    ctl = types.SimpleNamespace(cull_counts=[vis, 40, 0, 50, 10], entries=entries, packed_entries=True,
+                                sort_passes=2, depth_min_bits=0x40000000, depth_max_bits=0x41000000)
+    one = bench.pass_bytes("f32", ctl, n, 120)
+    assert one["preprocess"] == 16 * n + 32 * (n - 40 - 10) + 192 * vis + 12 * n + 64 * vis
+    assert one["depth sort"] == 8 * n + 16 * n * bench.depth_sort_passes(ctl)
+    assert one["tile sort"] == 8 * entries + 16 * entries * 2
+    assert one["ranges"] == 8 * entries + 8 * 120
+    four = bench.pass_bytes("f32", ctl, 4 * n, 480, views=4)
+    assert four["preprocess"] == 240 * n + 12 * 4 * n + 64 * vis
+    assert four["depth sort"] == 8 * 4 * n + 16 * 4 * n * bench.depth_sort_passes(ctl)
+    assert bench.pass_bytes("f16", ctl, 4 * n, 480, views=4)["preprocess"] == 128 * n + 48 * n + 64 * vis
+    # the depth sort's passes: the varying depth bits plus the no-tile bit, `bits` a pass
+    assert bench.depth_sort_passes(ctl, 8) == 4 and bench.depth_sort_passes(ctl, 9) == 3
