@@ -26,9 +26,12 @@ step         one pass over a workload's views: the 300-view orbit, the 64 batche
 value        views/s over all ranks, scene and cameras resident on the device: CUDA events on
              the launching stream around the K steps (barrier + synchronize on both sides, the
              max over ranks).
-e2e          the same views through the calls a host application makes (gsr_render_to_host,
-             gsr_render_views_to_host): cameras from host memory, every view's RGB8 image
-             copied into pinned host memory, synchronized every call.
+e2e          the same views through the calls a host application makes: cameras from host
+             memory, every view's RGB8 image copied into pinned host memory. Single views:
+             gsr_render_to_host, synchronized every call. Batched frames: the streaming call
+             gsr_render_views_to_host_async into two alternating pinned buffers, each frame's
+             copies waited for after the next frame is enqueued; the clock stops after the last
+             frame's images are in host memory.
 parity       per workload (the CPU leg, rank 0), one view (or one per resolution): the list
              (keys, values, tile ranges) bit for bit against the oracle's construction, the
              float image's PSNR and the 8-bit image's PSNR and largest difference against the
@@ -467,14 +470,25 @@ def render_call(r, frames: Frames, k: int, stream: int):
         r.render_views(call, stream)
 
 
-def to_host_call(r, frames: Frames, k: int, host: dict, stream: int):
+def to_host_call(r, frames: Frames, k: int, host: dict, stream: int, pending: list):
+    """One end-to-end call. Single views: gsr_render_to_host (synchronous). Batched frames: the
+    streaming form, gsr_render_views_to_host_async into one of two pinned buffers, then a wait
+    for the previous frame's ticket (so frame k's copies overlap frame k + 1's preprocess and
+    sorts); `pending` holds the ticket still outstanding."""
     call = frames.calls[k % len(frames.calls)]
     px = sum(w * h for w, h in frames.sizes[k % len(frames.sizes)])
-    buf = host[px]
     if frames.d == 1:
-        r.render_to_host(call, buf, stream)
-    else:
-        r.render_views_to_host(call, buf, stream)
+        r.render_to_host(call, host[px][0], stream)
+        return
+    ticket = r.render_views_to_host_async(call, host[px][k % 2], stream)
+    if pending:
+        r.host_wait(pending.pop())
+    pending.append(ticket)
+
+
+def drain(r, pending: list):
+    while pending:
+        r.host_wait(pending.pop())
 
 
 def time_form(r, frames: Frames, args, dist: Dist, sampler: Sampler, stream_obj):
@@ -516,21 +530,24 @@ def time_form(r, frames: Frames, args, dist: Dist, sampler: Sampler, stream_obj)
     clocks = sampler.summary()
     launches = r.kernel_launches() - launches0
     resizes = r.capacity()[2] - resizes0
-    # end to end: pinned host buffers per frame size
+    # end to end: two pinned host buffers per frame size (the streaming form alternates them)
     host = {}
     for sz in frames.sizes:
         px = sum(w * h for w, h in sz)
         if px not in host:
-            host[px] = torch.empty((px * 3,), dtype=torch.uint8).pin_memory().numpy()
+            host[px] = [torch.empty((px * 3,), dtype=torch.uint8).pin_memory().numpy() for _ in range(2)]
+    pending = []
     for j in range(min(calls, 3)):
-        to_host_call(r, frames, j, host, stream)
+        to_host_call(r, frames, j, host, stream, pending)
+    drain(r, pending)
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t0 = time.perf_counter()
     e0.record(stream_obj)
     for j in range(n_calls):
-        to_host_call(r, frames, j, host, stream)
+        to_host_call(r, frames, j, host, stream, pending)
+    drain(r, pending)  # the last frame's views are in host memory before the clock stops
     e1.record(stream_obj)
     e1.synchronize()
     e2e_ms = dist.max(max(e0.elapsed_time(e1), (time.perf_counter() - t0) * 1e3))
@@ -540,7 +557,10 @@ def time_form(r, frames: Frames, args, dist: Dist, sampler: Sampler, stream_obj)
     return {"views_per_frame": frames.d, "views_timed": int(views_all), "steps": args.steps,
             "views_per_s": round(views_all / (ms / 1e3), 3), "e2e_views_per_s": round(views_all / (e2e_ms / 1e3), 3),
             "ms_per_view": round(ms / views, 4), "ms_per_step": round(ms / args.steps, 3),
-            "e2e_ms_per_step": round(e2e_ms / args.steps, 3), "gpu_launches": int(launches),
+            "e2e_ms_per_step": round(e2e_ms / args.steps, 3),
+            "e2e_call": "gsr_render_to_host (synchronous)" if frames.d == 1 else
+                        "gsr_render_views_to_host_async, two pinned buffers, one frame in flight",
+            "gpu_launches": int(launches),
             "list_resizes_timed": int(resizes),
             # GsrCamera (200 B) per one-view call, GsrSplatCamera (108 B) per view of a batched call
             "h2d_bytes_per_step": int(frames.views_per_step * (200 if frames.d == 1 else 108)),

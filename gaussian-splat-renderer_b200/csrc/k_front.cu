@@ -538,8 +538,9 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
         const uint32_t records = a.count * a.viewCount;
         slot = size_t(blockIdx.x) * kFrontThreads + tid;
         const uint64_t* sorted = a.depthKeys[a.depthPlan->sortedBuffer & 1u];
-        rec = slot < records ? uint32_t(sorted[slot] & ((1ull << a.recordBits) - 1ull)) : 0u;
-        view = uint32_t(rec / a.count);
+        const uint64_t word = slot < records ? sorted[slot] : 0ull;
+        rec = uint32_t(word & ((1ull << a.recordBits) - 1ull));
+        view = a.depthViewShift ? uint32_t(word >> a.depthViewShift) : uint32_t(rec) / a.count;
         i = uint32_t(rec - size_t(view) * a.count);
         count = slot < records && view < a.viewCount ? a.tileCounts[rec] : 0u;
     } else {
@@ -549,6 +550,11 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
         slot = rec;
         count = i < a.count ? a.tileCounts[rec] : 0u;
     }
+    // (staging a warp's entries in shared memory for one coalesced write-out of its range
+    // measured slower: 0.494 against 0.424 ms for scan + emission of an 8-view 1080p frame)
+    auto putKey = [&](uint32_t k, uint64_t key) {
+        if (k < a.capacity) a.keys[k] = key;
+    };
     if (count > 0) {
         const uint32_t sentinel = a.totalTiles;
         const KeyLayout lay = keyLayout(a.ctl, sentinel, a.count, BINNING);
@@ -585,13 +591,11 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
                     for (uint32_t x = x0; x < x1 && written < count; ++x, ++written, ++k) {
                         const uint32_t tile = rowBase + x;
                         tileMax = tile > tileMax ? tile : tileMax;
-                        if (k < a.capacity) {
-                            if (lay.packed) {
-                                a.keys[k] = (uint64_t(tile) << tileShift) | packedBase;
-                            } else {
-                                a.keys[k] = (uint64_t(tile) << 32) | depthBits;
-                                a.values[k] = i;
-                            }
+                        if (lay.packed) {
+                            putKey(k, (uint64_t(tile) << tileShift) | packedBase);
+                        } else if (k < a.capacity) {
+                            a.keys[k] = (uint64_t(tile) << 32) | depthBits;
+                            a.values[k] = i;
                         }
                     }
                 }
@@ -600,10 +604,9 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
                 atomicAdd(&sMismatch, 1u);
                 tileMax = sentinel;
                 for (; written < count; ++written, ++k) {
-                    if (k >= a.capacity) continue;
                     if (lay.packed) {
-                        a.keys[k] = (uint64_t(sentinel) << tileShift) | packedBase;
-                    } else {
+                        putKey(k, (uint64_t(sentinel) << tileShift) | packedBase);
+                    } else if (k < a.capacity) {
                         a.keys[k] = (uint64_t(sentinel) << 32) | depthBits;
                         a.values[k] = i;
                     }
@@ -653,8 +656,8 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
         const uint32_t tileShift = lay.lowBits + lay.indexBits;
         auto emit = [&](uint32_t k, uint32_t tile) {
             if (lay.packed) {
-                a.keys[k] = (uint64_t(tile) << tileShift) | packedBase;
-            } else {
+                putKey(k, (uint64_t(tile) << tileShift) | packedBase);
+            } else if (k < a.capacity) {
                 a.keys[k] = (uint64_t(tile) << 32) | depthBits;
                 a.values[k] = i;
             }
@@ -670,14 +673,13 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
             for (int x = x0; x < x1 && written < count; ++x, ++written, ++k) {
                 const uint32_t tile = vw.tileBase + uint32_t(row) * uint32_t(gx) + uint32_t(x);
                 tileMax = tile > tileMax ? tile : tileMax;
-                if (k < a.capacity) emit(k, tile);
+                emit(k, tile);
             }
         }
         if (written != count) {
             atomicAdd(&sMismatch, 1u);
             tileMax = sentinel;
-            for (; written < count; ++written, ++k)
-                if (k < a.capacity) emit(k, sentinel);
+            for (; written < count; ++written, ++k) emit(k, sentinel);
         }
         atomicMax(&sTileMax, tileMax);
         sAny = 1;

@@ -563,6 +563,24 @@ struct GsrRenderer {
         uint64_t pixelOffset, pixels;
     };
     std::vector<RenderPart> parts;
+    // gsr_render_views_to_host_async: after the frame's copies the copy stream records
+    // imageCopied; the next frame's rasterization (of any kind) waits for it, so only the next
+    // frame's front overlaps this frame's copies (about 1 ms of copies against 2 ms of front
+    // for 8 views at 1080p). hostDone[t mod kHostTickets] marks the end of ticket t's copies
+    // (tickets complete in order).
+    bool hostAsync = false;
+    cudaEvent_t imageCopied = nullptr;
+    static constexpr uint32_t kHostTickets = 8;
+    cudaEvent_t hostDone[kHostTickets] = {};
+    uint64_t hostTickets = 0;
+    // the wait before a rasterization launch: an external event node when captured
+    int waitCopied(cudaEvent_t e, cudaStream_t stream) {
+        if (!e) return GSR_OK;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        GSR_CUDA(cudaStreamIsCapturing(stream, &cs));
+        GSR_CUDA(cudaStreamWaitEvent(stream, e, cs == cudaStreamCaptureStatusActive ? cudaEventWaitExternal : 0));
+        return GSR_OK;
+    }
     void planParts() {
         parts.clear();
         for (const GsrViewLayout& L : views)
@@ -580,6 +598,9 @@ struct GsrRenderer {
             if (e) cudaEventDestroy(e);
         if (captureStream) cudaStreamDestroy(captureStream);
         if (copyStream) cudaStreamDestroy(copyStream);
+        if (imageCopied) cudaEventDestroy(imageCopied);
+        for (cudaEvent_t e : hostDone)
+            if (e) cudaEventDestroy(e);
     }
 
     // the (view, tile) queue rasterizer: asked for, or chosen by the auto schedule for batches
@@ -667,6 +688,7 @@ struct GsrRenderer {
     // tiles and pixels over all views, and the list when the key width changes.
     int setLayout(const uint32_t* w, const uint32_t* h, uint32_t v) {
         if (v == 0 || v > GSR_MAX_VIEWS) return fail(GSR_ERROR_INVALID_ARGUMENT, "views %u (1..%u)", v, GSR_MAX_VIEWS);
+        if (copyStream) GSR_CUDA(cudaStreamSynchronize(copyStream));  // copies still reading the old images
         if (uint64_t(scene.count) * v > 0xFFFFF800ull)
             return fail(GSR_ERROR_INVALID_ARGUMENT, "views x gaussians = %llu exceeds 2^32",
                         (unsigned long long)(uint64_t(scene.count) * v));
@@ -820,13 +842,14 @@ struct GsrRenderer {
         static_assert(sizeof(DevCameraArgs) == sizeof(GsrSplatCamera), "camera layout");
         std::memcpy(slot.camHost, cams, sizeof(GsrSplatCamera) * v);
         // view by view: several per-tile views with their images wanted on the host
-        const bool split = hostCopies && v > 1 && !persistentRaster(v);
+        const bool split = hostCopies && (v > 1 || hostAsync) && !persistentRaster(v);
         if (split) planParts();
         while (split && slot.viewDone.size() < parts.size()) {
             cudaEvent_t e = nullptr;
             GSR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
             slot.viewDone.push_back(e);
         }
+
         splitViews = split;
         lastSplit = split;
         lastSlot = &slot;
@@ -1002,6 +1025,8 @@ struct GsrRenderer {
         }
         GSR_CUDA(launchRanges(ra, l.capacity, stream));
         mark(stream);
+        // the images may still be on their way to the host (the streaming call): wait for it
+        if (int rc = waitCopied(imageCopied, stream)) return rc;
         if (splitViews) {
             // inside a capture the view events become external event nodes (recorded by each
             // launch of the graph); outside one they are plain records
@@ -1373,6 +1398,8 @@ int gsr_renderer_create(const GsrSceneDesc* scene, const GsrSettings* settings, 
     rc = r->ensureViews(1);
     if (rc) return rc;
     for (auto& e : r->ev) GSR_CUDA(cudaEventCreate(&e));
+    GSR_CUDA(cudaEventCreateWithFlags(&r->imageCopied, cudaEventDisableTiming));
+    for (auto& e : r->hostDone) GSR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     *out = r.release();
     return GSR_OK;
 }
@@ -1575,6 +1602,48 @@ int gsr_render_views_to_host(GsrRenderer* r, const GsrSplatCamera* cameras, uint
     if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, the views need %llu",
                                    (unsigned long long)bytes, (unsigned long long)need);
     return copyFrameToHost(r, host, need, static_cast<cudaStream_t>(stream));
+}
+
+int gsr_render_views_to_host_async(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* host,
+                                   uint64_t bytes, void* stream, uint64_t* ticket) {
+    if (!r || !cameras || !host || !ticket) return fail(GSR_ERROR_INVALID_ARGUMENT, "null argument");
+    r->hostCopies = true;
+    r->hostAsync = true;
+    int rc = gsr_render_views(r, cameras, views, stream);
+    r->hostCopies = false;
+    r->hostAsync = false;
+    if (rc) return rc;
+    const bool rgb = r->rgb8.p != nullptr;
+    const uint64_t need = r->totalPixels * (rgb ? 3 : r->imageBytes());
+    if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, the views need %llu",
+                                   (unsigned long long)bytes, (unsigned long long)need);
+    if (!r->copyStream) GSR_CUDA(cudaStreamCreateWithFlags(&r->copyStream, cudaStreamNonBlocking));
+    const size_t bpp = rgb ? 3 : r->imageBytes();
+    const unsigned char* src = rgb ? r->rgb8.as<unsigned char>() : r->image.as<unsigned char>();
+    if (r->lastSplit) {  // each view as soon as it is rasterized
+        for (size_t j = 0; j < r->parts.size(); ++j) {
+            const size_t off = size_t(r->parts[j].pixelOffset) * bpp, len = size_t(r->parts[j].pixels) * bpp;
+            GSR_CUDA(cudaStreamWaitEvent(r->copyStream, r->lastSlot->viewDone[j], 0));
+            GSR_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(host) + off, src + off, len, cudaMemcpyDeviceToHost,
+                                     r->copyStream));
+        }
+    } else {  // the frame's image once the frame is done
+        GSR_CUDA(cudaStreamWaitEvent(r->copyStream, r->lastSlot->done, 0));
+        GSR_CUDA(cudaMemcpyAsync(host, src, need, cudaMemcpyDeviceToHost, r->copyStream));
+    }
+    GSR_CUDA(cudaEventRecord(r->imageCopied, r->copyStream));
+    const uint64_t t = r->hostTickets++;
+    GSR_CUDA(cudaEventRecord(r->hostDone[t % GsrRenderer::kHostTickets], r->copyStream));
+    *ticket = t;
+    return GSR_OK;
+}
+
+int gsr_renderer_host_wait(GsrRenderer* r, uint64_t ticket) {
+    if (!r) return fail(GSR_ERROR_INVALID_ARGUMENT, "null renderer");
+    if (ticket >= r->hostTickets) return fail(GSR_ERROR_INVALID_ARGUMENT, "ticket %llu was not issued", (unsigned long long)ticket);
+    // a ticket older than the ring waits for a later one (copies complete in order)
+    GSR_CUDA(cudaEventSynchronize(r->hostDone[ticket % GsrRenderer::kHostTickets]));
+    return GSR_OK;
 }
 
 int gsr_renderer_view_layout(GsrRenderer* r, uint32_t view, GsrViewLayout* out, uint32_t* views) {

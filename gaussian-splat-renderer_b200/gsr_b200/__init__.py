@@ -234,6 +234,9 @@ def load(build_if_missing: bool = True) -> C.CDLL:
         "gsr_renderer_view_image": (C.c_int, [vp, u32, C.POINTER(vp), C.POINTER(vp)]),
         "gsr_read_view_image": (C.c_int, [vp, u32, vp, vp]),
         "gsr_render_views_to_host": (C.c_int, [vp, C.POINTER(SplatCamera), u32, vp, u64, vp]),
+        "gsr_render_views_to_host_async": (C.c_int, [vp, C.POINTER(SplatCamera), u32, vp, u64, vp,
+                                                     C.POINTER(C.c_uint64)]),
+        "gsr_renderer_host_wait": (C.c_int, [vp, C.c_uint64]),
         "gsr_color_model_options_default": (None, [C.POINTER(ColorModelOptions)]),
         "gsr_color_model_train": (C.c_int, [C.POINTER(SceneDesc), C.POINTER(ColorModelOptions), C.POINTER(vp)]),
         "gsr_color_model_stats": (C.c_int, [vp, C.POINTER(ColorModelStats)]),
@@ -528,6 +531,18 @@ class Renderer:
     def render_views_to_host(self, cameras, out: np.ndarray, stream: int = 0):
         cams = cameras if isinstance(cameras, C.Array) else camera_array(cameras)
         check(load().gsr_render_views_to_host(self._h, cams, len(cams), out.ctypes.data, out.nbytes, C.c_void_p(stream)))
+
+    def render_views_to_host_async(self, cameras, out: np.ndarray, stream: int = 0) -> int:
+        """Enqueues the frame and its copies into `out` (which must stay untouched until
+        host_wait of the returned ticket)."""
+        cams = cameras if isinstance(cameras, C.Array) else camera_array(cameras)
+        t = C.c_uint64()
+        check(load().gsr_render_views_to_host_async(self._h, cams, len(cams), out.ctypes.data, out.nbytes,
+                                                    C.c_void_p(stream), C.byref(t)))
+        return t.value
+
+    def host_wait(self, ticket: int):
+        check(load().gsr_renderer_host_wait(self._h, C.c_uint64(ticket)))
 
     def view_layouts(self) -> list:
         n = C.c_uint32()

@@ -484,6 +484,18 @@ int gsr_read_view_image(GsrRenderer* r, uint32_t view, float* rgba, uint8_t* rgb
  * the same. */
 int gsr_render_views_to_host(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* host, uint64_t bytes,
                              void* stream);
+/* The streaming form of gsr_render_views_to_host (no reference counterpart): returns once the
+ * frame and its copies are enqueued, with a ticket; the images are in `host` after
+ * gsr_renderer_host_wait(r, ticket). Until then `host` must stay allocated and untouched, so a
+ * caller alternates between (at least) two host buffers. The next frame's preprocess and sorts
+ * run while this frame's copies are in flight; its rasterization (that of any later frame) waits
+ * for them (with the per-tile schedule, each view is copied as soon as it is rasterized; with
+ * the persistent schedule the image is copied whole after the frame). The images are those of
+ * gsr_render_views_to_host. A layout change (other view sizes) waits for copies in flight. */
+int gsr_render_views_to_host_async(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* host,
+                                   uint64_t bytes, void* stream, uint64_t* ticket);
+/* Blocks until the copies of `ticket` (and of every earlier ticket) are in host memory. */
+int gsr_renderer_host_wait(GsrRenderer* r, uint64_t ticket);
 
 /* lastStats / collectPending (splat_tile_renderer.h:167-181): the control block of the most
  * recent frame whose readback has completed (frames_in_flight frames late, no stall).
