@@ -637,11 +637,32 @@ def render_issue(passes: dict, clocks: dict, instructions: float | None):
     achieved = instructions / (ms * 1e-3) / 1e12
     peak = 148 * 4 * mhz * 1e6 / 1e12
     return {"bound": "issue", "achieved": round(achieved, 4), "peak": round(peak, 4), "unit": "T warp-instr/s",
-            "frac": round(achieved / peak, 4), "instructions_source": "ncu smsp__inst_issued.sum of one frame"}
+            "frac": round(achieved / peak, 4), "instructions_source": "ncu smsp__inst_executed.sum of one frame"}
 
 
-# warp instructions of one plain 1080p render pass, from an ncu capture of this build
-RENDER_WARP_INSTRUCTIONS_1080P = 228.0e6
+# warp instructions (smsp__inst_executed.sum) of one 1080p view's render pass and preprocess,
+# from an ncu capture of this build (the plain profiling mode, two launches of each kernel)
+RENDER_WARP_INSTRUCTIONS_1080P = 227.6e6
+PREPROCESS_WARP_INSTRUCTIONS_1080P = 76.43e6
+
+
+def issue_roofline(passes: dict, clocks: dict, views: int) -> dict | None:
+    """The two issue-bound kernels of a frame of `views` 1080p views against the warp-issue peak
+    (148 SMs x 4 schedulers x the sampled SM clock): their per-view instruction counts times the
+    views over the pass times."""
+    mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz")
+    if not mhz:
+        return None
+    peak = 148 * 4 * mhz * 1e6 / 1e12
+    out = {"unit": "T warp-instr/s", "peak": round(peak, 4),
+           "instructions_source": "ncu smsp__inst_executed.sum of one 1080p view, times the views"}
+    for name, key, per_view in (("preprocess", "reset + preprocess (depth keys)", PREPROCESS_WARP_INSTRUCTIONS_1080P),
+                                ("render", "render tiles", RENDER_WARP_INSTRUCTIONS_1080P)):
+        ms = passes.get(key)
+        if ms:
+            achieved = per_view * views / (ms * 1e-3) / 1e12
+            out[name] = {"ms": ms, "achieved": round(achieved, 4), "frac": round(achieved / peak, 4)}
+    return out
 
 
 def settle_and_tune(G, gs, cams, args, model=None, depths=(1, 2, 4, 8, 16), tile_sizes=None, probe=32):
@@ -1084,6 +1105,8 @@ def run_b200(args, dist: Dist):
         line["speedup_vs_plain"] = round(head["views_per_s"] / plain["views_per_s"], 4)
         line["roofline"] = head_roof
         line["render_issue"] = render_issue(plain["passes_ms"], plain["clocks"], RENDER_WARP_INSTRUCTIONS_1080P)
+        hb = configs["plain_1080p"]["batched"]
+        line["issue"] = issue_roofline(hb.get("passes_ms", {}), hb["clocks"], hb["views_per_frame"])
         line["render_flops"] = plain.get("render_flops")
         line["parity"] = configs["plain_1080p"].get("parity")
     line["configs"] = configs

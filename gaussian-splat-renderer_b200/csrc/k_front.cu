@@ -775,7 +775,7 @@ cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capaci
 // kept gaussians go to decoded[view][g]. The rounding points are the in-preprocess decode's
 // (BF16 inputs, weights and hidden units, FP32 accumulation); the bias is added after the
 // products instead of seeding the accumulator, so colours can differ in the last bits of FP32.
-constexpr uint32_t kDecodeTcThreads = 128, kDecodeTcCols = 128;
+constexpr uint32_t kDecodeTcThreads = 128, kDecodeTcCols = 64;  // layer 1 and 3 at column 0, layer 2 at 32
 struct alignas(128) DecodeTcSmem {
     alignas(128) unsigned char a1[128 * 16 * 2];  // layer inputs, M = 128 rows, K-major no swizzle
     alignas(128) unsigned char a2[128 * 32 * 2];
@@ -787,9 +787,9 @@ struct alignas(128) DecodeTcSmem {
     uint64_t mbar;
     uint32_t tmem;
 };
-// 56 KB a block: at most 4 blocks per SM, so the blocks' TMEM (128 columns each) always fits
-// the SM's 512 columns and no allocation waits.
-constexpr uint32_t kDecodeTcSmem = 56 * 1024;
+// 28 KB a block: at most 8 blocks per SM, so the blocks' TMEM (64 columns each) always fits the
+// SM's 512 columns and no allocation waits.
+constexpr uint32_t kDecodeTcSmem = 28 * 1024;
 static_assert(sizeof(DecodeTcSmem) + 128 <= kDecodeTcSmem, "the decode's shared memory");
 
 // Eight floats as BF16 into one 16-byte row chunk of an operand.
@@ -846,27 +846,38 @@ __global__ void __launch_bounds__(kDecodeTcThreads) decodeColoursTcKernel(const 
         tc::fenceAfterSync();
         return true;
     };
+    // the inputs of a tile: its latent and position, loaded one tile ahead (while the current
+    // tile's products run)
+    auto fetch = [&](uint32_t tile, uint4& q, float4& pa) {
+        const uint32_t g = tile / a.viewCount * 128u + tid;
+        q = make_uint4(0, 0, 0, 0xFFFFFFFFu);  // a fallback marker: no colour
+        pa = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (tile < tiles && g < a.count) {
+            q = __ldg(&a.latents[g]);
+            if (!latentIsFallback(q)) pa = loadPosAlpha<GEOM>(a.scene, g);
+        }
+    };
+    uint4 qNext;
+    float4 paNext;
+    fetch(blockIdx.x, qNext, paNext);
     for (uint32_t tile = blockIdx.x; tile < tiles && !failed; tile += gridDim.x) {
         const uint32_t view = tile % a.viewCount, g = tile / a.viewCount * 128u + tid;
+        const uint4 q = qNext;
+        const float4 pa = paNext;
         float f[16];
 #pragma unroll
         for (int k = 0; k < 16; ++k) f[k] = 0.0f;
-        bool kept = false;
-        if (g < a.count) {
-            const uint4 q = __ldg(&a.latents[g]);
-            kept = !latentIsFallback(q);
-            if (kept) {
-                const uint32_t qw[4] = {q.x, q.y, q.z, q.w};
+        const bool kept = g < a.count && !latentIsFallback(q);
+        if (kept) {
+            const uint32_t qw[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-                for (int k = 0; k < kMlpLatent; ++k) f[k] = __half2float(__ushort_as_half(uint16_t(qw[k >> 1] >> (16 * (k & 1)))));
-                const float4 pa = loadPosAlpha<GEOM>(a.scene, g);
-                const float camPos[3] = {a.cam[view].pos[0], a.cam[view].pos[1], a.cam[view].pos[2]};
-                float dir[3];
-                viewDirection(pa, camPos, dir);
-                f[8] = dir[0];
-                f[9] = dir[1];
-                f[10] = dir[2];
-            }
+            for (int k = 0; k < kMlpLatent; ++k) f[k] = __half2float(__ushort_as_half(uint16_t(qw[k >> 1] >> (16 * (k & 1)))));
+            const float camPos[3] = {a.cam[view].pos[0], a.cam[view].pos[1], a.cam[view].pos[2]};
+            float dir[3];
+            viewDirection(pa, camPos, dir);
+            f[8] = dir[0];
+            f[9] = dir[1];
+            f[10] = dir[2];
         }
         storeRowChunk(S.a1, tc::operandOffset(tid, 0, 16), f);
         storeRowChunk(S.a1, tc::operandOffset(tid, 8, 16), f + 8);
@@ -879,6 +890,7 @@ __global__ void __launch_bounds__(kDecodeTcThreads) decodeColoursTcKernel(const 
                     false);
             tc::commit(&S.mbar);
         }
+        fetch(tile + gridDim.x, qNext, paNext);
         if (!layerDone()) break;
         uint32_t acc[32];
         tc::ld32(tmem + lane0, acc);
@@ -916,13 +928,13 @@ __global__ void __launch_bounds__(kDecodeTcThreads) decodeColoursTcKernel(const 
         if (tid == 0) {
             tc::fenceAfterSync();
             for (uint32_t ks = 0; ks < 2; ++ks)
-                tc::mma(tmem + 64, tc::operandDescriptor(a3, ks, 32), tc::operandDescriptor(b3, ks, 32),
+                tc::mma(tmem, tc::operandDescriptor(a3, ks, 32), tc::operandDescriptor(b3, ks, 32),  // layer 1 read back
                         tc::instrDescriptorBf16(128, 16), ks > 0);
             tc::commit(&S.mbar);
         }
         if (!layerDone()) break;
         uint32_t out[16];
-        tc::ld16(tmem + lane0 + 64, out);
+        tc::ld16(tmem + lane0, out);
         tc::waitLd();
         if (kept)
             a.decoded[size_t(view) * a.count + g] =
@@ -1043,7 +1055,7 @@ cudaError_t launchDecodeTcT(const FrontArgs& a, cudaStream_t s) {
         int dev = 0, sms = 148, perSm = 4;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, decodeColoursTcKernel<GEOM>, kDecodeTcThreads, kDecodeTcSmem);
-        grid = sms * (perSm > 0 ? (perSm < 4 ? perSm : 4) : 1);
+        grid = sms * (perSm > 0 ? (perSm < 8 ? perSm : 8) : 1);
     }
     const uint32_t tiles = (a.count + 127u) / 128u * a.viewCount;
     const uint32_t blocks = tiles < uint32_t(grid) ? tiles : uint32_t(grid);
