@@ -105,6 +105,7 @@ uint32_t roundUpToBlock(uint64_t n) {
 struct DeviceTables {
     uint32_t* entries = nullptr;
     uint32_t* buckets = nullptr;
+    uint32_t* groups = nullptr;
 };
 std::mutex g_tablesMutex;
 DeviceTables g_tables[64];
@@ -121,9 +122,18 @@ int deviceTables(LogfFixups* out) {
         GSR_CUDA(cudaMalloc(&t.buckets, bb));
         GSR_CUDA(cudaMemcpy(t.entries, gsr_logf_fixups, eb, cudaMemcpyHostToDevice));
         GSR_CUDA(cudaMemcpy(t.buckets, gsr_logf_bucket_start, bb, cudaMemcpyHostToDevice));
+        // one bit per 32 consecutive inputs that hold a fixup, a word per bucket
+        std::vector<uint32_t> groups(gsr_logf_bucket_count, 0u);
+        for (uint32_t k = 0; k < gsr_logf_fixup_count; ++k) {
+            const uint32_t off = gsr_logf_fixups[k] >> 1;
+            groups[off >> 10] |= 1u << ((off >> 5) & 31u);
+        }
+        GSR_CUDA(cudaMalloc(&t.groups, bb));
+        GSR_CUDA(cudaMemcpy(t.groups, groups.data(), bb, cudaMemcpyHostToDevice));
     }
     out->entries = t.entries;
     out->bucketStart = t.buckets;
+    out->groups = t.groups;
     out->base = gsr_logf_fixup_base;
     out->last = gsr_logf_fixup_last;
     out->count = gsr_logf_fixup_count;
