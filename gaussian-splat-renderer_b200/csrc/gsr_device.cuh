@@ -134,7 +134,7 @@ __device__ __forceinline__ float libcLogf(float x, const LogfFixups& t) {
     if (xb < t.base || xb > t.last) return r;
     const uint32_t off = xb - t.base;
     const uint32_t b = off >> 10;
-    if (!((__ldg(&t.groups[b]) >> ((off >> 5) & 31u)) & 1u)) return r;  // no fixup among its 32 neighbours
+    if (!((__ldg(&t.groups[off >> 8]) >> ((off >> 3) & 31u)) & 1u)) return r;  // none among its 8 neighbours
     uint32_t lo = __ldg(&t.bucketStart[b]), hi = __ldg(&t.bucketStart[b + 1]);
     while (lo < hi) {  // lower bound of off in entries[lo, hi)
         const uint32_t mid = (lo + hi) >> 1;

@@ -56,8 +56,8 @@ static_assert(kStaticScanScratchBytes == 66048, "the size the header states");
 struct LogfFixups {
     const uint32_t* entries;       // ((x_bits - base) << 1) | up, sorted
     const uint32_t* bucketStart;   // per 1024-input bucket
-    const uint32_t* groups;        // per 1024-input bucket one word: bit g = inputs [32 g, 32 g + 32)
-                                   // of the bucket hold a fixup (most inputs are answered by it)
+    const uint32_t* groups;        // one bit per 8 consecutive inputs (word = off >> 8, bit = (off >> 3) & 31):
+                                   // set when one of them holds a fixup (most inputs are answered by it)
     uint32_t base, last, count;
 };
 

@@ -122,14 +122,14 @@ int deviceTables(LogfFixups* out) {
         GSR_CUDA(cudaMalloc(&t.buckets, bb));
         GSR_CUDA(cudaMemcpy(t.entries, gsr_logf_fixups, eb, cudaMemcpyHostToDevice));
         GSR_CUDA(cudaMemcpy(t.buckets, gsr_logf_bucket_start, bb, cudaMemcpyHostToDevice));
-        // one bit per 32 consecutive inputs that hold a fixup, a word per bucket
-        std::vector<uint32_t> groups(gsr_logf_bucket_count, 0u);
+        // one bit per 8 consecutive inputs, set when one of them holds a fixup (1 MB)
+        std::vector<uint32_t> groups(size_t(gsr_logf_bucket_count) * 4, 0u);
         for (uint32_t k = 0; k < gsr_logf_fixup_count; ++k) {
             const uint32_t off = gsr_logf_fixups[k] >> 1;
-            groups[off >> 10] |= 1u << ((off >> 5) & 31u);
+            groups[off >> 8] |= 1u << ((off >> 3) & 31u);
         }
-        GSR_CUDA(cudaMalloc(&t.groups, bb));
-        GSR_CUDA(cudaMemcpy(t.groups, groups.data(), bb, cudaMemcpyHostToDevice));
+        GSR_CUDA(cudaMalloc(&t.groups, groups.size() * 4));
+        GSR_CUDA(cudaMemcpy(t.groups, groups.data(), groups.size() * 4, cudaMemcpyHostToDevice));
     }
     out->entries = t.entries;
     out->bucketStart = t.buckets;
