@@ -852,7 +852,9 @@ struct GsrRenderer {
         static_assert(sizeof(DevCameraArgs) == sizeof(GsrSplatCamera), "camera layout");
         std::memcpy(slot.camHost, cams, sizeof(GsrSplatCamera) * v);
         // view by view: several per-tile views with their images wanted on the host
-        const bool split = hostCopies && (v > 1 || hostAsync) && !persistentRaster(v);
+        // (the streaming call rasterizes the frame whole: its copies overlap the next frame's
+        // front, so they need not start view by view)
+        const bool split = hostCopies && v > 1 && !hostAsync && !persistentRaster(v);
         if (split) planParts();
         while (split && slot.viewDone.size() < parts.size()) {
             cudaEvent_t e = nullptr;

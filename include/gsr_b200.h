@@ -489,9 +489,9 @@ int gsr_render_views_to_host(GsrRenderer* r, const GsrSplatCamera* cameras, uint
  * gsr_renderer_host_wait(r, ticket). Until then `host` must stay allocated and untouched, so a
  * caller alternates between (at least) two host buffers. The next frame's preprocess and sorts
  * run while this frame's copies are in flight; its rasterization (that of any later frame) waits
- * for them (with the per-tile schedule, each view is copied as soon as it is rasterized; with
- * the persistent schedule the image is copied whole after the frame). The images are those of
- * gsr_render_views_to_host. A layout change (other view sizes) waits for copies in flight. */
+ * for them. The frame is rasterized in one launch and its image copied whole after it (the
+ * copies overlap the next frame's front, not this frame's rasterization). The images are those
+ * of gsr_render_views_to_host. A layout change (other view sizes) waits for copies in flight. */
 int gsr_render_views_to_host_async(GsrRenderer* r, const GsrSplatCamera* cameras, uint32_t views, void* host,
                                    uint64_t bytes, void* stream, uint64_t* ticket);
 /* Blocks until the copies of `ticket` (and of every earlier ticket) are in host memory. */
