@@ -27,11 +27,10 @@ value        views/s over all ranks, scene and cameras resident on the device: C
              the launching stream around the K steps (barrier + synchronize on both sides, the
              max over ranks).
 e2e          the same views through the calls a host application makes: cameras from host
-             memory, every view's RGB8 image copied into pinned host memory. Single views:
-             gsr_render_to_host, synchronized every call. Batched frames: the streaming call
-             gsr_render_views_to_host_async into two alternating pinned buffers, each frame's
-             copies waited for after the next frame is enqueued; the clock stops after the last
-             frame's images are in host memory.
+             memory, every view's RGB8 image copied into pinned host memory, through the
+             streaming call gsr_render_views_to_host_async (one camera a frame for single views)
+             into two alternating pinned buffers, each frame's copies waited for after the next
+             frame is enqueued; the clock stops after the last frame's images are in host memory.
 parity       per workload (the CPU leg, rank 0), one view (or one per resolution): the list
              (keys, values, tile ranges) bit for bit against the oracle's construction, the
              float image's PSNR and the 8-bit image's PSNR and largest difference against the
@@ -453,6 +452,8 @@ class Frames:
         if views_per_frame == 1:
             self.calls = [G.to_c_camera(cams[v]) for v in order]
             self.sizes = [[(cams[v].width, cams[v].height)] for v in order]
+            # the same views as one-camera frames, for the streaming end-to-end call
+            self.stream_calls = [G.camera_array([cams[v]]) for v in order]
         else:
             self.calls, self.sizes = [], []
             for k in range(0, len(order), views_per_frame):
@@ -471,15 +472,13 @@ def render_call(r, frames: Frames, k: int, stream: int):
 
 
 def to_host_call(r, frames: Frames, k: int, host: dict, stream: int, pending: list):
-    """One end-to-end call. Single views: gsr_render_to_host (synchronous). Batched frames: the
-    streaming form, gsr_render_views_to_host_async into one of two pinned buffers, then a wait
-    for the previous frame's ticket (so frame k's copies overlap frame k + 1's preprocess and
-    sorts); `pending` holds the ticket still outstanding."""
-    call = frames.calls[k % len(frames.calls)]
+    """One end-to-end call: the streaming form, gsr_render_views_to_host_async (one camera a
+    frame for single views) into one of two pinned buffers, then a wait for the previous frame's
+    ticket (so frame k's copies overlap frame k + 1's preprocess and sorts); `pending` holds the
+    ticket still outstanding."""
+    calls = frames.stream_calls if frames.d == 1 else frames.calls
+    call = calls[k % len(calls)]
     px = sum(w * h for w, h in frames.sizes[k % len(frames.sizes)])
-    if frames.d == 1:
-        r.render_to_host(call, host[px][0], stream)
-        return
     ticket = r.render_views_to_host_async(call, host[px][k % 2], stream)
     if pending:
         r.host_wait(pending.pop())
@@ -558,12 +557,11 @@ def time_form(r, frames: Frames, args, dist: Dist, sampler: Sampler, stream_obj)
             "views_per_s": round(views_all / (ms / 1e3), 3), "e2e_views_per_s": round(views_all / (e2e_ms / 1e3), 3),
             "ms_per_view": round(ms / views, 4), "ms_per_step": round(ms / args.steps, 3),
             "e2e_ms_per_step": round(e2e_ms / args.steps, 3),
-            "e2e_call": "gsr_render_to_host (synchronous)" if frames.d == 1 else
-                        "gsr_render_views_to_host_async, two pinned buffers, one frame in flight",
+            "e2e_call": "gsr_render_views_to_host_async, two pinned buffers, one frame in flight",
             "gpu_launches": int(launches),
             "list_resizes_timed": int(resizes),
-            # GsrCamera (200 B) per one-view call, GsrSplatCamera (108 B) per view of a batched call
-            "h2d_bytes_per_step": int(frames.views_per_step * (200 if frames.d == 1 else 108)),
+            # a GsrSplatCamera (108 B) per view
+            "h2d_bytes_per_step": int(frames.views_per_step * 108),
             "d2h_bytes_per_step": int(d2h),
             "clocks": clocks}
 

@@ -18,7 +18,8 @@ def _frames():
     sizes = [(640, 360), (320, 240), (500, 300), (256, 256)]
     frames = []
     for k, a in enumerate(np.linspace(0.0, 2.0, 6)):
-        sz = sizes if k != 3 else [(400, 200), (640, 360)]  # one frame of another layout
+        # one frame of another layout, one of a single view
+        sz = [(400, 200), (640, 360)] if k == 3 else [(640, 360)] if k == 5 else sizes
         frames.append([scenes.viewer_camera((6.0 * np.sin(a + j), 0.4, 6.0 * np.cos(a + j)), (0.0, 0.0, 0.0), w, h)
                        for j, (w, h) in enumerate(sz)])
     return frames
