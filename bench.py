@@ -607,19 +607,21 @@ def render_flops(G, gs, args, frames: Frames, stream_obj, passes: dict, clocks: 
     (FMA) at the SM clock sampled under load (nominal, not measured)."""
     r = G.Renderer(gs, G.Settings(bounds="tight", adaptive_list=True, rgb8=True, budget_mb=args.budget_mb,
                                   tile_stats=True))
-    ev = te = 0
+    ev = te = slots = 0
     for k in range(n):
         render_call(r, frames, k, stream_obj.cuda_stream)
         stream_obj.synchronize()
         st, tested = r.read_tile_stats()
         ev += int(st[:, 2].sum())
+        slots += int(st[:, 5].sum())
         te += int(tested)
     r.close()
     ms = passes.get("render tiles")
     mhz = (clocks or {}).get("sm_mhz") or 1965.0
     peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
-    ev, te = ev / n, te / n
+    ev, te, slots = ev / n, te / n, slots / n
     return {"bound": "fp32", "flops_per_pair": 20, "evaluated_pairs": int(ev), "tested_pairs": int(te),
+            "lane_slots": int(slots), "lanes_testing": round(te / slots, 4) if slots else None,
             "algorithmic_tflops": round(20 * ev / (ms * 1e-3) / 1e12, 3),
             "kernel_tflops": round(20 * te / (ms * 1e-3) / 1e12, 3), "peak_tflops": round(peak, 2),
             "frac_algorithmic": round(20 * ev / (ms * 1e-3) / 1e12 / peak, 4),
