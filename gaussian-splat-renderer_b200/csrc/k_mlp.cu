@@ -6,7 +6,7 @@
 // point on the sphere from a hash of (g, j), the same in training and in the gate. A training
 // step draws `batch` pairs from a hash of (seed, step, k), so the run is reproducible bit for bit.
 //
-//   trainStep   on the tensor cores: a 128-thread block takes 512 samples in chunks of 64, each
+//   trainStep   on the tensor cores: a 128-thread block takes 256 samples in chunks of 64, each
 //               warp 16 of them. Forward (BF16 weights and activations, FP32 accumulation, the
 //               latent rounded to fp16 then BF16 as the tensor-core decode sees it), loss and
 //               backward (straight through the roundings) are mma.sync.m16n8k16 products whose
@@ -26,10 +26,10 @@ namespace gsr {
 
 namespace {
 
-// The tensor-core training step: blocks of 4 warps, chunks of 64 samples (16 per warp), 8
-// chunks (512 samples) a block. Row strides of the shared-memory matrices are K + 8 BF16 so
+// The tensor-core training step: blocks of 4 warps, chunks of 64 samples (16 per warp), 4
+// chunks (256 samples) a block. Row strides of the shared-memory matrices are K + 8 BF16 so
 // that the 8 rows an ldmatrix reads fall into distinct banks.
-constexpr int kTcWarps = 4, kTcThreads = kTcWarps * 32, kTcChunk = kTcWarps * 16, kTcChunks = 8;
+constexpr int kTcWarps = 4, kTcThreads = kTcWarps * 32, kTcChunk = kTcWarps * 16, kTcChunks = 4;
 constexpr int kTcBlockSamples = kTcChunk * kTcChunks;
 constexpr int S48 = kEncIn + 8, S64 = kEncHidden + 8, S32 = kMlpHidden + 8, S16 = 16 + 8;
 

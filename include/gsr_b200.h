@@ -349,7 +349,7 @@ int gsr_renderer_view_image(GsrRenderer* r, uint32_t view, const void** rgba, co
 typedef struct GsrColorModel GsrColorModel;
 typedef struct GsrColorModelOptions {
     uint32_t directions;   /* view directions per gaussian (uniform on the sphere); default 64 */
-    uint32_t batch;        /* (gaussian, direction) pairs per step, a multiple of 512; default 65536 */
+    uint32_t batch;        /* (gaussian, direction) pairs per step, a multiple of 256; default 65536 */
     uint32_t steps;        /* Adam steps; default 2000 */
     float learning_rate;   /* default 1e-3 (beta1 0.9, beta2 0.999, eps 1e-8) */
     uint32_t seed;         /* initial weights and the pair draws; default 1 */
