@@ -1630,19 +1630,10 @@ int gsr_render_views_to_host_async(GsrRenderer* r, const GsrSplatCamera* cameras
     if (bytes != need) return fail(GSR_ERROR_INVALID_ARGUMENT, "host buffer %llu bytes, the views need %llu",
                                    (unsigned long long)bytes, (unsigned long long)need);
     if (!r->copyStream) GSR_CUDA(cudaStreamCreateWithFlags(&r->copyStream, cudaStreamNonBlocking));
-    const size_t bpp = rgb ? 3 : r->imageBytes();
     const unsigned char* src = rgb ? r->rgb8.as<unsigned char>() : r->image.as<unsigned char>();
-    if (r->lastSplit) {  // each view as soon as it is rasterized
-        for (size_t j = 0; j < r->parts.size(); ++j) {
-            const size_t off = size_t(r->parts[j].pixelOffset) * bpp, len = size_t(r->parts[j].pixels) * bpp;
-            GSR_CUDA(cudaStreamWaitEvent(r->copyStream, r->lastSlot->viewDone[j], 0));
-            GSR_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(host) + off, src + off, len, cudaMemcpyDeviceToHost,
-                                     r->copyStream));
-        }
-    } else {  // the frame's image once the frame is done
-        GSR_CUDA(cudaStreamWaitEvent(r->copyStream, r->lastSlot->done, 0));
-        GSR_CUDA(cudaMemcpyAsync(host, src, need, cudaMemcpyDeviceToHost, r->copyStream));
-    }
+    // the frame was rasterized whole (no view-by-view split): its image once the frame is done
+    GSR_CUDA(cudaStreamWaitEvent(r->copyStream, r->lastSlot->done, 0));
+    GSR_CUDA(cudaMemcpyAsync(host, src, need, cudaMemcpyDeviceToHost, r->copyStream));
     GSR_CUDA(cudaEventRecord(r->imageCopied, r->copyStream));
     const uint64_t t = r->hostTickets++;
     GSR_CUDA(cudaEventRecord(r->hostDone[t % GsrRenderer::kHostTickets], r->copyStream));
