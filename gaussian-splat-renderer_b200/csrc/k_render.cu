@@ -1,14 +1,15 @@
 // The tile rasterizer (INRIA renderCUDA; the reference's shaders/tile_render.comp:281-400 and
 // the CPU reference's per-pixel loop, src/splat/reference_renderer.cpp:120-222).
 //
-// One 256-thread block per 16x16 tile, one thread per pixel; warp w owns pixel rows 2w, 2w+1.
+// One 256-thread block per 16x16 tile, one thread per pixel; warp w owns an 8 x 4 pixel block.
 // The tile's entries [ranges[tile].x, ranges[tile].y) are walked front to back in batches of
 // 256 records, double-buffered: while batch b is blended, the records of batch b+1 are gathered
 // into shared memory with cp.async (16-byte LDGSTS, the record of gaussian values[j]). Each
-// entry is then prepared once per block: the conic pre-scaled by -log2(e)/2 so that
-//   alpha = min(0.99, o * 2^(a' dx^2 + b' dx dy + c' dy^2))   ( = o * exp(power) )
-// costs one MUFU.EX2, and the axis-aligned box of its alpha >= 1/255 cutoff ellipse (the
-// reference's threshold with a wider margin, tile_coverage.cpp:24-50) so that a warp skips a
+// entry is then prepared once per block: its power, in base 2 and with log2(opacity) added,
+// expanded as a quadratic in the pixel's offset from a fixed cell origin (powerAt), so that
+//   alpha = min(0.99, 2^p) = min(0.99, o * exp(power))
+// costs five FMAs and one MUFU.EX2, and the warp strips its alpha >= 1/255 cutoff ellipse (the
+// reference's threshold with a wider margin, tile_coverage.cpp:24-50) meets, so that a warp skips a
 // splat that cannot reach any of its 32 pixels (every skipped pair has alpha < 1/255, which the
 // loop would skip anyway). Per pair, INRIA's test-before-accept rule:
 //   skip power > 0; skip alpha < 1/255; testT = T (1 - alpha); testT < 1e-4 -> done;
@@ -22,9 +23,10 @@
 // take the next tile from a queue counter until every tile of every view is done, which keeps
 // the SMs busy across views of uneven size.
 //
-// FMA contraction and the hardware exp2 make the float image differ from the CPU reference's
-// in the last bits (and, for pairs within an ulp of the 1/255 or 1e-4 thresholds, by one such
-// pair's contribution); tests bound it: float PSNR > 60 dB and the 8-bit image within 1/255.
+// The expanded power, FMA contraction and the hardware exp2 and log2 make the float image differ
+// from the CPU reference's in the last bits (and, for pairs within rounding of the 1/255 or 1e-4
+// thresholds, by one such pair's contribution); tests bound it: float PSNR > 60 dB and the 8-bit
+// image within 1/255. The image does not depend on the tile shape, the schedule or the gather.
 #include <cuda.h>  // CUtensorMap (the type only; maps are encoded by the host)
 
 #include "gsr_device.cuh"
@@ -146,12 +148,25 @@ struct StageArea<N, kGatherTma> {
 template <int N, int GATHER = kGatherCpAsync>
 struct RenderShared {
     StageArea<N, GATHER> st;
-    float4 conic[N];      // a', b', c' (pre-scaled), opacity
+    float4 power0[N];     // qa, qb, qc, d of the expanded power (powerAt)
+    float4 power1[N];     // e, f, the sign-test bound, -
     uint32_t strips[N];   // the warp strips the cutoff ellipse meets (stripMask)
     float4 color[N];      // r, g, b, -
-    float2 center[N];
     uint32_t tile;        // persistent schedule: the block's current tile
 };
+
+// The exponent of alpha in base 2, log2(o) + log2(e) * power, at pixel offset (X, Y) from the
+// origin of the 32 x 16 pixel cell that holds the tile (the same origin for every tile shape,
+// so the image does not depend on it). With qa, qb, qc the conic scaled by -log2(e)/2, -log2(e),
+// -log2(e)/2 and (cx, cy) the centre relative to the cell,
+//   qa (cx-X)^2 + qb (cx-X)(cy-Y) + qc (cy-Y)^2 + log2(o) = X (qa X + qb Y + d) + Y (qc Y + e) + f
+// with d = -(2 qa cx + qb cy), e = -(2 qc cy + qb cx), f = the left side at (0, 0): five FMAs a
+// pair and o folded in. The power > 0 test reads p > log2(o); for a positive definite conic the
+// power is never positive and the bound is +inf (the expanded sum's rounding near the centre
+// must not drop the splat there).
+__device__ __forceinline__ float powerAt(const float4& u, const float4& w, float X, float Y) {
+    return fmaf(X, fmaf(u.x, X, fmaf(u.y, Y, u.w)), fmaf(Y, fmaf(u.z, Y, w.x), w.y));
+}
 
 __device__ __forceinline__ uint32_t smemAddr(const void* p) { return uint32_t(__cvta_generic_to_shared(p)); }
 
@@ -336,6 +351,9 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
     const uint2* records24 = reinterpret_cast<const uint2*>(a.packed) + size_t(view) * a.count * 3;
     constexpr int mode = MODE;
     const float fx = float(px), fy = float(py);
+    // the pixel relative to its 32 x 16 cell (exact small integers)
+    const uint32_t cellX = (tx * kTW) & ~31u, cellY = (ty * kTH) & ~15u;
+    const float X = float(px - cellX), Y = float(py - cellY);
     // this warp's pixel strip
     float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
     bool done = !inside;
@@ -509,9 +527,16 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
             if constexpr (TILE == 32)
                 if (a.bounds != kBoundsCutoff || !ellipse) strips &= rectStrips32(r0.x, radius, tx * kTW);
             sm.strips[tid] = strips;
-            sm.conic[tid] = make_float4(-0.5f * kLog2e * A, -kLog2e * B, -0.5f * kLog2e * C, o);
+            // the expanded power about the cell origin (powerAt); only a record with strips is
+            // visited, so its opacity is at least 1/255 and log2(o) finite
+            const float qa = -0.5f * kLog2e * A, qb = -kLog2e * B, qc = -0.5f * kLog2e * C;
+            const float lg = __log2f(o);
+            const float cx = r0.x - float(cellX), cy = r0.y - float(cellY);
+            const float d = -fmaf(2.0f * qa, cx, qb * cy), e = -fmaf(2.0f * qc, cy, qb * cx);
+            const float f = fmaf(cx, fmaf(qa, cx, qb * cy), fmaf(cy, qc * cy, lg));
+            sm.power0[tid] = make_float4(qa, qb, qc, d);
+            sm.power1[tid] = make_float4(e, f, ellipse ? __int_as_float(0x7f800000) : lg, 0.0f);
             sm.color[tid] = r2;
-            sm.center[tid] = make_float2(r0.x, r0.y);
         }
         __syncthreads();
         const uint32_t n = range.y - start < kThreads ? range.y - start : kThreads;
@@ -526,14 +551,11 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
                     ++stIters;
                     stTested += done ? 0u : 1u;
                 }
-                const float2 c = sm.center[q];
-                const float4 co = sm.conic[q];
-                const float dx = c.x - fx;
-                const float dy = c.y - fy;
-                const float power2 = co.x * dx * dx + co.z * dy * dy + co.y * dx * dy;
-                const float alpha = fminf(kMaxAlpha, co.w * fastExp2(power2));
+                const float4 pw0 = sm.power0[q], pw1 = sm.power1[q];
+                const float p = powerAt(pw0, pw1, X, Y);
+                const float alpha = fminf(kMaxAlpha, fastExp2(p));
                 // skipped: a finished pixel, power > 0, alpha below 1/255 (one predicate)
-                if (done || power2 > 0.0f || alpha < (1.0f / 255.0f)) continue;
+                if (done || p > pw1.z || alpha < (1.0f / 255.0f)) continue;
                 if constexpr (CAP > 0) {
                     // the depth of the gaussian's maximum along the pixel ray: (v . b) / (v^T P v)
                     const float4 pa = ray[buf][0][q], pb = ray[buf][1][q];
