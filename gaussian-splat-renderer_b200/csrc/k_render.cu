@@ -6,7 +6,7 @@
 // 256 records, double-buffered: while batch b is blended, the records of batch b+1 are gathered
 // into shared memory with cp.async (16-byte LDGSTS, the record of gaussian values[j]). Each
 // entry is then prepared once per block: its power, in base 2 and with log2(opacity) added,
-// expanded as a quadratic in the pixel's offset from a fixed cell origin (powerAt), so that
+// expanded as a quadratic in the pixel's offset from the centre of its 32 x 16 cell (powerAt), so that
 //   alpha = min(0.99, 2^p) = min(0.99, o * exp(power))
 // costs five FMAs and one MUFU.EX2, and the warp strips its alpha >= 1/255 cutoff ellipse (the
 // reference's threshold with a wider margin, tile_coverage.cpp:24-50) meets, so that a warp skips a
@@ -156,7 +156,7 @@ struct RenderShared {
 };
 
 // The exponent of alpha in base 2, log2(o) + log2(e) * power, at pixel offset (X, Y) from the
-// origin of the 32 x 16 pixel cell that holds the tile (the same origin for every tile shape,
+// centre of the 32 x 16 pixel cell that holds the tile (the same origin for every tile shape,
 // so the image does not depend on it). With qa, qb, qc the conic scaled by -log2(e)/2, -log2(e),
 // -log2(e)/2 and (cx, cy) the centre relative to the cell,
 //   qa (cx-X)^2 + qb (cx-X)(cy-Y) + qc (cy-Y)^2 + log2(o) = X (qa X + qb Y + d) + Y (qc Y + e) + f
@@ -351,9 +351,9 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
     const uint2* records24 = reinterpret_cast<const uint2*>(a.packed) + size_t(view) * a.count * 3;
     constexpr int mode = MODE;
     const float fx = float(px), fy = float(py);
-    // the pixel relative to its 32 x 16 cell (exact small integers)
-    const uint32_t cellX = (tx * kTW) & ~31u, cellY = (ty * kTH) & ~15u;
-    const float X = float(px - cellX), Y = float(py - cellY);
+    // the pixel relative to the centre of its 32 x 16 cell (exact small integers, -16..15 and
+    // -8..7: the expansion's terms stay small against the power it sums to)
+    const float X = float(int(px) - int((tx * kTW) & ~31u) - 16), Y = float(int(py) - int((ty * kTH) & ~15u) - 8);
     // this warp's pixel strip
     float T = 1.0f, c0 = 0.0f, c1 = 0.0f, c2 = 0.0f;
     bool done = !inside;
@@ -444,27 +444,21 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
     uint32_t stEval = 0, stBlend = 0, stIters = 0, stFetched = 0, stTested = 0;
     bool stTerm = false;
 
+    // Two block barriers a batch: the vote, which also publishes the batch's gathered records (each
+    // thread has waited for its own copies) and orders the previous batch's reads of the staging
+    // buffer and of the prepared arrays before this batch overwrites them; and the end of the
+    // preparation. Every batch issued is waited for at the top of the next iteration, which
+    // always runs, so none is in flight after the loop.
     int buf = 0;
-    bool inFlight = false;  // TMA: the batch at `start` was issued and not yet waited for
-    if (range.x < range.y) {
-        issue(range.x, 0);
-        inFlight = true;
-    }
+    if (range.x < range.y) issue(range.x, 0);
     for (uint32_t start = range.x; start < range.y; start += kThreads, buf ^= 1) {
+        if constexpr (GATHER == kGatherTma) waitTma(buf);
+        else cpAsyncWait<0>();
         if (__syncthreads_count(done) == int(kThreads)) break;
         if constexpr (STATS) stFetched += range.y - start < kThreads ? range.y - start : kThreads;
-        // prefetch the next batch while this one is prepared and blended
+        // the next batch is gathered while this one is prepared and blended
         const uint32_t next = start + kThreads;
-        if constexpr (GATHER == kGatherTma) {
-            if (next < range.y) issue(next, buf ^ 1);
-            waitTma(buf);
-            inFlight = next < range.y;
-        } else {
-            if (next < range.y) issue(next, buf ^ 1);
-            else cpAsyncCommit();
-            cpAsyncWait<1>();
-        }
-        __syncthreads();
+        if (next < range.y) issue(next, buf ^ 1);
         if (start + tid < range.y) {
             float2 r0;  // cx, cy
             float A, B, C, o;
@@ -531,7 +525,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
             // visited, so its opacity is at least 1/255 and log2(o) finite
             const float qa = -0.5f * kLog2e * A, qb = -kLog2e * B, qc = -0.5f * kLog2e * C;
             const float lg = __log2f(o);
-            const float cx = r0.x - float(cellX), cy = r0.y - float(cellY);
+            const float cx = r0.x - (float(px) - X), cy = r0.y - (float(py) - Y);  // the cell centre: exact
             const float d = -fmaf(2.0f * qa, cx, qb * cy), e = -fmaf(2.0f * qc, cy, qb * cx);
             const float f = fmaf(cx, fmaf(qa, cx, qb * cy), fmaf(cy, qc * cy, lg));
             sm.power0[tid] = make_float4(qa, qb, qc, d);
@@ -591,9 +585,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
             if (!done && uint32_t(i) < window.count) blendOver(window.al[i], window.r[i], window.g[i], window.b[i], T, c0, c1, c2, done);
     }
     if constexpr (GATHER == kGatherTma) {
-        // a tile that ended early still has its next batch in flight: it lands before the
-        // buffers are reused (or the block exits); the phases are kept for the next tile
-        if (inFlight) waitTma(buf);
+        // no batch is in flight here (see the loop); the phases are kept for the next tile
         __syncthreads();
         if (tid == 0) {
             sm.st.uses[0] = phase0;
