@@ -478,8 +478,9 @@ __global__ void __launch_bounds__(kFrontThreads, 4) preprocessKernel(const __gri
             dmin = dmax = __float_as_uint(s.depth);  // positive: the bits order like the values
         }
         a.tileCounts[rec] = count;
-        // binning mode: the record's depth word, depth bits above the record index; records that
-        // emit no tile get all-ones depth bits and sort after every real depth (positive floats).
+        // binning mode: the record's depth word, depth bits above the record index (positive
+        // floats: the bits order like the depths); records that emit no tile get all-ones depth
+        // bits (the sort places them anywhere: they add no entry).
         // Frames of several views put the view above the depth bits: the depth sort then orders
         // by (view, depth, record), so the emission walks one view's records at a time (each
         // tile's entries come from one view, so the list is the same)

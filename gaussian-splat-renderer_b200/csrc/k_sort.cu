@@ -39,12 +39,17 @@ __device__ __forceinline__ uint64_t virtualKey(uint64_t key, uint32_t lowBits, u
 
 __device__ __forceinline__ uint64_t maskOf(uint32_t bits) { return bits >= 64 ? ~0ull : ((1ull << bits) - 1ull); }
 
-// The depth sort's key of a depth word: the varying depth bits (and the sentinel bit) above the
-// record index, with the view (the word's field at viewShift, when there is one) right above
-// them, so that (view, depth) costs no digit pass on the depth bits every real depth shares.
+// The depth sort's key of a depth word: its depth bits (above the record index) minus the
+// frame's smallest visible depth bits, in depthBits = bit_width(max - min) bits, with the view
+// (the word's field at viewShift, when there is one) right above them. Positive floats order like
+// their bits, so the offsets of the visible records order like their depths, and (view, depth)
+// costs no digit pass on the bits every real depth shares. (Offsets span fewer bits than the
+// bits where min and max differ: 24 against 25 for depths in [6, 22], one pass less at 8-bit
+// digits.) A record without tiles (all-ones depth bits) gets some key in the range: it emits no
+// entry, so where it sorts changes no offset and no list.
 __device__ __forceinline__ uint64_t depthVirtualKey(uint64_t word, uint32_t indexBits, uint32_t depthBits,
-                                                    uint32_t viewShift) {
-    const uint64_t depth = (word >> indexBits) & maskOf(depthBits);
+                                                    uint32_t depthMin, uint32_t viewShift) {
+    const uint64_t depth = uint64_t(uint32_t(word >> indexBits) - depthMin) & maskOf(depthBits);
     return viewShift ? ((word >> viewShift) << depthBits) | depth : depth;
 }
 
@@ -116,19 +121,20 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     __shared__ uint32_t sAny;
     DeviceControl* ctl = a.ctl;
     const uint32_t entries = a.frameMode == 2 ? a.count : ctl->c.entries;
-    uint32_t lowBits, keyBits, packed = 0, indexBits = 0, depthBits = 0, viewShift = 0;
+    uint32_t lowBits, keyBits, packed = 0, indexBits = 0, depthBits = 0, depthMin = 0, viewShift = 0;
     if (a.frameMode == 1) {
         const KeyLayout lay = keyLayout(ctl, a.tileCount, a.count, a.binning != 0);
         lowBits = lay.lowBits;
         packed = lay.packed;
         indexBits = lay.indexBits;
         keyBits = bitWidth(ctl->c.tile_max) + lowBits;
-    } else if (a.frameMode == 2) {  // binning mode's depth keys: W depth bits + the sentinel bit (+ the view)
+    } else if (a.frameMode == 2) {  // binning mode's depth keys: the depth offsets (+ the view)
         const uint32_t dmin = ctl->c.depth_min_bits, dmax = ctl->c.depth_max_bits;
         lowBits = 0;
         packed = 1;
         indexBits = a.indexBits;
-        depthBits = (dmin > dmax ? 0u : bitWidth(dmin ^ dmax)) + 1u;
+        depthMin = dmin > dmax ? 0u : dmin;
+        depthBits = dmin > dmax ? 0u : bitWidth(dmax - dmin);
         viewShift = a.viewBits ? a.indexBits + 32u : 0u;
         keyBits = depthBits + a.viewBits;
     } else {
@@ -156,7 +162,7 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
 #pragma unroll
         for (int j = 0; j < kHistItems; ++j) {
             if (base + j * 256 + threadIdx.x < entries) {
-                const uint64_t v = a.frameMode == 2 ? depthVirtualKey(k[j], indexBits, depthBits, viewShift)
+                const uint64_t v = a.frameMode == 2 ? depthVirtualKey(k[j], indexBits, depthBits, depthMin, viewShift)
                                    : packed          ? (k[j] >> indexBits)
                                                      : virtualKey(k[j], lowBits, keyMask);
                 for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][uint32_t(v >> (BITS * p)) & D::kMask], 1u);
@@ -212,6 +218,7 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
         plan->indexBits = indexBits;
         plan->digitBits = BITS;
         plan->depthBits = depthBits;
+        plan->depthMin = depthMin;
         plan->viewShift = viewShift;
         plan->sortedBuffer = activeCount & 1u;
         if (a.frameMode == 2) return;  // the list's own plan fills the control block
@@ -329,8 +336,10 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
     const uint64_t keyMask = maskOf(plan->keyBits);
     const uint32_t shift = BITS * p + (PAIRS || DEPTH ? 0u : plan->indexBits);
     const uint32_t indexBits = plan->indexBits, depthBits = plan->depthBits, viewShift = plan->viewShift;
+    const uint32_t depthMin = plan->depthMin;
     auto digit = [&](uint64_t k) -> uint32_t {
-        if constexpr (DEPTH) return uint32_t(depthVirtualKey(k, indexBits, depthBits, viewShift) >> shift) & D::kMask;
+        if constexpr (DEPTH)
+            return uint32_t(depthVirtualKey(k, indexBits, depthBits, depthMin, viewShift) >> shift) & D::kMask;
         return PAIRS ? uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & D::kMask : uint32_t(k >> shift) & D::kMask;
     };
 

@@ -121,7 +121,8 @@ struct SortPlan {
     uint32_t active[kMaxSortPasses];
     uint32_t inBuffer[kMaxSortPasses];
     uint32_t digitBits;     // digit width of the passes (7, 8 or 9)
-    uint32_t depthBits;     // the depth sort: varying depth bits + the sentinel bit of its virtual key
+    uint32_t depthBits;     // the depth sort: bits of (depth bits - depthMin) over the frame's visible records
+    uint32_t depthMin;      // the depth sort: the frame's smallest visible depth bits
     uint32_t viewShift;     // the depth sort: position of the view field in the words (0: none)
     uint32_t digitBase[kMaxSortPasses][kMaxSortBins];
     uint32_t hist[kMaxSortPasses][kMaxSortBins];
@@ -138,8 +139,9 @@ struct SortArgs {
     uint32_t passesLaunched;
     // plan source: frameMode = 1 derives the low bits from the frame's depth range and the high
     // bits from the largest tile id (binning = 1: tile-only keys, no depth bits); 2 = the depth
-    // keys of binning mode (packed, depth bits of the frame's range + the sentinel bit above a
-    // record index of indexBits); 0 uses fixedLowBits/fixedKeyBits (standalone sort).
+    // words of binning mode (the depth bits above a record index of indexBits, sorted by their
+    // offset from the frame's smallest visible depth bits); 0 uses fixedLowBits/fixedKeyBits
+    // (standalone sort).
     uint32_t frameMode;
     uint32_t fixedLowBits, fixedKeyBits;
     uint32_t tileCount, count;  // frame mode: the grid's tiles and N (for the entry layout)
