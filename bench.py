@@ -649,8 +649,8 @@ def render_issue(passes: dict, clocks: dict, instructions: float | None):
 
 # warp instructions (smsp__inst_executed.sum) of one 1080p view's render pass and preprocess,
 # from an ncu capture of this build (the plain profiling mode, two launches of each kernel)
-RENDER_WARP_INSTRUCTIONS_1080P = 227.6e6
-PREPROCESS_WARP_INSTRUCTIONS_1080P = 76.43e6
+RENDER_WARP_INSTRUCTIONS_1080P = 209.69e6
+PREPROCESS_WARP_INSTRUCTIONS_1080P = 75.17e6
 
 
 def issue_roofline(passes: dict, clocks: dict, views: int) -> dict | None:

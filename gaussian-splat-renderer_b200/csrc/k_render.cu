@@ -152,6 +152,7 @@ struct RenderShared {
     float4 power1[N];     // e, f, the sign-test bound, -
     uint32_t strips[N];   // the warp strips the cutoff ellipse meets (stripMask)
     float4 color[N];      // r, g, b, -
+    uint32_t hits[N / 32][32];  // per warp: the records of its current 32 that meet its strip, in list order
     uint32_t tile;        // persistent schedule: the block's current tile
 };
 
@@ -534,13 +535,20 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
         }
         __syncthreads();
         const uint32_t n = range.y - start < kThreads ? range.y - start : kThreads;
-        // the warp takes 32 records at a time, one per lane, and visits those that meet its strip
-        // in list order
+        // the warp takes 32 records at a time, one per lane, lists those that meet its strip in
+        // list order (each such lane writes its record at its rank among them) and visits the
+        // list: a load a record instead of finding and clearing the next set bit of the ballot
+        uint32_t* hits = sm.hits[warp];
+        const uint32_t below = (1u << lane) - 1u;
         for (uint32_t q0 = 0; q0 < n && !__all_sync(0xffffffffu, done); q0 += 32) {
             const uint32_t ql = q0 + lane;
             const bool hit = ql < n && ((sm.strips[ql] >> warp) & 1u) != 0u;
-            for (uint32_t m = __ballot_sync(0xffffffffu, hit); m != 0u; m &= m - 1u) {
-                const uint32_t q = q0 + uint32_t(__ffs(m)) - 1u;
+            const uint32_t m = __ballot_sync(0xffffffffu, hit);
+            if (hit) hits[__popc(m & below)] = ql;
+            __syncwarp();
+            const uint32_t listed = uint32_t(__popc(m));
+            for (uint32_t h = 0; h < listed; ++h) {
+                const uint32_t q = hits[h];
                 if constexpr (STATS) {
                     ++stIters;
                     stTested += done ? 0u : 1u;
@@ -577,6 +585,7 @@ __device__ __forceinline__ void renderTile(const RenderArgs& a, RenderShared<til
                 T = testT;
                 if constexpr (STATS) ++stBlend;
             }
+            __syncwarp();  // every lane has read the list before the next group writes it
         }
     }
     if constexpr (CAP > 0) {  // the end of the list: what waits is blended, nearest first
