@@ -327,9 +327,11 @@ PASS_NAMES = {"preprocess": "reset + preprocess (depth keys)", "depth sort": "de
               "scan + emission": "scan + duplicate (depth order)", "tile sort": "tile sort (total)",
               "ranges": "tile ranges"}
 
-# DRAM bytes of the same passes for one frame of plain_1080p, from one ncu capture of this
-# build (dram__bytes_read.sum + dram__bytes_write.sum); the bench cannot read the counters itself
-TRAFFIC_PLAIN_1080P_CAPTURE = (314.4 + 70.7 + 10.0 + 39.6 + 14.9 + 47.9 + 2.9) * 1e6
+# DRAM bytes of the same passes (preprocess to ranges) for one frame of plain_1080p, from one
+# ncu capture of this build (dram__bytes_read.sum + dram__bytes_write.sum: preprocess, depth
+# sort histogram and its 3 active passes, scan, emission, tile sort histogram and 2 passes,
+# ranges); the bench cannot read the counters itself
+TRAFFIC_PLAIN_1080P_CAPTURE = (315.3 + 70.7 + 10.0 + 3 * 10.0 + 14.9 + 48.8 + 3.2 + 41.5 + 41.7 + 41.6 + 41.5) * 1e6
 # the same for one batched frame of 8 views (preprocess, depth sort, scan, emission, tile sort,
 # ranges; the second tile-sort pass taken equal to the first, which the capture did not reach)
 TRAFFIC_BATCHED_1080P_CAPTURE: dict = {8: (469.7 + 747.5 + 79.6 + 4 * 79.4 + 121.7 + 135.4 + 675.5 + 332.2 +
