@@ -275,18 +275,12 @@ def workload(name: str):
 
 
 # ---- algorithmic bytes of the passes (binning list mode) ------------------------------------
-def depth_sort_passes(ctl, bits: int = 8, views: int = 1, records: int = 0) -> int:
+def depth_sort_passes(ctl, bits: int = 8) -> int:
     """Digit passes of the depth sort, `bits` a pass: the bits of the visible depths' offsets
-    from the frame's smallest (largest minus smallest depth bits), and above them the view field
-    of a frame of several views when the depth word has room for it (record bits + 32 + view
-    bits <= 64)."""
+    from the frame's smallest (largest minus smallest depth bits). Each view's records are sorted
+    as a run of their own, so the views of a batched frame add no pass."""
     lo, hi = ctl.depth_min_bits, ctl.depth_max_bits
     w = (hi - lo).bit_length() if lo <= hi else 0
-    if views > 1:
-        vb = (views - 1).bit_length()
-        rb = (records - 1).bit_length() if records > 1 else 1
-        if rb + 32 + vb <= 64:
-            w += vb
     return (w + bits - 1) // bits
 
 
@@ -316,7 +310,7 @@ def pass_bytes(scene_format: str, ctl, n: int, tiles: int, bits: int = 8, views:
     per_entry = 16 if ctl.packed_entries else 24
     return {
         "preprocess": float(pre),
-        "depth sort": float(8 * n + 16 * n * depth_sort_passes(ctl, bits, views, n)),
+        "depth sort": float(8 * n + 16 * n * depth_sort_passes(ctl, bits)),
         "scan + emission": float((8 + 4 + 4) * n + (8 + 4 + 4) * n + 16 * vis + 8 * m),
         "tile sort": float(8 * m + per_entry * m * ctl.sort_passes),
         "ranges": float(8 * m + 8 * tiles),

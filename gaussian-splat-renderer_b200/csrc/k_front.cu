@@ -696,11 +696,14 @@ __global__ void __launch_bounds__(kFrontThreads) duplicateKernel(const __grid_co
 
 // Per-frame reset of the control block (vkCmdUpdateBuffer of TileControl{N, 0, ...}) and of the
 // tile ranges (vkCmdFillBuffer 0), splat_tile_renderer.cpp:653-661. Block 0 resets the control
-// block and the sort histograms; every block zeroes a part of the ranges.
+// block and the sort histograms; every block zeroes a part of the ranges and of `clear` (the
+// depth sort's per-view digit counts).
 __global__ void frameBeginKernel(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint4* ranges,
-                                 uint32_t rangeVec4s, SortPlan* plan, uint32_t forceTimeout, SortPlan* plan2) {
+                                 uint32_t rangeVec4s, SortPlan* plan, uint32_t forceTimeout, SortPlan* plan2,
+                                 uint32_t* clear, uint32_t clearCount) {
     const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     for (uint32_t j = g; j < rangeVec4s; j += gridDim.x * blockDim.x) ranges[j] = make_uint4(0, 0, 0, 0);
+    for (uint32_t j = g; j < clearCount; j += gridDim.x * blockDim.x) clear[j] = 0;
     if (blockIdx.x != 0) return;
     SortPlan* plans[2] = {plan, plan2};
     for (int k = 0; k < 2; ++k) {
@@ -754,12 +757,13 @@ cudaError_t loadFrameBeginKernel() {
 
 cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint32_t* ranges,
                              uint32_t rangeWords, SortPlan* plan, uint32_t forceTimeout, cudaStream_t s,
-                             SortPlan* plan2) {
+                             SortPlan* plan2, uint32_t* clearWords, uint32_t clearCount) {
     const uint32_t vec4s = (rangeWords + 3) / 4;
-    uint32_t blocks = (vec4s + 255) / 256;
+    const uint32_t work = vec4s > clearCount ? vec4s : clearCount;
+    uint32_t blocks = (work + 255) / 256;
     blocks = blocks < 1 ? 1 : (blocks > 1184 ? 1184 : blocks);
     frameBeginKernel<<<blocks, 256, 0, s>>>(ctl, count, capacity, reinterpret_cast<uint4*>(ranges), vec4s, plan,
-                                             forceTimeout, plan2);
+                                             forceTimeout, plan2, clearWords, clearWords ? clearCount : 0u);
     return cudaGetLastError();
 }
 

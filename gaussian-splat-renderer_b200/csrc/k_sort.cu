@@ -40,17 +40,16 @@ __device__ __forceinline__ uint64_t virtualKey(uint64_t key, uint32_t lowBits, u
 __device__ __forceinline__ uint64_t maskOf(uint32_t bits) { return bits >= 64 ? ~0ull : ((1ull << bits) - 1ull); }
 
 // The depth sort's key of a depth word: its depth bits (above the record index) minus the
-// frame's smallest visible depth bits, in depthBits = bit_width(max - min) bits, with the view
-// (the word's field at viewShift, when there is one) right above them. Positive floats order like
-// their bits, so the offsets of the visible records order like their depths, and (view, depth)
-// costs no digit pass on the bits every real depth shares. (Offsets span fewer bits than the
+// frame's smallest visible depth bits, in depthBits = bit_width(max - min) bits. Positive floats
+// order like their bits, so the offsets of the visible records order like their depths, and no
+// digit pass is spent on the bits every real depth shares. (Offsets span fewer bits than the
 // bits where min and max differ: 24 against 25 for depths in [6, 22], one pass less at 8-bit
 // digits.) A record without tiles (all-ones depth bits) gets some key in the range: it emits no
-// entry, so where it sorts changes no offset and no list.
-__device__ __forceinline__ uint64_t depthVirtualKey(uint64_t word, uint32_t indexBits, uint32_t depthBits,
-                                                    uint32_t depthMin, uint32_t viewShift) {
-    const uint64_t depth = uint64_t(uint32_t(word >> indexBits) - depthMin) & maskOf(depthBits);
-    return viewShift ? ((word >> viewShift) << depthBits) | depth : depth;
+// entry, so where it sorts changes no offset and no list. The view is not part of the key: each
+// view's run of records is sorted on its own (SortArgs::segments).
+__device__ __forceinline__ uint32_t depthVirtualKey(uint64_t word, uint32_t indexBits, uint32_t depthBits,
+                                                    uint32_t depthMin) {
+    return (uint32_t(word >> indexBits) - depthMin) & uint32_t(maskOf(depthBits));
 }
 
 __device__ __forceinline__ uint32_t laneMaskLt() {
@@ -121,22 +120,22 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     __shared__ uint32_t sAny;
     DeviceControl* ctl = a.ctl;
     const uint32_t entries = a.frameMode == 2 ? a.count : ctl->c.entries;
-    uint32_t lowBits, keyBits, packed = 0, indexBits = 0, depthBits = 0, depthMin = 0, viewShift = 0;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t lowBits, keyBits, packed = 0, indexBits = 0, depthBits = 0, depthMin = 0;
     if (a.frameMode == 1) {
         const KeyLayout lay = keyLayout(ctl, a.tileCount, a.count, a.binning != 0);
         lowBits = lay.lowBits;
         packed = lay.packed;
         indexBits = lay.indexBits;
         keyBits = bitWidth(ctl->c.tile_max) + lowBits;
-    } else if (a.frameMode == 2) {  // binning mode's depth keys: the depth offsets (+ the view)
+    } else if (a.frameMode == 2) {  // binning mode's depth keys: the depth offsets, each view's run apart
         const uint32_t dmin = ctl->c.depth_min_bits, dmax = ctl->c.depth_max_bits;
         lowBits = 0;
         packed = 1;
         indexBits = a.indexBits;
         depthMin = dmin > dmax ? 0u : dmin;
         depthBits = dmin > dmax ? 0u : bitWidth(dmax - dmin);
-        viewShift = a.viewBits ? a.indexBits + 32u : 0u;
-        keyBits = depthBits + a.viewBits;
+        keyBits = depthBits;
     } else {
         lowBits = a.fixedLowBits;
         keyBits = a.fixedKeyBits;
@@ -152,29 +151,75 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     const uint64_t* keys = a.keys[0];
     // kHistItems independent loads per thread in flight before the counting
     constexpr uint32_t kChunk = 256 * kHistItems;
-    for (uint32_t base = blockIdx.x * kChunk; base < entries; base += gridDim.x * kChunk) {
-        uint64_t k[kHistItems];
+    static_assert(kChunk == kDepthSortTile, "a depth histogram chunk is one depth sort tile");
+    if (a.frameMode == 2) {
+        // the depth words, one view's run at a time: a block takes a contiguous share of the runs'
+        // tiles (none straddles two runs) and adds its counts to the run's histogram whenever the
+        // run changes, and at the end
+        const uint32_t tilesPerRun = (a.segLength + kChunk - 1) / kChunk;
+        const uint32_t chunks = tilesPerRun * a.segments;
+        const uint32_t per = (chunks + gridDim.x - 1) / gridDim.x;
+        const uint32_t c0 = blockIdx.x * per, c1 = c0 + per < chunks ? c0 + per : chunks;
+        auto flushRun = [&](uint32_t run) {
+            for (uint32_t p = 0; p < passes; ++p)
+                for (uint32_t d = threadIdx.x; d < uint32_t(D::kBins); d += 256) {
+                    const uint32_t c = sHist[p][d];
+                    if (c) {
+                        atomicAdd(&a.segHist[(size_t(run) * a.passesLaunched + p) * D::kBins + d], c);
+                        sHist[p][d] = 0;
+                    }
+                }
+        };
+        uint32_t run = c0 < c1 ? c0 / tilesPerRun : 0u;
+        for (uint32_t c = c0; c < c1; ++c) {
+            const uint32_t v = c / tilesPerRun;  // the same in every thread
+            if (v != run) {
+                __syncthreads();
+                flushRun(run);
+                __syncthreads();
+                run = v;
+            }
+            const uint32_t runEnd = (v + 1) * a.segLength;
+            const uint32_t base = v * a.segLength + (c - v * tilesPerRun) * kChunk;
+            uint64_t k[kHistItems];
 #pragma unroll
-        for (int j = 0; j < kHistItems; ++j) {
-            const uint32_t idx = base + j * 256 + threadIdx.x;
-            k[j] = idx < entries ? __ldg(&keys[idx]) : 0ull;
-        }
+            for (int j = 0; j < kHistItems; ++j) {
+                const uint32_t idx = base + j * 256 + threadIdx.x;
+                k[j] = idx < runEnd ? __ldg(&keys[idx]) : 0ull;
+            }
 #pragma unroll
-        for (int j = 0; j < kHistItems; ++j) {
-            if (base + j * 256 + threadIdx.x < entries) {
-                const uint64_t v = a.frameMode == 2 ? depthVirtualKey(k[j], indexBits, depthBits, depthMin, viewShift)
-                                   : packed          ? (k[j] >> indexBits)
-                                                     : virtualKey(k[j], lowBits, keyMask);
-                for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][uint32_t(v >> (BITS * p)) & D::kMask], 1u);
+            for (int j = 0; j < kHistItems; ++j) {
+                if (base + j * 256 + threadIdx.x < runEnd) {
+                    const uint32_t v2 = depthVirtualKey(k[j], indexBits, depthBits, depthMin);
+                    for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][(v2 >> (BITS * p)) & D::kMask], 1u);
+                }
             }
         }
-    }
-    __syncthreads();
-    for (uint32_t p = 0; p < passes; ++p)
-        for (uint32_t d = threadIdx.x; d < uint32_t(D::kBins); d += 256) {
-            const uint32_t c = sHist[p][d];
-            if (c) atomicAdd(&a.plan->hist[p][d], c);
+        __syncthreads();
+        if (c0 < c1) flushRun(run);
+    } else {
+        for (uint32_t base = blockIdx.x * kChunk; base < entries; base += gridDim.x * kChunk) {
+            uint64_t k[kHistItems];
+#pragma unroll
+            for (int j = 0; j < kHistItems; ++j) {
+                const uint32_t idx = base + j * 256 + threadIdx.x;
+                k[j] = idx < entries ? __ldg(&keys[idx]) : 0ull;
+            }
+#pragma unroll
+            for (int j = 0; j < kHistItems; ++j) {
+                if (base + j * 256 + threadIdx.x < entries) {
+                    const uint64_t v = packed ? (k[j] >> indexBits) : virtualKey(k[j], lowBits, keyMask);
+                    for (uint32_t p = 0; p < passes; ++p) atomicAdd(&sHist[p][uint32_t(v >> (BITS * p)) & D::kMask], 1u);
+                }
+            }
         }
+        __syncthreads();
+        for (uint32_t p = 0; p < passes; ++p)
+            for (uint32_t d = threadIdx.x; d < uint32_t(D::kBins); d += 256) {
+                const uint32_t c = sHist[p][d];
+                if (c) atomicAdd(&a.plan->hist[p][d], c);
+            }
+    }
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) sLast = atomicAdd(&ctl->histDone[a.frameMode == 2 ? 1 : 0], 1u) == gridDim.x - 1;
@@ -185,24 +230,59 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
     SortPlan* plan = a.plan;
     uint32_t activeCount = 0;
     for (uint32_t p = 0; p < kMaxSortPasses; ++p) {
-        uint32_t c[D::kPerThread];
+        bool active;
+        if (a.frameMode == 2) {
+            // each warp scans the runs warp, warp + 8, ...: the run's digit bases start at its first
+            // record; the pass is needed unless, in every run, one digit holds all of its keys
+            constexpr int kPerLane = D::kBins / 32;
+            if (threadIdx.x == 0) sAny = 0;
+            __syncthreads();
+            for (uint32_t v = warp; p < passes && v < a.segments; v += 8) {
+                const size_t at = (size_t(v) * a.passesLaunched + p) * D::kBins + lane * kPerLane;
+                uint32_t c[kPerLane], sum = 0;
+                bool whole = false;
 #pragma unroll
-        for (int q = 0; q < D::kPerThread; ++q) {
-            const uint32_t d = D::of(q);
-            c[q] = p < passes && d < uint32_t(D::kBins) ? ldAcquire32(&plan->hist[p][d]) : 0u;
+                for (int q = 0; q < kPerLane; ++q) {
+                    c[q] = ldAcquire32(&a.segHist[at + q]);
+                    whole |= c[q] == a.segLength;
+                    sum += c[q];
+                }
+                uint32_t incl = sum;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+                    if (lane >= uint32_t(o)) incl += t;
+                }
+                uint32_t base = v * a.segLength + incl - sum;
+#pragma unroll
+                for (int q = 0; q < kPerLane; ++q) {
+                    a.segBase[at + q] = base;
+                    base += c[q];
+                }
+                if (!__any_sync(0xFFFFFFFFu, whole) && lane == 0) sAny = 1;
+            }
+            __syncthreads();
+            active = p < passes && sAny;
+        } else {
+            uint32_t c[D::kPerThread];
+#pragma unroll
+            for (int q = 0; q < D::kPerThread; ++q) {
+                const uint32_t d = D::of(q);
+                c[q] = p < passes && d < uint32_t(D::kBins) ? ldAcquire32(&plan->hist[p][d]) : 0u;
+            }
+            if (threadIdx.x == 0) sAny = 0;
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < D::kPerThread; ++q)
+                if (p < passes && D::of(q) < uint32_t(D::kBins) && c[q] == entries) sAny = 1;  // one digit holds every key
+            __syncthreads();
+            active = p < passes && !sAny;
+            uint32_t excl[D::kPerThread];
+            blockScanDigits<BITS>(c, excl, sWarp);
+#pragma unroll
+            for (int q = 0; q < D::kPerThread; ++q)
+                if (D::of(q) < uint32_t(D::kBins)) plan->digitBase[p][D::of(q)] = excl[q];
         }
-        if (threadIdx.x == 0) sAny = 0;
-        __syncthreads();
-#pragma unroll
-        for (int q = 0; q < D::kPerThread; ++q)
-            if (p < passes && D::of(q) < uint32_t(D::kBins) && c[q] == entries) sAny = 1;  // one digit holds every key
-        __syncthreads();
-        const bool active = p < passes && !sAny;
-        uint32_t excl[D::kPerThread];
-        blockScanDigits<BITS>(c, excl, sWarp);
-#pragma unroll
-        for (int q = 0; q < D::kPerThread; ++q)
-            if (D::of(q) < uint32_t(D::kBins)) plan->digitBase[p][D::of(q)] = excl[q];
         if (threadIdx.x == 0) {
             plan->active[p] = active ? 1u : 0u;
             plan->inBuffer[p] = activeCount & 1u;
@@ -219,7 +299,6 @@ __global__ void __launch_bounds__(256) sortHistKernel(const __grid_constant__ So
         plan->digitBits = BITS;
         plan->depthBits = depthBits;
         plan->depthMin = depthMin;
-        plan->viewShift = viewShift;
         plan->sortedBuffer = activeCount & 1u;
         if (a.frameMode == 2) return;  // the list's own plan fills the control block
         ctl->c.packed_entries = packed;
@@ -325,8 +404,25 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
     for (int j = 0; j < 24 * kBins / 256; ++j) sWarpCnt[j * 256 + tid] = 0;
     __syncthreads();
     const uint32_t t = sTile;
-    const uint32_t tileBase = t * kTile;
-    if (tileBase >= entries || t >= a.maxTiles) return;
+    // the tile's keys [tileBase, tileEnd), and whether it starts its look-back chains (the list's
+    // first tile; in the depth sort, the first tile of its view's run, whose digits start at the
+    // run's first record)
+    uint32_t tileBase, tileEnd, seg = 0;
+    bool first;
+    if constexpr (DEPTH) {
+        const uint32_t tilesPerRun = (a.segLength + kTile - 1) / kTile;
+        if (t >= tilesPerRun * a.segments || t >= a.maxTiles) return;
+        seg = t / tilesPerRun;
+        const uint32_t local = t - seg * tilesPerRun;
+        tileBase = seg * a.segLength + local * kTile;
+        tileEnd = tileBase + kTile < (seg + 1) * a.segLength ? tileBase + kTile : (seg + 1) * a.segLength;
+        first = local == 0;
+    } else {
+        tileBase = t * kTile;
+        if (tileBase >= entries || t >= a.maxTiles) return;
+        tileEnd = entries;
+        first = t == 0;
+    }
     const uint32_t in = plan->inBuffer[p];
     const uint64_t* keysIn = a.keys[in];
     const uint32_t* valsIn = a.values[in];
@@ -335,11 +431,9 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
     const uint32_t lowBits = plan->lowBits;
     const uint64_t keyMask = maskOf(plan->keyBits);
     const uint32_t shift = BITS * p + (PAIRS || DEPTH ? 0u : plan->indexBits);
-    const uint32_t indexBits = plan->indexBits, depthBits = plan->depthBits, viewShift = plan->viewShift;
-    const uint32_t depthMin = plan->depthMin;
+    const uint32_t indexBits = plan->indexBits, depthBits = plan->depthBits, depthMin = plan->depthMin;
     auto digit = [&](uint64_t k) -> uint32_t {
-        if constexpr (DEPTH)
-            return uint32_t(depthVirtualKey(k, indexBits, depthBits, depthMin, viewShift) >> shift) & D::kMask;
+        if constexpr (DEPTH) return (depthVirtualKey(k, indexBits, depthBits, depthMin) >> shift) & D::kMask;
         return PAIRS ? uint32_t(virtualKey(k, lowBits, keyMask) >> shift) & D::kMask : uint32_t(k >> shift) & D::kMask;
     };
 
@@ -350,13 +444,13 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
 #pragma unroll
     for (int j = 0; j < kItems; ++j) {
         const uint32_t idx = itemBase + j * 32;
-        key[j] = idx < entries ? __ldg(&keysIn[idx]) : ~0ull;
-        if (PAIRS) val[PAIRS ? j : 0] = idx < entries ? __ldg(&valsIn[idx]) : 0u;
+        key[j] = idx < tileEnd ? __ldg(&keysIn[idx]) : ~0ull;
+        if (PAIRS) val[PAIRS ? j : 0] = idx < tileEnd ? __ldg(&valsIn[idx]) : 0u;
     }
     uint32_t* wc = sWarpCnt + warp * kBins;
 #pragma unroll
     for (int j = 0; j < kItems; ++j)
-        if (itemBase + j * 32 < entries) atomicAdd(&wc[digit(key[j])], 1u);
+        if (itemBase + j * 32 < tileEnd) atomicAdd(&wc[digit(key[j])], 1u);
     __syncthreads();
     const uint32_t epoch = ctl->c.epoch;
     uint64_t* status = a.status + (size_t(p) * a.maxTiles) * kBins;
@@ -372,7 +466,7 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
             sWarpCnt[w * kBins + d] = blockCount[q];
             blockCount[q] += c;
         }
-        stRelaxed(&status[size_t(t) * kBins + d], packStatus(epoch, t == 0 ? kFlagInclusive : kFlagAggregate, blockCount[q]));
+        stRelaxed(&status[size_t(t) * kBins + d], packStatus(epoch, first ? kFlagInclusive : kFlagAggregate, blockCount[q]));
     }
     uint32_t blockStart[P];
     blockScanDigits<BITS>(blockCount, blockStart, sScan);
@@ -402,7 +496,7 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
         prevDigit = dj;
         prevLeader = below == 0;
         const uint32_t pos = run + __popc(below);
-        if (itemBase + j * 32 < entries) {
+        if (itemBase + j * 32 < tileEnd) {
             sKeys[pos] = key[j];
             if (PAIRS) sVals[pos] = val[PAIRS ? j : 0];
         }
@@ -416,16 +510,18 @@ __device__ __forceinline__ void sortPassTiles(const SortArgs& a, uint32_t p, uns
         const uint32_t d = D::of(q);
         if (d >= uint32_t(kBins)) continue;
         uint32_t exclusive = 0;
-        if (t > 0) {
+        if (!first) {  // a chain ends at the first inclusive status: the run's (or the list's) first tile
             exclusive = digitLookback<kBins>(status, t, d, epoch, ctl);
             stRelaxed(&status[size_t(t) * kBins + d], packStatus(epoch, kFlagInclusive, exclusive + blockCount[q]));
         }
-        sOff[d] = plan->digitBase[p][d] + exclusive - blockStart[q];
+        const uint32_t digitBase =
+            DEPTH ? a.segBase[(size_t(seg) * a.passesLaunched + p) * kBins + d] : plan->digitBase[p][d];
+        sOff[d] = digitBase + exclusive - blockStart[q];
     }
     __syncthreads();
 
     // 4) write-out
-    const uint32_t n = entries - tileBase < uint32_t(kTile) ? entries - tileBase : uint32_t(kTile);
+    const uint32_t n = tileEnd - tileBase < uint32_t(kTile) ? tileEnd - tileBase : uint32_t(kTile);
 #pragma unroll 4
     for (uint32_t k = tid; k < n; k += kSortThreads) {
         const uint64_t kk = sKeys[k];

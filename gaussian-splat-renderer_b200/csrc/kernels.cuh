@@ -123,7 +123,6 @@ struct SortPlan {
     uint32_t digitBits;     // digit width of the passes (7, 8 or 9)
     uint32_t depthBits;     // the depth sort: bits of (depth bits - depthMin) over the frame's visible records
     uint32_t depthMin;      // the depth sort: the frame's smallest visible depth bits
-    uint32_t viewShift;     // the depth sort: position of the view field in the words (0: none)
     uint32_t digitBase[kMaxSortPasses][kMaxSortBins];
     uint32_t hist[kMaxSortPasses][kMaxSortBins];
     uint32_t sortedBuffer;  // the buffer that holds the result (active passes mod 2)
@@ -139,16 +138,23 @@ struct SortArgs {
     uint32_t passesLaunched;
     // plan source: frameMode = 1 derives the low bits from the frame's depth range and the high
     // bits from the largest tile id (binning = 1: tile-only keys, no depth bits); 2 = the depth
-    // words of binning mode (the depth bits above a record index of indexBits, sorted by their
-    // offset from the frame's smallest visible depth bits); 0 uses fixedLowBits/fixedKeyBits
-    // (standalone sort).
+    // words of binning mode (the depth bits above a record index of indexBits, each view's run
+    // sorted by their offset from the frame's smallest visible depth bits); 0 uses
+    // fixedLowBits/fixedKeyBits (standalone sort).
     uint32_t frameMode;
     uint32_t fixedLowBits, fixedKeyBits;
     uint32_t tileCount, count;  // frame mode: the grid's tiles and N (for the entry layout)
     uint32_t binning;
     uint32_t indexBits;         // frameMode 2: bits of the record index
     uint32_t digitBits;         // 7, 8 or 9 bits a pass
-    uint32_t viewBits;          // frameMode 2: bits of the view field above the depth bits (0: none)
+    // frameMode 2: the records are `segments` runs of segLength (one view's records each, in view
+    // order), sorted each on its own: tiles never straddle two runs (tile t is tile t mod
+    // ceil(segLength / tile) of run t / ceil(segLength / tile)), a run's first tile starts its
+    // look-back chains, and its digits start at the run's first record. segHist / segBase:
+    // [segments][passesLaunched][1 << digitBits] digit counts (zeroed by frameBegin) and bases.
+    uint32_t segments, segLength;
+    uint32_t* segHist;
+    uint32_t* segBase;
 };
 
 struct RenderArgs {
@@ -188,7 +194,7 @@ constexpr uint32_t kTileStatListLength = 0, kTileStatFetched = 1, kTileStatEvalu
 // ---- launchers (return cudaGetLastError()) ---------------------------------------------------
 cudaError_t launchFrameBegin(DeviceControl* ctl, uint32_t count, uint32_t capacity, uint32_t* ranges,
                              uint32_t rangeWords, SortPlan* plan, uint32_t forceTimeout, cudaStream_t s,
-                             SortPlan* plan2 = nullptr);
+                             SortPlan* plan2 = nullptr, uint32_t* clearWords = nullptr, uint32_t clearCount = 0);
 cudaError_t launchFront(const FrontArgs& a, uint32_t geometry, uint32_t color, cudaStream_t s);
 // Binning mode, split around the depth sort: preprocess + the depth keys, then (after the sort of
 // the depth keys) the scan of the counts in depth order and the emission in that order.

@@ -449,6 +449,8 @@ struct GsrRenderer {
     DevBuf control, plan;
     // binning mode: the records' depth words (ping-pong), their sort's look-back words and plan
     DevBuf depthKeys[2], depthStatus, depthPlan;
+    // the depth sort's per-view digit counts and bases, [views][depthPasses()][1 << digitBits] each
+    DevBuf depthRuns;
     bool binning() const { return settings.list_mode == GSR_LIST_BINNING; }
     // the radix digit width of both sorts, and the depth sort's passes: its keys are the varying
     // depth bits and the no-tile bit, at most 32 bits (depths are positive floats)
@@ -465,10 +467,15 @@ struct GsrRenderer {
         const uint32_t rb = n > 1 ? bitWidth(uint32_t(n - 1)) : 1u, vb = bitWidth(uint32_t(v - 1));
         return rb + 32u + vb <= 64u ? vb : 0u;
     }
-    // Passes launched for the depth sort: the depth word's 32 bits and the view bits (the plan
-    // skips the ones the frame's depth range does not need)
-    uint32_t depthPasses(size_t v) const { return (32u + depthViewBits(v) + digitBits() - 1u) / digitBits(); }
-    uint32_t depthPasses() const { return depthPasses(std::max<size_t>(views.size(), 1)); }
+    // Passes launched for the depth sort: the depth word's 32 bits (the plan skips the ones the
+    // frame's depth range does not need); each view's records are sorted as a run of their own,
+    // so the view costs no pass
+    uint32_t depthPasses() const { return (32u + digitBits() - 1u) / digitBits(); }
+    // its tiles: each view's run of N records in ceil(N / tile) tiles (none straddles two views)
+    uint32_t depthTiles(size_t v) const {
+        return uint32_t(v * ((size_t(scene.count) + kDepthSortTile - 1) / kDepthSortTile));
+    }
+    uint32_t depthRunWords(size_t v) const { return uint32_t(v * depthPasses() * statusWordsPerTile()); }
     size_t statusWordsPerTile() const { return size_t(1) << digitBits(); }
     // the output image: bytes per pixel, the kernel's format code, and the RGB8 companion
     uint32_t imageBytes() const {
@@ -676,9 +683,10 @@ struct GsrRenderer {
         if (tcDecode()) GSR_CUDA(decodedColours.alloc(n * 16));
         if (binning()) {
             for (auto& k : depthKeys) GSR_CUDA(k.alloc(n * 8));
-            GSR_CUDA(depthStatus.alloc(size_t(depthPasses(v)) * ((n + kDepthSortTile - 1) / kDepthSortTile) *
-                                       statusWordsPerTile() * 8));
+            GSR_CUDA(depthStatus.alloc(size_t(depthPasses()) * depthTiles(v) * statusWordsPerTile() * 8));
             GSR_CUDA(cudaMemset(depthStatus.p, 0, depthStatus.bytes));
+            GSR_CUDA(depthRuns.alloc(size_t(depthRunWords(v)) * 2 * 4));
+            GSR_CUDA(cudaMemset(depthRuns.p, 0, depthRuns.bytes));
         }
         GSR_CUDA(tileCounts.alloc(n * 4));
         GSR_CUDA(offsets.alloc(n * 4));
@@ -924,7 +932,9 @@ struct GsrRenderer {
         GSR_CUDA(cudaMemcpyAsync(slot.camDevice.p, slot.camHost, sizeof(DevCameraArgs) * viewCount,
                                  cudaMemcpyHostToDevice, stream));
         GSR_CUDA(launchFrameBegin(ctl, scene.count * viewCount, l.capacity, ranges.as<uint32_t>(), tileCount * 2,
-                                  sortPlan, forceTimeout, stream, binning() ? depthPlan.as<SortPlan>() : nullptr));
+                                  sortPlan, forceTimeout, stream, binning() ? depthPlan.as<SortPlan>() : nullptr,
+                                  binning() ? depthRuns.as<uint32_t>() : nullptr,
+                                  binning() ? depthRunWords(viewCount) : 0u));
         FrontArgs fa{};
         fa.cam = slot.camDevice.as<DevCameraArgs>();
         fa.views = viewsDevice.as<DevView>();
@@ -965,12 +975,13 @@ struct GsrRenderer {
             fa.depthViewShift = viewBits ? fa.recordBits + 32u : 0u;
             GSR_CUDA(launchFrontBinningKeys(fa, scene.geometry, scene.color, stream));
             mark(stream);
-            // the records by (depth, record index): 32 depth bits above the record index
+            // each view's records by (depth, record index): 32 depth bits above the record index,
+            // the views' runs sorted side by side in one launch per pass
             SortArgs sd{};
             sd.keys[0] = fa.depthKeys[0];
             sd.keys[1] = fa.depthKeys[1];
             sd.status = depthStatus.as<uint64_t>();
-            sd.maxTiles = uint32_t((size_t(scene.count) * viewCount + kDepthSortTile - 1) / kDepthSortTile);
+            sd.maxTiles = depthTiles(viewCount);
             sd.plan = depthPlan.as<SortPlan>();
             sd.ctl = ctl;
             sd.passesLaunched = depthPasses();
@@ -978,7 +989,10 @@ struct GsrRenderer {
             sd.frameMode = 2;
             sd.count = scene.count * viewCount;
             sd.indexBits = fa.recordBits;
-            sd.viewBits = viewBits;
+            sd.segments = viewCount;
+            sd.segLength = scene.count;
+            sd.segHist = depthRuns.as<uint32_t>();
+            sd.segBase = depthRuns.as<uint32_t>() + depthRunWords(allocViews);
             GSR_CUDA(launchSort(sd, 148 * 2, stream));
             mark(stream);
             GSR_CUDA(launchFrontBinningEmit(fa, stream));

@@ -136,14 +136,12 @@ def test_pass_bytes_model():
     assert one["ranges"] == 8 * entries + 8 * 120
     four = bench.pass_bytes("f32", ctl, 4 * n, 480, views=4)
     assert four["preprocess"] == 240 * n + 12 * 4 * n + 64 * vis
-    assert four["depth sort"] == 8 * 4 * n + 16 * 4 * n * bench.depth_sort_passes(ctl, 8, 4, 4 * n)
+    assert four["depth sort"] == 8 * 4 * n + 16 * 4 * n * bench.depth_sort_passes(ctl)
     assert bench.pass_bytes("f16", ctl, 4 * n, 480, views=4)["preprocess"] == 128 * n + 48 * n + 64 * vis
     # the depth sort's passes, `bits` a pass: the bits of the depth offsets from the smallest
-    # (0x41000000 - 0x40000000 = 2^24: 25 bits), and the view field above them
+    # (0x41000000 - 0x40000000 = 2^24: 25 bits); views add none (each view's run sorted apart)
     assert bench.depth_sort_passes(ctl, 8) == 4 and bench.depth_sort_passes(ctl, 9) == 3
-    assert bench.depth_sort_passes(ctl, 8, 4, 4 * n) == 4 and bench.depth_sort_passes(ctl, 9, 4, 4 * n) == 3
-    assert bench.depth_sort_passes(ctl, 8, 16, 16 * n) == 4 and bench.depth_sort_passes(ctl, 9, 16, 16 * n) == 4
     # depths in [6, 22]: offsets below 0xF00000 (24 bits, 3 passes of 8) where the bits that
     # differ between min and max are 25
     near = types.SimpleNamespace(depth_min_bits=0x40C00000, depth_max_bits=0x41B00000)
-    assert bench.depth_sort_passes(near, 8) == 3 and bench.depth_sort_passes(near, 8, 8, 8 * n) == 4
+    assert bench.depth_sort_passes(near, 8) == 3 and bench.depth_sort_passes(near, 7) == 4
