@@ -162,8 +162,10 @@ typedef struct GsrSettings {
                                           0 = off (the list's order), 1..64 */
     uint32_t sort_digit_bits;          /* radix digit width of the depth and list sorts: 7, 8 or 9 bits
                                           a pass; 0 = 8 (the reference's GpuRadixSort digits,
-                                          gpu_radix_sort.h:38-122). 9 bits sort a 1080p frame's
-                                          25-bit depth keys in 3 passes instead of 4 */
+                                          gpu_radix_sort.h:38-122). The depth keys are the depth
+                                          offsets from the frame's nearest record (24 bits on a
+                                          1080p orbit: 3 passes of 8 bits); 9 bits sort keys of
+                                          25-27 bits in 3 passes where 8 bits need 4 */
     uint32_t tile_stats;               /* 1: the instrumented rasterizer with per-tile statistics
                                           (TileSettings::stats, splat_tile_renderer.h:102); not with
                                           sort_window; read with gsr_read_tile_stats */
