@@ -326,10 +326,10 @@ PASS_NAMES = {"preprocess": "reset + preprocess (depth keys)", "depth sort": "de
 # sort histogram and its 3 active passes, scan, emission, tile sort histogram and 2 passes,
 # ranges); the bench cannot read the counters itself
 TRAFFIC_PLAIN_1080P_CAPTURE = (315.3 + 70.7 + 10.0 + 3 * 10.0 + 14.9 + 48.8 + 3.2 + 41.5 + 41.7 + 41.6 + 41.5) * 1e6
-# the same for one batched frame of 8 views (preprocess, depth sort, scan, emission, tile sort,
-# ranges; the second tile-sort pass taken equal to the first, which the capture did not reach)
-TRAFFIC_BATCHED_1080P_CAPTURE: dict = {8: (469.7 + 747.5 + 79.6 + 4 * 79.4 + 121.7 + 135.4 + 675.5 + 332.2 +
-                                           2 * (332.3 + 290.6) + 335.9) * 1e6}
+# the same for one batched frame of 8 views (preprocess, depth sort histogram and its 3 active
+# passes, scan, emission, tile sort histogram and 2 passes, ranges)
+TRAFFIC_BATCHED_1080P_CAPTURE: dict = {8: (471.2 + 750.4 + 79.5 + 3 * 79.4 + 90.2 + 135.7 + 676.3 + 332.4 +
+                                           (332.2 + 291.0) + (332.2 + 291.3) + 332.8) * 1e6}
 
 
 # ---- the CPU leg: the reference's renderer as the baseline and as the checker of the GPU's views
